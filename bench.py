@@ -1,0 +1,433 @@
+"""Benchmark of the batched cloth VBD step on B200.
+
+Workload (default): 4,096 independent cloth instances, grid side n ~ U{16..128} vertices from a seed,
+1 m x 1 m each, per-instance Young's modulus log-uniform in [1e3, 1e6] Pa (nu = 0.3, thickness 1e-3 m,
+Lame mu = E h / (2 (1 + nu)), lambda = E h nu / (1 - nu^2)), bending stiffness log-uniform in
+[1e-5, 1e-3], 1-4 random pinned corners, 0.2 kg/m^2, a ground plane, gravity -9.81, dt = 1/600 s,
+10 VBD iterations per substep, FP32, one persistent launch per substep replayed from a CUDA graph.
+A "step" is one substep of the whole batch. Inputs are synthetic (seeded); the working set
+(~10 GB) is far larger than the 126 MB L2, so no flush is needed between steps.
+
+metric: vertex-iterations/s = sum_i V_i x iterations x substeps / time of the solve (forward step,
+all iterations, velocity update). Particle-shape contact generation runs every step before the
+solve; it is timed separately and the rate including it is reported as well.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--instances 4096]
+
+--impl reference times the CPU implementation of the same step (the oracle restatement of the
+reference's SolverVBD, OpenMP over the vertices of a color, all host threads) on a bounded sample
+of the same instances.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "VBD vertex-iters/s on 1 B200, batched FP32 vs plain; pos err <=1e-4 vs FP64"
+UNIT = "vertex-iters/s"
+ITERATIONS = 10
+DT = 1.0 / 600.0
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def instance_params(seed: int, count: int):
+    rng = np.random.default_rng(seed)
+    sides = rng.integers(16, 129, size=count)
+    E = 10.0 ** rng.uniform(3.0, 6.0, size=count)
+    bend = 10.0 ** rng.uniform(-5.0, -3.0, size=count)
+    pins = [rng.choice(4, size=int(rng.integers(1, 5)), replace=False) for _ in range(count)]
+    return sides, E, bend, pins
+
+
+def build_instance(n, E, bend, pins, world_index):
+    from newton_chysx_b200 import sim
+
+    nu, h, density = 0.3, 1.0e-3, 0.2
+    mu = E * h / (2.0 * (1.0 + nu))
+    lam = E * h * nu / (1.0 - nu * nu)
+    b = sim.ModelBuilder(up_axis="Z", gravity=-9.81)
+    cell = 1.0 / (n - 1)
+    col, row = world_index % 64, world_index // 64
+    b.add_cloth_grid(pos=(1.5 * col, 1.5 * row, 0.6), rot=sim.quat_identity(), vel=(0.0, 0.0, 0.0), dim_x=n - 1,
+                     dim_y=n - 1, cell_x=cell, cell_y=cell, mass=density / (n * n), tri_ke=mu, tri_ka=lam, tri_kd=0.0,
+                     edge_ke=bend, edge_kd=0.0, particle_radius=5.0e-3)  # fmt: skip
+    corners = [0, n - 1, n * (n - 1), n * n - 1]
+    flags = b.particle_flags
+    for c in pins:
+        flags[corners[int(c)]] &= ~1
+    b.set_particle_flags(flags)
+    b.color(include_bending=True)
+    return b
+
+
+def _instance_from_template(tpl, n, E, bend, pins, world_index):
+    """A copy of the side-n template builder with this instance's materials, pins and placement.
+
+    Topology, rest poses, areas, rest angles and the coloring depend only on n (materials scale
+    the triangle/hinge stiffnesses but never zero them, so the coloring graph is unchanged)."""
+    import copy
+
+    nu, h = 0.3, 1.0e-3
+    mu = E * h / (2.0 * (1.0 + nu))
+    lam = E * h * nu / (1.0 - nu * nu)
+    b = copy.copy(tpl)
+    mats = tpl.tri_materials.copy()
+    mats[:, 0], mats[:, 1] = mu, lam
+    b._tri_mat = [mats]
+    props = tpl.edge_bending_properties.copy()
+    props[:, 0] = bend
+    b._edge_prop = [props]
+    col, row = world_index % 64, world_index // 64
+    b._q = [tpl.particle_q + np.array([1.5 * col, 1.5 * row, 0.0])]
+    flags = tpl.particle_flags.copy()
+    corners = [0, n - 1, n * (n - 1), n * n - 1]
+    for c in pins:
+        flags[corners[int(c)]] &= ~1
+    b._flags = [flags]
+    return b
+
+
+def build_batch(seed: int, count: int):
+    from newton_chysx_b200 import sim
+
+    sides, E, bend, pins = instance_params(seed, count)
+    templates = {int(n): build_instance(int(n), 1.0e4, 1.0e-4, [], 0) for n in np.unique(sides)}
+    top = sim.ModelBuilder(up_axis="Z", gravity=-9.81)
+    for i in range(count):
+        n = int(sides[i])
+        top.add_world(_instance_from_template(templates[n], n, float(E[i]), float(bend[i]), pins[i], i))
+    top.add_ground_plane()
+    return top, sides
+
+
+def bytes_per_vertex_iteration(V, T, E, contacts=True):
+    """Algorithmic bytes of one colour sweep (92 V + 68 T + 64 E + 96 V with contacts) per vertex."""
+    return (92.0 * V + 68.0 * T + 64.0 * E + (96.0 * V if contacts else 0.0)) / V
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")  # fmt: skip
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
+                                 f".clocks_{os.getpid()}.csv")  # fmt: skip
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)  # fmt: skip
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+            os.remove(self.path)
+        except Exception:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if len(r) >= 9]
+        smax = [float(r[2]) for r in rows if len(r) >= 9]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows if len(r) >= 9 for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(sm)}  # fmt: skip
+
+
+def run_ours(args):
+    import torch
+
+    import newton_chysx_b200 as nb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    t0 = time.time()
+    builder, sides = build_batch(args.seed + rank, args.instances)
+    model = builder.finalize(dev)
+    model.soft_contact_ke, model.soft_contact_kd, model.soft_contact_mu = 1.0e3, 10.0, 0.5
+    solver = nb.SolverVBD(model, iterations=ITERATIONS, schedule="persistent", lanes_per_vertex=args.lanes,
+                          block_size=args.block)  # fmt: skip
+    pipe = nb.CollisionPipeline(model, soft_contact_margin=0.01)
+    contacts = pipe.contacts()
+    setup_s = time.time() - t0
+    V, T, E = model.particle_count, model.tri_count, model.edge_count
+    states = [model.state(), model.state()]
+
+    # settle the batch for a few substeps so that contacts and motion are present, then capture
+    for k in range(max(args.warmup, 3)):
+        pipe.collide(states[k % 2], contacts)
+        solver.step(states[k % 2], states[(k + 1) % 2], None, contacts, DT)
+    torch.cuda.synchronize()
+    stream = torch.cuda.Stream(dev)
+    stream.wait_stream(torch.cuda.current_stream(dev))
+    g_collide = [torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()]
+    g_solve = [torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()]
+    with torch.cuda.stream(stream):
+        for p in range(2):
+            with torch.cuda.graph(g_collide[p], stream=stream):
+                pipe.collide(states[p], contacts)
+            with torch.cuda.graph(g_solve[p], stream=stream):
+                solver.step(states[p], states[1 - p], None, contacts, DT)
+    torch.cuda.current_stream(dev).wait_stream(stream)
+    torch.cuda.synchronize()
+    for k in range(args.warmup):
+        g_collide[k % 2].replay()
+        g_solve[k % 2].replay()
+    torch.cuda.synchronize()
+
+    K = args.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index) as clocks:
+        ev0.record()
+        for k in range(K):
+            g_collide[k % 2].replay()
+            ev[k][0].record()
+            g_solve[k % 2].replay()
+            ev[k][1].record()
+        ev1.record()
+        torch.cuda.synchronize()
+    solve_ms = sum(a.elapsed_time(b) for a, b in ev)
+    total_ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([solve_ms, total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        solve_ms, total_ms = float(t[0]), float(t[1])
+    errors = solver.device_errors()
+
+    vi_step = float(V) * ITERATIONS
+    value = world * vi_step * K / (solve_ms * 1e-3)
+    value_with_contacts = world * vi_step * K / (total_ms * 1e-3)
+    peak, peak_src = _peaks()
+    bvi = bytes_per_vertex_iteration(V, T, E, contacts=True)
+    achieved = bvi * vi_step / (solve_ms / K * 1e-3) / 1e9
+
+    # end to end through the public API with host buffers: pinned H2D of the step's inputs
+    # (q, qd), contact generation, the step, D2H of the result (q, qd)
+    e2e = None
+    if not args.no_e2e:
+        hq = torch.empty((V, 3), dtype=torch.float32, pin_memory=True)
+        hqd = torch.empty((V, 3), dtype=torch.float32, pin_memory=True)
+        hq.copy_(states[0].particle_q)
+        hqd.copy_(states[0].particle_qd)
+        oq = torch.empty_like(hq, pin_memory=True)
+        oqd = torch.empty_like(hqd, pin_memory=True)
+        Ke = max(1, min(K, args.e2e_steps))
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(Ke):
+            states[0].particle_q.copy_(hq, non_blocking=True)
+            states[0].particle_qd.copy_(hqd, non_blocking=True)
+            g_collide[0].replay()
+            g_solve[0].replay()
+            oq.copy_(states[1].particle_q, non_blocking=True)
+            oqd.copy_(states[1].particle_qd, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([e2e_ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t[0])
+        e2e = {"value": world * vi_step * Ke / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 2 * hq.numel() * 4,
+               "d2h_bytes_per_step": 2 * oq.numel() * 4, "steps": Ke}  # fmt: skip
+
+    out = None
+    if rank == 0:
+        out = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": K,
+            "warmup": args.warmup,
+            "ms_per_step": solve_ms / K,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded cloth grids, random-init materials)",
+            "config": {
+                "workload": f"batched cloth VBD, {args.instances} instances/GPU, side U{{16..128}}, ground contact",
+                "instances_per_gpu": args.instances,
+                "vertices_per_gpu": V,
+                "triangles_per_gpu": T,
+                "hinges_per_gpu": E,
+                "iterations": ITERATIONS,
+                "dt": DT,
+                "schedule": solver.schedule,
+                "lanes_per_vertex": solver.lanes_per_vertex,
+                "block_size": solver.block_size,
+                "l2": "inputs larger than L2 (~10 GB working set), no flush",
+                "parallelism": f"instance sharding x{world} (no collective)",
+                "timed": "solve only (forward, iterations, velocity); contact generation outside the solve events",
+                "setup_s": round(setup_s, 1),
+            },
+            "value_with_contact_generation": value_with_contacts,
+            "ms_per_step_with_contact_generation": total_ms / K,
+            "e2e": e2e,
+            "gpu_launches": K * (1 + solver.launches_per_step),
+            "roofline": {
+                "bound": "hbm",
+                "achieved": achieved,
+                "peak": peak,
+                "unit": "GB/s",
+                "frac": achieved / peak,
+                "traffic": args.traffic,
+                "peak_source": peak_src,
+                "bytes_per_vertex_iteration": bvi,
+                "kernel": "k_persistent (per-substep solve)",
+            },
+            "clocks": clocks.summary(),
+            "device_errors": errors,
+        }
+        if not args.no_cpu_baseline and world == 1:
+            out["cpu_baseline"] = cpu_baseline(args, seconds=args.cpu_seconds)
+    if dist:
+        g_collide.clear()
+        g_solve.clear()
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def cpu_baseline(args, seconds=15.0):
+    """The oracle (CPU restatement of the reference SolverVBD step) on a bounded sample of the batch."""
+    from oracle import vbd_oracle as orc
+    from tests.helpers import oracle_model_dict
+
+    sides, E, bend, pins = instance_params(args.seed, args.instances)
+    threads = orc.max_threads()
+    done_vi = 0
+    elapsed = 0.0
+    used = 0
+    for i in range(args.instances):
+        b = build_instance(int(sides[i]), float(E[i]), float(bend[i]), pins[i], i)
+        b.add_ground_plane()
+        m = b.finalize("cpu")
+        om = orc.Model(oracle_model_dict(m))
+        q = m.particle_q.numpy().astype(np.float64)
+        qd = np.zeros_like(q)
+        t = time.perf_counter()
+        cnt, p, s, bp, bv, nn = orc.soft_contacts(q, m.particle_radius.numpy(), m.particle_flags.numpy(), m.shape_type,
+                                                  m.shape_pos, m.shape_radius, 0.01)  # fmt: skip
+        contacts = orc.make_contacts(cnt, p, s, bp, bv, nn)
+        orc.step(om, q, qd, None, contacts, DT, ITERATIONS, precision=32, nthreads=threads)
+        elapsed += time.perf_counter() - t
+        done_vi += m.particle_count * ITERATIONS
+        used += 1
+        if elapsed >= seconds:
+            break
+    return {"value": done_vi / elapsed, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"first {used} of {args.instances} instances, one substep each ({done_vi} vertex-iterations)"}  # fmt: skip
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    from oracle import vbd_oracle as orc
+
+    orc.lib()
+    K, W = args.steps, args.warmup
+    per_step = max(2.0, args.cpu_seconds / max(K, 1))
+    for _ in range(min(W, 1)):
+        cpu_baseline(args, seconds=0.5)
+    vals = []
+    t0 = time.perf_counter()
+    for _ in range(K):
+        vals.append(cpu_baseline(args, seconds=per_step))
+    wall = time.perf_counter() - t0
+    v = statistics.mean(x["value"] for x in vals)
+    cb = dict(vals[-1])
+    cb["value"] = v
+    return {
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": K,
+        "warmup": W, "ms_per_step": wall * 1e3 / max(K, 1), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded cloth grids, random-init materials)",
+        "config": {"workload": f"batched cloth VBD, {args.instances} instances/GPU, side U{{16..128}}, ground contact",
+                   "iterations": ITERATIONS, "dt": DT, "sample_per_step_s": per_step},
+        "impl": "reference", "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }  # fmt: skip
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--instances", type=int, default=4096)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--lanes", type=int, default=0)
+    ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--traffic", type=float, default=None, help="DRAM bytes per launch from an ncu capture")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    out = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if out is not None:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

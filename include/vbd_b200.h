@@ -1,0 +1,193 @@
+/* C ABI of the B200 cloth Vertex Block Descent library (libvbd_b200.so).
+ *
+ * Drop-in boundary for the particle path of newton.solvers.SolverVBD (reference project
+ * caixiao-0725/newton-ChysX). Every pointer named *_dev is CUDA device memory in the reference's
+ * Model / State / Contacts layout (float32 vec3 = 3 packed floats, int32 indices); *_host is host
+ * memory. Functions return VBD_OK (0) or a negative VBD_ERR_* code and never abort the process.
+ * No function allocates device memory after vbd_create returns, so vbd_step can be captured in a
+ * CUDA graph on the caller's stream.
+ */
+#ifndef VBD_B200_H
+#define VBD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VBD_OK 0
+#define VBD_ERR_INVALID_ARGUMENT -1
+#define VBD_ERR_CUDA -2
+#define VBD_ERR_OUT_OF_MEMORY -3
+#define VBD_ERR_UNSUPPORTED -4
+#define VBD_ERR_EMPTY_COLORING -5
+
+/* Bits of the device-side error word (vbd_get_error). Kernels set bits instead of trapping. */
+#define VBD_DEVERR_NONFINITE 1          /* a solved displacement was NaN/Inf (position left unchanged) */
+#define VBD_DEVERR_CONTACT_OVERFLOW 2   /* more contacts on one particle than contact slots */
+#define VBD_DEVERR_SINGULAR_SKIPPED 4   /* |det H| <= 1e-8: update skipped, as the reference does */
+#define VBD_DEVERR_BAD_CONTACT 8        /* a contact names a particle or shape out of range (ignored) */
+
+/* Arithmetic of vbd_step. */
+#define VBD_PRECISION_FP32 0   /* FP32 throughout: the reference's arithmetic */
+#define VBD_PRECISION_MIXED 1  /* FP32 element math, FP64 3x3 solve below a conditioning threshold,
+                                  FP64 residual reductions */
+#define VBD_PRECISION_FP64 2   /* FP64 throughout (state in float64): the FP64 reference run */
+
+/* Scheduling of the per-color sweep. */
+#define VBD_SCHEDULE_AUTO 0
+#define VBD_SCHEDULE_PER_COLOR 1   /* one grid launch per color per iteration (large single cloth) */
+#define VBD_SCHEDULE_PERSISTENT 2  /* one launch per substep; one CTA owns one instance (world) at a time */
+
+typedef struct VbdModelDesc {
+  int32_t particle_count; /* V */
+  int32_t tri_count;      /* T */
+  int32_t edge_count;     /* E */
+  int32_t shape_count;    /* S */
+  /* particles (Model.particle_*) */
+  const float* particle_mass_dev;     /* [V] */
+  const float* particle_inv_mass_dev; /* [V] */
+  const int32_t* particle_flags_dev;  /* [V], bit 0 = ParticleFlags.ACTIVE */
+  const float* particle_radius_dev;   /* [V] */
+  /* triangles (Model.tri_*) */
+  const int32_t* tri_indices_dev;  /* [T,3] */
+  const float* tri_poses_dev;      /* [T,2,2] rest D^-1, row-major */
+  const float* tri_materials_dev;  /* [T,5]: mu, lambda, damping, drag, lift (first three read) */
+  const float* tri_areas_dev;      /* [T] */
+  /* bending hinges (Model.edge_*) */
+  const int32_t* edge_indices_dev;         /* [E,4]: o0, o1, v0, v1 (-1 = no opposite vertex) */
+  const float* edge_rest_angle_dev;        /* [E] */
+  const float* edge_rest_length_dev;       /* [E] */
+  const float* edge_bending_properties_dev;/* [E,2]: ke, kd */
+  /* coloring (Model.particle_color_groups, concatenated in sweep order) */
+  int32_t color_count;
+  const int32_t* color_offsets_host;   /* [color_count+1] */
+  const int32_t* color_particles_dev;  /* [V] */
+  /* worlds: particles of world w are [world_particle_start_host[w], world_particle_start_host[w+1]).
+     world_count <= 1 means one instance. Instances must not share triangles or hinges. */
+  int32_t world_count;
+  const int32_t* world_particle_start_host; /* [world_count+1] or NULL */
+  /* gravity: Model.gravity[0] (the reference VBD reads world 0 only) */
+  const float* gravity_dev; /* [3] */
+  /* particle-shape contact materials */
+  float soft_contact_ke, soft_contact_kd, soft_contact_mu; /* Model.soft_contact_* */
+  const float* shape_material_ke_dev; /* [S] */
+  const float* shape_material_kd_dev; /* [S] */
+  const float* shape_material_mu_dev; /* [S] */
+  const int32_t* shape_body_dev;      /* [S], -1 = static */
+  const float* body_com_dev;          /* [B,3] or NULL */
+} VbdModelDesc;
+
+typedef struct VbdSolverParams {
+  int32_t iterations;           /* SolverVBD(iterations=10) */
+  float friction_epsilon;       /* SolverVBD(friction_epsilon=1e-2) */
+  float avbd_linear_beta;       /* rigid_avbd_linear_beta (0 = fixed penalty k) */
+  float contact_k_start;        /* rigid_contact_k_start (seed when beta > 0) */
+  int32_t precision;            /* VBD_PRECISION_* */
+  float fp64_solve_threshold;   /* MIXED: FP64 solve when |det H| < thr * max|H_ij|^3 */
+  int32_t schedule;             /* VBD_SCHEDULE_* */
+  int32_t lanes_per_vertex;     /* 1,2,4,8,16,32; 0 = choose */
+  int32_t block_size;           /* threads per CTA; 0 = choose */
+  int32_t contact_slots;        /* contacts kept per particle; 0 = max(shape_count, 1) */
+} VbdSolverParams;
+
+typedef struct VbdContactsDesc {
+  const int32_t* soft_contact_count_dev; /* [1] */
+  int32_t soft_contact_max;
+  const int32_t* soft_contact_particle_dev; /* [max] */
+  const int32_t* soft_contact_shape_dev;    /* [max] */
+  const float* soft_contact_body_pos_dev;   /* [max,3] */
+  const float* soft_contact_body_vel_dev;   /* [max,3] */
+  const float* soft_contact_normal_dev;     /* [max,3] */
+} VbdContactsDesc;
+
+typedef struct VbdBodyState {
+  /* rigid body poses for particle-shape contacts on bodies (NULL when every shape is static).
+     body_q: [B,7] (p, quat xyzw); body_qd: [B,6] (linear, angular); body_q_prev: [B,7] or NULL. */
+  const float* body_q_dev;
+  const float* body_q_prev_dev;
+  const float* body_qd_dev;
+} VbdBodyState;
+
+typedef struct VbdSolver* VbdHandle;
+
+/* Replaces SolverVBD.__init__ (solver_vbd.py:196-541): builds the vertex->element adjacency
+   (particle_vbd_kernels.py:639-738 fill order, solver_vbd.py:1177-1337), packs the model for the
+   kernels and allocates all solver scratch. Returns VBD_ERR_EMPTY_COLORING like the reference's
+   ValueError (solver_vbd.py:533-537). */
+int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHandle* out);
+
+/* Re-reads the model arrays given to vbd_create (materials, rest state, masses, flags) after the
+   caller changed them in place; replaces SolverVBD.notify_model_changed (solver_vbd.py:779-782). */
+int vbd_refresh_model(VbdHandle h, void* stream);
+
+/* Replaces SolverVBD.step(state_in, state_out, control, contacts, dt) for particles
+   (solver_vbd.py:1575-1622): forward step, `iterations` colored VBD sweeps, velocity update.
+   Side effects as in the reference: q_in_dev is overwritten with the solution, q_out_dev holds the
+   same positions, qd_out_dev = (q - q_prev) / dt; qd_in_dev and particle_f_dev are read only.
+   contacts / bodies may be NULL. Launches on `stream` (a cudaStream_t), never synchronizes. */
+int vbd_step(VbdHandle h, float* q_in_dev, float* q_out_dev, const float* qd_in_dev, float* qd_out_dev,
+             const float* particle_f_dev, const VbdContactsDesc* contacts, const VbdBodyState* bodies, float dt,
+             void* stream);
+
+/* The same step on float64 state arrays (VBD_PRECISION_FP64 solvers only). */
+int vbd_step_f64(VbdHandle h, double* q_in_dev, double* q_out_dev, const double* qd_in_dev, double* qd_out_dev,
+                 const double* particle_f_dev, const VbdContactsDesc* contacts, const VbdBodyState* bodies, double dt,
+                 void* stream);
+
+/* Reads and clears the device error word (VBD_DEVERR_* bits). Synchronizes `stream`. */
+int vbd_get_error(VbdHandle h, int32_t* bits, void* stream);
+
+/* MIXED precision: FP64 sum over particles of |f|^2 at each iteration of the last step (the force
+   residual the block solve removes). n = iterations. Synchronizes `stream`. */
+int vbd_get_residuals(VbdHandle h, double* out_host, int32_t n, void* stream);
+
+/* Number of kernel launches one vbd_step issues (for accounting). */
+int vbd_launches_per_step(VbdHandle h, int32_t* out);
+
+/* Scheduling actually chosen (VBD_SCHEDULE_*, lanes per vertex, block size). */
+int vbd_get_config(VbdHandle h, int32_t* schedule, int32_t* lanes_per_vertex, int32_t* block_size);
+
+int vbd_destroy(VbdHandle h);
+
+/* ---------------------------------------------------------------- host-side model preparation */
+
+/* Particle coloring of the graph of ModelBuilder.color (builder.py:9304-9396,
+   graph_coloring.py:99-236): triangle edges plus, when include_bending, all pairs of each active
+   hinge's four vertices. Degree-ordered greedy assignment followed by a balancing pass that moves
+   vertices from the largest to the smallest admissible colors until max/min <= target_ratio.
+   Replaces wp.utils.graph_coloring_assign/balance (Warp native, not in the reference tree).
+   colors_out: [V]. Returns the number of colors (>= 0) or a negative error. */
+int vbd_color_particles(int32_t particle_count, int32_t tri_count, const int32_t* tri_indices_host,
+                        const float* tri_materials_host, int32_t edge_count, const int32_t* edge_indices_host,
+                        const float* edge_bending_properties_host, int32_t include_bending, float target_ratio,
+                        int32_t* colors_out);
+
+/* Vertex -> (element, order) adjacency in the reference layout (ParticleForceElementAdjacencyInfo,
+   particle_vbd_kernels.py:66-151, fill order :639-738): offsets count two ints per entry. */
+int vbd_build_adjacency(int32_t particle_count, int32_t tri_count, const int32_t* tri_indices_host,
+                        int32_t edge_count, const int32_t* edge_indices_host, int32_t* face_offsets_out,
+                        int32_t* faces_out, int32_t* edge_offsets_out, int32_t* edges_out);
+
+/* ---------------------------------------------------------------- particle-shape contacts */
+
+/* Soft contacts of active particles against static shapes, as CollisionPipeline.collide writes
+   them (collide.py:1212-1246, geometry/kernels.py:1001-1140) for shape types 0 = infinite plane
+   through shape_pos with unit normal shape_normal (GeoType.PLANE with zero extents; NULL normals
+   mean +Z) and 1 = sphere of radius shape_radius at shape_pos; at most 16 shapes. One contact per
+   (particle, shape) within margin + radius. As in the reference, slots come from an atomic
+   counter, so the order of contacts is not fixed; count_dev receives the number found (it may
+   exceed soft_contact_max, entries beyond it are dropped). */
+int vbd_soft_contacts(int32_t particle_count, const float* q_dev, const float* radius_dev, const int32_t* flags_dev,
+                      int32_t shape_count, const int32_t* shape_type_host, const float* shape_pos_host,
+                      const float* shape_radius_host, const float* shape_normal_host, float margin,
+                      int32_t soft_contact_max, int32_t* count_dev,
+                      int32_t* particle_dev, int32_t* shape_dev, float* body_pos_dev, float* body_vel_dev,
+                      float* normal_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VBD_B200_H */

@@ -1,0 +1,773 @@
+// Host side of libvbd_b200.so: the C ABI declared in include/vbd_b200.h.
+//
+// Replaces the particle part of SolverVBD (newton/_src/solvers/vbd/solver_vbd.py): the constructor's
+// adjacency build and scratch allocation (:442-541, :1177-1337), step() (:1575-1622) and the
+// collision pipeline's particle-shape contact generation for planes and spheres
+// (geometry/kernels.py:1001-1140). See vbd_kernels.cuh for the device side.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <vector>
+
+#include "vbd_b200.h"
+#include "vbd_kernels.cuh"
+
+using namespace vbd;
+
+namespace {
+
+#define CK(x)                                   \
+  do {                                          \
+    cudaError_t e_ = (x);                       \
+    if (e_ != cudaSuccess) return VBD_ERR_CUDA; \
+  } while (0)
+
+template <typename T>
+int dalloc(T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? VBD_ERR_OUT_OF_MEMORY : VBD_ERR_CUDA;
+  }
+  return VBD_OK;
+}
+
+// ------------------------------------------------------------------------------ packing kernels
+__global__ void k_pack_tris(int T, const int* __restrict__ idx, const float* __restrict__ pose,
+                            const float* __restrict__ mat, const float* __restrict__ area, int4* o_idx, float4* o_pose,
+                            float4* o_mat) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= T) return;
+  o_idx[t] = make_int4(idx[3 * t], idx[3 * t + 1], idx[3 * t + 2], 0);
+  o_pose[t] = make_float4(pose[4 * t], pose[4 * t + 1], pose[4 * t + 2], pose[4 * t + 3]);
+  o_mat[t] = make_float4(mat[5 * t], mat[5 * t + 1], mat[5 * t + 2], area[t]);
+}
+
+__global__ void k_pack_edges(int E, const int* __restrict__ idx, const float* __restrict__ ra,
+                             const float* __restrict__ rl, const float* __restrict__ bp, int4* o_idx, float4* o_prop) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  o_idx[e] = make_int4(idx[4 * e], idx[4 * e + 1], idx[4 * e + 2], idx[4 * e + 3]);
+  o_prop[e] = make_float4(ra[e], rl[e], bp[2 * e], bp[2 * e + 1]);
+}
+
+// ------------------------------------------------------------------------------ soft contacts
+constexpr int kMaxContactShapes = 16;
+struct ShapeTable {
+  int type[kMaxContactShapes];
+  float4 pos_radius[kMaxContactShapes];
+  float4 normal[kMaxContactShapes];  // plane normal (unit)
+};
+
+__global__ void k_soft_contacts(int n, const float* __restrict__ q, const float* __restrict__ radius,
+                                const int* __restrict__ flags, int S, const ShapeTable shapes, float margin, int cmax,
+                                int* count, int* particle, int* shape, float* body_pos, float* body_vel,
+                                float* normal) {
+  const long tid = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (tid >= long(n) * S) return;
+  const int i = int(tid / S), s = int(tid % S);
+  if (!(flags[i] & 1)) return;
+  const float4 sf = shapes.pos_radius[s];  // pos.xyz, radius
+  const float xl[3] = {q[3 * i] - sf.x, q[3 * i + 1] - sf.y, q[3 * i + 2] - sf.z};
+  float d, nn[3];
+  if (shapes.type[s] == 0) {
+    const float4 pn = shapes.normal[s];
+    d = xl[0] * pn.x + xl[1] * pn.y + xl[2] * pn.z;
+    nn[0] = pn.x, nn[1] = pn.y, nn[2] = pn.z;
+  } else {
+    const float L = sqrtf(xl[0] * xl[0] + xl[1] * xl[1] + xl[2] * xl[2]);
+    d = L - sf.w;
+    if (L > 1.0e-8f) {
+      nn[0] = xl[0] / L, nn[1] = xl[1] / L, nn[2] = xl[2] / L;
+    } else {
+      nn[0] = 0.f, nn[1] = 0.f, nn[2] = 1.f;
+    }
+  }
+  if (d < margin + radius[i]) {
+    const int k = atomicAdd(count, 1);
+    if (k < cmax) {
+      particle[k] = i;
+      shape[k] = s;
+      for (int j = 0; j < 3; ++j) {
+        body_pos[3 * k + j] = (j == 0 ? sf.x : j == 1 ? sf.y : sf.z) + xl[j] - nn[j] * d;
+        body_vel[3 * k + j] = 0.f;
+        normal[3 * k + j] = nn[j];
+      }
+    }
+  }
+}
+
+}  // namespace
+
+struct VbdSolver {
+  VbdModelDesc md;
+  VbdSolverParams prm;
+  int V = 0, T = 0, E = 0, S = 0;
+  int precision = VBD_PRECISION_FP32;
+  int schedule = VBD_SCHEDULE_PER_COLOR;
+  int L = 1;
+  int block = 256;
+  int grid_persistent = 0;
+  int K = 1;
+  // packed model
+  int4* tri_idx = nullptr;
+  float4* tri_pose = nullptr;
+  float4* tri_mat = nullptr;
+  int4* edge_idx = nullptr;
+  float4* edge_prop = nullptr;
+  int *face_off = nullptr, *face_adj = nullptr, *edge_off = nullptr, *edge_adj = nullptr;
+  // colors
+  std::vector<int> color_offsets;
+  // persistent plan
+  int W = 1;
+  int *inst_order = nullptr, *inst_vstart = nullptr, *inst_cptr = nullptr, *color_ranges = nullptr,
+      *color_verts = nullptr, *queue = nullptr;
+  // scratch
+  void *pos = nullptr, *qprev = nullptr, *inertia = nullptr;
+  int *slot_cnt = nullptr, *slots = nullptr;
+  float *c_k = nullptr, *c_ke = nullptr, *c_kd = nullptr, *c_mu = nullptr;
+  int c_cap = 0;
+  int* err = nullptr;
+  double* residual = nullptr;
+
+  ~VbdSolver() {
+    void* ps[] = {tri_idx, tri_pose, tri_mat, edge_idx, edge_prop, face_off, face_adj, edge_off, edge_adj,
+                  inst_order, inst_vstart, inst_cptr, color_ranges, color_verts, queue, pos, qprev, inertia,
+                  slot_cnt, slots, c_k, c_ke, c_kd, c_mu, err, residual};
+    for (void* p : ps)
+      if (p) cudaFree(p);
+  }
+};
+
+namespace {
+
+int pack_model(VbdSolver* h, cudaStream_t st) {
+  const VbdModelDesc& m = h->md;
+  if (h->T > 0) {
+    k_pack_tris<<<(h->T + 255) / 256, 256, 0, st>>>(h->T, m.tri_indices_dev, m.tri_poses_dev, m.tri_materials_dev,
+                                                     m.tri_areas_dev, h->tri_idx, h->tri_pose, h->tri_mat);
+    CK(cudaGetLastError());
+  }
+  if (h->E > 0) {
+    k_pack_edges<<<(h->E + 255) / 256, 256, 0, st>>>(h->E, m.edge_indices_dev, m.edge_rest_angle_dev,
+                                                      m.edge_rest_length_dev, m.edge_bending_properties_dev,
+                                                      h->edge_idx, h->edge_prop);
+    CK(cudaGetLastError());
+  }
+  return VBD_OK;
+}
+
+// Adjacency in the solver's packed form: one int per entry, (element << 2) | order, in the
+// reference's fill order (faces by triangle id; hinges by edge id with v0, v1, o0, o1), with
+// boundary hinges (o0 or o1 == -1, which contribute nothing, particle_vbd_kernels.py:1071-1072)
+// left out.
+void build_packed_adjacency(int V, int T, const int* tri, int E, const int* edges, std::vector<int>& foff,
+                            std::vector<int>& fadj, std::vector<int>& eoff, std::vector<int>& eadj) {
+  std::vector<int> cnt(V + 1, 0);
+  for (int t = 0; t < T; ++t)
+    for (int j = 0; j < 3; ++j) cnt[tri[3 * t + j] + 1]++;
+  foff.assign(V + 1, 0);
+  for (int i = 0; i < V; ++i) foff[i + 1] = foff[i] + cnt[i + 1];
+  fadj.assign(std::max(foff[V], 1), 0);
+  std::vector<int> fill(foff.begin(), foff.end() - 1);
+  for (int t = 0; t < T; ++t)
+    for (int j = 0; j < 3; ++j) {
+      const int v = tri[3 * t + j];
+      fadj[fill[v]++] = (t << 2) | j;
+    }
+  std::fill(cnt.begin(), cnt.end(), 0);
+  for (int e = 0; e < E; ++e) {
+    const int* ei = edges + 4 * e;
+    if (ei[0] < 0 || ei[1] < 0) continue;
+    for (int j = 0; j < 4; ++j) cnt[ei[j] + 1]++;
+  }
+  eoff.assign(V + 1, 0);
+  for (int i = 0; i < V; ++i) eoff[i + 1] = eoff[i] + cnt[i + 1];
+  eadj.assign(std::max(eoff[V], 1), 0);
+  fill.assign(eoff.begin(), eoff.end() - 1);
+  for (int e = 0; e < E; ++e) {
+    const int* ei = edges + 4 * e;
+    if (ei[0] < 0 || ei[1] < 0) continue;
+    eadj[fill[ei[2]]++] = (e << 2) | 2;
+    eadj[fill[ei[3]]++] = (e << 2) | 3;
+    eadj[fill[ei[0]]++] = (e << 2) | 0;
+    eadj[fill[ei[1]]++] = (e << 2) | 1;
+  }
+}
+
+template <typename T>
+int upload(T** d, const std::vector<T>& h) {
+  int rc = dalloc(d, h.size());
+  if (rc) return rc;
+  CK(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return VBD_OK;
+}
+
+template <typename R, int MODE>
+StepCtx<R> make_ctx(VbdSolver* h) {
+  StepCtx<R> c;
+  std::memset(&c, 0, sizeof(c));
+  const VbdModelDesc& m = h->md;
+  c.tri_idx = h->tri_idx;
+  c.tri_pose = h->tri_pose;
+  c.tri_mat = h->tri_mat;
+  c.edge_idx = h->edge_idx;
+  c.edge_prop = h->edge_prop;
+  c.face_off = h->face_off;
+  c.face_adj = h->face_adj;
+  c.edge_off = h->edge_off;
+  c.edge_adj = h->edge_adj;
+  c.mass = m.particle_mass_dev;
+  c.inv_mass = m.particle_inv_mass_dev;
+  c.flags = m.particle_flags_dev;
+  c.radius = m.particle_radius_dev;
+  c.gravity = m.gravity_dev;
+  c.pos = (pos4_t<R>*)h->pos;
+  c.qprev = (pos4_t<R>*)h->qprev;
+  c.inertia = (pos4_t<R>*)h->inertia;
+  c.K = h->K;
+  c.slot_cnt = h->slot_cnt;
+  c.slots = h->slots;
+  c.c_k = h->c_k;
+  c.c_ke = h->c_ke;
+  c.c_kd = h->c_kd;
+  c.c_mu = h->c_mu;
+  c.soft_ke = m.soft_contact_ke;
+  c.soft_kd = m.soft_contact_kd;
+  c.soft_mu = m.soft_contact_mu;
+  c.shape_ke = m.shape_material_ke_dev;
+  c.shape_kd = m.shape_material_kd_dev;
+  c.shape_mu = m.shape_material_mu_dev;
+  c.shape_body = m.shape_body_dev;
+  c.body_com = m.body_com_dev;
+  c.k_start = h->prm.avbd_linear_beta == 0.f ? -1.f : h->prm.contact_k_start;
+  c.beta = R(h->prm.avbd_linear_beta);
+  c.fric_eps = R(h->prm.friction_epsilon);
+  c.fp64_thr = h->prm.fp64_solve_threshold;
+  c.err = h->err;
+  c.residual = MODE == MODE_MIXED ? h->residual : nullptr;
+  c.V = h->V;
+  c.S = h->S;
+  return c;
+}
+
+template <typename R, int MODE, int L>
+void launch_color(const StepCtx<R>& c, const int* verts, int n, int it, int block, cudaStream_t st) {
+  const long threads = long(n) * L;
+  const int grid = int((threads + block - 1) / block);
+  if (grid > 0) k_color<R, L, MODE><<<grid, block, 0, st>>>(c, verts, n, it);
+}
+
+template <typename R, int MODE>
+void launch_color_any(int L, const StepCtx<R>& c, const int* verts, int n, int it, int block, cudaStream_t st) {
+  switch (L) {
+    case 1: launch_color<R, MODE, 1>(c, verts, n, it, block, st); break;
+    case 2: launch_color<R, MODE, 2>(c, verts, n, it, block, st); break;
+    case 4: launch_color<R, MODE, 4>(c, verts, n, it, block, st); break;
+    case 8: launch_color<R, MODE, 8>(c, verts, n, it, block, st); break;
+    case 16: launch_color<R, MODE, 16>(c, verts, n, it, block, st); break;
+    default: launch_color<R, MODE, 32>(c, verts, n, it, block, st); break;
+  }
+}
+
+template <typename R, int MODE>
+const void* persistent_fn(int L) {
+  switch (L) {
+    case 1: return (const void*)k_persistent<R, 1, MODE>;
+    case 2: return (const void*)k_persistent<R, 2, MODE>;
+    case 4: return (const void*)k_persistent<R, 4, MODE>;
+    case 8: return (const void*)k_persistent<R, 8, MODE>;
+    case 16: return (const void*)k_persistent<R, 16, MODE>;
+    default: return (const void*)k_persistent<R, 32, MODE>;
+  }
+}
+
+template <typename R, int MODE>
+void launch_persistent(int L, const StepCtx<R>& c, const PersistentPlan& p, int grid, int block, cudaStream_t st) {
+  switch (L) {
+    case 1: k_persistent<R, 1, MODE><<<grid, block, 0, st>>>(c, p); break;
+    case 2: k_persistent<R, 2, MODE><<<grid, block, 0, st>>>(c, p); break;
+    case 4: k_persistent<R, 4, MODE><<<grid, block, 0, st>>>(c, p); break;
+    case 8: k_persistent<R, 8, MODE><<<grid, block, 0, st>>>(c, p); break;
+    case 16: k_persistent<R, 16, MODE><<<grid, block, 0, st>>>(c, p); break;
+    default: k_persistent<R, 32, MODE><<<grid, block, 0, st>>>(c, p); break;
+  }
+}
+
+int ensure_contact_capacity(VbdSolver* h, int cmax, cudaStream_t st) {
+  if (cmax <= h->c_cap) return VBD_OK;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(st, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return VBD_ERR_UNSUPPORTED;  // growing buffers during capture
+  for (float** p : {&h->c_k, &h->c_ke, &h->c_kd, &h->c_mu}) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    int rc = dalloc(p, size_t(cmax));
+    if (rc) return rc;
+  }
+  h->c_cap = cmax;
+  return VBD_OK;
+}
+
+template <typename R, int MODE>
+int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const R* f_ext,
+              const VbdContactsDesc* contacts, const VbdBodyState* bodies, R dt, cudaStream_t st) {
+  if (!q_in || !q_out || !qd_in || !qd_out || !(dt > R(0))) return VBD_ERR_INVALID_ARGUMENT;
+  StepCtx<R> c = make_ctx<R, MODE>(h);
+  c.q_in = q_in;
+  c.q_out = q_out;
+  c.qd_in = qd_in;
+  c.qd_out = qd_out;
+  c.f_ext = f_ext;
+  c.dt = dt;
+  c.dt2r = R(1) / (dt * dt);
+  const bool has_c = contacts && contacts->soft_contact_max > 0 && contacts->soft_contact_count_dev;
+  if (has_c) {
+    int rc = ensure_contact_capacity(h, contacts->soft_contact_max, st);
+    if (rc) return rc;
+    c = make_ctx<R, MODE>(h);
+    c.q_in = q_in;
+    c.q_out = q_out;
+    c.qd_in = qd_in;
+    c.qd_out = qd_out;
+    c.f_ext = f_ext;
+    c.dt = dt;
+    c.dt2r = R(1) / (dt * dt);
+    c.has_contacts = 1;
+    c.c_count = contacts->soft_contact_count_dev;
+    c.c_max = contacts->soft_contact_max;
+    c.c_particle = contacts->soft_contact_particle_dev;
+    c.c_shape = contacts->soft_contact_shape_dev;
+    c.c_body_pos = contacts->soft_contact_body_pos_dev;
+    c.c_body_vel = contacts->soft_contact_body_vel_dev;
+    c.c_normal = contacts->soft_contact_normal_dev;
+    if (bodies) {
+      c.body_q = bodies->body_q_dev;
+      c.body_q_prev = bodies->body_q_prev_dev;
+      c.body_qd = bodies->body_qd_dev;
+    }
+  }
+  const int iters = h->prm.iterations;
+  if (MODE == MODE_MIXED) CK(cudaMemsetAsync(h->residual, 0, sizeof(double) * std::max(iters, 1), st));
+  if (h->schedule == VBD_SCHEDULE_PERSISTENT) {
+    CK(cudaMemsetAsync(h->queue, 0, sizeof(int), st));
+    if (has_c) {
+      CK(cudaMemsetAsync(h->slot_cnt, 0, sizeof(int) * h->V, st));
+      k_contact_prepare<R><<<(c.c_max + 255) / 256, 256, 0, st>>>(c);
+    }
+    PersistentPlan p{h->W, h->inst_order, h->inst_vstart, h->inst_cptr, h->color_ranges, h->color_verts, h->queue,
+                     iters};
+    launch_persistent<R, MODE>(h->L, c, p, h->grid_persistent, h->block, st);
+  } else {
+    k_forward<R><<<(h->V + 255) / 256, 256, 0, st>>>(c);
+    if (has_c) k_contact_prepare<R><<<(c.c_max + 255) / 256, 256, 0, st>>>(c);
+    const int* cp = h->md.color_particles_dev;
+    for (int it = 0; it < iters; ++it)
+      for (size_t col = 0; col + 1 < h->color_offsets.size(); ++col) {
+        const int a = h->color_offsets[col], b = h->color_offsets[col + 1];
+        launch_color_any<R, MODE>(h->L, c, cp + a, b - a, it, h->block, st);
+      }
+    k_finalize<R><<<(h->V + 255) / 256, 256, 0, st>>>(c);
+  }
+  CK(cudaGetLastError());
+  return VBD_OK;
+}
+
+int occupancy_grid(VbdSolver* h) {
+  const void* fn = nullptr;
+  if (h->precision == VBD_PRECISION_FP64)
+    fn = persistent_fn<double, MODE_FP64>(h->L);
+  else if (h->precision == VBD_PRECISION_MIXED)
+    fn = persistent_fn<float, MODE_MIXED>(h->L);
+  else
+    fn = persistent_fn<float, MODE_FP32>(h->L);
+  int dev = 0, sms = 0, per_sm = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, h->block, 0));
+  if (per_sm < 1) return VBD_ERR_INVALID_ARGUMENT;
+  h->grid_persistent = std::min(h->W, sms * per_sm);
+  return VBD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHandle* out) {
+  if (!model || !params || !out) return VBD_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  const VbdModelDesc& m = *model;
+  if (m.particle_count <= 0 || m.tri_count < 0 || m.edge_count < 0 || m.shape_count < 0)
+    return VBD_ERR_INVALID_ARGUMENT;
+  if (m.color_count <= 0 || !m.color_offsets_host || !m.color_particles_dev) return VBD_ERR_EMPTY_COLORING;
+  if (params->iterations < 0) return VBD_ERR_INVALID_ARGUMENT;
+  if (params->precision < 0 || params->precision > 2) return VBD_ERR_INVALID_ARGUMENT;
+  const int lpv = params->lanes_per_vertex;
+  if (lpv != 0 && lpv != 1 && lpv != 2 && lpv != 4 && lpv != 8 && lpv != 16 && lpv != 32)
+    return VBD_ERR_INVALID_ARGUMENT;
+  if (params->block_size != 0 && (params->block_size < 32 || params->block_size > 1024 || params->block_size % 32))
+    return VBD_ERR_INVALID_ARGUMENT;
+  if (params->contact_slots < 0 || params->contact_slots > 8) return VBD_ERR_INVALID_ARGUMENT;
+  if (m.color_offsets_host[0] != 0 || m.color_offsets_host[m.color_count] != m.particle_count)
+    return VBD_ERR_INVALID_ARGUMENT;
+  for (int c = 0; c < m.color_count; ++c)
+    if (m.color_offsets_host[c + 1] < m.color_offsets_host[c]) return VBD_ERR_INVALID_ARGUMENT;
+  if (!m.particle_mass_dev || !m.particle_inv_mass_dev || !m.particle_flags_dev || !m.particle_radius_dev ||
+      !m.gravity_dev)
+    return VBD_ERR_INVALID_ARGUMENT;
+  if (m.tri_count > 0 && (!m.tri_indices_dev || !m.tri_poses_dev || !m.tri_materials_dev || !m.tri_areas_dev))
+    return VBD_ERR_INVALID_ARGUMENT;
+  if (m.edge_count > 0 && (!m.edge_indices_dev || !m.edge_rest_angle_dev || !m.edge_rest_length_dev ||
+                           !m.edge_bending_properties_dev))
+    return VBD_ERR_INVALID_ARGUMENT;
+  if (m.shape_count > 0 &&
+      (!m.shape_material_ke_dev || !m.shape_material_kd_dev || !m.shape_material_mu_dev || !m.shape_body_dev))
+    return VBD_ERR_INVALID_ARGUMENT;
+  if (m.tri_count >= (1 << 29) || m.edge_count >= (1 << 29)) return VBD_ERR_UNSUPPORTED;
+
+  VbdSolver* h = new (std::nothrow) VbdSolver();
+  if (!h) return VBD_ERR_OUT_OF_MEMORY;
+  h->md = m;
+  h->prm = *params;
+  h->V = m.particle_count;
+  h->T = m.tri_count;
+  h->E = m.edge_count;
+  h->S = m.shape_count;
+  h->precision = params->precision;
+  h->K = params->contact_slots > 0 ? params->contact_slots : std::max(1, std::min(8, m.shape_count));
+  h->color_offsets.assign(m.color_offsets_host, m.color_offsets_host + m.color_count + 1);
+  int rc = VBD_OK;
+  auto fail = [&](int code) {
+    delete h;
+    return code;
+  };
+
+  // host copies of the topology for the adjacency and the instance plan (one-time)
+  std::vector<int> tri(3 * size_t(h->T)), edges(4 * size_t(h->E)), colp(h->V);
+  if (h->T && cudaMemcpy(tri.data(), m.tri_indices_dev, tri.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(VBD_ERR_CUDA);
+  if (h->E && cudaMemcpy(edges.data(), m.edge_indices_dev, edges.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(VBD_ERR_CUDA);
+  if (cudaMemcpy(colp.data(), m.color_particles_dev, size_t(h->V) * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(VBD_ERR_CUDA);
+  for (int t : tri)
+    if (t < 0 || t >= h->V) return fail(VBD_ERR_INVALID_ARGUMENT);
+  for (size_t i = 0; i < edges.size(); ++i)
+    if (edges[i] >= h->V || (edges[i] < 0 && (i % 4) >= 2) || edges[i] < -1) return fail(VBD_ERR_INVALID_ARGUMENT);
+  for (int p : colp)
+    if (p < 0 || p >= h->V) return fail(VBD_ERR_INVALID_ARGUMENT);
+
+  std::vector<int> foff, fadj, eoff, eadj;
+  build_packed_adjacency(h->V, h->T, tri.data(), h->E, edges.data(), foff, fadj, eoff, eadj);
+  if ((rc = upload(&h->face_off, foff)) || (rc = upload(&h->face_adj, fadj)) || (rc = upload(&h->edge_off, eoff)) ||
+      (rc = upload(&h->edge_adj, eadj)))
+    return fail(rc);
+  if ((rc = dalloc(&h->tri_idx, h->T)) || (rc = dalloc(&h->tri_pose, h->T)) || (rc = dalloc(&h->tri_mat, h->T)) ||
+      (rc = dalloc(&h->edge_idx, h->E)) || (rc = dalloc(&h->edge_prop, h->E)))
+    return fail(rc);
+  if ((rc = pack_model(h, 0))) return fail(rc);
+
+  // instances (worlds)
+  std::vector<int> wstart;
+  if (m.world_count > 1 && m.world_particle_start_host) {
+    wstart.assign(m.world_particle_start_host, m.world_particle_start_host + m.world_count + 1);
+    if (wstart[0] != 0 || wstart.back() != h->V) return fail(VBD_ERR_INVALID_ARGUMENT);
+    for (int w = 0; w < m.world_count; ++w)
+      if (wstart[w + 1] < wstart[w]) return fail(VBD_ERR_INVALID_ARGUMENT);
+  } else {
+    wstart = {0, h->V};
+  }
+  h->W = int(wstart.size()) - 1;
+  std::vector<int> world_of(h->V);
+  for (int w = 0; w < h->W; ++w)
+    for (int i = wstart[w]; i < wstart[w + 1]; ++i) world_of[i] = w;
+  for (int t = 0; t < h->T; ++t)
+    if (world_of[tri[3 * t]] != world_of[tri[3 * t + 1]] || world_of[tri[3 * t]] != world_of[tri[3 * t + 2]])
+      return fail(VBD_ERR_INVALID_ARGUMENT);
+  for (int e = 0; e < h->E; ++e)
+    for (int j = 0; j < 4; ++j)
+      if (edges[4 * e + j] >= 0 && world_of[edges[4 * e + j]] != world_of[edges[4 * e + 2]])
+        return fail(VBD_ERR_INVALID_ARGUMENT);
+  // per instance, per global color (in sweep order), the instance's particles of that color
+  std::vector<std::vector<std::vector<int>>> per(h->W);
+  for (size_t col = 0; col + 1 < h->color_offsets.size(); ++col) {
+    for (int w = 0; w < h->W; ++w) per[w].emplace_back();
+    for (int k = h->color_offsets[col]; k < h->color_offsets[col + 1]; ++k) per[world_of[colp[k]]][col].push_back(colp[k]);
+  }
+  std::vector<int> cptr(h->W + 1, 0), ranges, verts;
+  for (int w = 0; w < h->W; ++w) {
+    cptr[w] = int(ranges.size());
+    for (auto& g : per[w]) {
+      if (g.empty()) continue;
+      ranges.push_back(int(verts.size()));
+      verts.insert(verts.end(), g.begin(), g.end());
+    }
+    ranges.push_back(int(verts.size()));
+  }
+  cptr[h->W] = int(ranges.size());
+  // instance w's ranges are ranges[cptr[w] .. cptr[w+1]-1]; the kernel walks col in [cb, ce-1)
+  std::vector<int> order(h->W);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return wstart[a + 1] - wstart[a] > wstart[b + 1] - wstart[b]; });
+  if ((rc = upload(&h->inst_order, order)) || (rc = upload(&h->inst_vstart, wstart)) ||
+      (rc = upload(&h->inst_cptr, cptr)) || (rc = upload(&h->color_ranges, ranges)) ||
+      (rc = upload(&h->color_verts, verts)) || (rc = dalloc(&h->queue, 1)))
+    return fail(rc);
+
+  // scratch
+  const size_t p4 = h->precision == VBD_PRECISION_FP64 ? sizeof(double4) : sizeof(float4);
+  if ((rc = dalloc((char**)&h->pos, p4 * h->V)) || (rc = dalloc((char**)&h->qprev, p4 * h->V)) ||
+      (rc = dalloc((char**)&h->inertia, p4 * h->V)) || (rc = dalloc(&h->slot_cnt, h->V)) ||
+      (rc = dalloc(&h->slots, size_t(h->V) * h->K)) || (rc = dalloc(&h->err, 1)) ||
+      (rc = dalloc(&h->residual, std::max(params->iterations, 1))))
+    return fail(rc);
+  if (cudaMemset(h->err, 0, sizeof(int)) != cudaSuccess || cudaMemset(h->slot_cnt, 0, sizeof(int) * h->V) != cudaSuccess)
+    return fail(VBD_ERR_CUDA);
+
+  // scheduling
+  h->schedule = params->schedule;
+  if (h->schedule == VBD_SCHEDULE_AUTO) h->schedule = (h->W > 1 || h->V <= 4096) ? VBD_SCHEDULE_PERSISTENT : VBD_SCHEDULE_PER_COLOR;
+  h->L = lpv ? lpv : (h->schedule == VBD_SCHEDULE_PERSISTENT && h->W == 1 ? 8 : 1);
+  h->block = params->block_size ? params->block_size : (h->schedule == VBD_SCHEDULE_PERSISTENT ? 256 : 128);
+  if (h->schedule == VBD_SCHEDULE_PERSISTENT && (rc = occupancy_grid(h))) return fail(rc);
+  if (cudaDeviceSynchronize() != cudaSuccess) return fail(VBD_ERR_CUDA);
+  *out = h;
+  return VBD_OK;
+}
+
+int vbd_refresh_model(VbdHandle h, void* stream) {
+  if (!h) return VBD_ERR_INVALID_ARGUMENT;
+  return pack_model(h, (cudaStream_t)stream);
+}
+
+int vbd_step(VbdHandle h, float* q_in, float* q_out, const float* qd_in, float* qd_out, const float* f_ext,
+             const VbdContactsDesc* contacts, const VbdBodyState* bodies, float dt, void* stream) {
+  if (!h) return VBD_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (h->precision == VBD_PRECISION_FP64) return VBD_ERR_INVALID_ARGUMENT;
+  if (h->precision == VBD_PRECISION_MIXED)
+    return step_impl<float, MODE_MIXED>(h, q_in, q_out, qd_in, qd_out, f_ext, contacts, bodies, dt, st);
+  return step_impl<float, MODE_FP32>(h, q_in, q_out, qd_in, qd_out, f_ext, contacts, bodies, dt, st);
+}
+
+int vbd_step_f64(VbdHandle h, double* q_in, double* q_out, const double* qd_in, double* qd_out, const double* f_ext,
+                 const VbdContactsDesc* contacts, const VbdBodyState* bodies, double dt, void* stream) {
+  if (!h) return VBD_ERR_INVALID_ARGUMENT;
+  if (h->precision != VBD_PRECISION_FP64) return VBD_ERR_INVALID_ARGUMENT;
+  return step_impl<double, MODE_FP64>(h, q_in, q_out, qd_in, qd_out, f_ext, contacts, bodies, dt,
+                                      (cudaStream_t)stream);
+}
+
+int vbd_get_error(VbdHandle h, int32_t* bits, void* stream) {
+  if (!h || !bits) return VBD_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaMemcpyAsync(bits, h->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemsetAsync(h->err, 0, sizeof(int), st));
+  CK(cudaStreamSynchronize(st));
+  return VBD_OK;
+}
+
+int vbd_get_residuals(VbdHandle h, double* out, int32_t n, void* stream) {
+  if (!h || !out || n < 0 || n > std::max(h->prm.iterations, 1)) return VBD_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (n == 0) return VBD_OK;
+  CK(cudaMemcpyAsync(out, h->residual, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return VBD_OK;
+}
+
+int vbd_launches_per_step(VbdHandle h, int32_t* out) {
+  if (!h || !out) return VBD_ERR_INVALID_ARGUMENT;
+  if (h->schedule == VBD_SCHEDULE_PERSISTENT)
+    *out = 1 + (h->S > 0 ? 1 : 0);
+  else
+    *out = 2 + (h->S > 0 ? 1 : 0) + h->prm.iterations * (int(h->color_offsets.size()) - 1);
+  return VBD_OK;
+}
+
+int vbd_get_config(VbdHandle h, int32_t* schedule, int32_t* lanes, int32_t* block) {
+  if (!h) return VBD_ERR_INVALID_ARGUMENT;
+  if (schedule) *schedule = h->schedule;
+  if (lanes) *lanes = h->L;
+  if (block) *block = h->block;
+  return VBD_OK;
+}
+
+int vbd_destroy(VbdHandle h) {
+  if (!h) return VBD_ERR_INVALID_ARGUMENT;
+  cudaDeviceSynchronize();
+  delete h;
+  return VBD_OK;
+}
+
+int vbd_build_adjacency(int32_t V, int32_t T, const int32_t* tri, int32_t E, const int32_t* edges, int32_t* foff,
+                        int32_t* faces, int32_t* eoff, int32_t* eadj) {
+  if (V < 0 || T < 0 || E < 0 || (T && !tri) || (E && !edges) || !foff || !eoff) return VBD_ERR_INVALID_ARGUMENT;
+  std::vector<int> cnt(V, 0), fill(V, 0);
+  for (int t = 0; t < T; ++t)
+    for (int j = 0; j < 3; ++j) {
+      if (tri[3 * t + j] < 0 || tri[3 * t + j] >= V) return VBD_ERR_INVALID_ARGUMENT;
+      cnt[tri[3 * t + j]]++;
+    }
+  foff[0] = 0;
+  for (int i = 0; i < V; ++i) foff[i + 1] = foff[i] + 2 * cnt[i];
+  for (int t = 0; t < T; ++t)
+    for (int j = 0; j < 3; ++j) {
+      const int v = tri[3 * t + j];
+      const int o = foff[v] + 2 * fill[v]++;
+      faces[o] = t;
+      faces[o + 1] = j;
+    }
+  std::fill(cnt.begin(), cnt.end(), 0);
+  std::fill(fill.begin(), fill.end(), 0);
+  for (int e = 0; e < E; ++e) {
+    const int* ei = edges + 4 * e;
+    for (int j = 0; j < 4; ++j)
+      if (ei[j] >= V || (ei[j] < 0 && (j >= 2 || ei[j] != -1))) return VBD_ERR_INVALID_ARGUMENT;
+    cnt[ei[2]]++;
+    cnt[ei[3]]++;
+    if (ei[0] != -1) cnt[ei[0]]++;
+    if (ei[1] != -1) cnt[ei[1]]++;
+  }
+  eoff[0] = 0;
+  for (int i = 0; i < V; ++i) eoff[i + 1] = eoff[i] + 2 * cnt[i];
+  auto put = [&](int v, int e, int order) {
+    const int o = eoff[v] + 2 * fill[v]++;
+    eadj[o] = e;
+    eadj[o + 1] = order;
+  };
+  for (int e = 0; e < E; ++e) {
+    const int* ei = edges + 4 * e;
+    put(ei[2], e, 2);
+    put(ei[3], e, 3);
+    if (ei[0] != -1) put(ei[0], e, 0);
+    if (ei[1] != -1) put(ei[1], e, 1);
+  }
+  return VBD_OK;
+}
+
+int vbd_color_particles(int32_t V, int32_t T, const int32_t* tri, const float* tri_mat, int32_t E,
+                        const int32_t* edges, const float* edge_props, int32_t include_bending, float target_ratio,
+                        int32_t* colors) {
+  if (V < 0 || T < 0 || E < 0 || !colors) return VBD_ERR_INVALID_ARGUMENT;
+  if (V == 0) return 0;
+  // graph edges as (min, max) pairs, deduplicated (graph_coloring.py:45-51, 99-236)
+  std::vector<uint64_t> pairs;
+  pairs.reserve(size_t(3) * T + (include_bending ? size_t(6) * E : 0));
+  auto add = [&](int a, int b) {
+    if (a < 0 || b < 0 || a == b) return;
+    if (a > b) std::swap(a, b);
+    pairs.push_back((uint64_t(uint32_t(a)) << 32) | uint32_t(b));
+  };
+  for (int t = 0; t < T; ++t) {
+    if (tri_mat && tri_mat[5 * t] * tri_mat[5 * t + 1] == 0.f) continue;  // inactive triangle mask
+    add(tri[3 * t], tri[3 * t + 1]);
+    add(tri[3 * t], tri[3 * t + 2]);
+    add(tri[3 * t + 1], tri[3 * t + 2]);
+  }
+  if (include_bending)
+    for (int e = 0; e < E; ++e) {
+      if (edge_props && edge_props[2 * e] == 0.f && edge_props[2 * e + 1] == 0.f) continue;
+      const int* ei = edges + 4 * e;
+      for (int i = 0; i < 4; ++i)
+        for (int j = i + 1; j < 4; ++j) add(ei[i], ei[j]);
+    }
+  for (uint64_t p : pairs)
+    if (int(p >> 32) >= V || int(p & 0xffffffffu) >= V) return VBD_ERR_INVALID_ARGUMENT;
+  std::sort(pairs.begin(), pairs.end());
+  pairs.erase(std::unique(pairs.begin(), pairs.end()), pairs.end());
+  std::vector<int> off(V + 1, 0);
+  for (uint64_t p : pairs) {
+    off[int(p >> 32) + 1]++;
+    off[int(p & 0xffffffffu) + 1]++;
+  }
+  for (int i = 0; i < V; ++i) off[i + 1] += off[i];
+  std::vector<int> nb(off[V]), fill(off.begin(), off.end() - 1);
+  for (uint64_t p : pairs) {
+    const int a = int(p >> 32), b = int(p & 0xffffffffu);
+    nb[fill[a]++] = b;
+    nb[fill[b]++] = a;
+  }
+  // degree-ordered greedy (largest degree first, ties by index)
+  std::vector<int> order(V);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return off[a + 1] - off[a] > off[b + 1] - off[b]; });
+  std::fill(colors, colors + V, -1);
+  std::vector<int> mark;
+  int ncol = 0;
+  for (int v : order) {
+    for (int k = off[v]; k < off[v + 1]; ++k) {
+      const int c = colors[nb[k]];
+      if (c >= 0) {
+        if (c >= int(mark.size())) mark.resize(c + 1, -1);
+        mark[c] = v;
+      }
+    }
+    int c = 0;
+    while (c < int(mark.size()) && mark[c] == v) ++c;
+    colors[v] = c;
+    ncol = std::max(ncol, c + 1);
+  }
+  // balancing: move vertices from the largest color to the smallest admissible one
+  if (ncol > 1 && target_ratio > 1.f) {
+    std::vector<int> size(ncol, 0);
+    for (int v = 0; v < V; ++v) size[colors[v]]++;
+    for (int round = 0; round < 4 * ncol; ++round) {
+      const int cmax = int(std::max_element(size.begin(), size.end()) - size.begin());
+      const int cmin = int(std::min_element(size.begin(), size.end()) - size.begin());
+      if (size[cmin] > 0 && float(size[cmax]) / float(size[cmin]) <= target_ratio) break;
+      bool moved = false;
+      for (int v = 0; v < V && size[cmax] - size[cmin] > 1; ++v) {
+        if (colors[v] != cmax) continue;
+        bool ok = true;
+        for (int k = off[v]; k < off[v + 1] && ok; ++k) ok = colors[nb[k]] != cmin;
+        if (ok) {
+          colors[v] = cmin;
+          size[cmax]--;
+          size[cmin]++;
+          moved = true;
+        }
+      }
+      if (!moved) break;
+    }
+  }
+  return ncol;
+}
+
+int vbd_soft_contacts(int32_t n, const float* q, const float* radius, const int32_t* flags, int32_t S,
+                      const int32_t* shape_type, const float* shape_pos, const float* shape_radius,
+                      const float* shape_normal, float margin,
+                      int32_t cmax, int32_t* count, int32_t* particle, int32_t* shape, float* body_pos,
+                      float* body_vel, float* normal, void* stream) {
+  if (n < 0 || S < 0 || S > kMaxContactShapes || cmax < 0 || !count || (S && (!shape_type || !shape_pos)))
+    return VBD_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaMemsetAsync(count, 0, sizeof(int), st));
+  if (n == 0 || S == 0) return VBD_OK;
+  ShapeTable tab;
+  std::memset(&tab, 0, sizeof(tab));
+  for (int s = 0; s < S; ++s) {
+    if (shape_type[s] != 0 && shape_type[s] != 1) return VBD_ERR_UNSUPPORTED;
+    tab.type[s] = shape_type[s];
+    tab.pos_radius[s] = make_float4(shape_pos[3 * s], shape_pos[3 * s + 1], shape_pos[3 * s + 2],
+                                    shape_radius ? shape_radius[s] : 0.f);
+    float nx = 0.f, ny = 0.f, nz = 1.f;
+    if (shape_normal) nx = shape_normal[3 * s], ny = shape_normal[3 * s + 1], nz = shape_normal[3 * s + 2];
+    const float nl = sqrtf(nx * nx + ny * ny + nz * nz);
+    if (shape_type[s] == 0 && !(nl > 0.f)) return VBD_ERR_INVALID_ARGUMENT;
+    tab.normal[s] = nl > 0.f ? make_float4(nx / nl, ny / nl, nz / nl, 0.f) : make_float4(0.f, 0.f, 1.f, 0.f);
+  }
+  const long total = long(n) * S;
+  k_soft_contacts<<<int((total + 255) / 256), 256, 0, st>>>(n, q, radius, flags, S, tab, margin, cmax, count, particle,
+                                                            shape, body_pos, body_vel, normal);
+  CK(cudaGetLastError());
+  return VBD_OK;
+}
+
+}  // extern "C"

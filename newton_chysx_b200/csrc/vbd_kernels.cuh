@@ -1,0 +1,416 @@
+// Device side of the B200 cloth VBD step.
+//
+// One routine, solve_group<R, L, MODE>, performs the work of the reference's solve_elasticity
+// (particle_vbd_kernels.py:3135-3273) plus the per-color contact accumulation
+// (particle_vbd_kernels.py:2900-2967 with rigid_vbd_kernels.py:762-834) and the AVBD penalty update
+// (rigid_vbd_kernels.py:3755-3799) for one vertex, using L lanes of a warp:
+//   - the vertex's adjacency (faces, then hinges) is split round-robin over the L lanes;
+//   - the 9 partial sums (force 3, symmetric Hessian 6) are combined with xor-shuffles;
+//   - lane 0 adds inertia and contact terms, solves the 3x3 system and writes the new position.
+// Two schedulers call it: k_color (one launch per color, any model size) and k_persistent (one
+// launch per substep; a CTA takes whole instances from a work queue and sweeps all their colors
+// with __syncthreads between colors).
+//
+// Position update: the reference accumulates a displacement d and writes q = q_prev + d after every
+// color (apply_truncation_ts with t = 1 and no bound when self-contact is off,
+// particle_vbd_kernels.py:2877-2897). That is q += H^-1 f; this code applies it to q directly.
+#pragma once
+#include "vbd_elements.cuh"
+
+namespace vbd {
+
+enum Mode { MODE_FP32 = 0, MODE_MIXED = 1, MODE_FP64 = 2 };
+
+template <typename R>
+struct StepCtx {
+  using P4 = pos4_t<R>;
+  // packed model (solver-owned)
+  const int4* __restrict__ tri_idx;
+  const float4* __restrict__ tri_pose;
+  const float4* __restrict__ tri_mat;  // mu, lambda, damping, area
+  const int4* __restrict__ edge_idx;
+  const float4* __restrict__ edge_prop;  // rest angle, rest length, ke, kd
+  const int* __restrict__ face_off;      // [V+1], one int per entry
+  const int* __restrict__ face_adj;      // (tri << 2) | order
+  const int* __restrict__ edge_off;
+  const int* __restrict__ edge_adj;  // (edge << 2) | order; boundary hinges are left out
+  // model per particle (caller-owned, reference layout)
+  const float* __restrict__ mass;
+  const float* __restrict__ inv_mass;
+  const int* __restrict__ flags;
+  const float* __restrict__ radius;
+  const float* __restrict__ gravity;
+  // state (caller-owned)
+  R* q_in;
+  R* q_out;
+  const R* qd_in;
+  R* qd_out;
+  const R* f_ext;
+  // solver scratch
+  P4* pos;      // current positions (w unused)
+  P4* qprev;    // positions at the start of the step
+  P4* inertia;  // inertial target; w = mass, or 0 for a fixed particle
+  // contacts
+  int has_contacts;
+  int K;
+  int* slot_cnt;  // [V]
+  int* slots;     // [V*K]
+  const int* c_count;
+  int c_max;
+  const int* c_particle;
+  const int* c_shape;
+  const float* c_body_pos;
+  const float* c_body_vel;
+  const float* c_normal;
+  float* c_k;     // per-contact penalty stiffness (AVBD k)
+  float* c_ke;    // per-contact averaged stiffness (ceiling)
+  float* c_kd;
+  float* c_mu;
+  float soft_ke, soft_kd, soft_mu;
+  const float* shape_ke;
+  const float* shape_kd;
+  const float* shape_mu;
+  const int* shape_body;
+  const float* body_com;
+  const float* body_q;
+  const float* body_q_prev;
+  const float* body_qd;
+  float k_start;
+  R beta;
+  R dt, dt2r, fric_eps;
+  float fp64_thr;
+  int* err;
+  double* residual;  // [iterations] (MIXED)
+  int V;
+  int S;  // shape count
+};
+
+__device__ __forceinline__ void set_err(int* err, int bit) {
+  if (err) atomicOr(err, bit);
+}
+
+__device__ __forceinline__ vec3<float> ldv3(const float* a, int i) { return {a[3 * i], a[3 * i + 1], a[3 * i + 2]}; }
+
+// rotate v by quaternion (x, y, z, w)
+__device__ __forceinline__ vec3<float> qrot(const float* q, vec3<float> v) {
+  const vec3<float> u = {q[0], q[1], q[2]};
+  const float w = q[3];
+  return v * (2.f * w * w - 1.f) + cross(u, v) * (2.f * w) + u * (2.f * dot(u, v));
+}
+
+// ---------------------------------------------------------------------------------------------
+// forward step of one particle: particle_vbd_kernels.py:1782-1807
+template <typename R>
+__device__ __forceinline__ void forward_particle(const StepCtx<R>& c, int i) {
+  const vec3<R> q = {c.q_in[3 * i], c.q_in[3 * i + 1], c.q_in[3 * i + 2]};
+  const int fl = c.flags[i];
+  const float im = c.inv_mass[i];
+  const float m = c.mass[i];
+  const R msolve = ((fl & 1) && m != 0.f) ? R(m) : R(0);
+  c.qprev[i] = pk4(q, R(0));
+  if (!(fl & 1) || im == 0.f) {
+    c.inertia[i] = pk4(q, msolve);
+    c.pos[i] = pk4(q, R(0));
+    return;
+  }
+  const vec3<R> g = {R(c.gravity[0]), R(c.gravity[1]), R(c.gravity[2])};
+  vec3<R> fe = zero3<R>();
+  if (c.f_ext) fe = {c.f_ext[3 * i], c.f_ext[3 * i + 1], c.f_ext[3 * i + 2]};
+  const vec3<R> v = vec3<R>{c.qd_in[3 * i], c.qd_in[3 * i + 1], c.qd_in[3 * i + 2]} + (g + fe * R(im)) * c.dt;
+  const vec3<R> d = v * c.dt;
+  c.inertia[i] = pk4(q + d, msolve);
+  c.pos[i] = pk4(q + d, R(0));
+}
+
+// velocity update and state write-back: particle_vbd_kernels.py:1900-1903, solver_vbd.py:2335-2337
+template <typename R>
+__device__ __forceinline__ void finalize_particle(const StepCtx<R>& c, int i) {
+  const vec3<R> p = ld3<R>(c.pos[i]);
+  const vec3<R> qp = ld3<R>(c.qprev[i]);
+  const vec3<R> v = (p - qp) * (R(1) / c.dt);
+  c.q_in[3 * i] = p.x;
+  c.q_in[3 * i + 1] = p.y;
+  c.q_in[3 * i + 2] = p.z;
+  c.q_out[3 * i] = p.x;
+  c.q_out[3 * i + 1] = p.y;
+  c.q_out[3 * i + 2] = p.z;
+  c.qd_out[3 * i] = v.x;
+  c.qd_out[3 * i + 1] = v.y;
+  c.qd_out[3 * i + 2] = v.z;
+}
+
+// contact terms of one particle (lane 0 of the group)
+template <typename R>
+__device__ __forceinline__ void contacts_add(const StepCtx<R>& c, int v, vec3<R> x, vec3<R>& f, sym3<R>& H) {
+  int n = c.slot_cnt[v];
+  if (n <= 0) return;
+  if (n > c.K) n = c.K;
+  int ids[8];
+  for (int j = 0; j < n; ++j) ids[j] = c.slots[v * c.K + j];
+  // contact index order, as the reference's launch order over contacts
+  for (int a = 1; a < n; ++a) {
+    int key = ids[a], b = a - 1;
+    while (b >= 0 && ids[b] > key) {
+      ids[b + 1] = ids[b];
+      --b;
+    }
+    ids[b + 1] = key;
+  }
+  const R r = R(c.radius[v]);
+  for (int j = 0; j < n; ++j) {
+    const int t = ids[j];
+    const int s = c.c_shape[t];
+    const int b = (c.shape_body && s >= 0) ? c.shape_body[s] : -1;
+    const vec3<float> bp = ldv3(c.c_body_pos, t);
+    vec3<float> bxf = bp;
+    const float* X = (b >= 0 && c.body_q) ? c.body_q + 7 * b : nullptr;
+    if (X) bxf = qrot(X + 3, bp) + vec3<float>{X[0], X[1], X[2]};
+    const vec3<R> bx = {R(bxf.x), R(bxf.y), R(bxf.z)};
+    const vec3<float> nf = ldv3(c.c_normal, t);
+    const vec3<R> nn = {R(nf.x), R(nf.y), R(nf.z)};
+    const R pen = -(dot(nn, x - bx) - r);
+    R k = R(c.c_k[t]);
+    if (c.beta != R(0)) {
+      // AVBD penalty ramp with the position at the start of this iteration (unchanged until now)
+      k = vmin(k + c.beta * vmax(R(0), pen), R(c.c_ke[t]));
+      c.c_k[t] = float(k);
+    }
+    if (pen > R(0)) {
+      const vec3<R> dx = x - ld3<R>(c.qprev[v]);
+      const vec3<float> bvl = ldv3(c.c_body_vel, t);
+      vec3<float> bv = bvl;
+      if (X) {
+        bv = qrot(X + 3, bvl);
+        if (c.body_q_prev) {
+          const float* Xp = c.body_q_prev + 7 * b;
+          const vec3<float> bxp = qrot(Xp + 3, bp) + vec3<float>{Xp[0], Xp[1], Xp[2]};
+          bv = (bxf - bxp) * (1.f / float(c.dt)) + bv;
+        } else if (c.body_qd) {
+          const float* qd = c.body_qd + 6 * b;
+          vec3<float> com = c.body_com ? ldv3(c.body_com, b) : vec3<float>{0.f, 0.f, 0.f};
+          const vec3<float> rr = bxf - (qrot(X + 3, com) + vec3<float>{X[0], X[1], X[2]});
+          bv = vec3<float>{qd[0], qd[1], qd[2]} + cross(vec3<float>{qd[3], qd[4], qd[5]}, rr) + bv;
+        }
+      }
+      const vec3<R> rel = dx - vec3<R>{R(bv.x), R(bv.y), R(bv.z)} * c.dt;
+      contact_add<R>(pen, nn, rel, k, R(c.c_kd[t]), R(c.c_mu[t]), c.fric_eps, c.dt, f, H);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// One vertex solved by L lanes. All lanes of the warp must call this (it shuffles).
+template <typename R, int L, int MODE>
+__device__ __forceinline__ void solve_group(const StepCtx<R>& c, int v, bool valid, int sub, int iteration) {
+  vec3<R> f = zero3<R>();
+  sym3<R> H = szero<R>();
+  R m = R(0);
+  if (valid) m = R(c.inertia[v].w);
+  const bool active = valid && m != R(0);
+  if (active) {
+    const int fb = __ldg(c.face_off + v), fe = __ldg(c.face_off + v + 1);
+    const int eb = __ldg(c.edge_off + v), ee = __ldg(c.edge_off + v + 1);
+    const int nf = fe - fb;
+    const int n = nf + (ee - eb);
+    for (int it = sub; it < n; it += L) {
+      if (it < nf) {
+        const int a = __ldg(c.face_adj + fb + it);
+        const int t = a >> 2, ord = a & 3;
+        const float4 mat = __ldg(c.tri_mat + t);
+        if (mat.x > 0.f || mat.y > 0.f) {
+          const int4 ti = __ldg(c.tri_idx + t);
+          const float4 P = __ldg(c.tri_pose + t);
+          const R pose[4] = {R(P.x), R(P.y), R(P.z), R(P.w)};
+          const vec3<R> x0 = ld3<R>(c.pos[ti.x]), x1 = ld3<R>(c.pos[ti.y]), x2 = ld3<R>(c.pos[ti.z]);
+          vec3<R> xp[3];
+          if (mat.z > 0.f) {
+            xp[0] = ld3<R>(c.qprev[ti.x]);
+            xp[1] = ld3<R>(c.qprev[ti.y]);
+            xp[2] = ld3<R>(c.qprev[ti.z]);
+          }
+          membrane_add<R>(ord, x0, x1, x2, pose, R(mat.x), R(mat.y), R(mat.z), R(mat.w), c.dt, xp, f, H);
+        }
+      } else {
+        const int a = __ldg(c.edge_adj + eb + (it - nf));
+        const int e = a >> 2, ord = a & 3;
+        const float4 pr = __ldg(c.edge_prop + e);
+        if (pr.z > 0.f) {
+          const int4 ei = __ldg(c.edge_idx + e);
+          vec3<R> x[4];
+          x[0] = ld3<R>(c.pos[ei.x]);
+          x[1] = ld3<R>(c.pos[ei.y]);
+          x[2] = ld3<R>(c.pos[ei.z]);
+          x[3] = ld3<R>(c.pos[ei.w]);
+          vec3<R> xp[4];
+          if (pr.w > 0.f) {
+            xp[0] = ld3<R>(c.qprev[ei.x]);
+            xp[1] = ld3<R>(c.qprev[ei.y]);
+            xp[2] = ld3<R>(c.qprev[ei.z]);
+            xp[3] = ld3<R>(c.qprev[ei.w]);
+          }
+          bending_add<R>(ord, x, R(pr.x), R(pr.y), R(pr.z), R(pr.w), c.dt, xp, f, H);
+        }
+      }
+    }
+  }
+  if (L > 1) {
+    f.x = group_sum<L>(f.x);
+    f.y = group_sum<L>(f.y);
+    f.z = group_sum<L>(f.z);
+    H.xx = group_sum<L>(H.xx);
+    H.yy = group_sum<L>(H.yy);
+    H.zz = group_sum<L>(H.zz);
+    H.xy = group_sum<L>(H.xy);
+    H.xz = group_sum<L>(H.xz);
+    H.yz = group_sum<L>(H.yz);
+  }
+  const bool leader = active && sub == 0;
+  vec3<R> x = zero3<R>();
+  if (leader) {
+    x = ld3<R>(c.pos[v]);
+    const vec3<R> in = ld3<R>(c.inertia[v]);
+    const R md = m * c.dt2r;
+    f = f + md * (in - x);
+    H.xx += md;
+    H.yy += md;
+    H.zz += md;
+    if (c.has_contacts) contacts_add<R>(c, v, x, f, H);
+  }
+  if (MODE == MODE_MIXED && c.residual) {
+    // FP64 reduction of |f|^2 (the force residual the block solve removes): warp sum, one atomic per warp
+    double r2 = leader ? double(f.x) * double(f.x) + double(f.y) * double(f.y) + double(f.z) * double(f.z) : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+    if ((threadIdx.x & 31) == 0 && r2 != 0.0) atomicAdd(c.residual + iteration, r2);
+  }
+  if (!leader) return;
+  vec3<R> dlt;
+  bool ok;
+  if (MODE == MODE_MIXED) {
+    const R hmax = vmax(vmax(vmax(vabs(H.xx), vabs(H.yy)), vmax(vabs(H.zz), vabs(H.xy))), vmax(vabs(H.xz), vabs(H.yz)));
+    const R d = sdet(H);
+    if (vabs(d) < R(c.fp64_thr) * hmax * hmax * hmax) {
+      const sym3<double> Hd = {double(H.xx), double(H.yy), double(H.zz), double(H.xy), double(H.xz), double(H.yz)};
+      const vec3<double> fd = {double(f.x), double(f.y), double(f.z)};
+      const double dd = sdet(Hd);
+      ok = fabs(dd) > 1e-8;
+      const vec3<double> r = sadj_mul(Hd, fd) * (1.0 / dd);
+      dlt = {R(r.x), R(r.y), R(r.z)};
+    } else {
+      ok = vabs(d) > R(1e-8);
+      dlt = sadj_mul(H, f) * (R(1) / d);
+    }
+  } else {
+    const R d = sdet(H);
+    ok = vabs(d) > R(1e-8);
+    dlt = sadj_mul(H, f) * (R(1) / d);
+  }
+  if (!ok) {
+    set_err(c.err, 4);
+    return;
+  }
+  const vec3<R> xn = x + dlt;
+  if (!(isfinite(double(xn.x)) && isfinite(double(xn.y)) && isfinite(double(xn.z)))) {
+    set_err(c.err, 1);
+    return;
+  }
+  c.pos[v] = pk4(xn, R(0));
+}
+
+// ---------------------------------------------------------------------------------------------
+template <typename R>
+__global__ void k_forward(StepCtx<R> c) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= c.V) return;
+  forward_particle(c, i);
+  if (c.has_contacts) c.slot_cnt[i] = 0;
+}
+
+template <typename R>
+__global__ void k_finalize(StepCtx<R> c) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= c.V) return;
+  finalize_particle(c, i);
+}
+
+// Per-contact setup (init_body_particle_contacts, rigid_vbd_kernels.py:2318-2361) and the
+// particle -> contact slot table. Must run after the slot counters were cleared.
+template <typename R>
+__global__ void k_contact_prepare(StepCtx<R> c) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int count = *c.c_count;
+  if (count > c.c_max) count = c.c_max;
+  if (t >= count) return;
+  const int p = c.c_particle[t];
+  const int s = c.c_shape[t];
+  if (p < 0 || p >= c.V || s < 0 || s >= c.S) {
+    set_err(c.err, 8);
+    return;
+  }
+  const float ke = 0.5f * (c.soft_ke + c.shape_ke[s]);
+  const float kd = 0.5f * (c.soft_kd + c.shape_kd[s]);
+  const float mu = sqrtf(c.soft_mu * c.shape_mu[s]);
+  c.c_ke[t] = ke;
+  c.c_kd[t] = kd;
+  c.c_mu[t] = mu;
+  c.c_k[t] = c.k_start < 0.f ? ke : fminf(c.k_start, ke);
+  const int slot = atomicAdd(c.slot_cnt + p, 1);
+  if (slot < c.K)
+    c.slots[p * c.K + slot] = t;
+  else
+    set_err(c.err, 2);
+}
+
+template <typename R, int L, int MODE>
+__global__ void k_color(StepCtx<R> c, const int* __restrict__ verts, int n, int iteration) {
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int grp = gid / L, sub = gid % L;
+  const bool valid = grp < n;
+  const int v = valid ? __ldg(verts + grp) : 0;
+  solve_group<R, L, MODE>(c, v, valid, sub, iteration);
+}
+
+struct PersistentPlan {
+  int W;                      // instances
+  const int* inst_order;      // [W] processing order (largest first)
+  const int* inst_vstart;     // [W+1]
+  const int* inst_cptr;       // [W+1] into color_ranges: instance w owns ranges[cptr[w] .. cptr[w+1]]
+  const int* color_ranges;    // per instance: ncol+1 offsets into color_verts
+  const int* color_verts;     // particle ids grouped by instance then color
+  int* queue;                 // work counter, zero before launch
+  int iterations;
+};
+
+template <typename R, int L, int MODE>
+__global__ void k_persistent(StepCtx<R> c, PersistentPlan p) {
+  __shared__ int s_item;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = atomicAdd(p.queue, 1);
+    __syncthreads();
+    const int q = s_item;
+    if (q >= p.W) return;
+    const int w = __ldg(p.inst_order + q);
+    const int vs = __ldg(p.inst_vstart + w), ve = __ldg(p.inst_vstart + w + 1);
+    for (int i = vs + threadIdx.x; i < ve; i += blockDim.x) forward_particle(c, i);
+    __syncthreads();
+    const int cb = __ldg(p.inst_cptr + w), ce = __ldg(p.inst_cptr + w + 1);
+    const int per_round = blockDim.x / L;
+    const int grp_local = threadIdx.x / L, sub = threadIdx.x % L;
+    for (int it = 0; it < p.iterations; ++it) {
+      for (int col = cb; col + 1 < ce; ++col) {
+        const int a = __ldg(p.color_ranges + col), b = __ldg(p.color_ranges + col + 1);
+        for (int base = a; base < b; base += per_round) {
+          const int g = base + grp_local;
+          const bool valid = g < b;
+          const int v = valid ? __ldg(p.color_verts + g) : 0;
+          solve_group<R, L, MODE>(c, v, valid, sub, it);
+        }
+        __syncthreads();
+      }
+    }
+    for (int i = vs + threadIdx.x; i < ve; i += blockDim.x) finalize_particle(c, i);
+  }
+}
+
+}  // namespace vbd

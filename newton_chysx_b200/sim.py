@@ -1,0 +1,705 @@
+"""Cloth-side mirror of the reference's simulation data model (``newton/_src/sim``).
+
+The solver boundary is ``SolverVBD.step(state_in, state_out, control, contacts, dt)``; this module
+provides the objects that call carries, with the reference's field names and array layouts
+(``Model``, ``State``, ``Control``, ``Contacts``), plus the part of ``ModelBuilder`` that builds
+cloth (``add_cloth_grid``, ``add_cloth_mesh``, ``add_triangles``, ``add_edges``, ``color``,
+``add_world``, ground plane and sphere shapes) and a ``CollisionPipeline`` for particle-shape soft
+contacts. Arrays are torch tensors: float32 ``(N, 3)`` for vec3, ``(T, 2, 2)`` for mat22, int32
+indices — the memory layout of the reference's Warp arrays.
+
+Builder math follows ``newton/_src/sim/builder.py`` (``add_triangles :7716-7826``,
+``add_edges :7966-8061``, ``add_cloth_grid :8063-8186``, ``add_cloth_mesh :8188-8341``,
+``color :9304-9396``, world merge ``:3185-3193``), ``newton/_src/utils/mesh.py`` (``MeshAdjacency
+:183-262``) and ``newton/_src/sim/graph_coloring.py`` (``combine_independent_particle_coloring
+:382-426``), vectorised with numpy.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import enum
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+class ParticleFlags(enum.IntEnum):
+    """``newton/_src/geometry/flags.py:8-14``."""
+
+    ACTIVE = 1 << 0
+
+
+class GeoType(enum.IntEnum):
+    PLANE = 0
+    SPHERE = 1
+
+
+@dataclasses.dataclass
+class ShapeConfig:
+    """Material of a collision shape (the reference's ``ModelBuilder.ShapeConfig`` defaults)."""
+
+    ke: float = 2.5e3
+    kd: float = 100.0
+    mu: float = 1.0
+
+
+# ----------------------------------------------------------------------------- quaternions (x, y, z, w)
+def quat_identity():
+    return (0.0, 0.0, 0.0, 1.0)
+
+
+def quat_from_axis_angle(axis, angle):
+    a = np.asarray(axis, dtype=np.float64)
+    a = a / np.linalg.norm(a)
+    s = math.sin(angle * 0.5)
+    return (float(a[0] * s), float(a[1] * s), float(a[2] * s), math.cos(angle * 0.5))
+
+
+def quat_to_matrix(q):
+    x, y, z, w = (float(v) for v in q)
+    u = np.array([x, y, z])
+    e = np.eye(3)
+    cols = [e[i] * (2.0 * w * w - 1.0) + np.cross(u, e[i]) * 2.0 * w + u * 2.0 * np.dot(u, e[i]) for i in range(3)]
+    return np.stack(cols, axis=1)
+
+
+# ----------------------------------------------------------------------------- mesh adjacency
+def mesh_hinges(tri: np.ndarray) -> np.ndarray:
+    """Hinges ``(o0, o1, v0, v1)`` of a triangle mesh, in the order ``MeshAdjacency`` creates them.
+
+    For every triangle (in order) and its edges (0,1), (1,2), (2,0): the first triangle that has an
+    undirected edge fixes ``v0, v1`` (its winding) and ``o0``; the second sets ``o1``; edges with a
+    single triangle keep ``o1 = -1``; further triangles on a non-manifold edge are ignored.
+    """
+    tri = np.asarray(tri, dtype=np.int64).reshape(-1, 3)
+    if len(tri) == 0:
+        return np.zeros((0, 4), dtype=np.int32)
+    i0 = np.stack([tri[:, 0], tri[:, 1], tri[:, 2]], axis=1).reshape(-1)
+    i1 = np.stack([tri[:, 1], tri[:, 2], tri[:, 0]], axis=1).reshape(-1)
+    op = np.stack([tri[:, 2], tri[:, 0], tri[:, 1]], axis=1).reshape(-1)
+    lo, hi = np.minimum(i0, i1), np.maximum(i0, i1)
+    key = lo * (int(hi.max()) + 1) + hi
+    order = np.argsort(key, kind="stable")
+    ks = key[order]
+    start = np.ones(len(ks), dtype=bool)
+    start[1:] = ks[1:] != ks[:-1]
+    group_start = np.nonzero(start)[0]
+    first = order[group_start]
+    has_second = np.zeros(len(group_start), dtype=bool)
+    second = np.full(len(group_start), -1, dtype=np.int64)
+    nxt = group_start + 1
+    ok = nxt < len(ks)
+    ok[ok] &= ~start[nxt[ok]]
+    has_second[ok] = True
+    second[ok] = order[nxt[ok]]
+    creation = np.argsort(first, kind="stable")
+    first, second, has_second = first[creation], second[creation], has_second[creation]
+    out = np.empty((len(first), 4), dtype=np.int64)
+    out[:, 0] = op[first]
+    out[:, 1] = np.where(has_second, op[np.maximum(second, 0)], -1)
+    out[:, 2] = i0[first]
+    out[:, 3] = i1[first]
+    return out.astype(np.int32)
+
+
+def combine_independent_particle_coloring(groups_1, groups_2):
+    """Merge the colorings of two disconnected graphs (graph_coloring.py:382-426): the longer list is
+    sorted by ascending group size, the shorter by descending size, and groups of equal rank join."""
+    if len(groups_1) == 0:
+        return groups_2
+    if len(groups_2) == 0:
+        return groups_1
+    n = max(len(groups_1), len(groups_2))
+    if len(groups_1) < len(groups_2):
+        groups_1, groups_2 = groups_2, groups_1
+    g1 = sorted(groups_1, key=len)
+    g2 = sorted(groups_2, key=lambda g: -len(g))
+    out = []
+    for i in range(n):
+        a = g1[i] if i < len(g1) else None
+        b = g2[i] if i < len(g2) else None
+        if a is not None and b is not None:
+            out.append(np.concatenate([a, b]))
+        elif a is not None:
+            out.append(a)
+        else:
+            out.append(b)
+    return out
+
+
+class _ChunkedGroup:
+    """A color group kept as a list of arrays so that merging many worlds stays linear."""
+
+    __slots__ = ("chunks", "size")
+
+    def __init__(self, chunks, size):
+        self.chunks = chunks
+        self.size = size
+
+    def __len__(self):
+        return self.size
+
+    def array(self):
+        if len(self.chunks) == 1:
+            return self.chunks[0]
+        return np.concatenate(self.chunks).astype(np.int32)
+
+
+def _merge_chunked(groups_1, groups_2):
+    """``combine_independent_particle_coloring`` on chunked groups (same ordering rule)."""
+    if len(groups_1) == 0:
+        return groups_2
+    if len(groups_2) == 0:
+        return groups_1
+    n = max(len(groups_1), len(groups_2))
+    if len(groups_1) < len(groups_2):
+        groups_1, groups_2 = groups_2, groups_1
+    g1 = sorted(groups_1, key=len)
+    g2 = sorted(groups_2, key=lambda g: -len(g))
+    out = []
+    for i in range(n):
+        a = g1[i] if i < len(g1) else None
+        b = g2[i] if i < len(g2) else None
+        if a is not None and b is not None:
+            out.append(_ChunkedGroup(a.chunks + b.chunks, a.size + b.size))
+        else:
+            out.append(a if a is not None else b)
+    return out
+
+
+def color_particles(n, tri_indices, tri_materials, edge_indices, edge_props, include_bending=False,
+                    balance_colors=True, target_max_min_color_ratio=1.1):  # fmt: skip
+    """Color groups (list of int32 arrays, particles in index order) for VBD's Gauss-Seidel sweep."""
+    if n == 0:
+        return []
+    lib = _lib.load()
+    tri = np.ascontiguousarray(np.asarray(tri_indices, dtype=np.int32).reshape(-1, 3))
+    tm = np.ascontiguousarray(np.asarray(tri_materials, dtype=np.float32).reshape(-1, 5))
+    ed = np.ascontiguousarray(np.asarray(edge_indices, dtype=np.int32).reshape(-1, 4))
+    ep = np.ascontiguousarray(np.asarray(edge_props, dtype=np.float32).reshape(-1, 2))
+    if len(tri) == 0 and (not include_bending or len(ed) == 0):
+        return [np.arange(n, dtype=np.int32)]
+    colors = np.zeros(n, dtype=np.int32)
+    ip = C.POINTER(C.c_int32)
+    fp = C.POINTER(C.c_float)
+    ncol = lib.vbd_color_particles(
+        n, len(tri), tri.ctypes.data_as(ip), tm.ctypes.data_as(fp), len(ed), ed.ctypes.data_as(ip),
+        ep.ctypes.data_as(fp), int(bool(include_bending)), float(target_max_min_color_ratio if balance_colors else 0.0),
+        colors.ctypes.data_as(ip),
+    )  # fmt: skip
+    if ncol < 0:
+        _lib.check(ncol, "vbd_color_particles")
+    order = np.argsort(colors, kind="stable")
+    bounds = np.searchsorted(colors[order], np.arange(ncol + 1))
+    return [order[bounds[c]:bounds[c + 1]].astype(np.int32) for c in range(ncol)]
+
+
+# ----------------------------------------------------------------------------- builder
+class ModelBuilder:
+    """The cloth subset of the reference ``ModelBuilder``."""
+
+    ShapeConfig = ShapeConfig
+
+    def __init__(self, up_axis="Z", gravity: float = -9.81):
+        self.up_axis = {"X": 0, "Y": 1, "Z": 2}[up_axis.upper()] if isinstance(up_axis, str) else int(up_axis)
+        self.gravity = gravity
+        self.default_particle_radius = 0.1
+        self.default_tri_ke = 100.0
+        self.default_tri_ka = 100.0
+        self.default_tri_kd = 10.0
+        self.default_tri_drag = 0.0
+        self.default_tri_lift = 0.0
+        self.default_edge_ke = 100.0
+        self.default_edge_kd = 0.0
+        self.default_shape_cfg = ShapeConfig()
+        self._q, self._qd, self._mass, self._radius, self._flags, self._world = [], [], [], [], [], []
+        self._tri, self._tri_pose, self._tri_mat, self._tri_area = [], [], [], []
+        self._edge, self._edge_angle, self._edge_len, self._edge_prop = [], [], [], []
+        self._n = 0
+        self._t = 0
+        self._e = 0
+        self.shapes = []  # dicts: type, pos, normal, radius, ke, kd, mu, body
+        self._color_groups: list[_ChunkedGroup] = []
+        self.world_count = 0
+        self.current_world = -1
+        self.world_particle_start: list[int] = []
+
+    # -- counts
+    @property
+    def particle_count(self):
+        return self._n
+
+    @property
+    def tri_count(self):
+        return self._t
+
+    @property
+    def edge_count(self):
+        return self._e
+
+    @property
+    def shape_count(self):
+        return len(self.shapes)
+
+    @property
+    def up_vector(self):
+        v = [0.0, 0.0, 0.0]
+        v[self.up_axis] = 1.0
+        return tuple(v)
+
+    def _cat(self, lst, shape, dtype):
+        if not lst:
+            return np.zeros(shape, dtype=dtype)
+        return np.concatenate([np.asarray(a, dtype=dtype).reshape(shape) for a in lst])
+
+    @property
+    def particle_q(self):
+        return self._cat(self._q, (-1, 3), np.float64)
+
+    @property
+    def particle_mass(self):
+        return self._cat(self._mass, (-1,), np.float64)
+
+    @property
+    def particle_flags(self):
+        return self._cat(self._flags, (-1,), np.int32)
+
+    @property
+    def tri_indices(self):
+        return self._cat(self._tri, (-1, 3), np.int32)
+
+    @property
+    def tri_materials(self):
+        return self._cat(self._tri_mat, (-1, 5), np.float64)
+
+    @property
+    def edge_indices(self):
+        return self._cat(self._edge, (-1, 4), np.int32)
+
+    @property
+    def edge_bending_properties(self):
+        return self._cat(self._edge_prop, (-1, 2), np.float64)
+
+    def _set_particle_column(self, lst_name, values):
+        arr = self._cat(getattr(self, lst_name), (-1,), np.float64 if lst_name != "_flags" else np.int32)
+        arr[:] = values
+        setattr(self, lst_name, [arr])
+
+    def set_particle_flags(self, flags):
+        self._set_particle_column("_flags", np.asarray(flags, dtype=np.int32))
+
+    def set_particle_mass(self, mass):
+        self._set_particle_column("_mass", np.asarray(mass, dtype=np.float64))
+
+    # -- particles
+    def add_particles(self, pos, vel, mass, radius=None, flags=None):
+        pos = np.asarray(pos, dtype=np.float64).reshape(-1, 3)
+        n = len(pos)
+        self._q.append(pos)
+        self._qd.append(np.broadcast_to(np.asarray(vel, dtype=np.float64), (n, 3)).copy())
+        self._mass.append(np.broadcast_to(np.asarray(mass, dtype=np.float64), (n,)).copy())
+        r = self.default_particle_radius if radius is None else radius
+        self._radius.append(np.broadcast_to(np.asarray(r, dtype=np.float64), (n,)).copy())
+        f = int(ParticleFlags.ACTIVE) if flags is None else flags
+        self._flags.append(np.broadcast_to(np.asarray(f, dtype=np.int32), (n,)).copy())
+        self._world.append(np.full(n, self.current_world, dtype=np.int32))
+        start = self._n
+        self._n += n
+        return start
+
+    def add_particle(self, pos, vel, mass, radius=None, flags=None):
+        return self.add_particles([pos], [vel], [mass], radius, flags)
+
+    # -- triangles (builder.py:7716-7826)
+    def add_triangles(self, i, j, k, tri_ke=None, tri_ka=None, tri_kd=None, tri_drag=None, tri_lift=None):
+        i = np.asarray(i, dtype=np.int64)
+        j = np.asarray(j, dtype=np.int64)
+        k = np.asarray(k, dtype=np.int64)
+        q = self.particle_q
+        p, qq, r = q[i], q[j], q[k]
+        qp, rp = qq - p, r - p
+
+        def normalized(a):
+            ln = np.linalg.norm(a, axis=-1, keepdims=True)
+            ln[ln == 0] = 1.0
+            return a / ln
+
+        nrm = normalized(np.cross(qp, rp))
+        e1 = normalized(qp)
+        e2 = normalized(np.cross(nrm, e1))
+        R = np.concatenate((e1[..., None], e2[..., None]), axis=-1)
+        M = np.concatenate((qp[..., None], rp[..., None]), axis=-1)
+        D = np.matmul(R.transpose(0, 2, 1), M)
+        areas = np.linalg.det(D) / 2.0
+        areas[areas < 0.0] = 0.0
+        valid = areas > 0.0
+        D[~valid] = np.eye(2)
+        inv_D = np.linalg.inv(D)
+        n = len(i)
+
+        def col(v, d):
+            return np.broadcast_to(np.asarray(d if v is None else v, dtype=np.float64), (n,))
+
+        mats = np.stack([col(tri_ke, self.default_tri_ke), col(tri_ka, self.default_tri_ka),
+                         col(tri_kd, self.default_tri_kd), col(tri_drag, self.default_tri_drag),
+                         col(tri_lift, self.default_tri_lift)], axis=1)  # fmt: skip
+        self._tri.append(np.stack([i, j, k], axis=1)[valid].astype(np.int32))
+        self._tri_pose.append(inv_D[valid])
+        self._tri_mat.append(mats[valid])
+        self._tri_area.append(areas[valid])
+        self._t += int(valid.sum())
+        return areas
+
+    # -- bending hinges (builder.py:7966-8061)
+    def add_edges(self, i, j, k, l, rest=None, edge_ke=None, edge_kd=None):  # noqa: E741
+        i_, j_, k_, l_ = (np.asarray(a, dtype=np.int64) for a in (i, j, k, l))
+        q = self.particle_q
+        x3, x4 = q[k_], q[l_]
+        n = len(i_)
+        if rest is None:
+            rest = np.zeros(n, dtype=np.float64)
+            valid = (i_ != -1) & (j_ != -1)
+            x1, x2 = q[i_[valid]], q[j_[valid]]
+            x3v, x4v = x3[valid], x4[valid]
+
+            def normalized(a):
+                ln = np.linalg.norm(a, axis=-1, keepdims=True)
+                ln[ln == 0] = 1.0
+                return a / ln
+
+            n1 = normalized(np.cross(x3v - x1, x4v - x1))
+            n2 = normalized(np.cross(x4v - x2, x3v - x2))
+            e = normalized(x4v - x3v)
+            cos_t = np.clip((n1 * n2).sum(-1), -1.0, 1.0)
+            sin_t = (np.cross(n1, n2) * e).sum(-1)
+            rest[valid] = np.arctan2(sin_t, cos_t)
+        ke = np.broadcast_to(np.asarray(self.default_edge_ke if edge_ke is None else edge_ke, dtype=np.float64), (n,))
+        kd = np.broadcast_to(np.asarray(self.default_edge_kd if edge_kd is None else edge_kd, dtype=np.float64), (n,))
+        self._edge.append(np.stack([i_, j_, k_, l_], axis=1).astype(np.int32))
+        self._edge_angle.append(np.asarray(rest, dtype=np.float64))
+        self._edge_len.append(np.linalg.norm(x4 - x3, axis=1))
+        self._edge_prop.append(np.stack([ke, kd], axis=1))
+        self._e += n
+
+    # -- cloth (builder.py:8063-8341)
+    def add_cloth_mesh(self, pos, rot, scale, vel, vertices, indices, density, tri_ke=None, tri_ka=None, tri_kd=None,
+                       tri_drag=None, tri_lift=None, edge_ke=None, edge_kd=None, particle_radius=None):  # fmt: skip
+        tri_ke = self.default_tri_ke if tri_ke is None else tri_ke
+        tri_ka = self.default_tri_ka if tri_ka is None else tri_ka
+        tri_kd = self.default_tri_kd if tri_kd is None else tri_kd
+        tri_drag = self.default_tri_drag if tri_drag is None else tri_drag
+        tri_lift = self.default_tri_lift if tri_lift is None else tri_lift
+        edge_ke = self.default_edge_ke if edge_ke is None else edge_ke
+        edge_kd = self.default_edge_kd if edge_kd is None else edge_kd
+        radius = self.default_particle_radius if particle_radius is None else particle_radius
+        verts = np.asarray(vertices, dtype=np.float64).reshape(-1, 3) * scale
+        rot_m = quat_to_matrix(rot).astype(np.float32).astype(np.float64)
+        verts3 = verts @ rot_m.T + np.asarray(pos, dtype=np.float64)
+        nv = len(verts3)
+        start = self.add_particles(verts3, vel, np.zeros(nv), radius=radius)
+        inds = (start + np.asarray(indices, dtype=np.int64)).reshape(-1, 3)
+        t0 = self._t
+        areas = self.add_triangles(inds[:, 0], inds[:, 1], inds[:, 2], tri_ke, tri_ka, tri_kd, tri_drag, tri_lift)
+        mass = self.particle_mass
+        add = density * areas / 3.0
+        for c in range(3):
+            np.add.at(mass, inds[:, c], add)
+        self._mass = [mass]
+        tris = self.tri_indices[t0:self._t]
+        hinges = mesh_hinges(tris)
+        self.add_edges(hinges[:, 0], hinges[:, 1], hinges[:, 2], hinges[:, 3], edge_ke=edge_ke, edge_kd=edge_kd)
+
+    def add_cloth_grid(self, pos, rot, vel, dim_x, dim_y, cell_x, cell_y, mass, reverse_winding=False,
+                       fix_left=False, fix_right=False, fix_top=False, fix_bottom=False, tri_ke=None, tri_ka=None,
+                       tri_kd=None, tri_drag=None, tri_lift=None, edge_ke=None, edge_kd=None, particle_radius=None):  # fmt: skip
+        xs, ys = np.meshgrid(np.arange(dim_x + 1), np.arange(dim_y + 1))
+        vertices = np.stack([xs.ravel() * cell_x, ys.ravel() * cell_y, np.zeros(xs.size)], axis=1)
+        cx, cy = np.meshgrid(np.arange(1, dim_x + 1), np.arange(1, dim_y + 1))
+        cx, cy = cx.ravel(), cy.ravel()
+        w = dim_x + 1
+        v0 = (cy - 1) * w + (cx - 1)
+        v1 = (cy - 1) * w + cx
+        v2 = cy * w + cx
+        v3 = cy * w + (cx - 1)
+        if reverse_winding:
+            idx = np.stack([v0, v1, v2, v0, v2, v3], axis=1)
+        else:
+            idx = np.stack([v0, v1, v3, v1, v2, v3], axis=1)
+        start = self._n
+        total_mass = mass * (dim_x + 1) * (dim_x + 1)
+        total_area = cell_x * cell_y * dim_x * dim_y
+        density = total_mass / total_area
+        self.add_cloth_mesh(pos, rot, 1.0, vel, vertices, idx.reshape(-1), density, tri_ke, tri_ka, tri_kd, tri_drag,
+                            tri_lift, edge_ke, edge_kd, particle_radius)  # fmt: skip
+        gx, gy = xs.ravel(), ys.ravel()
+        fixed = (
+            ((gx == 0) & fix_left) | ((gx == dim_x) & fix_right) | ((gy == 0) & fix_bottom) | ((gy == dim_y) & fix_top)
+        )
+        flags = self.particle_flags
+        m = self.particle_mass
+        sl = slice(start, start + len(gx))
+        flags[sl] = np.where(fixed, flags[sl] & ~int(ParticleFlags.ACTIVE), int(ParticleFlags.ACTIVE))
+        m[sl] = np.where(fixed, 0.0, mass)
+        self._flags = [flags]
+        self._mass = [m]
+
+    # -- shapes
+    def add_ground_plane(self, cfg: ShapeConfig | None = None):
+        cfg = cfg or self.default_shape_cfg
+        self.shapes.append(dict(type=GeoType.PLANE, pos=(0.0, 0.0, 0.0), normal=self.up_vector, radius=0.0,
+                                ke=cfg.ke, kd=cfg.kd, mu=cfg.mu, body=-1))  # fmt: skip
+        return len(self.shapes) - 1
+
+    def add_shape_sphere(self, body=-1, xform=None, radius=1.0, cfg: ShapeConfig | None = None):
+        if body != -1:
+            raise NotImplementedError("only static spheres (body=-1) are supported")
+        cfg = cfg or self.default_shape_cfg
+        p = (0.0, 0.0, 0.0) if xform is None else tuple(float(v) for v in (xform[0] if len(xform) == 2 else xform[:3]))
+        self.shapes.append(dict(type=GeoType.SPHERE, pos=p, normal=(0.0, 0.0, 1.0), radius=float(radius), ke=cfg.ke,
+                                kd=cfg.kd, mu=cfg.mu, body=-1))  # fmt: skip
+        return len(self.shapes) - 1
+
+    # -- coloring (builder.py:9304-9396)
+    @property
+    def particle_color_groups(self) -> list[np.ndarray]:
+        return [g.array() for g in self._color_groups]
+
+    @particle_color_groups.setter
+    def particle_color_groups(self, groups):
+        self._color_groups = [_ChunkedGroup([np.asarray(g, dtype=np.int32)], len(g)) for g in groups]
+
+    def color(self, include_bending=False, balance_colors=True, target_max_min_color_ratio=1.1):
+        self.particle_color_groups = color_particles(
+            self._n, self.tri_indices, self.tri_materials, self.edge_indices, self.edge_bending_properties,
+            include_bending, balance_colors, target_max_min_color_ratio,
+        )  # fmt: skip
+
+    def set_coloring(self, groups):
+        self.particle_color_groups = groups
+
+    # -- worlds (builder.py:3038-3193)
+    def add_world(self, builder: ModelBuilder):
+        start = self._n
+        self.world_particle_start.append(start)
+        w = self.world_count
+        self.world_count += 1
+        n = builder._n
+        if n:
+            self._q.append(builder.particle_q)
+            self._qd.append(builder._cat(builder._qd, (-1, 3), np.float64))
+            self._mass.append(builder.particle_mass)
+            self._radius.append(builder._cat(builder._radius, (-1,), np.float64))
+            self._flags.append(builder.particle_flags)
+            self._world.append(np.full(n, w, dtype=np.int32))
+            self._n += n
+        if builder._t:
+            self._tri.append(builder.tri_indices + start)
+            self._tri_pose.append(builder._cat(builder._tri_pose, (-1, 2, 2), np.float64))
+            self._tri_mat.append(builder.tri_materials)
+            self._tri_area.append(builder._cat(builder._tri_area, (-1,), np.float64))
+            self._t += builder._t
+        if builder._e:
+            e = builder.edge_indices.copy()
+            e[e >= 0] += start
+            self._edge.append(e)
+            self._edge_angle.append(builder._cat(builder._edge_angle, (-1,), np.float64))
+            self._edge_len.append(builder._cat(builder._edge_len, (-1,), np.float64))
+            self._edge_prop.append(builder.edge_bending_properties)
+            self._e += builder._e
+        self.shapes.extend(dict(s) for s in builder.shapes)
+        translated = [_ChunkedGroup([c + start for c in g.chunks], g.size) for g in builder._color_groups]
+        self._color_groups = _merge_chunked(self._color_groups, translated)
+
+    def finalize(self, device="cuda") -> Model:
+        return Model._from_builder(self, device)
+
+
+# ----------------------------------------------------------------------------- model, state, contacts
+class Model:
+    """Arrays of a finalized cloth model (the reference ``Model`` fields the VBD path reads)."""
+
+    def __init__(self):
+        self.device = None
+        self.particle_count = self.tri_count = self.edge_count = self.shape_count = 0
+        self.body_count = 0
+        self.world_count = 1
+        self.spring_count = 0
+        self.tet_count = 0
+        self.soft_contact_ke = 1.0e3
+        self.soft_contact_kd = 10.0
+        self.soft_contact_mu = 0.5
+        self.soft_contact_margin = 0.01
+
+    @staticmethod
+    def _from_builder(b: ModelBuilder, device) -> Model:
+        m = Model()
+        dev = torch.device(device)
+        m.device = dev
+
+        def t(a, dtype):
+            return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device=dev)
+
+        f32, i32 = torch.float32, torch.int32
+        m.particle_count, m.tri_count, m.edge_count = b._n, b._t, b._e
+        mass = b.particle_mass
+        m.particle_q = t(b.particle_q, f32).reshape(-1, 3)
+        m.particle_qd = t(b._cat(b._qd, (-1, 3), np.float64), f32).reshape(-1, 3)
+        m.particle_mass = t(mass, f32)
+        m.particle_inv_mass = t(np.where(mass > 0.0, 1.0 / np.where(mass > 0.0, mass, 1.0), 0.0), f32)
+        m.particle_radius = t(b._cat(b._radius, (-1,), np.float64), f32)
+        m.particle_flags = t(b.particle_flags, i32)
+        m.particle_world = t(b._cat(b._world, (-1,), np.int32), i32)
+        m.tri_indices = t(b.tri_indices, i32).reshape(-1, 3)
+        m.tri_poses = t(b._cat(b._tri_pose, (-1, 2, 2), np.float64), f32).reshape(-1, 2, 2)
+        m.tri_materials = t(b.tri_materials, f32).reshape(-1, 5)
+        m.tri_areas = t(b._cat(b._tri_area, (-1,), np.float64), f32)
+        m.edge_indices = t(b.edge_indices, i32).reshape(-1, 4)
+        m.edge_rest_angle = t(b._cat(b._edge_angle, (-1,), np.float64), f32)
+        m.edge_rest_length = t(b._cat(b._edge_len, (-1,), np.float64), f32)
+        m.edge_bending_properties = t(b.edge_bending_properties, f32).reshape(-1, 2)
+        m.particle_color_groups = [t(g, i32) for g in b.particle_color_groups]
+        colors = np.full(b._n, -1, dtype=np.int32)
+        for c, g in enumerate(b.particle_color_groups):
+            colors[np.asarray(g)] = c
+        m.particle_colors = t(colors, i32)
+        nw = max(b.world_count, 1)
+        g = np.zeros((nw, 3))
+        g[:, b.up_axis] = b.gravity
+        m.gravity = t(g, f32)
+        m.up_axis = b.up_axis
+        m.world_count = nw
+        m.world_particle_start = None
+        if b.world_count > 1:
+            m.world_particle_start = np.array(b.world_particle_start + [b._n], dtype=np.int32)
+        m.shape_count = len(b.shapes)
+        S = m.shape_count
+        m.shape_type = np.array([int(s["type"]) for s in b.shapes], dtype=np.int32)
+        m.shape_pos = np.array([s["pos"] for s in b.shapes], dtype=np.float32).reshape(S, 3)
+        m.shape_normal = np.array([s["normal"] for s in b.shapes], dtype=np.float32).reshape(S, 3)
+        m.shape_radius = np.array([s["radius"] for s in b.shapes], dtype=np.float32).reshape(S)
+        m.shape_material_ke = t(np.array([s["ke"] for s in b.shapes]).reshape(S), f32)
+        m.shape_material_kd = t(np.array([s["kd"] for s in b.shapes]).reshape(S), f32)
+        m.shape_material_mu = t(np.array([s["mu"] for s in b.shapes]).reshape(S), f32)
+        m.shape_body = t(np.array([s["body"] for s in b.shapes], dtype=np.int32).reshape(S), i32)
+        m.body_com = None
+        return m
+
+    def set_gravity(self, gravity, world=None):
+        g = torch.as_tensor(gravity, dtype=torch.float32, device=self.device).reshape(-1, 3)
+        if world is None:
+            self.gravity[:] = g
+        else:
+            self.gravity[world] = g[0]
+
+    def state(self, requires_grad=None) -> State:
+        s = State()
+        s.particle_q = self.particle_q.clone()
+        s.particle_qd = self.particle_qd.clone()
+        s.particle_f = torch.zeros_like(self.particle_q)
+        return s
+
+    def control(self, requires_grad=None, clone_variables=True) -> Control:
+        return Control()
+
+    def contacts(self, soft_contact_max=None) -> Contacts:
+        return Contacts(self.particle_count * max(self.shape_count, 1) if soft_contact_max is None else soft_contact_max,
+                        self.device)
+
+    def collide(self, state: State, contacts: Contacts | None = None, soft_contact_margin=None):
+        contacts = contacts or self.contacts()
+        margin = self.soft_contact_margin if soft_contact_margin is None else soft_contact_margin
+        soft_contacts(self, state, contacts, margin)
+        return contacts
+
+
+class State:
+    """``newton/_src/sim/state.py:47`` (particle part)."""
+
+    def __init__(self):
+        self.particle_q = None
+        self.particle_qd = None
+        self.particle_f = None
+        self.body_q = None
+        self.body_qd = None
+        self.body_f = None
+
+    @property
+    def particle_count(self):
+        return 0 if self.particle_q is None else self.particle_q.shape[0]
+
+    def clear_forces(self):
+        if self.particle_f is not None:
+            self.particle_f.zero_()
+
+    def assign(self, other: State):
+        for k in ("particle_q", "particle_qd", "particle_f"):
+            a, b = getattr(self, k), getattr(other, k)
+            if a is not None and b is not None:
+                a.copy_(b)
+
+
+class Control:
+    pass
+
+
+class Contacts:
+    """Particle-shape soft contacts (``newton/_src/sim/contacts.py:268-295``)."""
+
+    def __init__(self, soft_contact_max: int, device):
+        n = int(soft_contact_max)
+        dev = torch.device(device)
+        self.soft_contact_max = n
+        self.soft_contact_count = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.soft_contact_particle = torch.full((n,), -1, dtype=torch.int32, device=dev)
+        self.soft_contact_shape = torch.full((n,), -1, dtype=torch.int32, device=dev)
+        self.soft_contact_body_pos = torch.zeros((n, 3), dtype=torch.float32, device=dev)
+        self.soft_contact_body_vel = torch.zeros((n, 3), dtype=torch.float32, device=dev)
+        self.soft_contact_normal = torch.zeros((n, 3), dtype=torch.float32, device=dev)
+
+    def clear(self):
+        self.soft_contact_count.zero_()
+
+
+def soft_contacts(model: Model, state: State, contacts: Contacts, margin: float):
+    """Particle vs static ground plane / sphere contacts on the GPU (``vbd_soft_contacts``)."""
+    lib = _lib.load()
+    S = model.shape_count
+    if S == 0:
+        contacts.soft_contact_count.zero_()
+        return
+    st = np.ascontiguousarray(model.shape_type, dtype=np.int32)
+    sp = np.ascontiguousarray(model.shape_pos, dtype=np.float32)
+    sr = np.ascontiguousarray(model.shape_radius, dtype=np.float32)
+    sn = np.ascontiguousarray(model.shape_normal, dtype=np.float32)
+    ip, fp = C.POINTER(C.c_int32), C.POINTER(C.c_float)
+    stream = torch.cuda.current_stream(model.device).cuda_stream
+    rc = lib.vbd_soft_contacts(
+        model.particle_count, state.particle_q.data_ptr(), model.particle_radius.data_ptr(),
+        model.particle_flags.data_ptr(), S, st.ctypes.data_as(ip), sp.ctypes.data_as(fp), sr.ctypes.data_as(fp),
+        sn.ctypes.data_as(fp), float(margin), contacts.soft_contact_max, contacts.soft_contact_count.data_ptr(),
+        contacts.soft_contact_particle.data_ptr(), contacts.soft_contact_shape.data_ptr(),
+        contacts.soft_contact_body_pos.data_ptr(), contacts.soft_contact_body_vel.data_ptr(),
+        contacts.soft_contact_normal.data_ptr(), C.c_void_p(stream),
+    )  # fmt: skip
+    _lib.check(rc, "vbd_soft_contacts")
+
+
+class CollisionPipeline:
+    """Particle-shape part of ``newton/_src/sim/collide.py:485`` (static planes and spheres)."""
+
+    def __init__(self, model: Model, soft_contact_max=None, soft_contact_margin=0.01, **_ignored):
+        self.model = model
+        self.soft_contact_margin = soft_contact_margin
+        self.soft_contact_max = (model.particle_count * max(model.shape_count, 1) if soft_contact_max is None
+                                 else soft_contact_max)  # fmt: skip
+
+    def contacts(self) -> Contacts:
+        return Contacts(self.soft_contact_max, self.model.device)
+
+    def collide(self, state: State, contacts: Contacts):
+        soft_contacts(self.model, state, contacts, self.soft_contact_margin)

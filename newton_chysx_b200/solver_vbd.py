@@ -1,0 +1,274 @@
+"""``SolverVBD``: drop-in for the particle (cloth) path of ``newton.solvers.SolverVBD``.
+
+Same constructor keywords (``newton/_src/solvers/vbd/solver_vbd.py:196-242``) and the same
+``step(state_in, state_out, control, contacts, dt)`` (``:1575-1622``) with the reference's side
+effects: ``state_in.particle_q`` receives the solution, ``state_out.particle_q`` the same positions and
+``state_out.particle_qd = (q - q_prev) / dt``. The work runs in ``libvbd_b200.so`` (hand-written
+sm_100a kernels) on the current torch CUDA stream, so a substep loop can be captured in a CUDA graph.
+
+Beyond the reference keywords:
+
+* ``precision``: ``"fp32"`` (the reference's arithmetic), ``"mixed"`` (FP64 3x3 solve for
+  ill-conditioned blocks and FP64 residual sums, see ``residuals()``), ``"fp64"`` (all FP64; the
+  state arrays must be float64).
+* ``schedule``: ``"per_color"`` (one launch per color and iteration), ``"persistent"`` (one launch
+  per substep, a CTA per cloth instance/world), ``"auto"``.
+* ``lanes_per_vertex`` / ``block_size``: launch shape (0 = default; see ``autotune``).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from .sim import Contacts, Model, State
+
+
+def _ptr(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+class SolverVBD:
+    def __init__(
+        self,
+        model: Model,
+        iterations: int = 10,
+        friction_epsilon: float = 1e-2,
+        integrate_with_external_rigid_solver: bool = False,
+        particle_enable_self_contact: bool = False,
+        particle_self_contact_radius: float = 0.2,
+        particle_self_contact_margin: float = 0.2,
+        particle_conservative_bound_relaxation: float = 0.85,
+        particle_vertex_contact_buffer_size: int = 32,
+        particle_edge_contact_buffer_size: int = 64,
+        particle_collision_detection_interval: int = 0,
+        particle_edge_parallel_epsilon: float = 1e-5,
+        particle_enable_tile_solve: bool = True,
+        particle_topological_contact_filter_threshold: int = 2,
+        particle_rest_shape_contact_exclusion_radius: float = 0.0,
+        particle_external_vertex_contact_filtering_map: dict | None = None,
+        particle_external_edge_contact_filtering_map: dict | None = None,
+        rigid_avbd_alpha: float = 0.95,
+        rigid_avbd_joint_alpha: float | None = None,
+        rigid_avbd_contact_alpha: float | None = None,
+        rigid_avbd_beta: float = 0.0,
+        rigid_avbd_linear_beta: float | None = None,
+        rigid_avbd_angular_beta: float | None = None,
+        rigid_avbd_gamma: float = 0.999,
+        rigid_contact_hard: bool = True,
+        rigid_contact_history: bool = False,
+        rigid_contact_stick_motion_eps: float = 1.0e-4,
+        rigid_contact_stick_freeze_translation_eps: float = 1.0e-4,
+        rigid_contact_stick_freeze_angular_eps: float = 1.0e-4,
+        rigid_contact_k_start: float = 1.0e2,
+        rigid_body_contact_buffer_size: int = 64,
+        rigid_body_particle_contact_buffer_size: int = 256,
+        rigid_joint_linear_ke: float = 1.0e5,
+        rigid_joint_angular_ke: float = 1.0e5,
+        rigid_joint_linear_k_start: float = 1.0e2,
+        rigid_joint_angular_k_start: float = 1.0e1,
+        rigid_joint_linear_kd: float = 0.0,
+        rigid_joint_angular_kd: float = 0.0,
+        rigid_enable_dahl_friction: bool | None = None,
+        *,
+        precision: str = "fp32",
+        schedule: str = "auto",
+        lanes_per_vertex: int = 0,
+        block_size: int = 0,
+        fp64_solve_threshold: float = 1e-3,
+        contact_slots: int = 0,
+    ):
+        if rigid_avbd_beta < 0:
+            raise ValueError(f"rigid_avbd_beta must be >= 0, got {rigid_avbd_beta}")
+        linear_beta = rigid_avbd_linear_beta if rigid_avbd_linear_beta is not None else rigid_avbd_beta
+        self.model = model
+        self.iterations = iterations
+        self.friction_epsilon = friction_epsilon
+        self.integrate_with_external_rigid_solver = integrate_with_external_rigid_solver
+        self.particle_enable_self_contact = particle_enable_self_contact
+        if particle_enable_self_contact:
+            if particle_self_contact_margin < particle_self_contact_radius:
+                raise ValueError(
+                    "particle_self_contact_margin is smaller than particle_self_contact_radius, this will result in "
+                    "missing contacts and cause instability."
+                )
+            raise NotImplementedError("particle self-contact is not available in this build")
+        if model.body_count > 0 and not integrate_with_external_rigid_solver:
+            raise NotImplementedError("rigid bodies (AVBD) are not part of this solver")
+        if model.particle_count == 0:
+            raise ValueError("model has no particles")
+        if len(model.particle_color_groups) == 0:
+            raise ValueError(
+                "model.particle_color_groups is empty! When using the SolverVBD you must call ModelBuilder.color() "
+                "or ModelBuilder.set_coloring() before calling ModelBuilder.finalize()."
+            )
+        if precision not in _lib.PRECISION:
+            raise ValueError(f"precision must be one of {list(_lib.PRECISION)}")
+        if schedule not in _lib.SCHEDULE:
+            raise ValueError(f"schedule must be one of {list(_lib.SCHEDULE)}")
+        if model.device is None or model.device.type != "cuda":
+            raise RuntimeError("SolverVBD needs a CUDA model (finalize(device='cuda'))")
+        self.precision = precision
+        self.device = model.device
+        self._lib = _lib.load()
+
+        groups = [g.to(torch.int32) for g in model.particle_color_groups]
+        self._color_offsets = np.concatenate([[0], np.cumsum([int(g.numel()) for g in groups])]).astype(np.int32)
+        self._color_particles = torch.cat(groups).contiguous()
+        if self._color_offsets[-1] != model.particle_count:
+            raise ValueError("particle_color_groups must cover every particle exactly once")
+        self._world_start = None
+        if getattr(model, "world_particle_start", None) is not None and model.world_count > 1:
+            self._world_start = np.ascontiguousarray(model.world_particle_start, dtype=np.int32)
+
+        md = _lib.VbdModelDesc()
+        md.particle_count = model.particle_count
+        md.tri_count = model.tri_count
+        md.edge_count = model.edge_count
+        md.shape_count = model.shape_count
+        md.particle_mass_dev = _ptr(model.particle_mass)
+        md.particle_inv_mass_dev = _ptr(model.particle_inv_mass)
+        md.particle_flags_dev = _ptr(model.particle_flags)
+        md.particle_radius_dev = _ptr(model.particle_radius)
+        md.tri_indices_dev = _ptr(model.tri_indices) if model.tri_count else None
+        md.tri_poses_dev = _ptr(model.tri_poses) if model.tri_count else None
+        md.tri_materials_dev = _ptr(model.tri_materials) if model.tri_count else None
+        md.tri_areas_dev = _ptr(model.tri_areas) if model.tri_count else None
+        md.edge_indices_dev = _ptr(model.edge_indices) if model.edge_count else None
+        md.edge_rest_angle_dev = _ptr(model.edge_rest_angle) if model.edge_count else None
+        md.edge_rest_length_dev = _ptr(model.edge_rest_length) if model.edge_count else None
+        md.edge_bending_properties_dev = _ptr(model.edge_bending_properties) if model.edge_count else None
+        md.color_count = len(groups)
+        md.color_offsets_host = self._color_offsets.ctypes.data_as(C.POINTER(C.c_int32))
+        md.color_particles_dev = _ptr(self._color_particles)
+        md.world_count = 0 if self._world_start is None else len(self._world_start) - 1
+        md.world_particle_start_host = (
+            None if self._world_start is None else self._world_start.ctypes.data_as(C.POINTER(C.c_int32))
+        )
+        md.gravity_dev = _ptr(model.gravity)
+        md.soft_contact_ke = float(model.soft_contact_ke)
+        md.soft_contact_kd = float(model.soft_contact_kd)
+        md.soft_contact_mu = float(model.soft_contact_mu)
+        if model.shape_count:
+            md.shape_material_ke_dev = _ptr(model.shape_material_ke)
+            md.shape_material_kd_dev = _ptr(model.shape_material_kd)
+            md.shape_material_mu_dev = _ptr(model.shape_material_mu)
+            md.shape_body_dev = _ptr(model.shape_body)
+        md.body_com_dev = _ptr(getattr(model, "body_com", None))
+        self._md = md
+
+        prm = _lib.VbdSolverParams()
+        prm.iterations = int(iterations)
+        prm.friction_epsilon = float(friction_epsilon)
+        prm.avbd_linear_beta = float(linear_beta)
+        prm.contact_k_start = float(rigid_contact_k_start)
+        prm.precision = _lib.PRECISION[precision]
+        prm.fp64_solve_threshold = float(fp64_solve_threshold)
+        prm.schedule = _lib.SCHEDULE[schedule]
+        prm.lanes_per_vertex = int(lanes_per_vertex)
+        prm.block_size = int(block_size)
+        prm.contact_slots = int(contact_slots)
+        self._prm = prm
+
+        h = C.c_void_p()
+        with torch.cuda.device(self.device):
+            rc = self._lib.vbd_create(C.byref(md), C.byref(prm), C.byref(h))
+        if rc == _lib.VBD_ERR_EMPTY_COLORING:
+            raise ValueError("model.particle_color_groups is empty")
+        _lib.check(rc, "vbd_create")
+        self._h = h
+        s, lanes, blk = C.c_int32(), C.c_int32(), C.c_int32()
+        self._lib.vbd_get_config(h, C.byref(s), C.byref(lanes), C.byref(blk))
+        self.schedule = _lib.SCHEDULE_NAME[s.value]
+        self.lanes_per_vertex = lanes.value
+        self.block_size = blk.value
+        n = C.c_int32()
+        self._lib.vbd_launches_per_step(h, C.byref(n))
+        self.launches_per_step = n.value
+
+    # ------------------------------------------------------------------ reference API
+    def step(self, state_in: State, state_out: State, control, contacts: Contacts | None, dt: float) -> None:
+        q_in, q_out, qd_in, qd_out = state_in.particle_q, state_out.particle_q, state_in.particle_qd, state_out.particle_qd
+        f = state_in.particle_f
+        want = torch.float64 if self.precision == "fp64" else torch.float32
+        for name, t in (("state_in.particle_q", q_in), ("state_out.particle_q", q_out), ("state_in.particle_qd", qd_in),
+                        ("state_out.particle_qd", qd_out)):  # fmt: skip
+            if t is None or t.dtype != want or not t.is_cuda or not t.is_contiguous():
+                raise TypeError(f"{name} must be a contiguous {want} CUDA tensor")
+            if t.numel() != 3 * self.model.particle_count:
+                raise ValueError(f"{name} must hold particle_count x 3 values")
+        if f is not None and (f.dtype != want or not f.is_contiguous() or f.numel() != 3 * self.model.particle_count):
+            raise TypeError(f"state_in.particle_f must be a contiguous {want} tensor of particle_count x 3")
+        cdesc = None
+        if contacts is not None and contacts.soft_contact_max > 0 and self.model.shape_count > 0:
+            for t in (contacts.soft_contact_particle, contacts.soft_contact_shape):
+                if t.dtype != torch.int32 or t.numel() < contacts.soft_contact_max or not t.is_contiguous():
+                    raise TypeError("contact index arrays must be contiguous int32 of soft_contact_max entries")
+            for t in (contacts.soft_contact_body_pos, contacts.soft_contact_body_vel, contacts.soft_contact_normal):
+                if t.dtype != torch.float32 or t.numel() < 3 * contacts.soft_contact_max or not t.is_contiguous():
+                    raise TypeError("contact vec3 arrays must be contiguous float32 of soft_contact_max x 3")
+            cdesc = _lib.VbdContactsDesc()
+            cdesc.soft_contact_count_dev = _ptr(contacts.soft_contact_count)
+            cdesc.soft_contact_max = int(contacts.soft_contact_max)
+            cdesc.soft_contact_particle_dev = _ptr(contacts.soft_contact_particle)
+            cdesc.soft_contact_shape_dev = _ptr(contacts.soft_contact_shape)
+            cdesc.soft_contact_body_pos_dev = _ptr(contacts.soft_contact_body_pos)
+            cdesc.soft_contact_body_vel_dev = _ptr(contacts.soft_contact_body_vel)
+            cdesc.soft_contact_normal_dev = _ptr(contacts.soft_contact_normal)
+        bodies = None
+        if getattr(state_in, "body_q", None) is not None:
+            bodies = _lib.VbdBodyState()
+            if self.integrate_with_external_rigid_solver:
+                bodies.body_q_dev = _ptr(state_out.body_q)
+                bodies.body_q_prev_dev = _ptr(state_in.body_q)
+                bodies.body_qd_dev = _ptr(state_out.body_qd)
+            else:
+                bodies.body_q_dev = _ptr(state_in.body_q)
+                bodies.body_qd_dev = _ptr(state_in.body_qd)
+        stream = C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        fn = self._lib.vbd_step_f64 if self.precision == "fp64" else self._lib.vbd_step
+        rc = fn(
+            self._h, _ptr(q_in), _ptr(q_out), _ptr(qd_in), _ptr(qd_out), _ptr(f),
+            None if cdesc is None else C.byref(cdesc), None if bodies is None else C.byref(bodies), float(dt), stream,
+        )  # fmt: skip
+        if rc == _lib.VBD_ERR_UNSUPPORTED:
+            raise RuntimeError("contact buffers must grow while a CUDA graph is being captured; step once before capturing")
+        _lib.check(rc, "vbd_step")
+
+    def notify_model_changed(self, flags: int = 0) -> None:
+        stream = C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        _lib.check(self._lib.vbd_refresh_model(self._h, stream), "vbd_refresh_model")
+
+    def rebuild_bvh(self, state: State) -> None:
+        """Self-contact BVH rebuild; a no-op while self-contact is off (as in the reference)."""
+
+    @staticmethod
+    def register_custom_attributes(builder) -> None:
+        """The reference registers rigid-body Dahl-friction attributes here; cloth needs none."""
+
+    # ------------------------------------------------------------------ diagnostics
+    def device_errors(self) -> int:
+        bits = C.c_int32()
+        stream = C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        _lib.check(self._lib.vbd_get_error(self._h, C.byref(bits), stream), "vbd_get_error")
+        return bits.value
+
+    def residuals(self) -> np.ndarray:
+        """FP64 per-iteration sums of |f|^2 of the last step (precision='mixed')."""
+        out = np.zeros(max(self.iterations, 1), dtype=np.float64)
+        stream = C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        _lib.check(self._lib.vbd_get_residuals(self._h, out.ctypes.data_as(C.POINTER(C.c_double)), self.iterations,
+                                               stream), "vbd_get_residuals")  # fmt: skip
+        return out
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                self._lib.vbd_destroy(h)
+            except Exception:
+                pass
+            self._h = None

@@ -1,0 +1,125 @@
+"""Shared test helpers: models from golden arrays, scene builders and oracle adapters."""
+
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import torch
+
+from newton_chysx_b200 import sim
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load_golden(name):
+    return dict(np.load(os.path.join(GOLDEN, name)))
+
+
+def model_from_golden(g, device="cuda") -> sim.Model:
+    """A Model with the golden fixture's arrays (float32), colors and contact materials."""
+    m = sim.Model()
+    dev = torch.device(device)
+    m.device = dev
+
+    def t(a, dt):
+        return torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=dev)
+
+    f32, i32 = torch.float32, torch.int32
+    n = len(g["model_particle_mass"])
+    m.particle_count = n
+    m.tri_count = len(g["model_tri_indices"])
+    m.edge_count = len(g["model_edge_indices"])
+    m.particle_q = t(g["model_particle_q"], f32)
+    m.particle_qd = t(g["model_particle_qd"], f32)
+    m.particle_mass = t(g["model_particle_mass"], f32)
+    m.particle_inv_mass = t(g["model_particle_inv_mass"], f32)
+    m.particle_radius = t(g["model_particle_radius"], f32)
+    m.particle_flags = t(g["model_particle_flags"], i32)
+    m.tri_indices = t(g["model_tri_indices"], i32)
+    m.tri_poses = t(g["model_tri_poses"], f32)
+    m.tri_materials = t(g["model_tri_materials"], f32)
+    m.tri_areas = t(g["model_tri_areas"], f32)
+    m.edge_indices = t(g["model_edge_indices"], i32)
+    m.edge_rest_angle = t(g["model_edge_rest_angle"], f32)
+    m.edge_rest_length = t(g["model_edge_rest_length"], f32)
+    m.edge_bending_properties = t(g["model_edge_bending_properties"], f32)
+    co, cp = g["color_offsets"], g["color_particles"]
+    m.particle_color_groups = [t(cp[co[c]:co[c + 1]], i32) for c in range(len(co) - 1)]
+    m.particle_colors = t(g["particle_colors"], i32)
+    m.gravity = t(np.asarray(g["gravity"]).reshape(1, 3), f32)
+    soft = g["soft"]
+    m.soft_contact_ke, m.soft_contact_kd, m.soft_contact_mu = float(soft[0]), float(soft[1]), float(soft[2])
+    shapes = np.asarray(g["shapes"]).reshape(-1, 3)
+    S = len(shapes)
+    m.shape_count = S
+    m.shape_material_ke = t(shapes[:, 0], f32)
+    m.shape_material_kd = t(shapes[:, 1], f32)
+    m.shape_material_mu = t(shapes[:, 2], f32)
+    m.shape_body = t(-np.ones(S), i32)
+    m.world_particle_start = None
+    return m
+
+
+def contacts_from_golden(g, s, device="cuda") -> sim.Contacts:
+    cp = g[f"s{s}_contact_particle"]
+    c = sim.Contacts(len(cp), device)
+    c.soft_contact_count.fill_(int(g[f"s{s}_contact_count"]))
+    c.soft_contact_particle.copy_(torch.as_tensor(cp, dtype=torch.int32))
+    c.soft_contact_shape.copy_(torch.as_tensor(g[f"s{s}_contact_shape"], dtype=torch.int32))
+    c.soft_contact_body_pos.copy_(torch.as_tensor(g[f"s{s}_contact_body_pos"], dtype=torch.float32))
+    c.soft_contact_body_vel.copy_(torch.as_tensor(g[f"s{s}_contact_body_vel"], dtype=torch.float32))
+    c.soft_contact_normal.copy_(torch.as_tensor(g[f"s{s}_contact_normal"], dtype=torch.float32))
+    return c
+
+
+def oracle_model_dict(model: sim.Model, friction_epsilon=1e-2, beta=0.0) -> dict:
+    """Arrays of a product Model in the oracle's dict form (float32 values widened to float64)."""
+    from oracle import vbd_oracle as orc
+
+    def h(x):
+        return x.detach().cpu().numpy()
+
+    n = model.particle_count
+    fo, fa, eo, ea = orc.build_adjacency(n, h(model.tri_indices), h(model.edge_indices))
+    groups = [h(g) for g in model.particle_color_groups]
+    colors = np.zeros(n, dtype=np.int32)
+    for c, g in enumerate(groups):
+        colors[g] = c
+    S = model.shape_count
+    shapes = np.zeros((max(S, 1), 3))
+    if S:
+        shapes = np.stack([h(model.shape_material_ke), h(model.shape_material_kd), h(model.shape_material_mu)], 1)
+    return dict(
+        particle_mass=h(model.particle_mass), particle_inv_mass=h(model.particle_inv_mass),
+        particle_radius=h(model.particle_radius), particle_flags=h(model.particle_flags),
+        tri_indices=h(model.tri_indices), tri_poses=h(model.tri_poses), tri_materials=h(model.tri_materials),
+        tri_areas=h(model.tri_areas), edge_indices=h(model.edge_indices), edge_rest_angle=h(model.edge_rest_angle),
+        edge_rest_length=h(model.edge_rest_length), edge_bending_properties=h(model.edge_bending_properties),
+        adj_face_offsets=fo, adj_faces=fa, adj_edge_offsets=eo, adj_edges=ea, particle_colors=colors,
+        color_offsets=np.concatenate([[0], np.cumsum([len(g) for g in groups])]).astype(np.int32),
+        color_particles=np.concatenate(groups).astype(np.int32), gravity=h(model.gravity)[0],
+        soft=np.array([model.soft_contact_ke, model.soft_contact_kd, model.soft_contact_mu]), shapes=shapes,
+        friction_epsilon=friction_epsilon, beta=beta,
+    )  # fmt: skip
+
+
+def cloth_grid_builder(n=32, side=1.0, E=1e4, nu=0.3, h=1e-3, density=0.2, bend=1e-4, radius=5e-3, hanging=True,
+                       height=0.05, pin_top_corners=True, up_axis="Z"):  # fmt: skip
+    """The plain-VBD scene: an n x n vertex sheet of `side` metres, StVK-like Lame from (E, nu, h)."""
+    mu = E * h / (2.0 * (1.0 + nu))
+    lam = E * h * nu / (1.0 - nu * nu)
+    b = sim.ModelBuilder(up_axis=up_axis, gravity=-9.81)
+    cell = side / (n - 1)
+    mass = density * side * side / (n * n)
+    rot = sim.quat_from_axis_angle((1.0, 0.0, 0.0), np.pi * 0.5) if hanging else sim.quat_identity()
+    b.add_cloth_grid(pos=(0.0, 0.0, height), rot=rot, vel=(0.0, 0.0, 0.0), dim_x=n - 1, dim_y=n - 1, cell_x=cell,
+                     cell_y=cell, mass=mass, tri_ke=mu, tri_ka=lam, tri_kd=0.0, edge_ke=bend, edge_kd=0.0,
+                     particle_radius=radius)  # fmt: skip
+    if pin_top_corners:
+        flags = b.particle_flags
+        flags[n * (n - 1)] &= ~int(sim.ParticleFlags.ACTIVE)
+        flags[n * n - 1] &= ~int(sim.ParticleFlags.ACTIVE)
+        b.set_particle_flags(flags)
+    b.color(include_bending=True)
+    return b

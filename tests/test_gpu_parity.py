@@ -1,0 +1,90 @@
+"""GPU parity: the CUDA step (through the C ABI) against the reference's own kernel code (golden
+vectors) and against the CPU oracle.
+
+Tolerances (positions in metres; the cloth side is 1 m, so these are relative to it):
+  * FP32 kernels vs float64 reference goldens: 1e-4 after each substep (FP32 rounding plus the
+    float32 rounding of the model arrays).
+  * FP64 kernels vs the FP64 oracle on the same float32 model arrays: 1e-9.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from newton_chysx_b200 import SolverVBD, sim
+from oracle import vbd_oracle as orc
+from tests.helpers import contacts_from_golden, load_golden, model_from_golden, oracle_model_dict
+
+pytestmark = pytest.mark.gpu
+
+FIXTURES = ["step_grid_ground.npz", "step_grid_sphere.npz", "step_complex_rest_angle.npz"]
+LAUNCH = [("per_color", 1), ("per_color", 4), ("persistent", 1), ("persistent", 8), ("persistent", 32)]
+
+
+def _state(arr, dtype=torch.float32):
+    return torch.as_tensor(np.ascontiguousarray(arr), dtype=dtype, device="cuda")
+
+
+def _run_golden_substep(solver, g, s, dtype=torch.float32):
+    st_in, st_out = sim.State(), sim.State()
+    st_in.particle_q = _state(g[f"s{s}_q_in"], dtype)
+    st_in.particle_qd = _state(g[f"s{s}_qd_in"], dtype)
+    st_in.particle_f = _state(g[f"s{s}_f_ext"], dtype)
+    st_out.particle_q = torch.zeros_like(st_in.particle_q)
+    st_out.particle_qd = torch.zeros_like(st_in.particle_qd)
+    contacts = contacts_from_golden(g, s)
+    solver.step(st_in, st_out, None, contacts, float(g["dt"]))
+    torch.cuda.synchronize()
+    return st_in, st_out
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+@pytest.mark.parametrize("schedule,lanes", LAUNCH)
+def test_fp32_step_matches_reference_goldens(name, schedule, lanes):
+    g = load_golden(name)
+    model = model_from_golden(g)
+    solver = SolverVBD(model, iterations=int(g["iterations"]), friction_epsilon=float(g["friction_epsilon"]),
+                       rigid_avbd_beta=float(g["beta"]), schedule=schedule, lanes_per_vertex=lanes)  # fmt: skip
+    assert solver.schedule == schedule and solver.lanes_per_vertex == lanes
+    for s in range(int(g["substeps"])):
+        st_in, st_out = _run_golden_substep(solver, g, s)
+        q_out = st_out.particle_q.cpu().numpy()
+        assert np.abs(q_out - g[f"s{s}_q_out"]).max() <= 1e-4
+        # reference side effect: state_in.particle_q holds the solution too
+        assert np.array_equal(st_in.particle_q.cpu().numpy(), q_out)
+        qd = st_out.particle_qd.cpu().numpy()
+        assert np.abs(qd - g[f"s{s}_qd_out"]).max() <= 1e-4 / float(g["dt"])
+        # particles that are not ACTIVE never move (test_cloth.py:944-948)
+        fixed = (g["model_particle_flags"] & 1) == 0
+        assert np.array_equal(q_out[fixed], g[f"s{s}_q_in"][fixed].astype(np.float32))
+    assert solver.device_errors() & ~4 == 0
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+@pytest.mark.parametrize("schedule", ["per_color", "persistent"])
+def test_fp64_step_matches_fp64_oracle(name, schedule):
+    g = load_golden(name)
+    model = model_from_golden(g)
+    solver = SolverVBD(model, iterations=int(g["iterations"]), friction_epsilon=float(g["friction_epsilon"]),
+                       rigid_avbd_beta=float(g["beta"]), precision="fp64", schedule=schedule)  # fmt: skip
+    om = orc.Model(oracle_model_dict(model, float(g["friction_epsilon"]), float(g["beta"])))
+    for s in range(int(g["substeps"])):
+        st_in, st_out = _run_golden_substep(solver, g, s, torch.float64)
+        c = contacts_from_golden(g, s)
+        oc = orc.make_contacts(int(c.soft_contact_count.item()), c.soft_contact_particle.cpu().numpy(),
+                               c.soft_contact_shape.cpu().numpy(), c.soft_contact_body_pos.cpu().numpy(),
+                               c.soft_contact_body_vel.cpu().numpy(), c.soft_contact_normal.cpu().numpy())  # fmt: skip
+        _, q_o, qd_o = orc.step(om, g[f"s{s}_q_in"], g[f"s{s}_qd_in"], g[f"s{s}_f_ext"], oc, float(g["dt"]),
+                                int(g["iterations"]), precision=64)  # fmt: skip
+        assert np.abs(st_out.particle_q.cpu().numpy() - q_o).max() <= 1e-9
+        assert np.abs(st_out.particle_qd.cpu().numpy() - qd_o).max() <= 1e-9 / float(g["dt"])
+
+
+def test_mixed_precision_matches_and_reports_residuals():
+    g = load_golden("step_grid_ground.npz")
+    model = model_from_golden(g)
+    solver = SolverVBD(model, iterations=int(g["iterations"]), precision="mixed", fp64_solve_threshold=1.0)
+    st_in, st_out = _run_golden_substep(solver, g, 0)
+    assert np.abs(st_out.particle_q.cpu().numpy() - g["s0_q_out"]).max() <= 1e-4
+    res = solver.residuals()
+    assert res.shape == (int(g["iterations"]),) and np.all(res > 0) and np.all(np.isfinite(res))
