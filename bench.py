@@ -407,12 +407,137 @@ def run_reference(args):
     }  # fmt: skip
 
 
+def run_plain(args):
+    """The plain drop-in used per instance: one SolverVBD per cloth, one step call per instance per
+    substep (per-color launches), on a sample of the batch; the rate is per vertex-iteration."""
+    import torch
+
+    import newton_chysx_b200 as nb
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    sides, E, bend, pins = instance_params(args.seed, args.instances)
+    idx = np.arange(min(args.plain_sample, args.instances))
+    items = []
+    for i in idx:
+        b = build_instance(int(sides[i]), float(E[i]), float(bend[i]), pins[i], int(i))
+        b.add_ground_plane()
+        m = b.finalize(dev)
+        m.soft_contact_ke, m.soft_contact_kd, m.soft_contact_mu = 1.0e3, 10.0, 0.5
+        solver = nb.SolverVBD(m, iterations=ITERATIONS, schedule="per_color", lanes_per_vertex=args.lanes or 4)
+        pipe = nb.CollisionPipeline(m, soft_contact_margin=0.01)
+        items.append((m, solver, pipe, pipe.contacts(), [m.state(), m.state()]))
+    V = sum(m.particle_count for m, *_ in items)
+
+    def substep(k):
+        for m, solver, pipe, c, st in items:
+            pipe.collide(st[k % 2], c)
+            solver.step(st[k % 2], st[(k + 1) % 2], None, c, DT)
+
+    for k in range(args.warmup):
+        substep(k)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(args.steps):
+        substep(k)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"workload": "plain per-instance drop-in", "value": V * ITERATIONS * args.steps / (ms * 1e-3), "unit": UNIT,
+            "instances": len(items), "vertices": V, "ms_per_step": ms / args.steps,
+            "launches_per_instance_step": items[0][1].launches_per_step + 1,
+            "note": "sample of the batch's first instances; eager per-instance step calls"}  # fmt: skip
+
+
+def build_precision_model(n=1024, seed=4, sliver_fraction=1e-3):
+    """1024 x 1024 sheet, per-triangle E log-uniform in [1e5, 1e8] Pa, 0.1% of vertex sites moved
+    towards a neighbour so that incident triangles keep ~1e-6 of their nominal rest area."""
+    from newton_chysx_b200 import sim
+
+    rng = np.random.default_rng(seed)
+    nu, h, density = 0.3, 1.0e-3, 0.2
+    cell = 1.0 / (n - 1)
+    xs, ys = np.meshgrid(np.arange(n), np.arange(n))
+    verts = np.stack([xs.ravel() * cell, ys.ravel() * cell, np.zeros(n * n)], axis=1)
+    sites = rng.choice(np.nonzero((xs.ravel() < n - 1) & (xs.ravel() > 0) & (ys.ravel() > 0) & (ys.ravel() < n - 1))[0],
+                       size=int(sliver_fraction * n * n), replace=False)  # fmt: skip
+    verts[sites, 0] += cell * (1.0 - 1.0e-6)  # next to its +x neighbour
+    cx, cy = np.meshgrid(np.arange(1, n), np.arange(1, n))
+    cx, cy = cx.ravel(), cy.ravel()
+    v0, v1, v2, v3 = (cy - 1) * n + cx - 1, (cy - 1) * n + cx, cy * n + cx, cy * n + cx - 1
+    idx = np.stack([v0, v1, v3, v1, v2, v3], axis=1).reshape(-1)
+    T = len(idx) // 3
+    E = 10.0 ** rng.uniform(5.0, 8.0, size=T)
+    b = sim.ModelBuilder(up_axis="Z", gravity=-9.81)
+    rot = sim.quat_from_axis_angle((1.0, 0.0, 0.0), np.pi * 0.5)
+    start = b.add_particles(verts @ sim.quat_to_matrix(rot).astype(np.float32).astype(np.float64).T
+                            + np.array([0.0, 0.0, 0.1]), (0, 0, 0), np.zeros(n * n), radius=5e-3)  # fmt: skip
+    tri = (start + idx).reshape(-1, 3)
+    areas = b.add_triangles(tri[:, 0], tri[:, 1], tri[:, 2], E * h / (2 * (1 + nu)), E * h * nu / (1 - nu * nu), 0.0)
+    assert np.all(areas > 0.0), "a sliver lost its area"
+    hinges = sim.mesh_hinges(b.tri_indices)
+    b.add_edges(hinges[:, 0], hinges[:, 1], hinges[:, 2], hinges[:, 3], edge_ke=1e-4, edge_kd=0.0)
+    mass = np.full(n * n, density / (n * n))
+    flags = b.particle_flags
+    for c in (n * (n - 1), n * n - 1):
+        flags[c] = 0
+        mass[c] = 0.0
+    b.set_particle_mass(mass)
+    b.set_particle_flags(flags)
+    b.color(include_bending=True)
+    return b, sites
+
+
+def run_precision(args):
+    """FP32 and mixed-precision positions against an all-FP64 run of the same kernels."""
+    import torch
+
+    import newton_chysx_b200 as nb
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    b, _ = build_precision_model(args.precision_n)
+    model = b.finalize(dev)
+    iters, frames = 30, args.precision_frames
+    out = {"workload": f"precision stress {args.precision_n}x{args.precision_n}", "frames": frames, "substeps": 10,
+           "iterations": iters, "vertices": model.particle_count, "triangles": model.tri_count}  # fmt: skip
+    final = {}
+    for prec in ("fp64", "fp32", "mixed"):
+        solver = nb.SolverVBD(model, iterations=iters, precision=prec, schedule="per_color", lanes_per_vertex=args.lanes or 1)
+        dtype = torch.float64 if prec == "fp64" else torch.float32
+        s0, s1 = model.state(), model.state()
+        for s_ in (s0, s1):
+            s_.particle_q, s_.particle_qd, s_.particle_f = (t.to(dtype) for t in (s_.particle_q, s_.particle_qd, s_.particle_f))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(frames * 10):
+            solver.step(s0, s1, None, None, DT)
+            s0, s1 = s1, s0
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        final[prec] = s0.particle_q.double().cpu().numpy()
+        out[prec] = {"vertex_iters_per_s": model.particle_count * iters * frames * 10 / (ms * 1e-3),
+                     "ms_per_substep": ms / (frames * 10), "device_errors": solver.device_errors()}  # fmt: skip
+        if prec == "mixed":
+            out[prec]["residual_last_step"] = solver.residuals().tolist()[-1]
+        del solver
+    for prec in ("fp32", "mixed"):
+        d = np.linalg.norm(final[prec] - final["fp64"], axis=1)
+        out[prec]["pos_err_max_m"] = float(d.max())
+        out[prec]["pos_err_rms_m"] = float(np.sqrt((d * d).mean()))
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["batched", "plain", "precision"], default="batched")
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--lanes", type=int, default=0)
@@ -421,10 +546,20 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--plain-sample", type=int, default=256)
+    ap.add_argument("--precision-n", type=int, default=1024)
+    ap.add_argument("--precision-frames", type=int, default=60)
     ap.add_argument("--traffic", type=float, default=None, help="DRAM bytes per launch from an ncu capture")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
-    out = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if args.impl == "reference":
+        out = run_reference(args)
+    elif args.workload == "plain":
+        out = run_plain(args)
+    elif args.workload == "precision":
+        out = run_precision(args)
+    else:
+        out = run_ours(args)
     if out is not None:
         print(json.dumps(out))
 

@@ -90,6 +90,9 @@ typedef struct VbdSolverParams {
   int32_t lanes_per_vertex;     /* 1,2,4,8,16,32; 0 = choose */
   int32_t block_size;           /* threads per CTA; 0 = choose */
   int32_t contact_slots;        /* contacts kept per particle; 0 = max(shape_count, 1) */
+  int32_t positions_in_shared;  /* persistent schedule, FP32/MIXED: keep each instance's positions in
+                                   shared memory during the sweep. 0 = when they fit, 1 = never,
+                                   2 = required (VBD_ERR_UNSUPPORTED if they do not fit) */
 } VbdSolverParams;
 
 typedef struct VbdContactsDesc {
@@ -146,8 +149,10 @@ int vbd_get_residuals(VbdHandle h, double* out_host, int32_t n, void* stream);
 /* Number of kernel launches one vbd_step issues (for accounting). */
 int vbd_launches_per_step(VbdHandle h, int32_t* out);
 
-/* Scheduling actually chosen (VBD_SCHEDULE_*, lanes per vertex, block size). */
-int vbd_get_config(VbdHandle h, int32_t* schedule, int32_t* lanes_per_vertex, int32_t* block_size);
+/* Scheduling actually chosen (VBD_SCHEDULE_*, lanes per vertex, block size, dynamic shared memory
+   per CTA of the persistent kernel; 0 = positions in global memory). Any pointer may be NULL. */
+int vbd_get_config(VbdHandle h, int32_t* schedule, int32_t* lanes_per_vertex, int32_t* block_size,
+                   int32_t* shared_bytes);
 
 int vbd_destroy(VbdHandle h);
 

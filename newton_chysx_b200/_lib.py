@@ -55,7 +55,7 @@ class VbdSolverParams(C.Structure):
         ("iterations", C.c_int32), ("friction_epsilon", C.c_float), ("avbd_linear_beta", C.c_float),
         ("contact_k_start", C.c_float), ("precision", C.c_int32), ("fp64_solve_threshold", C.c_float),
         ("schedule", C.c_int32), ("lanes_per_vertex", C.c_int32), ("block_size", C.c_int32),
-        ("contact_slots", C.c_int32),
+        ("contact_slots", C.c_int32), ("positions_in_shared", C.c_int32),
     ]  # fmt: skip
 
 
@@ -86,7 +86,7 @@ SIGNATURES = {
     "vbd_get_error": ([_vp, _ip, _vp], C.c_int),
     "vbd_get_residuals": ([_vp, _dp, C.c_int32, _vp], C.c_int),
     "vbd_launches_per_step": ([_vp, _ip], C.c_int),
-    "vbd_get_config": ([_vp, _ip, _ip, _ip], C.c_int),
+    "vbd_get_config": ([_vp, _ip, _ip, _ip, _ip], C.c_int),
     "vbd_destroy": ([_vp], C.c_int),
     "vbd_color_particles": (
         [C.c_int32, C.c_int32, _ip, _fp, C.c_int32, _ip, _fp, C.c_int32, C.c_float, _ip],

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <new>
 #include <numeric>
+#include <type_traits>
 #include <vector>
 
 #include "vbd_b200.h"
@@ -112,6 +113,8 @@ struct VbdSolver {
   int L = 1;
   int block = 256;
   int grid_persistent = 0;
+  size_t smem_bytes = 0;  // > 0: persistent kernel keeps instance positions in shared memory
+  int max_inst_v = 0;
   int K = 1;
   // packed model
   int4* tri_idx = nullptr;
@@ -274,27 +277,28 @@ void launch_color_any(int L, const StepCtx<R>& c, const int* verts, int n, int i
   }
 }
 
-template <typename R, int MODE>
+template <typename R, int MODE, bool SMEM>
 const void* persistent_fn(int L) {
   switch (L) {
-    case 1: return (const void*)k_persistent<R, 1, MODE>;
-    case 2: return (const void*)k_persistent<R, 2, MODE>;
-    case 4: return (const void*)k_persistent<R, 4, MODE>;
-    case 8: return (const void*)k_persistent<R, 8, MODE>;
-    case 16: return (const void*)k_persistent<R, 16, MODE>;
-    default: return (const void*)k_persistent<R, 32, MODE>;
+    case 1: return (const void*)k_persistent<R, 1, MODE, SMEM>;
+    case 2: return (const void*)k_persistent<R, 2, MODE, SMEM>;
+    case 4: return (const void*)k_persistent<R, 4, MODE, SMEM>;
+    case 8: return (const void*)k_persistent<R, 8, MODE, SMEM>;
+    case 16: return (const void*)k_persistent<R, 16, MODE, SMEM>;
+    default: return (const void*)k_persistent<R, 32, MODE, SMEM>;
   }
 }
 
-template <typename R, int MODE>
-void launch_persistent(int L, const StepCtx<R>& c, const PersistentPlan& p, int grid, int block, cudaStream_t st) {
+template <typename R, int MODE, bool SMEM>
+void launch_persistent(int L, const StepCtx<R>& c, const PersistentPlan& p, int grid, int block, size_t smem,
+                       cudaStream_t st) {
   switch (L) {
-    case 1: k_persistent<R, 1, MODE><<<grid, block, 0, st>>>(c, p); break;
-    case 2: k_persistent<R, 2, MODE><<<grid, block, 0, st>>>(c, p); break;
-    case 4: k_persistent<R, 4, MODE><<<grid, block, 0, st>>>(c, p); break;
-    case 8: k_persistent<R, 8, MODE><<<grid, block, 0, st>>>(c, p); break;
-    case 16: k_persistent<R, 16, MODE><<<grid, block, 0, st>>>(c, p); break;
-    default: k_persistent<R, 32, MODE><<<grid, block, 0, st>>>(c, p); break;
+    case 1: k_persistent<R, 1, MODE, SMEM><<<grid, block, smem, st>>>(c, p); break;
+    case 2: k_persistent<R, 2, MODE, SMEM><<<grid, block, smem, st>>>(c, p); break;
+    case 4: k_persistent<R, 4, MODE, SMEM><<<grid, block, smem, st>>>(c, p); break;
+    case 8: k_persistent<R, 8, MODE, SMEM><<<grid, block, smem, st>>>(c, p); break;
+    case 16: k_persistent<R, 16, MODE, SMEM><<<grid, block, smem, st>>>(c, p); break;
+    default: k_persistent<R, 32, MODE, SMEM><<<grid, block, smem, st>>>(c, p); break;
   }
 }
 
@@ -361,7 +365,14 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
     }
     PersistentPlan p{h->W, h->inst_order, h->inst_vstart, h->inst_cptr, h->color_ranges, h->color_verts, h->queue,
                      iters};
-    launch_persistent<R, MODE>(h->L, c, p, h->grid_persistent, h->block, st);
+    if constexpr (std::is_same<R, float>::value) {
+      if (h->smem_bytes > 0)
+        launch_persistent<R, MODE, true>(h->L, c, p, h->grid_persistent, h->block, h->smem_bytes, st);
+      else
+        launch_persistent<R, MODE, false>(h->L, c, p, h->grid_persistent, h->block, 0, st);
+    } else {
+      launch_persistent<R, MODE, false>(h->L, c, p, h->grid_persistent, h->block, 0, st);
+    }
   } else {
     k_forward<R><<<(h->V + 255) / 256, 256, 0, st>>>(c);
     if (has_c) k_contact_prepare<R><<<(c.c_max + 255) / 256, 256, 0, st>>>(c);
@@ -377,18 +388,21 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
   return VBD_OK;
 }
 
+const void* persistent_kernel(VbdSolver* h) {
+  const bool sm = h->smem_bytes > 0;
+  if (h->precision == VBD_PRECISION_FP64) return persistent_fn<double, MODE_FP64, false>(h->L);
+  if (h->precision == VBD_PRECISION_MIXED)
+    return sm ? persistent_fn<float, MODE_MIXED, true>(h->L) : persistent_fn<float, MODE_MIXED, false>(h->L);
+  return sm ? persistent_fn<float, MODE_FP32, true>(h->L) : persistent_fn<float, MODE_FP32, false>(h->L);
+}
+
 int occupancy_grid(VbdSolver* h) {
-  const void* fn = nullptr;
-  if (h->precision == VBD_PRECISION_FP64)
-    fn = persistent_fn<double, MODE_FP64>(h->L);
-  else if (h->precision == VBD_PRECISION_MIXED)
-    fn = persistent_fn<float, MODE_MIXED>(h->L);
-  else
-    fn = persistent_fn<float, MODE_FP32>(h->L);
+  const void* fn = persistent_kernel(h);
   int dev = 0, sms = 0, per_sm = 0;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, h->block, 0));
+  if (h->smem_bytes > 0) CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(h->smem_bytes)));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, h->block, h->smem_bytes));
   if (per_sm < 1) return VBD_ERR_INVALID_ARGUMENT;
   h->grid_persistent = std::min(h->W, sms * per_sm);
   return VBD_OK;
@@ -534,7 +548,21 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
   h->schedule = params->schedule;
   if (h->schedule == VBD_SCHEDULE_AUTO) h->schedule = (h->W > 1 || h->V <= 4096) ? VBD_SCHEDULE_PERSISTENT : VBD_SCHEDULE_PER_COLOR;
   h->L = lpv ? lpv : (h->schedule == VBD_SCHEDULE_PERSISTENT && h->W == 1 ? 8 : 1);
-  h->block = params->block_size ? params->block_size : (h->schedule == VBD_SCHEDULE_PERSISTENT ? 256 : 128);
+  for (int w = 0; w < h->W; ++w) h->max_inst_v = std::max(h->max_inst_v, wstart[w + 1] - wstart[w]);
+  if (h->schedule == VBD_SCHEDULE_PERSISTENT && h->precision != VBD_PRECISION_FP64 &&
+      params->positions_in_shared != 1) {
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+      return fail(VBD_ERR_CUDA);
+    const size_t need = size_t(12) * h->max_inst_v;
+    if (need + 64 <= size_t(optin)) h->smem_bytes = need;
+    else if (params->positions_in_shared == 2) return fail(VBD_ERR_UNSUPPORTED);
+  } else if (params->positions_in_shared == 2) {
+    return fail(VBD_ERR_UNSUPPORTED);
+  }
+  h->block = params->block_size ? params->block_size
+                                : (h->schedule == VBD_SCHEDULE_PERSISTENT ? (h->smem_bytes > 96 * 1024 ? 512 : 256) : 128);
   if (h->schedule == VBD_SCHEDULE_PERSISTENT && (rc = occupancy_grid(h))) return fail(rc);
   if (cudaDeviceSynchronize() != cudaSuccess) return fail(VBD_ERR_CUDA);
   *out = h;
@@ -591,11 +619,12 @@ int vbd_launches_per_step(VbdHandle h, int32_t* out) {
   return VBD_OK;
 }
 
-int vbd_get_config(VbdHandle h, int32_t* schedule, int32_t* lanes, int32_t* block) {
+int vbd_get_config(VbdHandle h, int32_t* schedule, int32_t* lanes, int32_t* block, int32_t* shared_bytes) {
   if (!h) return VBD_ERR_INVALID_ARGUMENT;
   if (schedule) *schedule = h->schedule;
   if (lanes) *lanes = h->L;
   if (block) *block = h->block;
+  if (shared_bytes) *shared_bytes = int32_t(h->smem_bytes);
   return VBD_OK;
 }
 

@@ -15,6 +15,8 @@
 // color (apply_truncation_ts with t = 1 and no bound when self-contact is off,
 // particle_vbd_kernels.py:2877-2897). That is q += H^-1 f; this code applies it to q directly.
 #pragma once
+#include <type_traits>
+
 #include "vbd_elements.cuh"
 
 namespace vbd {
@@ -98,10 +100,34 @@ __device__ __forceinline__ vec3<float> qrot(const float* q, vec3<float> v) {
   return v * (2.f * w * w - 1.f) + cross(u, v) * (2.f * w) + u * (2.f * dot(u, v));
 }
 
+// Where the current positions live during the sweep: the solver's global float4/double4 array, or
+// (persistent kernel, FP32) a packed float3 copy of one instance in shared memory.
+template <typename R>
+struct GlobalPos {
+  pos4_t<R>* p;
+  __device__ __forceinline__ vec3<R> ld(int i) const { return ld3<R>(p[i]); }
+  __device__ __forceinline__ void st(int i, vec3<R> v) const { p[i] = pk4(v, R(0)); }
+};
+
+struct SmemPos {
+  float* s;  // 3 floats per particle of the instance
+  int base;  // first particle of the instance
+  __device__ __forceinline__ vec3<float> ld(int i) const {
+    const float* a = s + 3 * (i - base);
+    return {a[0], a[1], a[2]};
+  }
+  __device__ __forceinline__ void st(int i, vec3<float> v) const {
+    float* a = s + 3 * (i - base);
+    a[0] = v.x;
+    a[1] = v.y;
+    a[2] = v.z;
+  }
+};
+
 // ---------------------------------------------------------------------------------------------
 // forward step of one particle: particle_vbd_kernels.py:1782-1807
-template <typename R>
-__device__ __forceinline__ void forward_particle(const StepCtx<R>& c, int i) {
+template <typename R, typename P>
+__device__ __forceinline__ void forward_particle(const StepCtx<R>& c, const P& pos, int i) {
   const vec3<R> q = {c.q_in[3 * i], c.q_in[3 * i + 1], c.q_in[3 * i + 2]};
   const int fl = c.flags[i];
   const float im = c.inv_mass[i];
@@ -110,7 +136,7 @@ __device__ __forceinline__ void forward_particle(const StepCtx<R>& c, int i) {
   c.qprev[i] = pk4(q, R(0));
   if (!(fl & 1) || im == 0.f) {
     c.inertia[i] = pk4(q, msolve);
-    c.pos[i] = pk4(q, R(0));
+    pos.st(i, q);
     return;
   }
   const vec3<R> g = {R(c.gravity[0]), R(c.gravity[1]), R(c.gravity[2])};
@@ -119,13 +145,13 @@ __device__ __forceinline__ void forward_particle(const StepCtx<R>& c, int i) {
   const vec3<R> v = vec3<R>{c.qd_in[3 * i], c.qd_in[3 * i + 1], c.qd_in[3 * i + 2]} + (g + fe * R(im)) * c.dt;
   const vec3<R> d = v * c.dt;
   c.inertia[i] = pk4(q + d, msolve);
-  c.pos[i] = pk4(q + d, R(0));
+  pos.st(i, q + d);
 }
 
 // velocity update and state write-back: particle_vbd_kernels.py:1900-1903, solver_vbd.py:2335-2337
-template <typename R>
-__device__ __forceinline__ void finalize_particle(const StepCtx<R>& c, int i) {
-  const vec3<R> p = ld3<R>(c.pos[i]);
+template <typename R, typename P>
+__device__ __forceinline__ void finalize_particle(const StepCtx<R>& c, const P& pos, int i) {
+  const vec3<R> p = pos.ld(i);
   const vec3<R> qp = ld3<R>(c.qprev[i]);
   const vec3<R> v = (p - qp) * (R(1) / c.dt);
   c.q_in[3 * i] = p.x;
@@ -200,8 +226,9 @@ __device__ __forceinline__ void contacts_add(const StepCtx<R>& c, int v, vec3<R>
 
 // ---------------------------------------------------------------------------------------------
 // One vertex solved by L lanes. All lanes of the warp must call this (it shuffles).
-template <typename R, int L, int MODE>
-__device__ __forceinline__ void solve_group(const StepCtx<R>& c, int v, bool valid, int sub, int iteration) {
+template <typename R, int L, int MODE, typename P>
+__device__ __forceinline__ void solve_group(const StepCtx<R>& c, const P& pos, int v, bool valid, int sub,
+                                            int iteration) {
   vec3<R> f = zero3<R>();
   sym3<R> H = szero<R>();
   R m = R(0);
@@ -219,9 +246,9 @@ __device__ __forceinline__ void solve_group(const StepCtx<R>& c, int v, bool val
         const float4 mat = __ldg(c.tri_mat + t);
         if (mat.x > 0.f || mat.y > 0.f) {
           const int4 ti = __ldg(c.tri_idx + t);
-          const float4 P = __ldg(c.tri_pose + t);
-          const R pose[4] = {R(P.x), R(P.y), R(P.z), R(P.w)};
-          const vec3<R> x0 = ld3<R>(c.pos[ti.x]), x1 = ld3<R>(c.pos[ti.y]), x2 = ld3<R>(c.pos[ti.z]);
+          const float4 dm = __ldg(c.tri_pose + t);
+          const R pose[4] = {R(dm.x), R(dm.y), R(dm.z), R(dm.w)};
+          const vec3<R> x0 = pos.ld(ti.x), x1 = pos.ld(ti.y), x2 = pos.ld(ti.z);
           vec3<R> xp[3];
           if (mat.z > 0.f) {
             xp[0] = ld3<R>(c.qprev[ti.x]);
@@ -237,10 +264,10 @@ __device__ __forceinline__ void solve_group(const StepCtx<R>& c, int v, bool val
         if (pr.z > 0.f) {
           const int4 ei = __ldg(c.edge_idx + e);
           vec3<R> x[4];
-          x[0] = ld3<R>(c.pos[ei.x]);
-          x[1] = ld3<R>(c.pos[ei.y]);
-          x[2] = ld3<R>(c.pos[ei.z]);
-          x[3] = ld3<R>(c.pos[ei.w]);
+          x[0] = pos.ld(ei.x);
+          x[1] = pos.ld(ei.y);
+          x[2] = pos.ld(ei.z);
+          x[3] = pos.ld(ei.w);
           vec3<R> xp[4];
           if (pr.w > 0.f) {
             xp[0] = ld3<R>(c.qprev[ei.x]);
@@ -267,7 +294,7 @@ __device__ __forceinline__ void solve_group(const StepCtx<R>& c, int v, bool val
   const bool leader = active && sub == 0;
   vec3<R> x = zero3<R>();
   if (leader) {
-    x = ld3<R>(c.pos[v]);
+    x = pos.ld(v);
     const vec3<R> in = ld3<R>(c.inertia[v]);
     const R md = m * c.dt2r;
     f = f + md * (in - x);
@@ -285,27 +312,32 @@ __device__ __forceinline__ void solve_group(const StepCtx<R>& c, int v, bool val
   }
   if (!leader) return;
   vec3<R> dlt;
-  bool ok;
+  double det_used;
   if (MODE == MODE_MIXED) {
     const R hmax = vmax(vmax(vmax(vabs(H.xx), vabs(H.yy)), vmax(vabs(H.zz), vabs(H.xy))), vmax(vabs(H.xz), vabs(H.yz)));
     const R d = sdet(H);
     if (vabs(d) < R(c.fp64_thr) * hmax * hmax * hmax) {
+      // ill-conditioned block: determinant and adjugate solve in FP64
       const sym3<double> Hd = {double(H.xx), double(H.yy), double(H.zz), double(H.xy), double(H.xz), double(H.yz)};
       const vec3<double> fd = {double(f.x), double(f.y), double(f.z)};
-      const double dd = sdet(Hd);
-      ok = fabs(dd) > 1e-8;
-      const vec3<double> r = sadj_mul(Hd, fd) * (1.0 / dd);
+      det_used = sdet(Hd);
+      const vec3<double> r = sadj_mul(Hd, fd) * (1.0 / det_used);
       dlt = {R(r.x), R(r.y), R(r.z)};
     } else {
-      ok = vabs(d) > R(1e-8);
+      det_used = double(d);
       dlt = sadj_mul(H, f) * (R(1) / d);
     }
   } else {
     const R d = sdet(H);
-    ok = vabs(d) > R(1e-8);
+    det_used = double(d);
     dlt = sadj_mul(H, f) * (R(1) / d);
   }
-  if (!ok) {
+  // the reference updates only when |det H| > 1e-8 (a NaN determinant fails that test too)
+  if (!isfinite(det_used)) {
+    set_err(c.err, 1);
+    return;
+  }
+  if (!(fabs(det_used) > 1e-8)) {
     set_err(c.err, 4);
     return;
   }
@@ -314,7 +346,7 @@ __device__ __forceinline__ void solve_group(const StepCtx<R>& c, int v, bool val
     set_err(c.err, 1);
     return;
   }
-  c.pos[v] = pk4(xn, R(0));
+  pos.st(v, xn);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -322,7 +354,7 @@ template <typename R>
 __global__ void k_forward(StepCtx<R> c) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= c.V) return;
-  forward_particle(c, i);
+  forward_particle(c, GlobalPos<R>{c.pos}, i);
   if (c.has_contacts) c.slot_cnt[i] = 0;
 }
 
@@ -330,7 +362,7 @@ template <typename R>
 __global__ void k_finalize(StepCtx<R> c) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= c.V) return;
-  finalize_particle(c, i);
+  finalize_particle(c, GlobalPos<R>{c.pos}, i);
 }
 
 // Per-contact setup (init_body_particle_contacts, rigid_vbd_kernels.py:2318-2361) and the
@@ -367,7 +399,7 @@ __global__ void k_color(StepCtx<R> c, const int* __restrict__ verts, int n, int 
   const int grp = gid / L, sub = gid % L;
   const bool valid = grp < n;
   const int v = valid ? __ldg(verts + grp) : 0;
-  solve_group<R, L, MODE>(c, v, valid, sub, iteration);
+  solve_group<R, L, MODE>(c, GlobalPos<R>{c.pos}, v, valid, sub, iteration);
 }
 
 struct PersistentPlan {
@@ -381,8 +413,12 @@ struct PersistentPlan {
   int iterations;
 };
 
-template <typename R, int L, int MODE>
+// One launch per substep. SMEM: the instance's positions stay in shared memory (3 floats per
+// particle) from the forward step to the write-back, so every neighbour gather of the sweep is a
+// shared-memory load; otherwise they live in the solver's global float4 array.
+template <typename R, int L, int MODE, bool SMEM>
 __global__ void k_persistent(StepCtx<R> c, PersistentPlan p) {
+  extern __shared__ float s_pos[];
   __shared__ int s_item;
   for (;;) {
     __syncthreads();
@@ -392,7 +428,14 @@ __global__ void k_persistent(StepCtx<R> c, PersistentPlan p) {
     if (q >= p.W) return;
     const int w = __ldg(p.inst_order + q);
     const int vs = __ldg(p.inst_vstart + w), ve = __ldg(p.inst_vstart + w + 1);
-    for (int i = vs + threadIdx.x; i < ve; i += blockDim.x) forward_particle(c, i);
+    using Pos = typename std::conditional<SMEM, SmemPos, GlobalPos<R>>::type;
+    Pos pos;
+    if constexpr (SMEM) {
+      pos = SmemPos{s_pos, vs};
+    } else {
+      pos = GlobalPos<R>{c.pos};
+    }
+    for (int i = vs + threadIdx.x; i < ve; i += blockDim.x) forward_particle(c, pos, i);
     __syncthreads();
     const int cb = __ldg(p.inst_cptr + w), ce = __ldg(p.inst_cptr + w + 1);
     const int per_round = blockDim.x / L;
@@ -404,12 +447,12 @@ __global__ void k_persistent(StepCtx<R> c, PersistentPlan p) {
           const int g = base + grp_local;
           const bool valid = g < b;
           const int v = valid ? __ldg(p.color_verts + g) : 0;
-          solve_group<R, L, MODE>(c, v, valid, sub, it);
+          solve_group<R, L, MODE>(c, pos, v, valid, sub, it);
         }
         __syncthreads();
       }
     }
-    for (int i = vs + threadIdx.x; i < ve; i += blockDim.x) finalize_particle(c, i);
+    for (int i = vs + threadIdx.x; i < ve; i += blockDim.x) finalize_particle(c, pos, i);
   }
 }
 

@@ -254,7 +254,7 @@ class ModelBuilder:
 
     def _cat(self, lst, shape, dtype):
         if not lst:
-            return np.zeros(shape, dtype=dtype)
+            return np.zeros(tuple(0 if d == -1 else d for d in shape), dtype=dtype)
         return np.concatenate([np.asarray(a, dtype=dtype).reshape(shape) for a in lst])
 
     @property

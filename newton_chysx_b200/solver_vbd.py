@@ -14,6 +14,8 @@ Beyond the reference keywords:
 * ``schedule``: ``"per_color"`` (one launch per color and iteration), ``"persistent"`` (one launch
   per substep, a CTA per cloth instance/world), ``"auto"``.
 * ``lanes_per_vertex`` / ``block_size``: launch shape (0 = default; see ``autotune``).
+* ``positions_in_shared``: ``"auto"`` / ``"off"`` / ``"on"`` — the persistent kernel keeps each
+  instance's positions in shared memory during the sweep (FP32 and mixed precision).
 """
 
 from __future__ import annotations
@@ -80,6 +82,7 @@ class SolverVBD:
         block_size: int = 0,
         fp64_solve_threshold: float = 1e-3,
         contact_slots: int = 0,
+        positions_in_shared: str = "auto",
     ):
         if rigid_avbd_beta < 0:
             raise ValueError(f"rigid_avbd_beta must be >= 0, got {rigid_avbd_beta}")
@@ -171,6 +174,7 @@ class SolverVBD:
         prm.lanes_per_vertex = int(lanes_per_vertex)
         prm.block_size = int(block_size)
         prm.contact_slots = int(contact_slots)
+        prm.positions_in_shared = {"auto": 0, "off": 1, "on": 2}[positions_in_shared]
         self._prm = prm
 
         h = C.c_void_p()
@@ -180,11 +184,12 @@ class SolverVBD:
             raise ValueError("model.particle_color_groups is empty")
         _lib.check(rc, "vbd_create")
         self._h = h
-        s, lanes, blk = C.c_int32(), C.c_int32(), C.c_int32()
-        self._lib.vbd_get_config(h, C.byref(s), C.byref(lanes), C.byref(blk))
+        s, lanes, blk, smem = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        self._lib.vbd_get_config(h, C.byref(s), C.byref(lanes), C.byref(blk), C.byref(smem))
         self.schedule = _lib.SCHEDULE_NAME[s.value]
         self.lanes_per_vertex = lanes.value
         self.block_size = blk.value
+        self.shared_bytes = smem.value
         n = C.c_int32()
         self._lib.vbd_launches_per_step(h, C.byref(n))
         self.launches_per_step = n.value

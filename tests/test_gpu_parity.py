@@ -18,7 +18,9 @@ from tests.helpers import contacts_from_golden, load_golden, model_from_golden, 
 pytestmark = pytest.mark.gpu
 
 FIXTURES = ["step_grid_ground.npz", "step_grid_sphere.npz", "step_complex_rest_angle.npz"]
-LAUNCH = [("per_color", 1), ("per_color", 4), ("persistent", 1), ("persistent", 8), ("persistent", 32)]
+# (schedule, lanes per vertex, positions in shared memory)
+LAUNCH = [("per_color", 1, "auto"), ("per_color", 4, "auto"), ("persistent", 1, "on"), ("persistent", 8, "on"),
+          ("persistent", 32, "on"), ("persistent", 1, "off"), ("persistent", 4, "off")]
 
 
 def _state(arr, dtype=torch.float32):
@@ -39,13 +41,15 @@ def _run_golden_substep(solver, g, s, dtype=torch.float32):
 
 
 @pytest.mark.parametrize("name", FIXTURES)
-@pytest.mark.parametrize("schedule,lanes", LAUNCH)
-def test_fp32_step_matches_reference_goldens(name, schedule, lanes):
+@pytest.mark.parametrize("schedule,lanes,shared", LAUNCH)
+def test_fp32_step_matches_reference_goldens(name, schedule, lanes, shared):
     g = load_golden(name)
     model = model_from_golden(g)
     solver = SolverVBD(model, iterations=int(g["iterations"]), friction_epsilon=float(g["friction_epsilon"]),
-                       rigid_avbd_beta=float(g["beta"]), schedule=schedule, lanes_per_vertex=lanes)  # fmt: skip
+                       rigid_avbd_beta=float(g["beta"]), schedule=schedule, lanes_per_vertex=lanes,
+                       positions_in_shared=shared)  # fmt: skip
     assert solver.schedule == schedule and solver.lanes_per_vertex == lanes
+    assert (solver.shared_bytes > 0) == (schedule == "persistent" and shared == "on")
     for s in range(int(g["substeps"])):
         st_in, st_out = _run_golden_substep(solver, g, s)
         q_out = st_out.particle_q.cpu().numpy()

@@ -161,8 +161,9 @@ def test_schedules_and_lane_counts_agree():
     b.add_ground_plane()
     model = b.finalize("cuda")
     results = []
-    for schedule, lanes in [("per_color", 1), ("per_color", 8), ("persistent", 1), ("persistent", 16)]:
-        solver = SolverVBD(model, iterations=10, schedule=schedule, lanes_per_vertex=lanes)
+    for schedule, lanes, shared in [("per_color", 1, "auto"), ("per_color", 8, "auto"), ("persistent", 1, "on"),
+                                    ("persistent", 16, "on"), ("persistent", 2, "off")]:
+        solver = SolverVBD(model, iterations=10, schedule=schedule, lanes_per_vertex=lanes, positions_in_shared=shared)
         s = _run(model, solver, 3, 10, 1.0 / 600.0, CollisionPipeline(model))
         results.append(s.particle_q.cpu().numpy())
     for r in results[1:]:
@@ -181,8 +182,12 @@ def test_batched_worlds_match_single_instances():
         singles.append(b)
     model = top.finalize("cuda")
     solver = SolverVBD(model, iterations=10, schedule="persistent")
+    assert solver.shared_bytes == 12 * max(n * n for n in sizes)
     s = _run(model, solver, 2, 10, 1.0 / 600.0)
     q = s.particle_q.cpu().numpy()
+    s_g = _run(model, SolverVBD(model, iterations=10, schedule="persistent", positions_in_shared="off"), 2, 10,
+               1.0 / 600.0)  # fmt: skip
+    assert np.abs(s_g.particle_q.cpu().numpy() - q).max() <= 1e-5
     start = 0
     for b in singles:
         m1 = b.finalize("cuda")
