@@ -195,7 +195,8 @@ def run_ours(args):
     model = builder.finalize(dev)
     model.soft_contact_ke, model.soft_contact_kd, model.soft_contact_mu = 1.0e3, 10.0, 0.5
     solver = nb.SolverVBD(model, iterations=ITERATIONS, schedule="persistent", lanes_per_vertex=args.lanes,
-                          block_size=args.block)  # fmt: skip
+                          block_size=args.block, positions_in_shared=args.shared, layout=args.layout,
+                          min_blocks_per_sm=args.occ)  # fmt: skip
     pipe = nb.CollisionPipeline(model, soft_contact_margin=0.01)
     contacts = pipe.contacts()
     setup_s = time.time() - t0
@@ -313,6 +314,9 @@ def run_ours(args):
                 "schedule": solver.schedule,
                 "lanes_per_vertex": solver.lanes_per_vertex,
                 "block_size": solver.block_size,
+                "positions_in_shared_bytes": solver.shared_bytes,
+                "layout": solver.layout,
+                "min_blocks_per_sm": args.occ,
                 "l2": "inputs larger than L2 (~10 GB working set), no flush",
                 "parallelism": f"instance sharding x{world} (no collective)",
                 "timed": "solve only (forward, iterations, velocity); contact generation outside the solve events",
@@ -490,7 +494,13 @@ def build_precision_model(n=1024, seed=4, sliver_fraction=1e-3):
 
 
 def run_precision(args):
-    """FP32 and mixed-precision positions against an all-FP64 run of the same kernels."""
+    """FP32 and mixed precision against all-FP64 runs of the same kernels on the precision stress sheet.
+
+    Three figures per precision: (1) the error of one substep started from the same FP64 state (the
+    arithmetic error of the step), sampled at several frames; (2) the trajectory error after all
+    frames; (3) next to it, the spread of two FP64 trajectories whose initial positions differ by
+    1e-12 m: past a bifurcation of the stiff, unconverged dynamics, any perturbation grows to the
+    same size, so trajectory differences below that spread say nothing about arithmetic."""
     import torch
 
     import newton_chysx_b200 as nb
@@ -502,32 +512,70 @@ def run_precision(args):
     iters, frames = 30, args.precision_frames
     out = {"workload": f"precision stress {args.precision_n}x{args.precision_n}", "frames": frames, "substeps": 10,
            "iterations": iters, "vertices": model.particle_count, "triangles": model.tri_count}  # fmt: skip
-    final = {}
-    for prec in ("fp64", "fp32", "mixed"):
-        solver = nb.SolverVBD(model, iterations=iters, precision=prec, schedule="per_color", lanes_per_vertex=args.lanes or 1)
-        dtype = torch.float64 if prec == "fp64" else torch.float32
+    solvers = {p: nb.SolverVBD(model, iterations=iters, precision=p, schedule="per_color") for p in ("fp64", "fp32", "mixed")}
+
+    def states(dtype):
         s0, s1 = model.state(), model.state()
         for s_ in (s0, s1):
             s_.particle_q, s_.particle_qd, s_.particle_f = (t.to(dtype) for t in (s_.particle_q, s_.particle_qd, s_.particle_f))
+        return s0, s1
+
+    def run(prec, perturb=0.0, sample_frames=()):
+        dtype = torch.float64 if prec == "fp64" else torch.float32
+        s0, s1 = states(dtype)
+        if perturb:
+            g = torch.Generator(device=dev).manual_seed(1)
+            s0.particle_q += perturb * torch.randn(s0.particle_q.shape, generator=g, device=dev, dtype=dtype)
+        samples, traj = {}, []
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(frames * 10):
-            solver.step(s0, s1, None, None, DT)
-            s0, s1 = s1, s0
-        e1.record()
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        final[prec] = s0.particle_q.double().cpu().numpy()
-        out[prec] = {"vertex_iters_per_s": model.particle_count * iters * frames * 10 / (ms * 1e-3),
-                     "ms_per_substep": ms / (frames * 10), "device_errors": solver.device_errors()}  # fmt: skip
-        if prec == "mixed":
-            out[prec]["residual_last_step"] = solver.residuals().tolist()[-1]
-        del solver
+        t_ms = 0.0
+        for f in range(frames):
+            for k in range(10):
+                if f in sample_frames and k == 0:
+                    samples[f] = (s0.particle_q.clone(), s0.particle_qd.clone())
+                e0.record()
+                solvers[prec].step(s0, s1, None, None, DT)
+                e1.record()
+                torch.cuda.synchronize()
+                t_ms += e0.elapsed_time(e1)
+                s0, s1 = s1, s0
+            traj.append(s0.particle_q.double().cpu().numpy())
+        return traj, samples, t_ms
+
+    def err(a, b):
+        d = np.linalg.norm(a - b, axis=1)
+        return {"max_m": float(d.max()), "rms_m": float(np.sqrt((d * d).mean()))}
+
+    sample_frames = sorted({0, frames // 4, frames // 2, frames - 1})
+    ref, samples, t64 = run("fp64", sample_frames=sample_frames)
+    pert, _, _ = run("fp64", perturb=1e-12)
+    out["fp64"] = {"vertex_iters_per_s": model.particle_count * iters * frames * 10 / (t64 * 1e-3),
+                   "device_errors": solvers["fp64"].device_errors()}  # fmt: skip
+    out["fp64_sensitivity_floor"] = {"perturbation_m": 1e-12,
+                                     "per_frame_max_m": [err(a, b)["max_m"] for a, b in zip(ref, pert, strict=True)]}  # fmt: skip
     for prec in ("fp32", "mixed"):
-        d = np.linalg.norm(final[prec] - final["fp64"], axis=1)
-        out[prec]["pos_err_max_m"] = float(d.max())
-        out[prec]["pos_err_rms_m"] = float(np.sqrt((d * d).mean()))
+        traj, _, t = run(prec)
+        o = {"vertex_iters_per_s": model.particle_count * iters * frames * 10 / (t * 1e-3),
+             "trajectory_error_final": err(traj[-1], ref[-1]),
+             "trajectory_error_per_frame_max_m": [err(a, b)["max_m"] for a, b in zip(traj, ref, strict=True)],
+             "device_errors": solvers[prec].device_errors()}  # fmt: skip
+        one = {}
+        for f, (q, qd) in samples.items():
+            s64_in, s64_out = states(torch.float64)
+            s64_in.particle_q.copy_(q)
+            s64_in.particle_qd.copy_(qd)
+            solvers["fp64"].step(s64_in, s64_out, None, None, DT)
+            s_in, s_out = states(torch.float32)
+            s_in.particle_q.copy_(q)
+            s_in.particle_qd.copy_(qd)
+            solvers[prec].step(s_in, s_out, None, None, DT)
+            torch.cuda.synchronize()
+            one[f"frame_{f}"] = err(s_out.particle_q.double().cpu().numpy(), s64_out.particle_q.cpu().numpy())
+        o["one_substep_error"] = one
+        if prec == "mixed":
+            o["residual_last_step"] = solvers[prec].residuals().tolist()
+        out[prec] = o
     return out
 
 
@@ -542,6 +590,9 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--lanes", type=int, default=0)
     ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--shared", choices=["auto", "on", "off"], default="auto")
+    ap.add_argument("--layout", choices=["auto", "ell", "csr"], default="auto")
+    ap.add_argument("--occ", type=int, default=0, help="resident 256-thread CTAs per SM the kernel is compiled for")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

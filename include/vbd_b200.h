@@ -40,6 +40,11 @@ extern "C" {
 #define VBD_SCHEDULE_PER_COLOR 1   /* one grid launch per color per iteration (large single cloth) */
 #define VBD_SCHEDULE_PERSISTENT 2  /* one launch per substep; one CTA owns one instance (world) at a time */
 
+/* Element data layout read by the sweep. */
+#define VBD_LAYOUT_AUTO 0
+#define VBD_LAYOUT_CSR 1  /* vertex -> element adjacency, element records gathered by id (any lanes/vertex) */
+#define VBD_LAYOUT_ELL 2  /* per-incidence stencil records in sweep order, slot-major (one lane/vertex) */
+
 typedef struct VbdModelDesc {
   int32_t particle_count; /* V */
   int32_t tri_count;      /* T */
@@ -93,6 +98,9 @@ typedef struct VbdSolverParams {
   int32_t positions_in_shared;  /* persistent schedule, FP32/MIXED: keep each instance's positions in
                                    shared memory during the sweep. 0 = when they fit, 1 = never,
                                    2 = required (VBD_ERR_UNSUPPORTED if they do not fit) */
+  int32_t layout;               /* VBD_LAYOUT_*; AUTO = ELL when lanes_per_vertex is 1 */
+  int32_t min_blocks_per_sm;    /* ELL + persistent, FP32/MIXED: 2..4 compiles the kernel for that many
+                                   resident CTAs of 256 threads per SM (fewer registers); 0 = none */
 } VbdSolverParams;
 
 typedef struct VbdContactsDesc {
@@ -139,6 +147,25 @@ int vbd_step_f64(VbdHandle h, double* q_in_dev, double* q_out_dev, const double*
                  const double* particle_f_dev, const VbdContactsDesc* contacts, const VbdBodyState* bodies, double dt,
                  void* stream);
 
+/* ---------------------------------------------------------------- differentiation (no reference
+   counterpart: the reference VBD kernels are built with enable_backward=False,
+   particle_vbd_kernels.py:27-28) */
+
+/* The forward substep of vbd_step (per-color sweep, no particle-shape contacts) that also records
+   what its adjoint needs: y [V,3] the inertial targets and checkpoints [(iterations+1),V,3] the
+   positions at the start of every iteration and at the end. Arrays are float32, or float64 for a
+   VBD_PRECISION_FP64 solver. q_out/qd_out receive the step's result (q_in is not modified). */
+int vbd_record_step(VbdHandle h, const void* q_in_dev, const void* qd_in_dev, const void* particle_f_dev, double dt,
+                    void* y_dev, void* checkpoints_dev, void* q_out_dev, void* qd_out_dev, void* stream);
+
+/* Reverse of that substep: from dL/dq_out and dL/dqd_out (either may be NULL = 0), writes dL/dq_in
+   and dL/dqd_in and ADDS the triangles' dL/dmu and dL/dlambda (Model.tri_materials columns 0 and 1)
+   into adj_tri_mu / adj_tri_lambda [T] (either may be NULL). The first call allocates
+   (colors + 2) x V x 3 work values; it returns VBD_ERR_UNSUPPORTED if that happens during a capture. */
+int vbd_adjoint_step(VbdHandle h, const void* q_in_dev, const void* y_dev, const void* checkpoints_dev, double dt,
+                     const void* adj_q_out_dev, const void* adj_qd_out_dev, void* adj_q_in_dev, void* adj_qd_in_dev,
+                     void* adj_tri_mu_dev, void* adj_tri_lambda_dev, void* stream);
+
 /* Reads and clears the device error word (VBD_DEVERR_* bits). Synchronizes `stream`. */
 int vbd_get_error(VbdHandle h, int32_t* bits, void* stream);
 
@@ -150,9 +177,10 @@ int vbd_get_residuals(VbdHandle h, double* out_host, int32_t n, void* stream);
 int vbd_launches_per_step(VbdHandle h, int32_t* out);
 
 /* Scheduling actually chosen (VBD_SCHEDULE_*, lanes per vertex, block size, dynamic shared memory
-   per CTA of the persistent kernel; 0 = positions in global memory). Any pointer may be NULL. */
+   per CTA of the persistent kernel (0 = positions in global memory), VBD_LAYOUT_*). Any pointer may
+   be NULL. */
 int vbd_get_config(VbdHandle h, int32_t* schedule, int32_t* lanes_per_vertex, int32_t* block_size,
-                   int32_t* shared_bytes);
+                   int32_t* shared_bytes, int32_t* layout);
 
 int vbd_destroy(VbdHandle h);
 

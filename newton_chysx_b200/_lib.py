@@ -26,6 +26,8 @@ VBD_DEVERR_SINGULAR_SKIPPED = 4
 PRECISION = {"fp32": 0, "mixed": 1, "fp64": 2}
 SCHEDULE = {"auto": 0, "per_color": 1, "persistent": 2}
 SCHEDULE_NAME = {v: k for k, v in SCHEDULE.items()}
+LAYOUT = {"auto": 0, "csr": 1, "ell": 2}
+LAYOUT_NAME = {v: k for k, v in LAYOUT.items()}
 
 _fp = C.POINTER(C.c_float)
 _dp = C.POINTER(C.c_double)
@@ -55,7 +57,8 @@ class VbdSolverParams(C.Structure):
         ("iterations", C.c_int32), ("friction_epsilon", C.c_float), ("avbd_linear_beta", C.c_float),
         ("contact_k_start", C.c_float), ("precision", C.c_int32), ("fp64_solve_threshold", C.c_float),
         ("schedule", C.c_int32), ("lanes_per_vertex", C.c_int32), ("block_size", C.c_int32),
-        ("contact_slots", C.c_int32), ("positions_in_shared", C.c_int32),
+        ("contact_slots", C.c_int32), ("positions_in_shared", C.c_int32), ("layout", C.c_int32),
+        ("min_blocks_per_sm", C.c_int32),
     ]  # fmt: skip
 
 
@@ -83,10 +86,12 @@ SIGNATURES = {
         [_vp, _vp, _vp, _vp, _vp, _vp, C.POINTER(VbdContactsDesc), C.POINTER(VbdBodyState), C.c_double, _vp],
         C.c_int,
     ),
+    "vbd_record_step": ([_vp, _vp, _vp, _vp, C.c_double, _vp, _vp, _vp, _vp, _vp], C.c_int),
+    "vbd_adjoint_step": ([_vp, _vp, _vp, _vp, C.c_double, _vp, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
     "vbd_get_error": ([_vp, _ip, _vp], C.c_int),
     "vbd_get_residuals": ([_vp, _dp, C.c_int32, _vp], C.c_int),
     "vbd_launches_per_step": ([_vp, _ip], C.c_int),
-    "vbd_get_config": ([_vp, _ip, _ip, _ip, _ip], C.c_int),
+    "vbd_get_config": ([_vp, _ip, _ip, _ip, _ip, _ip], C.c_int),
     "vbd_destroy": ([_vp], C.c_int),
     "vbd_color_particles": (
         [C.c_int32, C.c_int32, _ip, _fp, C.c_int32, _ip, _fp, C.c_int32, C.c_float, _ip],

@@ -1,0 +1,236 @@
+// Hand-written adjoint of the fixed-iteration VBD step (one substep, no particle-shape contacts).
+//
+// Forward map of one substep (vbd_kernels.cuh, CSR path, one lane per vertex):
+//   y   = q + (qd + (g + f_ext / m) dt) dt                    inertial target, also the first iterate
+//   for it < I, for color c, for v in c (Jacobi within the color, positions x of the color's start):
+//       g_v = (m / dt^2)(y_v - x_v) + sum_e f_e,v(x),   H_v = (m / dt^2) I + sum_e H_e,v(x)
+//       x_v <- x_v + H_v^-1 g_v          (skipped when |det H_v| <= 1e-8)
+//   q_out = x,   qd_out = (x - q) / dt
+//
+// Reverse of one color update x' = x + D(x), D_v = H_v^-1 g_v, given the adjoint a = dL/dx':
+//   w = H_v^-1 a_v        (H_v is symmetric)
+//   dL/dg_v = w,   dL/dH_v = -w D_v^T   (only its symmetric part meets the symmetric dH)
+//   dL/dx = a + [dg_v/dx]^T w + [dH_v/dx] : (-w D_v^T),   likewise for y and the element parameters.
+// The element terms f_e,v and H_e,v are differentiated with forward-mode dual numbers over the
+// element's vertex coordinates (and the triangle's mu, lambda), running the same element routines
+// as the forward pass. Vertices of one color are never neighbours, so the vertices written through
+// atomics (the neighbours, the triangle parameters) are never read by the same launch.
+#pragma once
+#include "vbd_dual.cuh"
+#include "vbd_kernels.cuh"
+
+namespace vbd {
+
+template <typename R>
+struct AdjCtx {
+  StepCtx<R> c;           // model arrays (CSR) and dt
+  const R* x;             // [V*3] positions at the start of the color (the forward state)
+  const R* y;             // [V*3] inertial targets
+  R* adj_x;               // [V*3] in: dL/dx', out: dL/dx (in place)
+  R* adj_y;               // [V*3] accumulated dL/dy
+  R* adj_mu;              // [T] accumulated dL/dmu (triangle), may be NULL
+  R* adj_lambda;          // [T] accumulated dL/dlambda, may be NULL
+};
+
+// mass used by the solve (0 for a fixed particle), as forward_particle stores it
+template <typename R>
+__device__ __forceinline__ R solve_mass(const StepCtx<R>& c, int v) {
+  const float m = c.mass[v];
+  return ((c.flags[v] & 1) && m != 0.f) ? R(m) : R(0);
+}
+
+template <typename R>
+__device__ __forceinline__ vec3<R> ldx(const R* a, int i) {
+  return {a[3 * i], a[3 * i + 1], a[3 * i + 2]};
+}
+
+template <typename R>
+__device__ __forceinline__ void atomic_add3(R* a, int i, vec3<R> v) {
+  atomicAdd(a + 3 * i, v.x);
+  atomicAdd(a + 3 * i + 1, v.y);
+  atomicAdd(a + 3 * i + 2, v.z);
+}
+
+// <g_bar, df> + <H_bar, dH> for one derivative slot k (H_bar symmetric, stored as 6 with the
+// off-diagonal entries counted twice)
+template <typename R, int N>
+__device__ __forceinline__ R contract(const vec3<Dual<R, N>>& f, const sym3<Dual<R, N>>& H, vec3<R> gb,
+                                      const sym3<R>& Hb, int k) {
+  return gb.x * f.x.d[k] + gb.y * f.y.d[k] + gb.z * f.z.d[k] + Hb.xx * H.xx.d[k] + Hb.yy * H.yy.d[k] +
+         Hb.zz * H.zz.d[k] + R(2) * (Hb.xy * H.xy.d[k] + Hb.xz * H.xz.d[k] + Hb.yz * H.yz.d[k]);
+}
+
+template <typename R>
+__device__ __forceinline__ void assemble(const StepCtx<R>& c, const R* X, int v, vec3<R>& f, sym3<R>& H) {
+  for (int a = c.face_off[v]; a < c.face_off[v + 1]; ++a) {
+    const int t = c.face_adj[a] >> 2, ord = c.face_adj[a] & 3;
+    const float4 mat = c.tri_mat[t];
+    if (!(mat.x > 0.f || mat.y > 0.f)) continue;
+    const int4 ti = c.tri_idx[t];
+    const float4 dm = c.tri_pose[t];
+    const R pose[4] = {R(dm.x), R(dm.y), R(dm.z), R(dm.w)};
+    membrane_add<R>(ord, ldx(X, ti.x), ldx(X, ti.y), ldx(X, ti.z), pose, R(mat.x), R(mat.y), R(0), R(mat.w), c.dt,
+                    nullptr, f, H);
+  }
+  for (int a = c.edge_off[v]; a < c.edge_off[v + 1]; ++a) {
+    const int e = c.edge_adj[a] >> 2, ord = c.edge_adj[a] & 3;
+    const float4 pr = c.edge_prop[e];
+    if (!(pr.z > 0.f)) continue;
+    const int4 ei = c.edge_idx[e];
+    const vec3<R> xs[4] = {ldx(X, ei.x), ldx(X, ei.y), ldx(X, ei.z), ldx(X, ei.w)};
+    bending_add<R>(ord, xs, R(pr.x), R(pr.y), R(pr.z), R(0), c.dt, nullptr, f, H);
+  }
+}
+
+template <typename R>
+__global__ void k_adjoint_color(AdjCtx<R> A, const int* __restrict__ verts, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const StepCtx<R>& c = A.c;
+  const int v = verts[k];
+  const R m = solve_mass(c, v);
+  if (m == R(0)) return;  // fixed particle: no update, the adjoint passes through unchanged
+  const R md = m * c.dt2r;
+  const vec3<R> x = ldx(A.x, v);
+  // forward quantities at this color's start
+  vec3<R> f = md * (ldx(A.y, v) - x);
+  sym3<R> H = sdiag(md);
+  assemble(c, A.x, v, f, H);
+  const R det = sdet(H);
+  if (!(fabs(double(det)) > 1e-8) || !isfinite(double(det))) return;  // update skipped: D = 0
+  const R idet = R(1) / det;
+  const vec3<R> D = sadj_mul(H, f) * idet;
+  const vec3<R> a = ldx(A.adj_x, v);
+  const vec3<R> w = sadj_mul(H, a) * idet;
+  // H_bar = -sym(w D^T)
+  const sym3<R> Hb = {-w.x * D.x, -w.y * D.y, -w.z * D.z, R(-0.5) * (w.x * D.y + w.y * D.x),
+                      R(-0.5) * (w.x * D.z + w.z * D.x), R(-0.5) * (w.y * D.z + w.z * D.y)};
+  // inertia term: g = md (y - x)
+  vec3<R> ax = a - md * w;
+  atomic_add3(A.adj_y, v, md * w);
+  // membranes: 9 coordinates + (mu, lambda)
+  for (int q = c.face_off[v]; q < c.face_off[v + 1]; ++q) {
+    const int t = c.face_adj[q] >> 2, ord = c.face_adj[q] & 3;
+    const float4 mat = c.tri_mat[t];
+    if (!(mat.x > 0.f || mat.y > 0.f)) continue;
+    const int4 ti = c.tri_idx[t];
+    const int vid[3] = {ti.x, ti.y, ti.z};
+    const float4 dm = c.tri_pose[t];
+    using D11 = Dual<R, 11>;
+    vec3<D11> xs[3];
+    for (int j = 0; j < 3; ++j) {
+      const vec3<R> p = ldx(A.x, vid[j]);
+      xs[j] = {D11::seed(p.x, 3 * j), D11::seed(p.y, 3 * j + 1), D11::seed(p.z, 3 * j + 2)};
+    }
+    const D11 pose[4] = {D11(R(dm.x)), D11(R(dm.y)), D11(R(dm.z)), D11(R(dm.w))};
+    vec3<D11> fd = {D11(R(0)), D11(R(0)), D11(R(0))};
+    sym3<D11> Hd = szero<D11>();
+    membrane_add<D11>(ord, xs[0], xs[1], xs[2], pose, D11::seed(R(mat.x), 9), D11::seed(R(mat.y), 10), D11(R(0)),
+                      D11(R(mat.w)), D11(c.dt), nullptr, fd, Hd);
+    for (int j = 0; j < 3; ++j) {
+      const vec3<R> gj = {contract(fd, Hd, w, Hb, 3 * j), contract(fd, Hd, w, Hb, 3 * j + 1),
+                          contract(fd, Hd, w, Hb, 3 * j + 2)};
+      if (vid[j] == v)
+        ax = ax + gj;
+      else
+        atomic_add3(A.adj_x, vid[j], gj);
+    }
+    if (A.adj_mu) atomicAdd(A.adj_mu + t, contract(fd, Hd, w, Hb, 9));
+    if (A.adj_lambda) atomicAdd(A.adj_lambda + t, contract(fd, Hd, w, Hb, 10));
+  }
+  // bending hinges: 12 coordinates
+  for (int q = c.edge_off[v]; q < c.edge_off[v + 1]; ++q) {
+    const int e = c.edge_adj[q] >> 2, ord = c.edge_adj[q] & 3;
+    const float4 pr = c.edge_prop[e];
+    if (!(pr.z > 0.f)) continue;
+    const int4 ei = c.edge_idx[e];
+    const int vid[4] = {ei.x, ei.y, ei.z, ei.w};
+    using D12 = Dual<R, 12>;
+    vec3<D12> xs[4];
+    for (int j = 0; j < 4; ++j) {
+      const vec3<R> p = ldx(A.x, vid[j]);
+      xs[j] = {D12::seed(p.x, 3 * j), D12::seed(p.y, 3 * j + 1), D12::seed(p.z, 3 * j + 2)};
+    }
+    vec3<D12> fd = {D12(R(0)), D12(R(0)), D12(R(0))};
+    sym3<D12> Hd = szero<D12>();
+    bending_add<D12>(ord, xs, D12(R(pr.x)), D12(R(pr.y)), D12(R(pr.z)), D12(R(0)), D12(c.dt), nullptr, fd, Hd);
+    for (int j = 0; j < 4; ++j) {
+      const vec3<R> gj = {contract(fd, Hd, w, Hb, 3 * j), contract(fd, Hd, w, Hb, 3 * j + 1),
+                          contract(fd, Hd, w, Hb, 3 * j + 2)};
+      if (vid[j] == v)
+        ax = ax + gj;
+      else
+        atomic_add3(A.adj_x, vid[j], gj);
+    }
+  }
+  A.adj_x[3 * v] = ax.x;
+  A.adj_x[3 * v + 1] = ax.y;
+  A.adj_x[3 * v + 2] = ax.z;
+}
+
+// one color of the forward sweep on plain (x, y) arrays: the state the adjoint differentiates
+template <typename R>
+__global__ void k_record_color(StepCtx<R> c, const R* __restrict__ xin, const R* __restrict__ y, R* xout,
+                               const int* __restrict__ verts, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int v = verts[k];
+  const R m = solve_mass(c, v);
+  if (m == R(0)) return;
+  const R md = m * c.dt2r;
+  const vec3<R> x = ldx(xin, v);
+  vec3<R> f = md * (ldx(y, v) - x);
+  sym3<R> H = sdiag(md);
+  assemble(c, xin, v, f, H);
+  const R det = sdet(H);
+  if (!(fabs(double(det)) > 1e-8) || !isfinite(double(det))) return;
+  const vec3<R> xn = x + sadj_mul(H, f) * (R(1) / det);
+  xout[3 * v] = xn.x;
+  xout[3 * v + 1] = xn.y;
+  xout[3 * v + 2] = xn.z;
+}
+
+// y (inertial target) and the mass flag of every particle, as forward_particle computes them
+template <typename R>
+__global__ void k_record_forward(StepCtx<R> c, R* y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= c.V) return;
+  forward_particle(c, GlobalPos<R>{c.pos}, i);
+  const vec3<R> p = ld3<R>(c.inertia[i]);
+  y[3 * i] = p.x;
+  y[3 * i + 1] = p.y;
+  y[3 * i + 2] = p.z;
+}
+
+// dL/dx of the last iterate from dL/dq_out and dL/dqd_out (q_out = x, qd_out = (x - q) / dt)
+template <typename R>
+__global__ void k_adjoint_begin(int n3, const R* aq, const R* aqd, R inv_dt, R* ax, R* ay) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n3) return;
+  ax[i] = (aq ? aq[i] : R(0)) + (aqd ? aqd[i] * inv_dt : R(0));
+  ay[i] = R(0);
+}
+
+// dL/dq_in, dL/dqd_in from dL/dy (the first iterate is y) and the direct qd_out term
+template <typename R>
+__global__ void k_adjoint_end(StepCtx<R> c, const R* ax, const R* ay, const R* aqd, R* aq_in, R* aqd_in) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= c.V) return;
+  const bool moves = (c.flags[i] & 1) && c.inv_mass[i] != 0.f;
+  for (int j = 0; j < 3; ++j) {
+    const R gy = ay[3 * i + j] + ax[3 * i + j];
+    aq_in[3 * i + j] = gy - (aqd ? aqd[3 * i + j] / c.dt : R(0));
+    if (aqd_in) aqd_in[3 * i + j] = moves ? gy * c.dt : R(0);
+  }
+}
+
+// q_out = x, qd_out = (x - q) / dt
+template <typename R>
+__global__ void k_record_finish(StepCtx<R> c, const R* x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 3 * c.V) return;
+  c.q_out[i] = x[i];
+  c.qd_out[i] = (x[i] - c.q_in[i]) / c.dt;
+}
+
+}  // namespace vbd

@@ -13,7 +13,8 @@
 #include <vector>
 
 #include "vbd_b200.h"
-#include "vbd_kernels.cuh"
+#include "vbd_adjoint.cuh"
+#include "vbd_ell.cuh"
 
 using namespace vbd;
 
@@ -115,6 +116,7 @@ struct VbdSolver {
   int grid_persistent = 0;
   size_t smem_bytes = 0;  // > 0: persistent kernel keeps instance positions in shared memory
   int max_inst_v = 0;
+  int occ = 0;  // ELL persistent kernel: compiled occupancy target (CTAs of 256 per SM), 0 = none
   int K = 1;
   // packed model
   int4* tri_idx = nullptr;
@@ -136,17 +138,175 @@ struct VbdSolver {
   int c_cap = 0;
   int* err = nullptr;
   double* residual = nullptr;
+  // stencil (ELL) layout
+  int layout = VBD_LAYOUT_CSR;
+  std::vector<int> ranges_host;     // per range: first index into range_verts_host (+ end)
+  std::vector<int> range_verts_host;  // processing order of the ELL records
+  int *range_nf = nullptr, *range_ne = nullptr;
+  long long *range_fbase = nullptr, *range_ebase = nullptr;
+  int2* face_nb = nullptr;
+  float4* face_dm = nullptr;
+  float2* face_mat = nullptr;
+  float* face_kd = nullptr;
+  int4* hinge_idx = nullptr;
+  float2* hinge_prop = nullptr;
+  float* hinge_kd = nullptr;
+  std::vector<int> ell_nf, ell_ne;
+  std::vector<long long> ell_fbase, ell_ebase;
+  long long ell_faces = 0, ell_hinges = 0;
+  bool ell_face_damping = false, ell_hinge_damping = false;
+  // adjoint work buffers (allocated by the first vbd_adjoint_step)
+  void* adj_work = nullptr;
+  size_t adj_work_bytes = 0;
+  // host copies of the topology (for re-packing the ELL records)
+  std::vector<int> h_tri, h_edges, h_foff, h_fadj, h_eoff, h_eadj;
 
   ~VbdSolver() {
     void* ps[] = {tri_idx, tri_pose, tri_mat, edge_idx, edge_prop, face_off, face_adj, edge_off, edge_adj,
                   inst_order, inst_vstart, inst_cptr, color_ranges, color_verts, queue, pos, qprev, inertia,
-                  slot_cnt, slots, c_k, c_ke, c_kd, c_mu, err, residual};
+                  slot_cnt, slots, c_k, c_ke, c_kd, c_mu, err, residual, range_nf, range_ne, range_fbase,
+                  range_ebase, face_nb, face_dm, face_mat, face_kd, hinge_idx, hinge_prop, hinge_kd, adj_work};
     for (void* p : ps)
       if (p) cudaFree(p);
   }
 };
 
 namespace {
+
+template <typename T>
+void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+template <typename T>
+int upload_into(T** d, const std::vector<T>& h) {
+  dfree(*d);
+  int rc = dalloc(d, h.size());
+  if (rc) return rc;
+  if (!h.empty() && cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+    return VBD_ERR_CUDA;
+  return VBD_OK;
+}
+
+template <typename T>
+int download(std::vector<T>& h, const T* d, size_t n) {
+  h.resize(n);
+  if (n && cudaMemcpy(h.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost) != cudaSuccess) return VBD_ERR_CUDA;
+  return VBD_OK;
+}
+
+// Builds the stencil records (vbd_ell.cuh) for the ranges in h->ranges_host / h->range_verts_host from
+// the caller's model arrays. Runs on the host at creation and on refresh.
+int build_ell(VbdSolver* h) {
+  const VbdModelDesc& m = h->md;
+  std::vector<float> pose, mat, area, ra, rl, bp;
+  int rc;
+  if ((rc = download(pose, m.tri_poses_dev, size_t(4) * h->T)) || (rc = download(mat, m.tri_materials_dev, size_t(5) * h->T)) ||
+      (rc = download(area, m.tri_areas_dev, size_t(h->T))) || (rc = download(ra, m.edge_rest_angle_dev, size_t(h->E))) ||
+      (rc = download(rl, m.edge_rest_length_dev, size_t(h->E))) ||
+      (rc = download(bp, m.edge_bending_properties_dev, size_t(2) * h->E)))
+    return rc;
+  const int R = int(h->ranges_host.size()) - 1;
+  h->ell_nf.assign(R, 0);
+  h->ell_ne.assign(R, 0);
+  h->ell_fbase.assign(R, 0);
+  h->ell_ebase.assign(R, 0);
+  long long nfaces = 0, nhinges = 0;
+  for (int r = 0; r < R; ++r) {
+    int nf = 0, ne = 0;
+    for (int k = h->ranges_host[r]; k < h->ranges_host[r + 1]; ++k) {
+      const int v = h->range_verts_host[k];
+      nf = std::max(nf, h->h_foff[v + 1] - h->h_foff[v]);
+      ne = std::max(ne, h->h_eoff[v + 1] - h->h_eoff[v]);
+    }
+    const long long n = h->ranges_host[r + 1] - h->ranges_host[r];
+    h->ell_nf[r] = nf;
+    h->ell_ne[r] = ne;
+    h->ell_fbase[r] = nfaces;
+    h->ell_ebase[r] = nhinges;
+    nfaces += n * nf;
+    nhinges += n * ne;
+  }
+  h->ell_faces = nfaces;
+  h->ell_hinges = nhinges;
+  bool fdamp = false, hdamp = false;
+  for (int t = 0; t < h->T; ++t) fdamp |= (mat[5 * t] > 0.f || mat[5 * t + 1] > 0.f) && mat[5 * t + 2] > 0.f;
+  for (int e = 0; e < h->E; ++e) hdamp |= bp[2 * e] > 0.f && bp[2 * e + 1] > 0.f;
+  h->ell_face_damping = fdamp;
+  h->ell_hinge_damping = hdamp;
+  std::vector<int2> fnb(size_t(nfaces), make_int2(0, 0));
+  std::vector<float4> fdm(size_t(nfaces), make_float4(0.f, 0.f, 0.f, 0.f));
+  std::vector<float2> fmat(size_t(nfaces), make_float2(0.f, 0.f));
+  std::vector<float> fkd(fdamp ? size_t(nfaces) : 0, 0.f);
+  std::vector<int4> hidx(size_t(nhinges), make_int4(0, 0, 0, 0));
+  std::vector<float2> hprop(size_t(nhinges), make_float2(0.f, 0.f));
+  std::vector<float> hkd(hdamp ? size_t(nhinges) : 0, 0.f);
+  for (int r = 0; r < R; ++r) {
+    const int a = h->ranges_host[r];
+    const long long n = h->ranges_host[r + 1] - a;
+    for (int j = 0; j < n; ++j) {
+      const int v = h->range_verts_host[a + j];
+      int s = 0;
+      for (int q = h->h_foff[v]; q < h->h_foff[v + 1]; ++q, ++s) {
+        const int t = h->h_fadj[q] >> 2, ord = h->h_fadj[q] & 3;
+        const long long i = h->ell_fbase[r] + s * n + j;
+        const int* ti = &h->h_tri[3 * size_t(t)];
+        const double D00 = pose[4 * t], D01 = pose[4 * t + 1], D10 = pose[4 * t + 2], D11 = pose[4 * t + 3];
+        double P00 = D00, P01 = D01, P10 = D10, P11 = D11;
+        if (ord == 1) {  // [x2 - x1, x0 - x1] = E [[-1,-1],[1,0]]  ->  D' = [[0,1],[-1,-1]] D
+          fnb[i] = make_int2(ti[2], ti[0]);
+          P00 = D10, P01 = D11, P10 = -D00 - D10, P11 = -D01 - D11;
+        } else if (ord == 2) {  // [x0 - x2, x1 - x2] = E [[0,1],[-1,-1]]  ->  D' = [[-1,-1],[1,0]] D
+          fnb[i] = make_int2(ti[0], ti[1]);
+          P00 = -D00 - D10, P01 = -D01 - D11, P10 = D00, P11 = D01;
+        } else {
+          fnb[i] = make_int2(ti[1], ti[2]);
+        }
+        fdm[i] = make_float4(float(P00), float(P01), float(P10), float(P11));
+        fmat[i] = make_float2(mat[5 * t] * area[t], mat[5 * t + 1] * area[t]);
+        if (fdamp) fkd[i] = mat[5 * t + 2];
+      }
+      s = 0;
+      for (int q = h->h_eoff[v]; q < h->h_eoff[v + 1]; ++q, ++s) {
+        const int e = h->h_eadj[q] >> 2, ord = h->h_eadj[q] & 3;
+        const long long i = h->ell_ebase[r] + s * n + j;
+        const int* ei = &h->h_edges[4 * size_t(e)];
+        hidx[i] = make_int4(ei[0], ei[1], ei[2], int(unsigned(ei[3]) | (unsigned(ord) << 30)));
+        const float ke = bp[2 * e];
+        hprop[i] = make_float2(ra[e], ke > 0.f ? ke * rl[e] : 0.f);
+        if (hdamp) hkd[i] = bp[2 * e + 1];
+      }
+    }
+  }
+  if ((rc = upload_into(&h->range_nf, h->ell_nf)) || (rc = upload_into(&h->range_ne, h->ell_ne)) ||
+      (rc = upload_into(&h->range_fbase, h->ell_fbase)) || (rc = upload_into(&h->range_ebase, h->ell_ebase)) ||
+      (rc = upload_into(&h->face_nb, fnb)) || (rc = upload_into(&h->face_dm, fdm)) ||
+      (rc = upload_into(&h->face_mat, fmat)) || (rc = upload_into(&h->hinge_idx, hidx)) ||
+      (rc = upload_into(&h->hinge_prop, hprop)))
+    return rc;
+  dfree(h->face_kd);
+  dfree(h->hinge_kd);
+  if (fdamp && (rc = upload_into(&h->face_kd, fkd))) return rc;
+  if (hdamp && (rc = upload_into(&h->hinge_kd, hkd))) return rc;
+  return VBD_OK;
+}
+
+EllView ell_view(const VbdSolver* h) {
+  EllView e;
+  e.range_nf = h->range_nf;
+  e.range_ne = h->range_ne;
+  e.range_fbase = h->range_fbase;
+  e.range_ebase = h->range_ebase;
+  e.face_nb = h->face_nb;
+  e.face_dm = h->face_dm;
+  e.face_mat = h->face_mat;
+  e.face_kd = h->ell_face_damping ? h->face_kd : nullptr;
+  e.hinge_idx = h->hinge_idx;
+  e.hinge_prop = h->hinge_prop;
+  e.hinge_kd = h->ell_hinge_damping ? h->hinge_kd : nullptr;
+  return e;
+}
 
 int pack_model(VbdSolver* h, cudaStream_t st) {
   const VbdModelDesc& m = h->md;
@@ -302,6 +462,17 @@ void launch_persistent(int L, const StepCtx<R>& c, const PersistentPlan& p, int 
   }
 }
 
+template <typename R, int MODE, bool SMEM>
+void launch_persistent_ell(int occ, const StepCtx<R>& c, const PersistentPlan& p, const EllView& e, int grid,
+                           int block, size_t smem, cudaStream_t st) {
+  switch (occ) {
+    case 2: k_persistent_ell<R, MODE, SMEM, 2><<<grid, block, smem, st>>>(c, p, e); break;
+    case 3: k_persistent_ell<R, MODE, SMEM, 3><<<grid, block, smem, st>>>(c, p, e); break;
+    case 4: k_persistent_ell<R, MODE, SMEM, 4><<<grid, block, smem, st>>>(c, p, e); break;
+    default: k_persistent_ell<R, MODE, SMEM, 0><<<grid, block, smem, st>>>(c, p, e); break;
+  }
+}
+
 int ensure_contact_capacity(VbdSolver* h, int cmax, cudaStream_t st) {
   if (cmax <= h->c_cap) return VBD_OK;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -356,7 +527,7 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
     }
   }
   const int iters = h->prm.iterations;
-  if (MODE == MODE_MIXED) CK(cudaMemsetAsync(h->residual, 0, sizeof(double) * std::max(iters, 1), st));
+  if (MODE == MODE_MIXED) CK(cudaMemsetAsync(h->residual, 0, sizeof(double) * 32 * std::max(iters, 1), st));
   if (h->schedule == VBD_SCHEDULE_PERSISTENT) {
     CK(cudaMemsetAsync(h->queue, 0, sizeof(int), st));
     if (has_c) {
@@ -365,7 +536,17 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
     }
     PersistentPlan p{h->W, h->inst_order, h->inst_vstart, h->inst_cptr, h->color_ranges, h->color_verts, h->queue,
                      iters};
-    if constexpr (std::is_same<R, float>::value) {
+    if (h->layout == VBD_LAYOUT_ELL) {
+      const EllView e = ell_view(h);
+      if constexpr (std::is_same<R, float>::value) {
+        if (h->smem_bytes > 0)
+          launch_persistent_ell<R, MODE, true>(h->occ, c, p, e, h->grid_persistent, h->block, h->smem_bytes, st);
+        else
+          launch_persistent_ell<R, MODE, false>(h->occ, c, p, e, h->grid_persistent, h->block, 0, st);
+      } else {
+        launch_persistent_ell<R, MODE, false>(0, c, p, e, h->grid_persistent, h->block, 0, st);
+      }
+    } else if constexpr (std::is_same<R, float>::value) {
       if (h->smem_bytes > 0)
         launch_persistent<R, MODE, true>(h->L, c, p, h->grid_persistent, h->block, h->smem_bytes, st);
       else
@@ -377,10 +558,15 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
     k_forward<R><<<(h->V + 255) / 256, 256, 0, st>>>(c);
     if (has_c) k_contact_prepare<R><<<(c.c_max + 255) / 256, 256, 0, st>>>(c);
     const int* cp = h->md.color_particles_dev;
+    const EllView e = ell_view(h);
     for (int it = 0; it < iters; ++it)
       for (size_t col = 0; col + 1 < h->color_offsets.size(); ++col) {
         const int a = h->color_offsets[col], b = h->color_offsets[col + 1];
-        launch_color_any<R, MODE>(h->L, c, cp + a, b - a, it, h->block, st);
+        if (h->layout == VBD_LAYOUT_ELL) {
+          if (b > a) k_color_ell<R, MODE><<<(b - a + h->block - 1) / h->block, h->block, 0, st>>>(c, e, cp + a, int(col), b - a, it);
+        } else {
+          launch_color_any<R, MODE>(h->L, c, cp + a, b - a, it, h->block, st);
+        }
       }
     k_finalize<R><<<(h->V + 255) / 256, 256, 0, st>>>(c);
   }
@@ -388,8 +574,25 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
   return VBD_OK;
 }
 
+template <typename R, int MODE, bool SMEM>
+const void* persistent_ell_fn(int occ) {
+  switch (occ) {
+    case 2: return (const void*)k_persistent_ell<R, MODE, SMEM, 2>;
+    case 3: return (const void*)k_persistent_ell<R, MODE, SMEM, 3>;
+    case 4: return (const void*)k_persistent_ell<R, MODE, SMEM, 4>;
+    default: return (const void*)k_persistent_ell<R, MODE, SMEM, 0>;
+  }
+}
+
+
 const void* persistent_kernel(VbdSolver* h) {
   const bool sm = h->smem_bytes > 0;
+  if (h->layout == VBD_LAYOUT_ELL) {
+    if (h->precision == VBD_PRECISION_FP64) return persistent_ell_fn<double, MODE_FP64, false>(0);
+    if (h->precision == VBD_PRECISION_MIXED)
+      return sm ? persistent_ell_fn<float, MODE_MIXED, true>(h->occ) : persistent_ell_fn<float, MODE_MIXED, false>(h->occ);
+    return sm ? persistent_ell_fn<float, MODE_FP32, true>(h->occ) : persistent_ell_fn<float, MODE_FP32, false>(h->occ);
+  }
   if (h->precision == VBD_PRECISION_FP64) return persistent_fn<double, MODE_FP64, false>(h->L);
   if (h->precision == VBD_PRECISION_MIXED)
     return sm ? persistent_fn<float, MODE_MIXED, true>(h->L) : persistent_fn<float, MODE_MIXED, false>(h->L);
@@ -405,6 +608,81 @@ int occupancy_grid(VbdSolver* h) {
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, h->block, h->smem_bytes));
   if (per_sm < 1) return VBD_ERR_INVALID_ARGUMENT;
   h->grid_persistent = std::min(h->W, sms * per_sm);
+  return VBD_OK;
+}
+
+template <typename R>
+int record_impl(VbdSolver* h, const R* q_in, const R* qd_in, const R* f_ext, R dt, R* y, R* ck, R* q_out, R* qd_out,
+                cudaStream_t st) {
+  StepCtx<R> c = make_ctx<R, MODE_FP32>(h);
+  c.q_in = const_cast<R*>(q_in);
+  c.qd_in = qd_in;
+  c.f_ext = f_ext;
+  c.q_out = q_out;
+  c.qd_out = qd_out;
+  c.dt = dt;
+  c.dt2r = R(1) / (dt * dt);
+  const int V = h->V, I = h->prm.iterations;
+  const size_t n3 = size_t(3) * V;
+  k_record_forward<R><<<(V + 255) / 256, 256, 0, st>>>(c, y);
+  CK(cudaMemcpyAsync(ck, y, n3 * sizeof(R), cudaMemcpyDeviceToDevice, st));
+  const int* cp = h->md.color_particles_dev;
+  for (int it = 0; it < I; ++it) {
+    R* cur = ck + size_t(it + 1) * n3;
+    CK(cudaMemcpyAsync(cur, ck + size_t(it) * n3, n3 * sizeof(R), cudaMemcpyDeviceToDevice, st));
+    for (size_t col = 0; col + 1 < h->color_offsets.size(); ++col) {
+      const int a = h->color_offsets[col], b = h->color_offsets[col + 1];
+      if (b > a) k_record_color<R><<<(b - a + 127) / 128, 128, 0, st>>>(c, cur, y, cur, cp + a, b - a);
+    }
+  }
+  k_record_finish<R><<<int((n3 + 255) / 256), 256, 0, st>>>(c, ck + size_t(I) * n3);
+  CK(cudaGetLastError());
+  return VBD_OK;
+}
+
+template <typename R>
+int adjoint_impl(VbdSolver* h, const R* q_in, const R* y, const R* ck, R dt, const R* aq_out, const R* aqd_out, R* aq_in,
+                 R* aqd_in, R* adj_mu, R* adj_lambda, cudaStream_t st) {
+  const int V = h->V, I = h->prm.iterations, C = int(h->color_offsets.size()) - 1;
+  const size_t n3 = size_t(3) * V;
+  const size_t need = (size_t(std::max(C, 1)) + 2) * n3 * sizeof(R);
+  if (h->adj_work_bytes < need) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return VBD_ERR_UNSUPPORTED;
+    if (h->adj_work) cudaFree(h->adj_work);
+    h->adj_work = nullptr;
+    h->adj_work_bytes = 0;
+    int rc = dalloc((char**)&h->adj_work, need);
+    if (rc) return rc;
+    h->adj_work_bytes = need;
+  }
+  R* S = (R*)h->adj_work;  // C color-start states
+  R* ax = S + size_t(std::max(C, 1)) * n3;
+  R* ay = ax + n3;
+  StepCtx<R> c = make_ctx<R, MODE_FP32>(h);
+  c.q_in = const_cast<R*>(q_in);
+  c.dt = dt;
+  c.dt2r = R(1) / (dt * dt);
+  k_adjoint_begin<R><<<int((n3 + 255) / 256), 256, 0, st>>>(int(n3), aq_out, aqd_out, R(1) / dt, ax, ay);
+  AdjCtx<R> A{c, nullptr, y, ax, ay, adj_mu, adj_lambda};
+  const int* cp = h->md.color_particles_dev;
+  for (int it = I - 1; it >= 0; --it) {
+    CK(cudaMemcpyAsync(S, ck + size_t(it) * n3, n3 * sizeof(R), cudaMemcpyDeviceToDevice, st));
+    for (int col = 0; col + 1 < C; ++col) {
+      R* nxt = S + size_t(col + 1) * n3;
+      CK(cudaMemcpyAsync(nxt, S + size_t(col) * n3, n3 * sizeof(R), cudaMemcpyDeviceToDevice, st));
+      const int a = h->color_offsets[col], b = h->color_offsets[col + 1];
+      if (b > a) k_record_color<R><<<(b - a + 127) / 128, 128, 0, st>>>(c, nxt, y, nxt, cp + a, b - a);
+    }
+    for (int col = C - 1; col >= 0; --col) {
+      A.x = S + size_t(col) * n3;
+      const int a = h->color_offsets[col], b = h->color_offsets[col + 1];
+      if (b > a) k_adjoint_color<R><<<(b - a + 63) / 64, 64, 0, st>>>(A, cp + a, b - a);
+    }
+  }
+  k_adjoint_end<R><<<(V + 255) / 256, 256, 0, st>>>(c, ax, ay, aqd_out, aq_in, aqd_in);
+  CK(cudaGetLastError());
   return VBD_OK;
 }
 
@@ -478,6 +756,12 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
 
   std::vector<int> foff, fadj, eoff, eadj;
   build_packed_adjacency(h->V, h->T, tri.data(), h->E, edges.data(), foff, fadj, eoff, eadj);
+  h->h_tri = tri;
+  h->h_edges = edges;
+  h->h_foff = foff;
+  h->h_fadj = fadj;
+  h->h_eoff = eoff;
+  h->h_eadj = eadj;
   if ((rc = upload(&h->face_off, foff)) || (rc = upload(&h->face_adj, fadj)) || (rc = upload(&h->edge_off, eoff)) ||
       (rc = upload(&h->edge_adj, eadj)))
     return fail(rc);
@@ -539,7 +823,7 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
   if ((rc = dalloc((char**)&h->pos, p4 * h->V)) || (rc = dalloc((char**)&h->qprev, p4 * h->V)) ||
       (rc = dalloc((char**)&h->inertia, p4 * h->V)) || (rc = dalloc(&h->slot_cnt, h->V)) ||
       (rc = dalloc(&h->slots, size_t(h->V) * h->K)) || (rc = dalloc(&h->err, 1)) ||
-      (rc = dalloc(&h->residual, std::max(params->iterations, 1))))
+      (rc = dalloc(&h->residual, size_t(std::max(params->iterations, 1)) * 32)))
     return fail(rc);
   if (cudaMemset(h->err, 0, sizeof(int)) != cudaSuccess || cudaMemset(h->slot_cnt, 0, sizeof(int) * h->V) != cudaSuccess)
     return fail(VBD_ERR_CUDA);
@@ -547,7 +831,8 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
   // scheduling
   h->schedule = params->schedule;
   if (h->schedule == VBD_SCHEDULE_AUTO) h->schedule = (h->W > 1 || h->V <= 4096) ? VBD_SCHEDULE_PERSISTENT : VBD_SCHEDULE_PER_COLOR;
-  h->L = lpv ? lpv : (h->schedule == VBD_SCHEDULE_PERSISTENT && h->W == 1 ? 8 : 1);
+  h->L = lpv ? lpv
+              : ((h->schedule == VBD_SCHEDULE_PERSISTENT && h->W == 1 && params->layout != VBD_LAYOUT_ELL) ? 8 : 1);
   for (int w = 0; w < h->W; ++w) h->max_inst_v = std::max(h->max_inst_v, wstart[w + 1] - wstart[w]);
   if (h->schedule == VBD_SCHEDULE_PERSISTENT && h->precision != VBD_PRECISION_FP64 &&
       params->positions_in_shared != 1) {
@@ -563,6 +848,32 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
   }
   h->block = params->block_size ? params->block_size
                                 : (h->schedule == VBD_SCHEDULE_PERSISTENT ? (h->smem_bytes > 96 * 1024 ? 512 : 256) : 128);
+  // element data layout: stencil records (one thread per vertex) unless lanes per vertex > 1 asks for CSR
+  if (params->layout == VBD_LAYOUT_ELL && h->L != 1) return fail(VBD_ERR_INVALID_ARGUMENT);
+  h->layout = (params->layout == VBD_LAYOUT_CSR || h->L != 1) ? VBD_LAYOUT_CSR : VBD_LAYOUT_ELL;
+  if (h->layout == VBD_LAYOUT_ELL && h->schedule == VBD_SCHEDULE_PERSISTENT && h->block > 512)
+    return fail(VBD_ERR_INVALID_ARGUMENT);
+  if (params->min_blocks_per_sm != 0) {
+    if (params->min_blocks_per_sm < 2 || params->min_blocks_per_sm > 4 || h->layout != VBD_LAYOUT_ELL ||
+        h->schedule != VBD_SCHEDULE_PERSISTENT || h->precision == VBD_PRECISION_FP64 ||
+        (params->block_size != 0 && params->block_size != 256))
+      return fail(VBD_ERR_INVALID_ARGUMENT);
+    h->occ = params->min_blocks_per_sm;
+    h->block = 256;
+  }
+  if (h->layout == VBD_LAYOUT_ELL) {
+    if (h->schedule == VBD_SCHEDULE_PERSISTENT) {
+      h->range_verts_host = verts;
+      h->ranges_host.clear();
+      for (int w = 0; w < h->W; ++w)
+        for (int k = cptr[w]; k + 1 < cptr[w + 1]; ++k) h->ranges_host.push_back(ranges[k]);
+      h->ranges_host.push_back(int(verts.size()));
+    } else {
+      h->range_verts_host = colp;
+      h->ranges_host = h->color_offsets;
+    }
+    if ((rc = build_ell(h))) return fail(rc);
+  }
   if (h->schedule == VBD_SCHEDULE_PERSISTENT && (rc = occupancy_grid(h))) return fail(rc);
   if (cudaDeviceSynchronize() != cudaSuccess) return fail(VBD_ERR_CUDA);
   *out = h;
@@ -571,7 +882,13 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
 
 int vbd_refresh_model(VbdHandle h, void* stream) {
   if (!h) return VBD_ERR_INVALID_ARGUMENT;
-  return pack_model(h, (cudaStream_t)stream);
+  int rc = pack_model(h, (cudaStream_t)stream);
+  if (rc) return rc;
+  if (h->layout == VBD_LAYOUT_ELL) {
+    if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return VBD_ERR_CUDA;
+    return build_ell(h);
+  }
+  return VBD_OK;
 }
 
 int vbd_step(VbdHandle h, float* q_in, float* q_out, const float* qd_in, float* qd_out, const float* f_ext,
@@ -592,6 +909,31 @@ int vbd_step_f64(VbdHandle h, double* q_in, double* q_out, const double* qd_in, 
                                       (cudaStream_t)stream);
 }
 
+int vbd_record_step(VbdHandle h, const void* q_in, const void* qd_in, const void* particle_f, double dt, void* y,
+                    void* checkpoints, void* q_out, void* qd_out, void* stream) {
+  if (!h || !q_in || !qd_in || !y || !checkpoints || !q_out || !qd_out || !(dt > 0.0)) return VBD_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (h->precision == VBD_PRECISION_FP64)
+    return record_impl<double>(h, (const double*)q_in, (const double*)qd_in, (const double*)particle_f, dt,
+                               (double*)y, (double*)checkpoints, (double*)q_out, (double*)qd_out, st);
+  return record_impl<float>(h, (const float*)q_in, (const float*)qd_in, (const float*)particle_f, float(dt), (float*)y,
+                            (float*)checkpoints, (float*)q_out, (float*)qd_out, st);
+}
+
+int vbd_adjoint_step(VbdHandle h, const void* q_in, const void* y, const void* checkpoints, double dt,
+                     const void* adj_q_out, const void* adj_qd_out, void* adj_q_in, void* adj_qd_in, void* adj_tri_mu,
+                     void* adj_tri_lambda, void* stream) {
+  if (!h || !q_in || !y || !checkpoints || !adj_q_in || !(dt > 0.0)) return VBD_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (h->precision == VBD_PRECISION_FP64)
+    return adjoint_impl<double>(h, (const double*)q_in, (const double*)y, (const double*)checkpoints, dt,
+                                (const double*)adj_q_out, (const double*)adj_qd_out, (double*)adj_q_in,
+                                (double*)adj_qd_in, (double*)adj_tri_mu, (double*)adj_tri_lambda, st);
+  return adjoint_impl<float>(h, (const float*)q_in, (const float*)y, (const float*)checkpoints, float(dt),
+                             (const float*)adj_q_out, (const float*)adj_qd_out, (float*)adj_q_in, (float*)adj_qd_in,
+                             (float*)adj_tri_mu, (float*)adj_tri_lambda, st);
+}
+
 int vbd_get_error(VbdHandle h, int32_t* bits, void* stream) {
   if (!h || !bits) return VBD_ERR_INVALID_ARGUMENT;
   cudaStream_t st = (cudaStream_t)stream;
@@ -605,8 +947,14 @@ int vbd_get_residuals(VbdHandle h, double* out, int32_t n, void* stream) {
   if (!h || !out || n < 0 || n > std::max(h->prm.iterations, 1)) return VBD_ERR_INVALID_ARGUMENT;
   cudaStream_t st = (cudaStream_t)stream;
   if (n == 0) return VBD_OK;
-  CK(cudaMemcpyAsync(out, h->residual, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
+  double buf[32];
+  for (int i = 0; i < n; ++i) {
+    CK(cudaMemcpyAsync(buf, h->residual + size_t(i) * 32, sizeof(buf), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double acc = 0.0;
+    for (double b : buf) acc += b;
+    out[i] = acc;
+  }
   return VBD_OK;
 }
 
@@ -619,8 +967,10 @@ int vbd_launches_per_step(VbdHandle h, int32_t* out) {
   return VBD_OK;
 }
 
-int vbd_get_config(VbdHandle h, int32_t* schedule, int32_t* lanes, int32_t* block, int32_t* shared_bytes) {
+int vbd_get_config(VbdHandle h, int32_t* schedule, int32_t* lanes, int32_t* block, int32_t* shared_bytes,
+                   int32_t* layout) {
   if (!h) return VBD_ERR_INVALID_ARGUMENT;
+  if (layout) *layout = h->layout;
   if (schedule) *schedule = h->schedule;
   if (lanes) *lanes = h->L;
   if (block) *block = h->block;

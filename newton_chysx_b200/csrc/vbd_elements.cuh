@@ -36,8 +36,8 @@ __host__ __device__ __forceinline__ void membrane_add(int ord, vec3<R> x0, vec3<
   const vec3<R> f1 = x01 * D01 + x02 * D11;
   const R f00 = dot(f0, f0), f11 = dot(f1, f1), f01 = dot(f0, f1);
   const R Jsq = vmax(f00 * f11 - f01 * f01, R(1.0e-20));
-  const R J = vsqrt(Jsq);
-  const R invJ = R(1) / J;
+  const R invJ = vrsqrt(Jsq);
+  const R J = Jsq * invJ;
   const R lnh = lmbd + mu;
   const R lsafe = (lnh < R(0) ? R(-1) : R(1)) * vmax(vabs(lnh), R(1.0e-6));
   const R alpha = R(1) + mu / lsafe;
@@ -90,11 +90,12 @@ __host__ __device__ __forceinline__ void bending_add(int ord, const vec3<R> x[4]
                                                      R kd, R dt, const vec3<R>* xp, vec3<R>& f, sym3<R>& H) {
   const vec3<R> x02 = x[2] - x[0], x03 = x[3] - x[0], x13 = x[3] - x[1], x12 = x[2] - x[1], e = x[3] - x[2];
   const vec3<R> N1 = cross(x02, x03), N2 = cross(x13, x12);
-  const R l1 = length(N1), l2 = length(N2), le = length(e);
-  const R eps = R(1.0e-6);
-  if (l1 < eps || l2 < eps || le < eps) return;
-  const R il1 = R(1) / l1, il2 = R(1) / l2;
-  const vec3<R> n1 = N1 * il1, n2 = N2 * il2, eh = e * (R(1) / le);
+  const R s1 = dot(N1, N1), s2 = dot(N2, N2), se = dot(e, e);
+  // |N1|, |N2|, |e| < 1e-6 (degenerate hinge): no contribution
+  const R eps2 = R(1.0e-12);
+  if (s1 < eps2 || s2 < eps2 || se < eps2) return;
+  const R il1 = vrsqrt(s1), il2 = vrsqrt(s2);
+  const vec3<R> n1 = N1 * il1, n2 = N2 * il2, eh = e * vrsqrt(se);
   const R s = dot(cross(n1, n2), eh);
   const R c = dot(n1, n2);
   const R theta = vatan2(s, c);

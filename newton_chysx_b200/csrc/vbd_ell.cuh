@@ -1,0 +1,229 @@
+// Stencil ("ELL") layout of the per-vertex element data, and the solve that reads it.
+//
+// The CSR path (vbd_kernels.cuh) reaches a triangle or hinge through the vertex adjacency and
+// gathers its record by element id, so the 32 lanes of a warp touch 32 unrelated records. Here
+// every (vertex, element) incidence gets its own record, prepared once per model, stored in the
+// order in which the sweep visits the vertices and slot-major within a color range:
+//     record(range r, slot s, vertex j of the range) at  base[r] + s * n[r] + j
+// so that lane j of a warp reading slot s of consecutive vertices reads consecutive addresses, and no
+// adjacency list sits on the dependent-load chain.
+//
+// Face record, with the solved vertex renumbered as vertex 0 of the triangle (cyclic order, so the
+// orientation is kept):
+//   int2   (a, b)            the other two vertices
+//   float4 D'^-1             rest inverse re-expressed for that numbering: [x_a - x, x_b - x] D'^-1 = F
+//   float2 (mu A, lambda A)  Lame coefficients times the rest area (the energy is homogeneous of degree
+//                            one in (mu, lambda), so scaling both by the area scales force and Hessian)
+//   float  damping           read only when the model has non-zero membrane damping
+// Hinge record:
+//   int4   (o0, o1, v0, v1)  with the solved vertex's role (0..3) in the top two bits of v1
+//   float2 (rest angle, ke * rest length)
+//   float  kd                read only when the model has non-zero bending damping
+// Empty slots (vertices with fewer elements than the range's maximum) carry zero stiffness.
+#pragma once
+#include "vbd_kernels.cuh"
+
+namespace vbd {
+
+struct EllView {
+  const int* range_nf;    // [ranges] face slots of the range
+  const int* range_ne;    // [ranges] hinge slots
+  const long long* range_fbase;  // [ranges] first face record of the range
+  const long long* range_ebase;  // [ranges] first hinge record
+  const int2* face_nb;
+  const float4* face_dm;
+  const float2* face_mat;
+  const float* face_kd;  // NULL when no membrane damping
+  const int4* hinge_idx;
+  const float2* hinge_prop;
+  const float* hinge_kd;  // NULL when no bending damping
+};
+
+// One vertex (thread) of range r at position j (0-based within the range).
+template <typename R, int MODE, typename P>
+__device__ __forceinline__ void solve_ell(const StepCtx<R>& c, const P& pos, const EllView& e, int r, int n, int j,
+                                          int v, int iteration) {
+  const pos4_t<R> in4 = c.inertia[v];
+  const R m = R(in4.w);
+  if (m == R(0)) return;
+  const vec3<R> x = pos.ld(v);
+  vec3<R> f = zero3<R>();
+  sym3<R> H = szero<R>();
+  const int nf = __ldg(e.range_nf + r), ne = __ldg(e.range_ne + r);
+  // Faces. The records of slot s + 1 are loaded while slot s is evaluated, so each thread keeps one
+  // global load in flight under the element math.
+  {
+    const long long b0 = __ldg(e.range_fbase + r) + j;
+    const float2* pm = e.face_mat + b0;
+    const int2* pn = e.face_nb + b0;
+    const float4* pd = e.face_dm + b0;
+    const float* pk = e.face_kd ? e.face_kd + b0 : nullptr;
+    float2 mat_n = make_float2(0.f, 0.f);
+    int2 nb_n = make_int2(0, 0);
+    float4 dm_n = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (nf > 0) {
+      mat_n = __ldg(pm);
+      nb_n = __ldg(pn);
+      dm_n = __ldg(pd);
+    }
+    for (int s = 0; s < nf; ++s) {
+      const float2 mat = mat_n;
+      const int2 nb = nb_n;
+      const float4 dm = dm_n;
+      const float kd = pk ? __ldg(pk) : 0.f;
+      if (s + 1 < nf) {
+        pm += n;
+        pn += n;
+        pd += n;
+        if (pk) pk += n;
+        mat_n = __ldg(pm);
+        nb_n = __ldg(pn);
+        dm_n = __ldg(pd);
+      }
+      if (!(mat.x > 0.f || mat.y > 0.f)) continue;
+      const R pose[4] = {R(dm.x), R(dm.y), R(dm.z), R(dm.w)};
+      vec3<R> xp[3];
+      if (kd > 0.f) {
+        xp[0] = ld3<R>(c.qprev[v]);
+        xp[1] = ld3<R>(c.qprev[nb.x]);
+        xp[2] = ld3<R>(c.qprev[nb.y]);
+      }
+      membrane_add<R>(0, x, pos.ld(nb.x), pos.ld(nb.y), pose, R(mat.x), R(mat.y), R(kd), R(1), c.dt, xp, f, H);
+    }
+  }
+  // Hinges, pipelined the same way.
+  {
+    const long long b0 = __ldg(e.range_ebase + r) + j;
+    const float2* pp = e.hinge_prop + b0;
+    const int4* pi = e.hinge_idx + b0;
+    const float* pk = e.hinge_kd ? e.hinge_kd + b0 : nullptr;
+    float2 pr_n = make_float2(0.f, 0.f);
+    int4 id_n = make_int4(0, 0, 0, 0);
+    if (ne > 0) {
+      pr_n = __ldg(pp);
+      id_n = __ldg(pi);
+    }
+    for (int s = 0; s < ne; ++s) {
+      const float2 pr = pr_n;
+      const int4 id = id_n;
+      const float kd = pk ? __ldg(pk) : 0.f;
+      if (s + 1 < ne) {
+        pp += n;
+        pi += n;
+        if (pk) pk += n;
+        pr_n = __ldg(pp);
+        id_n = __ldg(pi);
+      }
+      if (!(pr.y > 0.f)) continue;
+      const int ord = int((unsigned)id.w >> 30);
+      const int v1 = id.w & 0x3fffffff;
+      vec3<R> xs[4];
+      xs[0] = pos.ld(id.x);
+      xs[1] = pos.ld(id.y);
+      xs[2] = pos.ld(id.z);
+      xs[3] = pos.ld(v1);
+      vec3<R> xp[4];
+      if (kd > 0.f) {
+        xp[0] = ld3<R>(c.qprev[id.x]);
+        xp[1] = ld3<R>(c.qprev[id.y]);
+        xp[2] = ld3<R>(c.qprev[id.z]);
+        xp[3] = ld3<R>(c.qprev[v1]);
+      }
+      bending_add<R>(ord, xs, R(pr.x), R(1), R(pr.y), R(kd), c.dt, xp, f, H);
+    }
+  }
+  const R md = m * c.dt2r;
+  f = f + md * (ld3<R>(in4) - x);
+  H.xx += md;
+  H.yy += md;
+  H.zz += md;
+  if (c.has_contacts) contacts_add<R>(c, v, x, f, H);
+  if (MODE == MODE_MIXED && c.residual) {
+    const double r2 = double(f.x) * double(f.x) + double(f.y) * double(f.y) + double(f.z) * double(f.z);
+    atomicAdd(c.residual + 32 * iteration + (threadIdx.x & 31), r2);  // 32 slots, summed on the host
+  }
+  vec3<R> dlt;
+  double det_used;
+  if (MODE == MODE_MIXED) {
+    const R hmax = vmax(vmax(vmax(vabs(H.xx), vabs(H.yy)), vmax(vabs(H.zz), vabs(H.xy))), vmax(vabs(H.xz), vabs(H.yz)));
+    const R d = sdet(H);
+    if (!(vabs(d) >= R(c.fp64_thr) * hmax * hmax * hmax)) {  // ill-conditioned or not finite: FP64
+      const sym3<double> Hd = {double(H.xx), double(H.yy), double(H.zz), double(H.xy), double(H.xz), double(H.yz)};
+      const vec3<double> fd = {double(f.x), double(f.y), double(f.z)};
+      det_used = sdet(Hd);
+      const vec3<double> rr = sadj_mul(Hd, fd) * (1.0 / det_used);
+      dlt = {R(rr.x), R(rr.y), R(rr.z)};
+    } else {
+      det_used = double(d);
+      dlt = sadj_mul(H, f) * (R(1) / d);
+    }
+  } else {
+    const R d = sdet(H);
+    det_used = double(d);
+    dlt = sadj_mul(H, f) * (R(1) / d);
+  }
+  if (!isfinite(det_used)) {
+    set_err(c.err, 1);
+    return;
+  }
+  if (!(fabs(det_used) > 1e-8)) {
+    set_err(c.err, 4);
+    return;
+  }
+  const vec3<R> xn = x + dlt;
+  if (!(isfinite(double(xn.x)) && isfinite(double(xn.y)) && isfinite(double(xn.z)))) {
+    set_err(c.err, 1);
+    return;
+  }
+  pos.st(v, xn);
+}
+
+// Per-color launch: range r = color r; verts = the color's particles.
+template <typename R, int MODE>
+__global__ void k_color_ell(StepCtx<R> c, EllView e, const int* __restrict__ verts, int r, int n, int iteration) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  solve_ell<R, MODE>(c, GlobalPos<R>{c.pos}, e, r, n, j, __ldg(verts + j), iteration);
+}
+
+// One launch per substep, one CTA per instance at a time (ranges = the instance's colors).
+// OCC > 0: compiled for OCC resident CTAs of 256 threads per SM (register budget 65536 / (256 OCC));
+// OCC = 0: CTAs of up to 512 threads, up to 128 registers per thread.
+template <typename R, int MODE, bool SMEM, int OCC>
+__global__ void __launch_bounds__(OCC ? 256 : 512, OCC ? OCC : 1) k_persistent_ell(StepCtx<R> c, PersistentPlan p,
+                                                                                  EllView e) {
+  extern __shared__ float s_pos[];
+  __shared__ int s_item;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = atomicAdd(p.queue, 1);
+    __syncthreads();
+    const int q = s_item;
+    if (q >= p.W) return;
+    const int w = __ldg(p.inst_order + q);
+    const int vs = __ldg(p.inst_vstart + w), ve = __ldg(p.inst_vstart + w + 1);
+    using Pos = typename std::conditional<SMEM, SmemPos, GlobalPos<R>>::type;
+    Pos pos;
+    if constexpr (SMEM) {
+      pos = SmemPos{s_pos, vs};
+    } else {
+      pos = GlobalPos<R>{c.pos};
+    }
+    for (int i = vs + threadIdx.x; i < ve; i += blockDim.x) forward_particle(c, pos, i);
+    __syncthreads();
+    const int cb = __ldg(p.inst_cptr + w), ce = __ldg(p.inst_cptr + w + 1);
+    for (int it = 0; it < p.iterations; ++it) {
+      for (int col = cb; col + 1 < ce; ++col) {
+        // range index of (instance, color) = col - w: each instance has one more range offset than ranges
+        const int a = __ldg(p.color_ranges + col), b = __ldg(p.color_ranges + col + 1);
+        const int r = col - w;
+        for (int j = threadIdx.x; j < b - a; j += blockDim.x)
+          solve_ell<R, MODE>(c, pos, e, r, b - a, j, __ldg(p.color_verts + a + j), it);
+        __syncthreads();
+      }
+    }
+    for (int i = vs + threadIdx.x; i < ve; i += blockDim.x) finalize_particle(c, pos, i);
+  }
+}
+
+}  // namespace vbd

@@ -308,7 +308,7 @@ __device__ __forceinline__ void solve_group(const StepCtx<R>& c, const P& pos, i
     double r2 = leader ? double(f.x) * double(f.x) + double(f.y) * double(f.y) + double(f.z) * double(f.z) : 0.0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) r2 += __shfl_xor_sync(0xffffffffu, r2, o);
-    if ((threadIdx.x & 31) == 0 && r2 != 0.0) atomicAdd(c.residual + iteration, r2);
+    if ((threadIdx.x & 31) == 0 && r2 != 0.0) atomicAdd(c.residual + 32 * iteration, r2);
   }
   if (!leader) return;
   vec3<R> dlt;

@@ -42,6 +42,15 @@ template <typename R> __host__ __device__ __forceinline__ vec3<R> cross(vec3<R> 
 __host__ __device__ __forceinline__ float vsqrt(float x) { return sqrtf(x); }
 __host__ __device__ __forceinline__ double vsqrt(double x) { return sqrt(x); }
 __host__ __device__ __forceinline__ float vatan2(float y, float x) { return atan2f(y, x); }
+// reciprocal square root: the hardware approximation on the device for float, exact elsewhere
+__host__ __device__ __forceinline__ float vrsqrt(float x) {
+#ifdef __CUDA_ARCH__
+  return rsqrtf(x);
+#else
+  return 1.0f / sqrtf(x);
+#endif
+}
+__host__ __device__ __forceinline__ double vrsqrt(double x) { return 1.0 / sqrt(x); }
 __host__ __device__ __forceinline__ double vatan2(double y, double x) { return atan2(y, x); }
 template <typename R> __host__ __device__ __forceinline__ R vabs(R x) { return x < R(0) ? -x : x; }
 template <typename R> __host__ __device__ __forceinline__ R vmax(R a, R b) { return a > b ? a : b; }

@@ -16,6 +16,10 @@ Beyond the reference keywords:
 * ``lanes_per_vertex`` / ``block_size``: launch shape (0 = default; see ``autotune``).
 * ``positions_in_shared``: ``"auto"`` / ``"off"`` / ``"on"`` — the persistent kernel keeps each
   instance's positions in shared memory during the sweep (FP32 and mixed precision).
+* ``layout``: ``"ell"`` (per-incidence stencil records in sweep order, coalesced; one lane per
+  vertex), ``"csr"`` (adjacency + element records; any lanes per vertex), ``"auto"``.
+* ``min_blocks_per_sm``: 2..4 compiles the persistent stencil kernel for that many resident CTAs of
+  256 threads per SM (a register budget); 0 leaves the compiler's choice.
 """
 
 from __future__ import annotations
@@ -83,6 +87,8 @@ class SolverVBD:
         fp64_solve_threshold: float = 1e-3,
         contact_slots: int = 0,
         positions_in_shared: str = "auto",
+        layout: str = "auto",
+        min_blocks_per_sm: int = 0,
     ):
         if rigid_avbd_beta < 0:
             raise ValueError(f"rigid_avbd_beta must be >= 0, got {rigid_avbd_beta}")
@@ -175,6 +181,8 @@ class SolverVBD:
         prm.block_size = int(block_size)
         prm.contact_slots = int(contact_slots)
         prm.positions_in_shared = {"auto": 0, "off": 1, "on": 2}[positions_in_shared]
+        prm.layout = _lib.LAYOUT[layout]
+        prm.min_blocks_per_sm = int(min_blocks_per_sm)
         self._prm = prm
 
         h = C.c_void_p()
@@ -184,8 +192,9 @@ class SolverVBD:
             raise ValueError("model.particle_color_groups is empty")
         _lib.check(rc, "vbd_create")
         self._h = h
-        s, lanes, blk, smem = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
-        self._lib.vbd_get_config(h, C.byref(s), C.byref(lanes), C.byref(blk), C.byref(smem))
+        s, lanes, blk, smem, lay = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        self._lib.vbd_get_config(h, C.byref(s), C.byref(lanes), C.byref(blk), C.byref(smem), C.byref(lay))
+        self.layout = _lib.LAYOUT_NAME[lay.value]
         self.schedule = _lib.SCHEDULE_NAME[s.value]
         self.lanes_per_vertex = lanes.value
         self.block_size = blk.value

@@ -91,3 +91,35 @@ def test_contact(hostlib, golden_dir, prec, rtol):
         scale = max(np.abs(f_o).max(), np.abs(H_o).max())
         assert np.abs(out[:3] - f_o).max() <= rtol * scale
         assert np.abs(out[3:].reshape(3, 3) - H_o).max() <= rtol * scale
+
+
+def _reexpress(order, X, pose):
+    """The stencil record of vbd_b200.cu build_ell: the solved vertex renumbered as vertex 0."""
+    D00, D01, D10, D11 = pose
+    if order == 1:
+        Xr = np.stack([X[1], X[2], X[0]])
+        P = (D10, D11, -D00 - D10, -D01 - D11)
+    elif order == 2:
+        Xr = np.stack([X[2], X[0], X[1]])
+        P = (-D00 - D10, -D01 - D11, D00, D01)
+    else:
+        Xr, P = X.copy(), (D00, D01, D10, D11)
+    return Xr, np.array(P)
+
+
+@pytest.mark.parametrize("prec,rtol", [(64, 1e-9), (32, 3e-4)])
+def test_stencil_face_record_is_the_same_membrane(hostlib, golden_dir, prec, rtol):
+    for r in _cases(golden_dir, "membrane"):
+        X, Xp, pose = r[0:9].reshape(3, 3), r[9:18].reshape(3, 3), r[18:22]
+        area, mu, lam, damping, dt, order = r[22:28]
+        f_o, H_o = orc.element("membrane", 64, order, X.ravel(), Xp.ravel(), pose, area, mu, lam, damping, dt)
+        Xr, P = _reexpress(int(order), X, pose)
+        Xpr, _ = _reexpress(int(order), Xp, pose)
+        out, op = _p(np.zeros(12))
+        a, ap = _p(Xr.ravel())
+        b, bp = _p(Xpr.ravel())
+        c, cp = _p(P)
+        hostlib.host_membrane(prec, 0, ap, bp, cp, 1.0, mu * area, lam * area, damping, dt, op)
+        scale = max(np.abs(f_o).max(), np.abs(H_o).max())
+        assert np.abs(out[:3] - f_o).max() <= rtol * scale
+        assert np.abs(out[3:].reshape(3, 3) - H_o).max() <= rtol * scale

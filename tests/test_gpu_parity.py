@@ -18,9 +18,10 @@ from tests.helpers import contacts_from_golden, load_golden, model_from_golden, 
 pytestmark = pytest.mark.gpu
 
 FIXTURES = ["step_grid_ground.npz", "step_grid_sphere.npz", "step_complex_rest_angle.npz"]
-# (schedule, lanes per vertex, positions in shared memory)
-LAUNCH = [("per_color", 1, "auto"), ("per_color", 4, "auto"), ("persistent", 1, "on"), ("persistent", 8, "on"),
-          ("persistent", 32, "on"), ("persistent", 1, "off"), ("persistent", 4, "off")]
+# (schedule, lanes per vertex, positions in shared memory, element layout)
+LAUNCH = [("per_color", 1, "auto", "ell"), ("per_color", 1, "auto", "csr"), ("per_color", 4, "auto", "csr"),
+          ("persistent", 1, "on", "ell"), ("persistent", 1, "off", "ell"), ("persistent", 1, "on", "csr"),
+          ("persistent", 8, "on", "csr"), ("persistent", 32, "on", "csr"), ("persistent", 4, "off", "csr")]
 
 
 def _state(arr, dtype=torch.float32):
@@ -41,14 +42,14 @@ def _run_golden_substep(solver, g, s, dtype=torch.float32):
 
 
 @pytest.mark.parametrize("name", FIXTURES)
-@pytest.mark.parametrize("schedule,lanes,shared", LAUNCH)
-def test_fp32_step_matches_reference_goldens(name, schedule, lanes, shared):
+@pytest.mark.parametrize("schedule,lanes,shared,layout", LAUNCH)
+def test_fp32_step_matches_reference_goldens(name, schedule, lanes, shared, layout):
     g = load_golden(name)
     model = model_from_golden(g)
     solver = SolverVBD(model, iterations=int(g["iterations"]), friction_epsilon=float(g["friction_epsilon"]),
                        rigid_avbd_beta=float(g["beta"]), schedule=schedule, lanes_per_vertex=lanes,
-                       positions_in_shared=shared)  # fmt: skip
-    assert solver.schedule == schedule and solver.lanes_per_vertex == lanes
+                       positions_in_shared=shared, layout=layout)  # fmt: skip
+    assert solver.schedule == schedule and solver.lanes_per_vertex == lanes and solver.layout == layout
     assert (solver.shared_bytes > 0) == (schedule == "persistent" and shared == "on")
     for s in range(int(g["substeps"])):
         st_in, st_out = _run_golden_substep(solver, g, s)
@@ -66,11 +67,12 @@ def test_fp32_step_matches_reference_goldens(name, schedule, lanes, shared):
 
 @pytest.mark.parametrize("name", FIXTURES)
 @pytest.mark.parametrize("schedule", ["per_color", "persistent"])
-def test_fp64_step_matches_fp64_oracle(name, schedule):
+@pytest.mark.parametrize("layout", ["ell", "csr"])
+def test_fp64_step_matches_fp64_oracle(name, schedule, layout):
     g = load_golden(name)
     model = model_from_golden(g)
     solver = SolverVBD(model, iterations=int(g["iterations"]), friction_epsilon=float(g["friction_epsilon"]),
-                       rigid_avbd_beta=float(g["beta"]), precision="fp64", schedule=schedule)  # fmt: skip
+                       rigid_avbd_beta=float(g["beta"]), precision="fp64", schedule=schedule, layout=layout)  # fmt: skip
     om = orc.Model(oracle_model_dict(model, float(g["friction_epsilon"]), float(g["beta"])))
     for s in range(int(g["substeps"])):
         st_in, st_out = _run_golden_substep(solver, g, s, torch.float64)
@@ -84,10 +86,12 @@ def test_fp64_step_matches_fp64_oracle(name, schedule):
         assert np.abs(st_out.particle_qd.cpu().numpy() - qd_o).max() <= 1e-9 / float(g["dt"])
 
 
-def test_mixed_precision_matches_and_reports_residuals():
+@pytest.mark.parametrize("layout", ["ell", "csr"])
+def test_mixed_precision_matches_and_reports_residuals(layout):
     g = load_golden("step_grid_ground.npz")
     model = model_from_golden(g)
-    solver = SolverVBD(model, iterations=int(g["iterations"]), precision="mixed", fp64_solve_threshold=1.0)
+    solver = SolverVBD(model, iterations=int(g["iterations"]), precision="mixed", fp64_solve_threshold=1.0,
+                       layout=layout)  # fmt: skip
     st_in, st_out = _run_golden_substep(solver, g, 0)
     assert np.abs(st_out.particle_q.cpu().numpy() - g["s0_q_out"]).max() <= 1e-4
     res = solver.residuals()

@@ -161,9 +161,12 @@ def test_schedules_and_lane_counts_agree():
     b.add_ground_plane()
     model = b.finalize("cuda")
     results = []
-    for schedule, lanes, shared in [("per_color", 1, "auto"), ("per_color", 8, "auto"), ("persistent", 1, "on"),
-                                    ("persistent", 16, "on"), ("persistent", 2, "off")]:
-        solver = SolverVBD(model, iterations=10, schedule=schedule, lanes_per_vertex=lanes, positions_in_shared=shared)
+    for schedule, lanes, shared, layout in [("per_color", 1, "auto", "ell"), ("per_color", 1, "auto", "csr"),
+                                            ("per_color", 8, "auto", "csr"), ("persistent", 1, "on", "ell"),
+                                            ("persistent", 1, "off", "ell"), ("persistent", 16, "on", "csr"),
+                                            ("persistent", 2, "off", "csr")]:
+        solver = SolverVBD(model, iterations=10, schedule=schedule, lanes_per_vertex=lanes, positions_in_shared=shared,
+                           layout=layout)  # fmt: skip
         s = _run(model, solver, 3, 10, 1.0 / 600.0, CollisionPipeline(model))
         results.append(s.particle_q.cpu().numpy())
     for r in results[1:]:
@@ -185,9 +188,10 @@ def test_batched_worlds_match_single_instances():
     assert solver.shared_bytes == 12 * max(n * n for n in sizes)
     s = _run(model, solver, 2, 10, 1.0 / 600.0)
     q = s.particle_q.cpu().numpy()
-    s_g = _run(model, SolverVBD(model, iterations=10, schedule="persistent", positions_in_shared="off"), 2, 10,
-               1.0 / 600.0)  # fmt: skip
-    assert np.abs(s_g.particle_q.cpu().numpy() - q).max() <= 1e-5
+    for shared, layout in [("off", "ell"), ("on", "csr"), ("off", "csr")]:
+        s_g = _run(model, SolverVBD(model, iterations=10, schedule="persistent", positions_in_shared=shared,
+                                    layout=layout), 2, 10, 1.0 / 600.0)  # fmt: skip
+        assert np.abs(s_g.particle_q.cpu().numpy() - q).max() <= 1e-5
     start = 0
     for b in singles:
         m1 = b.finalize("cuda")
