@@ -22,6 +22,7 @@ extern "C" {
 #define VBD_ERR_OUT_OF_MEMORY -3
 #define VBD_ERR_UNSUPPORTED -4
 #define VBD_ERR_EMPTY_COLORING -5
+#define VBD_ERR_TOO_LARGE -6 /* vbd_step_noalloc: the model exceeds its fixed scratch */
 
 /* Bits of the device-side error word (vbd_get_error). Kernels set bits instead of trapping. */
 #define VBD_DEVERR_NONFINITE 1          /* a solved displacement was NaN/Inf (position left unchanged) */
@@ -183,6 +184,39 @@ int vbd_get_config(VbdHandle h, int32_t* schedule, int32_t* lanes_per_vertex, in
                    int32_t* shared_bytes, int32_t* layout);
 
 int vbd_destroy(VbdHandle h);
+
+/* ---------------------------------------------------------------- step without allocation */
+
+/* Vertex -> element adjacency in the reference layout, as vbd_build_adjacency writes it (offsets
+   count two ints per entry; entries are (element, order) pairs), copied to device memory. */
+typedef struct VbdRefAdjacency {
+  const int32_t* face_offsets_dev; /* [V+1] */
+  const int32_t* faces_dev;
+  const int32_t* edge_offsets_dev; /* [V+1] */
+  const int32_t* edges_dev;
+} VbdRefAdjacency;
+
+#define VBD_NOALLOC_MAX_PARTICLES 32768
+#define VBD_NOALLOC_MAX_CONTACT_SLOTS 4
+
+/* A cloth step for callers that may not allocate device memory: a host application that owns all
+   device memory through its own pool and forbids plug-ins to call cudaMalloc, or code that steps the
+   cloth while capturing a larger CUDA graph, where an allocation would break the capture. No
+   counterpart in the reference (there, SolverVBD.__init__ always allocates its scratch).
+   Takes the model arrays in the reference layout (only the particle, triangle, hinge, color, gravity
+   and shape-material fields of VbdModelDesc are read) and the adjacency above, and runs the same
+   per-color FP32 step as vbd_step with the same side effects on the state arrays. It calls no
+   cudaMalloc/cudaFree: its per-particle scratch is one fixed __device__ array of 2,228,224 bytes
+   (VBD_NOALLOC_MAX_PARTICLES particles) that every GPU loading the library keeps until exit. The first
+   call with a device current looks up that array's address (cudaGetSymbolAddress); make it before any
+   stream capture. All calls share the array: calls that overlap on the GPU race and must be serialised.
+   Limits: at most VBD_NOALLOC_MAX_PARTICLES particles (else VBD_ERR_TOO_LARGE, nothing launched), at
+   most VBD_NOALLOC_MAX_CONTACT_SLOTS contacts per particle, static shapes with a fixed penalty
+   (avbd beta = 0, the reference default). Inputs are trusted like the reference kernels trust theirs. */
+int vbd_step_noalloc(const VbdModelDesc* model, const VbdRefAdjacency* adjacency, int32_t iterations,
+                     float friction_epsilon, float* q_in_dev, float* q_out_dev, const float* qd_in_dev,
+                     float* qd_out_dev, const float* particle_f_dev, const VbdContactsDesc* contacts, float dt,
+                     void* stream);
 
 /* ---------------------------------------------------------------- host-side model preparation */
 

@@ -18,6 +18,8 @@ VBD_ERR_CUDA = -2
 VBD_ERR_OUT_OF_MEMORY = -3
 VBD_ERR_UNSUPPORTED = -4
 VBD_ERR_EMPTY_COLORING = -5
+VBD_ERR_TOO_LARGE = -6
+VBD_NOALLOC_MAX_PARTICLES = 32768
 
 VBD_DEVERR_NONFINITE = 1
 VBD_DEVERR_CONTACT_OVERFLOW = 2
@@ -74,6 +76,10 @@ class VbdBodyState(C.Structure):
     _fields_ = [("body_q_dev", _vp), ("body_q_prev_dev", _vp), ("body_qd_dev", _vp)]
 
 
+class VbdRefAdjacency(C.Structure):
+    _fields_ = [("face_offsets_dev", _vp), ("faces_dev", _vp), ("edge_offsets_dev", _vp), ("edges_dev", _vp)]
+
+
 # every symbol the header declares, with its ctypes signature
 SIGNATURES = {
     "vbd_create": ([C.POINTER(VbdModelDesc), C.POINTER(VbdSolverParams), C.POINTER(_vp)], C.c_int),
@@ -98,6 +104,11 @@ SIGNATURES = {
         C.c_int,
     ),
     "vbd_build_adjacency": ([C.c_int32, C.c_int32, _ip, C.c_int32, _ip, _ip, _ip, _ip, _ip], C.c_int),
+    "vbd_step_noalloc": (
+        [C.POINTER(VbdModelDesc), C.POINTER(VbdRefAdjacency), C.c_int32, C.c_float, _vp, _vp, _vp, _vp, _vp,
+         C.POINTER(VbdContactsDesc), C.c_float, _vp],
+        C.c_int,
+    ),
     "vbd_soft_contacts": (
         [C.c_int32, _vp, _vp, _vp, C.c_int32, _ip, _fp, _fp, _fp, C.c_float, C.c_int32, _vp, _vp, _vp, _vp, _vp,
          _vp, _vp],
@@ -139,5 +150,6 @@ def check(rc: int, what: str):
         VBD_ERR_OUT_OF_MEMORY: "out of device memory",
         VBD_ERR_UNSUPPORTED: "unsupported",
         VBD_ERR_EMPTY_COLORING: "empty coloring",
+        VBD_ERR_TOO_LARGE: "model exceeds the no-allocation scratch",
     }
     raise VbdError(f"{what} failed: {names.get(rc, rc)} ({rc})")

@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
-SOURCES = ["vbd_b200.cu"]
+SOURCES = ["vbd_b200.cu", "vbd_noalloc.cu"]
 HEADERS = ["vbd_math.cuh", "vbd_elements.cuh", "vbd_kernels.cuh", "vbd_ell.cuh", "vbd_dual.cuh", "vbd_adjoint.cuh"]
 OUT = os.path.join(HERE, "libvbd_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
