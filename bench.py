@@ -119,6 +119,23 @@ def build_batch(seed: int, count: int):
     return top, sides
 
 
+def max_over_ranks(values, device=None):
+    """Element-wise max of per-rank timings (the multi-GPU time is the slowest rank's)."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()):
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def rank_seed(seed: int, rank: int) -> int:
+    """Each rank simulates its own batch of the same size (weak scaling, no data-path collective)."""
+    return seed + rank
+
+
 def bytes_per_vertex_iteration(V, T, E, contacts=True):
     """Algorithmic bytes of one colour sweep (92 V + 68 T + 64 E + 96 V with contacts) per vertex."""
     return (92.0 * V + 68.0 * T + 64.0 * E + (96.0 * V if contacts else 0.0)) / V
@@ -191,12 +208,23 @@ def run_ours(args):
     torch.cuda.set_device(dev)
 
     t0 = time.time()
-    builder, sides = build_batch(args.seed + rank, args.instances)
+    if args.tune:
+        # launch shape from the autotuner, timed on the batch's first instances (same size distribution)
+        from newton_chysx_b200 import autotune
+
+        sub, _ = build_batch(rank_seed(args.seed, rank), min(args.instances, args.tune_instances))
+        sub_model = sub.finalize(dev)
+        sub_model.soft_contact_ke, sub_model.soft_contact_kd, sub_model.soft_contact_mu = 1.0e3, 10.0, 0.5
+        shape = autotune.tune(sub_model, schedule="persistent", iterations=ITERATIONS, dt=DT)
+        del sub, sub_model
+    else:
+        shape = dict(schedule="persistent", lanes_per_vertex=args.lanes, block_size=args.block,
+                     positions_in_shared=args.shared, layout=args.layout, min_blocks_per_sm=args.occ)  # fmt: skip
+    tune_s = time.time() - t0
+    builder, sides = build_batch(rank_seed(args.seed, rank), args.instances)
     model = builder.finalize(dev)
     model.soft_contact_ke, model.soft_contact_kd, model.soft_contact_mu = 1.0e3, 10.0, 0.5
-    solver = nb.SolverVBD(model, iterations=ITERATIONS, schedule="persistent", lanes_per_vertex=args.lanes,
-                          block_size=args.block, positions_in_shared=args.shared, layout=args.layout,
-                          min_blocks_per_sm=args.occ)  # fmt: skip
+    solver = nb.SolverVBD(model, iterations=ITERATIONS, **shape)
     pipe = nb.CollisionPipeline(model, soft_contact_margin=0.01)
     contacts = pipe.contacts()
     setup_s = time.time() - t0
@@ -242,10 +270,7 @@ def run_ours(args):
         torch.cuda.synchronize()
     solve_ms = sum(a.elapsed_time(b) for a, b in ev)
     total_ms = ev0.elapsed_time(ev1)
-    if dist:
-        t = torch.tensor([solve_ms, total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        solve_ms, total_ms = float(t[0]), float(t[1])
+    solve_ms, total_ms = max_over_ranks([solve_ms, total_ms], device=dev)
     errors = solver.device_errors()
 
     vi_step = float(V) * ITERATIONS
@@ -280,11 +305,7 @@ def run_ours(args):
             oqd.copy_(states[1].particle_qd, non_blocking=True)
         e1.record()
         torch.cuda.synchronize()
-        e2e_ms = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([e2e_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t[0])
+        e2e_ms = max_over_ranks([e0.elapsed_time(e1)], device=dev)[0]
         e2e = {"value": world * vi_step * Ke / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 2 * hq.numel() * 4,
                "d2h_bytes_per_step": 2 * oq.numel() * 4, "steps": Ke}  # fmt: skip
 
@@ -316,7 +337,9 @@ def run_ours(args):
                 "block_size": solver.block_size,
                 "positions_in_shared_bytes": solver.shared_bytes,
                 "layout": solver.layout,
-                "min_blocks_per_sm": args.occ,
+                "launch_shape": shape,
+                "autotuned": bool(args.tune),
+                "tune_s": round(tune_s, 1),
                 "l2": "inputs larger than L2 (~10 GB working set), no flush",
                 "parallelism": f"instance sharding x{world} (no collective)",
                 "timed": "solve only (forward, iterations, velocity); contact generation outside the solve events",
@@ -591,8 +614,10 @@ def main():
     ap.add_argument("--lanes", type=int, default=0)
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--shared", choices=["auto", "on", "off"], default="auto")
-    ap.add_argument("--layout", choices=["auto", "ell", "csr"], default="auto")
+    ap.add_argument("--layout", choices=["auto", "ell16", "ell", "csr"], default="auto")
     ap.add_argument("--occ", type=int, default=0, help="resident 256-thread CTAs per SM the kernel is compiled for")
+    ap.add_argument("--no-tune", dest="tune", action="store_false", help="use the launch-shape flags, not the autotuner")
+    ap.add_argument("--tune-instances", type=int, default=1024)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -45,6 +45,8 @@ extern "C" {
 #define VBD_LAYOUT_AUTO 0
 #define VBD_LAYOUT_CSR 1  /* vertex -> element adjacency, element records gathered by id (any lanes/vertex) */
 #define VBD_LAYOUT_ELL 2  /* per-incidence stencil records in sweep order, slot-major (one lane/vertex) */
+#define VBD_LAYOUT_ELL16 3 /* the same with 16-bit instance-local vertex ids: 32-byte face and 16-byte hinge
+                              records (persistent schedule, instances below 65536 particles, no hinge damping) */
 
 typedef struct VbdModelDesc {
   int32_t particle_count; /* V */
@@ -99,7 +101,7 @@ typedef struct VbdSolverParams {
   int32_t positions_in_shared;  /* persistent schedule, FP32/MIXED: keep each instance's positions in
                                    shared memory during the sweep. 0 = when they fit, 1 = never,
                                    2 = required (VBD_ERR_UNSUPPORTED if they do not fit) */
-  int32_t layout;               /* VBD_LAYOUT_*; AUTO = ELL when lanes_per_vertex is 1 */
+  int32_t layout;               /* VBD_LAYOUT_*; AUTO = ELL16 where it applies, else ELL when lanes_per_vertex is 1 */
   int32_t min_blocks_per_sm;    /* ELL + persistent, FP32/MIXED: 2..4 compiles the kernel for that many
                                    resident CTAs of 256 threads per SM (fewer registers); 0 = none */
 } VbdSolverParams;

@@ -151,10 +151,12 @@ struct VbdSolver {
   int4* hinge_idx = nullptr;
   float2* hinge_prop = nullptr;
   float* hinge_kd = nullptr;
+  uint4 *ell16_faceA = nullptr, *ell16_faceB = nullptr, *ell16_hinge = nullptr;
   std::vector<int> ell_nf, ell_ne;
   std::vector<long long> ell_fbase, ell_ebase;
   long long ell_faces = 0, ell_hinges = 0;
   bool ell_face_damping = false, ell_hinge_damping = false;
+  std::vector<int> inst_start_of_vertex;  // first particle of each particle's instance
   // adjoint work buffers (allocated by the first vbd_adjoint_step)
   void* adj_work = nullptr;
   size_t adj_work_bytes = 0;
@@ -165,13 +167,20 @@ struct VbdSolver {
     void* ps[] = {tri_idx, tri_pose, tri_mat, edge_idx, edge_prop, face_off, face_adj, edge_off, edge_adj,
                   inst_order, inst_vstart, inst_cptr, color_ranges, color_verts, queue, pos, qprev, inertia,
                   slot_cnt, slots, c_k, c_ke, c_kd, c_mu, err, residual, range_nf, range_ne, range_fbase,
-                  range_ebase, face_nb, face_dm, face_mat, face_kd, hinge_idx, hinge_prop, hinge_kd, adj_work};
+                  range_ebase, face_nb, face_dm, face_mat, face_kd, hinge_idx, hinge_prop, hinge_kd, adj_work,
+                  ell16_faceA, ell16_faceB, ell16_hinge};
     for (void* p : ps)
       if (p) cudaFree(p);
   }
 };
 
 namespace {
+
+inline unsigned __float_as_uint_host(float f) {
+  unsigned u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
 
 template <typename T>
 void dfree(T*& p) {
@@ -280,8 +289,46 @@ int build_ell(VbdSolver* h) {
     }
   }
   if ((rc = upload_into(&h->range_nf, h->ell_nf)) || (rc = upload_into(&h->range_ne, h->ell_ne)) ||
-      (rc = upload_into(&h->range_fbase, h->ell_fbase)) || (rc = upload_into(&h->range_ebase, h->ell_ebase)) ||
-      (rc = upload_into(&h->face_nb, fnb)) || (rc = upload_into(&h->face_dm, fdm)) ||
+      (rc = upload_into(&h->range_fbase, h->ell_fbase)) || (rc = upload_into(&h->range_ebase, h->ell_ebase)))
+    return rc;
+  if (h->layout == VBD_LAYOUT_ELL16) {
+    // instance-local 16-bit ids: world_of each range's vertices is the instance of the range
+    std::vector<uint4> fa(static_cast<size_t>(nfaces)), fb(static_cast<size_t>(nfaces)), hr(static_cast<size_t>(nhinges));
+    for (int r = 0; r < R; ++r) {
+      const int a = h->ranges_host[r];
+      if (h->ranges_host[r + 1] == a) continue;
+      const int vs = h->inst_start_of_vertex[h->range_verts_host[a]];
+      const long long n = h->ranges_host[r + 1] - a;
+      for (long long s = 0; s < h->ell_nf[r]; ++s)
+        for (long long j = 0; j < n; ++j) {
+          const long long i = h->ell_fbase[r] + s * n + j;
+          const unsigned la = unsigned(fnb[i].x - vs), lb = unsigned(fnb[i].y - vs);
+          const float mk = fmat[i].x > 0.f || fmat[i].y > 0.f ? 1.f : 0.f;
+          fa[i] = make_uint4(mk > 0.f ? (la | (lb << 16)) : 0u, __float_as_uint_host(fmat[i].x),
+                             __float_as_uint_host(fmat[i].y), __float_as_uint_host(fdm[i].x));
+          fb[i] = make_uint4(__float_as_uint_host(fdm[i].y), __float_as_uint_host(fdm[i].z),
+                             __float_as_uint_host(fdm[i].w), __float_as_uint_host(fdamp ? fkd[i] : 0.f));
+        }
+      for (long long s = 0; s < h->ell_ne[r]; ++s)
+        for (long long j = 0; j < n; ++j) {
+          const long long i = h->ell_ebase[r] + s * n + j;
+          const int4 id = hidx[i];
+          const int role = int(unsigned(id.w) >> 30);
+          const int ids[4] = {id.x, id.y, id.z, id.w & 0x3fffffff};
+          unsigned o[3] = {0u, 0u, 0u};
+          for (int q = 0, k = 0; q < 4; ++q)
+            if (q != role) o[k++] = unsigned(ids[q] - vs);
+          const bool live = hprop[i].y > 0.f;
+          hr[i] = make_uint4(live ? (o[0] | (o[1] << 16)) : 0u, live ? (o[2] | (unsigned(role) << 16)) : 0u,
+                             __float_as_uint_host(hprop[i].x), __float_as_uint_host(hprop[i].y));
+        }
+    }
+    if ((rc = upload_into(&h->ell16_faceA, fa)) || (rc = upload_into(&h->ell16_faceB, fb)) ||
+        (rc = upload_into(&h->ell16_hinge, hr)))
+      return rc;
+    return VBD_OK;
+  }
+  if ((rc = upload_into(&h->face_nb, fnb)) || (rc = upload_into(&h->face_dm, fdm)) ||
       (rc = upload_into(&h->face_mat, fmat)) || (rc = upload_into(&h->hinge_idx, hidx)) ||
       (rc = upload_into(&h->hinge_prop, hprop)))
     return rc;
@@ -290,6 +337,18 @@ int build_ell(VbdSolver* h) {
   if (fdamp && (rc = upload_into(&h->face_kd, fkd))) return rc;
   if (hdamp && (rc = upload_into(&h->hinge_kd, hkd))) return rc;
   return VBD_OK;
+}
+
+Ell16View ell16_view(const VbdSolver* h) {
+  Ell16View e;
+  e.range_nf = h->range_nf;
+  e.range_ne = h->range_ne;
+  e.range_fbase = h->range_fbase;
+  e.range_ebase = h->range_ebase;
+  e.faceA = h->ell16_faceA;
+  e.faceB = h->ell16_faceB;
+  e.hinge = h->ell16_hinge;
+  return e;
 }
 
 EllView ell_view(const VbdSolver* h) {
@@ -463,6 +522,17 @@ void launch_persistent(int L, const StepCtx<R>& c, const PersistentPlan& p, int 
 }
 
 template <typename R, int MODE, bool SMEM>
+void launch_persistent_ell16(int occ, const StepCtx<R>& c, const PersistentPlan& p, const Ell16View& e, int grid,
+                             int block, size_t smem, cudaStream_t st) {
+  switch (occ) {
+    case 2: k_persistent_ell16<R, MODE, SMEM, 2><<<grid, block, smem, st>>>(c, p, e); break;
+    case 3: k_persistent_ell16<R, MODE, SMEM, 3><<<grid, block, smem, st>>>(c, p, e); break;
+    case 4: k_persistent_ell16<R, MODE, SMEM, 4><<<grid, block, smem, st>>>(c, p, e); break;
+    default: k_persistent_ell16<R, MODE, SMEM, 0><<<grid, block, smem, st>>>(c, p, e); break;
+  }
+}
+
+template <typename R, int MODE, bool SMEM>
 void launch_persistent_ell(int occ, const StepCtx<R>& c, const PersistentPlan& p, const EllView& e, int grid,
                            int block, size_t smem, cudaStream_t st) {
   switch (occ) {
@@ -536,7 +606,17 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
     }
     PersistentPlan p{h->W, h->inst_order, h->inst_vstart, h->inst_cptr, h->color_ranges, h->color_verts, h->queue,
                      iters};
-    if (h->layout == VBD_LAYOUT_ELL) {
+    if (h->layout == VBD_LAYOUT_ELL16) {
+      const Ell16View e = ell16_view(h);
+      if constexpr (std::is_same<R, float>::value) {
+        if (h->smem_bytes > 0)
+          launch_persistent_ell16<R, MODE, true>(h->occ, c, p, e, h->grid_persistent, h->block, h->smem_bytes, st);
+        else
+          launch_persistent_ell16<R, MODE, false>(h->occ, c, p, e, h->grid_persistent, h->block, 0, st);
+      } else {
+        launch_persistent_ell16<R, MODE, false>(0, c, p, e, h->grid_persistent, h->block, 0, st);
+      }
+    } else if (h->layout == VBD_LAYOUT_ELL) {
       const EllView e = ell_view(h);
       if constexpr (std::is_same<R, float>::value) {
         if (h->smem_bytes > 0)
@@ -575,6 +655,16 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
 }
 
 template <typename R, int MODE, bool SMEM>
+const void* persistent_ell16_fn(int occ) {
+  switch (occ) {
+    case 2: return (const void*)k_persistent_ell16<R, MODE, SMEM, 2>;
+    case 3: return (const void*)k_persistent_ell16<R, MODE, SMEM, 3>;
+    case 4: return (const void*)k_persistent_ell16<R, MODE, SMEM, 4>;
+    default: return (const void*)k_persistent_ell16<R, MODE, SMEM, 0>;
+  }
+}
+
+template <typename R, int MODE, bool SMEM>
 const void* persistent_ell_fn(int occ) {
   switch (occ) {
     case 2: return (const void*)k_persistent_ell<R, MODE, SMEM, 2>;
@@ -587,6 +677,12 @@ const void* persistent_ell_fn(int occ) {
 
 const void* persistent_kernel(VbdSolver* h) {
   const bool sm = h->smem_bytes > 0;
+  if (h->layout == VBD_LAYOUT_ELL16) {
+    if (h->precision == VBD_PRECISION_FP64) return persistent_ell16_fn<double, MODE_FP64, false>(0);
+    if (h->precision == VBD_PRECISION_MIXED)
+      return sm ? persistent_ell16_fn<float, MODE_MIXED, true>(h->occ) : persistent_ell16_fn<float, MODE_MIXED, false>(h->occ);
+    return sm ? persistent_ell16_fn<float, MODE_FP32, true>(h->occ) : persistent_ell16_fn<float, MODE_FP32, false>(h->occ);
+  }
   if (h->layout == VBD_LAYOUT_ELL) {
     if (h->precision == VBD_PRECISION_FP64) return persistent_ell_fn<double, MODE_FP64, false>(0);
     if (h->precision == VBD_PRECISION_MIXED)
@@ -848,20 +944,41 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
   }
   h->block = params->block_size ? params->block_size
                                 : (h->schedule == VBD_SCHEDULE_PERSISTENT ? (h->smem_bytes > 96 * 1024 ? 512 : 256) : 128);
-  // element data layout: stencil records (one thread per vertex) unless lanes per vertex > 1 asks for CSR
-  if (params->layout == VBD_LAYOUT_ELL && h->L != 1) return fail(VBD_ERR_INVALID_ARGUMENT);
-  h->layout = (params->layout == VBD_LAYOUT_CSR || h->L != 1) ? VBD_LAYOUT_CSR : VBD_LAYOUT_ELL;
-  if (h->layout == VBD_LAYOUT_ELL && h->schedule == VBD_SCHEDULE_PERSISTENT && h->block > 512)
+  // element data layout: stencil records (one thread per vertex) unless lanes per vertex > 1 asks for CSR;
+  // the compact 16-bit records when the persistent schedule runs instances below 65536 particles and no
+  // hinge carries damping
+  if ((params->layout == VBD_LAYOUT_ELL || params->layout == VBD_LAYOUT_ELL16) && h->L != 1)
+    return fail(VBD_ERR_INVALID_ARGUMENT);
+  bool any_hinge_damping = false;
+  {
+    std::vector<float> bp;
+    if (h->E && (rc = download(bp, m.edge_bending_properties_dev, size_t(2) * h->E))) return fail(rc);
+    for (int e = 0; e < h->E; ++e) any_hinge_damping |= bp[2 * e] > 0.f && bp[2 * e + 1] > 0.f;
+  }
+  const bool ell16_ok = h->schedule == VBD_SCHEDULE_PERSISTENT && h->max_inst_v < 65536 && !any_hinge_damping;
+  if (params->layout == VBD_LAYOUT_ELL16 && !ell16_ok) return fail(VBD_ERR_UNSUPPORTED);
+  if (params->layout == VBD_LAYOUT_CSR || h->L != 1)
+    h->layout = VBD_LAYOUT_CSR;
+  else if (params->layout == VBD_LAYOUT_ELL16 || (params->layout == VBD_LAYOUT_AUTO && ell16_ok))
+    h->layout = VBD_LAYOUT_ELL16;
+  else
+    h->layout = VBD_LAYOUT_ELL;
+  h->inst_start_of_vertex.assign(h->V, 0);
+  for (int w = 0; w < h->W; ++w)
+    for (int i = wstart[w]; i < wstart[w + 1]; ++i) h->inst_start_of_vertex[i] = wstart[w];
+  if ((h->layout == VBD_LAYOUT_ELL || h->layout == VBD_LAYOUT_ELL16) && h->schedule == VBD_SCHEDULE_PERSISTENT &&
+      h->block > 512)
     return fail(VBD_ERR_INVALID_ARGUMENT);
   if (params->min_blocks_per_sm != 0) {
-    if (params->min_blocks_per_sm < 2 || params->min_blocks_per_sm > 4 || h->layout != VBD_LAYOUT_ELL ||
+    if (params->min_blocks_per_sm < 2 || params->min_blocks_per_sm > 4 ||
+        (h->layout != VBD_LAYOUT_ELL && h->layout != VBD_LAYOUT_ELL16) ||
         h->schedule != VBD_SCHEDULE_PERSISTENT || h->precision == VBD_PRECISION_FP64 ||
         (params->block_size != 0 && params->block_size != 256))
       return fail(VBD_ERR_INVALID_ARGUMENT);
     h->occ = params->min_blocks_per_sm;
     h->block = 256;
   }
-  if (h->layout == VBD_LAYOUT_ELL) {
+  if (h->layout == VBD_LAYOUT_ELL || h->layout == VBD_LAYOUT_ELL16) {
     if (h->schedule == VBD_SCHEDULE_PERSISTENT) {
       h->range_verts_host = verts;
       h->ranges_host.clear();
@@ -884,7 +1001,7 @@ int vbd_refresh_model(VbdHandle h, void* stream) {
   if (!h) return VBD_ERR_INVALID_ARGUMENT;
   int rc = pack_model(h, (cudaStream_t)stream);
   if (rc) return rc;
-  if (h->layout == VBD_LAYOUT_ELL) {
+  if (h->layout == VBD_LAYOUT_ELL || h->layout == VBD_LAYOUT_ELL16) {
     if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return VBD_ERR_CUDA;
     return build_ell(h);
   }

@@ -8,15 +8,17 @@
 //                k = ke * rest_length, Hessian k dtheta dtheta^T). The reference forms all four
 //                dtheta/dx_k through 3x3 products of projected skew matrices
 //                (compute_normalized_vector_derivative / compute_angle_derivative, :1028-1054).
-//                Here the same derivative is evaluated in closed vector form:
-//                  P1 = I - n1 n1^T,  P2 = I - n2 n2^T,
-//                  w1 = cos * (n2 x e) - sin * n2,  w2 = cos * (n1 x e) + sin * n1,
-//                  dtheta/dx0 = -(e  x P1 w1) / |N1|
-//                  dtheta/dx1 = -(e  x P2 w2) / |N2|
-//                  dtheta/dx2 =  (x03 x P1 w1) / |N1| + (x13 x P2 w2) / |N2|
-//                  dtheta/dx3 = -(x02 x P1 w1) / |N1| - (x12 x P2 w2) / |N2|
-//                which follows from d(n_hat)^T w = -(1/|N|) a x (P w) for d(n_hat) = (1/|N|) P skew(a).
-//                Only the derivative of the vertex being solved is formed unless damping needs all four.
+//                Because the unit normals n1, n2 are orthogonal to the unit edge e and
+//                n2 = cos(theta) n1 + sin(theta) (e x n1), that expression reduces exactly to the classic
+//                dihedral gradient (Bridson et al. 2003, "Simulation of clothing with folds and
+//                wrinkles"), with N1 = x02 x x03, N2 = x13 x x12:
+//                  dtheta/dx0 = -|e| / |N1| n1
+//                  dtheta/dx1 = -|e| / |N2| n2
+//                  dtheta/dx2 =  (x03 . e) / |N1| n1 + (x13 . e) / |N2| n2
+//                  dtheta/dx3 = -(x02 . e) / |N1| n1 - (x12 . e) / |N2| n2
+//                i.e. alpha n1 + beta n2 with two scalars chosen by the vertex's role, the same
+//                instructions for every lane of a warp. Only the solved vertex's derivative is formed
+//                unless damping needs all four.
 //  * contact   - rigid_vbd_kernels.py:727-759, 891-934 (penalty, approach damping, IPC-smoothed
 //                isotropic friction).
 #pragma once
@@ -94,31 +96,32 @@ __host__ __device__ __forceinline__ void bending_add(int ord, const vec3<R> x[4]
   // |N1|, |N2|, |e| < 1e-6 (degenerate hinge): no contribution
   const R eps2 = R(1.0e-12);
   if (s1 < eps2 || s2 < eps2 || se < eps2) return;
-  const R il1 = vrsqrt(s1), il2 = vrsqrt(s2);
-  const vec3<R> n1 = N1 * il1, n2 = N2 * il2, eh = e * vrsqrt(se);
+  const R il1 = vrsqrt(s1), il2 = vrsqrt(s2), ile = vrsqrt(se);
+  const vec3<R> n1 = N1 * il1, n2 = N2 * il2, eh = e * ile;
   const R s = dot(cross(n1, n2), eh);
   const R c = dot(n1, n2);
   const R theta = vatan2(s, c);
   const R k = ke * rest_length;
   const R dE = k * (theta - rest_angle);
-  vec3<R> w1 = c * cross(n2, eh) - s * n2;
-  vec3<R> w2 = c * cross(n1, eh) + s * n1;
-  w1 = (w1 - n1 * dot(n1, w1)) * il1;  // P1 w1 / |N1|
-  w2 = (w2 - n2 * dot(n2, w2)) * il2;  // P2 w2 / |N2|
-  vec3<R> d;
-  if (ord == 0)
-    d = -cross(e, w1);
-  else if (ord == 1)
-    d = -cross(e, w2);
-  else if (ord == 2)
-    d = cross(x03, w1) + cross(x13, w2);
-  else
-    d = -(cross(x02, w1) + cross(x12, w2));
+  const R le = se * ile;  // |e|
+  // dtheta/dx_ord = alpha n1 + beta n2
+  R alpha, beta;
+  if (ord <= 1) {
+    alpha = ord == 0 ? -le * il1 : R(0);
+    beta = ord == 1 ? -le * il2 : R(0);
+  } else {
+    const vec3<R> a1 = ord == 2 ? x03 : -x02;
+    const vec3<R> a2 = ord == 2 ? x13 : -x12;
+    alpha = dot(a1, eh) * il1;
+    beta = dot(a2, eh) * il2;
+  }
+  const vec3<R> d = alpha * n1 + beta * n2;
   f = f + (-dE) * d;
   R hk = k;
   if (kd > R(0)) {
-    const vec3<R> d0 = -cross(e, w1), d1 = -cross(e, w2);
-    const vec3<R> d2 = cross(x03, w1) + cross(x13, w2), d3 = -(cross(x02, w1) + cross(x12, w2));
+    const vec3<R> d0 = (-le * il1) * n1, d1 = (-le * il2) * n2;
+    const vec3<R> d2 = (dot(x03, eh) * il1) * n1 + (dot(x13, eh) * il2) * n2;
+    const vec3<R> d3 = (-dot(x02, eh) * il1) * n1 - (dot(x12, eh) * il2) * n2;
     const R inv_dt = R(1) / dt;
     const R dth = (dot(d0, x[0] - xp[0]) + dot(d1, x[1] - xp[1]) + dot(d2, x[2] - xp[2]) + dot(d3, x[3] - xp[3])) *
                   inv_dt;

@@ -227,3 +227,176 @@ __global__ void __launch_bounds__(OCC ? 256 : 512, OCC ? OCC : 1) k_persistent_e
 }
 
 }  // namespace vbd
+
+namespace vbd {
+
+// ---------------------------------------------------------------------------------------------
+// Compact stencil records for instances of fewer than 65536 particles (persistent schedule):
+// vertex ids are 16-bit offsets from the instance's first particle, so that
+//   face  = 32 bytes in two 16-byte halves (two arrays, each read fully coalesced):
+//           A = (a | b << 16, mu A, lambda A, D'00)      B = (D'01, D'10, D'11, damping)
+//   hinge = 16 bytes: (i0 | i1 << 16, i2 | role << 16, rest angle, ke * rest length)
+//           where i0, i1, i2 are the hinge's other three vertices in (o0, o1, v0, v1) order and role
+//           (0..3) is the solved vertex's place among the four. Hinge damping is not stored: models
+//           with non-zero hinge damping use the 32-bit stencil layout.
+struct Ell16View {
+  const int* range_nf;
+  const int* range_ne;
+  const long long* range_fbase;
+  const long long* range_ebase;
+  const uint4* faceA;
+  const uint4* faceB;
+  const uint4* hinge;
+};
+
+template <typename R, int MODE, typename P>
+__device__ __forceinline__ void solve_ell16(const StepCtx<R>& c, const P& pos, const Ell16View& e, int r, int n, int j,
+                                            int v, int vs, int iteration) {
+  const pos4_t<R> in4 = c.inertia[v];
+  const R m = R(in4.w);
+  if (m == R(0)) return;
+  const vec3<R> x = pos.ld(v);
+  vec3<R> f = zero3<R>();
+  sym3<R> H = szero<R>();
+  const int nf = __ldg(e.range_nf + r), ne = __ldg(e.range_ne + r);
+  {
+    const long long b0 = __ldg(e.range_fbase + r) + j;
+    const uint4* pa = e.faceA + b0;
+    const uint4* pb = e.faceB + b0;
+    uint4 A_n = make_uint4(0u, 0u, 0u, 0u), B_n = make_uint4(0u, 0u, 0u, 0u);
+    if (nf > 0) {
+      A_n = __ldg(pa);
+      B_n = __ldg(pb);
+    }
+    for (int s = 0; s < nf; ++s) {
+      const uint4 A = A_n, B = B_n;
+      if (s + 1 < nf) {
+        pa += n;
+        pb += n;
+        A_n = __ldg(pa);
+        B_n = __ldg(pb);
+      }
+      const float muA = __uint_as_float(A.y), lmA = __uint_as_float(A.z);
+      if (!(muA > 0.f || lmA > 0.f)) continue;
+      const R pose[4] = {R(__uint_as_float(A.w)), R(__uint_as_float(B.x)), R(__uint_as_float(B.y)),
+                         R(__uint_as_float(B.z))};
+      const float kd = __uint_as_float(B.w);
+      const int ia = vs + int(A.x & 0xffffu), ib = vs + int(A.x >> 16);
+      vec3<R> xp[3];
+      if (kd > 0.f) {
+        xp[0] = ld3<R>(c.qprev[v]);
+        xp[1] = ld3<R>(c.qprev[ia]);
+        xp[2] = ld3<R>(c.qprev[ib]);
+      }
+      membrane_add<R>(0, x, pos.ld(ia), pos.ld(ib), pose, R(muA), R(lmA), R(kd), R(1), c.dt, xp, f, H);
+    }
+  }
+  {
+    const long long b0 = __ldg(e.range_ebase + r) + j;
+    const uint4* ph = e.hinge + b0;
+    uint4 h_n = make_uint4(0u, 0u, 0u, 0u);
+    if (ne > 0) h_n = __ldg(ph);
+    for (int s = 0; s < ne; ++s) {
+      const uint4 hh = h_n;
+      if (s + 1 < ne) {
+        ph += n;
+        h_n = __ldg(ph);
+      }
+      const float k = __uint_as_float(hh.w);
+      if (!(k > 0.f)) continue;
+      const int role = int((hh.y >> 16) & 3u);
+      const vec3<R> o0 = pos.ld(vs + int(hh.x & 0xffffu));
+      const vec3<R> o1 = pos.ld(vs + int(hh.x >> 16));
+      const vec3<R> o2 = pos.ld(vs + int(hh.y & 0xffffu));
+      // put the solved vertex back at its place among the four
+      vec3<R> xs[4];
+      xs[0] = role == 0 ? x : o0;
+      xs[1] = role == 0 ? o0 : (role == 1 ? x : o1);
+      xs[2] = role <= 1 ? o1 : (role == 2 ? x : o2);
+      xs[3] = role == 3 ? x : o2;
+      bending_add<R>(role, xs, R(__uint_as_float(hh.z)), R(1), R(k), R(0), c.dt, nullptr, f, H);
+    }
+  }
+  const R md = m * c.dt2r;
+  f = f + md * (ld3<R>(in4) - x);
+  H.xx += md;
+  H.yy += md;
+  H.zz += md;
+  if (c.has_contacts) contacts_add<R>(c, v, x, f, H);
+  if (MODE == MODE_MIXED && c.residual) {
+    const double r2 = double(f.x) * double(f.x) + double(f.y) * double(f.y) + double(f.z) * double(f.z);
+    atomicAdd(c.residual + 32 * iteration + (threadIdx.x & 31), r2);
+  }
+  vec3<R> dlt;
+  double det_used;
+  if (MODE == MODE_MIXED) {
+    const R hmax = vmax(vmax(vmax(vabs(H.xx), vabs(H.yy)), vmax(vabs(H.zz), vabs(H.xy))), vmax(vabs(H.xz), vabs(H.yz)));
+    const R d = sdet(H);
+    if (!(vabs(d) >= R(c.fp64_thr) * hmax * hmax * hmax)) {
+      const sym3<double> Hd = {double(H.xx), double(H.yy), double(H.zz), double(H.xy), double(H.xz), double(H.yz)};
+      const vec3<double> fd = {double(f.x), double(f.y), double(f.z)};
+      det_used = sdet(Hd);
+      const vec3<double> rr = sadj_mul(Hd, fd) * (1.0 / det_used);
+      dlt = {R(rr.x), R(rr.y), R(rr.z)};
+    } else {
+      det_used = double(d);
+      dlt = sadj_mul(H, f) * (R(1) / d);
+    }
+  } else {
+    const R d = sdet(H);
+    det_used = double(d);
+    dlt = sadj_mul(H, f) * (R(1) / d);
+  }
+  if (!isfinite(det_used)) {
+    set_err(c.err, 1);
+    return;
+  }
+  if (!(fabs(det_used) > 1e-8)) {
+    set_err(c.err, 4);
+    return;
+  }
+  const vec3<R> xn = x + dlt;
+  if (!(isfinite(double(xn.x)) && isfinite(double(xn.y)) && isfinite(double(xn.z)))) {
+    set_err(c.err, 1);
+    return;
+  }
+  pos.st(v, xn);
+}
+
+template <typename R, int MODE, bool SMEM, int OCC>
+__global__ void __launch_bounds__(OCC ? 256 : 512, OCC ? OCC : 1) k_persistent_ell16(StepCtx<R> c, PersistentPlan p,
+                                                                                    Ell16View e) {
+  extern __shared__ float s_pos[];
+  __shared__ int s_item;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = atomicAdd(p.queue, 1);
+    __syncthreads();
+    const int q = s_item;
+    if (q >= p.W) return;
+    const int w = __ldg(p.inst_order + q);
+    const int vs = __ldg(p.inst_vstart + w), ve = __ldg(p.inst_vstart + w + 1);
+    using Pos = typename std::conditional<SMEM, SmemPos, GlobalPos<R>>::type;
+    Pos pos;
+    if constexpr (SMEM) {
+      pos = SmemPos{s_pos, vs};
+    } else {
+      pos = GlobalPos<R>{c.pos};
+    }
+    for (int i = vs + threadIdx.x; i < ve; i += blockDim.x) forward_particle(c, pos, i);
+    __syncthreads();
+    const int cb = __ldg(p.inst_cptr + w), ce = __ldg(p.inst_cptr + w + 1);
+    for (int it = 0; it < p.iterations; ++it) {
+      for (int col = cb; col + 1 < ce; ++col) {
+        const int a = __ldg(p.color_ranges + col), b = __ldg(p.color_ranges + col + 1);
+        const int r = col - w;
+        for (int j = threadIdx.x; j < b - a; j += blockDim.x)
+          solve_ell16<R, MODE>(c, pos, e, r, b - a, j, __ldg(p.color_verts + a + j), vs, it);
+        __syncthreads();
+      }
+    }
+    for (int i = vs + threadIdx.x; i < ve; i += blockDim.x) finalize_particle(c, pos, i);
+  }
+}
+
+}  // namespace vbd
