@@ -17,6 +17,15 @@ unchanged:
   ``_compute_body_particle_contact_force :727-759``, ``_eval_body_particle_contact :762-834``,
   ``compute_projected_isotropic_friction :891-934``, ``init_body_particle_contacts :2318-2361``,
   ``update_duals_body_particle_contacts :3755-3799``;
+* self-contact: ``particle_vbd_kernels.py`` ``evaluate_self_contact_force_norm :1193-1222``,
+  ``damp_collision :1225-1238``, ``evaluate_edge_edge_contact_2_vertices :1371-1506``,
+  ``evaluate_vertex_triangle_collision_force_hessian_4_vertices :1599-1745``, ``compute_friction :1748-1779``,
+  ``accumulate_self_contact_force_and_hessian :1930-2071``, the n-ring filters ``:2074-2255``, the
+  division planes and ``planar_truncation_t :2475-2742``, ``apply_planar_truncation_parallel_by_collision
+  :2744-2874``; ``geometry/kernels.py`` ``triangle_closest_point :64-128``, the detection kernels
+  ``:1229-1497``; ``math/__init__.py`` ``orthonormal_basis``; ``geometry/broad_phase_common.py``
+  ``binary_search``. ``SelfContactRef`` mirrors ``TriMeshCollisionDetector`` (``tri_mesh_collision.py:91-413``)
+  with the shim's brute-force box query standing in for ``wp.Bvh``;
 * ``newton/_src/sim/builder.py``: ``add_triangles :7716-7826``, ``add_edges :7966-8061``,
   ``add_cloth_grid :8063-8186``, ``add_cloth_mesh :8188-8341``; ``newton/_src/utils/mesh.py``:
   ``MeshAdjacency :183-262``.
@@ -52,6 +61,24 @@ class ParticleFlags:
     ACTIVE = 1 << 0
 
 
+class _BvhLoopRewrite(ast.NodeTransformer):
+    """``while wp.bvh_query_next(query, i): ...`` -> ``for i in query: ...``.
+
+    Warp's ``bvh_query_next`` writes the next primitive index through its second argument, which
+    plain Python cannot do; the shim's ``bvh_query_aabb`` returns the list of hits instead. The loop
+    body (including its ``continue`` statements) is unchanged."""
+
+    def visit_While(self, node):
+        self.generic_visit(node)
+        t = node.test
+        if isinstance(t, ast.Call) and isinstance(t.func, ast.Attribute) and t.func.attr == "bvh_query_next":
+            query, index = t.args
+            loop = ast.For(target=ast.Name(id=index.id, ctx=ast.Store()), iter=query, body=node.body, orelse=[],
+                           type_comment=None)  # fmt: skip
+            return ast.copy_location(loop, node)
+        return node
+
+
 def _lift(path: str, names: set[str], ns: dict, classes: dict[str, set[str]] | None = None):
     """Execute the named top-level functions (and selected class methods) of ``path`` in ``ns``."""
     with open(path) as f:
@@ -71,9 +98,14 @@ def _lift(path: str, names: set[str], ns: dict, classes: dict[str, set[str]] | N
     found = set()
     for node in tree.body:
         if isinstance(node, ast.FunctionDef) and node.name in names:
-            mod = ast.Module(body=[strip(node)], type_ignores=[])
+            fn = ast.fix_missing_locations(_BvhLoopRewrite().visit(strip(node)))
+            mod = ast.Module(body=[fn], type_ignores=[])
             exec(compile(mod, path, "exec"), ns)
             found.add(node.name)
+        if isinstance(node, ast.Assign) and len(node.targets) == 1 and isinstance(node.targets[0], ast.Name):
+            if node.targets[0].id in names:  # module constants such as ``X = wp.constant(0)``
+                exec(compile(ast.Module(body=[node], type_ignores=[]), path, "exec"), ns)
+                found.add(node.targets[0].id)
         if classes and isinstance(node, ast.ClassDef) and node.name in classes:
             wanted = classes[node.name]
             if wanted == {"*"}:
@@ -147,6 +179,55 @@ def load_reference(ref: str) -> dict:
             "apply_truncation_ts",
             "accumulate_particle_body_contact_force_and_hessian",
             "solve_elasticity",
+        },
+        ns,
+    )
+    # self-contact (particle_vbd_kernels.py:1193-2255, 2475-2874) and its geometry helpers
+    ns["mat32"] = wp.mat32
+    _lift(os.path.join(ref, "newton/_src/math/__init__.py"), {"orthonormal_basis"}, ns)
+    _lift(os.path.join(ref, "newton/_src/geometry/broad_phase_common.py"), {"binary_search"}, ns)
+    _lift(
+        os.path.join(ref, "newton/_src/geometry/kernels.py"),
+        {
+            "triangle_closest_point",
+            "vertex_adjacent_to_triangle",
+            "vertex_triangle_collision_detection_kernel",
+            "edge_colliding_edges_detection_kernel",
+            "TRI_CONTACT_FEATURE_VERTEX_A",
+            "TRI_CONTACT_FEATURE_VERTEX_B",
+            "TRI_CONTACT_FEATURE_VERTEX_C",
+            "TRI_CONTACT_FEATURE_EDGE_AB",
+            "TRI_CONTACT_FEATURE_EDGE_AC",
+            "TRI_CONTACT_FEATURE_EDGE_BC",
+            "TRI_CONTACT_FEATURE_FACE_INTERIOR",
+            "VERTEX_COLLISION_BUFFER_OVERFLOW_INDEX",
+            "TRI_COLLISION_BUFFER_OVERFLOW_INDEX",
+            "EDGE_COLLISION_BUFFER_OVERFLOW_INDEX",
+        },
+        ns,
+    )
+    _lift(
+        os.path.join(vbd, "particle_vbd_kernels.py"),
+        {
+            "NUM_THREADS_PER_COLLISION_PRIMITIVE",
+            "evaluate_self_contact_force_norm",
+            "damp_collision",
+            "evaluate_edge_edge_contact_2_vertices",
+            "evaluate_vertex_triangle_collision_force_hessian_4_vertices",
+            "compute_friction",
+            "accumulate_self_contact_force_and_hessian",
+            "_csr_row",
+            "set_to_csr",
+            "one_ring_vertices",
+            "leq_n_ring_vertices",
+            "build_vertex_n_ring_tris_collision_filter",
+            "build_edge_n_ring_edge_collision_filter",
+            "segment_plane_intersects",
+            "create_vertex_triangle_division_plane_closest_pt",
+            "robust_edge_pair_normal",
+            "create_edge_edge_division_plane_closest_pt",
+            "planar_truncation_t",
+            "apply_planar_truncation_parallel_by_collision",
         },
         ns,
     )
@@ -323,8 +404,82 @@ class RefScene:
         self.particle_colors = wp.scalar_array(colors, int)
 
 
-def ref_step(sc: RefScene, q_in, qd_in, f_ext, contacts, dt, iterations, friction_epsilon=1e-2, beta=0.0):
-    """One ``SolverVBD.step`` without self-contact and without rigid bodies (static shapes only)."""
+class SelfContactRef:
+    """Self-contact state of ``SolverVBD`` (``solver_vbd.py:489-526, 1339-1404``) and its
+    ``TriMeshCollisionDetector`` (``tri_mesh_collision.py:91-413``) for a shim run."""
+
+    def __init__(self, ns, sc: RefScene, *, radius, margin, relaxation=0.85, vertex_buffer=32, edge_buffer=64,
+                 interval=0, ee_eps=1e-5, ring=2, rest_exclusion=0.0):  # fmt: skip
+        self.ns, self.sc = ns, sc
+        m = sc.m
+        self.V, self.T, self.E = sc.n, len(m["tri_indices"]), len(m["edge_indices"])
+        self.radius, self.margin, self.relaxation = radius, margin, relaxation
+        self.vb, self.eb, self.interval, self.ee_eps = vertex_buffer, edge_buffer, interval, ee_eps
+        self.ring, self.rest_exclusion = ring, rest_exclusion
+        f_off, f_adj, e_off, e_adj = sc.adjacency_np
+        self.vt_filter = self.ee_filter = (None, None)
+        if ring >= 2:  # _compute_particle_contact_filtering_list (solver_vbd.py:1339-1404)
+            vt_sets = ns["build_vertex_n_ring_tris_collision_filter"](ring, self.V, m["edge_indices"], e_adj, e_off, f_adj,
+                                                                      f_off)  # fmt: skip
+            ee_sets = ns["build_edge_n_ring_edge_collision_filter"](ring, m["edge_indices"], e_adj, e_off)
+            self.vt_filter = ns["set_to_csr"](vt_sets)
+            self.ee_filter = ns["set_to_csr"](ee_sets)
+        self.rest_q = wp.vec_array(m["particle_q"])  # particle_q_rest = model.particle_q
+        self.vt_offsets = wp.scalar_array(np.arange(self.V + 1) * vertex_buffer, int)
+        self.vt_sizes = wp.scalar_array(np.full(self.V, vertex_buffer), int)
+        self.ee_offsets = wp.scalar_array(np.arange(self.E + 1) * edge_buffer, int)
+        self.ee_sizes = wp.scalar_array(np.full(self.E, edge_buffer), int)
+        self.launch_size = max(self.V, self.E) * ns["NUM_THREADS_PER_COLLISION_PRIMITIVE"]
+
+    def detect(self, pos):
+        """``_collision_detection_penetration_free`` after its position copy (solver_vbd.py:2834-2850)."""
+        ns, m = self.ns, self.sc.m
+        P = wp.to_numpy(pos)
+        tri, edg = m["tri_indices"], m["edge_indices"]
+        bvh_tris = wp.Bvh(np.minimum(np.minimum(P[tri[:, 0]], P[tri[:, 1]]), P[tri[:, 2]]),
+                          np.maximum(np.maximum(P[tri[:, 0]], P[tri[:, 1]]), P[tri[:, 2]]))  # fmt: skip
+        bvh_edges = wp.Bvh(np.minimum(P[edg[:, 2]], P[edg[:, 3]]), np.maximum(P[edg[:, 2]], P[edg[:, 3]]))
+        self.resize_flags = wp.scalar_array(np.zeros(4), int)
+        self.vt = wp.scalar_array(-np.ones(2 * self.V * self.vb), int)
+        self.vt_count = wp.scalar_array(np.zeros(self.V), int)
+        self.vt_min = wp.scalar_array(np.zeros(self.V))
+        tri_min = wp.scalar_array(np.full(self.T, self.margin))
+        vf, vfo = self.vt_filter
+        wp.launch(
+            ns["vertex_triangle_collision_detection_kernel"], self.V, self.margin, self.rest_exclusion, bvh_tris, pos,
+            self.sc.tri_indices, self.vt_offsets, self.vt_sizes, None, None,
+            None if vf is None else wp.scalar_array(vf, int), None if vfo is None else wp.scalar_array(vfo, int),
+            self.rest_q, self.vt, self.vt_count, self.vt_min, None, None, tri_min, self.resize_flags,
+        )  # fmt: skip
+        self.ee = wp.scalar_array(-np.ones(2 * self.E * self.eb), int)
+        self.ee_count = wp.scalar_array(np.zeros(self.E), int)
+        self.ee_min = wp.scalar_array(np.zeros(self.E))
+        ef, efo = self.ee_filter
+        wp.launch(
+            ns["edge_colliding_edges_detection_kernel"], self.E, self.margin, self.rest_exclusion, bvh_edges, pos,
+            self.sc.edge_indices, self.ee_offsets, self.ee_sizes, self.ee_eps,
+            None if ef is None else wp.scalar_array(ef, int), None if efo is None else wp.scalar_array(efo, int),
+            self.rest_q, self.ee, self.ee_count, self.ee_min, self.resize_flags,
+        )  # fmt: skip
+        self.info = [types.SimpleNamespace(
+            vertex_colliding_triangles=self.vt, vertex_colliding_triangles_offsets=self.vt_offsets,
+            vertex_colliding_triangles_buffer_sizes=self.vt_sizes, edge_colliding_edges=self.ee,
+            edge_colliding_edges_offsets=self.ee_offsets, edge_colliding_edges_buffer_sizes=self.ee_sizes,
+        )]  # fmt: skip
+
+    def record(self):
+        return {
+            "vt": np.array(self.vt.items, dtype=np.int32), "vt_count": np.array(self.vt_count.items, dtype=np.int32),
+            "vt_min": np.array(self.vt_min.items), "ee": np.array(self.ee.items, dtype=np.int32),
+            "ee_count": np.array(self.ee_count.items, dtype=np.int32), "ee_min": np.array(self.ee_min.items),
+            "resize_flags": np.array(self.resize_flags.items, dtype=np.int32),
+        }  # fmt: skip
+
+
+def ref_step(sc: RefScene, q_in, qd_in, f_ext, contacts, dt, iterations, friction_epsilon=1e-2, beta=0.0, selfc=None,
+             trace=None):  # fmt: skip
+    """One ``SolverVBD.step`` without rigid bodies (static shapes only); ``selfc`` turns self-contact on.
+    ``trace`` (a list) receives the collision buffers of every detection."""
     ns = sc.ns
     n = sc.n
     state_in_q = wp.vec_array(q_in)
@@ -358,15 +513,33 @@ def ref_step(sc: RefScene, q_in, qd_in, f_ext, contacts, dt, iterations, frictio
     # _initialize_particles (solver_vbd.py:1731-1766)
     pos_prev_cd = wp.vec_array(wp.to_numpy(state_in_q))
     disp = wp.vec_array(np.zeros((n, 3)))
+
+    def detect():
+        pos_prev_cd.items = [wp.Vec(x.a) for x in state_in_q.items]
+        disp.items = [wp.vec3() for _ in range(n)]
+        selfc.detect(state_in_q)
+        if trace is not None:
+            trace.append(selfc.record())
+
+    if selfc is not None:
+        detect()
     wp.launch(
         ns["forward_step"], n, dt, sc.gravity, q_prev, state_in_q, state_in_qd, sc.inv_mass, particle_f,
         sc.flags, inertia, disp,
     )  # fmt: skip
     ts = wp.scalar_array(np.ones(n))
 
-    def truncate():
+    def truncate():  # _penetration_free_truncation (solver_vbd.py:1669-1729)
         ts.items = [1.0] * n
-        wp.launch(ns["apply_truncation_ts"], n, pos_prev_cd, disp, ts, wp.inf, disp, state_in_q)
+        if selfc is None:
+            wp.launch(ns["apply_truncation_ts"], n, pos_prev_cd, disp, ts, wp.inf, disp, state_in_q)
+            return
+        wp.launch(
+            ns["apply_planar_truncation_parallel_by_collision"], selfc.launch_size, pos_prev_cd, disp, sc.tri_indices,
+            sc.edge_indices, selfc.info, selfc.ee_eps, selfc.relaxation, ts,
+        )  # fmt: skip
+        wp.launch(ns["apply_truncation_ts"], n, pos_prev_cd, disp, ts, selfc.margin * selfc.relaxation * 0.5, disp,
+                  state_in_q)  # fmt: skip
 
     truncate()
     for _it in range(iterations):
@@ -375,6 +548,9 @@ def ref_step(sc: RefScene, q_in, qd_in, f_ext, contacts, dt, iterations, frictio
             ns["update_duals_body_particle_contacts"], cmax, cnt, c_particle, c_shape, c_body_pos, c_normal,
             state_in_q, sc.radius, sc.shape_body, sc.empty, mat_ke, beta, pen_k,
         )  # fmt: skip
+        # _solve_particle_iteration (solver_vbd.py:2151-2337)
+        if selfc is not None and ((selfc.interval == 0 and _it == 0) or (selfc.interval >= 1 and _it % selfc.interval == 0)):
+            detect()
         forces = wp.vec_array(np.zeros((n, 3)))
         hessians = wp.mat33_array(np.zeros((n, 3, 3)))
         for color in range(len(sc.groups)):
@@ -384,6 +560,12 @@ def ref_step(sc: RefScene, q_in, qd_in, f_ext, contacts, dt, iterations, frictio
                 sc.shape_mu, sc.shape_body, sc.empty, None, sc.empty, sc.empty, c_shape, c_body_pos, c_body_vel,
                 c_normal, forces, hessians,
             )  # fmt: skip
+            if selfc is not None:
+                wp.launch(
+                    ns["accumulate_self_contact_force_and_hessian"], selfc.launch_size, dt, color, q_prev, state_in_q,
+                    sc.particle_colors, sc.tri_indices, sc.edge_indices, selfc.info, selfc.radius, sc.soft_ke,
+                    sc.soft_kd, sc.soft_mu, friction_epsilon, selfc.ee_eps, forces, hessians,
+                )  # fmt: skip
             group = wp.scalar_array(sc.groups[color], int)
             wp.launch(
                 ns["solve_elasticity"], len(sc.groups[color]), dt, group, q_prev, state_in_q, sc.mass, inertia,
@@ -427,15 +609,21 @@ def scene_grid(ns, *, dim, cell, pos, rot, vel, mass, mu, lam, tri_kd, edge_ke, 
 
 
 def run_scene(ns, name, b: FakeBuilder, *, gravity, soft, shapes, contact_fn, dt, iterations, substeps, seed, beta=0.0,
-              friction_epsilon=1e-2, f_ext_scale=0.0):  # fmt: skip
+              friction_epsilon=1e-2, f_ext_scale=0.0, self_contact=None, q_start=None, qd_start=None):  # fmt: skip
     m = b.arrays()
     colors, groups = greedy_coloring(len(m["particle_q"]), m["tri_indices"], m["edge_indices"], m["edge_bending_properties"])
     sc = RefScene(ns, m, groups, colors, gravity, soft, shapes)
+    selfc = None if self_contact is None else SelfContactRef(ns, sc, **self_contact)
     n = sc.n
     rng = np.random.default_rng(seed)
-    q = m["particle_q"].copy()
-    qd = m["particle_qd"].copy()
+    q = m["particle_q"].copy() if q_start is None else np.asarray(q_start, dtype=np.float64).copy()
+    qd = m["particle_qd"].copy() if qd_start is None else np.asarray(qd_start, dtype=np.float64).copy()
     out = {f"model_{k}": v for k, v in m.items()}
+    if selfc is not None:
+        out.update({f"sc_{k}": np.float64(v) for k, v in self_contact.items()})
+        for key, (flat, offs) in (("vt_filter", selfc.vt_filter), ("ee_filter", selfc.ee_filter)):
+            if flat is not None:
+                out[f"sc_{key}"], out[f"sc_{key}_offsets"] = flat.astype(np.int32), offs.astype(np.int32)
     f_off, f_adj, e_off, e_adj = sc.adjacency_np
     out.update(
         adj_face_offsets=f_off.astype(np.int32), adj_faces=f_adj.astype(np.int32),
@@ -454,8 +642,17 @@ def run_scene(ns, name, b: FakeBuilder, *, gravity, soft, shapes, contact_fn, dt
         out[f"s{s}_q_in"], out[f"s{s}_qd_in"], out[f"s{s}_f_ext"] = q.copy(), qd.copy(), f_ext
         out[f"s{s}_contact_count"], out[f"s{s}_contact_particle"], out[f"s{s}_contact_shape"] = cnt, cp, cs
         out[f"s{s}_contact_body_pos"], out[f"s{s}_contact_body_vel"], out[f"s{s}_contact_normal"] = cbp, cbv, cn
-        q_in_after, q_out, qd_out = ref_step(sc, q, qd, f_ext, contacts, dt, iterations, friction_epsilon, beta)
+        trace = []
+        q_in_after, q_out, qd_out = ref_step(sc, q, qd, f_ext, contacts, dt, iterations, friction_epsilon, beta, selfc,
+                                             trace)  # fmt: skip
         out[f"s{s}_q_in_after"], out[f"s{s}_q_out"], out[f"s{s}_qd_out"] = q_in_after, q_out, qd_out
+        for k, rec in enumerate(trace):  # collision buffers of each detection of this substep
+            for key, val in rec.items():
+                out[f"s{s}_cd{k}_{key}"] = val
+        if trace:
+            nvt = sum(int(min(c, selfc.vb)) for c in trace[0]["vt_count"])
+            nee = sum(int(min(c, selfc.eb)) for c in trace[0]["ee_count"])
+            print(f"  {name}: substep {s} detections={len(trace)} vt pairs={nvt} ee pairs={nee}")
         q, qd = q_out, qd_out
         print(f"  {name}: substep {s} contacts={len(contacts)} |dq|max={np.abs(q_out - out[f's{s}_q_in']).max():.3e}")
     return out
@@ -509,6 +706,73 @@ def element_cases(ns, seed=7):
         f, H = ns["_compute_body_particle_contact_force"](pen, wp.vec3(n), wp.vec3(rel), ke, kd, mu, eps, dt)
         con.append(np.concatenate([[pen], n, rel, [ke, kd, mu, eps, dt], f.a, H.a.ravel()]))
     return {"membrane": np.array(mem), "bending": np.array(bend), "contact": np.array(con)}
+
+
+def selfcontact_cases(ns, seed=11):
+    """Per-pair goldens of the self-contact terms and of the division-plane truncation."""
+    rng = np.random.default_rng(seed)
+    radius, ke, kd, mu, eps, dt = 0.02, 1.0e4, 1.0e-3, 0.4, 1.0e-2, 1.0 / 600.0
+    vt, ee, vtp, eep, cp = [], [], [], [], []
+    for i in range(96):
+        a, b, c = rng.normal(scale=0.05, size=(3, 3))
+        n = np.cross(b - a, c - a)
+        n /= np.linalg.norm(n)
+        w = rng.dirichlet([1.0, 1.0, 1.0]) if i % 3 else rng.uniform(-0.5, 1.2, size=3)
+        w = w / w.sum()
+        # distances covering the quadratic (< d_min), log-barrier (< r/2), linear (< r) and no-contact regions
+        d = [5e-6, 0.004, 0.013, 0.025][i % 4] * (1.0 if i % 8 < 4 else -1.0)
+        p = w[0] * a + w[1] * b + w[2] * c + n * d
+        X = np.stack([a, b, c, p])
+        Xa = X + rng.normal(scale=[1e-3, 1e-5, 0.0][i % 3], size=(4, 3))
+        res = ns["evaluate_vertex_triangle_collision_force_hessian_4_vertices"](
+            3, 0, wp.vec_array(X), wp.vec_array(Xa), wp.array2d([[0, 1, 2]], int), radius, ke, kd, mu, eps, dt)
+        fs = np.concatenate([np.asarray(res[1 + k].a) for k in range(4)])
+        hs = np.concatenate([np.asarray(res[5 + k].a).ravel() for k in range(4)])
+        vt.append(np.concatenate([X.ravel(), Xa.ravel(), [float(res[0])], fs, hs]))
+        cpt, bary, feat = ns["triangle_closest_point"](wp.vec3(a), wp.vec3(b), wp.vec3(c), wp.vec3(p))
+        cp.append(np.concatenate([X.ravel(), cpt.a, bary.a, [feat]]))
+        disp = rng.normal(scale=0.01, size=(4, 3))
+        dummy, nrm, dpt = ns["create_vertex_triangle_division_plane_closest_pt"](
+            wp.vec3(p), wp.vec3(disp[3]), wp.vec3(a), wp.vec3(disp[0]), wp.vec3(b), wp.vec3(disp[1]), wp.vec3(c),
+            wp.vec3(disp[2]))  # fmt: skip
+        ts = [ns["planar_truncation_t"](wp.vec3(x), wp.vec3(dx), nrm, dpt, 1e-5, 0.85)
+              for x, dx in ((p, disp[3]), (a, disp[0]), (b, disp[1]), (c, disp[2]))]  # fmt: skip
+        vtp.append(np.concatenate([X.ravel(), disp.ravel(), [float(x) for x in dummy], nrm.a, dpt.a, ts]))
+    for i in range(96):
+        p1, q1 = rng.normal(scale=0.05, size=(2, 3))
+        u = rng.normal(size=3)
+        u -= u.dot(q1 - p1) * (q1 - p1) / np.dot(q1 - p1, q1 - p1)
+        u /= np.linalg.norm(u)
+        s0, t0 = rng.uniform(-0.3, 1.3, size=2)
+        d = [5e-6, 0.004, 0.013, 0.025][i % 4]
+        dir2 = rng.normal(size=3)
+        p2c = p1 + (q1 - p1) * s0 + u * d
+        p2 = p2c - dir2 * 0.05 * t0
+        q2 = p2 + dir2 * 0.05
+        X = np.stack([p1, q1, p2, q2])
+        Xa = X + rng.normal(scale=[1e-3, 1e-5, 0.0][i % 3], size=(4, 3))
+        edges = wp.array2d([[-1, -1, 0, 1], [-1, -1, 2, 3]], int)
+        res = ns["evaluate_edge_edge_contact_2_vertices"](0, 1, wp.vec_array(X), wp.vec_array(Xa), edges, radius, ke, kd,
+                                                          mu, eps, dt, 1e-5)  # fmt: skip
+        st = wp.closest_point_edge_edge(wp.vec3(p1), wp.vec3(q1), wp.vec3(p2), wp.vec3(q2), 1e-5)
+        ee.append(np.concatenate([X.ravel(), Xa.ravel(), [float(res[0])], res[1].a, res[2].a, res[3].a.ravel(),
+                                  res[4].a.ravel(), st.a]))  # fmt: skip
+        disp = rng.normal(scale=0.01, size=(4, 3))
+        dummy, nrm, dpt = ns["create_edge_edge_division_plane_closest_pt"](
+            wp.vec3(p1), wp.vec3(disp[0]), wp.vec3(q1), wp.vec3(disp[1]), wp.vec3(p2), wp.vec3(disp[2]), wp.vec3(q2),
+            wp.vec3(disp[3]))  # fmt: skip
+        ts = [ns["planar_truncation_t"](wp.vec3(X[k]), wp.vec3(disp[k]), nrm, dpt, 1e-5, 0.85) for k in range(4)]
+        eep.append(np.concatenate([X.ravel(), disp.ravel(), [float(x) for x in dummy], nrm.a, dpt.a, ts]))
+    norm = []
+    for dis in np.concatenate([np.geomspace(1e-7, 0.03, 40), [1e-5, 0.01, 0.02]]):
+        dEdD, d2E = ns["evaluate_self_contact_force_norm"](float(dis), radius, ke)
+        norm.append([dis, dEdD, d2E])
+    return {"vt": np.array(vt), "ee": np.array(ee), "vt_plane": np.array(vtp), "ee_plane": np.array(eep),
+            "closest": np.array(cp), "norm": np.array(norm)}  # fmt: skip
+
+
+def rot_z(deg):
+    return wp.quat_from_axis_angle(wp.vec3(0.0, 0.0, 1.0), math.radians(deg))
 
 
 def main():
@@ -567,6 +831,59 @@ def main():
         contact_fn=None, dt=1.0 / 600.0, iterations=5, substeps=3, seed=3,
     )  # fmt: skip
     np.savez_compressed(os.path.join(args.out, "step_complex_rest_angle.npz"), **out)
+
+    np.savez_compressed(os.path.join(args.out, "selfcontact_elements.npz"), **selfcontact_cases(ns))
+    print("selfcontact_elements.npz written")
+
+    # Self-contact: a sheet pinned at its corners and a second sheet, turned by 17 degrees about z,
+    # falling onto it from 15 mm. Vertex noise of 2 mm keeps edge pairs away from the parallel case.
+    b = FakeBuilder(ns)
+    mass = 0.2 * 0.01
+    b.add_cloth_grid(
+        pos=wp.vec3(-0.3, -0.3, 0.0), rot=wp.quat_identity(), vel=wp.vec3(0.0, 0.0, 0.0), dim_x=6, dim_y=6,
+        cell_x=0.1, cell_y=0.1, mass=mass, tri_ke=mu, tri_ka=lam, tri_kd=1e-3, edge_ke=1e-3, edge_kd=0.0,
+        particle_radius=5e-3,
+    )  # fmt: skip
+    for p in (0, 6, 42, 48):
+        b.particle_flags[p] = 0
+    rz = rot_z(17.0)
+    c = wp.transform_vector((np.zeros(3), rz), wp.vec3(0.3, 0.3, 0.0))
+    b.add_cloth_grid(
+        pos=wp.vec3(-c[0], -c[1], 0.015), rot=rz, vel=wp.vec3(0.0, 0.0, -2.0), dim_x=6, dim_y=6, cell_x=0.1,
+        cell_y=0.1, mass=mass, tri_ke=mu, tri_ka=lam, tri_kd=1e-3, edge_ke=1e-3, edge_kd=0.0, particle_radius=5e-3,
+    )  # fmt: skip
+    rng = np.random.default_rng(21)
+    q0 = np.array(b.particle_q) + rng.normal(scale=2e-3, size=(len(b.particle_q), 3))
+    out = run_scene(
+        ns, "sc_two_layers", b, gravity=(0.0, 0.0, -9.81), soft=(1.0e2, 1.0e-3, 0.4), shapes=[], contact_fn=None,
+        dt=1.0 / 600.0, iterations=4, substeps=3, seed=4, q_start=q0,
+        self_contact=dict(radius=0.02, margin=0.035, relaxation=0.85, interval=0, ring=2),
+    )  # fmt: skip
+    np.savez_compressed(os.path.join(args.out, "step_selfcontact_layers.npz"), **out)
+
+    # Self-contact: a sheet folded onto itself (upper half 16 mm above the lower half, moving down at
+    # 1.5 m/s), dt = 1/100 so that the isotropic displacement bound acts; 3-ring filter, rest-shape
+    # exclusion radius, collision detection every second iteration.
+    b = FakeBuilder(ns)
+    b.add_cloth_grid(
+        pos=wp.vec3(0.0, 0.0, 0.0), rot=wp.quat_identity(), vel=wp.vec3(0.0, 0.0, 0.0), dim_x=8, dim_y=8, cell_x=0.05,
+        cell_y=0.05, mass=0.2 * 0.0025, tri_ke=mu, tri_ka=lam, tri_kd=0.0, edge_ke=1e-3, edge_kd=1e-4,
+        particle_radius=5e-3,
+    )  # fmt: skip
+    q0 = np.array(b.particle_q)
+    qd0 = np.zeros_like(q0)
+    upper = q0[:, 0] > 0.2 + 1e-9
+    q0[upper, 0] = 0.4 - q0[upper, 0]
+    q0[upper, 2] = 0.016
+    qd0[upper, 2] = -1.5
+    rng = np.random.default_rng(22)
+    q0 += rng.normal(scale=1.5e-3, size=q0.shape)
+    out = run_scene(
+        ns, "sc_fold", b, gravity=(0.0, 0.0, -9.81), soft=(2.0e3, 1.0e-2, 0.6), shapes=[], contact_fn=None,
+        dt=1.0 / 100.0, iterations=4, substeps=3, seed=5, q_start=q0, qd_start=qd0,
+        self_contact=dict(radius=0.012, margin=0.02, relaxation=0.85, interval=2, ring=3, rest_exclusion=0.06),
+    )  # fmt: skip
+    np.savez_compressed(os.path.join(args.out, "step_selfcontact_fold.npz"), **out)
 
 
 def _complex_rest_angle_mesh(ref):

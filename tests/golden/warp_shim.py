@@ -14,7 +14,13 @@ Only the subset of Warp semantics that those kernels touch is provided:
   atan2 sqrt max min abs sign`` with Warp's definitions (``sign(0) == 1``, ``normalize(0) == 0``);
 * rigid transforms as ``(p, q)`` with ``q = (x, y, z, w)``;
 * arrays indexed by ``a[i]`` / ``a[i, j]`` and truthy when non-empty (Warp tests the pointer);
-* ``tid()`` driven by the launcher below and ``atomic_add`` as a plain read-modify-write.
+* ``tid()`` driven by the launcher below, ``atomic_add`` / ``atomic_min`` as plain read-modify-writes;
+* ``closest_point_edge_edge``: Warp implements it natively (not in the reference tree). Here it is
+  restated from the published segment-segment closest-point method (C. Ericson, *Real-Time Collision
+  Detection*, 2005, sec. 5.1.9) with ``epsilon`` as the degenerate-segment threshold on squared lengths;
+* ``bvh_query_aabb``: a brute-force query that yields every primitive whose box overlaps the query box,
+  in index order (the set a BVH returns; Warp's traversal order is not reproduced). ``make_golden.py``
+  rewrites ``while wp.bvh_query_next(query, i):`` loops into ``for i in query:``.
 """
 
 from __future__ import annotations
@@ -28,6 +34,7 @@ DTYPE = np.float64
 inf = math.inf
 float32 = float
 int32 = int
+bool = bool  # noqa: A001 - ``wp.bool``
 
 
 class Vec:
@@ -57,6 +64,9 @@ class Vec:
 
     def __getitem__(self, i):
         return float(self.a[i])
+
+    def __setitem__(self, i, x):
+        self.a[i] = x
 
     def __len__(self):
         return len(self.a)
@@ -144,8 +154,16 @@ def _mat_ctor(r, c):
 
 vec3 = _vec_ctor(3)
 vec2 = _vec_ctor(2)
+vec4 = _vec_ctor(4)
 mat22 = _mat_ctor(2, 2)
 mat33 = _mat_ctor(3, 3)
+mat32 = _mat_ctor(3, 2)
+uint64 = int
+
+
+def vector(*args, length=None, dtype=None):
+    """``wp.vector(..., length=n, dtype=wp.bool)``: a plain list of the values."""
+    return list(args)
 
 
 def spatial_vector(*args):
@@ -210,12 +228,24 @@ def sqrt(x):
     return math.sqrt(x)
 
 
-def max(a, b):  # noqa: A001
+def max(a, b=None):  # noqa: A001
+    if b is None:  # reduction over the components of a vector
+        return float(a.a.max())
+    if isinstance(a, Vec):
+        return Vec(np.maximum(a.a, b.a))
     return a if a > b else b
 
 
-def min(a, b):  # noqa: A001
+def min(a, b=None):  # noqa: A001
+    if b is None:
+        return float(a.a.min())
+    if isinstance(a, Vec):
+        return Vec(np.minimum(a.a, b.a))
     return a if a < b else b
+
+
+def clamp(x, lo, hi):
+    return lo if x < lo else (hi if x > hi else x)
 
 
 def abs(x):  # noqa: A001
@@ -227,6 +257,10 @@ def sign(x):
 
 
 def static(x):
+    return x
+
+
+def constant(x):
     return x
 
 
@@ -307,7 +341,55 @@ def tid():
 
 
 def atomic_add(arr, idx, value):
-    arr[idx] = arr[idx] + value
+    old = arr[idx]
+    arr[idx] = old + value
+    return old
+
+
+def atomic_min(arr, idx, value):
+    old = arr[idx]
+    if value < old:
+        arr[idx] = value
+    return old
+
+
+def closest_point_edge_edge(p1, q1, p2, q2, epsilon):
+    """Closest points of segments p1-q1 and p2-q2: returns vec3(s, t, distance) (Ericson, sec. 5.1.9)."""
+    d1, d2 = q1.a - p1.a, q2.a - p2.a
+    r = p1.a - p2.a
+    a, e, f = float(np.dot(d1, d1)), float(np.dot(d2, d2)), float(np.dot(d2, r))
+    if a <= epsilon and e <= epsilon:
+        s = t = 0.0
+    elif a <= epsilon:
+        s, t = 0.0, clamp(f / e, 0.0, 1.0)
+    else:
+        c = float(np.dot(d1, r))
+        if e <= epsilon:
+            s, t = clamp(-c / a, 0.0, 1.0), 0.0
+        else:
+            b = float(np.dot(d1, d2))
+            denom = a * e - b * b
+            s = clamp((b * f - c * e) / denom, 0.0, 1.0) if denom != 0.0 else 0.0
+            t = (b * s + f) / e
+            if t < 0.0:
+                t, s = 0.0, clamp(-c / a, 0.0, 1.0)
+            elif t > 1.0:
+                t, s = 1.0, clamp((b - c) / a, 0.0, 1.0)
+    c1, c2 = p1.a + d1 * s, p2.a + d2 * t
+    return Vec([s, t, float(np.sqrt(np.dot(c1 - c2, c1 - c2)))])
+
+
+class Bvh:
+    """Primitive boxes; ``bvh_query_aabb`` tests them all."""
+
+    def __init__(self, lowers, uppers):
+        self.lo = np.asarray(lowers, dtype=DTYPE).reshape(-1, 3)
+        self.hi = np.asarray(uppers, dtype=DTYPE).reshape(-1, 3)
+
+
+def bvh_query_aabb(bvh, lower, upper):
+    hit = np.all(bvh.lo <= upper.a, axis=1) & np.all(bvh.hi >= lower.a, axis=1)
+    return [int(i) for i in np.nonzero(hit)[0]]
 
 
 def launch(kernel, dim, *args):
