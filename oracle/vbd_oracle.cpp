@@ -20,6 +20,12 @@
 //              solver_vbd.py:1575-1622, 1669-1766, 2151-2337, 2339-2376, 2763-2774 (sequencing)
 //   adjacency  particle_vbd_kernels.py:639-738 (count/fill order)
 //   contacts   geometry/kernels.py:1001-1140 for PLANE (infinite) and SPHERE shapes
+//   self-contact particle_vbd_kernels.py:1193-1222 (barrier), 1225-1238 (damping), 1371-1506 (edge-edge),
+//              1599-1745 (vertex-triangle), 1748-1779 (friction), 1930-2071 (accumulation),
+//              2475-2741 (division planes, step fractions), 2744-2897 (truncation);
+//              geometry/kernels.py:64-128 (triangle closest point), 1252-1497 (detection semantics);
+//              math/__init__.py orthonormal_basis; solver_vbd.py:1669-1766, 2151-2337, 2834-2850
+//   edge-edge closest points: Warp native (closest_point_edge_edge), restated from Ericson 2005 sec. 5.1.9
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -328,10 +334,554 @@ struct Contacts {
 template <typename R> inline V3<R> ld(const double* a, int i) { return {R(a[3 * i]), R(a[3 * i + 1]), R(a[3 * i + 2])}; }
 template <typename R> inline V3<R> ld(const std::vector<V3<R>>& a, int i) { return a[i]; }
 
-// One SolverVBD.step without self-contact and without rigid bodies (static shapes only).
+// ------------------------------------------------------------------------------------ self-contact
+// Closest point on triangle (a, b, c) to p, with the reference's branch order
+// (geometry/kernels.py:64-128): vertex regions A, B, C first, then edges AB, AC, BC, then the interior.
+// feature: 0..2 vertex A..C, 3 edge AB, 4 edge AC, 5 edge BC, 6 interior.
+template <typename R>
+V3<R> tri_closest(V3<R> a, V3<R> b, V3<R> c, V3<R> p, R bary[3], int& feature) {
+  const V3<R> ab = b - a, ac = c - a, ap = p - a;
+  const R d1 = dot(ab, ap), d2 = dot(ac, ap);
+  if (d1 <= R(0) && d2 <= R(0)) {
+    bary[0] = 1, bary[1] = 0, bary[2] = 0, feature = 0;
+    return a;
+  }
+  const V3<R> bp = p - b;
+  const R d3 = dot(ab, bp), d4 = dot(ac, bp);
+  if (d3 >= R(0) && d4 <= d3) {
+    bary[0] = 0, bary[1] = 1, bary[2] = 0, feature = 1;
+    return b;
+  }
+  const V3<R> cp = p - c;
+  const R d5 = dot(ab, cp), d6 = dot(ac, cp);
+  if (d6 >= R(0) && d5 <= d6) {
+    bary[0] = 0, bary[1] = 0, bary[2] = 1, feature = 2;
+    return c;
+  }
+  const R vc = d1 * d4 - d3 * d2;
+  if (vc <= R(0) && d1 >= R(0) && d3 <= R(0)) {
+    const R v = d1 / (d1 - d3);
+    bary[0] = R(1) - v, bary[1] = v, bary[2] = 0, feature = 3;
+    return a + v * ab;
+  }
+  const R vb = d5 * d2 - d1 * d6;
+  if (vb <= R(0) && d2 >= R(0) && d6 <= R(0)) {
+    const R v = d2 / (d2 - d6);
+    bary[0] = R(1) - v, bary[1] = 0, bary[2] = v, feature = 4;
+    return a + v * ac;
+  }
+  const R va = d3 * d6 - d5 * d4;
+  if (va <= R(0) && (d4 - d3) >= R(0) && (d5 - d6) >= R(0)) {
+    const R v = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+    bary[0] = 0, bary[1] = R(1) - v, bary[2] = v, feature = 5;
+    return b + v * (c - b);
+  }
+  const R denom = R(1) / (va + vb + vc);
+  const R v = vb * denom, w = vc * denom;
+  bary[0] = R(1) - v - w, bary[1] = v, bary[2] = w, feature = 6;
+  return a + v * ab + w * ac;
+}
+
+template <typename R> inline R rclamp(R x, R lo, R hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
+// Closest points of segments p1-q1 and p2-q2 (s, t and their distance). Warp's closest_point_edge_edge
+// is native code outside the reference tree; this restates the published segment-segment method
+// (C. Ericson, Real-Time Collision Detection, 2005, sec. 5.1.9), eps bounding the squared lengths of
+// degenerate segments. Exactly parallel segments take s = 0.
+template <typename R>
+void edge_closest(V3<R> p1, V3<R> q1, V3<R> p2, V3<R> q2, R eps, R& s, R& t, R& dist) {
+  const V3<R> d1 = q1 - p1, d2 = q2 - p2, r = p1 - p2;
+  const R a = dot(d1, d1), e = dot(d2, d2), f = dot(d2, r);
+  if (a <= eps && e <= eps) {
+    s = t = R(0);
+  } else if (a <= eps) {
+    s = R(0);
+    t = rclamp(f / e, R(0), R(1));
+  } else {
+    const R c = dot(d1, r);
+    if (e <= eps) {
+      t = R(0);
+      s = rclamp(-c / a, R(0), R(1));
+    } else {
+      const R b = dot(d1, d2);
+      const R denom = a * e - b * b;
+      s = denom != R(0) ? rclamp((b * f - c * e) / denom, R(0), R(1)) : R(0);
+      t = (b * s + f) / e;
+      if (t < R(0)) {
+        t = R(0);
+        s = rclamp(-c / a, R(0), R(1));
+      } else if (t > R(1)) {
+        t = R(1);
+        s = rclamp((b - c) / a, R(0), R(1));
+      }
+    }
+  }
+  dist = length((p1 + d1 * s) - (p2 + d2 * t));
+}
+
+// math/__init__.py orthonormal_basis
+template <typename R>
+void onb(V3<R> n, V3<R>& b1, V3<R>& b2) {
+  if (n.z < R(0)) {
+    const R a = R(1) / (R(1) - n.z), b = n.x * n.y * a;
+    b1 = v3<R>(R(1) - n.x * n.x * a, -b, n.x);
+    b2 = v3<R>(b, n.y * n.y * a - R(1), -n.y);
+  } else {
+    const R a = R(1) / (R(1) + n.z), b = -n.x * n.y * a;
+    b1 = v3<R>(R(1) - n.x * n.x * a, b, -n.x);
+    b2 = v3<R>(b, R(1) - n.y * n.y * a, -n.y);
+  }
+}
+
+// particle_vbd_kernels.py:1193-1222: dE/dd and d2E/dd2 of the self-contact barrier
+template <typename R>
+void sc_norm(R dis, R radius, R k, R& dEdD, R& d2E) {
+  const R tau = radius * R(0.5), d_min = R(1.0e-5);
+  if (tau > dis && dis > d_min) {
+    const R k2 = tau * tau * k;
+    dEdD = -k2 / dis;
+    d2E = k2 / (dis * dis);
+  } else if (dis <= d_min) {
+    const R k2 = tau * tau * k;
+    const R dm2 = d_min * d_min;
+    dEdD = k2 * (dis - R(2) * d_min) / dm2;
+    d2E = k2 / dm2;
+  } else {
+    dEdD = -k * (radius - dis);
+    d2E = k;
+  }
+}
+
+// particle_vbd_kernels.py:1748-1779 (compute_friction with T = [b1 b2])
+template <typename R>
+void sc_friction(R mu, R fn, V3<R> b1, V3<R> b2, V3<R> dx, R eps_u, V3<R>& f, M3<R>& H) {
+  const R u0 = dot(b1, dx), u1 = dot(b2, dx);
+  const R un = std::sqrt(u0 * u0 + u1 * u1);
+  if (un > R(0)) {
+    const R f1 = un > eps_u ? R(1) / un : (-un / eps_u + R(2)) / eps_u;
+    f = (-mu * fn) * ((f1 * u0) * b1 + (f1 * u1) * b2);
+    H = (mu * fn * f1) * (outer(b1, b1) + outer(b2, b2));
+  } else {
+    f = v3<R>(0, 0, 0);
+    H = mzero<R>();
+  }
+}
+
+// particle_vbd_kernels.py:1225-1238
+template <typename R>
+void sc_damp(V3<R> disp, V3<R> n, const M3<R>& H, R kd, R dt, V3<R>& f, M3<R>& Hd) {
+  if (dot(disp, n) > R(0)) {
+    Hd = (kd / dt) * H;
+    f = Hd * disp;
+  } else {
+    f = v3<R>(0, 0, 0);
+    Hd = mzero<R>();
+  }
+}
+
+// Vertex-triangle contact on all four vertices (particle_vbd_kernels.py:1599-1745).
+// x = (a, b, c, p), xa = the same at the start of the step.
+template <typename R>
+bool sc_vt(const V3<R> x[4], const V3<R> xa[4], R radius, R ke, R kd, R mu, R eps, R dt, V3<R> f[4], M3<R> H[4]) {
+  R bary[3];
+  int feat;
+  const V3<R> cp = tri_closest(x[0], x[1], x[2], x[3], bary, feat);
+  const V3<R> diff = x[3] - cp;
+  const R dis = length(diff);
+  const V3<R> n = diff / dis;
+  if (!(R(0) < dis && dis < radius)) return false;
+  const R bs[4] = {-bary[0], -bary[1], -bary[2], R(1)};
+  R dEdD, d2E;
+  sc_norm(dis, radius, ke, dEdD, d2E);
+  const V3<R> cf = -dEdD * n;
+  const M3<R> cH = d2E * outer(n, n);
+  const V3<R> cpp = bary[0] * xa[0] + bary[1] * xa[1] + bary[2] * xa[2];
+  const V3<R> dx = (x[3] - xa[3]) - (cp - cpp);
+  V3<R> b1, b2;
+  onb(n, b1, b2);
+  V3<R> ff;
+  M3<R> fH;
+  sc_friction(mu, -dEdD, b1, b2, dx, eps * dt, ff, fH);
+  const R sgn[4] = {R(-1), R(-1), R(-1), R(1)};
+  for (int k = 0; k < 4; ++k) {
+    f[k] = cf * bs[k];
+    H[k] = cH * bs[k] * bs[k];
+    V3<R> df;
+    M3<R> dH;
+    sc_damp(xa[k] - x[k], n * sgn[k], H[k], kd, dt, df, dH);
+    f[k] = f[k] + (df + bs[k] * ff);
+    H[k] = H[k] + (dH + (bs[k] * bs[k]) * fH);
+  }
+  return true;
+}
+
+// Edge-edge contact on the two vertices of the first edge (particle_vbd_kernels.py:1371-1506).
+// x = (e1.v0, e1.v1, e2.v0, e2.v1).
+template <typename R>
+bool sc_ee(const V3<R> x[4], const V3<R> xa[4], R radius, R ke, R kd, R mu, R eps, R dt, R ee_eps, V3<R> f[2],
+           M3<R> H[2]) {
+  R s, t, dis;
+  edge_closest(x[0], x[1], x[2], x[3], ee_eps, s, t, dis);
+  const V3<R> c1 = x[0] + (x[1] - x[0]) * s, c2 = x[2] + (x[3] - x[2]) * t;
+  const V3<R> n = (c1 - c2) / dis;
+  if (!(R(0) < dis && dis < radius)) return false;
+  const R bs[2] = {R(1) - s, s};
+  R dEdD, d2E;
+  sc_norm(dis, radius, ke, dEdD, d2E);
+  const V3<R> cf = -dEdD * n;
+  const M3<R> cH = d2E * outer(n, n);
+  const V3<R> c1p = xa[0] + (xa[1] - xa[0]) * s, c2p = xa[2] + (xa[3] - xa[2]) * t;
+  const V3<R> dx = (c1 - c1p) - (c2 - c2p);
+  V3<R> b1, b2;
+  onb(n, b1, b2);
+  V3<R> ff;
+  M3<R> fH;
+  sc_friction(mu, -dEdD, b1, b2, dx, eps * dt, ff, fH);
+  for (int k = 0; k < 2; ++k) {
+    f[k] = cf * bs[k];
+    H[k] = cH * bs[k] * bs[k];
+    V3<R> df;
+    M3<R> dH;
+    sc_damp(xa[k] - x[k], n, H[k], kd, dt, df, dH);
+    f[k] = f[k] + (df + bs[k] * ff);
+    H[k] = H[k] + (dH + (bs[k] * bs[k]) * fH);
+  }
+  return true;
+}
+
+// particle_vbd_kernels.py:2475-2498 (coplanar segments never count here)
+template <typename R>
+bool seg_plane(V3<R> v, V3<R> dv, V3<R> n, V3<R> d, R eps_par, R near, R far) {
+  const R nv = dot(n, dv), num = -dot(n, v - d);
+  if (std::fabs(nv) < eps_par) return false;
+  const R t = num / nv;
+  return t >= near && t <= R(1) + far;
+}
+
+template <typename R> inline V3<R> normalize(V3<R> a) {
+  const R l = length(a);
+  return l > R(0) ? a / l : v3<R>(0, 0, 0);
+}
+
+// particle_vbd_kernels.py:2500-2558. x = (v, t1, t2, t3), dx their displacements; dummy[k] = no cut.
+template <typename R>
+void vt_plane(const V3<R> x[4], const V3<R> dx[4], bool dummy[4], V3<R>& n, V3<R>& d) {
+  R bary[3];
+  int feat;
+  const V3<R> cp = tri_closest(x[1], x[2], x[3], x[0], bary, feat);
+  const V3<R> nh = x[0] - cp;
+  if (length(nh) < R(1e-12)) {
+    for (int k = 0; k < 4; ++k) dummy[k] = false;
+    n = v3<R>(0, 0, 0);
+    d = x[0];
+    return;
+  }
+  n = normalize(nh);
+  const R dvn = rmax(-dot(n, dx[0]), R(0));
+  const R dtn = rmax(rmax(dot(n, dx[1]), dot(n, dx[2])), rmax(dot(n, dx[3]), R(0)));
+  if (dtn + dvn == R(0)) {
+    d = cp + R(0.5) * nh;
+  } else {
+    const R l = rclamp(dtn / (dtn + dvn), R(0.05), R(0.95));
+    d = cp + l * nh;
+  }
+  dummy[0] = dvn == R(0) ? true : !seg_plane(x[0], dx[0], n, d, R(1e-6), R(-1e-8), R(1e-8));
+  for (int k = 1; k < 4; ++k)
+    dummy[k] = dtn == R(0) ? true : !seg_plane(x[k], dx[k], n, d, R(1e-6), R(-1e-8), R(1e-8));
+}
+
+// particle_vbd_kernels.py:2561-2628
+template <typename R>
+V3<R> robust_pair_normal(V3<R> a0, V3<R> a1, V3<R> b0, V3<R> b1, R eps = R(1e-6)) {
+  V3<R> d0 = a1 - a0, d1 = b1 - b0;
+  const R l0 = length(d0), l1 = length(d1);
+  d0 = l0 > eps ? d0 / l0 : v3<R>(0, 0, 0);
+  d1 = l1 > eps ? d1 / l1 : v3<R>(0, 0, 0);
+  V3<R> n = cross(d0, d1);
+  R ln = length(n);
+  if (ln > eps) return n / ln;
+  V3<R> ref = d0;
+  if (length(ref) <= eps) ref = d1;
+  if (length(ref) <= eps) return v3<R>(1, 0, 0);
+  const V3<R> bridge = R(0.5) * ((b0 + b1) - (a0 + a1));
+  const R bl = length(bridge);
+  if (bl > eps) {
+    n = cross(ref, bridge / bl);
+    ln = length(n);
+    if (ln > eps) return n / ln;
+  }
+  V3<R> axis = v3<R>(1, 0, 0);
+  if (std::fabs(dot(ref, axis)) > R(0.9)) axis = v3<R>(0, 1, 0);
+  n = cross(ref, axis);
+  ln = length(n);
+  if (ln > eps) return n / ln;
+  n = cross(ref, v3<R>(0, 0, 1));
+  ln = length(n);
+  if (ln > eps) return n / ln;
+  return v3<R>(1, 0, 0);
+}
+
+// particle_vbd_kernels.py:2631-2702. x = (e0.v0, e0.v1, e1.v0, e1.v1).
+template <typename R>
+void ee_plane(const V3<R> x[4], const V3<R> dx[4], bool dummy[4], V3<R>& n, V3<R>& d) {
+  R s, t, dist;
+  edge_closest(x[0], x[1], x[2], x[3], R(1e-6), s, t, dist);
+  const V3<R> c1 = x[0] + (x[1] - x[0]) * s, c2 = x[2] + (x[3] - x[2]) * t;
+  const V3<R> nh = c1 - c2;
+  if (length(nh) < R(1e-12)) {
+    for (int k = 0; k < 4; ++k) dummy[k] = false;
+    n = robust_pair_normal(x[0], x[1], x[2], x[3]);
+    d = c1 * R(0.5) + c2 * R(0.5);
+    return;
+  }
+  n = normalize(nh);
+  const R de0 = rmax(rmax(-dot(n, dx[0]), -dot(n, dx[1])), R(0));
+  const R de1 = rmax(rmax(dot(n, dx[2]), dot(n, dx[3])), R(0));
+  if (de0 + de1 == R(0)) {
+    d = c2 + R(0.5) * nh;
+  } else {
+    const R l = rclamp(de1 / (de1 + de0), R(0.05), R(0.95));
+    d = c2 + l * nh;
+  }
+  for (int k = 0; k < 2; ++k) dummy[k] = de0 == R(0) ? true : !seg_plane(x[k], dx[k], n, d, R(1e-6), R(-1e-8), R(1e-6));
+  for (int k = 2; k < 4; ++k) dummy[k] = de1 == R(0) ? true : !seg_plane(x[k], dx[k], n, d, R(1e-6), R(-1e-8), R(1e-6));
+}
+
+// particle_vbd_kernels.py:2724-2741
+template <typename R>
+R plane_t(V3<R> v, V3<R> dv, V3<R> n, V3<R> d, R eps, R gamma, R gamma_min = R(1e-3)) {
+  const R den = dot(n, dv);
+  if (std::fabs(den) < eps) return R(1);
+  const R t = dot(n, d - v) / den;
+  if (t < R(0)) return R(1);
+  return rclamp(rmin(t * gamma, t - gamma_min), R(0), R(1));
+}
+
+struct SelfContact {
+  double radius, margin, relaxation, edge_parallel_epsilon, rest_exclusion;
+  int vertex_buffer, edge_buffer, interval;
+  const double* rest_q;  // model.particle_q (rest-shape distance filter)
+  const int *vt_filter_offsets, *vt_filter;  // sorted CSR per vertex, or null
+  const int *ee_filter_offsets, *ee_filter;  // sorted CSR per edge, or null
+};
+
+inline bool in_sorted(const int* off, const int* list, int row, int key) {
+  if (!off) return false;
+  int lo = off[row], hi = off[row + 1];
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (list[mid] > key) hi = mid; else lo = mid + 1;
+  }
+  return hi > off[row] && list[hi - 1] == key;
+}
+
+// Collision buffers of TriMeshCollisionDetector (tri_mesh_collision.py:18-40): per vertex
+// vertex_buffer slots of (vertex, triangle), per edge edge_buffer slots of (edge, edge), -1 when empty.
+template <typename R>
+struct SCBuffers {
+  std::vector<int> vt, vt_count, ee, ee_count;
+  std::vector<R> vt_min, ee_min;
+  int flags[4] = {0, 0, 0, 0};
+};
+
+// Brute-force detection with the semantics of vertex_triangle_collision_detection_kernel and
+// edge_colliding_edges_detection_kernel (geometry/kernels.py:1252-1497): a primitive pair is recorded
+// when its distance is below the margin, it is not topologically adjacent or filtered, and (with a
+// positive exclusion radius) its rest-shape distance is not below that radius. Slots are filled in
+// increasing primitive index; the count includes pairs past the buffer (overflow flag 0 / 2).
+template <typename R>
+void sc_detect(const Model& M, const SelfContact& S, const std::vector<V3<R>>& pos, SCBuffers<R>& B, int nthreads) {
+  const int n = M.n, T = M.T, E = M.E, vb = S.vertex_buffer, eb = S.edge_buffer;
+  const R margin = R(S.margin), rmin_q = R(S.rest_exclusion), eps = R(S.edge_parallel_epsilon);
+  B.vt.assign(size_t(2) * n * vb, -1);
+  B.vt_count.assign(n, 0);
+  B.vt_min.assign(n, margin);
+  B.ee.assign(size_t(2) * E * eb, -1);
+  B.ee_count.assign(E, 0);
+  B.ee_min.assign(E, margin);
+  for (int k = 0; k < 4; ++k) B.flags[k] = 0;
+  std::vector<V3<R>> tlo(T), thi(T), elo(E), ehi(E);
+  auto vmin3 = [](V3<R> a, V3<R> b) { return v3<R>(rmin(a.x, b.x), rmin(a.y, b.y), rmin(a.z, b.z)); };
+  auto vmax3 = [](V3<R> a, V3<R> b) { return v3<R>(rmax(a.x, b.x), rmax(a.y, b.y), rmax(a.z, b.z)); };
+  for (int t = 0; t < T; ++t) {
+    const int* ti = M.tri_indices + 3 * t;
+    tlo[t] = vmin3(vmin3(pos[ti[0]], pos[ti[1]]), pos[ti[2]]);
+    thi[t] = vmax3(vmax3(pos[ti[0]], pos[ti[1]]), pos[ti[2]]);
+  }
+  for (int e = 0; e < E; ++e) {
+    const int* ei = M.edge_indices + 4 * e;
+    elo[e] = vmin3(pos[ei[2]], pos[ei[3]]);
+    ehi[e] = vmax3(pos[ei[2]], pos[ei[3]]);
+  }
+  auto overlap = [](V3<R> alo, V3<R> ahi, V3<R> blo, V3<R> bhi) {
+    return alo.x <= bhi.x && alo.y <= bhi.y && alo.z <= bhi.z && ahi.x >= blo.x && ahi.y >= blo.y && ahi.z >= blo.z;
+  };
+  int ovf_v = 0, ovf_e = 0;
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 16) reduction(| : ovf_v)
+  for (int v = 0; v < n; ++v) {
+    const V3<R> p = pos[v];
+    const V3<R> lo = v3<R>(p.x - margin, p.y - margin, p.z - margin), hi = v3<R>(p.x + margin, p.y + margin, p.z + margin);
+    int cnt = 0;
+    R mn = margin;
+    for (int t = 0; t < T; ++t) {
+      if (!overlap(lo, hi, tlo[t], thi[t])) continue;
+      const int* ti = M.tri_indices + 3 * t;
+      if (v == ti[0] || v == ti[1] || v == ti[2]) continue;
+      if (in_sorted(S.vt_filter_offsets, S.vt_filter, v, t)) continue;
+      R bary[3];
+      int feat;
+      const R dist = length(tri_closest(pos[ti[0]], pos[ti[1]], pos[ti[2]], p, bary, feat) - p);
+      if (rmin_q > R(0)) {
+        const V3<R> rv = ld<R>(S.rest_q, v);
+        const R dref = length(tri_closest(ld<R>(S.rest_q, ti[0]), ld<R>(S.rest_q, ti[1]), ld<R>(S.rest_q, ti[2]), rv,
+                                          bary, feat) - rv);
+        if (dref < rmin_q) continue;
+      }
+      if (dist < margin) {
+        mn = rmin(mn, dist);
+        if (cnt < vb) {
+          B.vt[2 * (size_t(v) * vb + cnt)] = v;
+          B.vt[2 * (size_t(v) * vb + cnt) + 1] = t;
+        } else {
+          ovf_v = 1;
+        }
+        ++cnt;
+      }
+    }
+    B.vt_count[v] = cnt;
+    B.vt_min[v] = mn;
+  }
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 16) reduction(| : ovf_e)
+  for (int e = 0; e < E; ++e) {
+    const int* ei = M.edge_indices + 4 * e;
+    const V3<R> lo = elo[e] - v3<R>(margin, margin, margin), hi = ehi[e] + v3<R>(margin, margin, margin);
+    int cnt = 0;
+    R mn = margin;
+    for (int e2 = 0; e2 < E; ++e2) {
+      if (!overlap(lo, hi, elo[e2], ehi[e2])) continue;
+      const int* fi = M.edge_indices + 4 * e2;
+      if (ei[2] == fi[2] || ei[2] == fi[3] || ei[3] == fi[2] || ei[3] == fi[3]) continue;
+      if (in_sorted(S.ee_filter_offsets, S.ee_filter, e, e2)) continue;
+      R s, t, dist;
+      edge_closest(pos[ei[2]], pos[ei[3]], pos[fi[2]], pos[fi[3]], eps, s, t, dist);
+      if (rmin_q > R(0)) {
+        R dref;
+        edge_closest(ld<R>(S.rest_q, ei[2]), ld<R>(S.rest_q, ei[3]), ld<R>(S.rest_q, fi[2]), ld<R>(S.rest_q, fi[3]), eps,
+                     s, t, dref);
+        if (dref < rmin_q) continue;
+      }
+      if (dist < margin) {
+        mn = rmin(mn, dist);
+        if (cnt < eb) {
+          B.ee[2 * (size_t(e) * eb + cnt)] = e;
+          B.ee[2 * (size_t(e) * eb + cnt) + 1] = e2;
+        } else {
+          ovf_e = 1;
+        }
+        ++cnt;
+      }
+    }
+    B.ee_count[e] = cnt;
+    B.ee_min[e] = mn;
+  }
+  B.flags[0] = ovf_v;
+  B.flags[2] = ovf_e;
+}
+
+// accumulate_self_contact_force_and_hessian (particle_vbd_kernels.py:1930-2071), in the order of its
+// thread ids run one after another: thread 4p+j takes slots j, j+4, ... of edge p, then of vertex p.
+template <typename R>
+void sc_accumulate(const Model& M, const SelfContact& S, const SCBuffers<R>& B, int color, const std::vector<V3<R>>& pos,
+                   const std::vector<V3<R>>& q_prev, R dt, std::vector<V3<R>>& forces, std::vector<M3<R>>& hess) {
+  const int n = M.n, E = M.E, vb = S.vertex_buffer, eb = S.edge_buffer;
+  const int P = n > E ? n : E;
+  const R radius = R(S.radius), ke = R(M.soft_ke), kd = R(M.soft_kd), mu = R(M.soft_mu), eps = R(M.friction_epsilon);
+  const R ee_eps = R(S.edge_parallel_epsilon);
+  const int* col = M.particle_colors;
+  for (int p = 0; p < P; ++p)
+    for (int j = 0; j < 4; ++j) {
+      if (p < E)
+        for (int k = j; k < eb; k += 4) {
+          const int e2 = B.ee[2 * (size_t(p) * eb + k) + 1];
+          if (e2 == -1) continue;
+          const int* ei = M.edge_indices + 4 * p;
+          const int* fi = M.edge_indices + 4 * e2;
+          if (col[ei[2]] != color && col[ei[3]] != color) continue;
+          const int ids[4] = {ei[2], ei[3], fi[2], fi[3]};
+          V3<R> x[4], xa[4], f[2];
+          M3<R> H[2];
+          for (int m = 0; m < 4; ++m) x[m] = pos[ids[m]], xa[m] = q_prev[ids[m]];
+          if (sc_ee(x, xa, radius, ke, kd, mu, eps, dt, ee_eps, f, H))
+            for (int m = 0; m < 2; ++m)
+              if (col[ids[m]] == color) {
+                forces[ids[m]] = forces[ids[m]] + f[m];
+                hess[ids[m]] = hess[ids[m]] + H[m];
+              }
+        }
+      if (p < n)
+        for (int k = j; k < vb; k += 4) {
+          const int t = B.vt[2 * (size_t(p) * vb + k) + 1];
+          if (t == -1) continue;
+          const int* ti = M.tri_indices + 3 * t;
+          const int ids[4] = {ti[0], ti[1], ti[2], p};
+          if (col[p] != color && col[ti[0]] != color && col[ti[1]] != color && col[ti[2]] != color) continue;
+          V3<R> x[4], xa[4], f[4];
+          M3<R> H[4];
+          for (int m = 0; m < 4; ++m) x[m] = pos[ids[m]], xa[m] = q_prev[ids[m]];
+          if (sc_vt(x, xa, radius, ke, kd, mu, eps, dt, f, H)) {
+            const int order[4] = {3, 0, 1, 2};  // particle first, then a, b, c, as the reference adds them
+            for (int m : order)
+              if (col[ids[m]] == color) {
+                forces[ids[m]] = forces[ids[m]] + f[m];
+                hess[ids[m]] = hess[ids[m]] + H[m];
+              }
+          }
+        }
+    }
+}
+
+// apply_planar_truncation_parallel_by_collision (particle_vbd_kernels.py:2744-2874): per-vertex minimum of
+// the division-plane step fractions over all recorded pairs. pos = positions at the last detection.
+template <typename R>
+void sc_truncation_ts(const Model& M, const SelfContact& S, const SCBuffers<R>& B, const std::vector<V3<R>>& pos,
+                      const std::vector<V3<R>>& disp, std::vector<R>& ts) {
+  const int n = M.n, E = M.E, vb = S.vertex_buffer, eb = S.edge_buffer;
+  const R eps = R(S.edge_parallel_epsilon), gamma = R(S.relaxation);
+  for (int i = 0; i < n; ++i) ts[i] = R(1);
+  for (int e = 0; e < E; ++e)
+    for (int k = 0; k < eb; ++k) {
+      const int e2 = B.ee[2 * (size_t(e) * eb + k) + 1];
+      if (e2 == -1) continue;
+      const int* ei = M.edge_indices + 4 * e;
+      const int* fi = M.edge_indices + 4 * e2;
+      const int ids[4] = {ei[2], ei[3], fi[2], fi[3]};
+      V3<R> x[4], dx[4], nn, d;
+      bool dummy[4];
+      for (int m = 0; m < 4; ++m) x[m] = pos[ids[m]], dx[m] = disp[ids[m]];
+      ee_plane(x, dx, dummy, nn, d);
+      for (int m = 0; m < 4; ++m)
+        if (!dummy[m]) ts[ids[m]] = rmin(ts[ids[m]], plane_t(x[m], dx[m], nn, d, eps, gamma));
+    }
+  for (int v = 0; v < n; ++v)
+    for (int k = 0; k < vb; ++k) {
+      const int t = B.vt[2 * (size_t(v) * vb + k) + 1];
+      if (t == -1) continue;
+      const int* ti = M.tri_indices + 3 * t;
+      const int ids[4] = {v, ti[0], ti[1], ti[2]};
+      V3<R> x[4], dx[4], nn, d;
+      bool dummy[4];
+      for (int m = 0; m < 4; ++m) x[m] = pos[ids[m]], dx[m] = disp[ids[m]];
+      vt_plane(x, dx, dummy, nn, d);
+      for (int m = 0; m < 4; ++m)
+        if (!dummy[m]) ts[ids[m]] = rmin(ts[ids[m]], plane_t(x[m], dx[m], nn, d, eps, gamma));
+    }
+}
+
+// One SolverVBD.step without rigid bodies (static shapes only); S != nullptr turns particle
+// self-contact on (solver_vbd.py:1669-1766, 2151-2337, 2834-2850).
 template <typename R>
 int step(const Model& M, double* q_in, const double* qd_in, const double* f_ext, const Contacts& Cn, R dt,
-         int iterations, double* q_out, double* qd_out, int nthreads) {
+         int iterations, double* q_out, double* qd_out, int nthreads, const SelfContact* S = nullptr) {
   const int n = M.n;
   std::vector<V3<R>> pos(n), q_prev(n), inertia(n), disp(n), pos_cd(n), forces(n);
   std::vector<M3<R>> hess(n);
@@ -351,7 +901,11 @@ int step(const Model& M, double* q_in, const double* qd_in, const double* f_ext,
     mat_mu[c] = amu;
     pen_k[c] = k_start < R(0) ? ake : rmin(k_start, ake);
   }
-  // _initialize_particles: pos_prev_collision_detection = q, displacements = 0, forward_step
+  // _initialize_particles: pos_prev_collision_detection = q, displacements = 0 (after a collision
+  // detection with self-contact on), forward_step
+  SCBuffers<R> B;
+  std::vector<R> ts(n, R(1));
+  if (S) sc_detect(M, *S, pos, B, nthreads);
   const V3<R> g = ld<R>(M.gravity, 0);
   for (int i = 0; i < n; ++i) {
     pos_cd[i] = pos[i];
@@ -365,9 +919,22 @@ int step(const Model& M, double* q_in, const double* qd_in, const double* f_ext,
     inertia[i] = pos[i] + vel * dt;
     disp[i] = vel * dt;
   }
-  // apply_truncation_ts with t = 1, max_displacement = inf: pos = pos_cd + disp
+  // apply_truncation_ts: without self-contact t = 1, max_displacement = inf: pos = pos_cd + disp; with
+  // it, t from the division planes of all recorded pairs and |disp| <= margin * relaxation / 2
   auto truncate = [&]() {
-    for (int i = 0; i < n; ++i) pos[i] = pos_cd[i] + disp[i];
+    if (!S) {
+      for (int i = 0; i < n; ++i) pos[i] = pos_cd[i] + disp[i];
+      return;
+    }
+    sc_truncation_ts(M, *S, B, pos_cd, disp, ts);
+    const R max_d = R(S->margin) * R(S->relaxation) * R(0.5);
+    for (int i = 0; i < n; ++i) {
+      V3<R> d = disp[i] * ts[i];
+      const R len = length(d);
+      if (len > max_d) d = d * max_d / len;
+      disp[i] = d;
+      pos[i] = pos_cd[i] + d;
+    }
   };
   truncate();
   const R dt2r = R(1) / (dt * dt);
@@ -380,6 +947,14 @@ int step(const Model& M, double* q_in, const double* qd_in, const double* f_ext,
       R pen = -(dot(nn, pos[p] - bx) - R(M.radius[p]));
       pen = rmax(R(0), pen);
       pen_k[c] = rmin(pen_k[c] + beta * pen, mat_ke[c]);
+    }
+    if (S && ((S->interval == 0 && it == 0) || (S->interval >= 1 && it % S->interval == 0))) {
+      // _collision_detection_penetration_free (solver_vbd.py:2834-2850)
+      for (int i = 0; i < n; ++i) {
+        pos_cd[i] = pos[i];
+        disp[i] = v3<R>(0, 0, 0);
+      }
+      sc_detect(M, *S, pos, B, nthreads);
     }
     for (int i = 0; i < n; ++i) {
       forces[i] = v3<R>(0, 0, 0);
@@ -403,6 +978,7 @@ int step(const Model& M, double* q_in, const double* qd_in, const double* f_ext,
           hess[p] = hess[p] + H;
         }
       }
+      if (S) sc_accumulate(M, *S, B, color, pos, q_prev, dt, forces, hess);
       // solve_elasticity (particle_vbd_kernels.py:3135-3273)
       const int c0 = M.color_offsets[color], c1 = M.color_offsets[color + 1];
 #pragma omp parallel for num_threads(nthreads) schedule(static)
@@ -513,6 +1089,148 @@ int oracle_vbd_step(const OracleModel* m, double* q_in, const double* qd_in, con
   if (precision == 32)
     return step<float>(M, q_in, qd_in, f_ext, C, float(dt), iterations, q_out, qd_out, nthreads);
   return -1;
+}
+
+struct OracleSelfContact {
+  double radius, margin, relaxation, edge_parallel_epsilon, rest_exclusion;
+  int vertex_buffer, edge_buffer, interval;
+  const double* rest_q;
+  const int *vt_filter_offsets, *vt_filter, *ee_filter_offsets, *ee_filter;
+};
+static_assert(sizeof(OracleSelfContact) == sizeof(SelfContact), "layout");
+
+// oracle_vbd_step with particle self-contact on.
+int oracle_vbd_step_sc(const OracleModel* m, double* q_in, const double* qd_in, const double* f_ext,
+                       const OracleContacts* c, const OracleSelfContact* sc, double dt, int iterations, double* q_out,
+                       double* qd_out, int precision, int nthreads) {
+  Model M;
+  std::memcpy(&M, m, sizeof(M));
+  SelfContact S;
+  std::memcpy(&S, sc, sizeof(S));
+  Contacts C{c->count, c->max, c->particle, c->shape, c->body_pos, c->body_vel, c->normal};
+  if (nthreads < 1) nthreads = 1;
+  if (precision == 64) return step<double>(M, q_in, qd_in, f_ext, C, dt, iterations, q_out, qd_out, nthreads, &S);
+  if (precision == 32)
+    return step<float>(M, q_in, qd_in, f_ext, C, float(dt), iterations, q_out, qd_out, nthreads, &S);
+  return -1;
+}
+
+// One collision detection at positions q (n x 3). Outputs as TriMeshCollisionInfo: vt[2*n*vb],
+// vt_count[n], vt_min[n], ee[2*E*eb], ee_count[E], ee_min[E], flags[4].
+int oracle_collide(const OracleModel* m, const OracleSelfContact* sc, const double* q, int precision, int* vt,
+                   int* vt_count, double* vt_min, int* ee, int* ee_count, double* ee_min, int* flags, int nthreads) {
+  Model M;
+  std::memcpy(&M, m, sizeof(M));
+  SelfContact S;
+  std::memcpy(&S, sc, sizeof(S));
+  auto run = [&](auto tag) {
+    using R = decltype(tag);
+    std::vector<V3<R>> pos(M.n);
+    for (int i = 0; i < M.n; ++i) pos[i] = ld<R>(q, i);
+    SCBuffers<R> B;
+    sc_detect(M, S, pos, B, nthreads < 1 ? 1 : nthreads);
+    std::copy(B.vt.begin(), B.vt.end(), vt);
+    std::copy(B.vt_count.begin(), B.vt_count.end(), vt_count);
+    for (int i = 0; i < M.n; ++i) vt_min[i] = double(B.vt_min[i]);
+    std::copy(B.ee.begin(), B.ee.end(), ee);
+    std::copy(B.ee_count.begin(), B.ee_count.end(), ee_count);
+    for (int i = 0; i < M.E; ++i) ee_min[i] = double(B.ee_min[i]);
+    for (int k = 0; k < 4; ++k) flags[k] = B.flags[k];
+  };
+  if (precision == 64)
+    run(double());
+  else
+    run(float());
+  return 0;
+}
+
+// Self-contact pair terms. x/xa: 4 points (12 doubles). Vertex-triangle: x = (a, b, c, p), out = 4 forces
+// then 4 Hessians (48). Edge-edge: x = (e1.v0, e1.v1, e2.v0, e2.v1), out = 2 forces, 2 Hessians (24).
+// Return 1 when the pair is in contact.
+int oracle_sc_vt(int precision, const double* x, const double* xa, double radius, double ke, double kd, double mu,
+                 double eps, double dt, double* out) {
+  int hit = 0;
+  auto run = [&](auto tag) {
+    using R = decltype(tag);
+    V3<R> X[4], XA[4], f[4];
+    M3<R> H[4];
+    for (int k = 0; k < 4; ++k) X[k] = ld<R>(x, k), XA[k] = ld<R>(xa, k);
+    hit = sc_vt(X, XA, R(radius), R(ke), R(kd), R(mu), R(eps), R(dt), f, H);
+    for (int k = 0; k < 4; ++k) {
+      out[3 * k] = hit ? f[k].x : 0.0, out[3 * k + 1] = hit ? f[k].y : 0.0, out[3 * k + 2] = hit ? f[k].z : 0.0;
+      for (int i = 0; i < 9; ++i) out[12 + 9 * k + i] = hit ? double(H[k].m[i / 3][i % 3]) : 0.0;
+    }
+  };
+  if (precision == 64)
+    run(double());
+  else
+    run(float());
+  return hit;
+}
+
+int oracle_sc_ee(int precision, const double* x, const double* xa, double radius, double ke, double kd, double mu,
+                 double eps, double dt, double ee_eps, double* out) {
+  int hit = 0;
+  auto run = [&](auto tag) {
+    using R = decltype(tag);
+    V3<R> X[4], XA[4], f[2];
+    M3<R> H[2];
+    for (int k = 0; k < 4; ++k) X[k] = ld<R>(x, k), XA[k] = ld<R>(xa, k);
+    hit = sc_ee(X, XA, R(radius), R(ke), R(kd), R(mu), R(eps), R(dt), R(ee_eps), f, H);
+    for (int k = 0; k < 2; ++k) {
+      out[3 * k] = hit ? f[k].x : 0.0, out[3 * k + 1] = hit ? f[k].y : 0.0, out[3 * k + 2] = hit ? f[k].z : 0.0;
+      for (int i = 0; i < 9; ++i) out[6 + 9 * k + i] = hit ? double(H[k].m[i / 3][i % 3]) : 0.0;
+    }
+  };
+  if (precision == 64)
+    run(double());
+  else
+    run(float());
+  return hit;
+}
+
+// Division plane of a pair and the step fractions of its four vertices. kind 0: vertex-triangle,
+// x = (v, t1, t2, t3); kind 1: edge-edge. out = dummy[4], n[3], d[3], t[4] (14 doubles).
+int oracle_sc_plane(int precision, int kind, const double* x, const double* dx, double eps, double gamma, double* out) {
+  auto run = [&](auto tag) {
+    using R = decltype(tag);
+    V3<R> X[4], DX[4], n, d;
+    bool dummy[4];
+    for (int k = 0; k < 4; ++k) X[k] = ld<R>(x, k), DX[k] = ld<R>(dx, k);
+    if (kind == 0)
+      vt_plane(X, DX, dummy, n, d);
+    else
+      ee_plane(X, DX, dummy, n, d);
+    for (int k = 0; k < 4; ++k) out[k] = dummy[k] ? 1.0 : 0.0;
+    out[4] = n.x, out[5] = n.y, out[6] = n.z, out[7] = d.x, out[8] = d.y, out[9] = d.z;
+    for (int k = 0; k < 4; ++k) out[10 + k] = plane_t(X[k], DX[k], n, d, R(eps), R(gamma));
+  };
+  if (precision == 64)
+    run(double());
+  else
+    run(float());
+  return 0;
+}
+
+// Closest point on a triangle: x = (a, b, c, p); out = point[3], bary[3], feature.
+int oracle_tri_closest(const double* x, double* out) {
+  double bary[3];
+  int feat;
+  V3<double> c = tri_closest(ld<double>(x, 0), ld<double>(x, 1), ld<double>(x, 2), ld<double>(x, 3), bary, feat);
+  out[0] = c.x, out[1] = c.y, out[2] = c.z, out[3] = bary[0], out[4] = bary[1], out[5] = bary[2], out[6] = feat;
+  return 0;
+}
+
+// Closest points of two segments: x = (p1, q1, p2, q2); out = s, t, distance.
+int oracle_edge_closest(const double* x, double eps, double* out) {
+  edge_closest(ld<double>(x, 0), ld<double>(x, 1), ld<double>(x, 2), ld<double>(x, 3), eps, out[0], out[1], out[2]);
+  return 0;
+}
+
+// dE/dd and d2E/dd2 of the self-contact barrier.
+int oracle_sc_norm(double dis, double radius, double k, double* out) {
+  sc_norm(dis, radius, k, out[0], out[1]);
+  return 0;
 }
 
 // Element-level entry points (force 3 + Hessian 9 written to out[12]).

@@ -43,6 +43,44 @@ class OracleContacts(C.Structure):
     ]  # fmt: skip
 
 
+class OracleSelfContact(C.Structure):
+    _fields_ = [
+        ("radius", C.c_double), ("margin", C.c_double), ("relaxation", C.c_double),
+        ("edge_parallel_epsilon", C.c_double), ("rest_exclusion", C.c_double), ("vertex_buffer", C.c_int),
+        ("edge_buffer", C.c_int), ("interval", C.c_int), ("rest_q", _dp), ("vt_filter_offsets", _ip),
+        ("vt_filter", _ip), ("ee_filter_offsets", _ip), ("ee_filter", _ip),
+    ]  # fmt: skip
+
+
+class SelfContact:
+    """Self-contact settings with the ``SolverVBD`` keyword meanings (``solver_vbd.py:204-216``).
+    ``vt_filter`` / ``ee_filter`` are (flat, offsets) CSR lists of filtered triangles per vertex and
+    filtered edges per edge, each row sorted, or None."""
+
+    def __init__(self, rest_q, *, radius, margin, relaxation=0.85, vertex_buffer=32, edge_buffer=64, interval=0,
+                 edge_parallel_epsilon=1e-5, rest_exclusion=0.0, vt_filter=None, ee_filter=None):  # fmt: skip
+        self._keep = []
+
+        def ints(a):
+            if a is None:
+                return None
+            arr, ptr = _i(a)
+            self._keep.append(arr)
+            return ptr
+
+        rq, rqp = _d(np.asarray(rest_q).reshape(-1))
+        self._keep.append(rq)
+        vf, vfo = vt_filter if vt_filter is not None else (None, None)
+        ef, efo = ee_filter if ee_filter is not None else (None, None)
+        self.vertex_buffer, self.edge_buffer = int(vertex_buffer), int(edge_buffer)
+        self.s = OracleSelfContact(
+            radius=radius, margin=margin, relaxation=relaxation, edge_parallel_epsilon=edge_parallel_epsilon,
+            rest_exclusion=rest_exclusion, vertex_buffer=self.vertex_buffer, edge_buffer=self.edge_buffer,
+            interval=int(interval), rest_q=rqp, vt_filter_offsets=ints(vfo), vt_filter=ints(vf),
+            ee_filter_offsets=ints(efo), ee_filter=ints(ef),
+        )  # fmt: skip
+
+
 def build() -> str:
     """Compile the oracle library with ``make`` (idempotent)."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
@@ -67,6 +105,19 @@ def lib():
             C.c_int, _dp, _dp, _ip, C.c_int, _ip, _dp, _dp, C.c_double, C.c_int, _ip, _ip, _dp, _dp, _dp,
         ]  # fmt: skip
         _lib.oracle_max_threads.restype = C.c_int
+        _lib.oracle_vbd_step_sc.argtypes = [
+            C.POINTER(OracleModel), _dp, _dp, _dp, C.POINTER(OracleContacts), C.POINTER(OracleSelfContact), C.c_double,
+            C.c_int, _dp, _dp, C.c_int, C.c_int,
+        ]  # fmt: skip
+        _lib.oracle_collide.argtypes = [
+            C.POINTER(OracleModel), C.POINTER(OracleSelfContact), _dp, C.c_int, _ip, _ip, _dp, _ip, _ip, _dp, _ip, C.c_int,
+        ]  # fmt: skip
+        _lib.oracle_sc_vt.argtypes = [C.c_int, _dp, _dp] + [C.c_double] * 6 + [_dp]
+        _lib.oracle_sc_ee.argtypes = [C.c_int, _dp, _dp] + [C.c_double] * 7 + [_dp]
+        _lib.oracle_sc_plane.argtypes = [C.c_int, C.c_int, _dp, _dp, C.c_double, C.c_double, _dp]
+        _lib.oracle_tri_closest.argtypes = [_dp, _dp]
+        _lib.oracle_edge_closest.argtypes = [_dp, C.c_double, _dp]
+        _lib.oracle_sc_norm.argtypes = [C.c_double, C.c_double, C.c_double, _dp]
     return _lib
 
 
@@ -149,7 +200,8 @@ def make_contacts(count, particle, shape, body_pos, body_vel, normal):
     return c, keep
 
 
-def step(model: Model, q_in, qd_in, f_ext, contacts=None, dt=1.0 / 600.0, iterations=10, precision=64, nthreads=1):
+def step(model: Model, q_in, qd_in, f_ext, contacts=None, dt=1.0 / 600.0, iterations=10, precision=64, nthreads=1,
+         self_contact: SelfContact | None = None):  # fmt: skip
     """One VBD step. Returns (q_in_after, q_out, qd_out), mirroring the reference's state side effects."""
     n = model.n
     q, qp = _d(np.array(q_in, dtype=np.float64).reshape(-1))
@@ -160,7 +212,12 @@ def step(model: Model, q_in, qd_in, f_ext, contacts=None, dt=1.0 / 600.0, iterat
     if contacts is None:
         contacts = make_contacts(0, np.zeros(1), np.zeros(1), np.zeros(3), np.zeros(3), np.zeros(3))
     c, _keep = contacts
-    rc = lib().oracle_vbd_step(C.byref(model.s), qp, qdp, fp, C.byref(c), dt, iterations, qop, vop, precision, nthreads)
+    if self_contact is None:
+        rc = lib().oracle_vbd_step(C.byref(model.s), qp, qdp, fp, C.byref(c), dt, iterations, qop, vop, precision,
+                                   nthreads)  # fmt: skip
+    else:
+        rc = lib().oracle_vbd_step_sc(C.byref(model.s), qp, qdp, fp, C.byref(c), C.byref(self_contact.s), dt,
+                                      iterations, qop, vop, precision, nthreads)  # fmt: skip
     if rc != 0:
         raise RuntimeError(f"oracle_vbd_step failed: {rc}")
     return q.reshape(-1, 3), qo.reshape(-1, 3), vo.reshape(-1, 3)
@@ -207,3 +264,62 @@ def element(kind, precision, *args):
     else:
         raise ValueError(kind)
     return out[:3].copy(), out[3:].reshape(3, 3).copy()
+
+
+def collide(model: Model, sc: SelfContact, q, precision=64, nthreads=1) -> dict:
+    """One self-contact detection at positions q; the buffers of ``TriMeshCollisionInfo``."""
+    n, E = model.n, model.s.E
+    qq, qp = _d(np.asarray(q).reshape(-1))
+    vt, vtp = _i(np.zeros(2 * n * sc.vertex_buffer))
+    vc, vcp = _i(np.zeros(n))
+    vm, vmp = _d(np.zeros(n))
+    ee, eep = _i(np.zeros(max(2 * E * sc.edge_buffer, 1)))
+    ec, ecp = _i(np.zeros(max(E, 1)))
+    em, emp = _d(np.zeros(max(E, 1)))
+    fl, flp = _i(np.zeros(4))
+    lib().oracle_collide(C.byref(model.s), C.byref(sc.s), qp, precision, vtp, vcp, vmp, eep, ecp, emp, flp, nthreads)
+    return {"vt": vt, "vt_count": vc, "vt_min": vm, "ee": ee[: 2 * E * sc.edge_buffer], "ee_count": ec[:E],
+            "ee_min": em[:E], "resize_flags": fl}  # fmt: skip
+
+
+def sc_pair(kind, precision, x, xa, radius, ke, kd, mu, eps, dt, ee_eps=1e-5):
+    """Self-contact pair term. kind "vt": x = (a, b, c, p) -> forces (4, 3), Hessians (4, 3, 3);
+    kind "ee": x = (e1.v0, e1.v1, e2.v0, e2.v1) -> forces (2, 3), Hessians (2, 3, 3) of e1's vertices."""
+    x_, xp = _d(np.asarray(x).reshape(-1))
+    a_, ap = _d(np.asarray(xa).reshape(-1))
+    if kind == "vt":
+        out, op = _d(np.zeros(48))
+        hit = lib().oracle_sc_vt(precision, xp, ap, radius, ke, kd, mu, eps, dt, op)
+        return bool(hit), out[:12].reshape(4, 3), out[12:].reshape(4, 3, 3)
+    out, op = _d(np.zeros(24))
+    hit = lib().oracle_sc_ee(precision, xp, ap, radius, ke, kd, mu, eps, dt, ee_eps, op)
+    return bool(hit), out[:6].reshape(2, 3), out[6:].reshape(2, 3, 3)
+
+
+def sc_plane(kind, precision, x, dx, eps=1e-5, gamma=0.85):
+    """Division plane of a pair: (dummy[4], n, d, t[4]); kind "vt": x = (v, t1, t2, t3), "ee": two edges."""
+    x_, xp = _d(np.asarray(x).reshape(-1))
+    d_, dp = _d(np.asarray(dx).reshape(-1))
+    out, op = _d(np.zeros(14))
+    lib().oracle_sc_plane(precision, 0 if kind == "vt" else 1, xp, dp, eps, gamma, op)
+    return out[:4] != 0.0, out[4:7], out[7:10], out[10:14]
+
+
+def tri_closest(a, b, c, p):
+    x_, xp = _d(np.concatenate([a, b, c, p]))
+    out, op = _d(np.zeros(7))
+    lib().oracle_tri_closest(xp, op)
+    return out[:3], out[3:6], int(out[6])
+
+
+def edge_closest(p1, q1, p2, q2, eps=1e-5):
+    x_, xp = _d(np.concatenate([p1, q1, p2, q2]))
+    out, op = _d(np.zeros(3))
+    lib().oracle_edge_closest(xp, eps, op)
+    return out
+
+
+def sc_norm(dis, radius, k):
+    out, op = _d(np.zeros(2))
+    lib().oracle_sc_norm(dis, radius, k, op)
+    return out[0], out[1]

@@ -723,7 +723,7 @@ def selfcontact_cases(ns, seed=11):
         d = [5e-6, 0.004, 0.013, 0.025][i % 4] * (1.0 if i % 8 < 4 else -1.0)
         p = w[0] * a + w[1] * b + w[2] * c + n * d
         X = np.stack([a, b, c, p])
-        Xa = X + rng.normal(scale=[1e-3, 1e-5, 0.0][i % 3], size=(4, 3))
+        Xa = X + rng.normal(scale=[1e-3, 1e-5, 1e-7][i % 3], size=(4, 3))
         res = ns["evaluate_vertex_triangle_collision_force_hessian_4_vertices"](
             3, 0, wp.vec_array(X), wp.vec_array(Xa), wp.array2d([[0, 1, 2]], int), radius, ke, kd, mu, eps, dt)
         fs = np.concatenate([np.asarray(res[1 + k].a) for k in range(4)])
@@ -750,7 +750,7 @@ def selfcontact_cases(ns, seed=11):
         p2 = p2c - dir2 * 0.05 * t0
         q2 = p2 + dir2 * 0.05
         X = np.stack([p1, q1, p2, q2])
-        Xa = X + rng.normal(scale=[1e-3, 1e-5, 0.0][i % 3], size=(4, 3))
+        Xa = X + rng.normal(scale=[1e-3, 1e-5, 1e-7][i % 3], size=(4, 3))
         edges = wp.array2d([[-1, -1, 0, 1], [-1, -1, 2, 3]], int)
         res = ns["evaluate_edge_edge_contact_2_vertices"](0, 1, wp.vec_array(X), wp.vec_array(Xa), edges, radius, ke, kd,
                                                           mu, eps, dt, 1e-5)  # fmt: skip
