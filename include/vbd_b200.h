@@ -220,6 +220,76 @@ int vbd_step_noalloc(const VbdModelDesc* model, const VbdRefAdjacency* adjacency
                      float* qd_out_dev, const float* particle_f_dev, const VbdContactsDesc* contacts, float dt,
                      void* stream);
 
+/* ---------------------------------------------------------------- particle self-contact */
+
+/* Self-contact settings, with the meaning of the SolverVBD keywords (solver_vbd.py:204-216). */
+typedef struct VbdSelfContactDesc {
+  double radius;                /* particle_self_contact_radius: contact distance of the barrier */
+  double margin;                /* particle_self_contact_margin: detection distance (>= radius) */
+  double relaxation;            /* particle_conservative_bound_relaxation (gamma of the truncation) */
+  double edge_parallel_epsilon; /* particle_edge_parallel_epsilon */
+  double rest_exclusion_radius; /* particle_rest_shape_contact_exclusion_radius (0 = off) */
+  int32_t vertex_buffer_size;   /* particle_vertex_contact_buffer_size: triangles kept per vertex */
+  int32_t edge_buffer_size;     /* particle_edge_contact_buffer_size: edges kept per edge */
+  int32_t detection_interval;   /* particle_collision_detection_interval */
+  const float* rest_q_dev;      /* [V,3] Model.particle_q (rest shape); read when rest_exclusion_radius > 0 */
+  /* collision filters (vbd_build_contact_filters plus the external filtering maps), CSR, or NULL */
+  const int32_t* vt_filter_offsets_host; /* [V+1] */
+  const int32_t* vt_filter_host;         /* triangles skipped per vertex */
+  const int32_t* ee_filter_offsets_host; /* [E+1] */
+  const int32_t* ee_filter_host;         /* edges skipped per edge */
+} VbdSelfContactDesc;
+
+/* Turns on particle self-contact for h (SolverVBD(particle_enable_self_contact=True),
+   solver_vbd.py:489-526): vertex-triangle and edge-edge barrier contact with damping and friction
+   (particle_vbd_kernels.py:1193-1779, accumulated per color as :1930-2071), with stiffness, damping and
+   friction taken from the model's soft_contact_ke/kd/mu as the reference does; collision detection
+   (tri_mesh_collision.py:333-413, geometry/kernels.py:1252-1497) at the start of each step and at the
+   iterations i with i % interval == 0 (interval 0: i == 0 only; negative: never), and the
+   penetration-free truncation after the forward step and after every color (particle_vbd_kernels.py:
+   2475-2897, solver_vbd.py:1669-1766, 2151-2337). Needs the per-color schedule with the CSR layout
+   (else VBD_ERR_UNSUPPORTED). Allocates its buffers here (synchronizes the device); VBD_ERR_TOO_LARGE
+   when V x vertex_buffer_size or E x edge_buffer_size reaches 2^29. A second call replaces the settings. */
+int vbd_set_self_contact(VbdHandle h, const VbdSelfContactDesc* desc);
+
+/* Pairs recorded by the last detection of h's step and its overflow flags (bit 0: a vertex had more
+   triangles than vertex_buffer_size, bit 2: an edge had more edges than edge_buffer_size; the
+   lowest ids are kept). Synchronizes the stream. */
+int vbd_get_self_contact_counts(VbdHandle h, int32_t* vt_pairs, int32_t* ee_pairs, int32_t* flags, void* stream);
+
+/* Topological collision filters of SolverVBD._compute_particle_contact_filtering_list for a threshold
+   ring >= 2 (build_vertex_n_ring_tris_collision_filter / build_edge_n_ring_edge_collision_filter,
+   particle_vbd_kernels.py:2107-2255): per vertex v the triangles incident to a vertex within ring - 1
+   edge steps of v other than v, less v's own triangles; per edge (a, b) the edges with an endpoint within
+   ring - 1 steps of a or b other than a and b, less the edges in which a or b takes any of the four
+   roles. Rows sorted. Call once with vt_list/ee_list NULL to get the offsets ([V+1], [E+1]), then with
+   lists of vt_offsets[V] and ee_offsets[E] ints. */
+int vbd_build_contact_filters(int32_t particle_count, int32_t tri_count, const int32_t* tri_indices_host,
+                              int32_t edge_count, const int32_t* edge_indices_host, int32_t ring,
+                              int32_t* vt_offsets_out, int32_t* vt_list_out, int32_t* ee_offsets_out,
+                              int32_t* ee_list_out);
+
+/* Stand-alone detector with the buffers of TriMeshCollisionDetector (tri_mesh_collision.py:91-413):
+   vertex_colliding_triangles (2 ints per slot: vertex, triangle; -1 when empty), its counts and
+   minimum distances, edge_colliding_edges likewise, and resize_flags (index 0 vertex, 2 edge overflow;
+   set, never cleared, as the reference does). Pairs closer than max_query_radius, not adjacent, not
+   filtered and, when min_query_radius > 0, not closer than that in ref_pos (the reference's
+   min_distance_filtering_ref_pos). Slots hold the lowest primitive ids in increasing order. */
+typedef struct VbdCollider* VbdColliderHandle;
+int vbd_collider_create(int32_t particle_count, int32_t tri_count, const int32_t* tri_indices_dev, int32_t edge_count,
+                        const int32_t* edge_indices_dev, int32_t vertex_buffer_size, int32_t edge_buffer_size,
+                        float edge_parallel_epsilon, const int32_t* vt_filter_offsets_host,
+                        const int32_t* vt_filter_host, const int32_t* ee_filter_offsets_host,
+                        const int32_t* ee_filter_host, VbdColliderHandle* out);
+/* what: bit 0 vertex-triangle (vertex_triangle_collision_detection), bit 1 edge-edge
+   (edge_edge_collision_detection). Outputs of a pass not asked for are not touched. */
+int vbd_collider_detect(VbdColliderHandle h, int32_t what, const float* pos_dev, float max_query_radius,
+                        float min_query_radius, const float* ref_pos_dev, int32_t* vertex_colliding_triangles_dev,
+                        int32_t* vertex_colliding_triangles_count_dev, float* vertex_colliding_triangles_min_dist_dev,
+                        int32_t* edge_colliding_edges_dev, int32_t* edge_colliding_edges_count_dev,
+                        float* edge_colliding_edges_min_dist_dev, int32_t* resize_flags_dev, void* stream);
+int vbd_collider_destroy(VbdColliderHandle h);
+
 /* ---------------------------------------------------------------- host-side model preparation */
 
 /* Particle coloring of the graph of ModelBuilder.color (builder.py:9304-9396,

@@ -80,6 +80,16 @@ class VbdRefAdjacency(C.Structure):
     _fields_ = [("face_offsets_dev", _vp), ("faces_dev", _vp), ("edge_offsets_dev", _vp), ("edges_dev", _vp)]
 
 
+class VbdSelfContactDesc(C.Structure):
+    _fields_ = [
+        ("radius", C.c_double), ("margin", C.c_double), ("relaxation", C.c_double),
+        ("edge_parallel_epsilon", C.c_double), ("rest_exclusion_radius", C.c_double),
+        ("vertex_buffer_size", C.c_int32), ("edge_buffer_size", C.c_int32), ("detection_interval", C.c_int32),
+        ("rest_q_dev", _vp), ("vt_filter_offsets_host", _ip), ("vt_filter_host", _ip),
+        ("ee_filter_offsets_host", _ip), ("ee_filter_host", _ip),
+    ]  # fmt: skip
+
+
 # every symbol the header declares, with its ctypes signature
 SIGNATURES = {
     "vbd_create": ([C.POINTER(VbdModelDesc), C.POINTER(VbdSolverParams), C.POINTER(_vp)], C.c_int),
@@ -109,6 +119,18 @@ SIGNATURES = {
          C.POINTER(VbdContactsDesc), C.c_float, _vp],
         C.c_int,
     ),
+    "vbd_set_self_contact": ([_vp, C.POINTER(VbdSelfContactDesc)], C.c_int),
+    "vbd_get_self_contact_counts": ([_vp, _ip, _ip, _ip, _vp], C.c_int),
+    "vbd_build_contact_filters": ([C.c_int32, C.c_int32, _ip, C.c_int32, _ip, C.c_int32, _ip, _ip, _ip, _ip], C.c_int),
+    "vbd_collider_create": (
+        [C.c_int32, C.c_int32, _vp, C.c_int32, _vp, C.c_int32, C.c_int32, C.c_float, _ip, _ip, _ip, _ip, C.POINTER(_vp)],
+        C.c_int,
+    ),
+    "vbd_collider_detect": (
+        [_vp, C.c_int32, _vp, C.c_float, C.c_float, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+        C.c_int,
+    ),
+    "vbd_collider_destroy": ([_vp], C.c_int),
     "vbd_soft_contacts": (
         [C.c_int32, _vp, _vp, _vp, C.c_int32, _ip, _fp, _fp, _fp, C.c_float, C.c_int32, _vp, _vp, _vp, _vp, _vp,
          _vp, _vp],
@@ -150,6 +172,6 @@ def check(rc: int, what: str):
         VBD_ERR_OUT_OF_MEMORY: "out of device memory",
         VBD_ERR_UNSUPPORTED: "unsupported",
         VBD_ERR_EMPTY_COLORING: "empty coloring",
-        VBD_ERR_TOO_LARGE: "model exceeds the no-allocation scratch",
+        VBD_ERR_TOO_LARGE: "model too large for the fixed buffers",
     }
     raise VbdError(f"{what} failed: {names.get(rc, rc)} ({rc})")

@@ -14,6 +14,7 @@
 
 #include "vbd_b200.h"
 #include "vbd_adjoint.cuh"
+#include "vbd_collide.cuh"
 #include "vbd_ell.cuh"
 
 using namespace vbd;
@@ -105,6 +106,17 @@ __global__ void k_soft_contacts(int n, const float* __restrict__ q, const float*
 
 }  // namespace
 
+namespace {
+void sc_release(ScBuffers& b) {
+  void* ps[] = {b.bcount, b.bstart, b.ekey, b.eprim, b.blo, b.bhi, b.stats, b.vt_tri, b.vt_count, b.vt_min,
+                b.ee_edge, b.ee_count, b.ee_min, b.flags, b.tmp, b.vt_off, b.vt_pairs, b.ee_off, b.ee_pairs,
+                b.ent_cnt, b.ent_off, b.ent, b.vt_foff, b.vt_f, b.ee_foff, b.ee_f, b.scan_tmp};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  b = ScBuffers();
+}
+}  // namespace
+
 struct VbdSolver {
   VbdModelDesc md;
   VbdSolverParams prm;
@@ -162,15 +174,23 @@ struct VbdSolver {
   size_t adj_work_bytes = 0;
   // host copies of the topology (for re-packing the ELL records)
   std::vector<int> h_tri, h_edges, h_foff, h_fadj, h_eoff, h_eadj;
+  // particle self-contact (vbd_set_self_contact)
+  bool sc_on = false;
+  ScBuffers sc;
+  double sc_radius = 0, sc_margin = 0, sc_relax = 0.85, sc_ee_eps = 1e-5, sc_rest_excl = 0;
+  int sc_interval = 0;
+  const float* sc_rest_q = nullptr;
+  void *sc_pos_cd = nullptr, *sc_disp = nullptr, *sc_ts = nullptr;
 
   ~VbdSolver() {
     void* ps[] = {tri_idx, tri_pose, tri_mat, edge_idx, edge_prop, face_off, face_adj, edge_off, edge_adj,
                   inst_order, inst_vstart, inst_cptr, color_ranges, color_verts, queue, pos, qprev, inertia,
                   slot_cnt, slots, c_k, c_ke, c_kd, c_mu, err, residual, range_nf, range_ne, range_fbase,
                   range_ebase, face_nb, face_dm, face_mat, face_kd, hinge_idx, hinge_prop, hinge_kd, adj_work,
-                  ell16_faceA, ell16_faceB, ell16_hinge};
+                  ell16_faceA, ell16_faceB, ell16_hinge, sc_pos_cd, sc_disp, sc_ts};
     for (void* p : ps)
       if (p) cudaFree(p);
+    sc_release(sc);
   }
 };
 
@@ -474,6 +494,7 @@ StepCtx<R> make_ctx(VbdSolver* h) {
   c.residual = MODE == MODE_MIXED ? h->residual : nullptr;
   c.V = h->V;
   c.S = h->S;
+  c.dual_in_solve = 1;
   return c;
 }
 
@@ -540,6 +561,184 @@ void launch_persistent_ell(int occ, const StepCtx<R>& c, const PersistentPlan& p
     case 3: k_persistent_ell<R, MODE, SMEM, 3><<<grid, block, smem, st>>>(c, p, e); break;
     case 4: k_persistent_ell<R, MODE, SMEM, 4><<<grid, block, smem, st>>>(c, p, e); break;
     default: k_persistent_ell<R, MODE, SMEM, 0><<<grid, block, smem, st>>>(c, p, e); break;
+  }
+}
+
+// ------------------------------------------------------------------------------ self-contact (host)
+struct ScSetup {
+  double margin, rest_excl, ee_eps;
+  const float* rest_q;
+  int* err;
+};
+
+// Buffers of one detector for V particles, T triangles and E edges (positions of type R).
+template <typename R>
+int sc_alloc(ScBuffers& b, int V, int T, int E, int vb, int eb) {
+  int rc;
+  b.V = V, b.T = T, b.E = E, b.vb = vb, b.eb = eb;
+  const int P = std::max(T, E);
+  int nb = 1024;
+  while (nb < 4 * P && nb < (1 << 30)) nb <<= 1;
+  b.nbuckets = nb;
+  b.gcap = 8LL * std::max(P, 1);
+  b.ecap = 4LL * V * vb + 2LL * E * eb;
+  if ((rc = dalloc(&b.bcount, size_t(nb) + 1)) || (rc = dalloc(&b.bstart, size_t(nb) + 1)) ||
+      (rc = dalloc(&b.ekey, size_t(b.gcap))) || (rc = dalloc(&b.eprim, size_t(b.gcap))) ||
+      (rc = dalloc((pos4_t<R>**)&b.blo, size_t(std::max(P, 1)))) ||
+      (rc = dalloc((pos4_t<R>**)&b.bhi, size_t(std::max(P, 1)))) || (rc = dalloc(&b.stats, 4)) ||
+      (rc = dalloc(&b.vt_tri, size_t(V) * vb)) || (rc = dalloc(&b.vt_count, size_t(V))) ||
+      (rc = dalloc((R**)&b.vt_min, size_t(V))) || (rc = dalloc(&b.ee_edge, size_t(E) * eb)) ||
+      (rc = dalloc(&b.ee_count, size_t(E))) || (rc = dalloc((R**)&b.ee_min, size_t(E))) ||
+      (rc = dalloc(&b.flags, 4)) || (rc = dalloc(&b.tmp, size_t(std::max(V, E)) + 1)) ||
+      (rc = dalloc(&b.vt_off, size_t(V) + 1)) || (rc = dalloc(&b.vt_pairs, size_t(V) * vb)) ||
+      (rc = dalloc(&b.ee_off, size_t(E) + 1)) || (rc = dalloc(&b.ee_pairs, size_t(E) * eb)) ||
+      (rc = dalloc(&b.ent_cnt, size_t(V) + 1)) || (rc = dalloc(&b.ent_off, size_t(V) + 1)) ||
+      (rc = dalloc(&b.ent, size_t(b.ecap))))
+    return rc;
+  size_t b1 = 0, b2 = 0;
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, b1, b.bcount, b.bstart, nb + 1));
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, b2, b.tmp, b.vt_off, std::max(V, E) + 1));
+  b.scan_bytes = std::max(b1, b2);
+  if ((rc = dalloc((char**)&b.scan_tmp, b.scan_bytes))) return rc;
+  CK(cudaMemset(b.flags, 0, 4 * sizeof(int)));
+  return VBD_OK;
+}
+
+template <typename T>
+int scan(ScBuffers& b, const T* in, T* out, int n, cudaStream_t st) {
+  size_t bytes = b.scan_bytes;
+  CK(cub::DeviceScan::ExclusiveSum(b.scan_tmp, bytes, in, out, n, st));
+  return VBD_OK;
+}
+
+// One detection at positions pos (grid build + narrow phase for triangles, then edges).
+template <typename R>
+int sc_detect(ScBuffers& b, const ScSetup& p, const int4* tri_idx, const int4* edge_idx, const pos4_t<R>* pos,
+              int what, cudaStream_t st) {
+  ScQuery q;
+  q.V = b.V, q.T = b.T, q.E = b.E, q.vb = b.vb, q.eb = b.eb, q.nb = b.nbuckets;
+  q.margin = float(p.margin), q.rest_excl = float(p.rest_excl), q.ee_eps = float(p.ee_eps);
+  q.tri_idx = tri_idx, q.edge_idx = edge_idx, q.rest_q = p.rest_q;
+  q.vt_foff = b.vt_foff, q.vt_f = b.vt_f, q.ee_foff = b.ee_foff, q.ee_f = b.ee_f;
+  q.bstart = b.bstart, q.ekey = b.ekey, q.eprim = b.eprim, q.stats = b.stats, q.flags = b.flags;
+  q.gcap = (unsigned)std::min<long long>(b.gcap, 0xFFFFFFFFLL);
+  pos4_t<R>* lo = (pos4_t<R>*)b.blo;
+  pos4_t<R>* hi = (pos4_t<R>*)b.bhi;
+  for (int kind = 0; kind < 2; ++kind) {
+    if (!(what & (1 << kind))) continue;
+    const int P = kind == 0 ? b.T : b.E;
+    const int Q = kind == 0 ? b.V : b.E;
+    if (Q == 0) continue;
+    if (P == 0) {  // nothing to collide with
+      CK(cudaMemsetAsync(kind == 0 ? b.vt_count : b.ee_count, 0, sizeof(int) * Q, st));
+      k_sc_fill<R><<<(Q + 255) / 256, 256, 0, st>>>(Q, (R*)(kind == 0 ? b.vt_min : b.ee_min), R(p.margin));
+      continue;
+    }
+    CK(cudaMemsetAsync(b.stats, 0, 2 * sizeof(double), st));
+    k_sc_boxes<R><<<(P + 255) / 256, 256, 0, st>>>(kind, P, pos, tri_idx, edge_idx, lo, hi, b.stats);
+    k_sc_cell<<<1, 1, 0, st>>>(b.stats, P, p.margin);
+    CK(cudaMemsetAsync(b.bcount, 0, sizeof(unsigned) * (size_t(b.nbuckets) + 1), st));
+    k_sc_grid<R, false><<<(P + 255) / 256, 256, 0, st>>>(P, lo, hi, b.stats, b.nbuckets, b.bcount, nullptr, nullptr,
+                                                          nullptr, 0, b.flags);
+    int rc = scan<unsigned>(b, b.bcount, b.bstart, b.nbuckets + 1, st);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(b.bcount, 0, sizeof(unsigned) * (size_t(b.nbuckets) + 1), st));
+    k_sc_grid<R, true><<<(P + 255) / 256, 256, 0, st>>>(P, lo, hi, b.stats, b.nbuckets, b.bcount, b.bstart, b.ekey,
+                                                         b.eprim, b.gcap, b.flags);
+    if (kind == 0)
+      k_sc_query_vt<R><<<(Q + 127) / 128, 128, 0, st>>>(q, pos, lo, hi, b.vt_tri, b.vt_count, (R*)b.vt_min);
+    else
+      k_sc_query_ee<R><<<(Q + 127) / 128, 128, 0, st>>>(q, pos, lo, hi, b.ee_edge, b.ee_count, (R*)b.ee_min);
+  }
+  CK(cudaGetLastError());
+  return VBD_OK;
+}
+
+// Dense pair lists and per-vertex entry lists of the last detection.
+int sc_compact(ScBuffers& b, const int4* tri_idx, const int4* edge_idx, cudaStream_t st) {
+  int rc;
+  k_sc_stored<<<(b.V + 256) / 256, 256, 0, st>>>(b.V, b.vb, b.vt_count, b.tmp);
+  if ((rc = scan<int>(b, b.tmp, b.vt_off, b.V + 1, st))) return rc;
+  if (b.V) k_sc_pairs<<<(b.V + 255) / 256, 256, 0, st>>>(b.V, b.vb, b.vt_count, b.vt_tri, b.vt_off, b.vt_pairs);
+  k_sc_stored<<<(b.E + 256) / 256, 256, 0, st>>>(b.E, b.eb, b.ee_count, b.tmp);
+  if ((rc = scan<int>(b, b.tmp, b.ee_off, b.E + 1, st))) return rc;
+  if (b.E) k_sc_pairs<<<(b.E + 255) / 256, 256, 0, st>>>(b.E, b.eb, b.ee_count, b.ee_edge, b.ee_off, b.ee_pairs);
+  CK(cudaMemsetAsync(b.ent_cnt, 0, sizeof(int) * (size_t(b.V) + 1), st));
+  k_sc_entries<false><<<kScGridBlocks, 256, 0, st>>>(tri_idx, edge_idx, b.vt_off + b.V, b.ee_off + b.E, b.vt_pairs,
+                                                      b.ee_pairs, b.ent_cnt, nullptr, nullptr, 0, b.flags);
+  if ((rc = scan<int>(b, b.ent_cnt, b.ent_off, b.V + 1, st))) return rc;
+  CK(cudaMemsetAsync(b.ent_cnt, 0, sizeof(int) * (size_t(b.V) + 1), st));
+  k_sc_entries<true><<<kScGridBlocks, 256, 0, st>>>(tri_idx, edge_idx, b.vt_off + b.V, b.ee_off + b.E, b.vt_pairs,
+                                                     b.ee_pairs, b.ent_cnt, b.ent_off, b.ent, b.ecap, b.flags);
+  k_sc_sort_entries<<<(b.V + 127) / 128, 128, 0, st>>>(b.V, b.ent_off, b.ent);
+  CK(cudaGetLastError());
+  return VBD_OK;
+}
+
+// Copies a host CSR filter (rows sorted here) to the device; rows = number of rows, ids < limit.
+int sc_upload_filter(const int32_t* off_h, const int32_t* list_h, int rows, int limit, int** off_d, int** list_d) {
+  *off_d = nullptr, *list_d = nullptr;
+  if (!off_h) return VBD_OK;
+  if (off_h[0] != 0) return VBD_ERR_INVALID_ARGUMENT;
+  for (int i = 0; i < rows; ++i)
+    if (off_h[i + 1] < off_h[i]) return VBD_ERR_INVALID_ARGUMENT;
+  const int n = off_h[rows];
+  if (n > 0 && !list_h) return VBD_ERR_INVALID_ARGUMENT;
+  std::vector<int> off(off_h, off_h + rows + 1), list(list_h, list_h + n);
+  for (int v : list)
+    if (v < 0 || v >= limit) return VBD_ERR_INVALID_ARGUMENT;
+  for (int i = 0; i < rows; ++i) std::sort(list.begin() + off[i], list.begin() + off[i + 1]);
+  int rc = upload(off_d, off);
+  if (rc) return rc;
+  if (list.empty()) list.push_back(0);
+  return upload(list_d, list);
+}
+
+ScSetup sc_setup(VbdSolver* h) { return {h->sc_margin, h->sc_rest_excl, h->sc_ee_eps, h->sc_rest_q, h->err}; }
+
+// _collision_detection_penetration_free: positions at detection, zero displacements, detect, compact.
+template <typename R>
+int sc_collide(VbdSolver* h, const R* q_state, cudaStream_t st) {
+  pos4_t<R>* pcd = (pos4_t<R>*)h->sc_pos_cd;
+  pos4_t<R>* dsp = (pos4_t<R>*)h->sc_disp;
+  if (q_state)
+    k_sc_begin_from_state<R><<<(h->V + 255) / 256, 256, 0, st>>>(h->V, q_state, pcd, dsp);
+  else
+    k_sc_begin_from_pos<R><<<(h->V + 255) / 256, 256, 0, st>>>(h->V, (const pos4_t<R>*)h->pos, pcd, dsp);
+  int rc = sc_detect<R>(h->sc, sc_setup(h), h->tri_idx, h->edge_idx, pcd, 3, st);
+  if (rc) return rc;
+  return sc_compact(h->sc, h->tri_idx, h->edge_idx, st);
+}
+
+// _penetration_free_truncation with self-contact on.
+template <typename R>
+void sc_truncate(VbdSolver* h, cudaStream_t st) {
+  ScBuffers& b = h->sc;
+  k_sc_trunc_pairs<R><<<kScGridBlocks, 256, 0, st>>>(h->tri_idx, h->edge_idx, b.vt_off + b.V, b.ee_off + b.E,
+                                                      b.vt_pairs, b.ee_pairs, (const pos4_t<R>*)h->sc_pos_cd,
+                                                      (const pos4_t<R>*)h->sc_disp, R(h->sc_ee_eps), R(h->sc_relax),
+                                                      (R*)h->sc_ts);
+  k_sc_trunc_apply<R><<<(h->V + 255) / 256, 256, 0, st>>>(h->V, (R*)h->sc_ts, R(h->sc_margin * h->sc_relax * 0.5),
+                                                           (const pos4_t<R>*)h->sc_pos_cd, (pos4_t<R>*)h->sc_disp,
+                                                           (pos4_t<R>*)h->pos);
+}
+
+template <typename R, int MODE, int L>
+void launch_color_sc(const StepCtx<R>& c, const int* verts, int n, int it, int block, cudaStream_t st) {
+  const long threads = long(n) * L;
+  const int grid = int((threads + block - 1) / block);
+  if (grid > 0) k_color<R, L, MODE, true><<<grid, block, 0, st>>>(c, verts, n, it);
+}
+
+template <typename R, int MODE>
+void launch_color_sc_any(int L, const StepCtx<R>& c, const int* verts, int n, int it, int block, cudaStream_t st) {
+  switch (L) {
+    case 1: launch_color_sc<R, MODE, 1>(c, verts, n, it, block, st); break;
+    case 2: launch_color_sc<R, MODE, 2>(c, verts, n, it, block, st); break;
+    case 4: launch_color_sc<R, MODE, 4>(c, verts, n, it, block, st); break;
+    case 8: launch_color_sc<R, MODE, 8>(c, verts, n, it, block, st); break;
+    case 16: launch_color_sc<R, MODE, 16>(c, verts, n, it, block, st); break;
+    default: launch_color_sc<R, MODE, 32>(c, verts, n, it, block, st); break;
   }
 }
 
@@ -634,6 +833,37 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
     } else {
       launch_persistent<R, MODE, false>(h->L, c, p, h->grid_persistent, h->block, 0, st);
     }
+  } else if (h->sc_on) {
+    // self-contact (solver_vbd.py:1731-1766, 2151-2337): detection at the step's start positions, forward
+    // step, truncation; per iteration an optional re-detection, then per color the solve and a truncation
+    c.disp = (pos4_t<R>*)h->sc_disp;
+    c.pos_cd = (pos4_t<R>*)h->sc_pos_cd;
+    c.ent_off = h->sc.ent_off;
+    c.ent = h->sc.ent;
+    c.vt_pairs = h->sc.vt_pairs;
+    c.ee_pairs = h->sc.ee_pairs;
+    c.sc_radius = h->sc_radius;
+    c.sc_ee_eps = h->sc_ee_eps;
+    const bool sep_duals = has_c && c.beta != R(0);
+    c.dual_in_solve = sep_duals ? 0 : 1;
+    int rc = sc_collide<R>(h, q_in, st);
+    if (rc) return rc;
+    k_forward<R><<<(h->V + 255) / 256, 256, 0, st>>>(c);
+    if (has_c) k_contact_prepare<R><<<(c.c_max + 255) / 256, 256, 0, st>>>(c);
+    sc_truncate<R>(h, st);
+    const int* cp = h->md.color_particles_dev;
+    for (int it = 0; it < iters; ++it) {
+      if (sep_duals) k_contact_duals<R><<<(c.c_max + 255) / 256, 256, 0, st>>>(c);
+      if ((h->sc_interval == 0 && it == 0) || (h->sc_interval >= 1 && it % h->sc_interval == 0)) {
+        if ((rc = sc_collide<R>(h, nullptr, st))) return rc;
+      }
+      for (size_t col = 0; col + 1 < h->color_offsets.size(); ++col) {
+        const int a = h->color_offsets[col], b = h->color_offsets[col + 1];
+        launch_color_sc_any<R, MODE>(h->L, c, cp + a, b - a, it, h->block, st);
+        sc_truncate<R>(h, st);
+      }
+    }
+    k_finalize<R><<<(h->V + 255) / 256, 256, 0, st>>>(c);
   } else {
     k_forward<R><<<(h->V + 255) / 256, 256, 0, st>>>(c);
     if (has_c) k_contact_prepare<R><<<(c.c_max + 255) / 256, 256, 0, st>>>(c);
@@ -1077,10 +1307,21 @@ int vbd_get_residuals(VbdHandle h, double* out, int32_t n, void* stream) {
 
 int vbd_launches_per_step(VbdHandle h, int32_t* out) {
   if (!h || !out) return VBD_ERR_INVALID_ARGUMENT;
-  if (h->schedule == VBD_SCHEDULE_PERSISTENT)
+  const int C = int(h->color_offsets.size()) - 1, I = h->prm.iterations;
+  if (h->schedule == VBD_SCHEDULE_PERSISTENT) {
     *out = 1 + (h->S > 0 ? 1 : 0);
-  else
-    *out = 2 + (h->S > 0 ? 1 : 0) + h->prm.iterations * (int(h->color_offsets.size()) - 1);
+  } else if (h->sc_on) {
+    // kernels of this library per detection: 1 copy + per primitive kind (boxes, cell, count, fill, query)
+    // + compaction (2 x (stored, pairs) + entry count, fill, sort); the six cub scans are not counted
+    const int detect = 1 + 2 * 5 + 4 + 3;
+    int n_det = 1;
+    for (int it = 0; it < I; ++it)
+      if ((h->sc_interval == 0 && it == 0) || (h->sc_interval >= 1 && it % h->sc_interval == 0)) ++n_det;
+    const bool duals = h->S > 0 && h->prm.avbd_linear_beta != 0.f;
+    *out = 2 + (h->S > 0 ? 1 : 0) + n_det * detect + 2 + I * (C * 3 + (duals ? 1 : 0));
+  } else {
+    *out = 2 + (h->S > 0 ? 1 : 0) + I * C;
+  }
   return VBD_OK;
 }
 
@@ -1263,6 +1504,288 @@ int vbd_soft_contacts(int32_t n, const float* q, const float* radius, const int3
   k_soft_contacts<<<int((total + 255) / 256), 256, 0, st>>>(n, q, radius, flags, S, tab, margin, cmax, count, particle,
                                                             shape, body_pos, body_vel, normal);
   CK(cudaGetLastError());
+  return VBD_OK;
+}
+
+int vbd_set_self_contact(VbdHandle h, const VbdSelfContactDesc* d) {
+  if (!h || !d) return VBD_ERR_INVALID_ARGUMENT;
+  if (!(d->radius > 0.0) || !(d->margin >= d->radius) || !(d->relaxation > 0.0) || d->vertex_buffer_size < 1 ||
+      d->edge_buffer_size < 1 || !(d->edge_parallel_epsilon >= 0.0) || !(d->rest_exclusion_radius >= 0.0))
+    return VBD_ERR_INVALID_ARGUMENT;
+  if (d->rest_exclusion_radius > 0.0 && !d->rest_q_dev) return VBD_ERR_INVALID_ARGUMENT;
+  if (h->schedule != VBD_SCHEDULE_PER_COLOR || h->layout != VBD_LAYOUT_CSR) return VBD_ERR_UNSUPPORTED;
+  const long long V = h->V, E = h->E;
+  if (V * d->vertex_buffer_size >= (1LL << 29) || E * d->edge_buffer_size >= (1LL << 29) ||
+      4 * V * d->vertex_buffer_size + 2 * E * d->edge_buffer_size >= (1LL << 31))
+    return VBD_ERR_TOO_LARGE;
+  if (cudaDeviceSynchronize() != cudaSuccess) return VBD_ERR_CUDA;
+  sc_release(h->sc);
+  for (void** p : {&h->sc_pos_cd, &h->sc_disp, &h->sc_ts}) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
+  h->sc_on = false;
+  const bool f64 = h->precision == VBD_PRECISION_FP64;
+  int rc = f64 ? sc_alloc<double>(h->sc, h->V, h->T, h->E, d->vertex_buffer_size, d->edge_buffer_size)
+               : sc_alloc<float>(h->sc, h->V, h->T, h->E, d->vertex_buffer_size, d->edge_buffer_size);
+  if (rc) return rc;
+  if ((rc = sc_upload_filter(d->vt_filter_offsets_host, d->vt_filter_host, h->V, h->T, &h->sc.vt_foff, &h->sc.vt_f)) ||
+      (rc = sc_upload_filter(d->ee_filter_offsets_host, d->ee_filter_host, h->E, h->E, &h->sc.ee_foff, &h->sc.ee_f)))
+    return rc;
+  const size_t p4 = f64 ? sizeof(double4) : sizeof(float4);
+  if ((rc = dalloc((char**)&h->sc_pos_cd, p4 * h->V)) || (rc = dalloc((char**)&h->sc_disp, p4 * h->V)) ||
+      (rc = dalloc((char**)&h->sc_ts, (f64 ? 8 : 4) * size_t(h->V))))
+    return rc;
+  if (f64)
+    k_sc_fill<double><<<(h->V + 255) / 256, 256>>>(h->V, (double*)h->sc_ts, 1.0);
+  else
+    k_sc_fill<float><<<(h->V + 255) / 256, 256>>>(h->V, (float*)h->sc_ts, 1.f);
+  CK(cudaGetLastError());
+  CK(cudaDeviceSynchronize());
+  h->sc_radius = d->radius;
+  h->sc_margin = d->margin;
+  h->sc_relax = d->relaxation;
+  h->sc_ee_eps = d->edge_parallel_epsilon;
+  h->sc_rest_excl = d->rest_exclusion_radius;
+  h->sc_interval = d->detection_interval;
+  h->sc_rest_q = d->rest_q_dev;
+  h->sc_on = true;
+  return VBD_OK;
+}
+
+int vbd_get_self_contact_counts(VbdHandle h, int32_t* vt_pairs, int32_t* ee_pairs, int32_t* flags, void* stream) {
+  if (!h || !h->sc_on) return VBD_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  int nv = 0, ne = 0, fl[4] = {0, 0, 0, 0};
+  CK(cudaMemcpyAsync(&nv, h->sc.vt_off + h->V, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&ne, h->sc.ee_off + h->E, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(fl, h->sc.flags, sizeof(fl), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (vt_pairs) *vt_pairs = nv;
+  if (ee_pairs) *ee_pairs = ne;
+  if (flags) *flags = fl[0] | (fl[2] << 2) | (fl[3] << 3);
+  return VBD_OK;
+}
+
+int vbd_build_contact_filters(int32_t V, int32_t T, const int32_t* tri, int32_t E, const int32_t* edges, int32_t ring,
+                              int32_t* vt_off, int32_t* vt_list, int32_t* ee_off, int32_t* ee_list) {
+  if (V < 0 || T < 0 || E < 0 || ring < 2 || (T && !tri) || (E && !edges) || !vt_off || !ee_off)
+    return VBD_ERR_INVALID_ARGUMENT;
+  for (long long i = 0; i < 3LL * T; ++i)
+    if (tri[i] < 0 || tri[i] >= V) return VBD_ERR_INVALID_ARGUMENT;
+  for (int e = 0; e < E; ++e)
+    for (int j = 0; j < 4; ++j)
+      if (edges[4 * e + j] < -1 || edges[4 * e + j] >= V || (j >= 2 && edges[4 * e + j] < 0))
+        return VBD_ERR_INVALID_ARGUMENT;
+  // vertex -> faces, vertex -> edges in any role, vertex -> edges it is an endpoint of, one-ring neighbours
+  std::vector<std::vector<int>> vf(V), ve_any(V), ve_end(V), nbr(V);
+  for (int t = 0; t < T; ++t)
+    for (int j = 0; j < 3; ++j) vf[tri[3 * t + j]].push_back(t);
+  for (int e = 0; e < E; ++e) {
+    const int* ei = edges + 4 * e;
+    for (int j = 0; j < 4; ++j)
+      if (ei[j] >= 0) ve_any[ei[j]].push_back(e);
+    ve_end[ei[2]].push_back(e);
+    ve_end[ei[3]].push_back(e);
+    if (ei[2] != ei[3]) {
+      nbr[ei[2]].push_back(ei[3]);
+      nbr[ei[3]].push_back(ei[2]);
+    }
+  }
+  for (auto& l : nbr) {
+    std::sort(l.begin(), l.end());
+    l.erase(std::unique(l.begin(), l.end()), l.end());
+  }
+  // vertices within ring - 1 steps of v (including v), as leq_n_ring_vertices / one_ring_vertices
+  std::vector<int> mark(V, -1), ringv;
+  auto ring_of = [&](int v, int stamp, std::vector<int>& out) {
+    out.clear();
+    std::vector<int> frontier{v};
+    if (mark[v] != stamp) {
+      mark[v] = stamp;
+      out.push_back(v);
+    }
+    for (int k = 0; k < ring - 1 && !frontier.empty(); ++k) {
+      std::vector<int> next;
+      for (int u : frontier)
+        for (int w : nbr[u])
+          if (mark[w] != stamp) {
+            mark[w] = stamp;
+            out.push_back(w);
+            next.push_back(w);
+          }
+      frontier.swap(next);
+    }
+  };
+  // pass over vertices: triangles touching a ring vertex other than v, minus v's own triangles
+  std::vector<int> row;
+  long long total = 0;
+  vt_off[0] = 0;
+  int stamp = 0;
+  for (int v = 0; v < V; ++v) {
+    ring_of(v, stamp++, ringv);
+    row.clear();
+    for (int w : ringv)
+      if (w != v) row.insert(row.end(), vf[w].begin(), vf[w].end());
+    std::sort(row.begin(), row.end());
+    row.erase(std::unique(row.begin(), row.end()), row.end());
+    std::vector<int> own = vf[v];
+    std::sort(own.begin(), own.end());
+    std::vector<int> keep;
+    std::set_difference(row.begin(), row.end(), own.begin(), own.end(), std::back_inserter(keep));
+    if (vt_list)
+      std::copy(keep.begin(), keep.end(), vt_list + total);
+    total += keep.size();
+    if (total >= (1LL << 31)) return VBD_ERR_TOO_LARGE;
+    vt_off[v + 1] = int(total);
+  }
+  // pass over edges: edges with an endpoint in either endpoint's ring (other than the endpoints),
+  // minus edges in which an endpoint takes any role
+  total = 0;
+  ee_off[0] = 0;
+  std::vector<int> r1, r2;
+  for (int e = 0; e < E; ++e) {
+    const int a = edges[4 * e + 2], b = edges[4 * e + 3];
+    ring_of(a, stamp++, r1);
+    ring_of(b, stamp++, r2);
+    row.clear();
+    for (const auto* lst : {&r1, &r2})
+      for (int w : *lst)
+        if (w != a && w != b) row.insert(row.end(), ve_end[w].begin(), ve_end[w].end());
+    std::sort(row.begin(), row.end());
+    row.erase(std::unique(row.begin(), row.end()), row.end());
+    std::vector<int> own = ve_any[a];
+    own.insert(own.end(), ve_any[b].begin(), ve_any[b].end());
+    std::sort(own.begin(), own.end());
+    std::vector<int> keep;
+    std::set_difference(row.begin(), row.end(), own.begin(), own.end(), std::back_inserter(keep));
+    if (ee_list)
+      std::copy(keep.begin(), keep.end(), ee_list + total);
+    total += keep.size();
+    if (total >= (1LL << 31)) return VBD_ERR_TOO_LARGE;
+    ee_off[e + 1] = int(total);
+  }
+  return VBD_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------ standalone detector
+struct VbdCollider {
+  int V = 0, T = 0, E = 0;
+  int4* tri_idx = nullptr;
+  int4* edge_idx = nullptr;
+  float4* pos = nullptr;
+  double ee_eps = 1e-5;
+  ScBuffers b;
+  ~VbdCollider() {
+    for (void* p : {(void*)tri_idx, (void*)edge_idx, (void*)pos})
+      if (p) cudaFree(p);
+    sc_release(b);
+  }
+};
+
+namespace {
+__global__ void k_col_pack(int T, const int* __restrict__ tri, int E, const int* __restrict__ edges, int4* ti, int4* ei) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < T) ti[i] = make_int4(tri[3 * i], tri[3 * i + 1], tri[3 * i + 2], 0);
+  if (i < E) ei[i] = make_int4(edges[4 * i], edges[4 * i + 1], edges[4 * i + 2], edges[4 * i + 3]);
+}
+__global__ void k_col_pos(int V, const float* __restrict__ q, float4* p) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < V) p[i] = make_float4(q[3 * i], q[3 * i + 1], q[3 * i + 2], 0.f);
+}
+// reference layout: 2 ints (primitive, partner) per slot, -1 in unused slots
+__global__ void k_col_export(int P, int cap, const int* __restrict__ list, const int* __restrict__ cnt,
+                             const float* __restrict__ mn, int* out, int* out_cnt, float* out_min) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P) return;
+  const int n = min(cnt[i], cap);
+  for (int k = 0; k < cap; ++k) {
+    out[2 * (size_t(i) * cap + k)] = k < n ? i : -1;
+    out[2 * (size_t(i) * cap + k) + 1] = k < n ? list[size_t(i) * cap + k] : -1;
+  }
+  if (out_cnt) out_cnt[i] = cnt[i];
+  if (out_min) out_min[i] = mn[i];
+}
+__global__ void k_col_flags(const int* __restrict__ f, int* out) {
+  if (threadIdx.x < 3 && f[threadIdx.x]) out[threadIdx.x] = 1;
+}
+}  // namespace
+
+extern "C" {
+
+int vbd_collider_create(int32_t V, int32_t T, const int32_t* tri_dev, int32_t E, const int32_t* edges_dev,
+                        int32_t vertex_buffer_size, int32_t edge_buffer_size, float edge_parallel_epsilon,
+                        const int32_t* vt_filter_offsets_host, const int32_t* vt_filter_host,
+                        const int32_t* ee_filter_offsets_host, const int32_t* ee_filter_host, VbdColliderHandle* out) {
+  if (!out || V < 0 || T < 0 || E < 0 || (T && !tri_dev) || (E && !edges_dev) || vertex_buffer_size < 1 ||
+      edge_buffer_size < 1)
+    return VBD_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  VbdCollider* c = new (std::nothrow) VbdCollider();
+  if (!c) return VBD_ERR_OUT_OF_MEMORY;
+  c->V = V, c->T = T, c->E = E, c->ee_eps = edge_parallel_epsilon;
+  int rc;
+  if ((rc = dalloc(&c->tri_idx, size_t(T))) || (rc = dalloc(&c->edge_idx, size_t(E))) ||
+      (rc = dalloc(&c->pos, size_t(V))) || (rc = sc_alloc<float>(c->b, V, T, E, vertex_buffer_size, edge_buffer_size)) ||
+      (rc = sc_upload_filter(vt_filter_offsets_host, vt_filter_host, V, T, &c->b.vt_foff, &c->b.vt_f)) ||
+      (rc = sc_upload_filter(ee_filter_offsets_host, ee_filter_host, E, E, &c->b.ee_foff, &c->b.ee_f))) {
+    delete c;
+    return rc;
+  }
+  // the indices are checked once here, as vbd_create checks a model's
+  std::vector<int> ht(3 * size_t(T)), he(4 * size_t(E));
+  if ((T && cudaMemcpy(ht.data(), tri_dev, ht.size() * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+      (E && cudaMemcpy(he.data(), edges_dev, he.size() * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)) {
+    delete c;
+    return VBD_ERR_CUDA;
+  }
+  bool ok = true;
+  for (int v : ht) ok = ok && v >= 0 && v < V;
+  for (size_t i = 0; i < he.size(); ++i) ok = ok && he[i] < V && he[i] >= ((i % 4) >= 2 ? 0 : -1);
+  if (!ok) {
+    delete c;
+    return VBD_ERR_INVALID_ARGUMENT;
+  }
+  const int n = std::max(T, E);
+  if (n > 0) k_col_pack<<<(n + 255) / 256, 256>>>(T, tri_dev, E, edges_dev, c->tri_idx, c->edge_idx);
+  if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+    delete c;
+    return VBD_ERR_CUDA;
+  }
+  *out = c;
+  return VBD_OK;
+}
+
+int vbd_collider_detect(VbdColliderHandle c, int32_t what, const float* pos_dev, float max_query_radius,
+                        float min_query_radius, const float* ref_pos_dev, int32_t* vt_dev, int32_t* vt_count_dev,
+                        float* vt_min_dev, int32_t* ee_dev, int32_t* ee_count_dev, float* ee_min_dev,
+                        int32_t* resize_flags_dev, void* stream) {
+  if (!c || !pos_dev || !(max_query_radius >= 0.f) || (what & ~3) || (min_query_radius > 0.f && !ref_pos_dev))
+    return VBD_ERR_INVALID_ARGUMENT;
+  if (((what & 1) && !vt_dev) || ((what & 2) && !ee_dev)) return VBD_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (c->V) k_col_pos<<<(c->V + 255) / 256, 256, 0, st>>>(c->V, pos_dev, c->pos);
+  CK(cudaMemsetAsync(c->b.flags, 0, 4 * sizeof(int), st));
+  ScSetup p{double(max_query_radius), double(min_query_radius), c->ee_eps, ref_pos_dev, nullptr};
+  int rc = sc_detect<float>(c->b, p, c->tri_idx, c->edge_idx, c->pos, what, st);
+  if (rc) return rc;
+  if ((what & 1) && c->V)
+    k_col_export<<<(c->V + 255) / 256, 256, 0, st>>>(c->V, c->b.vb, c->b.vt_tri, c->b.vt_count, (const float*)c->b.vt_min,
+                                                     vt_dev, vt_count_dev, vt_min_dev);
+  if ((what & 2) && c->E)
+    k_col_export<<<(c->E + 255) / 256, 256, 0, st>>>(c->E, c->b.eb, c->b.ee_edge, c->b.ee_count, (const float*)c->b.ee_min,
+                                                     ee_dev, ee_count_dev, ee_min_dev);
+  if (resize_flags_dev) k_col_flags<<<1, 32, 0, st>>>(c->b.flags, resize_flags_dev);
+  CK(cudaGetLastError());
+  return VBD_OK;
+}
+
+int vbd_collider_destroy(VbdColliderHandle c) {
+  if (!c) return VBD_ERR_INVALID_ARGUMENT;
+  cudaDeviceSynchronize();
+  delete c;
   return VBD_OK;
 }
 

@@ -18,6 +18,7 @@
 #include <type_traits>
 
 #include "vbd_elements.cuh"
+#include "vbd_selfcontact.cuh"
 
 namespace vbd {
 
@@ -85,6 +86,15 @@ struct StepCtx {
   double* residual;  // [iterations] (MIXED)
   int V;
   int S;  // shape count
+  // self-contact (per-color schedule): positions move as q = q_cd + disp, see vbd_collide.cuh
+  int dual_in_solve;  // 1: AVBD penalty update fused into the solve (positions fixed within an iteration)
+  P4* disp;           // displacement since the last detection, or null
+  P4* pos_cd;         // positions at the last detection
+  const int* ent_off;   // [V+1] per-vertex self-contact entries
+  const unsigned* ent;  // (kind << 31) | (slot << 29) | pair
+  const int2* vt_pairs;  // (vertex, triangle)
+  const int2* ee_pairs;  // (edge, edge)
+  double sc_radius, sc_ee_eps;
 };
 
 __device__ __forceinline__ void set_err(int* err, int bit) {
@@ -137,6 +147,7 @@ __device__ __forceinline__ void forward_particle(const StepCtx<R>& c, const P& p
   if (!(fl & 1) || im == 0.f) {
     c.inertia[i] = pk4(q, msolve);
     pos.st(i, q);
+    if (c.disp) c.disp[i] = pk4(zero3<R>(), R(0));
     return;
   }
   const vec3<R> g = {R(c.gravity[0]), R(c.gravity[1]), R(c.gravity[2])};
@@ -146,6 +157,7 @@ __device__ __forceinline__ void forward_particle(const StepCtx<R>& c, const P& p
   const vec3<R> d = v * c.dt;
   c.inertia[i] = pk4(q + d, msolve);
   pos.st(i, q + d);
+  if (c.disp) c.disp[i] = pk4(d, R(0));
 }
 
 // velocity update and state write-back: particle_vbd_kernels.py:1900-1903, solver_vbd.py:2335-2337
@@ -196,7 +208,7 @@ __device__ __forceinline__ void contacts_add(const StepCtx<R>& c, int v, vec3<R>
     const vec3<R> nn = {R(nf.x), R(nf.y), R(nf.z)};
     const R pen = -(dot(nn, x - bx) - r);
     R k = R(c.c_k[t]);
-    if (c.beta != R(0)) {
+    if (c.beta != R(0) && c.dual_in_solve) {
       // AVBD penalty ramp with the position at the start of this iteration (unchanged until now)
       k = vmin(k + c.beta * vmax(R(0), pen), R(c.c_ke[t]));
       c.c_k[t] = float(k);
@@ -226,7 +238,35 @@ __device__ __forceinline__ void contacts_add(const StepCtx<R>& c, int v, vec3<R>
 
 // ---------------------------------------------------------------------------------------------
 // One vertex solved by L lanes. All lanes of the warp must call this (it shuffles).
-template <typename R, int L, int MODE, typename P>
+// Self-contact term of one entry of vertex v's list (see vbd_collide.cuh for the encoding).
+template <typename R, typename P>
+__device__ __forceinline__ void self_contact_add(const StepCtx<R>& c, const P& pos, unsigned code, vec3<R>& f,
+                                                 sym3<R>& H) {
+  const int pair = int(code & 0x1FFFFFFFu), slot = int((code >> 29) & 3u);
+  int ids[4];
+  if (code >> 31) {
+    const int2 pr = __ldg(c.ee_pairs + pair);
+    const int4 a = __ldg(c.edge_idx + pr.x), b = __ldg(c.edge_idx + pr.y);
+    ids[0] = a.z, ids[1] = a.w, ids[2] = b.z, ids[3] = b.w;
+  } else {
+    const int2 pr = __ldg(c.vt_pairs + pair);
+    const int4 t = __ldg(c.tri_idx + pr.y);
+    ids[0] = t.x, ids[1] = t.y, ids[2] = t.z, ids[3] = pr.x;
+  }
+  vec3<R> x[4], xa[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) x[k] = pos.ld(ids[k]), xa[k] = ld3<R>(c.qprev[ids[k]]);
+  const R eps_u = c.fric_eps * c.dt;
+  if (code >> 31)
+    sc_ee_add<R>(slot, x, xa, R(c.sc_radius), R(c.soft_ke), R(c.soft_kd), R(c.soft_mu), eps_u, c.dt, R(c.sc_ee_eps), f, H);
+  else
+    sc_vt_add<R>(slot, x, xa, R(c.sc_radius), R(c.soft_ke), R(c.soft_kd), R(c.soft_mu), eps_u, c.dt, f, H);
+}
+
+// SC: self-contact on. The vertex's self-contact entries join its faces and hinges in the lane split, and
+// the solve adds its step to the displacement since the last detection instead of moving the vertex
+// (the truncation pass that follows each color moves it, as apply_truncation_ts does).
+template <typename R, int L, int MODE, typename P, bool SC = false>
 __device__ __forceinline__ void solve_group(const StepCtx<R>& c, const P& pos, int v, bool valid, int sub,
                                             int iteration) {
   vec3<R> f = zero3<R>();
@@ -238,9 +278,16 @@ __device__ __forceinline__ void solve_group(const StepCtx<R>& c, const P& pos, i
     const int fb = __ldg(c.face_off + v), fe = __ldg(c.face_off + v + 1);
     const int eb = __ldg(c.edge_off + v), ee = __ldg(c.edge_off + v + 1);
     const int nf = fe - fb;
-    const int n = nf + (ee - eb);
+    const int nfe = nf + (ee - eb);
+    int cb = 0, n = nfe;
+    if (SC) {
+      cb = __ldg(c.ent_off + v);
+      n += __ldg(c.ent_off + v + 1) - cb;
+    }
     for (int it = sub; it < n; it += L) {
-      if (it < nf) {
+      if (SC && it >= nfe) {
+        self_contact_add<R>(c, pos, __ldg(c.ent + cb + (it - nfe)), f, H);
+      } else if (it < nf) {
         const int a = __ldg(c.face_adj + fb + it);
         const int t = a >> 2, ord = a & 3;
         const float4 mat = __ldg(c.tri_mat + t);
@@ -292,6 +339,7 @@ __device__ __forceinline__ void solve_group(const StepCtx<R>& c, const P& pos, i
     H.yz = group_sum<L>(H.yz);
   }
   const bool leader = active && sub == 0;
+  if (SC && valid && !active && sub == 0) c.disp[v] = pk4(zero3<R>(), R(0));  // as the reference's solve does
   vec3<R> x = zero3<R>();
   if (leader) {
     x = pos.ld(v);
@@ -346,7 +394,10 @@ __device__ __forceinline__ void solve_group(const StepCtx<R>& c, const P& pos, i
     set_err(c.err, 1);
     return;
   }
-  pos.st(v, xn);
+  if (SC)
+    c.disp[v] = pk4(ld3<R>(c.disp[v]) + dlt, R(0));
+  else
+    pos.st(v, xn);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -393,13 +444,38 @@ __global__ void k_contact_prepare(StepCtx<R> c) {
     set_err(c.err, 2);
 }
 
-template <typename R, int L, int MODE>
+template <typename R, int L, int MODE, bool SC = false>
 __global__ void k_color(StepCtx<R> c, const int* __restrict__ verts, int n, int iteration) {
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   const int grp = gid / L, sub = gid % L;
   const bool valid = grp < n;
   const int v = valid ? __ldg(verts + grp) : 0;
-  solve_group<R, L, MODE>(c, GlobalPos<R>{c.pos}, v, valid, sub, iteration);
+  solve_group<R, L, MODE, GlobalPos<R>, SC>(c, GlobalPos<R>{c.pos}, v, valid, sub, iteration);
+}
+
+// AVBD penalty update of every contact at the start of an iteration (update_duals_body_particle_contacts,
+// rigid_vbd_kernels.py:3755-3799); used when positions can move between an iteration's start and a
+// vertex's color (self-contact truncation), where the update cannot be fused into the solve.
+template <typename R>
+__global__ void k_contact_duals(StepCtx<R> c) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int count = *c.c_count;
+  if (count > c.c_max) count = c.c_max;
+  if (t >= count) return;
+  const int v = c.c_particle[t];
+  const int s = c.c_shape[t];
+  if (v < 0 || v >= c.V || s < 0 || s >= c.S) return;
+  const int b = (c.shape_body && s >= 0) ? c.shape_body[s] : -1;
+  vec3<float> bxf = ldv3(c.c_body_pos, t);
+  if (b >= 0 && c.body_q) {
+    const float* X = c.body_q + 7 * b;
+    bxf = qrot(X + 3, bxf) + vec3<float>{X[0], X[1], X[2]};
+  }
+  const vec3<R> bx = {R(bxf.x), R(bxf.y), R(bxf.z)};
+  const vec3<float> nf = ldv3(c.c_normal, t);
+  const vec3<R> nn = {R(nf.x), R(nf.y), R(nf.z)};
+  const R pen = -(dot(nn, ld3<R>(c.pos[v]) - bx) - R(c.radius[v]));
+  c.c_k[t] = float(vmin(R(c.c_k[t]) + c.beta * vmax(R(0), pen), R(c.c_ke[t])));
 }
 
 struct PersistentPlan {

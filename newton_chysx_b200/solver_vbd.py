@@ -20,6 +20,10 @@ Beyond the reference keywords:
   vertex), ``"csr"`` (adjacency + element records; any lanes per vertex), ``"auto"``.
 * ``min_blocks_per_sm``: 2..4 compiles the persistent stencil kernel for that many resident CTAs of
   256 threads per SM (a register budget); 0 leaves the compiler's choice.
+
+Particle self-contact (``particle_enable_self_contact=True`` and the ``particle_self_contact_*``
+keywords) runs on the per-color schedule with the csr layout; see ``collision.py`` for the filters and
+the stand-alone detector.
 """
 
 from __future__ import annotations
@@ -98,13 +102,21 @@ class SolverVBD:
         self.friction_epsilon = friction_epsilon
         self.integrate_with_external_rigid_solver = integrate_with_external_rigid_solver
         self.particle_enable_self_contact = particle_enable_self_contact
+        self.particle_self_contact_radius = particle_self_contact_radius
+        self.particle_self_contact_margin = particle_self_contact_margin
+        self.particle_conservative_bound_relaxation = particle_conservative_bound_relaxation
+        self.particle_collision_detection_interval = particle_collision_detection_interval
+        self.particle_topological_contact_filter_threshold = particle_topological_contact_filter_threshold
+        self.particle_rest_shape_contact_exclusion_radius = particle_rest_shape_contact_exclusion_radius
         if particle_enable_self_contact:
             if particle_self_contact_margin < particle_self_contact_radius:
                 raise ValueError(
                     "particle_self_contact_margin is smaller than particle_self_contact_radius, this will result in "
                     "missing contacts and cause instability."
                 )
-            raise NotImplementedError("particle self-contact is not available in this build")
+            if schedule not in ("auto", "per_color") or layout not in ("auto", "csr"):
+                raise ValueError("particle self-contact runs on the per_color schedule with the csr layout")
+            schedule, layout = "per_color", "csr"
         if model.body_count > 0 and not integrate_with_external_rigid_solver:
             raise NotImplementedError("rigid bodies (AVBD) are not part of this solver")
         if model.particle_count == 0:
@@ -199,9 +211,54 @@ class SolverVBD:
         self.lanes_per_vertex = lanes.value
         self.block_size = blk.value
         self.shared_bytes = smem.value
+        if particle_enable_self_contact:
+            self._set_self_contact(
+                particle_vertex_contact_buffer_size, particle_edge_contact_buffer_size, particle_edge_parallel_epsilon,
+                particle_external_vertex_contact_filtering_map, particle_external_edge_contact_filtering_map,
+            )  # fmt: skip
         n = C.c_int32()
         self._lib.vbd_launches_per_step(h, C.byref(n))
         self.launches_per_step = n.value
+
+    def _set_self_contact(self, vertex_buffer, edge_buffer, edge_eps, external_vertex_map, external_edge_map):
+        """Collision filters and detector set-up of ``_init_particle_system`` (solver_vbd.py:489-526,
+        1339-1404), handed to ``vbd_set_self_contact``."""
+        from .collision import build_contact_filters
+
+        m = self.model
+        vt = ee = None
+        if m.tri_count:
+            vt, ee = build_contact_filters(
+                m.particle_count, m.tri_indices, m.edge_indices, self.particle_topological_contact_filter_threshold,
+                external_vertex_map, external_edge_map,
+            )  # fmt: skip
+        self._filters = (vt, ee)  # kept alive while the call copies them
+        d = _lib.VbdSelfContactDesc()
+        d.radius = float(self.particle_self_contact_radius)
+        d.margin = float(self.particle_self_contact_margin)
+        d.relaxation = float(self.particle_conservative_bound_relaxation)
+        d.edge_parallel_epsilon = float(edge_eps)
+        d.rest_exclusion_radius = float(self.particle_rest_shape_contact_exclusion_radius)
+        d.vertex_buffer_size = int(vertex_buffer)
+        d.edge_buffer_size = int(edge_buffer)
+        d.detection_interval = int(self.particle_collision_detection_interval)
+        self._rest_q = m.particle_q.detach().to(torch.float32).contiguous()
+        d.rest_q_dev = _ptr(self._rest_q)
+        ip = C.POINTER(C.c_int32)
+        if vt is not None:
+            d.vt_filter_host, d.vt_filter_offsets_host = vt[0].ctypes.data_as(ip), vt[1].ctypes.data_as(ip)
+        if ee is not None:
+            d.ee_filter_host, d.ee_filter_offsets_host = ee[0].ctypes.data_as(ip), ee[1].ctypes.data_as(ip)
+        with torch.cuda.device(self.device):
+            _lib.check(self._lib.vbd_set_self_contact(self._h, C.byref(d)), "vbd_set_self_contact")
+
+    def self_contact_counts(self) -> tuple[int, int, int]:
+        """(vertex-triangle pairs, edge-edge pairs, overflow flags) of the last detection of the last step."""
+        nv, ne, fl = C.c_int32(), C.c_int32(), C.c_int32()
+        stream = C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        _lib.check(self._lib.vbd_get_self_contact_counts(self._h, C.byref(nv), C.byref(ne), C.byref(fl), stream),
+                   "vbd_get_self_contact_counts")  # fmt: skip
+        return nv.value, ne.value, fl.value
 
     # ------------------------------------------------------------------ reference API
     def step(self, state_in: State, state_out: State, control, contacts: Contacts | None, dt: float) -> None:
@@ -257,7 +314,8 @@ class SolverVBD:
         _lib.check(self._lib.vbd_refresh_model(self._h, stream), "vbd_refresh_model")
 
     def rebuild_bvh(self, state: State) -> None:
-        """Self-contact BVH rebuild; a no-op while self-contact is off (as in the reference)."""
+        """The reference rebuilds its self-contact BVHs here. This solver's detector rebuilds its grid
+        at every detection, so there is nothing to do."""
 
     @staticmethod
     def register_custom_attributes(builder) -> None:

@@ -1,0 +1,247 @@
+"""GPU parity of particle self-contact (vertex-triangle and edge-edge contact, detection, truncation).
+
+Tolerances (positions in metres):
+  * FP32 kernels vs the float64 reference goldens: 1e-4 after each substep;
+  * FP64 kernels vs the FP64 oracle on the same float32 model arrays: 1e-9 per substep, 1e-7 over a
+    multi-substep trajectory;
+  * detection: the same pairs in the same slots as the reference's detection kernels (goldens) and the
+    oracle's brute force; minimum distances to 1e-6 (float32 arithmetic against float64).
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from newton_chysx_b200 import SolverVBD, sim
+from newton_chysx_b200.collision import TriMeshCollisionDetector, build_contact_filters
+from oracle import vbd_oracle as orc
+from tests.helpers import load_golden, model_from_golden, oracle_model_dict
+
+pytestmark = pytest.mark.gpu
+
+SCENES = ["step_selfcontact_layers.npz", "step_selfcontact_fold.npz"]
+
+
+def _t(a, dtype=torch.float32):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device="cuda")
+
+
+def _sc_kwargs(g):
+    return dict(
+        particle_enable_self_contact=True, particle_self_contact_radius=float(g["sc_radius"]),
+        particle_self_contact_margin=float(g["sc_margin"]),
+        particle_conservative_bound_relaxation=float(g["sc_relaxation"]),
+        particle_collision_detection_interval=int(g["sc_interval"]),
+        particle_topological_contact_filter_threshold=int(g["sc_ring"]),
+        particle_rest_shape_contact_exclusion_radius=float(g["sc_rest_exclusion"]),
+    )  # fmt: skip
+
+
+def _solver(g, model, **kw):
+    return SolverVBD(model, iterations=int(g["iterations"]), friction_epsilon=float(g["friction_epsilon"]),
+                     **_sc_kwargs(g), **kw)  # fmt: skip
+
+
+def _step(solver, q, qd, f, dt, dtype=torch.float32):
+    st_in, st_out = sim.State(), sim.State()
+    st_in.particle_q, st_in.particle_qd, st_in.particle_f = _t(q, dtype), _t(qd, dtype), _t(f, dtype)
+    st_out.particle_q = torch.zeros_like(st_in.particle_q)
+    st_out.particle_qd = torch.zeros_like(st_in.particle_qd)
+    solver.step(st_in, st_out, None, None, dt)
+    torch.cuda.synchronize()
+    return st_in, st_out
+
+
+def _oracle(model, g_or_kw):
+    d = oracle_model_dict(model, 1e-2, 0.0)
+    d["soft"] = d["soft"].astype(np.float32).astype(np.float64)  # the C ABI carries them as float
+    return orc.Model(d)
+
+
+def _oracle_sc(model, kw, vertex_buffer=32, edge_buffer=64):
+    vt, ee = build_contact_filters(model.particle_count, model.tri_indices, model.edge_indices,
+                                   kw["particle_topological_contact_filter_threshold"])  # fmt: skip
+    return orc.SelfContact(
+        model.particle_q.cpu().numpy().astype(np.float64), radius=kw["particle_self_contact_radius"],
+        margin=kw["particle_self_contact_margin"], relaxation=kw["particle_conservative_bound_relaxation"],
+        interval=kw["particle_collision_detection_interval"],
+        rest_exclusion=kw["particle_rest_shape_contact_exclusion_radius"], vt_filter=vt, ee_filter=ee,
+        vertex_buffer=vertex_buffer, edge_buffer=edge_buffer,
+    )  # fmt: skip
+
+
+@pytest.mark.parametrize("name", SCENES)
+@pytest.mark.parametrize("lanes", [1, 4])
+def test_fp32_selfcontact_step_matches_reference_goldens(name, lanes):
+    g = load_golden(name)
+    model = model_from_golden(g)
+    solver = _solver(g, model, lanes_per_vertex=lanes)
+    assert solver.schedule == "per_color" and solver.layout == "csr" and solver.lanes_per_vertex == lanes
+    for s in range(int(g["substeps"])):
+        st_in, st_out = _step(solver, g[f"s{s}_q_in"], g[f"s{s}_qd_in"], g[f"s{s}_f_ext"], float(g["dt"]))
+        q = st_out.particle_q.cpu().numpy()
+        assert np.abs(q - g[f"s{s}_q_out"]).max() <= 1e-4, (name, s)
+        assert np.array_equal(st_in.particle_q.cpu().numpy(), q)
+        nv, ne, flags = solver.self_contact_counts()
+        assert nv > 0 and ne > 0 and flags == 0
+    assert solver.device_errors() & ~4 == 0
+
+
+@pytest.mark.parametrize("name", SCENES)
+def test_fp64_selfcontact_step_matches_fp64_oracle(name):
+    g = load_golden(name)
+    model = model_from_golden(g)
+    solver = _solver(g, model, precision="fp64")
+    om, osc = _oracle(model, g), _oracle_sc(model, _sc_kwargs(g))
+    for s in range(int(g["substeps"])):
+        _, st_out = _step(solver, g[f"s{s}_q_in"], g[f"s{s}_qd_in"], g[f"s{s}_f_ext"], float(g["dt"]), torch.float64)
+        _, q_o, qd_o = orc.step(om, g[f"s{s}_q_in"], g[f"s{s}_qd_in"], g[f"s{s}_f_ext"], None, float(g["dt"]),
+                                int(g["iterations"]), 64, self_contact=osc)  # fmt: skip
+        assert np.abs(st_out.particle_q.cpu().numpy() - q_o).max() <= 1e-9, (name, s)
+        assert np.abs(st_out.particle_qd.cpu().numpy() - qd_o).max() <= 1e-9 / float(g["dt"])
+
+
+@pytest.mark.parametrize("name", SCENES)
+def test_detector_matches_reference_detection(name):
+    """TriMeshCollisionDetector buffers at the step's start positions == the reference kernels' buffers."""
+    g = load_golden(name)
+    model = model_from_golden(g)
+    det = TriMeshCollisionDetector(model, vertex_collision_buffer_pre_alloc=32, edge_collision_buffer_pre_alloc=64,
+                                   vertex_triangle_filtering_list=g["sc_vt_filter"],
+                                   vertex_triangle_filtering_list_offsets=g["sc_vt_filter_offsets"],
+                                   edge_filtering_list=g["sc_ee_filter"],
+                                   edge_filtering_list_offsets=g["sc_ee_filter_offsets"])  # fmt: skip
+    for s in range(int(g["substeps"])):
+        det.refit(_t(g[f"s{s}_q_in"]))
+        kw = dict(min_query_radius=float(g["sc_rest_exclusion"]), min_distance_filtering_ref_pos=model.particle_q)
+        det.vertex_triangle_collision_detection(float(g["sc_margin"]), **kw)
+        det.edge_edge_collision_detection(float(g["sc_margin"]), **kw)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(det.vertex_colliding_triangles.cpu().numpy(), g[f"s{s}_cd0_vt"])
+        np.testing.assert_array_equal(det.vertex_colliding_triangles_count.cpu().numpy(), g[f"s{s}_cd0_vt_count"])
+        np.testing.assert_array_equal(det.edge_colliding_edges.cpu().numpy(), g[f"s{s}_cd0_ee"])
+        np.testing.assert_array_equal(det.edge_colliding_edges_count.cpu().numpy(), g[f"s{s}_cd0_ee_count"])
+        assert np.abs(det.vertex_colliding_triangles_min_dist.cpu().numpy() - g[f"s{s}_cd0_vt_min"]).max() <= 1e-6
+        assert np.abs(det.edge_colliding_edges_min_dist.cpu().numpy() - g[f"s{s}_cd0_ee_min"]).max() <= 1e-6
+        assert det.resize_flags.sum().item() == 0
+
+
+def _crumpled(n=48, seed=3, layers=2):
+    """Stacked, turned and noisy sheets: many vertex-triangle and edge-edge proximities."""
+    b = sim.ModelBuilder(up_axis="Z", gravity=-9.81)
+    for k in range(layers):
+        rot = sim.quat_from_axis_angle((0.0, 0.0, 1.0), 0.3 * k)
+        b.add_cloth_grid(pos=(-0.5, -0.5, 0.004 * k), rot=rot, vel=(0.0, 0.0, -0.5 * k), dim_x=n - 1, dim_y=n - 1,
+                         cell_x=1.0 / (n - 1), cell_y=1.0 / (n - 1), mass=2e-4, tri_ke=5.0, tri_ka=5.0, tri_kd=0.0,
+                         edge_ke=1e-4, edge_kd=0.0, particle_radius=2e-3)  # fmt: skip
+    b.color(include_bending=True)
+    model = b.finalize("cuda")
+    rng = np.random.default_rng(seed)
+    q = model.particle_q.cpu().numpy() + rng.normal(scale=1.5e-3, size=(model.particle_count, 3))
+    return model, q.astype(np.float32)
+
+
+@pytest.mark.parametrize("vb,eb", [(32, 64), (2, 3)])
+def test_detector_matches_brute_force(vb, eb):
+    """Grid detection == the oracle's brute force (all pairs), including buffer overflow (lowest ids kept)."""
+    model, q = _crumpled()
+    margin = 6e-3
+    vt, ee = build_contact_filters(model.particle_count, model.tri_indices, model.edge_indices, 2)
+    det = TriMeshCollisionDetector(model, vertex_collision_buffer_pre_alloc=vb, edge_collision_buffer_pre_alloc=eb,
+                                   vertex_triangle_filtering_list=vt[0], vertex_triangle_filtering_list_offsets=vt[1],
+                                   edge_filtering_list=ee[0], edge_filtering_list_offsets=ee[1])  # fmt: skip
+    det.refit(_t(q))
+    det.vertex_triangle_collision_detection(margin)
+    det.edge_edge_collision_detection(margin)
+    torch.cuda.synchronize()
+    om = _oracle(model, None)
+    osc = orc.SelfContact(np.zeros((model.particle_count, 3)), radius=margin, margin=margin, vt_filter=vt,
+                          ee_filter=ee, vertex_buffer=vb, edge_buffer=eb)  # fmt: skip
+    ref = orc.collide(om, osc, q.astype(np.float64), precision=32, nthreads=orc.max_threads())
+    got_vt = det.vertex_colliding_triangles.cpu().numpy()
+    got_ee = det.edge_colliding_edges.cpu().numpy()
+    assert ref["vt_count"].sum() > model.particle_count // 4 and ref["ee_count"].sum() > 0
+    np.testing.assert_array_equal(det.vertex_colliding_triangles_count.cpu().numpy(), ref["vt_count"])
+    np.testing.assert_array_equal(det.edge_colliding_edges_count.cpu().numpy(), ref["ee_count"])
+    np.testing.assert_array_equal(got_vt, ref["vt"])
+    np.testing.assert_array_equal(got_ee, ref["ee"])
+    assert np.abs(det.vertex_colliding_triangles_min_dist.cpu().numpy() - ref["vt_min"]).max() <= 1e-6
+    overflow = vb < 32
+    assert bool(det.resize_flags[0].item()) == overflow and bool(det.resize_flags[2].item()) == overflow
+
+
+def _layers_scene(n=12):
+    model, q = _crumpled(n=n, seed=5)
+    qd = np.zeros_like(q)
+    qd[model.particle_count // 2 :, 2] = -0.5
+    kw = dict(particle_enable_self_contact=True, particle_self_contact_radius=2e-3, particle_self_contact_margin=3.5e-3,
+              particle_conservative_bound_relaxation=0.85, particle_collision_detection_interval=0,
+              particle_topological_contact_filter_threshold=2, particle_rest_shape_contact_exclusion_radius=0.0)  # fmt: skip
+    return model, q, qd, kw
+
+
+def test_fp64_selfcontact_trajectory_matches_oracle():
+    model, q, qd, kw = _layers_scene()
+    model.soft_contact_ke, model.soft_contact_kd, model.soft_contact_mu = 1.0e2, 1.0e-4, 0.3
+    solver = SolverVBD(model, iterations=5, precision="fp64", **kw)
+    om, osc = _oracle(model, None), _oracle_sc(model, kw)
+    dt = 1.0 / 600.0
+    qg, qdg = q.astype(np.float64), qd.astype(np.float64)
+    qo, qdo = qg.copy(), qdg.copy()
+    f = np.zeros_like(qg)
+    for _ in range(8):
+        _, st_out = _step(solver, qg, qdg, f, dt, torch.float64)
+        qg, qdg = st_out.particle_q.cpu().numpy(), st_out.particle_qd.cpu().numpy()
+        _, qo, qdo = orc.step(om, qo, qdo, f, None, dt, 5, 64, self_contact=osc)
+    assert np.abs(qg - qo).max() <= 1e-7
+    assert solver.self_contact_counts()[0] > 0
+
+
+def test_selfcontact_graph_capture_and_determinism():
+    model, q, qd, kw = _layers_scene(24)
+    solver = SolverVBD(model, iterations=4, **kw)
+    dt = 1.0 / 600.0
+
+    def run(steps):
+        s0, s1 = model.state(), model.state()
+        s0.particle_q.copy_(_t(q))
+        s0.particle_qd.copy_(_t(qd))
+        for _ in range(steps):
+            solver.step(s0, s1, None, None, dt)
+            s0, s1 = s1, s0
+        torch.cuda.synchronize()
+        return s0.particle_q.clone()
+
+    a, b = run(3), run(3)
+    assert torch.equal(a, b)  # no atomics in the sums: bitwise repeatable
+    s0, s1 = model.state(), model.state()
+    s0.particle_q.copy_(_t(q))
+    s0.particle_qd.copy_(_t(qd))
+    solver.step(s0, s1, None, None, dt)  # sizes every buffer before capture
+    s0.particle_q.copy_(_t(q))
+    s0.particle_qd.copy_(_t(qd))
+    graph = torch.cuda.CUDAGraph()
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(stream):
+        with torch.cuda.graph(graph, stream=stream):
+            solver.step(s0, s1, None, None, dt)
+            solver.step(s1, s0, None, None, dt)
+    torch.cuda.current_stream().wait_stream(stream)
+    s0.particle_q.copy_(_t(q))
+    s0.particle_qd.copy_(_t(qd))
+    graph.replay()
+    solver.step(s0, s1, None, None, dt)
+    torch.cuda.synchronize()
+    assert torch.equal(s1.particle_q, a)
+    assert torch.isfinite(a).all()
+
+
+def test_selfcontact_needs_per_color_csr():
+    model, q, qd, kw = _layers_scene(8)
+    with pytest.raises(ValueError):
+        SolverVBD(model, schedule="persistent", **kw)
+    with pytest.raises(ValueError):
+        SolverVBD(model, layout="ell", **kw)
+    with pytest.raises(ValueError):
+        SolverVBD(model, **dict(kw, particle_self_contact_margin=1e-3))
