@@ -477,6 +477,141 @@ def run_plain(args):
             "note": "sample of the batch's first instances; eager per-instance step calls"}  # fmt: skip
 
 
+SC_ITERATIONS = 20
+
+
+def build_selfcontact_model(dev, n=256):
+    """Plain drop-in at scale: an n x n sheet (1 m side, E = 1e4 Pa, nu = 0.3, h = 1e-3 m, 0.2 kg/m^2,
+    bending 1e-4) flat at z = 0.5 m above a fixed sphere of radius 0.3 m at the origin."""
+    import newton_chysx_b200 as nb
+
+    E, nu, h = 1.0e4, 0.3, 1.0e-3
+    b = nb.ModelBuilder(up_axis="Z", gravity=-9.81)
+    b.add_cloth_grid(pos=(-0.5, -0.5, 0.5), rot=nb.quat_identity(), vel=(0.0, 0.0, 0.0), dim_x=n - 1, dim_y=n - 1,
+                     cell_x=1.0 / (n - 1), cell_y=1.0 / (n - 1), mass=0.2 / (n * n), tri_ke=E * h / (2.0 * (1.0 + nu)),
+                     tri_ka=E * h * nu / (1.0 - nu * nu), tri_kd=0.0, edge_ke=1e-4, edge_kd=0.0,
+                     particle_radius=2e-3)  # fmt: skip
+    b.add_shape_sphere(radius=0.3)
+    b.color(include_bending=True)
+    m = b.finalize(dev)
+    m.soft_contact_ke, m.soft_contact_kd, m.soft_contact_mu = 1.0e4, 1.0e-2, 0.5
+    return m
+
+
+SC_KW = dict(particle_enable_self_contact=True, particle_self_contact_radius=2e-3, particle_self_contact_margin=3.5e-3,
+             particle_collision_detection_interval=0, particle_topological_contact_filter_threshold=2)  # fmt: skip
+
+
+def run_selfcontact(args):
+    """Config of the plain drop-in at scale: one 256 x 256 cloth (65,536 vertices, 130,050 triangles)
+    dropped onto a sphere with vertex-triangle and edge-edge self-contact, 20 iterations per substep,
+    dt = 1/600 s. The sheet first falls and drapes untimed (--sc-settle-frames x 10 substeps); then K
+    substeps (collision generation + step) are timed, replayed from a CUDA graph of one substep."""
+    import torch
+
+    import newton_chysx_b200 as nb
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    m = build_selfcontact_model(dev, args.sc_n)
+    solver = nb.SolverVBD(m, iterations=SC_ITERATIONS, lanes_per_vertex=args.lanes or 1, **SC_KW)
+    pipe = nb.CollisionPipeline(m, soft_contact_margin=0.01)
+    contacts = pipe.contacts()
+    s0, s1 = m.state(), m.state()
+    t0 = time.perf_counter()
+    settle = args.sc_settle_frames * 10 + args.warmup
+    for k in range(settle):
+        pipe.collide(s0, contacts)
+        solver.step(s0, s1, None, contacts, DT)
+        s0, s1 = s1, s0
+    torch.cuda.synchronize()
+    settle_s = time.perf_counter() - t0
+    q_settled, qd_settled = s0.particle_q.clone(), s0.particle_qd.clone()
+    # one substep (ping-pong pair) per graph replay
+    graph = torch.cuda.CUDAGraph()
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(stream), torch.cuda.graph(graph, stream=stream):
+        pipe.collide(s0, contacts)
+        solver.step(s0, s1, None, contacts, DT)
+        pipe.collide(s1, contacts)
+        solver.step(s1, s0, None, contacts, DT)
+    torch.cuda.current_stream().wait_stream(stream)
+    s0.particle_q.copy_(q_settled)
+    s0.particle_qd.copy_(qd_settled)
+    pairs = []
+    K = max(2, args.steps + (args.steps % 2))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index or 0) as clk:
+        e0.record()
+        for _ in range(K // 2):
+            graph.replay()
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / K
+    pairs = solver.self_contact_counts()
+    V = m.particle_count
+    value = V * SC_ITERATIONS / (ms * 1e-3)
+    out = {
+        "metric": "VBD vertex-iters/s on 1 B200, plain drop-in with self-contact", "value": value, "unit": UNIT,
+        "n_gpus": 1, "steps": K, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (cloth grid dropped on a sphere)",
+        "config": {"workload": f"plain drop-in at scale: {args.sc_n}x{args.sc_n} cloth on a sphere, self-contact",
+                   "vertices": V, "triangles": m.tri_count, "edges": m.edge_count, "iterations": SC_ITERATIONS,
+                   "dt": DT, "self_contact": {k: v for k, v in SC_KW.items() if k != "particle_enable_self_contact"},
+                   "settled_substeps": settle, "settle_s": round(settle_s, 2),
+                   "timed": "sphere contact generation + step, one CUDA graph per two substeps",
+                   "l2": "working set below L2; the step is launch- and latency-bound, see launches_per_step"},
+        "launches_per_step": solver.launches_per_step + 1, "colors": len(m.particle_color_groups),
+        "self_contact_pairs": {"vertex_triangle": pairs[0], "edge_edge": pairs[1], "overflow_flags": pairs[2]},
+        "clocks": clk.summary(), "device_errors": solver.device_errors(),
+        "finite": bool(torch.isfinite(s0.particle_q).all().item()),
+    }  # fmt: skip
+    if not args.no_e2e:  # public API with host state: H2D of (q, qd), step, D2H of q
+        hq = q_settled.cpu().pin_memory()
+        hqd = qd_settled.cpu().pin_memory()
+        out_q = torch.empty_like(hq).pin_memory()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(K):
+            s0.particle_q.copy_(hq, non_blocking=True)
+            s0.particle_qd.copy_(hqd, non_blocking=True)
+            pipe.collide(s0, contacts)
+            solver.step(s0, s1, None, contacts, DT)
+            out_q.copy_(s1.particle_q, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        ms_e = e0.elapsed_time(e1) / K
+        out["e2e"] = {"value": V * SC_ITERATIONS / (ms_e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 2 * hq.numel() * 4,
+                      "d2h_bytes_per_step": out_q.numel() * 4, "steps": K}  # fmt: skip
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_selfcontact(m, q_settled.cpu().numpy(), qd_settled.cpu().numpy())
+    return out
+
+
+def cpu_baseline_selfcontact(m, q, qd):
+    """The oracle (FP32, all host threads, box-grid detection) on one substep of the same settled state."""
+    from newton_chysx_b200.collision import build_contact_filters
+    from oracle import vbd_oracle as orc
+    from tests.helpers import oracle_model_dict
+
+    threads = orc.max_threads()
+    om = orc.Model(oracle_model_dict(m))
+    vt, ee = build_contact_filters(m.particle_count, m.tri_indices, m.edge_indices, 2)
+    sc = orc.SelfContact(m.particle_q.cpu().numpy().astype(np.float64), radius=SC_KW["particle_self_contact_radius"],
+                         margin=SC_KW["particle_self_contact_margin"], vt_filter=vt, ee_filter=ee)  # fmt: skip
+    q = q.astype(np.float64)
+    t = time.perf_counter()
+    cnt, p, s, bp, bv, nn = orc.soft_contacts(q, m.particle_radius.cpu().numpy(), m.particle_flags.cpu().numpy(),
+                                              m.shape_type, m.shape_pos, m.shape_radius, 0.01)  # fmt: skip
+    orc.step(om, q, qd.astype(np.float64), None, orc.make_contacts(cnt, p, s, bp, bv, nn), DT, SC_ITERATIONS,
+             precision=32, nthreads=threads, self_contact=sc)  # fmt: skip
+    el = time.perf_counter() - t
+    return {"value": m.particle_count * SC_ITERATIONS / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "one substep of the same settled 256x256 state (self-contact detection on a box grid)"}  # fmt: skip
+
+
 def build_precision_model(n=1024, seed=4, sliver_fraction=1e-3):
     """1024 x 1024 sheet, per-triangle E log-uniform in [1e5, 1e8] Pa, 0.1% of vertex sites moved
     towards a neighbour so that incident triangles keep ~1e-6 of their nominal rest area."""
@@ -608,7 +743,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["batched", "plain", "precision"], default="batched")
+    ap.add_argument("--workload", choices=["batched", "plain", "precision", "selfcontact"], default="batched")
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--lanes", type=int, default=0)
@@ -626,6 +761,8 @@ def main():
     ap.add_argument("--precision-n", type=int, default=1024)
     ap.add_argument("--precision-frames", type=int, default=60)
     ap.add_argument("--traffic", type=float, default=None, help="DRAM bytes per launch from an ncu capture")
+    ap.add_argument("--sc-n", type=int, default=256, help="selfcontact workload: grid side (vertices)")
+    ap.add_argument("--sc-settle-frames", type=int, default=40, help="selfcontact workload: untimed frames first")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     if args.impl == "reference":
@@ -634,6 +771,8 @@ def main():
         out = run_plain(args)
     elif args.workload == "precision":
         out = run_precision(args)
+    elif args.workload == "selfcontact":
+        out = run_selfcontact(args)
     else:
         out = run_ours(args)
     if out is not None:

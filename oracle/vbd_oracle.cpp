@@ -29,7 +29,10 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <algorithm>
 #include <limits>
+#include <numeric>
+#include <utility>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -663,6 +666,48 @@ struct SelfContact {
   const double* rest_q;  // model.particle_q (rest-shape distance filter)
   const int *vt_filter_offsets, *vt_filter;  // sorted CSR per vertex, or null
   const int *ee_filter_offsets, *ee_filter;  // sorted CSR per edge, or null
+  int brute_force;  // 1: test every primitive; 0: only those a uniform grid of boxes returns (same result)
+};
+
+// Candidate lists for box queries: every primitive whose box overlaps the query box, in increasing id
+// (the candidates of a brute-force scan that survive its box test). Cell size >= the largest box, so
+// a box covers at most 2 cells per axis.
+template <typename R>
+struct BoxGrid {
+  double inv = 0.0;
+  std::vector<std::pair<long long, int>> cells;
+  static long long key(long long x, long long y, long long z) {
+    return ((x & 0x1FFFFF) << 42) | ((y & 0x1FFFFF) << 21) | (z & 0x1FFFFF);
+  }
+  long long c(R x) const { return (long long)std::floor(double(x) * inv); }
+  void build(const std::vector<V3<R>>& lo, const std::vector<V3<R>>& hi, double pad) {
+    double ext = 0.0;
+    for (size_t i = 0; i < lo.size(); ++i)
+      ext = std::max(ext, double(std::max(std::max(hi[i].x - lo[i].x, hi[i].y - lo[i].y), hi[i].z - lo[i].z)));
+    double size = std::max(ext, pad) * 1.01;
+    if (!(size > 1e-9) || !(size < 1e30)) size = size < 1e30 ? 1e-9 : 1e30;
+    inv = 1.0 / size;
+    cells.clear();
+    for (size_t i = 0; i < lo.size(); ++i)
+      for (long long x = c(lo[i].x); x <= c(hi[i].x); ++x)
+        for (long long y = c(lo[i].y); y <= c(hi[i].y); ++y)
+          for (long long z = c(lo[i].z); z <= c(hi[i].z); ++z) cells.push_back({key(x, y, z), int(i)});
+    std::sort(cells.begin(), cells.end());
+  }
+  void query(V3<R> qlo, V3<R> qhi, std::vector<int>& out) const {
+    out.clear();
+    for (long long x = c(qlo.x); x <= c(qhi.x); ++x)
+      for (long long y = c(qlo.y); y <= c(qhi.y); ++y)
+        for (long long z = c(qlo.z); z <= c(qhi.z); ++z) {
+          auto r = std::equal_range(cells.begin(), cells.end(), std::make_pair(key(x, y, z), 0),
+                                    [](const std::pair<long long, int>& a, const std::pair<long long, int>& b) {
+                                      return a.first < b.first;
+                                    });
+          for (auto it = r.first; it != r.second; ++it) out.push_back(it->second);
+        }
+    std::sort(out.begin(), out.end());
+    out.erase(std::unique(out.begin(), out.end()), out.end());
+  }
 };
 
 inline bool in_sorted(const int* off, const int* list, int row, int key) {
@@ -717,13 +762,24 @@ void sc_detect(const Model& M, const SelfContact& S, const std::vector<V3<R>>& p
     return alo.x <= bhi.x && alo.y <= bhi.y && alo.z <= bhi.z && ahi.x >= blo.x && ahi.y >= blo.y && ahi.z >= blo.z;
   };
   int ovf_v = 0, ovf_e = 0;
+  BoxGrid<R> tgrid, egrid;
+  if (!S.brute_force) {
+    tgrid.build(tlo, thi, 2.0 * S.margin);
+    egrid.build(elo, ehi, 2.0 * S.margin);
+  }
+  std::vector<int> all_t(T), all_e(E);
+  std::iota(all_t.begin(), all_t.end(), 0);
+  std::iota(all_e.begin(), all_e.end(), 0);
 #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 16) reduction(| : ovf_v)
   for (int v = 0; v < n; ++v) {
     const V3<R> p = pos[v];
     const V3<R> lo = v3<R>(p.x - margin, p.y - margin, p.z - margin), hi = v3<R>(p.x + margin, p.y + margin, p.z + margin);
     int cnt = 0;
     R mn = margin;
-    for (int t = 0; t < T; ++t) {
+    std::vector<int> cand;
+    if (!S.brute_force) tgrid.query(lo, hi, cand);
+    const std::vector<int>& list = S.brute_force ? all_t : cand;
+    for (int t : list) {
       if (!overlap(lo, hi, tlo[t], thi[t])) continue;
       const int* ti = M.tri_indices + 3 * t;
       if (v == ti[0] || v == ti[1] || v == ti[2]) continue;
@@ -757,7 +813,10 @@ void sc_detect(const Model& M, const SelfContact& S, const std::vector<V3<R>>& p
     const V3<R> lo = elo[e] - v3<R>(margin, margin, margin), hi = ehi[e] + v3<R>(margin, margin, margin);
     int cnt = 0;
     R mn = margin;
-    for (int e2 = 0; e2 < E; ++e2) {
+    std::vector<int> cand;
+    if (!S.brute_force) egrid.query(lo, hi, cand);
+    const std::vector<int>& list = S.brute_force ? all_e : cand;
+    for (int e2 : list) {
       if (!overlap(lo, hi, elo[e2], ehi[e2])) continue;
       const int* fi = M.edge_indices + 4 * e2;
       if (ei[2] == fi[2] || ei[2] == fi[3] || ei[3] == fi[2] || ei[3] == fi[3]) continue;
@@ -1096,6 +1155,7 @@ struct OracleSelfContact {
   int vertex_buffer, edge_buffer, interval;
   const double* rest_q;
   const int *vt_filter_offsets, *vt_filter, *ee_filter_offsets, *ee_filter;
+  int brute_force;
 };
 static_assert(sizeof(OracleSelfContact) == sizeof(SelfContact), "layout");
 

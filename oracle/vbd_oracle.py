@@ -48,17 +48,19 @@ class OracleSelfContact(C.Structure):
         ("radius", C.c_double), ("margin", C.c_double), ("relaxation", C.c_double),
         ("edge_parallel_epsilon", C.c_double), ("rest_exclusion", C.c_double), ("vertex_buffer", C.c_int),
         ("edge_buffer", C.c_int), ("interval", C.c_int), ("rest_q", _dp), ("vt_filter_offsets", _ip),
-        ("vt_filter", _ip), ("ee_filter_offsets", _ip), ("ee_filter", _ip),
+        ("vt_filter", _ip), ("ee_filter_offsets", _ip), ("ee_filter", _ip), ("brute_force", C.c_int),
     ]  # fmt: skip
 
 
 class SelfContact:
     """Self-contact settings with the ``SolverVBD`` keyword meanings (``solver_vbd.py:204-216``).
     ``vt_filter`` / ``ee_filter`` are (flat, offsets) CSR lists of filtered triangles per vertex and
-    filtered edges per edge, each row sorted, or None."""
+    filtered edges per edge, each row sorted, or None. ``brute_force`` tests every primitive pair in
+    the detection instead of the candidates of a box grid (the same pairs, slower)."""
 
     def __init__(self, rest_q, *, radius, margin, relaxation=0.85, vertex_buffer=32, edge_buffer=64, interval=0,
-                 edge_parallel_epsilon=1e-5, rest_exclusion=0.0, vt_filter=None, ee_filter=None):  # fmt: skip
+                 edge_parallel_epsilon=1e-5, rest_exclusion=0.0, vt_filter=None, ee_filter=None,
+                 brute_force=False):  # fmt: skip
         self._keep = []
 
         def ints(a):
@@ -77,7 +79,7 @@ class SelfContact:
             radius=radius, margin=margin, relaxation=relaxation, edge_parallel_epsilon=edge_parallel_epsilon,
             rest_exclusion=rest_exclusion, vertex_buffer=self.vertex_buffer, edge_buffer=self.edge_buffer,
             interval=int(interval), rest_q=rqp, vt_filter_offsets=ints(vfo), vt_filter=ints(vf),
-            ee_filter_offsets=ints(efo), ee_filter=ints(ef),
+            ee_filter_offsets=ints(efo), ee_filter=ints(ef), brute_force=int(bool(brute_force)),
         )  # fmt: skip
 
 

@@ -33,7 +33,7 @@ def _sc_kwargs(g):
         particle_conservative_bound_relaxation=float(g["sc_relaxation"]),
         particle_collision_detection_interval=int(g["sc_interval"]),
         particle_topological_contact_filter_threshold=int(g["sc_ring"]),
-        particle_rest_shape_contact_exclusion_radius=float(g["sc_rest_exclusion"]),
+        particle_rest_shape_contact_exclusion_radius=float(g.get("sc_rest_exclusion", 0.0)),
     )  # fmt: skip
 
 
@@ -113,7 +113,7 @@ def test_detector_matches_reference_detection(name):
                                    edge_filtering_list_offsets=g["sc_ee_filter_offsets"])  # fmt: skip
     for s in range(int(g["substeps"])):
         det.refit(_t(g[f"s{s}_q_in"]))
-        kw = dict(min_query_radius=float(g["sc_rest_exclusion"]), min_distance_filtering_ref_pos=model.particle_q)
+        kw = dict(min_query_radius=float(g.get("sc_rest_exclusion", 0.0)), min_distance_filtering_ref_pos=model.particle_q)
         det.vertex_triangle_collision_detection(float(g["sc_margin"]), **kw)
         det.edge_edge_collision_detection(float(g["sc_margin"]), **kw)
         torch.cuda.synchronize()
