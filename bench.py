@@ -612,6 +612,96 @@ def cpu_baseline_selfcontact(m, q, qd):
             "sample": "one substep of the same settled 256x256 state (self-contact detection on a box grid)"}  # fmt: skip
 
 
+def run_adjoint(args):
+    """Differentiable config: 64 x 64 hanging cloth (two top corners pinned), 60 frames x 10 substeps x 10
+    iterations; loss = mean squared distance of the final positions to a seeded target (rest shape plus
+    N(0, 0.05^2) per coordinate); gradient w.r.t. per-triangle Young's moduli (through the Lame map) and the
+    initial velocity by the hand-written adjoint, checked against FP64 central differences (h = 1e-4) along
+    32 seeded random directions."""
+    import torch
+
+    import newton_chysx_b200 as nb
+    from newton_chysx_b200.adjoint import DifferentiableVBD, lame_from_young
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    n, nu, h_th, frames = 64, 0.3, 1.0e-3, args.adjoint_frames
+    substeps = frames * 10
+    b = nb.ModelBuilder(up_axis="Z", gravity=-9.81)
+    rot = nb.quat_from_axis_angle((1.0, 0.0, 0.0), np.pi * 0.5)
+    b.add_cloth_grid(pos=(0.0, 0.0, 1.0), rot=rot, vel=(0.0, 0.0, 0.0), dim_x=n - 1, dim_y=n - 1, cell_x=1.0 / (n - 1),
+                     cell_y=1.0 / (n - 1), mass=0.2 / (n * n), tri_ke=1.0, tri_ka=1.0, tri_kd=0.0, edge_ke=1e-4,
+                     edge_kd=0.0, particle_radius=5e-3)  # fmt: skip
+    flags = b.particle_flags
+    flags[n * (n - 1)] &= ~int(nb.ParticleFlags.ACTIVE)
+    flags[n * n - 1] &= ~int(nb.ParticleFlags.ACTIVE)
+    b.set_particle_flags(flags)
+    b.color(include_bending=True)
+    model = b.finalize(dev)
+    rng = np.random.default_rng(args.seed)
+    T = model.tri_count
+    E = torch.tensor(10.0 ** rng.uniform(3.5, 4.5, size=T), dtype=torch.float64, device=dev)
+    q0 = model.particle_q.to(torch.float64)
+    qd0 = torch.zeros_like(q0)
+    target = q0 + torch.tensor(rng.normal(0.0, 0.05, size=q0.shape), dtype=torch.float64, device=dev)
+
+    def loss_of(sim, mu, lam, v0):
+        q, _ = sim.rollout(q0.to(sim.dtype), v0.to(sim.dtype), mu, lam, DT, substeps)
+        return ((q.to(torch.float64) - target) ** 2).sum(dim=1).mean()
+
+    out = {"workload": f"differentiable {n}x{n}, {frames} frames x 10 substeps x 10 iterations",
+           "vertices": model.particle_count, "triangles": T, "substeps": substeps}  # fmt: skip
+    grads = {}
+    for prec in ("fp64", "fp32"):
+        sim = DifferentiableVBD(model, iterations=ITERATIONS, precision=prec)
+        mu0, lam0 = lame_from_young(E, nu, h_th)
+        times = []
+        for rep in range(2):  # the first pass allocates the autograd buffers
+            mu, lam = mu0.clone().requires_grad_(True), lam0.clone().requires_grad_(True)
+            v0 = qd0.clone().requires_grad_(True)
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            L = loss_of(sim, mu, lam, v0)
+            torch.cuda.synchronize()
+            tf = time.perf_counter() - t
+            L.backward()
+            torch.cuda.synchronize()
+            times.append((tf, time.perf_counter() - t))
+        grads[prec] = (sim, mu.grad.detach(), lam.grad.detach(), v0.grad.detach(), float(L))
+        tf, tt = times[-1]
+        vi = model.particle_count * ITERATIONS * substeps
+        out[prec] = {"loss": float(L), "forward_s": tf, "forward_backward_s": tt,
+                     "forward_vertex_iters_per_s": vi / tf, "backward_vertex_iters_per_s": vi / (tt - tf)}  # fmt: skip
+    sim, gmu, glam, gv, _ = grads["fp64"]
+    h = 1e-4
+    worst, rels = 0.0, []
+    drng = np.random.default_rng(args.seed + 1)
+    for _ in range(args.adjoint_directions):
+        dE = torch.tensor(drng.normal(size=T), device=dev, dtype=torch.float64)
+        dv = torch.tensor(drng.normal(size=q0.shape), device=dev, dtype=torch.float64)
+        dE, dv = dE / dE.abs().max(), dv / dv.norm()
+        with torch.no_grad():
+            mu_p, lam_p = lame_from_young(E * (1.0 + h * dE), nu, h_th)
+            mu_m, lam_m = lame_from_young(E * (1.0 - h * dE), nu, h_th)
+            fd = float(loss_of(sim, mu_p, lam_p, qd0 + h * dv) - loss_of(sim, mu_m, lam_m, qd0 - h * dv))
+            # the model stores the Lame coefficients in float32: predict with the perturbation applied
+            d_mu = mu_p.float().double() - mu_m.float().double()
+            d_lam = lam_p.float().double() - lam_m.float().double()
+            ad = float((gmu * d_mu).sum() + (glam * d_lam).sum() + (gv * (2.0 * h * dv)).sum())
+        rel = abs(ad - fd) / max(abs(fd), 1e-30)
+        rels.append(rel)
+        worst = max(worst, rel)
+    g32 = grads["fp32"]
+    out["fd_check"] = {"directions": args.adjoint_directions, "h": h, "max_rel_err": worst,
+                       "median_rel_err": float(np.median(rels)), "tolerance": 1e-3, "pass": worst <= 1e-3}  # fmt: skip
+    out["fp32_vs_fp64_grad_rel"] = {
+        "mu": float((g32[1].double() - gmu).norm() / gmu.norm()),
+        "lambda": float((g32[2].double() - glam).norm() / glam.norm()),
+        "velocity": float((g32[3].double() - gv).norm() / gv.norm()),
+    }
+    return out
+
+
 def build_precision_model(n=1024, seed=4, sliver_fraction=1e-3):
     """1024 x 1024 sheet, per-triangle E log-uniform in [1e5, 1e8] Pa, 0.1% of vertex sites moved
     towards a neighbour so that incident triangles keep ~1e-6 of their nominal rest area."""
@@ -743,7 +833,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["batched", "plain", "precision", "selfcontact"], default="batched")
+    ap.add_argument("--workload", choices=["batched", "plain", "precision", "selfcontact", "adjoint"], default="batched")
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--lanes", type=int, default=0)
@@ -763,6 +853,8 @@ def main():
     ap.add_argument("--traffic", type=float, default=None, help="DRAM bytes per launch from an ncu capture")
     ap.add_argument("--sc-n", type=int, default=256, help="selfcontact workload: grid side (vertices)")
     ap.add_argument("--sc-settle-frames", type=int, default=40, help="selfcontact workload: untimed frames first")
+    ap.add_argument("--adjoint-frames", type=int, default=60)
+    ap.add_argument("--adjoint-directions", type=int, default=32)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     if args.impl == "reference":
@@ -773,6 +865,8 @@ def main():
         out = run_precision(args)
     elif args.workload == "selfcontact":
         out = run_selfcontact(args)
+    elif args.workload == "adjoint":
+        out = run_adjoint(args)
     else:
         out = run_ours(args)
     if out is not None:

@@ -1,8 +1,8 @@
 """B200-native cloth Vertex Block Descent: a drop-in for ``newton.solvers.SolverVBD``'s particle path.
 
 Public API mirrors the reference names: ``ModelBuilder``, ``Model``, ``State``, ``Control``,
-``Contacts``, ``CollisionPipeline``, ``ParticleFlags`` and ``SolverVBD``; ``solvers.SolverVBD`` is
-the same class. The solver runs in ``libvbd_b200.so`` (hand-written CUDA for sm_100a).
+``Contacts``, ``CollisionPipeline``, ``ParticleFlags``, ``TriMeshCollisionDetector`` and ``SolverVBD``;
+``solvers.SolverVBD`` is the same class. The solver runs in ``libvbd_b200.so`` (hand-written CUDA for sm_100a).
 """
 
 from .sim import (
@@ -18,6 +18,7 @@ from .sim import (
     quat_from_axis_angle,
     quat_identity,
 )
+from .collision import TriMeshCollisionDetector
 from .solver_vbd import SolverVBD
 
 
@@ -36,6 +37,7 @@ __all__ = [
     "ShapeConfig",
     "SolverVBD",
     "State",
+    "TriMeshCollisionDetector",
     "quat_from_axis_angle",
     "quat_identity",
     "solvers",

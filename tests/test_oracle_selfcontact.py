@@ -151,3 +151,21 @@ def test_selfcontact_step_fp32(golden_dir, name):
             self_contact=sc,
         )  # fmt: skip
         assert np.abs(q_out - g[f"s{s}_q_out"]).max() <= 1e-4, (name, s)
+
+
+def test_box_grid_detection_equals_brute_force(golden_dir):
+    """The oracle's box-grid candidate search gives exactly the brute-force buffers, overflow included."""
+    g = _load(golden_dir, "step_selfcontact_fold.npz")
+    model, _ = _scene(g)
+    rng = np.random.default_rng(1)
+    q = g["s0_q_in"] + rng.normal(scale=4e-3, size=g["s0_q_in"].shape)  # denser contacts
+    for vb, eb in ((32, 64), (2, 3)):
+        kw = dict(radius=0.012, margin=0.03, vertex_buffer=vb, edge_buffer=eb, rest_exclusion=0.02,
+                  vt_filter=(g["sc_vt_filter"], g["sc_vt_filter_offsets"]),
+                  ee_filter=(g["sc_ee_filter"], g["sc_ee_filter_offsets"]))  # fmt: skip
+        a = orc.collide(model, orc.SelfContact(g["model_particle_q"], **kw), q, 64)
+        b = orc.collide(model, orc.SelfContact(g["model_particle_q"], brute_force=True, **kw), q, 64)
+        for k in a:
+            np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+        assert a["vt_count"].sum() > 0 and a["ee_count"].sum() > 0
+        assert (a["resize_flags"][0] == 1) == (vb == 2)
