@@ -47,6 +47,10 @@ extern "C" {
 #define VBD_LAYOUT_ELL 2  /* per-incidence stencil records in sweep order, slot-major (one lane/vertex) */
 #define VBD_LAYOUT_ELL16 3 /* the same with 16-bit instance-local vertex ids: 32-byte face and 16-byte hinge
                               records (persistent schedule, instances below 65536 particles, no hinge damping) */
+#define VBD_LAYOUT_RING 4  /* one-ring fan records (16-bit instance-local ids): each vertex walks its fan once,
+                              sharing every incident face normal between the membrane, the two spoke hinges and
+                              the rim hinge of that face (persistent schedule, instances below 65536 particles,
+                              manifold fans of at most 8 triangles, no hinge damping) */
 
 typedef struct VbdModelDesc {
   int32_t particle_count; /* V */

@@ -28,7 +28,7 @@ VBD_DEVERR_SINGULAR_SKIPPED = 4
 PRECISION = {"fp32": 0, "mixed": 1, "fp64": 2}
 SCHEDULE = {"auto": 0, "per_color": 1, "persistent": 2}
 SCHEDULE_NAME = {v: k for k, v in SCHEDULE.items()}
-LAYOUT = {"auto": 0, "csr": 1, "ell": 2, "ell16": 3}
+LAYOUT = {"auto": 0, "csr": 1, "ell": 2, "ell16": 3, "ring": 4}
 LAYOUT_NAME = {v: k for k, v in LAYOUT.items()}
 
 _fp = C.POINTER(C.c_float)

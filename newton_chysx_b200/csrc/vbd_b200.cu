@@ -16,6 +16,7 @@
 #include "vbd_adjoint.cuh"
 #include "vbd_collide.cuh"
 #include "vbd_ell.cuh"
+#include "vbd_ring.cuh"
 
 using namespace vbd;
 
@@ -164,6 +165,12 @@ struct VbdSolver {
   float2* hinge_prop = nullptr;
   float* hinge_kd = nullptr;
   uint4 *ell16_faceA = nullptr, *ell16_faceB = nullptr, *ell16_hinge = nullptr;
+  // one-ring layout (vbd_ring.cuh)
+  int* ring_nslot = nullptr;
+  long long *ring_base = nullptr, *ring_vbase = nullptr;
+  uint4 *ring_A = nullptr, *ring_B = nullptr;
+  float4* ring_H = nullptr;
+  unsigned* ring_hdr = nullptr;
   std::vector<int> ell_nf, ell_ne;
   std::vector<long long> ell_fbase, ell_ebase;
   long long ell_faces = 0, ell_hinges = 0;
@@ -187,7 +194,8 @@ struct VbdSolver {
                   inst_order, inst_vstart, inst_cptr, color_ranges, color_verts, queue, pos, qprev, inertia,
                   slot_cnt, slots, c_k, c_ke, c_kd, c_mu, err, residual, range_nf, range_ne, range_fbase,
                   range_ebase, face_nb, face_dm, face_mat, face_kd, hinge_idx, hinge_prop, hinge_kd, adj_work,
-                  ell16_faceA, ell16_faceB, ell16_hinge, sc_pos_cd, sc_disp, sc_ts};
+                  ell16_faceA, ell16_faceB, ell16_hinge, sc_pos_cd, sc_disp, sc_ts, ring_nslot, ring_base,
+                  ring_vbase, ring_A, ring_B, ring_H, ring_hdr};
     for (void* p : ps)
       if (p) cudaFree(p);
     sc_release(sc);
@@ -357,6 +365,204 @@ int build_ell(VbdSolver* h) {
   if (fdamp && (rc = upload_into(&h->face_kd, fkd))) return rc;
   if (hdamp && (rc = upload_into(&h->hinge_kd, hkd))) return rc;
   return VBD_OK;
+}
+
+// One-ring records (vbd_ring.cuh) for the ranges in h->ranges_host / h->range_verts_host. Returns
+// VBD_ERR_UNSUPPORTED when a vertex's triangles do not form one fan of at most kRingMax triangles, or
+// when a hinge of the model does not sit where the fan walk evaluates it (a spoke between two fan
+// triangles, or a rim whose opposite vertices are the vertex and the outer vertex).
+int build_ring(VbdSolver* h) {
+  const VbdModelDesc& m = h->md;
+  std::vector<float> pose, mat, area, ra, rl, bp;
+  int rc;
+  if ((rc = download(pose, m.tri_poses_dev, size_t(4) * h->T)) || (rc = download(mat, m.tri_materials_dev, size_t(5) * h->T)) ||
+      (rc = download(area, m.tri_areas_dev, size_t(h->T))) || (rc = download(ra, m.edge_rest_angle_dev, size_t(h->E))) ||
+      (rc = download(rl, m.edge_rest_length_dev, size_t(h->E))) ||
+      (rc = download(bp, m.edge_bending_properties_dev, size_t(2) * h->E)))
+    return rc;
+  // interior hinges with stiffness, by their edge
+  auto key = [](int a, int b) { return a < b ? (uint64_t(unsigned(a)) << 32) | unsigned(b) : (uint64_t(unsigned(b)) << 32) | unsigned(a); };
+  std::vector<std::pair<uint64_t, int>> emap;
+  std::vector<int> live_count(h->V, 0);
+  for (int e = 0; e < h->E; ++e) {
+    const int* ei = &h->h_edges[4 * size_t(e)];
+    if (ei[0] < 0 || ei[1] < 0 || !(bp[2 * e] > 0.f)) continue;
+    if (bp[2 * e + 1] > 0.f) return VBD_ERR_UNSUPPORTED;  // hinge damping is not stored
+    emap.push_back({key(ei[2], ei[3]), e});
+    for (int q = 0; q < 4; ++q) live_count[ei[q]]++;
+  }
+  std::sort(emap.begin(), emap.end());
+  for (size_t i = 1; i < emap.size(); ++i)
+    if (emap[i].first == emap[i - 1].first) return VBD_ERR_UNSUPPORTED;  // two hinges on one edge
+  auto hinge_of = [&](int a, int b) -> int {
+    auto it = std::lower_bound(emap.begin(), emap.end(), std::make_pair(key(a, b), -1));
+    return (it != emap.end() && it->first == key(a, b)) ? it->second : -1;
+  };
+  const int R = int(h->ranges_host.size()) - 1;
+  std::vector<int> nslot(R, 0);
+  std::vector<long long> base(R, 0), vbase(R, 0);
+  // per vertex fan: ring ids, face (triangle, order) per slot, closed flag
+  struct Fan {
+    int k = 0;
+    bool closed = false;
+    int ring[kRingMax];
+    int tri[kRingMax];
+    int ord[kRingMax];
+  };
+  std::vector<Fan> fans(h->V);
+  for (int v = 0; v < h->V; ++v) {
+    Fan& F = fans[v];
+    const int nf = h->h_foff[v + 1] - h->h_foff[v];
+    if (nf == 0) continue;
+    if (nf > kRingMax) return VBD_ERR_UNSUPPORTED;
+    int fa[kRingMax], fb[kRingMax], ft[kRingMax], fo[kRingMax];
+    for (int q = 0; q < nf; ++q) {
+      const int t = h->h_fadj[h->h_foff[v] + q] >> 2, ord = h->h_fadj[h->h_foff[v] + q] & 3;
+      const int* ti = &h->h_tri[3 * size_t(t)];
+      fa[q] = ti[(ord + 1) % 3];
+      fb[q] = ti[(ord + 2) % 3];
+      ft[q] = t;
+      fo[q] = ord;
+    }
+    // start: a first vertex that no face ends in (open fan), else the first face's (closed fan)
+    int start = -1, nstart = 0;
+    for (int q = 0; q < nf; ++q) {
+      bool incoming = false;
+      for (int u = 0; u < nf; ++u) incoming |= fb[u] == fa[q];
+      if (!incoming) {
+        start = q;
+        ++nstart;
+      }
+    }
+    if (nstart > 1) return VBD_ERR_UNSUPPORTED;
+    F.closed = nstart == 0;
+    int q = F.closed ? 0 : start, used = 0;
+    std::vector<char> seen(nf, 0);
+    F.k = 0;
+    while (true) {
+      if (seen[q] || F.k >= kRingMax) return VBD_ERR_UNSUPPORTED;
+      seen[q] = 1;
+      ++used;
+      F.ring[F.k] = fa[q];
+      F.tri[F.k] = ft[q];
+      F.ord[F.k] = fo[q];
+      ++F.k;
+      int nq = -1;
+      for (int u = 0; u < nf; ++u)
+        if (fa[u] == fb[q]) {
+          if (nq >= 0) return VBD_ERR_UNSUPPORTED;
+          nq = u;
+        }
+      if (nq < 0) {  // open fan ends at fb[q]
+        if (F.closed || F.k >= kRingMax) return VBD_ERR_UNSUPPORTED;
+        F.ring[F.k] = fb[q];
+        F.tri[F.k] = -1;
+        ++F.k;
+        break;
+      }
+      if (F.closed && nq == 0) break;
+      q = nq;
+    }
+    if (used != nf) return VBD_ERR_UNSUPPORTED;
+  }
+  long long nrec = 0, nv = 0;
+  for (int r = 0; r < R; ++r) {
+    int ns = 0;
+    for (int k = h->ranges_host[r]; k < h->ranges_host[r + 1]; ++k) ns = std::max(ns, fans[h->range_verts_host[k]].k);
+    nslot[r] = ns;
+    base[r] = nrec;
+    vbase[r] = nv;
+    const long long n = h->ranges_host[r + 1] - h->ranges_host[r];
+    nrec += n * ns;
+    nv += n;
+  }
+  std::vector<uint4> A(size_t(std::max(nrec, 1LL)), make_uint4(0u, 0u, 0u, 0u)), B(A.size(), make_uint4(0u, 0u, 0u, 0u));
+  std::vector<float4> Hh(A.size(), make_float4(0.f, 0.f, 0.f, 0.f));
+  std::vector<unsigned> hdr(size_t(std::max(nv, 1LL)), 0u);
+  for (int r = 0; r < R; ++r) {
+    const int a0 = h->ranges_host[r];
+    const long long n = h->ranges_host[r + 1] - a0;
+    for (long long j = 0; j < n; ++j) {
+      const int v = h->range_verts_host[a0 + j];
+      const Fan& F = fans[v];
+      const int vs = h->inst_start_of_vertex[v];
+      hdr[vbase[r] + j] = unsigned(F.k) | (F.closed ? 0x100u : 0u);
+      int found = 0;
+      for (int i = 0; i < F.k; ++i) {
+        const long long idx = base[r] + i * n + j;
+        const int inext = i + 1 < F.k ? i + 1 : (F.closed ? 0 : -1);
+        const int iprev = i > 0 ? i - 1 : (F.closed ? F.k - 1 : -1);
+        unsigned o_loc = 0xffffu;
+        float mu = 0.f, lm = 0.f, kd = 0.f;
+        double P00 = 0, P01 = 0, P10 = 0, P11 = 0;
+        float4 hv = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (inext >= 0) {  // face i
+          const int t = F.tri[i], ord = F.ord[i];
+          const double D00 = pose[4 * t], D01 = pose[4 * t + 1], D10 = pose[4 * t + 2], D11 = pose[4 * t + 3];
+          P00 = D00, P01 = D01, P10 = D10, P11 = D11;
+          if (ord == 1) {
+            P00 = D10, P01 = D11, P10 = -D00 - D10, P11 = -D01 - D11;
+          } else if (ord == 2) {
+            P00 = -D00 - D10, P01 = -D01 - D11, P10 = D00, P11 = D01;
+          }
+          mu = mat[5 * t] * area[t];
+          lm = mat[5 * t + 1] * area[t];
+          kd = mat[5 * t + 2];
+          // rim hinge (v, o, r_i, r_{i+1})
+          const int e = hinge_of(F.ring[i], F.ring[inext]);
+          if (e >= 0) {
+            const int* ei = &h->h_edges[4 * size_t(e)];
+            int o;
+            if (ei[0] == v) o = ei[1];
+            else if (ei[1] == v) o = ei[0];
+            else return VBD_ERR_UNSUPPORTED;
+            const float sgn = (ei[0] == v ? 1.f : -1.f) * (ei[2] == F.ring[i] ? 1.f : -1.f);
+            hv.z = sgn * ra[e];
+            hv.w = bp[2 * e] * rl[e];
+            o_loc = unsigned(o - vs);
+            ++found;
+          }
+        }
+        if (inext >= 0 && iprev >= 0) {  // spoke (r_{i+1}, r_{i-1}, v, r_i)
+          const int e = hinge_of(v, F.ring[i]);
+          if (e >= 0) {
+            const int* ei = &h->h_edges[4 * size_t(e)];
+            const int rn = F.ring[inext], rp = F.ring[iprev];
+            if (!((ei[0] == rn && ei[1] == rp) || (ei[0] == rp && ei[1] == rn))) return VBD_ERR_UNSUPPORTED;
+            const float sgn = (ei[0] == rn ? 1.f : -1.f) * (ei[2] == v ? 1.f : -1.f);
+            hv.x = sgn * ra[e];
+            hv.y = bp[2 * e] * rl[e];
+            ++found;
+          }
+        }
+        const unsigned r_loc = unsigned(F.ring[i] - vs);
+        A[idx] = make_uint4(r_loc | (o_loc << 16), __float_as_uint_host(mu), __float_as_uint_host(lm),
+                            __float_as_uint_host(float(P00)));
+        B[idx] = make_uint4(__float_as_uint_host(float(P01)), __float_as_uint_host(float(P10)),
+                            __float_as_uint_host(float(P11)), __float_as_uint_host(kd));
+        Hh[idx] = hv;
+      }
+      if (found != live_count[v]) return VBD_ERR_UNSUPPORTED;  // a hinge the fan walk would miss
+    }
+  }
+  std::vector<int> ns(nslot);
+  if ((rc = upload_into(&h->ring_nslot, ns)) || (rc = upload_into(&h->ring_base, base)) ||
+      (rc = upload_into(&h->ring_vbase, vbase)) || (rc = upload_into(&h->ring_A, A)) || (rc = upload_into(&h->ring_B, B)) ||
+      (rc = upload_into(&h->ring_H, Hh)) || (rc = upload_into(&h->ring_hdr, hdr)))
+    return rc;
+  return VBD_OK;
+}
+
+RingView ring_view(const VbdSolver* h) {
+  RingView e;
+  e.range_nslot = h->ring_nslot;
+  e.range_base = h->ring_base;
+  e.range_vbase = h->ring_vbase;
+  e.A = h->ring_A;
+  e.B = h->ring_B;
+  e.H = h->ring_H;
+  e.hdr = h->ring_hdr;
+  return e;
 }
 
 Ell16View ell16_view(const VbdSolver* h) {
@@ -550,6 +756,17 @@ void launch_persistent_ell16(int occ, const StepCtx<R>& c, const PersistentPlan&
     case 3: k_persistent_ell16<R, MODE, SMEM, 3><<<grid, block, smem, st>>>(c, p, e); break;
     case 4: k_persistent_ell16<R, MODE, SMEM, 4><<<grid, block, smem, st>>>(c, p, e); break;
     default: k_persistent_ell16<R, MODE, SMEM, 0><<<grid, block, smem, st>>>(c, p, e); break;
+  }
+}
+
+template <typename R, int MODE, bool SMEM>
+void launch_persistent_ring(int occ, const StepCtx<R>& c, const PersistentPlan& p, const RingView& e, int grid,
+                            int block, size_t smem, cudaStream_t st) {
+  switch (occ) {
+    case 2: k_persistent_ring<R, MODE, SMEM, 2><<<grid, block, smem, st>>>(c, p, e); break;
+    case 3: k_persistent_ring<R, MODE, SMEM, 3><<<grid, block, smem, st>>>(c, p, e); break;
+    case 4: k_persistent_ring<R, MODE, SMEM, 4><<<grid, block, smem, st>>>(c, p, e); break;
+    default: k_persistent_ring<R, MODE, SMEM, 0><<<grid, block, smem, st>>>(c, p, e); break;
   }
 }
 
@@ -805,7 +1022,17 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
     }
     PersistentPlan p{h->W, h->inst_order, h->inst_vstart, h->inst_cptr, h->color_ranges, h->color_verts, h->queue,
                      iters};
-    if (h->layout == VBD_LAYOUT_ELL16) {
+    if (h->layout == VBD_LAYOUT_RING) {
+      const RingView e = ring_view(h);
+      if constexpr (std::is_same<R, float>::value) {
+        if (h->smem_bytes > 0)
+          launch_persistent_ring<R, MODE, true>(h->occ, c, p, e, h->grid_persistent, h->block, h->smem_bytes, st);
+        else
+          launch_persistent_ring<R, MODE, false>(h->occ, c, p, e, h->grid_persistent, h->block, 0, st);
+      } else {
+        launch_persistent_ring<R, MODE, false>(0, c, p, e, h->grid_persistent, h->block, 0, st);
+      }
+    } else if (h->layout == VBD_LAYOUT_ELL16) {
       const Ell16View e = ell16_view(h);
       if constexpr (std::is_same<R, float>::value) {
         if (h->smem_bytes > 0)
@@ -885,6 +1112,16 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
 }
 
 template <typename R, int MODE, bool SMEM>
+const void* persistent_ring_fn(int occ) {
+  switch (occ) {
+    case 2: return (const void*)k_persistent_ring<R, MODE, SMEM, 2>;
+    case 3: return (const void*)k_persistent_ring<R, MODE, SMEM, 3>;
+    case 4: return (const void*)k_persistent_ring<R, MODE, SMEM, 4>;
+    default: return (const void*)k_persistent_ring<R, MODE, SMEM, 0>;
+  }
+}
+
+template <typename R, int MODE, bool SMEM>
 const void* persistent_ell16_fn(int occ) {
   switch (occ) {
     case 2: return (const void*)k_persistent_ell16<R, MODE, SMEM, 2>;
@@ -907,6 +1144,12 @@ const void* persistent_ell_fn(int occ) {
 
 const void* persistent_kernel(VbdSolver* h) {
   const bool sm = h->smem_bytes > 0;
+  if (h->layout == VBD_LAYOUT_RING) {
+    if (h->precision == VBD_PRECISION_FP64) return persistent_ring_fn<double, MODE_FP64, false>(0);
+    if (h->precision == VBD_PRECISION_MIXED)
+      return sm ? persistent_ring_fn<float, MODE_MIXED, true>(h->occ) : persistent_ring_fn<float, MODE_MIXED, false>(h->occ);
+    return sm ? persistent_ring_fn<float, MODE_FP32, true>(h->occ) : persistent_ring_fn<float, MODE_FP32, false>(h->occ);
+  }
   if (h->layout == VBD_LAYOUT_ELL16) {
     if (h->precision == VBD_PRECISION_FP64) return persistent_ell16_fn<double, MODE_FP64, false>(0);
     if (h->precision == VBD_PRECISION_MIXED)
@@ -1177,7 +1420,8 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
   // element data layout: stencil records (one thread per vertex) unless lanes per vertex > 1 asks for CSR;
   // the compact 16-bit records when the persistent schedule runs instances below 65536 particles and no
   // hinge carries damping
-  if ((params->layout == VBD_LAYOUT_ELL || params->layout == VBD_LAYOUT_ELL16) && h->L != 1)
+  if ((params->layout == VBD_LAYOUT_ELL || params->layout == VBD_LAYOUT_ELL16 || params->layout == VBD_LAYOUT_RING) &&
+      h->L != 1)
     return fail(VBD_ERR_INVALID_ARGUMENT);
   bool any_hinge_damping = false;
   {
@@ -1186,9 +1430,12 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
     for (int e = 0; e < h->E; ++e) any_hinge_damping |= bp[2 * e] > 0.f && bp[2 * e + 1] > 0.f;
   }
   const bool ell16_ok = h->schedule == VBD_SCHEDULE_PERSISTENT && h->max_inst_v < 65536 && !any_hinge_damping;
-  if (params->layout == VBD_LAYOUT_ELL16 && !ell16_ok) return fail(VBD_ERR_UNSUPPORTED);
+  if ((params->layout == VBD_LAYOUT_ELL16 || params->layout == VBD_LAYOUT_RING) && !ell16_ok)
+    return fail(VBD_ERR_UNSUPPORTED);
   if (params->layout == VBD_LAYOUT_CSR || h->L != 1)
     h->layout = VBD_LAYOUT_CSR;
+  else if (params->layout == VBD_LAYOUT_RING)
+    h->layout = VBD_LAYOUT_RING;
   else if (params->layout == VBD_LAYOUT_ELL16 || (params->layout == VBD_LAYOUT_AUTO && ell16_ok))
     h->layout = VBD_LAYOUT_ELL16;
   else
@@ -1196,19 +1443,19 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
   h->inst_start_of_vertex.assign(h->V, 0);
   for (int w = 0; w < h->W; ++w)
     for (int i = wstart[w]; i < wstart[w + 1]; ++i) h->inst_start_of_vertex[i] = wstart[w];
-  if ((h->layout == VBD_LAYOUT_ELL || h->layout == VBD_LAYOUT_ELL16) && h->schedule == VBD_SCHEDULE_PERSISTENT &&
-      h->block > 512)
+  if ((h->layout == VBD_LAYOUT_ELL || h->layout == VBD_LAYOUT_ELL16 || h->layout == VBD_LAYOUT_RING) &&
+      h->schedule == VBD_SCHEDULE_PERSISTENT && h->block > 512)
     return fail(VBD_ERR_INVALID_ARGUMENT);
   if (params->min_blocks_per_sm != 0) {
     if (params->min_blocks_per_sm < 2 || params->min_blocks_per_sm > 4 ||
-        (h->layout != VBD_LAYOUT_ELL && h->layout != VBD_LAYOUT_ELL16) ||
+        (h->layout != VBD_LAYOUT_ELL && h->layout != VBD_LAYOUT_ELL16 && h->layout != VBD_LAYOUT_RING) ||
         h->schedule != VBD_SCHEDULE_PERSISTENT || h->precision == VBD_PRECISION_FP64 ||
         (params->block_size != 0 && params->block_size != 256))
       return fail(VBD_ERR_INVALID_ARGUMENT);
     h->occ = params->min_blocks_per_sm;
     h->block = 256;
   }
-  if (h->layout == VBD_LAYOUT_ELL || h->layout == VBD_LAYOUT_ELL16) {
+  if (h->layout == VBD_LAYOUT_ELL || h->layout == VBD_LAYOUT_ELL16 || h->layout == VBD_LAYOUT_RING) {
     if (h->schedule == VBD_SCHEDULE_PERSISTENT) {
       h->range_verts_host = verts;
       h->ranges_host.clear();
@@ -1219,7 +1466,7 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
       h->range_verts_host = colp;
       h->ranges_host = h->color_offsets;
     }
-    if ((rc = build_ell(h))) return fail(rc);
+    if ((rc = h->layout == VBD_LAYOUT_RING ? build_ring(h) : build_ell(h))) return fail(rc);
   }
   if (h->schedule == VBD_SCHEDULE_PERSISTENT && (rc = occupancy_grid(h))) return fail(rc);
   if (cudaDeviceSynchronize() != cudaSuccess) return fail(VBD_ERR_CUDA);
@@ -1231,8 +1478,16 @@ int vbd_refresh_model(VbdHandle h, void* stream) {
   if (!h) return VBD_ERR_INVALID_ARGUMENT;
   int rc = pack_model(h, (cudaStream_t)stream);
   if (rc) return rc;
-  if (h->layout == VBD_LAYOUT_ELL || h->layout == VBD_LAYOUT_ELL16) {
+  if (h->layout == VBD_LAYOUT_ELL || h->layout == VBD_LAYOUT_ELL16 || h->layout == VBD_LAYOUT_RING) {
     if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return VBD_ERR_CUDA;
+    if (h->layout == VBD_LAYOUT_RING) {
+      for (void** p : {(void**)&h->ring_nslot, (void**)&h->ring_base, (void**)&h->ring_vbase, (void**)&h->ring_A,
+                       (void**)&h->ring_B, (void**)&h->ring_H, (void**)&h->ring_hdr}) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+      }
+      return build_ring(h);
+    }
     return build_ell(h);
   }
   return VBD_OK;

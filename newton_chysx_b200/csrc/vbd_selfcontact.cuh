@@ -175,11 +175,6 @@ __host__ __device__ __forceinline__ void sc_friction(R mu, R fn, vec3<R> n, vec3
   }
 }
 
-struct ScParams {
-  float radius, ke, kd, mu;
-  float ee_eps;
-};
-
 // Vertex-triangle pair, x = (a, b, c, p) current and xa at the start of the step. Adds the term of slot
 // `order` (0..2: triangle vertex, 3: the colliding vertex). Returns false when the pair is not in contact.
 template <typename R>
@@ -198,9 +193,11 @@ __device__ __forceinline__ bool sc_vt_add(int order, const vec3<R> x[4], const v
   vec3<R> ff;
   sym3<R> fH;
   sc_friction(mu, -dEdD, n, dx, eps_u, ff, fH);
-  const R w = order == 3 ? R(1) : -bary[order];
+  // the slot's weight and displacement picked with selects (no dynamic indexing of local arrays)
+  const R w = order == 3 ? R(1) : -(order == 0 ? bary[0] : (order == 1 ? bary[1] : bary[2]));
   const R sgn = order == 3 ? R(1) : R(-1);
-  sc_slot_add(w, sgn, n, dEdD, d2E, xa[order] - x[order], ff, fH, kd / dt, f, H);
+  const vec3<R> disp = order == 0 ? xa[0] - x[0] : (order == 1 ? xa[1] - x[1] : (order == 2 ? xa[2] - x[2] : xa[3] - x[3]));
+  sc_slot_add(w, sgn, n, dEdD, d2E, disp, ff, fH, kd / dt, f, H);
   return true;
 }
 
@@ -221,7 +218,8 @@ __device__ __forceinline__ bool sc_ee_add(int order, const vec3<R> x[4], const v
   sym3<R> fH;
   sc_friction(mu, -dEdD, n, dx, eps_u, ff, fH);
   const R w = order == 0 ? R(1) - s : s;
-  sc_slot_add(w, R(1), n, dEdD, d2E, xa[order] - x[order], ff, fH, kd / dt, f, H);
+  const vec3<R> disp = order == 0 ? xa[0] - x[0] : xa[1] - x[1];
+  sc_slot_add(w, R(1), n, dEdD, d2E, disp, ff, fH, kd / dt, f, H);
   return true;
 }
 

@@ -22,7 +22,8 @@ FIXTURES = ["step_grid_ground.npz", "step_grid_sphere.npz", "step_complex_rest_a
 LAUNCH = [("per_color", 1, "auto", "ell"), ("per_color", 1, "auto", "csr"), ("per_color", 4, "auto", "csr"),
           ("persistent", 1, "on", "ell"), ("persistent", 1, "off", "ell"), ("persistent", 1, "on", "csr"),
           ("persistent", 8, "on", "csr"), ("persistent", 32, "on", "csr"), ("persistent", 4, "off", "csr"),
-          ("persistent", 1, "on", "ell16"), ("persistent", 1, "off", "ell16")]
+          ("persistent", 1, "on", "ell16"), ("persistent", 1, "off", "ell16"), ("persistent", 1, "on", "ring"),
+          ("persistent", 1, "off", "ring")]
 
 
 def _state(arr, dtype=torch.float32):
@@ -46,8 +47,8 @@ def _run_golden_substep(solver, g, s, dtype=torch.float32):
 @pytest.mark.parametrize("schedule,lanes,shared,layout", LAUNCH)
 def test_fp32_step_matches_reference_goldens(name, schedule, lanes, shared, layout):
     g = load_golden(name)
-    if layout == "ell16" and np.any(g["model_edge_bending_properties"][:, 1] > 0.0):
-        pytest.skip("the 16-bit stencil layout does not store hinge damping")
+    if layout in ("ell16", "ring") and np.any(g["model_edge_bending_properties"][:, 1] > 0.0):
+        pytest.skip("the 16-bit stencil and one-ring layouts do not store hinge damping")
     model = model_from_golden(g)
     solver = SolverVBD(model, iterations=int(g["iterations"]), friction_epsilon=float(g["friction_epsilon"]),
                        rigid_avbd_beta=float(g["beta"]), schedule=schedule, lanes_per_vertex=lanes,

@@ -165,7 +165,8 @@ def test_schedules_and_lane_counts_agree():
                                             ("per_color", 8, "auto", "csr"), ("persistent", 1, "on", "ell"),
                                             ("persistent", 1, "off", "ell"), ("persistent", 16, "on", "csr"),
                                             ("persistent", 2, "off", "csr"), ("persistent", 1, "on", "ell16"),
-                                            ("persistent", 1, "off", "ell16")]:
+                                            ("persistent", 1, "off", "ell16"), ("persistent", 1, "on", "ring"),
+                                            ("persistent", 1, "off", "ring")]:
         solver = SolverVBD(model, iterations=10, schedule=schedule, lanes_per_vertex=lanes, positions_in_shared=shared,
                            layout=layout)  # fmt: skip
         s = _run(model, solver, 3, 10, 1.0 / 600.0, CollisionPipeline(model))
@@ -190,7 +191,8 @@ def test_batched_worlds_match_single_instances():
     s = _run(model, solver, 2, 10, 1.0 / 600.0)
     q = s.particle_q.cpu().numpy()
     assert solver.layout == "ell16"
-    for shared, layout in [("off", "ell"), ("on", "csr"), ("off", "csr"), ("off", "ell16")]:
+    for shared, layout in [("off", "ell"), ("on", "csr"), ("off", "csr"), ("off", "ell16"), ("off", "ring"),
+                           ("on", "ring")]:
         s_g = _run(model, SolverVBD(model, iterations=10, schedule="persistent", positions_in_shared=shared,
                                     layout=layout), 2, 10, 1.0 / 600.0)  # fmt: skip
         assert np.abs(s_g.particle_q.cpu().numpy() - q).max() <= 1e-5
