@@ -40,6 +40,13 @@ ITERATIONS = 10
 DT = 1.0 / 600.0
 
 
+# DRAM bytes (read + write) per vertex-iteration of the solve kernel, from one ncu capture per layout of the
+# first 512 instances of this workload; the traffic of a full launch scales with its vertex-iterations.
+NCU_TRAFFIC_PER_VI = {
+    "ell16": (548.0, "ncu capture, 512 instances (profiles/k_persistent_ell16_batched512.md), scaled by vertex-iterations"),
+}
+
+
 def _peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -309,6 +316,10 @@ def run_ours(args):
         e2e = {"value": world * vi_step * Ke / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 2 * hq.numel() * 4,
                "d2h_bytes_per_step": 2 * oq.numel() * 4, "steps": Ke}  # fmt: skip
 
+    traffic, traffic_src = args.traffic, "--traffic (ncu capture)" if args.traffic is not None else None
+    if traffic is None and solver.layout in NCU_TRAFFIC_PER_VI:
+        per_vi, traffic_src = NCU_TRAFFIC_PER_VI[solver.layout]
+        traffic = per_vi * vi_step
     out = None
     if rank == 0:
         out = {
@@ -355,7 +366,8 @@ def run_ours(args):
                 "peak": peak,
                 "unit": "GB/s",
                 "frac": achieved / peak,
-                "traffic": args.traffic,
+                "traffic": traffic,
+                "traffic_source": traffic_src,
                 "peak_source": peak_src,
                 "bytes_per_vertex_iteration": bvi,
                 "kernel": "k_persistent (per-substep solve)",

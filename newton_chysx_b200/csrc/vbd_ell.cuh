@@ -239,6 +239,12 @@ namespace vbd {
 //           where i0, i1, i2 are the hinge's other three vertices in (o0, o1, v0, v1) order and role
 //           (0..3) is the solved vertex's place among the four. Hinge damping is not stored: models
 //           with non-zero hinge damping use the 32-bit stencil layout.
+// Stencil records are read once per sweep and never again before the next iteration: ask L2 for the
+// records a few slots ahead (no registers held), and load them with the streaming hint so that they do
+// not push the vertex positions out of L1.
+constexpr int kRecordPrefetch = 3;
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 struct Ell16View {
   const int* range_nf;
   const int* range_ne;
@@ -265,16 +271,24 @@ __device__ __forceinline__ void solve_ell16(const StepCtx<R>& c, const P& pos, c
     const uint4* pb = e.faceB + b0;
     uint4 A_n = make_uint4(0u, 0u, 0u, 0u), B_n = make_uint4(0u, 0u, 0u, 0u);
     if (nf > 0) {
-      A_n = __ldg(pa);
-      B_n = __ldg(pb);
+      A_n = __ldcs(pa);
+      B_n = __ldcs(pb);
+    }
+    for (int q = 1; q < kRecordPrefetch && q < nf; ++q) {
+      prefetch_l2(pa + (long long)q * n);
+      prefetch_l2(pb + (long long)q * n);
     }
     for (int s = 0; s < nf; ++s) {
       const uint4 A = A_n, B = B_n;
+      if (s + kRecordPrefetch < nf) {
+        prefetch_l2(pa + (long long)kRecordPrefetch * n);
+        prefetch_l2(pb + (long long)kRecordPrefetch * n);
+      }
       if (s + 1 < nf) {
         pa += n;
         pb += n;
-        A_n = __ldg(pa);
-        B_n = __ldg(pb);
+        A_n = __ldcs(pa);
+        B_n = __ldcs(pb);
       }
       const float muA = __uint_as_float(A.y), lmA = __uint_as_float(A.z);
       if (!(muA > 0.f || lmA > 0.f)) continue;
@@ -295,12 +309,14 @@ __device__ __forceinline__ void solve_ell16(const StepCtx<R>& c, const P& pos, c
     const long long b0 = __ldg(e.range_ebase + r) + j;
     const uint4* ph = e.hinge + b0;
     uint4 h_n = make_uint4(0u, 0u, 0u, 0u);
-    if (ne > 0) h_n = __ldg(ph);
+    if (ne > 0) h_n = __ldcs(ph);
+    for (int q = 1; q < kRecordPrefetch && q < ne; ++q) prefetch_l2(ph + (long long)q * n);
     for (int s = 0; s < ne; ++s) {
       const uint4 hh = h_n;
+      if (s + kRecordPrefetch < ne) prefetch_l2(ph + (long long)kRecordPrefetch * n);
       if (s + 1 < ne) {
         ph += n;
-        h_n = __ldg(ph);
+        h_n = __ldcs(ph);
       }
       const float k = __uint_as_float(hh.w);
       if (!(k > 0.f)) continue;
