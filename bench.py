@@ -626,16 +626,18 @@ def cpu_baseline_selfcontact(m, q, qd):
 
 
 def run_adjoint(args):
-    """Differentiable config: 64 x 64 hanging cloth (a curtain: the whole top row pinned), 60 frames x 10
-    substeps x 10 iterations; loss = mean squared distance of the final positions to a seeded target (rest
-    shape plus N(0, 0.05^2) per coordinate); gradient w.r.t. per-triangle Young's moduli (through the Lame
-    map) and the initial velocity by the hand-written adjoint, checked against FP64 central differences
-    (h = 1e-4) along 32 seeded random directions.
+    """Differentiable config: 64 x 64 hanging cloth (a curtain: the whole top row pinned, bending ke 1e-2),
+    60 frames x 10 substeps x 10 iterations; loss = mean squared distance of the final positions to a
+    seeded target (rest shape plus N(0, 0.05^2) per coordinate); gradient w.r.t. per-triangle Young's
+    moduli (through the Lame map) and the initial velocity by the hand-written adjoint, checked against
+    FP64 central differences (h = 1e-4) along 32 seeded random directions.
 
-    The whole top row is pinned because a sheet hung from two corners starts on an unstable equilibrium:
-    the flat sheet sags and compresses in its middle, so any out-of-plane velocity grows into buckling
-    exponentially, and its derivative w.r.t. the initial velocity is ~1e14 after 240 substeps. Central
-    differences then only agree with the adjoint below h ~ 1e-7 (measured), not at h = 1e-4."""
+    Why a curtain with some bending stiffness: a sheet hung from two corners, or one whose bending is
+    negligible (ke 1e-4), passes through compressed states where out-of-plane motion buckles
+    exponentially; the derivative w.r.t. the initial velocity then grows to ~1e14 after 240 substeps and
+    central differences agree with the adjoint only below h ~ 1e-7 (measured), so a check at h = 1e-4
+    says nothing. With the top row pinned and ke = 1e-2 the 600-substep derivatives stay O(1e-4) and
+    central differences agree to ~1e-6."""
     import torch
 
     import newton_chysx_b200 as nb
@@ -648,7 +650,7 @@ def run_adjoint(args):
     b = nb.ModelBuilder(up_axis="Z", gravity=-9.81)
     rot = nb.quat_from_axis_angle((1.0, 0.0, 0.0), np.pi * 0.5)
     b.add_cloth_grid(pos=(0.0, 0.0, 1.0), rot=rot, vel=(0.0, 0.0, 0.0), dim_x=n - 1, dim_y=n - 1, cell_x=1.0 / (n - 1),
-                     cell_y=1.0 / (n - 1), mass=0.2 / (n * n), tri_ke=1.0, tri_ka=1.0, tri_kd=0.0, edge_ke=1e-4,
+                     cell_y=1.0 / (n - 1), mass=0.2 / (n * n), tri_ke=1.0, tri_ka=1.0, tri_kd=0.0, edge_ke=1e-2,
                      edge_kd=0.0, particle_radius=5e-3)  # fmt: skip
     flags = b.particle_flags
     for i in range(n * (n - 1), n * n):
@@ -688,7 +690,7 @@ def run_adjoint(args):
         grads[prec] = (sim, mu.grad.detach(), lam.grad.detach(), v0.grad.detach(), float(L.detach()))
         tf, tt = times[-1]
         vi = model.particle_count * ITERATIONS * substeps
-        out[prec] = {"loss": float(L), "forward_s": tf, "forward_backward_s": tt,
+        out[prec] = {"loss": float(L.detach()), "forward_s": tf, "forward_backward_s": tt,
                      "forward_vertex_iters_per_s": vi / tf, "backward_vertex_iters_per_s": vi / (tt - tf)}  # fmt: skip
     sim, gmu, glam, gv, _ = grads["fp64"]
     h = 1e-4
