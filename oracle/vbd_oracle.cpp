@@ -18,7 +18,8 @@
 //              2877-2897 (apply_truncation_ts), 2900-2967 (contact accumulation),
 //              3135-3273 (solve_elasticity, the non-tile accumulation order)
 //              solver_vbd.py:1575-1622, 1669-1766, 2151-2337, 2339-2376, 2763-2774 (sequencing)
-//   adjacency  particle_vbd_kernels.py:639-738 (count/fill order)
+//   adjacency  particle_vbd_kernels.py:639-738, 774-825 (count/fill order)
+//   springs    particle_vbd_kernels.py:2299-2397; tetrahedra :154-224, 335-546 (stable Neo-Hookean)
 //   contacts   geometry/kernels.py:1001-1140 for PLANE (infinite) and SPHERE shapes
 //   self-contact particle_vbd_kernels.py:1193-1222 (barrier), 1225-1238 (damping), 1371-1506 (edge-edge),
 //              1599-1745 (vertex-triangle), 1748-1779 (friction), 1930-2071 (accumulation),
@@ -88,6 +89,11 @@ template <typename R> inline M3<R> operator*(M3<R> a, R s) {
   return a;
 }
 template <typename R> inline M3<R> operator*(R s, M3<R> a) { return a * s; }
+template <typename R> inline M3<R> operator/(M3<R> a, R s) {
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) a.m[i][j] /= s;
+  return a;
+}
 template <typename R> inline M3<R> operator-(M3<R> a) { return a * R(-1); }
 template <typename R> inline M3<R> operator*(const M3<R>& a, const M3<R>& b) {
   M3<R> r = mzero<R>();
@@ -311,6 +317,80 @@ void contact_force(R pen, V3<R> n, V3<R> rel, R ke, R kd, R mu, R fric_eps, R dt
   hessian = hessian + fH;
 }
 
+// ------------------------------------------------------------------------------------ springs, tetrahedra
+// particle_vbd_kernels.py:2299-2343 (evaluate_spring_force_and_hessian_both_vertices): forces on both
+// endpoints and the shared Hessian k (I - l0/l (I - d d^T / l^2)) plus damping (kd/dt) H.
+template <typename R>
+void spring_both(V3<R> x0, V3<R> x1, V3<R> xa0, V3<R> xa1, R l0, R ke, R kd, R dt, V3<R>& f0, V3<R>& f1, M3<R>& Ht) {
+  const V3<R> diff = x0 - x1;
+  R len = length(diff);
+  len = rmax(len, R(1e-8));
+  const V3<R> base = (ke * (l0 - len) / len) * diff;
+  const M3<R> I = ident<R>();
+  const M3<R> Hs = ke * (I - (l0 / len) * (I - outer(diff, diff) / (len * len)));
+  const M3<R> hd = Hs * (kd / dt);
+  f0 = base + hd * (xa0 - x0);
+  f1 = -base + hd * (xa1 - x1);
+  Ht = Hs + hd;
+}
+
+// particle_vbd_kernels.py:335-473 (evaluate_volumetric_neo_hookean_force_and_hessian) with the vertex block
+// of assemble_tet_vertex_force_and_hessian (:154-224) written out: with P = V (mu F + s cof(F)) and the
+// 9x9 Hessian V (mu I + lambda_nh c c^T), c = vec(cof F), the block for the vertex with row m of the rest
+// inverse is  f = -V (mu F m + s cof(F) m),  h = V (mu |m|^2 I + lambda_nh g g^T),  g = cof(F) m.
+template <typename R>
+void tet_force(int order, const V3<R> x[4], const V3<R> xp[4], const R Dinv[9], R mu, R lmbd, R damping, R dt, V3<R>& f,
+               M3<R>& h) {
+  M3<R> D;
+  for (int i = 0; i < 9; ++i) D.m[i / 3][i % 3] = Dinv[i];
+  const R rest_volume = R(1) / (det(D) * R(6));
+  M3<R> Ds;
+  const V3<R> c1 = x[1] - x[0], c2 = x[2] - x[0], c3 = x[3] - x[0];
+  Ds.m[0][0] = c1.x, Ds.m[1][0] = c1.y, Ds.m[2][0] = c1.z;
+  Ds.m[0][1] = c2.x, Ds.m[1][1] = c2.y, Ds.m[2][1] = c2.z;
+  Ds.m[0][2] = c3.x, Ds.m[1][2] = c3.y, Ds.m[2][2] = c3.z;
+  const M3<R> F = Ds * D;
+  const R J = det(F);
+  const R mu_nh = mu, lmbd_nh = lmbd + mu;
+  const R lsafe = rsign(lmbd_nh) * rmax(std::fabs(lmbd_nh), R(1e-6));
+  const R alpha = R(1) + mu_nh / lsafe;
+  M3<R> cof;  // cofactor: cof[a][i] = d det F / d F[a][i]
+  cof.m[0][0] = F.m[1][1] * F.m[2][2] - F.m[1][2] * F.m[2][1];
+  cof.m[0][1] = F.m[1][2] * F.m[2][0] - F.m[1][0] * F.m[2][2];
+  cof.m[0][2] = F.m[1][0] * F.m[2][1] - F.m[1][1] * F.m[2][0];
+  cof.m[1][0] = F.m[0][2] * F.m[2][1] - F.m[0][1] * F.m[2][2];
+  cof.m[1][1] = F.m[0][0] * F.m[2][2] - F.m[0][2] * F.m[2][0];
+  cof.m[1][2] = F.m[0][1] * F.m[2][0] - F.m[0][0] * F.m[2][1];
+  cof.m[2][0] = F.m[0][1] * F.m[1][2] - F.m[0][2] * F.m[1][1];
+  cof.m[2][1] = F.m[0][2] * F.m[1][0] - F.m[0][0] * F.m[1][2];
+  cof.m[2][2] = F.m[0][0] * F.m[1][1] - F.m[0][1] * F.m[1][0];
+  const R s = lmbd_nh * (J - alpha);
+  V3<R> m;
+  if (order == 0)
+    m = v3<R>(-(Dinv[0] + Dinv[3] + Dinv[6]), -(Dinv[1] + Dinv[4] + Dinv[7]), -(Dinv[2] + Dinv[5] + Dinv[8]));
+  else
+    m = v3<R>(Dinv[3 * (order - 1)], Dinv[3 * (order - 1) + 1], Dinv[3 * (order - 1) + 2]);
+  const V3<R> Fm = F * m, g = cof * m;
+  f = (-rest_volume) * (mu_nh * Fm + s * g);
+  h = rest_volume * ((mu_nh * dot(m, m)) * ident<R>() + lmbd_nh * outer(g, g));
+  if (damping > R(0)) {
+    const R inv_dt = R(1) / dt;
+    M3<R> Dd;
+    const V3<R> d0 = x[0] - xp[0];
+    const V3<R> e1 = ((x[1] - xp[1]) - d0) * inv_dt, e2 = ((x[2] - xp[2]) - d0) * inv_dt, e3 = ((x[3] - xp[3]) - d0) * inv_dt;
+    Dd.m[0][0] = e1.x, Dd.m[1][0] = e1.y, Dd.m[2][0] = e1.z;
+    Dd.m[0][1] = e2.x, Dd.m[1][1] = e2.y, Dd.m[2][1] = e2.z;
+    Dd.m[0][2] = e3.x, Dd.m[1][2] = e3.y, Dd.m[2][2] = e3.z;
+    const M3<R> Fd = Dd * D;
+    R cfd = 0;  // c . vec(F_dot)
+    for (int a = 0; a < 3; ++a)
+      for (int i = 0; i < 3; ++i) cfd += cof.m[a][i] * Fd.m[a][i];
+    // P_damp = damping V (mu vec(F_dot) + lambda_nh c (c . vec(F_dot))), contracted with m
+    f = f + (-damping * rest_volume) * (mu_nh * (Fd * m) + (lmbd_nh * cfd) * g);
+    h = h * (R(1) + damping * inv_dt);
+  }
+}
+
 // ------------------------------------------------------------------------------------ model
 struct Model {
   int n, T, E, C, S;
@@ -326,6 +406,14 @@ struct Model {
   double soft_ke, soft_kd, soft_mu;
   const double *shape_ke, *shape_kd, *shape_mu;
   double friction_epsilon, beta;
+  // springs and tetrahedra (0 / null when the model has none)
+  int spring_count;
+  const int* spring_indices;  // [2 * spring_count]
+  const double *spring_rest_length, *spring_stiffness, *spring_damping;
+  int tet_count;
+  const int* tet_indices;          // [4 * tet_count]
+  const double *tet_poses, *tet_materials;  // rest D^-1 (row-major 3x3), (mu, lambda, damping)
+  const int *adj_tet_offsets, *adj_tets;    // reference layout: two ints (tet, order) per entry
 };
 
 struct Contacts {
@@ -1037,6 +1125,23 @@ int step(const Model& M, double* q_in, const double* qd_in, const double* f_ext,
           hess[p] = hess[p] + H;
         }
       }
+      // accumulate_spring_force_and_hessian (particle_vbd_kernels.py:2346-2397), in spring order
+      for (int sp = 0; sp < M.spring_count; ++sp) {
+        const int a = M.spring_indices[2 * sp], b = M.spring_indices[2 * sp + 1];
+        if (M.particle_colors[a] != color && M.particle_colors[b] != color) continue;
+        V3<R> f0, f1;
+        M3<R> Hs;
+        spring_both(pos[a], pos[b], q_prev[a], q_prev[b], R(M.spring_rest_length[sp]), R(M.spring_stiffness[sp]),
+                    R(M.spring_damping[sp]), dt, f0, f1, Hs);
+        if (M.particle_colors[a] == color) {
+          forces[a] = forces[a] + f0;
+          hess[a] = hess[a] + Hs;
+        }
+        if (M.particle_colors[b] == color) {
+          forces[b] = forces[b] + f1;
+          hess[b] = hess[b] + Hs;
+        }
+      }
       if (S) sc_accumulate(M, *S, B, color, pos, q_prev, dt, forces, hess);
       // solve_elasticity (particle_vbd_kernels.py:3135-3273)
       const int c0 = M.color_offsets[color], c1 = M.color_offsets[color + 1];
@@ -1085,6 +1190,22 @@ int step(const Model& M, double* q_in, const double* qd_in, const double* f_ext,
             h = h + he;
           }
         }
+        if (M.tet_count)
+          for (int a = M.adj_tet_offsets[v]; a < M.adj_tet_offsets[v + 1]; a += 2) {
+            const int t = M.adj_tets[a], o = M.adj_tets[a + 1];
+            const double* tm = M.tet_materials + 3 * t;
+            if (!(tm[0] > 0.0 || tm[1] > 0.0)) continue;
+            const int* ti = M.tet_indices + 4 * t;
+            V3<R> xs[4], xps[4];
+            for (int j = 0; j < 4; ++j) xs[j] = pos[ti[j]], xps[j] = q_prev[ti[j]];
+            R Dinv[9];
+            for (int j = 0; j < 9; ++j) Dinv[j] = R(M.tet_poses[9 * t + j]);
+            V3<R> ft;
+            M3<R> ht;
+            tet_force<R>(o, xs, xps, Dinv, R(tm[0]), R(tm[1]), R(tm[2]), dt, ft, ht);
+            f = f + ft;
+            h = h + ht;
+          }
         h = h + hess[v];
         f = f + forces[v];
         R d = det(h);
@@ -1126,6 +1247,13 @@ struct OracleModel {
   double soft_ke, soft_kd, soft_mu;
   const double *shape_ke, *shape_kd, *shape_mu;
   double friction_epsilon, beta;
+  int spring_count;
+  const int* spring_indices;
+  const double *spring_rest_length, *spring_stiffness, *spring_damping;
+  int tet_count;
+  const int* tet_indices;
+  const double *tet_poses, *tet_materials;
+  const int *adj_tet_offsets, *adj_tets;
 };
 
 struct OracleContacts {
@@ -1290,6 +1418,62 @@ int oracle_edge_closest(const double* x, double eps, double* out) {
 // dE/dd and d2E/dd2 of the self-contact barrier.
 int oracle_sc_norm(double dis, double radius, double k, double* out) {
   sc_norm(dis, radius, k, out[0], out[1]);
+  return 0;
+}
+
+// Tetrahedron term for the vertex of `order`: x, xp 12 doubles, Dinv 9 (row-major); out = force 3 + Hessian 9.
+int oracle_tet(int precision, int order, const double* x, const double* xp, const double* Dinv, double mu, double lmbd,
+               double damping, double dt, double* out) {
+  auto run = [&](auto tag) {
+    using R = decltype(tag);
+    V3<R> X[4], XP[4], f;
+    M3<R> h;
+    R D[9];
+    for (int k = 0; k < 4; ++k) X[k] = ld<R>(x, k), XP[k] = ld<R>(xp, k);
+    for (int k = 0; k < 9; ++k) D[k] = R(Dinv[k]);
+    tet_force<R>(order, X, XP, D, R(mu), R(lmbd), R(damping), R(dt), f, h);
+    out[0] = f.x, out[1] = f.y, out[2] = f.z;
+    for (int i = 0; i < 9; ++i) out[3 + i] = h.m[i / 3][i % 3];
+  };
+  if (precision == 64)
+    run(double());
+  else
+    run(float());
+  return 0;
+}
+
+// Spring: x, xa 6 doubles; out = f0 3, f1 3, Hessian 9.
+int oracle_spring(int precision, const double* x, const double* xa, double rest, double ke, double kd, double dt,
+                  double* out) {
+  auto run = [&](auto tag) {
+    using R = decltype(tag);
+    V3<R> f0, f1;
+    M3<R> H;
+    spring_both<R>(ld<R>(x, 0), ld<R>(x, 1), ld<R>(xa, 0), ld<R>(xa, 1), R(rest), R(ke), R(kd), R(dt), f0, f1, H);
+    out[0] = f0.x, out[1] = f0.y, out[2] = f0.z, out[3] = f1.x, out[4] = f1.y, out[5] = f1.z;
+    for (int i = 0; i < 9; ++i) out[6 + i] = H.m[i / 3][i % 3];
+  };
+  if (precision == 64)
+    run(double());
+  else
+    run(float());
+  return 0;
+}
+
+// Vertex -> (tet, order) adjacency in the reference's fill order (particle_vbd_kernels.py:774-825).
+int oracle_build_tet_adjacency(int n, int T4, const int* tets, int* offsets /*n+1*/, int* adj /*8 T4*/) {
+  std::vector<int> cnt(n, 0), fill(n, 0);
+  for (int t = 0; t < T4; ++t)
+    for (int j = 0; j < 4; ++j) cnt[tets[4 * t + j]]++;
+  offsets[0] = 0;
+  for (int i = 0; i < n; ++i) offsets[i + 1] = offsets[i] + 2 * cnt[i];
+  for (int t = 0; t < T4; ++t)
+    for (int j = 0; j < 4; ++j) {
+      const int v = tets[4 * t + j];
+      const int o = offsets[v] + 2 * fill[v]++;
+      adj[o] = t;
+      adj[o + 1] = j;
+    }
   return 0;
 }
 

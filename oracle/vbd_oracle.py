@@ -33,6 +33,9 @@ class OracleModel(C.Structure):
         ("gravity", _dp), ("soft_ke", C.c_double), ("soft_kd", C.c_double), ("soft_mu", C.c_double),
         ("shape_ke", _dp), ("shape_kd", _dp), ("shape_mu", _dp),
         ("friction_epsilon", C.c_double), ("beta", C.c_double),
+        ("spring_count", C.c_int), ("spring_indices", _ip), ("spring_rest_length", _dp), ("spring_stiffness", _dp),
+        ("spring_damping", _dp), ("tet_count", C.c_int), ("tet_indices", _ip), ("tet_poses", _dp),
+        ("tet_materials", _dp), ("adj_tet_offsets", _ip), ("adj_tets", _ip),
     ]  # fmt: skip
 
 
@@ -120,6 +123,9 @@ def lib():
         _lib.oracle_tri_closest.argtypes = [_dp, _dp]
         _lib.oracle_edge_closest.argtypes = [_dp, C.c_double, _dp]
         _lib.oracle_sc_norm.argtypes = [C.c_double, C.c_double, C.c_double, _dp]
+        _lib.oracle_tet.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp] + [C.c_double] * 4 + [_dp]
+        _lib.oracle_spring.argtypes = [C.c_int, _dp, _dp] + [C.c_double] * 4 + [_dp]
+        _lib.oracle_build_tet_adjacency.argtypes = [C.c_int, C.c_int, _ip, _ip, _ip]
     return _lib
 
 
@@ -135,6 +141,32 @@ def _i(a):
 
 def max_threads() -> int:
     return int(lib().oracle_max_threads())
+
+
+def build_tet_adjacency(n, tet_indices):
+    """Vertex→(tet, order) CSR in the reference's fill order; offsets count 2 ints per entry."""
+    tet, tp = _i(np.asarray(tet_indices).reshape(-1, 4))
+    to, top = _i(np.zeros(n + 1))
+    ta, tap = _i(np.zeros(max(8 * len(tet), 1)))
+    lib().oracle_build_tet_adjacency(n, len(tet), tp, top, tap)
+    return to, ta[: to[-1]].copy()
+
+
+def tet_element(precision, order, x, xp, Dinv, mu, lmbd, damping, dt):
+    x_, xp_p = _d(np.asarray(x).reshape(-1))
+    p_, pp = _d(np.asarray(xp).reshape(-1))
+    D_, dp = _d(np.asarray(Dinv).reshape(-1))
+    out, op = _d(np.zeros(12))
+    lib().oracle_tet(precision, int(order), xp_p, pp, dp, mu, lmbd, damping, dt, op)
+    return out[:3].copy(), out[3:].reshape(3, 3).copy()
+
+
+def spring_element(precision, x, xa, rest, ke, kd, dt):
+    x_, xp_ = _d(np.asarray(x).reshape(-1))
+    a_, ap = _d(np.asarray(xa).reshape(-1))
+    out, op = _d(np.zeros(15))
+    lib().oracle_spring(precision, xp_, ap, rest, ke, kd, dt, op)
+    return out[:3].copy(), out[3:6].copy(), out[6:].reshape(3, 3).copy()
 
 
 def build_adjacency(n, tri_indices, edge_indices):
@@ -188,6 +220,24 @@ class Model:
             soft_mu=soft[2], shape_ke=skp, shape_kd=skdp, shape_mu=smup,
             friction_epsilon=float(m.get("friction_epsilon", 1e-2)), beta=float(m.get("beta", 0.0)),
         )  # fmt: skip
+        ns = len(np.asarray(m.get("spring_rest_length", ())))
+        if ns:
+            self.s.spring_count = ns
+            self.s.spring_indices = i("spring_indices", (-1,))
+            self.s.spring_rest_length = d("spring_rest_length")
+            self.s.spring_stiffness = d("spring_stiffness")
+            self.s.spring_damping = d("spring_damping")
+        nt = len(np.asarray(m.get("tet_indices", np.zeros((0, 4)))).reshape(-1, 4))
+        if nt:
+            if "adj_tet_offsets" not in m:
+                m = dict(m)
+                m["adj_tet_offsets"], m["adj_tets"] = build_tet_adjacency(self.n, m["tet_indices"])
+            self.s.tet_count = nt
+            self.s.tet_indices = i("tet_indices", (-1,))
+            self.s.tet_poses = d("tet_poses", (-1,))
+            self.s.tet_materials = d("tet_materials", (-1,))
+            self.s.adj_tet_offsets = i("adj_tet_offsets")
+            self.s.adj_tets = i("adj_tets")
 
 
 def make_contacts(count, particle, shape, body_pos, body_vel, normal):

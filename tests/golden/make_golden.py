@@ -182,6 +182,23 @@ def load_reference(ref: str) -> dict:
         },
         ns,
     )
+    # volumetric (tetrahedra) and spring elements (particle_vbd_kernels.py:150-242, 335-546, 774-825, 2258-2397)
+    ns["vec9"], ns["mat99"], ns["mat93"], ns["mat43"] = wp._vec_ctor(9), wp._mat_ctor(9, 9), wp._mat_ctor(9, 3), wp._mat_ctor(4, 3)
+    _lift(
+        os.path.join(vbd, "particle_vbd_kernels.py"),
+        {
+            "get_vertex_num_adjacent_tets",
+            "get_vertex_adjacent_tet_id_order",
+            "_count_num_adjacent_tets",
+            "_fill_adjacent_tets",
+            "assemble_tet_vertex_force_and_hessian",
+            "evaluate_volumetric_neo_hookean_force_and_hessian",
+            "compute_cofactor",
+            "evaluate_spring_force_and_hessian_both_vertices",
+            "accumulate_spring_force_and_hessian",
+        },
+        ns,
+    )
     # self-contact (particle_vbd_kernels.py:1193-2255, 2475-2874) and its geometry helpers
     ns["mat32"] = wp.mat32
     _lift(os.path.join(ref, "newton/_src/math/__init__.py"), {"orthonormal_basis"}, ns)
@@ -236,7 +253,8 @@ def load_reference(ref: str) -> dict:
         os.path.join(ref, "newton/_src/sim/builder.py"),
         set(),
         ns,
-        classes={"ModelBuilder": {"add_triangles", "add_edges", "add_cloth_grid", "add_cloth_mesh"}},
+        classes={"ModelBuilder": {"add_triangles", "add_edges", "add_cloth_grid", "add_cloth_mesh", "add_particle",
+                                  "add_spring", "add_triangle", "add_tetrahedron", "add_edge", "add_soft_grid"}},
     )
     return ns
 
@@ -289,8 +307,48 @@ class FakeBuilder:
         }
 
 
-def greedy_coloring(n, tri_indices, edge_indices, edge_props):
-    """Greedy coloring of the particle graph of ``construct_particle_graph`` (graph_coloring.py:199-236)."""
+class SoftBuilder(FakeBuilder):
+    """FakeBuilder plus the particle, spring and tetrahedron fields that ``add_soft_grid`` and friends
+    append to; particle positions are kept as shim vectors, as the reference's builder math expects."""
+
+    def __init__(self, ns):
+        super().__init__(ns)
+        self.particle_world, self.current_world = [], -1
+        self.spring_indices, self.spring_rest_length, self.spring_stiffness = [], [], []
+        self.spring_damping, self.spring_control = [], []
+        self.tet_indices, self.tet_poses, self.tet_activations, self.tet_materials = [], [], [], []
+        for name in ("add_particle", "add_spring", "add_triangle", "add_tetrahedron", "add_edge", "add_soft_grid"):
+            setattr(self, name, types.MethodType(ns[name], self))
+
+    @property
+    def particle_count(self):
+        return len(self.particle_q)
+
+    def arrays(self) -> dict:
+        q = [np.asarray(x, dtype=np.float64) for x in self.particle_q]
+        qd = [np.asarray(x, dtype=np.float64) for x in self.particle_qd]
+        saved = self.particle_q, self.particle_qd
+        self.particle_q, self.particle_qd = q, qd
+        try:
+            out = super().arrays()
+        finally:
+            self.particle_q, self.particle_qd = saved
+        out.update(
+            spring_indices=np.array(self.spring_indices, dtype=np.int32).reshape(-1, 2),
+            spring_rest_length=np.array(self.spring_rest_length, dtype=np.float64),
+            spring_stiffness=np.array(self.spring_stiffness, dtype=np.float64),
+            spring_damping=np.array(self.spring_damping, dtype=np.float64),
+            tet_indices=np.array(self.tet_indices, dtype=np.int32).reshape(-1, 4),
+            tet_poses=np.array(self.tet_poses, dtype=np.float64).reshape(-1, 3, 3),
+            tet_materials=np.array(self.tet_materials, dtype=np.float64).reshape(-1, 3),
+        )  # fmt: skip
+        return out
+
+
+def greedy_coloring(n, tri_indices, edge_indices, edge_props, tet_indices=(), spring_indices=()):
+    """Greedy coloring of the particle graph of ``construct_particle_graph`` (graph_coloring.py:199-236):
+    triangle edges, active hinges' vertex pairs, tetrahedra's vertex pairs, plus the springs' endpoints
+    (the solve needs them in different colors)."""
     adj = [set() for _ in range(n)]
 
     def link(a, b):
@@ -307,6 +365,12 @@ def greedy_coloring(n, tri_indices, edge_indices, edge_props):
             for i in range(4):
                 for j in range(i + 1, 4):
                     link(e[i], e[j])
+    for t in tet_indices:
+        for i in range(4):
+            for j in range(i + 1, 4):
+                link(t[i], t[j])
+    for sp in spring_indices:
+        link(sp[0], sp[1])
     colors = -np.ones(n, dtype=np.int32)
     for v in sorted(range(n), key=lambda v: -len(adj[v])):
         used = {colors[u] for u in adj[v]}
@@ -364,6 +428,16 @@ def build_adjacency(ns, tri_indices, edge_indices, n):
     return f_off, np.array(f_adj.items), e_off, np.array(e_adj.items)
 
 
+def build_tet_adjacency(ns, tet_indices, n):
+    tets = wp.array2d(np.asarray(tet_indices).reshape(-1, 4), int)
+    cnt = wp.scalar_array(np.zeros(n, dtype=np.int64), int)
+    ns["_count_num_adjacent_tets"](tets, cnt)
+    off = np.concatenate([[0], np.cumsum(np.array(cnt.items) * 2)]).astype(np.int64)
+    adj = wp.scalar_array(np.zeros(int(off[-1]), dtype=np.int64), int)
+    ns["_fill_adjacent_tets"](tets, wp.scalar_array(off, int), wp.scalar_array(np.zeros(n), int), adj)
+    return off, np.array(adj.items)
+
+
 class RefScene:
     """Model arrays as shim arrays, plus the solver scratch of ``SolverVBD._init_particle_system``."""
 
@@ -376,12 +450,27 @@ class RefScene:
         self.colors = colors
         self.gravity = wp.vec_array(np.asarray(gravity).reshape(1, 3))
         f_off, f_adj, e_off, e_adj = build_adjacency(ns, m["tri_indices"], m["edge_indices"], n)
+        t_off, t_adj = build_tet_adjacency(ns, m.get("tet_indices", np.zeros((0, 4), np.int32)), n)
         self.adj = types.SimpleNamespace(
             v_adj_faces=wp.scalar_array(f_adj, int),
             v_adj_faces_offsets=wp.scalar_array(f_off, int),
             v_adj_edges=wp.scalar_array(e_adj, int),
             v_adj_edges_offsets=wp.scalar_array(e_off, int),
+            v_adj_tets=wp.scalar_array(t_adj, int),
+            v_adj_tets_offsets=wp.scalar_array(t_off, int),
         )
+        self.tet_adjacency_np = (t_off, t_adj)
+        nt = len(m.get("tet_indices", ()))
+        self.tet_indices = wp.array2d(m["tet_indices"], int) if nt else wp.Array([])
+        self.tet_poses = wp.mat33_array(m["tet_poses"]) if nt else wp.Array([])
+        self.tet_materials = wp.array2d(m["tet_materials"]) if nt else wp.Array([])
+        ns_ = len(m.get("spring_rest_length", ()))
+        self.spring_count = ns_
+        if ns_:
+            self.spring_indices = wp.scalar_array(np.asarray(m["spring_indices"]).reshape(-1), int)
+            self.spring_rest_length = wp.scalar_array(m["spring_rest_length"])
+            self.spring_stiffness = wp.scalar_array(m["spring_stiffness"])
+            self.spring_damping = wp.scalar_array(m["spring_damping"])
         self.adjacency_np = (f_off, f_adj, e_off, e_adj)
         self.mass = wp.scalar_array(m["particle_mass"])
         self.inv_mass = wp.scalar_array(m["particle_inv_mass"])
@@ -560,6 +649,12 @@ def ref_step(sc: RefScene, q_in, qd_in, f_ext, contacts, dt, iterations, frictio
                 sc.shape_mu, sc.shape_body, sc.empty, None, sc.empty, sc.empty, c_shape, c_body_pos, c_body_vel,
                 c_normal, forces, hessians,
             )  # fmt: skip
+            if sc.spring_count:  # solver_vbd.py:2224-2243
+                wp.launch(
+                    ns["accumulate_spring_force_and_hessian"], sc.spring_count, dt, color, q_prev, state_in_q,
+                    sc.particle_colors, sc.spring_count, sc.spring_indices, sc.spring_rest_length, sc.spring_stiffness,
+                    sc.spring_damping, forces, hessians,
+                )  # fmt: skip
             if selfc is not None:
                 wp.launch(
                     ns["accumulate_self_contact_force_and_hessian"], selfc.launch_size, dt, color, q_prev, state_in_q,
@@ -570,8 +665,8 @@ def ref_step(sc: RefScene, q_in, qd_in, f_ext, contacts, dt, iterations, frictio
             wp.launch(
                 ns["solve_elasticity"], len(sc.groups[color]), dt, group, q_prev, state_in_q, sc.mass, inertia,
                 sc.flags, sc.tri_indices, sc.tri_poses, sc.tri_materials, sc.tri_areas, sc.edge_indices,
-                sc.edge_rest_angle, sc.edge_rest_length, sc.edge_bending_properties, sc.empty, sc.empty,
-                sc.empty, sc.adj, forces, hessians, disp,
+                sc.edge_rest_angle, sc.edge_rest_length, sc.edge_bending_properties, sc.tet_indices, sc.tet_poses,
+                sc.tet_materials, sc.adj, forces, hessians, disp,
             )  # fmt: skip
             truncate()
         state_out_q = wp.vec_array(wp.to_numpy(state_in_q))
@@ -611,7 +706,8 @@ def scene_grid(ns, *, dim, cell, pos, rot, vel, mass, mu, lam, tri_kd, edge_ke, 
 def run_scene(ns, name, b: FakeBuilder, *, gravity, soft, shapes, contact_fn, dt, iterations, substeps, seed, beta=0.0,
               friction_epsilon=1e-2, f_ext_scale=0.0, self_contact=None, q_start=None, qd_start=None):  # fmt: skip
     m = b.arrays()
-    colors, groups = greedy_coloring(len(m["particle_q"]), m["tri_indices"], m["edge_indices"], m["edge_bending_properties"])
+    colors, groups = greedy_coloring(len(m["particle_q"]), m["tri_indices"], m["edge_indices"], m["edge_bending_properties"],
+                                     m.get("tet_indices", ()), m.get("spring_indices", ()))  # fmt: skip
     sc = RefScene(ns, m, groups, colors, gravity, soft, shapes)
     selfc = None if self_contact is None else SelfContactRef(ns, sc, **self_contact)
     n = sc.n
@@ -619,6 +715,8 @@ def run_scene(ns, name, b: FakeBuilder, *, gravity, soft, shapes, contact_fn, dt
     q = m["particle_q"].copy() if q_start is None else np.asarray(q_start, dtype=np.float64).copy()
     qd = m["particle_qd"].copy() if qd_start is None else np.asarray(qd_start, dtype=np.float64).copy()
     out = {f"model_{k}": v for k, v in m.items()}
+    if len(m.get("tet_indices", ())):
+        out["adj_tet_offsets"], out["adj_tets"] = (a.astype(np.int32) for a in sc.tet_adjacency_np)
     if selfc is not None:
         out.update({f"sc_{k}": np.float64(v) for k, v in self_contact.items()})
         for key, (flat, offs) in (("vt_filter", selfc.vt_filter), ("ee_filter", selfc.ee_filter)):
@@ -771,6 +869,38 @@ def selfcontact_cases(ns, seed=11):
             "closest": np.array(cp), "norm": np.array(norm)}  # fmt: skip
 
 
+def soft_cases(ns, seed=13):
+    """Per-element goldens of the volumetric Neo-Hookean tetrahedron and of the spring."""
+    rng = np.random.default_rng(seed)
+    tet, spr = [], []
+    for i in range(64):
+        rest = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]]) * rng.uniform(0.02, 0.2)
+        rest += rng.normal(scale=0.01, size=(4, 3))
+        Dm = (rest[1:] - rest[0]).T
+        if np.linalg.det(Dm) <= 0.0:
+            rest[[1, 2]] = rest[[2, 1]]
+            Dm = (rest[1:] - rest[0]).T
+        X = rest @ (np.eye(3) + rng.normal(scale=0.2, size=(3, 3))).T + rng.normal(size=3)
+        Xp = X + rng.normal(scale=1e-3, size=(4, 3))
+        mu, lam = rng.uniform(1e2, 1e5), rng.uniform(0.0, 1e5)
+        damping = 0.0 if i % 2 == 0 else rng.uniform(1e-4, 1e-2)
+        dt, order = 1.0 / 600.0, i % 4
+        f, H = ns["evaluate_volumetric_neo_hookean_force_and_hessian"](
+            0, order, wp.vec_array(Xp), wp.vec_array(X), wp.array2d([[0, 1, 2, 3]], int), wp.mat33(np.linalg.inv(Dm)),
+            mu, lam, damping, dt)  # fmt: skip
+        tet.append(np.concatenate([X.ravel(), Xp.ravel(), np.linalg.inv(Dm).ravel(), [mu, lam, damping, dt, order], f.a,
+                                   H.a.ravel()]))  # fmt: skip
+    for i in range(32):
+        X = rng.normal(scale=0.1, size=(2, 3))
+        Xa = X + rng.normal(scale=1e-3, size=(2, 3))
+        rest, ke, kd, dt = rng.uniform(0.05, 0.3), rng.uniform(1.0, 1e4), [0.0, 1e-2][i % 2], 1.0 / 600.0
+        v0, v1, f0, f1, H = ns["evaluate_spring_force_and_hessian_both_vertices"](
+            0, dt, wp.vec_array(X), wp.vec_array(Xa), wp.scalar_array([0, 1], int), wp.scalar_array([rest]),
+            wp.scalar_array([ke]), wp.scalar_array([kd]))  # fmt: skip
+        spr.append(np.concatenate([X.ravel(), Xa.ravel(), [rest, ke, kd, dt], f0.a, f1.a, H.a.ravel()]))
+    return {"tet": np.array(tet), "spring": np.array(spr)}
+
+
 def rot_z(deg):
     return wp.quat_from_axis_angle(wp.vec3(0.0, 0.0, 1.0), math.radians(deg))
 
@@ -834,6 +964,30 @@ def main():
 
     np.savez_compressed(os.path.join(args.out, "selfcontact_elements.npz"), **selfcontact_cases(ns))
     print("selfcontact_elements.npz written")
+
+    np.savez_compressed(os.path.join(args.out, "soft_elements.npz"), **soft_cases(ns))
+    print("soft_elements.npz written")
+
+    # Volumetric: a 3 x 2 x 2-cell tetrahedral block (add_soft_grid, 5 tetrahedra per cell, damped), 4 mm
+    # above the ground and moving down and sideways, hung from a fixed anchor particle by three springs and
+    # braced by one diagonal spring.
+    b = SoftBuilder(ns)
+    b.add_soft_grid(
+        pos=wp.vec3(0.0, 0.0, 0.004), rot=wp.quat_identity(), vel=wp.vec3(0.2, 0.0, -0.8), dim_x=3, dim_y=2,
+        dim_z=2, cell_x=0.05, cell_y=0.05, cell_z=0.05, density=500.0, k_mu=2.0e4, k_lambda=3.0e4, k_damp=1.0e-3,
+        particle_radius=5e-3,
+    )  # fmt: skip
+    nv = len(b.particle_q)
+    anchor = b.add_particle(wp.vec3(0.075, 0.05, 0.4), wp.vec3(0.0, 0.0, 0.0), 0.0, 5e-3)
+    for corner in (nv - 1, nv - 4, nv - 12):
+        b.add_spring(anchor, corner, 2.0e2, 1.0e-2, 0.0)
+    b.add_spring(0, nv - 1, 5.0e2, 0.0, 0.0)
+    out = run_scene(
+        ns, "soft_block", b, gravity=(0.0, 0.0, -9.81), soft=(1.0e4, 1.0, 0.5), shapes=[(1.0e4, 1.0, 0.6)],
+        contact_fn=lambda q, r, f: plane_contacts(q, r, f, margin=0.01), dt=1.0 / 600.0, iterations=5, substeps=3,
+        seed=6,
+    )  # fmt: skip
+    np.savez_compressed(os.path.join(args.out, "step_soft_block.npz"), **out)
 
     # Self-contact: a sheet pinned at its corners and a second sheet, turned by 17 degrees about z,
     # falling onto it from 15 mm. Vertex noise of 2 mm keeps edge pairs away from the parallel case.

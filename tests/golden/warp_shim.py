@@ -111,6 +111,9 @@ class Mat:
     def __getitem__(self, ij):
         return float(self.a[ij])
 
+    def __setitem__(self, ij, x):
+        self.a[ij] = x
+
     def __array__(self, dtype=None, copy=None):
         return self.a if dtype is None else self.a.astype(dtype)
 
@@ -176,6 +179,10 @@ def spatial_top(v):
 
 def spatial_bottom(v):
     return Vec(v.a[3:])
+
+
+def matrix_from_cols(*cols):
+    return Mat(np.stack([c.a for c in cols], axis=1))
 
 
 def dot(a, b):
@@ -293,6 +300,10 @@ def quat_to_matrix(q):
 
 def transform_identity():
     return (np.zeros(3), np.array([0.0, 0.0, 0.0, 1.0]))
+
+
+def quat_rotate(q, v):
+    return Vec(_quat_rotate(np.asarray(q, dtype=DTYPE), np.asarray(v.a if isinstance(v, Vec) else v, dtype=DTYPE)))
 
 
 def transform_point(X, p):
