@@ -89,6 +89,21 @@ typedef struct VbdModelDesc {
   const float* shape_material_mu_dev; /* [S] */
   const int32_t* shape_body_dev;      /* [S], -1 = static */
   const float* body_com_dev;          /* [B,3] or NULL */
+  /* springs (Model.spring_*; spring_count 0 = none). Forces on both ends, as
+     evaluate_spring_force_and_hessian_both_vertices (particle_vbd_kernels.py:2299-2343). The reference's
+     coloring leaves springs out: a spring whose ends share a color is summed before that color's solve from
+     the positions before it (accumulate_spring_force_and_hessian, :2347-2397), as the reference does. */
+  int32_t spring_count;
+  const int32_t* spring_indices_dev;   /* [2*spring_count]: end 0, end 1 */
+  const float* spring_rest_length_dev; /* [spring_count] */
+  const float* spring_stiffness_dev;   /* [spring_count] */
+  const float* spring_damping_dev;     /* [spring_count] */
+  /* tetrahedra (Model.tet_*; tet_count 0 = none): volumetric stable Neo-Hookean
+     (evaluate_volumetric_neo_hookean_force_and_hessian, particle_vbd_kernels.py:335-473) */
+  int32_t tet_count;
+  const int32_t* tet_indices_dev;   /* [N,4] */
+  const float* tet_poses_dev;       /* [N,3,3] rest D^-1, row-major */
+  const float* tet_materials_dev;   /* [N,3]: mu, lambda, damping */
 } VbdModelDesc;
 
 typedef struct VbdSolverParams {
@@ -133,7 +148,9 @@ typedef struct VbdSolver* VbdHandle;
 /* Replaces SolverVBD.__init__ (solver_vbd.py:196-541): builds the vertex->element adjacency
    (particle_vbd_kernels.py:639-738 fill order, solver_vbd.py:1177-1337), packs the model for the
    kernels and allocates all solver scratch. Returns VBD_ERR_EMPTY_COLORING like the reference's
-   ValueError (solver_vbd.py:533-537). */
+   ValueError (solver_vbd.py:533-537). Models with springs or tetrahedra run on the CSR layout (AUTO picks
+   it; ELL, ELL16 and RING return VBD_ERR_UNSUPPORTED); like triangles and hinges, springs and tetrahedra
+   must not span instances (worlds). */
 int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHandle* out);
 
 /* Re-reads the model arrays given to vbd_create (materials, rest state, masses, flags) after the
@@ -161,7 +178,8 @@ int vbd_step_f64(VbdHandle h, double* q_in_dev, double* q_out_dev, const double*
 /* The forward substep of vbd_step (per-color sweep, no particle-shape contacts) that also records
    what its adjoint needs: y [V,3] the inertial targets and checkpoints [(iterations+1),V,3] the
    positions at the start of every iteration and at the end. Arrays are float32, or float64 for a
-   VBD_PRECISION_FP64 solver. q_out/qd_out receive the step's result (q_in is not modified). */
+   VBD_PRECISION_FP64 solver. q_out/qd_out receive the step's result (q_in is not modified).
+   VBD_ERR_UNSUPPORTED for models with springs or tetrahedra (the adjoint covers cloth only). */
 int vbd_record_step(VbdHandle h, const void* q_in_dev, const void* qd_in_dev, const void* particle_f_dev, double dt,
                     void* y_dev, void* checkpoints_dev, void* q_out_dev, void* qd_out_dev, void* stream);
 
@@ -218,7 +236,8 @@ typedef struct VbdRefAdjacency {
    stream capture. All calls share the array: calls that overlap on the GPU race and must be serialised.
    Limits: at most VBD_NOALLOC_MAX_PARTICLES particles (else VBD_ERR_TOO_LARGE, nothing launched), at
    most VBD_NOALLOC_MAX_CONTACT_SLOTS contacts per particle, static shapes with a fixed penalty
-   (avbd beta = 0, the reference default). Inputs are trusted like the reference kernels trust theirs. */
+   (avbd beta = 0, the reference default), no springs or tetrahedra (else VBD_ERR_UNSUPPORTED). Inputs are
+   trusted like the reference kernels trust theirs. */
 int vbd_step_noalloc(const VbdModelDesc* model, const VbdRefAdjacency* adjacency, int32_t iterations,
                      float friction_epsilon, float* q_in_dev, float* q_out_dev, const float* qd_in_dev,
                      float* qd_out_dev, const float* particle_f_dev, const VbdContactsDesc* contacts, float dt,
@@ -306,6 +325,13 @@ int vbd_color_particles(int32_t particle_count, int32_t tri_count, const int32_t
                         const float* tri_materials_host, int32_t edge_count, const int32_t* edge_indices_host,
                         const float* edge_bending_properties_host, int32_t include_bending, float target_ratio,
                         int32_t* colors_out);
+
+/* The same greedy coloring and balancing on any particle graph, given as pair_count (a, b) index pairs
+   (duplicates and a == b ignored): the graph of ModelBuilder.color for models with tetrahedra, whose six
+   vertex pairs per active tet (mu * lambda != 0) join the triangle and hinge pairs
+   (construct_tetmesh_graph_edges, graph_coloring.py:53-96). Returns the number of colors or an error. */
+int vbd_color_graph(int32_t particle_count, int32_t pair_count, const int32_t* pairs_host, float target_ratio,
+                    int32_t* colors_out);
 
 /* Vertex -> (element, order) adjacency in the reference layout (ParticleForceElementAdjacencyInfo,
    particle_vbd_kernels.py:66-151, fill order :639-738): offsets count two ints per entry. */

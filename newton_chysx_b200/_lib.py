@@ -51,6 +51,9 @@ class VbdModelDesc(C.Structure):
         ("soft_contact_ke", C.c_float), ("soft_contact_kd", C.c_float), ("soft_contact_mu", C.c_float),
         ("shape_material_ke_dev", _vp), ("shape_material_kd_dev", _vp), ("shape_material_mu_dev", _vp),
         ("shape_body_dev", _vp), ("body_com_dev", _vp),
+        ("spring_count", C.c_int32), ("spring_indices_dev", _vp), ("spring_rest_length_dev", _vp),
+        ("spring_stiffness_dev", _vp), ("spring_damping_dev", _vp),
+        ("tet_count", C.c_int32), ("tet_indices_dev", _vp), ("tet_poses_dev", _vp), ("tet_materials_dev", _vp),
     ]  # fmt: skip
 
 
@@ -113,6 +116,7 @@ SIGNATURES = {
         [C.c_int32, C.c_int32, _ip, _fp, C.c_int32, _ip, _fp, C.c_int32, C.c_float, _ip],
         C.c_int,
     ),
+    "vbd_color_graph": ([C.c_int32, C.c_int32, _ip, C.c_float, _ip], C.c_int),
     "vbd_build_adjacency": ([C.c_int32, C.c_int32, _ip, C.c_int32, _ip, _ip, _ip, _ip, _ip], C.c_int),
     "vbd_step_noalloc": (
         [C.POINTER(VbdModelDesc), C.POINTER(VbdRefAdjacency), C.c_int32, C.c_float, _vp, _vp, _vp, _vp, _vp,

@@ -10,8 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
-SOURCES = ["vbd_b200.cu", "vbd_noalloc.cu"]
-HEADERS = ["vbd_math.cuh", "vbd_elements.cuh", "vbd_kernels.cuh", "vbd_ell.cuh", "vbd_dual.cuh", "vbd_adjoint.cuh"]
+SOURCES = ["vbd_b200.cu", "vbd_soft.cu", "vbd_noalloc.cu"]
 OUT = os.path.join(HERE, "libvbd_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -27,21 +26,35 @@ def stale() -> bool:
     if not os.path.exists(OUT):
         return True
     t = os.path.getmtime(OUT)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "vbd_b200.h"),
-                                                                 __file__]  # fmt: skip
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".h"))]
+    deps += [os.path.join(ROOT, "include", "vbd_b200.h"), __file__]
     return any(os.path.getmtime(d) > t for d in deps)
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compiles each source to an object in parallel, then links the shared library."""
     if not force and not stale():
         return OUT
     tmp = OUT + ".tmp"
-    cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-cudart", "static",
-           "-Wno-deprecated-declarations", "-I", os.path.join(ROOT, "include"), "-o", tmp,
-           *[os.path.join(CSRC, s) for s in SOURCES]]  # fmt: skip
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    common = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Wno-deprecated-declarations",
+              "-I", os.path.join(ROOT, "include")]  # fmt: skip
+    objs, procs = [], []
+    for src in SOURCES:
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
+        cmd = [*common, "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        objs.append(obj)
+        procs.append((cmd, subprocess.Popen(cmd)))
+    failed = [cmd for cmd, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
+    link = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs]
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        print(" ".join(link))
+    subprocess.run(link, check=True)
     os.replace(tmp, OUT)
     return OUT
 

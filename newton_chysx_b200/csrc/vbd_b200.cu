@@ -17,6 +17,7 @@
 #include "vbd_collide.cuh"
 #include "vbd_ell.cuh"
 #include "vbd_ring.cuh"
+#include "vbd_soft.h"
 
 using namespace vbd;
 
@@ -57,6 +58,26 @@ __global__ void k_pack_edges(int E, const int* __restrict__ idx, const float* __
   if (e >= E) return;
   o_idx[e] = make_int4(idx[4 * e], idx[4 * e + 1], idx[4 * e + 2], idx[4 * e + 3]);
   o_prop[e] = make_float4(ra[e], rl[e], bp[2 * e], bp[2 * e + 1]);
+}
+
+__global__ void k_pack_springs(int N, const int* __restrict__ idx, const float* __restrict__ rest,
+                               const float* __restrict__ ke, const float* __restrict__ kd, int2* o_idx, float4* o_prop) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  o_idx[i] = make_int2(idx[2 * i], idx[2 * i + 1]);
+  o_prop[i] = make_float4(rest[i], ke[i], kd[i], 0.f);
+}
+
+__global__ void k_pack_tets(int N, const int* __restrict__ idx, const float* __restrict__ pose,
+                            const float* __restrict__ mat, int4* o_idx, float4* o_pose) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= N) return;
+  o_idx[t] = make_int4(idx[4 * t], idx[4 * t + 1], idx[4 * t + 2], idx[4 * t + 3]);
+  const float* d = pose + 9 * size_t(t);
+  const float* m = mat + 3 * size_t(t);
+  o_pose[3 * t] = make_float4(d[0], d[1], d[2], m[0]);
+  o_pose[3 * t + 1] = make_float4(d[3], d[4], d[5], m[1]);
+  o_pose[3 * t + 2] = make_float4(d[6], d[7], d[8], m[2]);
 }
 
 // ------------------------------------------------------------------------------ soft contacts
@@ -138,6 +159,17 @@ struct VbdSolver {
   int4* edge_idx = nullptr;
   float4* edge_prop = nullptr;
   int *face_off = nullptr, *face_adj = nullptr, *edge_off = nullptr, *edge_adj = nullptr;
+  // springs and tetrahedra
+  int NS = 0, NT = 0;
+  bool soft = false;
+  int n_same_springs = 0;
+  int2* spr_idx = nullptr;
+  float4* spr_prop = nullptr;
+  int *spr_off = nullptr, *spr_adj = nullptr, *sspr_off = nullptr, *sspr_adj = nullptr;
+  void* spr_acc = nullptr;
+  int4* tet_idx = nullptr;
+  float4* tet_pose = nullptr;
+  int *tet_off = nullptr, *tet_adj = nullptr;
   // colors
   std::vector<int> color_offsets;
   // persistent plan
@@ -195,7 +227,8 @@ struct VbdSolver {
                   slot_cnt, slots, c_k, c_ke, c_kd, c_mu, err, residual, range_nf, range_ne, range_fbase,
                   range_ebase, face_nb, face_dm, face_mat, face_kd, hinge_idx, hinge_prop, hinge_kd, adj_work,
                   ell16_faceA, ell16_faceB, ell16_hinge, sc_pos_cd, sc_disp, sc_ts, ring_nslot, ring_base,
-                  ring_vbase, ring_A, ring_B, ring_H, ring_hdr};
+                  ring_vbase, ring_A, ring_B, ring_H, ring_hdr, spr_idx, spr_prop, spr_off, spr_adj, sspr_off,
+                  sspr_adj, spr_acc, tet_idx, tet_pose, tet_off, tet_adj};
     for (void* p : ps)
       if (p) cudaFree(p);
     sc_release(sc);
@@ -606,7 +639,55 @@ int pack_model(VbdSolver* h, cudaStream_t st) {
                                                       h->edge_idx, h->edge_prop);
     CK(cudaGetLastError());
   }
+  if (h->NS > 0) {
+    k_pack_springs<<<(h->NS + 255) / 256, 256, 0, st>>>(h->NS, m.spring_indices_dev, m.spring_rest_length_dev,
+                                                         m.spring_stiffness_dev, m.spring_damping_dev, h->spr_idx,
+                                                         h->spr_prop);
+    CK(cudaGetLastError());
+  }
+  if (h->NT > 0) {
+    k_pack_tets<<<(h->NT + 255) / 256, 256, 0, st>>>(h->NT, m.tet_indices_dev, m.tet_poses_dev, m.tet_materials_dev,
+                                                      h->tet_idx, h->tet_pose);
+    CK(cudaGetLastError());
+  }
   return VBD_OK;
+}
+
+// Vertex -> tetrahedron entries (tet << 2) | order, by tet id (the reference's fill order,
+// solver_vbd.py:1261-1297 with _fill_adjacent_tets), and vertex -> spring entries (spring << 1) | end by
+// spring id, split into springs whose other end has another color (solved with the vertex's elements) and
+// springs whose ends share a color (summed before the color's solve).
+void build_soft_adjacency(int V, int NT, const int* tets, int NS, const int* springs, const std::vector<int>& color_of,
+                          std::vector<int>& toff, std::vector<int>& tadj, std::vector<int>& soff,
+                          std::vector<int>& sadj, std::vector<int>& ssoff, std::vector<int>& ssadj) {
+  toff.assign(V + 1, 0);
+  for (int t = 0; t < NT; ++t)
+    for (int j = 0; j < 4; ++j) toff[tets[4 * t + j] + 1]++;
+  for (int i = 0; i < V; ++i) toff[i + 1] += toff[i];
+  tadj.assign(std::max(toff[V], 1), 0);
+  std::vector<int> fill(toff.begin(), toff.end() - 1);
+  for (int t = 0; t < NT; ++t)
+    for (int j = 0; j < 4; ++j) tadj[fill[tets[4 * t + j]]++] = (t << 2) | j;
+  soff.assign(V + 1, 0);
+  ssoff.assign(V + 1, 0);
+  for (int k = 0; k < NS; ++k) {
+    const int a = springs[2 * k], b = springs[2 * k + 1];
+    std::vector<int>& o = color_of[a] == color_of[b] ? ssoff : soff;
+    o[a + 1]++;
+    o[b + 1]++;
+  }
+  for (int i = 0; i < V; ++i) soff[i + 1] += soff[i], ssoff[i + 1] += ssoff[i];
+  sadj.assign(std::max(soff[V], 1), 0);
+  ssadj.assign(std::max(ssoff[V], 1), 0);
+  std::vector<int> f1(soff.begin(), soff.end() - 1), f2(ssoff.begin(), ssoff.end() - 1);
+  for (int k = 0; k < NS; ++k) {
+    const int a = springs[2 * k], b = springs[2 * k + 1];
+    const bool same = color_of[a] == color_of[b];
+    std::vector<int>& adj = same ? ssadj : sadj;
+    std::vector<int>& fl = same ? f2 : f1;
+    adj[fl[a]++] = (k << 1);
+    adj[fl[b]++] = (k << 1) | 1;
+  }
 }
 
 // Adjacency in the solver's packed form: one int per entry, (element << 2) | order, in the
@@ -701,6 +782,20 @@ StepCtx<R> make_ctx(VbdSolver* h) {
   c.V = h->V;
   c.S = h->S;
   c.dual_in_solve = 1;
+  if (h->soft) {
+    c.spr_idx = h->spr_idx;
+    c.spr_prop = h->spr_prop;
+    c.spr_off = h->spr_off;
+    c.spr_adj = h->spr_adj;
+    c.sspr_off = h->sspr_off;
+    c.sspr_adj = h->sspr_adj;
+    c.n_same_springs = h->n_same_springs;
+    c.spr_acc = (R*)h->spr_acc;
+    c.tet_idx = h->tet_idx;
+    c.tet_pose = h->tet_pose;
+    c.tet_off = h->tet_off;
+    c.tet_adj = h->tet_adj;
+  }
   return c;
 }
 
@@ -1052,6 +1147,15 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
       } else {
         launch_persistent_ell<R, MODE, false>(0, c, p, e, h->grid_persistent, h->block, 0, st);
       }
+    } else if (h->soft) {
+      if constexpr (std::is_same<R, float>::value) {
+        if (h->smem_bytes > 0)
+          launch_persistent_soft<R, MODE, true>(h->L, c, p, h->grid_persistent, h->block, h->smem_bytes, st);
+        else
+          launch_persistent_soft<R, MODE, false>(h->L, c, p, h->grid_persistent, h->block, 0, st);
+      } else {
+        launch_persistent_soft<R, MODE, false>(h->L, c, p, h->grid_persistent, h->block, 0, st);
+      }
     } else if constexpr (std::is_same<R, float>::value) {
       if (h->smem_bytes > 0)
         launch_persistent<R, MODE, true>(h->L, c, p, h->grid_persistent, h->block, h->smem_bytes, st);
@@ -1086,7 +1190,10 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
       }
       for (size_t col = 0; col + 1 < h->color_offsets.size(); ++col) {
         const int a = h->color_offsets[col], b = h->color_offsets[col + 1];
-        launch_color_sc_any<R, MODE>(h->L, c, cp + a, b - a, it, h->block, st);
+        if (h->soft)
+          launch_color_soft<R, MODE>(true, h->L, c, cp + a, b - a, it, h->block, st);
+        else
+          launch_color_sc_any<R, MODE>(h->L, c, cp + a, b - a, it, h->block, st);
         sc_truncate<R>(h, st);
       }
     }
@@ -1101,6 +1208,8 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
         const int a = h->color_offsets[col], b = h->color_offsets[col + 1];
         if (h->layout == VBD_LAYOUT_ELL) {
           if (b > a) k_color_ell<R, MODE><<<(b - a + h->block - 1) / h->block, h->block, 0, st>>>(c, e, cp + a, int(col), b - a, it);
+        } else if (h->soft) {
+          launch_color_soft<R, MODE>(false, h->L, c, cp + a, b - a, it, h->block, st);
         } else {
           launch_color_any<R, MODE>(h->L, c, cp + a, b - a, it, h->block, st);
         }
@@ -1161,6 +1270,12 @@ const void* persistent_kernel(VbdSolver* h) {
     if (h->precision == VBD_PRECISION_MIXED)
       return sm ? persistent_ell_fn<float, MODE_MIXED, true>(h->occ) : persistent_ell_fn<float, MODE_MIXED, false>(h->occ);
     return sm ? persistent_ell_fn<float, MODE_FP32, true>(h->occ) : persistent_ell_fn<float, MODE_FP32, false>(h->occ);
+  }
+  if (h->soft) {
+    if (h->precision == VBD_PRECISION_FP64) return persistent_soft_fn<double, MODE_FP64, false>(h->L);
+    if (h->precision == VBD_PRECISION_MIXED)
+      return sm ? persistent_soft_fn<float, MODE_MIXED, true>(h->L) : persistent_soft_fn<float, MODE_MIXED, false>(h->L);
+    return sm ? persistent_soft_fn<float, MODE_FP32, true>(h->L) : persistent_soft_fn<float, MODE_FP32, false>(h->L);
   }
   if (h->precision == VBD_PRECISION_FP64) return persistent_fn<double, MODE_FP64, false>(h->L);
   if (h->precision == VBD_PRECISION_MIXED)
@@ -1255,6 +1370,68 @@ int adjoint_impl(VbdSolver* h, const R* q_in, const R* y, const R* ck, R dt, con
   return VBD_OK;
 }
 
+// Greedy coloring of a graph given as (min, max) pairs (deduplicated here), then the balancing pass.
+int color_pairs(int V, std::vector<uint64_t>& pairs, float target_ratio, int32_t* colors) {
+  std::sort(pairs.begin(), pairs.end());
+  pairs.erase(std::unique(pairs.begin(), pairs.end()), pairs.end());
+  std::vector<int> off(V + 1, 0);
+  for (uint64_t p : pairs) {
+    off[int(p >> 32) + 1]++;
+    off[int(p & 0xffffffffu) + 1]++;
+  }
+  for (int i = 0; i < V; ++i) off[i + 1] += off[i];
+  std::vector<int> nb(off[V]), fill(off.begin(), off.end() - 1);
+  for (uint64_t p : pairs) {
+    const int a = int(p >> 32), b = int(p & 0xffffffffu);
+    nb[fill[a]++] = b;
+    nb[fill[b]++] = a;
+  }
+  // degree-ordered greedy (largest degree first, ties by index)
+  std::vector<int> order(V);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return off[a + 1] - off[a] > off[b + 1] - off[b]; });
+  std::fill(colors, colors + V, -1);
+  std::vector<int> mark;
+  int ncol = 0;
+  for (int v : order) {
+    for (int k = off[v]; k < off[v + 1]; ++k) {
+      const int c = colors[nb[k]];
+      if (c >= 0) {
+        if (c >= int(mark.size())) mark.resize(c + 1, -1);
+        mark[c] = v;
+      }
+    }
+    int c = 0;
+    while (c < int(mark.size()) && mark[c] == v) ++c;
+    colors[v] = c;
+    ncol = std::max(ncol, c + 1);
+  }
+  // balancing: move vertices from the largest color to the smallest admissible one
+  if (ncol > 1 && target_ratio > 1.f) {
+    std::vector<int> size(ncol, 0);
+    for (int v = 0; v < V; ++v) size[colors[v]]++;
+    for (int round = 0; round < 4 * ncol; ++round) {
+      const int cmax = int(std::max_element(size.begin(), size.end()) - size.begin());
+      const int cmin = int(std::min_element(size.begin(), size.end()) - size.begin());
+      if (size[cmin] > 0 && float(size[cmax]) / float(size[cmin]) <= target_ratio) break;
+      bool moved = false;
+      for (int v = 0; v < V && size[cmax] - size[cmin] > 1; ++v) {
+        if (colors[v] != cmax) continue;
+        bool ok = true;
+        for (int k = off[v]; k < off[v + 1] && ok; ++k) ok = colors[nb[k]] != cmin;
+        if (ok) {
+          colors[v] = cmin;
+          size[cmax]--;
+          size[cmin]++;
+          moved = true;
+        }
+      }
+      if (!moved) break;
+    }
+  }
+  return ncol;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1289,7 +1466,19 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
   if (m.shape_count > 0 &&
       (!m.shape_material_ke_dev || !m.shape_material_kd_dev || !m.shape_material_mu_dev || !m.shape_body_dev))
     return VBD_ERR_INVALID_ARGUMENT;
-  if (m.tri_count >= (1 << 29) || m.edge_count >= (1 << 29)) return VBD_ERR_UNSUPPORTED;
+  if (m.spring_count < 0 || m.tet_count < 0) return VBD_ERR_INVALID_ARGUMENT;
+  if (m.spring_count > 0 && (!m.spring_indices_dev || !m.spring_rest_length_dev || !m.spring_stiffness_dev ||
+                             !m.spring_damping_dev))
+    return VBD_ERR_INVALID_ARGUMENT;
+  if (m.tet_count > 0 && (!m.tet_indices_dev || !m.tet_poses_dev || !m.tet_materials_dev))
+    return VBD_ERR_INVALID_ARGUMENT;
+  if (m.tri_count >= (1 << 29) || m.edge_count >= (1 << 29) || m.tet_count >= (1 << 29) ||
+      m.spring_count >= (1 << 30))
+    return VBD_ERR_UNSUPPORTED;
+  const bool soft = m.spring_count > 0 || m.tet_count > 0;
+  if (soft && (params->layout == VBD_LAYOUT_ELL || params->layout == VBD_LAYOUT_ELL16 ||
+               params->layout == VBD_LAYOUT_RING))
+    return VBD_ERR_UNSUPPORTED;
 
   VbdSolver* h = new (std::nothrow) VbdSolver();
   if (!h) return VBD_ERR_OUT_OF_MEMORY;
@@ -1299,6 +1488,9 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
   h->T = m.tri_count;
   h->E = m.edge_count;
   h->S = m.shape_count;
+  h->NS = m.spring_count;
+  h->NT = m.tet_count;
+  h->soft = soft;
   h->precision = params->precision;
   h->K = params->contact_slots > 0 ? params->contact_slots : std::max(1, std::min(8, m.shape_count));
   h->color_offsets.assign(m.color_offsets_host, m.color_offsets_host + m.color_count + 1);
@@ -1322,6 +1514,15 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
     if (edges[i] >= h->V || (edges[i] < 0 && (i % 4) >= 2) || edges[i] < -1) return fail(VBD_ERR_INVALID_ARGUMENT);
   for (int p : colp)
     if (p < 0 || p >= h->V) return fail(VBD_ERR_INVALID_ARGUMENT);
+  std::vector<int> springs(2 * size_t(h->NS)), tets(4 * size_t(h->NT));
+  if (h->NS && cudaMemcpy(springs.data(), m.spring_indices_dev, springs.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(VBD_ERR_CUDA);
+  if (h->NT && cudaMemcpy(tets.data(), m.tet_indices_dev, tets.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(VBD_ERR_CUDA);
+  for (int i : springs)
+    if (i < 0 || i >= h->V) return fail(VBD_ERR_INVALID_ARGUMENT);
+  for (int i : tets)
+    if (i < 0 || i >= h->V) return fail(VBD_ERR_INVALID_ARGUMENT);
 
   std::vector<int> foff, fadj, eoff, eadj;
   build_packed_adjacency(h->V, h->T, tri.data(), h->E, edges.data(), foff, fadj, eoff, eadj);
@@ -1337,6 +1538,22 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
   if ((rc = dalloc(&h->tri_idx, h->T)) || (rc = dalloc(&h->tri_pose, h->T)) || (rc = dalloc(&h->tri_mat, h->T)) ||
       (rc = dalloc(&h->edge_idx, h->E)) || (rc = dalloc(&h->edge_prop, h->E)))
     return fail(rc);
+  if (soft) {
+    std::vector<int> color_of(h->V, -1);
+    for (size_t col = 0; col + 1 < h->color_offsets.size(); ++col)
+      for (int k = h->color_offsets[col]; k < h->color_offsets[col + 1]; ++k) color_of[colp[k]] = int(col);
+    std::vector<int> toff, tadj, soff, sadj, ssoff, ssadj;
+    build_soft_adjacency(h->V, h->NT, tets.data(), h->NS, springs.data(), color_of, toff, tadj, soff, sadj, ssoff,
+                         ssadj);
+    h->n_same_springs = ssoff[h->V];
+    const size_t racc = h->precision == VBD_PRECISION_FP64 ? sizeof(double) : sizeof(float);
+    if ((rc = upload(&h->tet_off, toff)) || (rc = upload(&h->tet_adj, tadj)) || (rc = upload(&h->spr_off, soff)) ||
+        (rc = upload(&h->spr_adj, sadj)) || (rc = upload(&h->sspr_off, ssoff)) || (rc = upload(&h->sspr_adj, ssadj)) ||
+        (rc = dalloc(&h->spr_idx, std::max(h->NS, 1))) || (rc = dalloc(&h->spr_prop, std::max(h->NS, 1))) ||
+        (rc = dalloc(&h->tet_idx, std::max(h->NT, 1))) || (rc = dalloc(&h->tet_pose, 3 * size_t(std::max(h->NT, 1)))))
+      return fail(rc);
+    if (h->n_same_springs && (rc = dalloc((char**)&h->spr_acc, racc * 9 * size_t(h->V)))) return fail(rc);
+  }
   if ((rc = pack_model(h, 0))) return fail(rc);
 
   // instances (worlds)
@@ -1360,6 +1577,11 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
     for (int j = 0; j < 4; ++j)
       if (edges[4 * e + j] >= 0 && world_of[edges[4 * e + j]] != world_of[edges[4 * e + 2]])
         return fail(VBD_ERR_INVALID_ARGUMENT);
+  for (int k = 0; k < h->NS; ++k)
+    if (world_of[springs[2 * k]] != world_of[springs[2 * k + 1]]) return fail(VBD_ERR_INVALID_ARGUMENT);
+  for (int t = 0; t < h->NT; ++t)
+    for (int j = 1; j < 4; ++j)
+      if (world_of[tets[4 * t + j]] != world_of[tets[4 * t]]) return fail(VBD_ERR_INVALID_ARGUMENT);
   // per instance, per global color (in sweep order), the instance's particles of that color
   std::vector<std::vector<std::vector<int>>> per(h->W);
   for (size_t col = 0; col + 1 < h->color_offsets.size(); ++col) {
@@ -1432,7 +1654,7 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
   const bool ell16_ok = h->schedule == VBD_SCHEDULE_PERSISTENT && h->max_inst_v < 65536 && !any_hinge_damping;
   if ((params->layout == VBD_LAYOUT_ELL16 || params->layout == VBD_LAYOUT_RING) && !ell16_ok)
     return fail(VBD_ERR_UNSUPPORTED);
-  if (params->layout == VBD_LAYOUT_CSR || h->L != 1)
+  if (params->layout == VBD_LAYOUT_CSR || h->L != 1 || h->soft)
     h->layout = VBD_LAYOUT_CSR;
   else if (params->layout == VBD_LAYOUT_RING)
     h->layout = VBD_LAYOUT_RING;
@@ -1514,6 +1736,7 @@ int vbd_step_f64(VbdHandle h, double* q_in, double* q_out, const double* qd_in, 
 int vbd_record_step(VbdHandle h, const void* q_in, const void* qd_in, const void* particle_f, double dt, void* y,
                     void* checkpoints, void* q_out, void* qd_out, void* stream) {
   if (!h || !q_in || !qd_in || !y || !checkpoints || !q_out || !qd_out || !(dt > 0.0)) return VBD_ERR_INVALID_ARGUMENT;
+  if (h->soft) return VBD_ERR_UNSUPPORTED;
   cudaStream_t st = (cudaStream_t)stream;
   if (h->precision == VBD_PRECISION_FP64)
     return record_impl<double>(h, (const double*)q_in, (const double*)qd_in, (const double*)particle_f, dt,
@@ -1526,6 +1749,7 @@ int vbd_adjoint_step(VbdHandle h, const void* q_in, const void* y, const void* c
                      const void* adj_q_out, const void* adj_qd_out, void* adj_q_in, void* adj_qd_in, void* adj_tri_mu,
                      void* adj_tri_lambda, void* stream) {
   if (!h || !q_in || !y || !checkpoints || !adj_q_in || !(dt > 0.0)) return VBD_ERR_INVALID_ARGUMENT;
+  if (h->soft) return VBD_ERR_UNSUPPORTED;
   cudaStream_t st = (cudaStream_t)stream;
   if (h->precision == VBD_PRECISION_FP64)
     return adjoint_impl<double>(h, (const double*)q_in, (const double*)y, (const double*)checkpoints, dt,
@@ -1573,9 +1797,9 @@ int vbd_launches_per_step(VbdHandle h, int32_t* out) {
     for (int it = 0; it < I; ++it)
       if ((h->sc_interval == 0 && it == 0) || (h->sc_interval >= 1 && it % h->sc_interval == 0)) ++n_det;
     const bool duals = h->S > 0 && h->prm.avbd_linear_beta != 0.f;
-    *out = 2 + (h->S > 0 ? 1 : 0) + n_det * detect + 2 + I * (C * 3 + (duals ? 1 : 0));
+    *out = 2 + (h->S > 0 ? 1 : 0) + n_det * detect + 2 + I * (C * (h->n_same_springs ? 4 : 3) + (duals ? 1 : 0));
   } else {
-    *out = 2 + (h->S > 0 ? 1 : 0) + I * C;
+    *out = 2 + (h->S > 0 ? 1 : 0) + I * C * (h->n_same_springs ? 2 : 1);
   }
   return VBD_OK;
 }
@@ -1644,6 +1868,21 @@ int vbd_build_adjacency(int32_t V, int32_t T, const int32_t* tri, int32_t E, con
   return VBD_OK;
 }
 
+int vbd_color_graph(int32_t V, int32_t pair_count, const int32_t* pairs_host, float target_ratio, int32_t* colors) {
+  if (V < 0 || pair_count < 0 || (pair_count && !pairs_host) || !colors) return VBD_ERR_INVALID_ARGUMENT;
+  if (V == 0) return 0;
+  std::vector<uint64_t> pairs;
+  pairs.reserve(pair_count);
+  for (int k = 0; k < pair_count; ++k) {
+    int a = pairs_host[2 * k], b = pairs_host[2 * k + 1];
+    if (a < 0 || b < 0 || a >= V || b >= V) return VBD_ERR_INVALID_ARGUMENT;
+    if (a == b) continue;
+    if (a > b) std::swap(a, b);
+    pairs.push_back((uint64_t(uint32_t(a)) << 32) | uint32_t(b));
+  }
+  return color_pairs(V, pairs, target_ratio, colors);
+}
+
 int vbd_color_particles(int32_t V, int32_t T, const int32_t* tri, const float* tri_mat, int32_t E,
                         const int32_t* edges, const float* edge_props, int32_t include_bending, float target_ratio,
                         int32_t* colors) {
@@ -1672,65 +1911,9 @@ int vbd_color_particles(int32_t V, int32_t T, const int32_t* tri, const float* t
     }
   for (uint64_t p : pairs)
     if (int(p >> 32) >= V || int(p & 0xffffffffu) >= V) return VBD_ERR_INVALID_ARGUMENT;
-  std::sort(pairs.begin(), pairs.end());
-  pairs.erase(std::unique(pairs.begin(), pairs.end()), pairs.end());
-  std::vector<int> off(V + 1, 0);
-  for (uint64_t p : pairs) {
-    off[int(p >> 32) + 1]++;
-    off[int(p & 0xffffffffu) + 1]++;
-  }
-  for (int i = 0; i < V; ++i) off[i + 1] += off[i];
-  std::vector<int> nb(off[V]), fill(off.begin(), off.end() - 1);
-  for (uint64_t p : pairs) {
-    const int a = int(p >> 32), b = int(p & 0xffffffffu);
-    nb[fill[a]++] = b;
-    nb[fill[b]++] = a;
-  }
-  // degree-ordered greedy (largest degree first, ties by index)
-  std::vector<int> order(V);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return off[a + 1] - off[a] > off[b + 1] - off[b]; });
-  std::fill(colors, colors + V, -1);
-  std::vector<int> mark;
-  int ncol = 0;
-  for (int v : order) {
-    for (int k = off[v]; k < off[v + 1]; ++k) {
-      const int c = colors[nb[k]];
-      if (c >= 0) {
-        if (c >= int(mark.size())) mark.resize(c + 1, -1);
-        mark[c] = v;
-      }
-    }
-    int c = 0;
-    while (c < int(mark.size()) && mark[c] == v) ++c;
-    colors[v] = c;
-    ncol = std::max(ncol, c + 1);
-  }
-  // balancing: move vertices from the largest color to the smallest admissible one
-  if (ncol > 1 && target_ratio > 1.f) {
-    std::vector<int> size(ncol, 0);
-    for (int v = 0; v < V; ++v) size[colors[v]]++;
-    for (int round = 0; round < 4 * ncol; ++round) {
-      const int cmax = int(std::max_element(size.begin(), size.end()) - size.begin());
-      const int cmin = int(std::min_element(size.begin(), size.end()) - size.begin());
-      if (size[cmin] > 0 && float(size[cmax]) / float(size[cmin]) <= target_ratio) break;
-      bool moved = false;
-      for (int v = 0; v < V && size[cmax] - size[cmin] > 1; ++v) {
-        if (colors[v] != cmax) continue;
-        bool ok = true;
-        for (int k = off[v]; k < off[v + 1] && ok; ++k) ok = colors[nb[k]] != cmin;
-        if (ok) {
-          colors[v] = cmin;
-          size[cmax]--;
-          size[cmin]++;
-          moved = true;
-        }
-      }
-      if (!moved) break;
-    }
-  }
-  return ncol;
+  return color_pairs(V, pairs, target_ratio, colors);
 }
+
 
 int vbd_soft_contacts(int32_t n, const float* q, const float* radius, const int32_t* flags, int32_t S,
                       const int32_t* shape_type, const float* shape_pos, const float* shape_radius,

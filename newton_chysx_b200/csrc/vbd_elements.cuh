@@ -21,6 +21,9 @@
 //                unless damping needs all four.
 //  * contact   - rigid_vbd_kernels.py:727-759, 891-934 (penalty, approach damping, IPC-smoothed
 //                isotropic friction).
+//  * spring    - particle_vbd_kernels.py:2299-2343 (linear spring with damping).
+//  * tetrahedron - particle_vbd_kernels.py:335-473 (volumetric stable Neo-Hookean), contracted to the
+//                vertex's 3x3 block in closed form.
 #pragma once
 #include "vbd_math.cuh"
 
@@ -161,6 +164,87 @@ __host__ __device__ __forceinline__ void contact_add(R pen, vec3<R> n, vec3<R> r
     souter_add(H, n, -scale);
   }
   f = f + force;
+}
+
+// Linear spring between the solved vertex (end `end` of the spring: 0 or 1) and its partner,
+// particle_vbd_kernels.py:2299-2343 (evaluate_spring_force_and_hessian_both_vertices): with d = x_0 - x_1
+// and l = max(|d|, 1e-8), the elastic force on end 0 is ke (l0 - l) / l d (the negative on end 1), the
+// Hessian ke (I - l0 / l (I - d d^T / l^2)) = ke (1 - l0 / l) I + ke l0 / l^3 d d^T, and damping adds
+// (kd / dt) H (x_prev - x) to the force and (kd / dt) H to the Hessian. xa = the vertex's position at the
+// start of the step, read only when kd != 0.
+template <typename R>
+__host__ __device__ __forceinline__ void spring_add(int end, vec3<R> x, vec3<R> x_other, vec3<R> xa, R rest, R ke,
+                                                    R kd, R dt, vec3<R>& f, sym3<R>& H) {
+  const vec3<R> d = end == 0 ? x - x_other : x_other - x;
+  const R l = vmax(length(d), R(1.0e-8));
+  const R il = R(1) / l;
+  const vec3<R> base = (ke * (rest - l) * il) * d;
+  sym3<R> h = sdiag(ke * (R(1) - rest * il));
+  souter_add(h, d, ke * rest * il * il * il);
+  vec3<R> force = end == 0 ? base : -base;
+  if (kd != R(0)) {
+    const R c = kd / dt;
+    force = force + c * smul(h, xa - x);
+    h = (R(1) + c) * h;
+  }
+  f = f + force;
+  H = H + h;
+}
+
+// Volumetric stable Neo-Hookean tetrahedron, particle_vbd_kernels.py:335-473, for the vertex of order
+// `ord` (0..3). dm = rest D^-1 (row-major 3x3), mat = (mu, lambda, damping). With F = Ds D^-1 (columns
+// F_0, F_1, F_2), cof(F) the cofactor matrix (columns F_1 x F_2, F_2 x F_0, F_0 x F_1), V the rest volume
+// 1 / (6 det D^-1) and m the vertex's row of d vec(F) / dx (row ord-1 of D^-1, or minus the sum of its rows
+// for ord 0), the reference's 9x9 forms contract in closed form to
+//   f = -V (mu F m + s cof(F) m),  s = lambda_nh (det F - alpha)
+//   H =  V (mu |m|^2 I + lambda_nh g g^T),  g = cof(F) m
+// with lambda_nh = lambda + mu, alpha = 1 + mu / lambda_nh (|lambda_nh| floored at 1e-6). Damping adds
+// -damping V (mu Fdot m + lambda_nh (cof(F) : Fdot) g) to f and scales H by 1 + damping / dt.
+template <typename R>
+__host__ __device__ __forceinline__ void tet_add(int ord, const vec3<R> x[4], const vec3<R>* xp, const R dm[9], R mu,
+                                                 R lmbd, R damping, R dt, vec3<R>& f, sym3<R>& H) {
+  const R det_dm = dm[0] * (dm[4] * dm[8] - dm[5] * dm[7]) - dm[1] * (dm[3] * dm[8] - dm[5] * dm[6]) +
+                   dm[2] * (dm[3] * dm[7] - dm[4] * dm[6]);
+  const R vol = R(1) / (det_dm * R(6));
+  const vec3<R> c1 = x[1] - x[0], c2 = x[2] - x[0], c3 = x[3] - x[0];
+  const vec3<R> F0 = c1 * dm[0] + c2 * dm[3] + c3 * dm[6];
+  const vec3<R> F1 = c1 * dm[1] + c2 * dm[4] + c3 * dm[7];
+  const vec3<R> F2 = c1 * dm[2] + c2 * dm[5] + c3 * dm[8];
+  const vec3<R> C0 = cross(F1, F2), C1 = cross(F2, F0), C2 = cross(F0, F1);
+  const R J = dot(F0, C0);
+  const R lnh = lmbd + mu;
+  const R lsafe = (lnh < R(0) ? R(-1) : R(1)) * vmax(vabs(lnh), R(1.0e-6));
+  const R alpha = R(1) + mu / lsafe;
+  const R s = lnh * (J - alpha);
+  // row selection by comparisons, not by a computed index, so that dm stays in registers
+  vec3<R> m;
+  if (ord == 0)
+    m = {-(dm[0] + dm[3] + dm[6]), -(dm[1] + dm[4] + dm[7]), -(dm[2] + dm[5] + dm[8])};
+  else if (ord == 1)
+    m = {dm[0], dm[1], dm[2]};
+  else if (ord == 2)
+    m = {dm[3], dm[4], dm[5]};
+  else
+    m = {dm[6], dm[7], dm[8]};
+  const vec3<R> Fm = F0 * m.x + F1 * m.y + F2 * m.z;
+  const vec3<R> g = C0 * m.x + C1 * m.y + C2 * m.z;
+  vec3<R> force = (-vol) * (mu * Fm + s * g);
+  sym3<R> h = sdiag(vol * mu * dot(m, m));
+  souter_add(h, g, vol * lnh);
+  if (damping > R(0)) {
+    const R inv_dt = R(1) / dt;
+    const vec3<R> d0 = x[0] - xp[0];
+    const vec3<R> e1 = ((x[1] - xp[1]) - d0) * inv_dt, e2 = ((x[2] - xp[2]) - d0) * inv_dt,
+                  e3 = ((x[3] - xp[3]) - d0) * inv_dt;
+    const vec3<R> G0 = e1 * dm[0] + e2 * dm[3] + e3 * dm[6];
+    const vec3<R> G1 = e1 * dm[1] + e2 * dm[4] + e3 * dm[7];
+    const vec3<R> G2 = e1 * dm[2] + e2 * dm[5] + e3 * dm[8];
+    const R cfd = dot(C0, G0) + dot(C1, G1) + dot(C2, G2);
+    force = force + (-damping * vol) * (mu * (G0 * m.x + G1 * m.y + G2 * m.z) + (lnh * cfd) * g);
+    h = (R(1) + damping * inv_dt) * h;
+  }
+  f = f + force;
+  H = H + h;
 }
 
 }  // namespace vbd

@@ -95,6 +95,19 @@ struct StepCtx {
   const int2* vt_pairs;  // (vertex, triangle)
   const int2* ee_pairs;  // (edge, edge)
   double sc_radius, sc_ee_eps;
+  // springs and tetrahedra (solve_group<..., SOFT = true>)
+  const int2* __restrict__ spr_idx;     // endpoints
+  const float4* __restrict__ spr_prop;  // rest length, ke, kd
+  const int* __restrict__ spr_off;      // [V+1] springs whose other end has another color: (spring << 1) | end
+  const int* __restrict__ spr_adj;
+  const int* __restrict__ sspr_off;     // [V+1] springs whose ends share a color (summed before the color's solve)
+  const int* __restrict__ sspr_adj;
+  int n_same_springs;                   // entries of sspr_adj; 0 = no pre-pass
+  R* spr_acc;                           // [V, 9] pre-pass sums: f xyz, H xx yy zz xy xz yz
+  const int4* __restrict__ tet_idx;
+  const float4* __restrict__ tet_pose;  // [3 per tet]: rows of rest D^-1, w = mu, lambda, damping
+  const int* __restrict__ tet_off;      // [V+1]
+  const int* __restrict__ tet_adj;      // (tet << 2) | order
 };
 
 __device__ __forceinline__ void set_err(int* err, int bit) {
@@ -263,10 +276,60 @@ __device__ __forceinline__ void self_contact_add(const StepCtx<R>& c, const P& p
     sc_vt_add<R>(slot, x, xa, R(c.sc_radius), R(c.soft_ke), R(c.soft_kd), R(c.soft_mu), eps_u, c.dt, f, H);
 }
 
+// Spring term of one entry (spring << 1) | end of vertex v's spring list.
+template <typename R, typename P>
+__device__ __forceinline__ void spring_entry_add(const StepCtx<R>& c, const P& pos, int v, int a, vec3<R>& f,
+                                                 sym3<R>& H) {
+  const int sp = a >> 1, end = a & 1;
+  const int2 ij = __ldg(c.spr_idx + sp);
+  const float4 pr = __ldg(c.spr_prop + sp);
+  const vec3<R> xa = pr.z != 0.f ? ld3<R>(c.qprev[v]) : zero3<R>();
+  spring_add<R>(end, pos.ld(v), pos.ld(end == 0 ? ij.y : ij.x), xa, R(pr.x), R(pr.y), R(pr.z), c.dt, f, H);
+}
+
+// Tetrahedron term of one entry (tet << 2) | order.
+template <typename R, typename P>
+__device__ __forceinline__ void tet_entry_add(const StepCtx<R>& c, const P& pos, int a, vec3<R>& f, sym3<R>& H) {
+  const int t = a >> 2, ord = a & 3;
+  const float4 r0 = __ldg(c.tet_pose + 3 * t), r1 = __ldg(c.tet_pose + 3 * t + 1), r2 = __ldg(c.tet_pose + 3 * t + 2);
+  if (!(r0.w > 0.f || r1.w > 0.f)) return;  // the reference skips tets with mu <= 0 and lambda <= 0
+  const int4 ti = __ldg(c.tet_idx + t);
+  const R dm[9] = {R(r0.x), R(r0.y), R(r0.z), R(r1.x), R(r1.y), R(r1.z), R(r2.x), R(r2.y), R(r2.z)};
+  vec3<R> x[4], xp[4];
+  x[0] = pos.ld(ti.x);
+  x[1] = pos.ld(ti.y);
+  x[2] = pos.ld(ti.z);
+  x[3] = pos.ld(ti.w);
+  if (r2.w > 0.f) {
+    xp[0] = ld3<R>(c.qprev[ti.x]);
+    xp[1] = ld3<R>(c.qprev[ti.y]);
+    xp[2] = ld3<R>(c.qprev[ti.z]);
+    xp[3] = ld3<R>(c.qprev[ti.w]);
+  }
+  tet_add<R>(ord, x, xp, dm, R(r0.w), R(r1.w), R(r2.w), c.dt, f, H);
+}
+
+// Sum of the springs of vertex v whose two ends share v's color, at the positions before the color's
+// solve (accumulate_spring_force_and_hessian, particle_vbd_kernels.py:2347-2397, runs before the solve
+// of each color, so both ends see the other's position from before it); the solve adds it.
+template <typename R, typename P>
+__device__ __forceinline__ void spring_prepass_vertex(const StepCtx<R>& c, const P& pos, int v) {
+  const int b = __ldg(c.sspr_off + v), e = __ldg(c.sspr_off + v + 1);
+  if (b == e) return;
+  vec3<R> f = zero3<R>();
+  sym3<R> H = szero<R>();
+  for (int k = b; k < e; ++k) spring_entry_add<R>(c, pos, v, __ldg(c.sspr_adj + k), f, H);
+  R* o = c.spr_acc + 9 * size_t(v);
+  o[0] = f.x, o[1] = f.y, o[2] = f.z, o[3] = H.xx, o[4] = H.yy, o[5] = H.zz, o[6] = H.xy, o[7] = H.xz, o[8] = H.yz;
+}
+
 // SC: self-contact on. The vertex's self-contact entries join its faces and hinges in the lane split, and
 // the solve adds its step to the displacement since the last detection instead of moving the vertex
 // (the truncation pass that follows each color moves it, as apply_truncation_ts does).
-template <typename R, int L, int MODE, typename P, bool SC = false>
+// SOFT: the model has springs or tetrahedra; the vertex's tets and cross-color springs join the lane split
+// after its hinges (solve_elasticity, particle_vbd_kernels.py:3136-3280, adds tets after hinges and the
+// pre-accumulated springs and contacts last).
+template <typename R, int L, int MODE, typename P, bool SC = false, bool SOFT = false>
 __device__ __forceinline__ void solve_group(const StepCtx<R>& c, const P& pos, int v, bool valid, int sub,
                                             int iteration) {
   vec3<R> f = zero3<R>();
@@ -278,7 +341,14 @@ __device__ __forceinline__ void solve_group(const StepCtx<R>& c, const P& pos, i
     const int fb = __ldg(c.face_off + v), fe = __ldg(c.face_off + v + 1);
     const int eb = __ldg(c.edge_off + v), ee = __ldg(c.edge_off + v + 1);
     const int nf = fe - fb;
-    const int nfe = nf + (ee - eb);
+    int nfe = nf + (ee - eb);
+    int tb = 0, nfet = nfe, sb = 0;
+    if (SOFT) {
+      tb = __ldg(c.tet_off + v);
+      nfet = nfe + (__ldg(c.tet_off + v + 1) - tb);
+      sb = __ldg(c.spr_off + v);
+      nfe = nfet + (__ldg(c.spr_off + v + 1) - sb);  // from here on: every element entry
+    }
     int cb = 0, n = nfe;
     if (SC) {
       cb = __ldg(c.ent_off + v);
@@ -287,6 +357,10 @@ __device__ __forceinline__ void solve_group(const StepCtx<R>& c, const P& pos, i
     for (int it = sub; it < n; it += L) {
       if (SC && it >= nfe) {
         self_contact_add<R>(c, pos, __ldg(c.ent + cb + (it - nfe)), f, H);
+      } else if (SOFT && it >= nfet) {
+        spring_entry_add<R>(c, pos, v, __ldg(c.spr_adj + sb + (it - nfet)), f, H);
+      } else if (SOFT && it >= nf + (ee - eb)) {
+        tet_entry_add<R>(c, pos, __ldg(c.tet_adj + tb + (it - nf - (ee - eb))), f, H);
       } else if (it < nf) {
         const int a = __ldg(c.face_adj + fb + it);
         const int t = a >> 2, ord = a & 3;
@@ -350,6 +424,11 @@ __device__ __forceinline__ void solve_group(const StepCtx<R>& c, const P& pos, i
     H.yy += md;
     H.zz += md;
     if (c.has_contacts) contacts_add<R>(c, v, x, f, H);
+    if (SOFT && c.n_same_springs && __ldg(c.sspr_off + v + 1) > __ldg(c.sspr_off + v)) {
+      const R* a = c.spr_acc + 9 * size_t(v);
+      f = f + vec3<R>{a[0], a[1], a[2]};
+      H = H + sym3<R>{a[3], a[4], a[5], a[6], a[7], a[8]};
+    }
   }
   if (MODE == MODE_MIXED && c.residual) {
     // FP64 reduction of |f|^2 (the force residual the block solve removes): warp sum, one atomic per warp
@@ -444,13 +523,20 @@ __global__ void k_contact_prepare(StepCtx<R> c) {
     set_err(c.err, 2);
 }
 
-template <typename R, int L, int MODE, bool SC = false>
+template <typename R, int L, int MODE, bool SC = false, bool SOFT = false>
 __global__ void k_color(StepCtx<R> c, const int* __restrict__ verts, int n, int iteration) {
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   const int grp = gid / L, sub = gid % L;
   const bool valid = grp < n;
   const int v = valid ? __ldg(verts + grp) : 0;
-  solve_group<R, L, MODE, GlobalPos<R>, SC>(c, GlobalPos<R>{c.pos}, v, valid, sub, iteration);
+  solve_group<R, L, MODE, GlobalPos<R>, SC, SOFT>(c, GlobalPos<R>{c.pos}, v, valid, sub, iteration);
+}
+
+// Same-color spring sums of one color's vertices (per-color schedule), before that color's solve.
+template <typename R>
+__global__ void k_spring_prepass(StepCtx<R> c, const int* __restrict__ verts, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) spring_prepass_vertex<R>(c, GlobalPos<R>{c.pos}, __ldg(verts + i));
 }
 
 // AVBD penalty update of every contact at the start of an iteration (update_duals_body_particle_contacts,
@@ -492,7 +578,7 @@ struct PersistentPlan {
 // One launch per substep. SMEM: the instance's positions stay in shared memory (3 floats per
 // particle) from the forward step to the write-back, so every neighbour gather of the sweep is a
 // shared-memory load; otherwise they live in the solver's global float4 array.
-template <typename R, int L, int MODE, bool SMEM>
+template <typename R, int L, int MODE, bool SMEM, bool SOFT = false>
 __global__ void k_persistent(StepCtx<R> c, PersistentPlan p) {
   extern __shared__ float s_pos[];
   __shared__ int s_item;
@@ -519,11 +605,15 @@ __global__ void k_persistent(StepCtx<R> c, PersistentPlan p) {
     for (int it = 0; it < p.iterations; ++it) {
       for (int col = cb; col + 1 < ce; ++col) {
         const int a = __ldg(p.color_ranges + col), b = __ldg(p.color_ranges + col + 1);
+        if (SOFT && c.n_same_springs) {
+          for (int g = a + threadIdx.x; g < b; g += blockDim.x) spring_prepass_vertex<R>(c, pos, __ldg(p.color_verts + g));
+          __syncthreads();
+        }
         for (int base = a; base < b; base += per_round) {
           const int g = base + grp_local;
           const bool valid = g < b;
           const int v = valid ? __ldg(p.color_verts + g) : 0;
-          solve_group<R, L, MODE>(c, pos, v, valid, sub, it);
+          solve_group<R, L, MODE, Pos, false, SOFT>(c, pos, v, valid, sub, it);
         }
         __syncthreads();
       }

@@ -236,6 +236,7 @@ extern "C" int vbd_step_noalloc(const VbdModelDesc* m, const VbdRefAdjacency* ad
     return VBD_ERR_INVALID_ARGUMENT;
   if (m->particle_count <= 0 || m->color_count <= 0 || !m->color_offsets_host || !m->color_particles_dev)
     return VBD_ERR_INVALID_ARGUMENT;
+  if (m->spring_count != 0 || m->tet_count != 0) return VBD_ERR_UNSUPPORTED;
   if (m->particle_count > kMaxP) return VBD_ERR_TOO_LARGE;
   if (!adj->face_offsets_dev || !adj->edge_offsets_dev || (m->tri_count > 0 && !adj->faces_dev) ||
       (m->edge_count > 0 && !adj->edges_dev))

@@ -172,8 +172,41 @@ def _merge_chunked(groups_1, groups_2):
     return out
 
 
+def particle_graph_pairs(tri_indices, tri_materials, edge_indices, edge_props, include_bending, tet_indices,
+                         tet_materials):  # fmt: skip
+    """Vertex pairs of the coloring graph of ``construct_particle_graph`` (graph_coloring.py:200-240):
+    the three edges of every triangle with mu * lambda != 0, with ``include_bending`` the six vertex pairs
+    of every hinge with ke or kd != 0 (pairs with a -1 left out), and the six vertex pairs of every
+    tetrahedron with mu * lambda != 0. Springs are not part of the graph, as in the reference."""
+    parts = []
+    tri = np.asarray(tri_indices, dtype=np.int32).reshape(-1, 3)
+    tm = np.asarray(tri_materials, dtype=np.float32).reshape(-1, 5)
+    if len(tri):
+        tri = tri[(tm[:, 0] * tm[:, 1]) != 0]
+        parts += [tri[:, [0, 1]], tri[:, [0, 2]], tri[:, [1, 2]]]
+    ed = np.asarray(edge_indices, dtype=np.int32).reshape(-1, 4)
+    ep = np.asarray(edge_props, dtype=np.float32).reshape(-1, 2)
+    if include_bending and len(ed):
+        ed = ed[(ep[:, 0] != 0) | (ep[:, 1] != 0)]
+        for a in range(4):
+            for b in range(a + 1, 4):
+                pr = ed[:, [a, b]]
+                parts.append(pr[(pr >= 0).all(axis=1)])
+    tt = np.asarray(tet_indices, dtype=np.int32).reshape(-1, 4)
+    tmat = np.asarray(tet_materials, dtype=np.float32).reshape(-1, 3)
+    if len(tt):
+        tt = tt[(tmat[:, 0] * tmat[:, 1]) != 0]
+        for a in range(4):
+            for b in range(a + 1, 4):
+                parts.append(tt[:, [a, b]])
+    if not parts:
+        return np.zeros((0, 2), dtype=np.int32)
+    return np.ascontiguousarray(np.concatenate(parts).astype(np.int32))
+
+
 def color_particles(n, tri_indices, tri_materials, edge_indices, edge_props, include_bending=False,
-                    balance_colors=True, target_max_min_color_ratio=1.1):  # fmt: skip
+                    balance_colors=True, target_max_min_color_ratio=1.1, tet_indices=None,
+                    tet_materials=None):  # fmt: skip
     """Color groups (list of int32 arrays, particles in index order) for VBD's Gauss-Seidel sweep."""
     if n == 0:
         return []
@@ -182,16 +215,23 @@ def color_particles(n, tri_indices, tri_materials, edge_indices, edge_props, inc
     tm = np.ascontiguousarray(np.asarray(tri_materials, dtype=np.float32).reshape(-1, 5))
     ed = np.ascontiguousarray(np.asarray(edge_indices, dtype=np.int32).reshape(-1, 4))
     ep = np.ascontiguousarray(np.asarray(edge_props, dtype=np.float32).reshape(-1, 2))
-    if len(tri) == 0 and (not include_bending or len(ed) == 0):
+    has_tets = tet_indices is not None and len(np.asarray(tet_indices).reshape(-1)) > 0
+    if len(tri) == 0 and (not include_bending or len(ed) == 0) and not has_tets:
         return [np.arange(n, dtype=np.int32)]
     colors = np.zeros(n, dtype=np.int32)
     ip = C.POINTER(C.c_int32)
     fp = C.POINTER(C.c_float)
-    ncol = lib.vbd_color_particles(
-        n, len(tri), tri.ctypes.data_as(ip), tm.ctypes.data_as(fp), len(ed), ed.ctypes.data_as(ip),
-        ep.ctypes.data_as(fp), int(bool(include_bending)), float(target_max_min_color_ratio if balance_colors else 0.0),
-        colors.ctypes.data_as(ip),
-    )  # fmt: skip
+    ratio = float(target_max_min_color_ratio if balance_colors else 0.0)
+    if has_tets:
+        pairs = particle_graph_pairs(tri, tm, ed, ep, include_bending, tet_indices, tet_materials)
+        if len(pairs) == 0:
+            return [np.arange(n, dtype=np.int32)]
+        ncol = lib.vbd_color_graph(n, len(pairs), pairs.ctypes.data_as(ip), ratio, colors.ctypes.data_as(ip))
+    else:
+        ncol = lib.vbd_color_particles(
+            n, len(tri), tri.ctypes.data_as(ip), tm.ctypes.data_as(fp), len(ed), ed.ctypes.data_as(ip),
+            ep.ctypes.data_as(fp), int(bool(include_bending)), ratio, colors.ctypes.data_as(ip),
+        )  # fmt: skip
     if ncol < 0:
         _lib.check(ncol, "vbd_color_particles")
     order = np.argsort(colors, kind="stable")
@@ -201,7 +241,8 @@ def color_particles(n, tri_indices, tri_materials, edge_indices, edge_props, inc
 
 # ----------------------------------------------------------------------------- builder
 class ModelBuilder:
-    """The cloth subset of the reference ``ModelBuilder``."""
+    """The particle subset of the reference ``ModelBuilder``: particles, cloth triangles and hinges,
+    springs, tetrahedra, static shapes, worlds and coloring."""
 
     ShapeConfig = ShapeConfig
 
@@ -220,9 +261,13 @@ class ModelBuilder:
         self._q, self._qd, self._mass, self._radius, self._flags, self._world = [], [], [], [], [], []
         self._tri, self._tri_pose, self._tri_mat, self._tri_area = [], [], [], []
         self._edge, self._edge_angle, self._edge_len, self._edge_prop = [], [], [], []
+        self._spr, self._spr_rest, self._spr_ke, self._spr_kd, self._spr_ctl = [], [], [], [], []
+        self._tet, self._tet_pose, self._tet_mat = [], [], []
         self._n = 0
         self._t = 0
         self._e = 0
+        self._s = 0
+        self._tt = 0
         self.shapes = []  # dicts: type, pos, normal, radius, ke, kd, mu, body
         self._color_groups: list[_ChunkedGroup] = []
         self.world_count = 0
@@ -245,6 +290,14 @@ class ModelBuilder:
     @property
     def shape_count(self):
         return len(self.shapes)
+
+    @property
+    def spring_count(self):
+        return self._s
+
+    @property
+    def tet_count(self):
+        return self._tt
 
     @property
     def up_vector(self):
@@ -284,6 +337,23 @@ class ModelBuilder:
     @property
     def edge_bending_properties(self):
         return self._cat(self._edge_prop, (-1, 2), np.float64)
+
+    @property
+    def spring_indices(self):
+        """Flat ``[2 * spring_count]`` (end 0, end 1 per spring), the reference's layout."""
+        return self._cat(self._spr, (-1,), np.int32)
+
+    @property
+    def tet_indices(self):
+        return self._cat(self._tet, (-1, 4), np.int32)
+
+    @property
+    def tet_poses(self):
+        return self._cat(self._tet_pose, (-1, 3, 3), np.float64)
+
+    @property
+    def tet_materials(self):
+        return self._cat(self._tet_mat, (-1, 3), np.float64)
 
     def _set_particle_column(self, lst_name, values):
         arr = self._cat(getattr(self, lst_name), (-1,), np.float64 if lst_name != "_flags" else np.int32)
@@ -354,6 +424,56 @@ class ModelBuilder:
         self._tri_area.append(areas[valid])
         self._t += int(valid.sum())
         return areas
+
+    # -- springs (builder.py:7584-7633)
+    def add_springs(self, i, j, ke, kd, control=0.0):
+        """Springs between particles i[k] and j[k]; the rest length is their current distance, computed in
+        float32 as the reference does."""
+        i = np.atleast_1d(np.asarray(i, dtype=np.int64))
+        j = np.atleast_1d(np.asarray(j, dtype=np.int64))
+        n = len(i)
+        q = self.particle_q.astype(np.float32)
+        d = q[i] - q[j]
+        rest = np.sqrt((d * d).sum(axis=1, dtype=np.float32)).astype(np.float64)
+
+        def col(v):
+            return np.broadcast_to(np.asarray(v, dtype=np.float64), (n,)).copy()
+
+        self._spr.append(np.stack([i, j], axis=1).reshape(-1).astype(np.int32))
+        self._spr_rest.append(rest)
+        self._spr_ke.append(col(ke))
+        self._spr_kd.append(col(kd))
+        self._spr_ctl.append(col(control))
+        self._s += n
+
+    def add_spring(self, i, j, ke, kd, control=0.0):
+        self.add_springs([i], [j], ke, kd, control)
+
+    # -- tetrahedra (builder.py:7827-7892)
+    def add_tetrahedra(self, i, j, k, l, k_mu=1.0e3, k_lambda=1.0e3, k_damp=0.0):  # noqa: E741
+        """Volumetric Neo-Hookean tetrahedra (i, j, k, l) with the rest pose of the current positions. As in
+        the reference, tetrahedra whose rest volume is not positive are not added. Returns the volumes."""
+        idx = [np.atleast_1d(np.asarray(a, dtype=np.int64)) for a in (i, j, k, l)]
+        n = len(idx[0])
+        q = self.particle_q
+        p = q[idx[0]]
+        Dm = np.stack([q[idx[1]] - p, q[idx[2]] - p, q[idx[3]] - p], axis=2)  # columns
+        vol = np.linalg.det(Dm) / 6.0 if n else np.zeros(0)
+        valid = vol > 0.0
+        inv = np.linalg.inv(Dm[valid]) if valid.any() else np.zeros((0, 3, 3))
+
+        def col(v):
+            return np.broadcast_to(np.asarray(v, dtype=np.float64), (n,))
+
+        mats = np.stack([col(k_mu), col(k_lambda), col(k_damp)], axis=1)[valid]
+        self._tet.append(np.stack(idx, axis=1)[valid].astype(np.int32))
+        self._tet_pose.append(inv)
+        self._tet_mat.append(mats)
+        self._tt += int(valid.sum())
+        return vol
+
+    def add_tetrahedron(self, i, j, k, l, k_mu=1.0e3, k_lambda=1.0e3, k_damp=0.0):  # noqa: E741
+        return float(self.add_tetrahedra([i], [j], [k], [l], k_mu, k_lambda, k_damp)[0])
 
     # -- bending hinges (builder.py:7966-8061)
     def add_edges(self, i, j, k, l, rest=None, edge_ke=None, edge_kd=None):  # noqa: E741
@@ -448,6 +568,58 @@ class ModelBuilder:
         self._flags = [flags]
         self._mass = [m]
 
+    # -- volumetric grid (builder.py:8445-8611)
+    def add_soft_grid(self, pos, rot, vel, dim_x, dim_y, dim_z, cell_x, cell_y, cell_z, density, k_mu, k_lambda,
+                      k_damp, fix_left=False, fix_right=False, fix_top=False, fix_bottom=False, tri_ke=0.0, tri_ka=0.0,
+                      tri_kd=0.0, tri_drag=0.0, tri_lift=0.0, add_surface_mesh_edges=True, edge_ke=0.0, edge_kd=0.0,
+                      particle_radius=None, label=None):  # fmt: skip
+        """A box of dim_x x dim_y x dim_z cells, five tetrahedra per cell in the alternating pattern of the
+        reference, its boundary faces as triangles (for contact; zero stiffness by default) and, with
+        add_surface_mesh_edges, the hinges of that surface. Every particle gets the mass of one cell;
+        fix_* set the mass of a side's particles to 0."""
+        del label
+        nx, ny, nz = dim_x + 1, dim_y + 1, dim_z + 1
+        zz, yy, xx = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+        xx, yy, zz = xx.ravel(), yy.ravel(), zz.ravel()
+        local = np.stack([xx * cell_x, yy * cell_y, zz * cell_z], axis=1)
+        rot_m = quat_to_matrix(rot).astype(np.float32).astype(np.float64)
+        verts = local @ rot_m.T + np.asarray(pos, dtype=np.float64)
+        m = np.full(len(xx), cell_x * cell_y * cell_z * density, dtype=np.float64)
+        fixed = ((xx == 0) & fix_left) | ((xx == dim_x) & fix_right) | ((yy == dim_y) & fix_top) | ((yy == 0) & fix_bottom)
+        m[fixed] = 0.0
+        radius = self.default_particle_radius if particle_radius is None else particle_radius
+        start = self.add_particles(verts, vel, m, radius=radius)
+
+        def gi(x, y, z):
+            return start + nx * ny * z + nx * y + x
+
+        cz, cy, cx = np.meshgrid(np.arange(dim_z), np.arange(dim_y), np.arange(dim_x), indexing="ij")
+        cx, cy, cz = cx.ravel(), cy.ravel(), cz.ravel()
+        v = [gi(cx, cy, cz), gi(cx + 1, cy, cz), gi(cx + 1, cy, cz + 1), gi(cx, cy, cz + 1), gi(cx, cy + 1, cz),
+             gi(cx + 1, cy + 1, cz), gi(cx + 1, cy + 1, cz + 1), gi(cx, cy + 1, cz + 1)]  # fmt: skip
+        odd = ((cx & 1) ^ (cy & 1) ^ (cz & 1)).astype(bool)
+        pat_odd = [(0, 1, 4, 3), (2, 3, 6, 1), (5, 4, 1, 6), (7, 6, 3, 4), (4, 1, 6, 3)]
+        pat_even = [(1, 2, 5, 0), (3, 0, 7, 2), (4, 7, 0, 5), (6, 5, 2, 7), (5, 2, 7, 0)]
+        tets = np.empty((len(cx), 5, 4), dtype=np.int64)
+        for t in range(5):
+            for c in range(4):
+                tets[:, t, c] = np.where(odd, v[pat_odd[t][c]], v[pat_even[t][c]])
+        tets = tets.reshape(-1, 4)
+        self.add_tetrahedra(tets[:, 0], tets[:, 1], tets[:, 2], tets[:, 3], k_mu, k_lambda, k_damp)
+        # boundary faces: the faces (i,k,j), (j,k,l), (i,j,l), (i,l,k) of every tet that no other tet shares,
+        # in the order of their first appearance
+        f = np.stack([tets[:, [0, 2, 1]], tets[:, [1, 2, 3]], tets[:, [0, 1, 3]], tets[:, [0, 3, 2]]], axis=1).reshape(-1, 3)
+        if len(f):
+            key = np.sort(f, axis=1)
+            _, first, counts = np.unique(key, axis=0, return_index=True, return_counts=True)
+            keep = np.sort(first[counts == 1])
+            faces = f[keep]
+            t0 = self._t
+            self.add_triangles(faces[:, 0], faces[:, 1], faces[:, 2], tri_ke, tri_ka, tri_kd, tri_drag, tri_lift)
+            if add_surface_mesh_edges and self._t > t0:
+                h = mesh_hinges(self.tri_indices[t0:self._t])
+                self.add_edges(h[:, 0], h[:, 1], h[:, 2], h[:, 3], edge_ke=edge_ke, edge_kd=edge_kd)
+
     # -- shapes
     def add_ground_plane(self, cfg: ShapeConfig | None = None):
         cfg = cfg or self.default_shape_cfg
@@ -476,7 +648,7 @@ class ModelBuilder:
     def color(self, include_bending=False, balance_colors=True, target_max_min_color_ratio=1.1):
         self.particle_color_groups = color_particles(
             self._n, self.tri_indices, self.tri_materials, self.edge_indices, self.edge_bending_properties,
-            include_bending, balance_colors, target_max_min_color_ratio,
+            include_bending, balance_colors, target_max_min_color_ratio, self.tet_indices, self.tet_materials,
         )  # fmt: skip
 
     def set_coloring(self, groups):
@@ -511,6 +683,18 @@ class ModelBuilder:
             self._edge_len.append(builder._cat(builder._edge_len, (-1,), np.float64))
             self._edge_prop.append(builder.edge_bending_properties)
             self._e += builder._e
+        if builder._s:
+            self._spr.append(builder.spring_indices + start)
+            self._spr_rest.append(builder._cat(builder._spr_rest, (-1,), np.float64))
+            self._spr_ke.append(builder._cat(builder._spr_ke, (-1,), np.float64))
+            self._spr_kd.append(builder._cat(builder._spr_kd, (-1,), np.float64))
+            self._spr_ctl.append(builder._cat(builder._spr_ctl, (-1,), np.float64))
+            self._s += builder._s
+        if builder._tt:
+            self._tet.append(builder.tet_indices + start)
+            self._tet_pose.append(builder.tet_poses)
+            self._tet_mat.append(builder.tet_materials)
+            self._tt += builder._tt
         self.shapes.extend(dict(s) for s in builder.shapes)
         translated = [_ChunkedGroup([c + start for c in g.chunks], g.size) for g in builder._color_groups]
         self._color_groups = _merge_chunked(self._color_groups, translated)
@@ -562,6 +746,15 @@ class Model:
         m.edge_rest_angle = t(b._cat(b._edge_angle, (-1,), np.float64), f32)
         m.edge_rest_length = t(b._cat(b._edge_len, (-1,), np.float64), f32)
         m.edge_bending_properties = t(b.edge_bending_properties, f32).reshape(-1, 2)
+        m.spring_count, m.tet_count = b._s, b._tt
+        m.spring_indices = t(b.spring_indices, i32).reshape(-1)
+        m.spring_rest_length = t(b._cat(b._spr_rest, (-1,), np.float64), f32)
+        m.spring_stiffness = t(b._cat(b._spr_ke, (-1,), np.float64), f32)
+        m.spring_damping = t(b._cat(b._spr_kd, (-1,), np.float64), f32)
+        m.spring_control = t(b._cat(b._spr_ctl, (-1,), np.float64), f32)
+        m.tet_indices = t(b.tet_indices, i32).reshape(-1, 4)
+        m.tet_poses = t(b.tet_poses, f32).reshape(-1, 3, 3)
+        m.tet_materials = t(b.tet_materials, f32).reshape(-1, 3)
         m.particle_color_groups = [t(g, i32) for g in b.particle_color_groups]
         colors = np.full(b._n, -1, dtype=np.int32)
         for c, g in enumerate(b.particle_color_groups):

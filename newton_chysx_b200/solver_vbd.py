@@ -186,6 +186,18 @@ class SolverVBD:
             md.shape_material_mu_dev = _ptr(model.shape_material_mu)
             md.shape_body_dev = _ptr(model.shape_body)
         md.body_com_dev = _ptr(getattr(model, "body_com", None))
+        ns, nt = int(getattr(model, "spring_count", 0) or 0), int(getattr(model, "tet_count", 0) or 0)
+        if ns:
+            md.spring_count = ns
+            md.spring_indices_dev = _ptr(model.spring_indices)
+            md.spring_rest_length_dev = _ptr(model.spring_rest_length)
+            md.spring_stiffness_dev = _ptr(model.spring_stiffness)
+            md.spring_damping_dev = _ptr(model.spring_damping)
+        if nt:
+            md.tet_count = nt
+            md.tet_indices_dev = _ptr(model.tet_indices)
+            md.tet_poses_dev = _ptr(model.tet_poses)
+            md.tet_materials_dev = _ptr(model.tet_materials)
         self._md = md
 
         prm = _lib.VbdSolverParams()

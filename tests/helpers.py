@@ -58,6 +58,17 @@ def model_from_golden(g, device="cuda") -> sim.Model:
     m.shape_material_mu = t(shapes[:, 2], f32)
     m.shape_body = t(-np.ones(S), i32)
     m.world_particle_start = None
+    if "model_spring_indices" in g:
+        m.spring_count = len(g["model_spring_rest_length"])
+        m.spring_indices = t(np.asarray(g["model_spring_indices"]).reshape(-1), i32)
+        m.spring_rest_length = t(g["model_spring_rest_length"], f32)
+        m.spring_stiffness = t(g["model_spring_stiffness"], f32)
+        m.spring_damping = t(g["model_spring_damping"], f32)
+    if "model_tet_indices" in g:
+        m.tet_count = len(g["model_tet_indices"])
+        m.tet_indices = t(g["model_tet_indices"], i32)
+        m.tet_poses = t(g["model_tet_poses"], f32)
+        m.tet_materials = t(g["model_tet_materials"], f32)
     return m
 
 
@@ -90,7 +101,7 @@ def oracle_model_dict(model: sim.Model, friction_epsilon=1e-2, beta=0.0) -> dict
     shapes = np.zeros((max(S, 1), 3))
     if S:
         shapes = np.stack([h(model.shape_material_ke), h(model.shape_material_kd), h(model.shape_material_mu)], 1)
-    return dict(
+    d = dict(
         particle_mass=h(model.particle_mass), particle_inv_mass=h(model.particle_inv_mass),
         particle_radius=h(model.particle_radius), particle_flags=h(model.particle_flags),
         tri_indices=h(model.tri_indices), tri_poses=h(model.tri_poses), tri_materials=h(model.tri_materials),
@@ -102,6 +113,12 @@ def oracle_model_dict(model: sim.Model, friction_epsilon=1e-2, beta=0.0) -> dict
         soft=np.array([model.soft_contact_ke, model.soft_contact_kd, model.soft_contact_mu]), shapes=shapes,
         friction_epsilon=friction_epsilon, beta=beta,
     )  # fmt: skip
+    if getattr(model, "spring_count", 0):
+        d.update(spring_indices=h(model.spring_indices), spring_rest_length=h(model.spring_rest_length),
+                 spring_stiffness=h(model.spring_stiffness), spring_damping=h(model.spring_damping))  # fmt: skip
+    if getattr(model, "tet_count", 0):
+        d.update(tet_indices=h(model.tet_indices), tet_poses=h(model.tet_poses), tet_materials=h(model.tet_materials))
+    return d
 
 
 def cloth_grid_builder(n=32, side=1.0, E=1e4, nu=0.3, h=1e-3, density=0.2, bend=1e-4, radius=5e-3, hanging=True,
