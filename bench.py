@@ -625,6 +625,161 @@ def cpu_baseline_selfcontact(m, q, qd):
             "sample": "one substep of the same settled 256x256 state (self-contact detection on a box grid)"}  # fmt: skip
 
 
+def build_soft_model(dev, worlds, seed=5):
+    """Volumetric batch: `worlds` tetrahedral blocks of 8 x 4 x 4 cells (5 tets per cell, 225 particles, 640
+    tets; 2 cm cells, 500 kg/m^3, mu 2e4 Pa, lambda 3e4 Pa, damping 1e-3), each hung from a fixed anchor by
+    four springs at its top corners, falling onto a ground plane from a seeded height and velocity."""
+    import torch
+
+    import newton_chysx_b200 as nb
+
+    tpl = nb.ModelBuilder(up_axis="Z", gravity=-9.81)
+    tpl.add_soft_grid(pos=(0.0, 0.0, 0.0), rot=nb.quat_identity(), vel=(0.0, 0.0, 0.0), dim_x=8, dim_y=4, dim_z=4,
+                      cell_x=0.02, cell_y=0.02, cell_z=0.02, density=500.0, k_mu=2.0e4, k_lambda=3.0e4, k_damp=1.0e-3,
+                      particle_radius=2e-3)  # fmt: skip
+    nv = tpl.particle_count
+    anchor = tpl.add_particle((0.08, 0.04, 0.5), (0.0, 0.0, 0.0), 0.0, 2e-3)
+    for c in (nv - 1, nv - 9, nv - 1 - 9 * 4, nv - 9 - 9 * 4):
+        tpl.add_spring(anchor, c, 50.0, 1e-2, 0.0)
+    tpl.color()
+    b = nb.ModelBuilder(up_axis="Z", gravity=-9.81)
+    for _ in range(worlds):
+        b.add_world(tpl)
+    b.add_ground_plane()
+    m = b.finalize(dev)
+    rng = np.random.default_rng(seed)
+    n1 = tpl.particle_count
+    lift = np.repeat(rng.uniform(0.01, 0.05, worlds), n1)
+    vx = np.repeat(rng.normal(0.0, 0.2, worlds), n1)
+    block = np.tile(np.arange(n1) < nv, worlds)
+    with torch.no_grad():
+        m.particle_q[:, 2] += torch.as_tensor(np.where(block, lift, 0.0), dtype=torch.float32, device=dev)
+        m.particle_qd[:, 0] = torch.as_tensor(np.where(block, vx, 0.0), dtype=torch.float32, device=dev)
+        m.particle_qd[:, 2] = torch.as_tensor(np.where(block, -0.5, 0.0), dtype=torch.float32, device=dev)
+    m.soft_contact_ke, m.soft_contact_kd, m.soft_contact_mu = 1.0e4, 1.0e-2, 0.5
+    return m
+
+
+def run_soft(args):
+    """Soft bodies (tetrahedra + springs), batched: --instances blocks (default 4,096) on the persistent schedule
+    (one CTA per block), 10 iterations, dt = 1/600 s, ground contact. The step is timed from a CUDA graph of two
+    substeps. The per-instance working set (about 60 KB of tet records and adjacency) stays in L1/L2 for the
+    instance's 10 iterations, so DRAM moves each instance's data about once per substep: the kernel is bound by
+    its arithmetic and by gather latency, not by HBM; the roofline fraction says so."""
+    import torch
+
+    import newton_chysx_b200 as nb
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    W = args.instances
+    t0 = time.perf_counter()
+    m = build_soft_model(dev, W)
+    build_s = time.perf_counter() - t0
+    solver = nb.SolverVBD(m, iterations=ITERATIONS, schedule="persistent", lanes_per_vertex=args.lanes)
+    pipe = nb.CollisionPipeline(m, soft_contact_margin=0.01)
+    contacts = pipe.contacts()
+    s0, s1 = m.state(), m.state()
+    for _ in range(args.warmup):
+        pipe.collide(s0, contacts)
+        solver.step(s0, s1, None, contacts, DT)
+        s0, s1 = s1, s0
+    torch.cuda.synchronize()
+    q_w, qd_w = s0.particle_q.clone(), s0.particle_qd.clone()
+    graph = torch.cuda.CUDAGraph()
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(stream), torch.cuda.graph(graph, stream=stream):
+        pipe.collide(s0, contacts)
+        solver.step(s0, s1, None, contacts, DT)
+        pipe.collide(s1, contacts)
+        solver.step(s1, s0, None, contacts, DT)
+    torch.cuda.current_stream().wait_stream(stream)
+    s0.particle_q.copy_(q_w)
+    s0.particle_qd.copy_(qd_w)
+    K = max(2, args.steps + (args.steps % 2))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index or 0) as clk:
+        e0.record()
+        for _ in range(K // 2):
+            graph.replay()
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / K
+    V = m.particle_count
+    value = V * ITERATIONS / (ms * 1e-3)
+    # algorithmic DRAM bytes per substep: every instance's records read once (tet int4 + 3 float4 = 64 B, spring
+    # int2 + float4 = 24 B, adjacency 4 B per incidence and 2 x 4 B offsets per vertex), the particle arrays the
+    # step reads (q, qd, mass, inv mass, flags: 36 B) and writes (q twice, qd: 36 B)
+    T, S = m.tet_count, m.spring_count
+    alg = T * 64 + S * 24 + 4 * (4 * T + 2 * S) + V * (2 * 2 * 4) + V * 72
+    peak, peak_src = _peaks()
+    achieved = alg / (ms * 1e-3) / 1e9
+    out = {
+        "metric": "VBD vertex-iters/s on 1 B200, batched soft bodies (tetrahedra + springs)", "value": value,
+        "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded tetrahedral blocks on springs)",
+        "config": {"workload": f"{W} tetrahedral blocks 8x4x4 cells hung by springs over a ground plane",
+                   "vertices": V, "tets": T, "springs": S, "iterations": ITERATIONS, "dt": DT,
+                   "schedule": solver.schedule, "lanes_per_vertex": solver.lanes_per_vertex,
+                   "build_s": round(build_s, 1),
+                   "timed": "ground contact generation + step, one CUDA graph per two substeps",
+                   "l2": "per-instance working set stays on chip for its iterations; DRAM sees it once per substep"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_source": peak_src, "algorithmic_bytes_per_step": alg,
+                     "note": "algorithmic bytes per substep / substep time; compute- and latency-bound"},
+        "gpu_launches": K * (solver.launches_per_step + 1), "colors": len(m.particle_color_groups),
+        "clocks": clk.summary(), "device_errors": solver.device_errors(),
+        "finite": bool(torch.isfinite(s0.particle_q).all().item()),
+    }  # fmt: skip
+    if not args.no_e2e:
+        hq, hqd = q_w.cpu().pin_memory(), qd_w.cpu().pin_memory()
+        out_q = torch.empty_like(hq).pin_memory()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(K):
+            s0.particle_q.copy_(hq, non_blocking=True)
+            s0.particle_qd.copy_(hqd, non_blocking=True)
+            pipe.collide(s0, contacts)
+            solver.step(s0, s1, None, contacts, DT)
+            out_q.copy_(s1.particle_q, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        ms_e = e0.elapsed_time(e1) / K
+        out["e2e"] = {"value": V * ITERATIONS / (ms_e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 2 * hq.numel() * 4,
+                      "d2h_bytes_per_step": out_q.numel() * 4, "steps": K}  # fmt: skip
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_soft()
+    return out
+
+
+def cpu_baseline_soft(sample_worlds=256, seconds=10.0):
+    """The oracle (FP32, all host threads) on `sample_worlds` blocks of the same workload, substep after substep
+    until `seconds` have passed."""
+    import torch
+
+    from oracle import vbd_oracle as orc
+    from tests.helpers import oracle_model_dict
+
+    m = build_soft_model(torch.device("cpu"), sample_worlds)
+    threads = orc.max_threads()
+    om = orc.Model(oracle_model_dict(m))
+    q = m.particle_q.double().numpy()
+    qd = m.particle_qd.double().numpy()
+    cnt, p, s, bp, bv, nn = orc.soft_contacts(q, m.particle_radius.numpy(), m.particle_flags.numpy(), m.shape_type,
+                                              m.shape_pos, m.shape_radius, 0.01)  # fmt: skip
+    t = time.perf_counter()
+    n = 0
+    while n == 0 or time.perf_counter() - t < seconds:
+        _, q, qd = orc.step(om, q, qd, None, orc.make_contacts(cnt, p, s, bp, bv, nn), DT, ITERATIONS, precision=32,
+                            nthreads=threads)  # fmt: skip
+        n += 1
+    el = time.perf_counter() - t
+    return {"value": n * m.particle_count * ITERATIONS / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} substeps of {sample_worlds} blocks of the same workload (contacts of the first substep)"}  # fmt: skip
+
+
 def run_adjoint(args):
     """Differentiable config: 64 x 64 hanging cloth (a curtain: the whole top row pinned, bending ke 1e-2),
     60 frames x 10 substeps x 10 iterations; loss = mean squared distance of the final positions to a
@@ -853,7 +1008,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["batched", "plain", "precision", "selfcontact", "adjoint"], default="batched")
+    ap.add_argument("--workload", choices=["batched", "plain", "precision", "selfcontact", "adjoint", "soft"],
+                    default="batched")
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--lanes", type=int, default=0)
@@ -887,6 +1043,8 @@ def main():
         out = run_selfcontact(args)
     elif args.workload == "adjoint":
         out = run_adjoint(args)
+    elif args.workload == "soft":
+        out = run_soft(args)
     else:
         out = run_ours(args)
     if out is not None:
