@@ -7,7 +7,8 @@ changes the speed of the sweep on a B200:
 * the element layout: ``ell16`` / ``ell`` (per-incidence stencil records with 16-bit or 32-bit vertex
   ids, one lane per vertex) or ``csr`` (adjacency + element records) with 1, 2 or 4 lanes per vertex;
 * the persistent kernel's register budget (``min_blocks_per_sm``: 2, 3, 4 CTAs of 256 threads per SM,
-  or the compiler's choice) and whether an instance's positions live in shared memory;
+  or the compiler's choice), whether an instance's positions live in shared memory, and whether the ell16
+  kernel stages its stencil records through shared memory (``record_stages``);
 * the block size of the per-color schedule.
 
 Each candidate is a separate solver on the same model; results do not depend on the choice beyond
@@ -30,6 +31,9 @@ def candidates(model: Model, schedule: str):
         for layout in ("ell16", "ell"):
             for occ in (0, 2, 3, 4):
                 out.append(dict(layout=layout, lanes_per_vertex=1, positions_in_shared="off", min_blocks_per_sm=occ))
+                if layout == "ell16":
+                    out.append(dict(layout=layout, lanes_per_vertex=1, positions_in_shared="off", min_blocks_per_sm=occ,
+                                    record_stages=4))  # fmt: skip
             out.append(dict(layout=layout, lanes_per_vertex=1, positions_in_shared="on"))
         for lanes, shared in itertools.product((1, 2, 4), ("off", "on")):
             out.append(dict(layout="csr", lanes_per_vertex=lanes, positions_in_shared=shared))

@@ -18,6 +18,7 @@
 #include "vbd_ell.cuh"
 #include "vbd_ring.cuh"
 #include "vbd_soft.h"
+#include "vbd_ell16_staged.h"
 
 using namespace vbd;
 
@@ -151,6 +152,7 @@ struct VbdSolver {
   size_t smem_bytes = 0;  // > 0: persistent kernel keeps instance positions in shared memory
   int max_inst_v = 0;
   int occ = 0;  // ELL persistent kernel: compiled occupancy target (CTAs of 256 per SM), 0 = none
+  int stages = 0;  // ELL16 persistent kernel: records staged through shared memory (kEll16Stages), 0 = not
   int K = 1;
   // packed model
   int4* tri_idx = nullptr;
@@ -607,6 +609,7 @@ Ell16View ell16_view(const VbdSolver* h) {
   e.faceA = h->ell16_faceA;
   e.faceB = h->ell16_faceB;
   e.hinge = h->ell16_hinge;
+  e.ring_offset = int(h->smem_bytes);
   return e;
 }
 
@@ -1130,7 +1133,12 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
     } else if (h->layout == VBD_LAYOUT_ELL16) {
       const Ell16View e = ell16_view(h);
       if constexpr (std::is_same<R, float>::value) {
-        if (h->smem_bytes > 0)
+        const size_t ss = ell16_staged_smem(h->smem_bytes, h->block);
+        if (h->stages && h->smem_bytes > 0)
+          launch_persistent_ell16_staged<R, MODE, true>(h->occ, c, p, e, h->grid_persistent, h->block, ss, st);
+        else if (h->stages)
+          launch_persistent_ell16_staged<R, MODE, false>(h->occ, c, p, e, h->grid_persistent, h->block, ss, st);
+        else if (h->smem_bytes > 0)
           launch_persistent_ell16<R, MODE, true>(h->occ, c, p, e, h->grid_persistent, h->block, h->smem_bytes, st);
         else
           launch_persistent_ell16<R, MODE, false>(h->occ, c, p, e, h->grid_persistent, h->block, 0, st);
@@ -1259,6 +1267,13 @@ const void* persistent_kernel(VbdSolver* h) {
       return sm ? persistent_ring_fn<float, MODE_MIXED, true>(h->occ) : persistent_ring_fn<float, MODE_MIXED, false>(h->occ);
     return sm ? persistent_ring_fn<float, MODE_FP32, true>(h->occ) : persistent_ring_fn<float, MODE_FP32, false>(h->occ);
   }
+  if (h->layout == VBD_LAYOUT_ELL16 && h->stages) {
+    if (h->precision == VBD_PRECISION_MIXED)
+      return sm ? persistent_ell16_staged_fn<float, MODE_MIXED, true>(h->occ)
+                : persistent_ell16_staged_fn<float, MODE_MIXED, false>(h->occ);
+    return sm ? persistent_ell16_staged_fn<float, MODE_FP32, true>(h->occ)
+              : persistent_ell16_staged_fn<float, MODE_FP32, false>(h->occ);
+  }
   if (h->layout == VBD_LAYOUT_ELL16) {
     if (h->precision == VBD_PRECISION_FP64) return persistent_ell16_fn<double, MODE_FP64, false>(0);
     if (h->precision == VBD_PRECISION_MIXED)
@@ -1288,8 +1303,9 @@ int occupancy_grid(VbdSolver* h) {
   int dev = 0, sms = 0, per_sm = 0;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  if (h->smem_bytes > 0) CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(h->smem_bytes)));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, h->block, h->smem_bytes));
+  const size_t dyn = h->stages ? ell16_staged_smem(h->smem_bytes, h->block) : h->smem_bytes;
+  if (dyn > 0) CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, h->block, dyn));
   if (per_sm < 1) return VBD_ERR_INVALID_ARGUMENT;
   h->grid_persistent = std::min(h->W, sms * per_sm);
   return VBD_OK;
@@ -1693,6 +1709,17 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
       h->ranges_host = h->color_offsets;
     }
     if ((rc = h->layout == VBD_LAYOUT_RING ? build_ring(h) : build_ell(h))) return fail(rc);
+  }
+  if (params->record_stages != 0) {
+    if (params->record_stages != kEll16Stages || h->layout != VBD_LAYOUT_ELL16 || h->schedule != VBD_SCHEDULE_PERSISTENT ||
+        h->precision == VBD_PRECISION_FP64)
+      return fail(VBD_ERR_INVALID_ARGUMENT);
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+      return fail(VBD_ERR_CUDA);
+    if (ell16_staged_smem(h->smem_bytes, h->block) > size_t(optin)) return fail(VBD_ERR_UNSUPPORTED);
+    h->stages = params->record_stages;
   }
   if (h->schedule == VBD_SCHEDULE_PERSISTENT && (rc = occupancy_grid(h))) return fail(rc);
   if (cudaDeviceSynchronize() != cudaSuccess) return fail(VBD_ERR_CUDA);

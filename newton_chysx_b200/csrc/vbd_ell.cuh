@@ -21,6 +21,8 @@
 //   float  kd                read only when the model has non-zero bending damping
 // Empty slots (vertices with fewer elements than the range's maximum) carry zero stiffness.
 #pragma once
+#include <cstdint>
+
 #include "vbd_kernels.cuh"
 
 namespace vbd {
@@ -253,11 +255,64 @@ struct Ell16View {
   const uint4* faceA;
   const uint4* faceB;
   const uint4* hinge;
+  int ring_offset;  // STAGES > 0: byte offset of the record ring in dynamic shared memory
 };
 
-template <typename R, int MODE, typename P>
-__device__ __forceinline__ void solve_ell16(const StepCtx<R>& c, const P& pos, const Ell16View& e, int r, int n, int j,
-                                            int v, int vs, int iteration) {
+// Staged record fetch (STAGES > 0): each thread streams its own records through a ring of STAGES 16-byte
+// shared-memory cells per array with cp.async (.cg: cached in L2 only), STAGES - 1 slots ahead of use. The
+// loads then wait in the copy path instead of holding registers, and a thread reads only the cells it filled
+// itself, so the ring needs no barrier: cp.async.wait_group orders the copies of one thread.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Membrane term of one 32-byte face record (A, B halves) for the solved vertex v at x.
+template <typename R, typename P>
+__device__ __forceinline__ void ell16_face(const StepCtx<R>& c, const P& pos, int v, int vs, vec3<R> x, uint4 A, uint4 B,
+                                           vec3<R>& f, sym3<R>& H) {
+  const float muA = __uint_as_float(A.y), lmA = __uint_as_float(A.z);
+  if (!(muA > 0.f || lmA > 0.f)) return;
+  const R pose[4] = {R(__uint_as_float(A.w)), R(__uint_as_float(B.x)), R(__uint_as_float(B.y)),
+                     R(__uint_as_float(B.z))};
+  const float kd = __uint_as_float(B.w);
+  const int ia = vs + int(A.x & 0xffffu), ib = vs + int(A.x >> 16);
+  vec3<R> xp[3];
+  if (kd > 0.f) {
+    xp[0] = ld3<R>(c.qprev[v]);
+    xp[1] = ld3<R>(c.qprev[ia]);
+    xp[2] = ld3<R>(c.qprev[ib]);
+  }
+  membrane_add<R>(0, x, pos.ld(ia), pos.ld(ib), pose, R(muA), R(lmA), R(kd), R(1), c.dt, xp, f, H);
+}
+
+// Bending term of one 16-byte hinge record for the solved vertex at x.
+template <typename R, typename P>
+__device__ __forceinline__ void ell16_hinge(const P& pos, int vs, vec3<R> x, uint4 hh, R dt, vec3<R>& f, sym3<R>& H) {
+  const float k = __uint_as_float(hh.w);
+  if (!(k > 0.f)) return;
+  const int role = int((hh.y >> 16) & 3u);
+  const vec3<R> o0 = pos.ld(vs + int(hh.x & 0xffffu));
+  const vec3<R> o1 = pos.ld(vs + int(hh.x >> 16));
+  const vec3<R> o2 = pos.ld(vs + int(hh.y & 0xffffu));
+  // put the solved vertex back at its place among the four
+  vec3<R> xs[4];
+  xs[0] = role == 0 ? x : o0;
+  xs[1] = role == 0 ? o0 : (role == 1 ? x : o1);
+  xs[2] = role <= 1 ? o1 : (role == 2 ? x : o2);
+  xs[3] = role == 3 ? x : o2;
+  bending_add<R>(role, xs, R(__uint_as_float(hh.z)), R(1), R(k), R(0), dt, nullptr, f, H);
+}
+
+// ring: STAGES > 0 only, this block's record ring (2 x STAGES x blockDim cells).
+template <typename R, int MODE, int STAGES, typename P>
+__device__ __forceinline__ void solve_ell16(const StepCtx<R>& c, const P& pos, const Ell16View& e, uint4* ring, int r,
+                                            int n, int j, int v, int vs, int iteration) {
   const pos4_t<R> in4 = c.inertia[v];
   const R m = R(in4.w);
   if (m == R(0)) return;
@@ -265,72 +320,94 @@ __device__ __forceinline__ void solve_ell16(const StepCtx<R>& c, const P& pos, c
   vec3<R> f = zero3<R>();
   sym3<R> H = szero<R>();
   const int nf = __ldg(e.range_nf + r), ne = __ldg(e.range_ne + r);
-  {
-    const long long b0 = __ldg(e.range_fbase + r) + j;
-    const uint4* pa = e.faceA + b0;
-    const uint4* pb = e.faceB + b0;
-    uint4 A_n = make_uint4(0u, 0u, 0u, 0u), B_n = make_uint4(0u, 0u, 0u, 0u);
-    if (nf > 0) {
-      A_n = __ldcs(pa);
-      B_n = __ldcs(pb);
-    }
-    for (int q = 1; q < kRecordPrefetch && q < nf; ++q) {
-      prefetch_l2(pa + (long long)q * n);
-      prefetch_l2(pb + (long long)q * n);
-    }
-    for (int s = 0; s < nf; ++s) {
-      const uint4 A = A_n, B = B_n;
-      if (s + kRecordPrefetch < nf) {
-        prefetch_l2(pa + (long long)kRecordPrefetch * n);
-        prefetch_l2(pb + (long long)kRecordPrefetch * n);
-      }
-      if (s + 1 < nf) {
-        pa += n;
-        pb += n;
+  const long long fb = __ldg(e.range_fbase + r) + j, eb = __ldg(e.range_ebase + r) + j;
+  if constexpr (STAGES == 0) {
+    {
+      const uint4* pa = e.faceA + fb;
+      const uint4* pb = e.faceB + fb;
+      uint4 A_n = make_uint4(0u, 0u, 0u, 0u), B_n = make_uint4(0u, 0u, 0u, 0u);
+      if (nf > 0) {
         A_n = __ldcs(pa);
         B_n = __ldcs(pb);
       }
-      const float muA = __uint_as_float(A.y), lmA = __uint_as_float(A.z);
-      if (!(muA > 0.f || lmA > 0.f)) continue;
-      const R pose[4] = {R(__uint_as_float(A.w)), R(__uint_as_float(B.x)), R(__uint_as_float(B.y)),
-                         R(__uint_as_float(B.z))};
-      const float kd = __uint_as_float(B.w);
-      const int ia = vs + int(A.x & 0xffffu), ib = vs + int(A.x >> 16);
-      vec3<R> xp[3];
-      if (kd > 0.f) {
-        xp[0] = ld3<R>(c.qprev[v]);
-        xp[1] = ld3<R>(c.qprev[ia]);
-        xp[2] = ld3<R>(c.qprev[ib]);
+      for (int q = 1; q < kRecordPrefetch && q < nf; ++q) {
+        prefetch_l2(pa + (long long)q * n);
+        prefetch_l2(pb + (long long)q * n);
       }
-      membrane_add<R>(0, x, pos.ld(ia), pos.ld(ib), pose, R(muA), R(lmA), R(kd), R(1), c.dt, xp, f, H);
+      for (int s = 0; s < nf; ++s) {
+        const uint4 A = A_n, B = B_n;
+        if (s + kRecordPrefetch < nf) {
+          prefetch_l2(pa + (long long)kRecordPrefetch * n);
+          prefetch_l2(pb + (long long)kRecordPrefetch * n);
+        }
+        if (s + 1 < nf) {
+          pa += n;
+          pb += n;
+          A_n = __ldcs(pa);
+          B_n = __ldcs(pb);
+        }
+        ell16_face<R>(c, pos, v, vs, x, A, B, f, H);
+      }
     }
-  }
-  {
-    const long long b0 = __ldg(e.range_ebase + r) + j;
-    const uint4* ph = e.hinge + b0;
-    uint4 h_n = make_uint4(0u, 0u, 0u, 0u);
-    if (ne > 0) h_n = __ldcs(ph);
-    for (int q = 1; q < kRecordPrefetch && q < ne; ++q) prefetch_l2(ph + (long long)q * n);
-    for (int s = 0; s < ne; ++s) {
-      const uint4 hh = h_n;
-      if (s + kRecordPrefetch < ne) prefetch_l2(ph + (long long)kRecordPrefetch * n);
-      if (s + 1 < ne) {
-        ph += n;
-        h_n = __ldcs(ph);
+    {
+      const uint4* ph = e.hinge + eb;
+      uint4 h_n = make_uint4(0u, 0u, 0u, 0u);
+      if (ne > 0) h_n = __ldcs(ph);
+      for (int q = 1; q < kRecordPrefetch && q < ne; ++q) prefetch_l2(ph + (long long)q * n);
+      for (int s = 0; s < ne; ++s) {
+        const uint4 hh = h_n;
+        if (s + kRecordPrefetch < ne) prefetch_l2(ph + (long long)kRecordPrefetch * n);
+        if (s + 1 < ne) {
+          ph += n;
+          h_n = __ldcs(ph);
+        }
+        ell16_hinge<R>(pos, vs, x, hh, c.dt, f, H);
       }
-      const float k = __uint_as_float(hh.w);
-      if (!(k > 0.f)) continue;
-      const int role = int((hh.y >> 16) & 3u);
-      const vec3<R> o0 = pos.ld(vs + int(hh.x & 0xffffu));
-      const vec3<R> o1 = pos.ld(vs + int(hh.x >> 16));
-      const vec3<R> o2 = pos.ld(vs + int(hh.y & 0xffffu));
-      // put the solved vertex back at its place among the four
-      vec3<R> xs[4];
-      xs[0] = role == 0 ? x : o0;
-      xs[1] = role == 0 ? o0 : (role == 1 ? x : o1);
-      xs[2] = role <= 1 ? o1 : (role == 2 ? x : o2);
-      xs[3] = role == 3 ? x : o2;
-      bending_add<R>(role, xs, R(__uint_as_float(hh.z)), R(1), R(k), R(0), c.dt, nullptr, f, H);
+    }
+  } else {
+    const int t = threadIdx.x, bd = blockDim.x;
+    uint4* ra = ring + t;                // cell (stage k) at ra[k * bd]
+    uint4* rb = ring + STAGES * bd + t;
+    {
+      const uint4* pa = e.faceA + fb;
+      const uint4* pb = e.faceB + fb;
+#pragma unroll
+      for (int q = 0; q < STAGES - 1; ++q) {
+        if (q < nf) {
+          cp_async16(ra + q * bd, pa + (long long)q * n);
+          cp_async16(rb + q * bd, pb + (long long)q * n);
+        }
+        cp_async_commit();
+      }
+      for (int s = 0; s < nf; ++s) {
+        const int q = s + STAGES - 1;
+        if (q < nf) {
+          const int k = q % STAGES;
+          cp_async16(ra + k * bd, pa + (long long)q * n);
+          cp_async16(rb + k * bd, pb + (long long)q * n);
+        }
+        cp_async_commit();
+        cp_async_wait<STAGES - 1>();  // the group of slot s is complete
+        const int k = s % STAGES;
+        const uint4 A = ra[k * bd], B = rb[k * bd];
+        ell16_face<R>(c, pos, v, vs, x, A, B, f, H);
+      }
+    }
+    {
+      const uint4* ph = e.hinge + eb;
+#pragma unroll
+      for (int q = 0; q < STAGES - 1; ++q) {
+        if (q < ne) cp_async16(ra + q * bd, ph + (long long)q * n);
+        cp_async_commit();
+      }
+      for (int s = 0; s < ne; ++s) {
+        const int q = s + STAGES - 1;
+        if (q < ne) cp_async16(ra + (q % STAGES) * bd, ph + (long long)q * n);
+        cp_async_commit();
+        cp_async_wait<STAGES - 1>();
+        const uint4 hh = ra[(s % STAGES) * bd];
+        ell16_hinge<R>(pos, vs, x, hh, c.dt, f, H);
+      }
     }
   }
   const R md = m * c.dt2r;
@@ -379,11 +456,17 @@ __device__ __forceinline__ void solve_ell16(const StepCtx<R>& c, const P& pos, c
   pos.st(v, xn);
 }
 
-template <typename R, int MODE, bool SMEM, int OCC>
+// STAGES > 0: the record ring (2 x STAGES x blockDim cells of 16 bytes) lives in dynamic shared memory at
+// e.ring_offset (rounded up to 16 bytes), after the instance positions when SMEM.
+template <typename R, int MODE, bool SMEM, int OCC, int STAGES = 0>
 __global__ void __launch_bounds__(OCC ? 256 : 512, OCC ? OCC : 1) k_persistent_ell16(StepCtx<R> c, PersistentPlan p,
                                                                                     Ell16View e) {
   extern __shared__ float s_pos[];
   __shared__ int s_item;
+  // ring start rounded up to 16 bytes (the launch adds 16 bytes of slack for this)
+  uint4* ring = nullptr;
+  if constexpr (STAGES > 0)
+    ring = reinterpret_cast<uint4*>((reinterpret_cast<uintptr_t>(s_pos) + size_t(e.ring_offset) + 15) & ~uintptr_t(15));
   for (;;) {
     __syncthreads();
     if (threadIdx.x == 0) s_item = atomicAdd(p.queue, 1);
@@ -407,7 +490,7 @@ __global__ void __launch_bounds__(OCC ? 256 : 512, OCC ? OCC : 1) k_persistent_e
         const int a = __ldg(p.color_ranges + col), b = __ldg(p.color_ranges + col + 1);
         const int r = col - w;
         for (int j = threadIdx.x; j < b - a; j += blockDim.x)
-          solve_ell16<R, MODE>(c, pos, e, r, b - a, j, __ldg(p.color_verts + a + j), vs, it);
+          solve_ell16<R, MODE, STAGES>(c, pos, e, ring, r, b - a, j, __ldg(p.color_verts + a + j), vs, it);
         __syncthreads();
       }
     }
