@@ -1641,9 +1641,9 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
   // default lanes per vertex: 8 for one persistent instance and for models with tetrahedra or springs (a
   // vertex of a tet mesh has ~11 incident tets; 8 lanes measured fastest on 4,096 blocks of 640 tets: 5.3 ms
   // per substep against 19.1 / 10.0 / 6.1 / 6.8 ms with 1 / 2 / 4 / 16), else 1 (one lane per stencil row)
-  h->L = lpv ? lpv
-             : (((h->schedule == VBD_SCHEDULE_PERSISTENT && h->W == 1 && params->layout != VBD_LAYOUT_ELL) || soft) ? 8
-                                                                                                                : 1);
+  const bool stencil_asked = params->layout == VBD_LAYOUT_ELL || params->layout == VBD_LAYOUT_ELL16 ||
+                             params->layout == VBD_LAYOUT_RING;
+  h->L = lpv ? lpv : (((h->schedule == VBD_SCHEDULE_PERSISTENT && h->W == 1 && !stencil_asked) || soft) ? 8 : 1);
   for (int w = 0; w < h->W; ++w) h->max_inst_v = std::max(h->max_inst_v, wstart[w + 1] - wstart[w]);
   if (h->schedule == VBD_SCHEDULE_PERSISTENT && h->precision != VBD_PRECISION_FP64 &&
       params->positions_in_shared != 1) {
