@@ -227,7 +227,7 @@ def run_ours(args):
     else:
         shape = dict(schedule="persistent", lanes_per_vertex=args.lanes, block_size=args.block,
                      positions_in_shared=args.shared, layout=args.layout, min_blocks_per_sm=args.occ,
-                     record_stages=args.stages)  # fmt: skip
+                     pair_vertices=args.pair)  # fmt: skip
     tune_s = time.time() - t0
     builder, sides = build_batch(rank_seed(args.seed, rank), args.instances)
     model = builder.finalize(dev)
@@ -1018,7 +1018,7 @@ def main():
     ap.add_argument("--shared", choices=["auto", "on", "off"], default="auto")
     ap.add_argument("--layout", choices=["auto", "ring", "ell16", "ell", "csr"], default="auto")
     ap.add_argument("--occ", type=int, default=0, help="resident 256-thread CTAs per SM the kernel is compiled for")
-    ap.add_argument("--stages", type=int, default=0, help="ell16: stencil records staged through shared memory (4)")
+    ap.add_argument("--pair", action="store_true", help="ell16: two vertices per thread in paired FP32 instructions")
     ap.add_argument("--no-tune", dest="tune", action="store_false", help="use the launch-shape flags, not the autotuner")
     ap.add_argument("--tune-instances", type=int, default=1024)
     ap.add_argument("--e2e-steps", type=int, default=5)

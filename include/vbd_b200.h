@@ -123,9 +123,9 @@ typedef struct VbdSolverParams {
   int32_t layout;               /* VBD_LAYOUT_*; AUTO = ELL16 where it applies, else ELL when lanes_per_vertex is 1 */
   int32_t min_blocks_per_sm;    /* ELL + persistent, FP32/MIXED: 2..4 compiles the kernel for that many
                                    resident CTAs of 256 threads per SM (fewer registers); 0 = none */
-  int32_t record_stages;        /* ELL16 + persistent, FP32/MIXED: 4 = each thread streams its stencil records
-                                   through a 4-deep shared-memory ring with cp.async (2 x 4 x block_size x 16
-                                   bytes of shared memory per CTA) instead of register prefetch; 0 = off */
+  int32_t pair_vertices;        /* ELL16 + persistent, FP32: 1 = each thread solves two vertices of a color at
+                                   once, one per lane of the paired FP32 instructions (FFMA2/FADD2/FMUL2);
+                                   0 = one vertex per thread */
 } VbdSolverParams;
 
 typedef struct VbdContactsDesc {

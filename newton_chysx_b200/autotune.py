@@ -8,7 +8,7 @@ changes the speed of the sweep on a B200:
   ids, one lane per vertex) or ``csr`` (adjacency + element records) with 1, 2 or 4 lanes per vertex;
 * the persistent kernel's register budget (``min_blocks_per_sm``: 2, 3, 4 CTAs of 256 threads per SM,
   or the compiler's choice), whether an instance's positions live in shared memory, and whether the ell16
-  kernel stages its stencil records through shared memory (``record_stages``);
+  kernel pairs two vertices per thread in paired FP32 instructions (``pair_vertices``);
 * the block size of the per-color schedule.
 
 Each candidate is a separate solver on the same model; results do not depend on the choice beyond
@@ -33,7 +33,7 @@ def candidates(model: Model, schedule: str):
                 out.append(dict(layout=layout, lanes_per_vertex=1, positions_in_shared="off", min_blocks_per_sm=occ))
                 if layout == "ell16":
                     out.append(dict(layout=layout, lanes_per_vertex=1, positions_in_shared="off", min_blocks_per_sm=occ,
-                                    record_stages=4))  # fmt: skip
+                                    pair_vertices=True))  # fmt: skip
             out.append(dict(layout=layout, lanes_per_vertex=1, positions_in_shared="on"))
         for lanes, shared in itertools.product((1, 2, 4), ("off", "on")):
             out.append(dict(layout="csr", lanes_per_vertex=lanes, positions_in_shared=shared))

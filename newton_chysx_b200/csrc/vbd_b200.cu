@@ -18,7 +18,7 @@
 #include "vbd_ell.cuh"
 #include "vbd_ring.cuh"
 #include "vbd_soft.h"
-#include "vbd_ell16_staged.h"
+#include "vbd_ell16_pair.h"
 
 using namespace vbd;
 
@@ -152,7 +152,7 @@ struct VbdSolver {
   size_t smem_bytes = 0;  // > 0: persistent kernel keeps instance positions in shared memory
   int max_inst_v = 0;
   int occ = 0;  // ELL persistent kernel: compiled occupancy target (CTAs of 256 per SM), 0 = none
-  int stages = 0;  // ELL16 persistent kernel: records staged through shared memory (kEll16Stages), 0 = not
+  bool pair = false;  // ELL16 persistent kernel, FP32: two vertices per thread in paired FP32 arithmetic
   int K = 1;
   // packed model
   int4* tri_idx = nullptr;
@@ -609,7 +609,6 @@ Ell16View ell16_view(const VbdSolver* h) {
   e.faceA = h->ell16_faceA;
   e.faceB = h->ell16_faceB;
   e.hinge = h->ell16_hinge;
-  e.ring_offset = int(h->smem_bytes);
   return e;
 }
 
@@ -1133,11 +1132,10 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
     } else if (h->layout == VBD_LAYOUT_ELL16) {
       const Ell16View e = ell16_view(h);
       if constexpr (std::is_same<R, float>::value) {
-        const size_t ss = ell16_staged_smem(h->smem_bytes, h->block);
-        if (h->stages && h->smem_bytes > 0)
-          launch_persistent_ell16_staged<R, MODE, true>(h->occ, c, p, e, h->grid_persistent, h->block, ss, st);
-        else if (h->stages)
-          launch_persistent_ell16_staged<R, MODE, false>(h->occ, c, p, e, h->grid_persistent, h->block, ss, st);
+        if (MODE == MODE_FP32 && h->pair && h->smem_bytes > 0)
+          launch_persistent_ell16_pair<true>(h->occ, c, p, e, h->grid_persistent, h->block, h->smem_bytes, st);
+        else if (MODE == MODE_FP32 && h->pair)
+          launch_persistent_ell16_pair<false>(h->occ, c, p, e, h->grid_persistent, h->block, 0, st);
         else if (h->smem_bytes > 0)
           launch_persistent_ell16<R, MODE, true>(h->occ, c, p, e, h->grid_persistent, h->block, h->smem_bytes, st);
         else
@@ -1267,13 +1265,8 @@ const void* persistent_kernel(VbdSolver* h) {
       return sm ? persistent_ring_fn<float, MODE_MIXED, true>(h->occ) : persistent_ring_fn<float, MODE_MIXED, false>(h->occ);
     return sm ? persistent_ring_fn<float, MODE_FP32, true>(h->occ) : persistent_ring_fn<float, MODE_FP32, false>(h->occ);
   }
-  if (h->layout == VBD_LAYOUT_ELL16 && h->stages) {
-    if (h->precision == VBD_PRECISION_MIXED)
-      return sm ? persistent_ell16_staged_fn<float, MODE_MIXED, true>(h->occ)
-                : persistent_ell16_staged_fn<float, MODE_MIXED, false>(h->occ);
-    return sm ? persistent_ell16_staged_fn<float, MODE_FP32, true>(h->occ)
-              : persistent_ell16_staged_fn<float, MODE_FP32, false>(h->occ);
-  }
+  if (h->layout == VBD_LAYOUT_ELL16 && h->pair)
+    return sm ? persistent_ell16_pair_fn<true>(h->occ) : persistent_ell16_pair_fn<false>(h->occ);
   if (h->layout == VBD_LAYOUT_ELL16) {
     if (h->precision == VBD_PRECISION_FP64) return persistent_ell16_fn<double, MODE_FP64, false>(0);
     if (h->precision == VBD_PRECISION_MIXED)
@@ -1303,7 +1296,7 @@ int occupancy_grid(VbdSolver* h) {
   int dev = 0, sms = 0, per_sm = 0;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  const size_t dyn = h->stages ? ell16_staged_smem(h->smem_bytes, h->block) : h->smem_bytes;
+  const size_t dyn = h->smem_bytes;
   if (dyn > 0) CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, h->block, dyn));
   if (per_sm < 1) return VBD_ERR_INVALID_ARGUMENT;
@@ -1710,16 +1703,11 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
     }
     if ((rc = h->layout == VBD_LAYOUT_RING ? build_ring(h) : build_ell(h))) return fail(rc);
   }
-  if (params->record_stages != 0) {
-    if (params->record_stages != kEll16Stages || h->layout != VBD_LAYOUT_ELL16 || h->schedule != VBD_SCHEDULE_PERSISTENT ||
-        h->precision == VBD_PRECISION_FP64)
+  if (params->pair_vertices != 0) {
+    if (params->pair_vertices != 1 || h->layout != VBD_LAYOUT_ELL16 || h->schedule != VBD_SCHEDULE_PERSISTENT ||
+        h->precision != VBD_PRECISION_FP32)
       return fail(VBD_ERR_INVALID_ARGUMENT);
-    int dev = 0, optin = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
-      return fail(VBD_ERR_CUDA);
-    if (ell16_staged_smem(h->smem_bytes, h->block) > size_t(optin)) return fail(VBD_ERR_UNSUPPORTED);
-    h->stages = params->record_stages;
+    h->pair = true;
   }
   if (h->schedule == VBD_SCHEDULE_PERSISTENT && (rc = occupancy_grid(h))) return fail(rc);
   if (cudaDeviceSynchronize() != cudaSuccess) return fail(VBD_ERR_CUDA);

@@ -21,9 +21,8 @@
 //   float  kd                read only when the model has non-zero bending damping
 // Empty slots (vertices with fewer elements than the range's maximum) carry zero stiffness.
 #pragma once
-#include <cstdint>
-
 #include "vbd_kernels.cuh"
+#include "vbd_pair.cuh"
 
 namespace vbd {
 
@@ -255,22 +254,7 @@ struct Ell16View {
   const uint4* faceA;
   const uint4* faceB;
   const uint4* hinge;
-  int ring_offset;  // STAGES > 0: byte offset of the record ring in dynamic shared memory
 };
-
-// Staged record fetch (STAGES > 0): each thread streams its own records through a ring of STAGES 16-byte
-// shared-memory cells per array with cp.async (.cg: cached in L2 only), STAGES - 1 slots ahead of use. The
-// loads then wait in the copy path instead of holding registers, and a thread reads only the cells it filled
-// itself, so the ring needs no barrier: cp.async.wait_group orders the copies of one thread.
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 
 // Membrane term of one 32-byte face record (A, B halves) for the solved vertex v at x.
 template <typename R, typename P>
@@ -309,10 +293,9 @@ __device__ __forceinline__ void ell16_hinge(const P& pos, int vs, vec3<R> x, uin
   bending_add<R>(role, xs, R(__uint_as_float(hh.z)), R(1), R(k), R(0), dt, nullptr, f, H);
 }
 
-// ring: STAGES > 0 only, this block's record ring (2 x STAGES x blockDim cells).
-template <typename R, int MODE, int STAGES, typename P>
-__device__ __forceinline__ void solve_ell16(const StepCtx<R>& c, const P& pos, const Ell16View& e, uint4* ring, int r,
-                                            int n, int j, int v, int vs, int iteration) {
+template <typename R, int MODE, typename P>
+__device__ __forceinline__ void solve_ell16(const StepCtx<R>& c, const P& pos, const Ell16View& e, int r, int n, int j,
+                                            int v, int vs, int iteration) {
   const pos4_t<R> in4 = c.inertia[v];
   const R m = R(in4.w);
   if (m == R(0)) return;
@@ -321,7 +304,7 @@ __device__ __forceinline__ void solve_ell16(const StepCtx<R>& c, const P& pos, c
   sym3<R> H = szero<R>();
   const int nf = __ldg(e.range_nf + r), ne = __ldg(e.range_ne + r);
   const long long fb = __ldg(e.range_fbase + r) + j, eb = __ldg(e.range_ebase + r) + j;
-  if constexpr (STAGES == 0) {
+  {
     {
       const uint4* pa = e.faceA + fb;
       const uint4* pb = e.faceB + fb;
@@ -361,51 +344,6 @@ __device__ __forceinline__ void solve_ell16(const StepCtx<R>& c, const P& pos, c
           ph += n;
           h_n = __ldcs(ph);
         }
-        ell16_hinge<R>(pos, vs, x, hh, c.dt, f, H);
-      }
-    }
-  } else {
-    const int t = threadIdx.x, bd = blockDim.x;
-    uint4* ra = ring + t;                // cell (stage k) at ra[k * bd]
-    uint4* rb = ring + STAGES * bd + t;
-    {
-      const uint4* pa = e.faceA + fb;
-      const uint4* pb = e.faceB + fb;
-#pragma unroll
-      for (int q = 0; q < STAGES - 1; ++q) {
-        if (q < nf) {
-          cp_async16(ra + q * bd, pa + (long long)q * n);
-          cp_async16(rb + q * bd, pb + (long long)q * n);
-        }
-        cp_async_commit();
-      }
-      for (int s = 0; s < nf; ++s) {
-        const int q = s + STAGES - 1;
-        if (q < nf) {
-          const int k = q % STAGES;
-          cp_async16(ra + k * bd, pa + (long long)q * n);
-          cp_async16(rb + k * bd, pb + (long long)q * n);
-        }
-        cp_async_commit();
-        cp_async_wait<STAGES - 1>();  // the group of slot s is complete
-        const int k = s % STAGES;
-        const uint4 A = ra[k * bd], B = rb[k * bd];
-        ell16_face<R>(c, pos, v, vs, x, A, B, f, H);
-      }
-    }
-    {
-      const uint4* ph = e.hinge + eb;
-#pragma unroll
-      for (int q = 0; q < STAGES - 1; ++q) {
-        if (q < ne) cp_async16(ra + q * bd, ph + (long long)q * n);
-        cp_async_commit();
-      }
-      for (int s = 0; s < ne; ++s) {
-        const int q = s + STAGES - 1;
-        if (q < ne) cp_async16(ra + (q % STAGES) * bd, ph + (long long)q * n);
-        cp_async_commit();
-        cp_async_wait<STAGES - 1>();
-        const uint4 hh = ra[(s % STAGES) * bd];
         ell16_hinge<R>(pos, vs, x, hh, c.dt, f, H);
       }
     }
@@ -456,17 +394,151 @@ __device__ __forceinline__ void solve_ell16(const StepCtx<R>& c, const P& pos, c
   pos.st(v, xn);
 }
 
-// STAGES > 0: the record ring (2 x STAGES x blockDim cells of 16 bytes) lives in dynamic shared memory at
-// e.ring_offset (rounded up to 16 bytes), after the instance positions when SMEM.
-template <typename R, int MODE, bool SMEM, int OCC, int STAGES = 0>
+// Two vertices of one color range (records j0 and j1, particles v0 and v1) solved together, one per lane of
+// the paired FP32 arithmetic of vbd_pair.cuh: the same terms, order and 3x3 solve as solve_ell16 in FP32. When
+// has1 is false lane 1 repeats lane 0 and is discarded. A face with damping falls back to the scalar membrane
+// for that slot. Contacts and the checks of the solve run per lane.
+template <typename P>
+__device__ __forceinline__ void solve_ell16_pair(const StepCtx<float>& c, const P& pos, const Ell16View& e, int r, int n,
+                                                 int j0, int j1, int v0, int v1, bool has1, int vs) {
+  const float4 in0 = c.inertia[v0], in1 = c.inertia[v1];
+  const bool act0 = in0.w != 0.f, act1 = has1 && in1.w != 0.f;
+  if (!act0 && !act1) return;
+  const vec3<float> xs0 = pos.ld(v0), xs1 = pos.ld(v1);
+  const pv3 x = pv3_of(xs0, xs1);
+  pv3 f = {pfs(0.f), pfs(0.f), pfs(0.f)};
+  psym H = {pfs(0.f), pfs(0.f), pfs(0.f), pfs(0.f), pfs(0.f), pfs(0.f)};
+  const int nf = __ldg(e.range_nf + r), ne = __ldg(e.range_ne + r);
+  const long long fb = __ldg(e.range_fbase + r);
+  {
+    const uint4* pa = e.faceA + fb;
+    const uint4* pb = e.faceB + fb;
+    for (int q = 0; q < kRecordPrefetch && q < nf; ++q) {
+      prefetch_l2(pa + (long long)q * n + j0);
+      prefetch_l2(pb + (long long)q * n + j0);
+      prefetch_l2(pa + (long long)q * n + j1);
+      prefetch_l2(pb + (long long)q * n + j1);
+    }
+    for (int s = 0; s < nf; ++s, pa += n, pb += n) {
+      if (s + kRecordPrefetch < nf) {
+        prefetch_l2(pa + (long long)kRecordPrefetch * n + j0);
+        prefetch_l2(pb + (long long)kRecordPrefetch * n + j0);
+        prefetch_l2(pa + (long long)kRecordPrefetch * n + j1);
+        prefetch_l2(pb + (long long)kRecordPrefetch * n + j1);
+      }
+      const uint4 A0 = __ldcs(pa + j0), B0 = __ldcs(pb + j0), A1 = __ldcs(pa + j1), B1 = __ldcs(pb + j1);
+      if (__uint_as_float(B0.w) > 0.f || __uint_as_float(B1.w) > 0.f) {
+        // damped face: scalar membrane per lane
+        vec3<float> fl = zero3<float>();
+        sym3<float> hl = szero<float>();
+        ell16_face<float>(c, pos, v0, vs, xs0, A0, B0, fl, hl);
+        f.x.v.x += fl.x, f.y.v.x += fl.y, f.z.v.x += fl.z;
+        H.xx.v.x += hl.xx, H.yy.v.x += hl.yy, H.zz.v.x += hl.zz, H.xy.v.x += hl.xy, H.xz.v.x += hl.xz, H.yz.v.x += hl.yz;
+        fl = zero3<float>();
+        hl = szero<float>();
+        ell16_face<float>(c, pos, v1, vs, xs1, A1, B1, fl, hl);
+        f.x.v.y += fl.x, f.y.v.y += fl.y, f.z.v.y += fl.z;
+        H.xx.v.y += hl.xx, H.yy.v.y += hl.yy, H.zz.v.y += hl.zz, H.xy.v.y += hl.xy, H.xz.v.y += hl.xz, H.yz.v.y += hl.yz;
+        continue;
+      }
+      float mu0 = __uint_as_float(A0.y), lm0 = __uint_as_float(A0.z);
+      float mu1 = __uint_as_float(A1.y), lm1 = __uint_as_float(A1.z);
+      const bool on0 = mu0 > 0.f || lm0 > 0.f, on1 = mu1 > 0.f || lm1 > 0.f;
+      if (!on0 && !on1) continue;
+      if (!on0) mu0 = lm0 = 0.f;  // an inactive face in one lane adds exactly zero
+      if (!on1) mu1 = lm1 = 0.f;
+      const pv3 xa = pv3_of(pos.ld(vs + int(A0.x & 0xffffu)), pos.ld(vs + int(A1.x & 0xffffu)));
+      const pv3 xb = pv3_of(pos.ld(vs + int(A0.x >> 16)), pos.ld(vs + int(A1.x >> 16)));
+      pmembrane_add(x, xa, xb, pf2(__uint_as_float(A0.w), __uint_as_float(A1.w)),
+                    pf2(__uint_as_float(B0.x), __uint_as_float(B1.x)), pf2(__uint_as_float(B0.y), __uint_as_float(B1.y)),
+                    pf2(__uint_as_float(B0.z), __uint_as_float(B1.z)), pf2(mu0, mu1), pf2(lm0, lm1), f, H);
+    }
+  }
+  {
+    const uint4* ph = e.hinge + __ldg(e.range_ebase + r);
+    for (int q = 0; q < kRecordPrefetch && q < ne; ++q) {
+      prefetch_l2(ph + (long long)q * n + j0);
+      prefetch_l2(ph + (long long)q * n + j1);
+    }
+    for (int s = 0; s < ne; ++s, ph += n) {
+      if (s + kRecordPrefetch < ne) {
+        prefetch_l2(ph + (long long)kRecordPrefetch * n + j0);
+        prefetch_l2(ph + (long long)kRecordPrefetch * n + j1);
+      }
+      const uint4 h0 = __ldcs(ph + j0), h1 = __ldcs(ph + j1);
+      float k0 = __uint_as_float(h0.w), k1 = __uint_as_float(h1.w);
+      const bool on0 = k0 > 0.f, on1 = k1 > 0.f;
+      if (!on0 && !on1) continue;
+      if (!on0) k0 = 0.f;
+      if (!on1) k1 = 0.f;
+      const int role0 = int((h0.y >> 16) & 3u), role1 = int((h1.y >> 16) & 3u);
+      vec3<float> a[4], b[4];
+      {
+        const vec3<float> o0 = pos.ld(vs + int(h0.x & 0xffffu)), o1 = pos.ld(vs + int(h0.x >> 16)),
+                          o2 = pos.ld(vs + int(h0.y & 0xffffu));
+        a[0] = role0 == 0 ? xs0 : o0;
+        a[1] = role0 == 0 ? o0 : (role0 == 1 ? xs0 : o1);
+        a[2] = role0 <= 1 ? o1 : (role0 == 2 ? xs0 : o2);
+        a[3] = role0 == 3 ? xs0 : o2;
+      }
+      {
+        const vec3<float> o0 = pos.ld(vs + int(h1.x & 0xffffu)), o1 = pos.ld(vs + int(h1.x >> 16)),
+                          o2 = pos.ld(vs + int(h1.y & 0xffffu));
+        b[0] = role1 == 0 ? xs1 : o0;
+        b[1] = role1 == 0 ? o0 : (role1 == 1 ? xs1 : o1);
+        b[2] = role1 <= 1 ? o1 : (role1 == 2 ? xs1 : o2);
+        b[3] = role1 == 3 ? xs1 : o2;
+      }
+      const pv3 xh[4] = {pv3_of(a[0], b[0]), pv3_of(a[1], b[1]), pv3_of(a[2], b[2]), pv3_of(a[3], b[3])};
+      pbending_add(xh, pf2(__uint_as_float(h0.z), __uint_as_float(h1.z)), pf2(k0, k1), role0, role1, f, H);
+    }
+  }
+  const pf md = pf2(in0.w, in1.w) * pfs(c.dt2r);
+  f = pfma(pv3_of(vec3<float>{in0.x, in0.y, in0.z}, vec3<float>{in1.x, in1.y, in1.z}) - x, md, f);
+  H.xx = H.xx + md;
+  H.yy = H.yy + md;
+  H.zz = H.zz + md;
+  if (c.has_contacts) {
+    vec3<float> fl = lane0(f);
+    sym3<float> hl = lane0(H);
+    if (act0) contacts_add<float>(c, v0, xs0, fl, hl);
+    vec3<float> fr = lane1(f);
+    sym3<float> hr = lane1(H);
+    if (act1) contacts_add<float>(c, v1, xs1, fr, hr);
+    f = pv3_of(fl, fr);
+    H = {pf2(hl.xx, hr.xx), pf2(hl.yy, hr.yy), pf2(hl.zz, hr.zz), pf2(hl.xy, hr.xy), pf2(hl.xz, hr.xz), pf2(hl.yz, hr.yz)};
+  }
+  // 3x3 solve by adjugate (sdet, sadj_mul)
+  const pf cxx = pfms(H.yz, H.yz, H.yy * H.zz), cyy = pfms(H.xz, H.xz, H.xx * H.zz), czz = pfms(H.xy, H.xy, H.xx * H.yy);
+  const pf cxy = pfms(H.xy, H.zz, H.xz * H.yz), cxz = pfms(H.xz, H.yy, H.xy * H.yz), cyz = pfms(H.xx, H.yz, H.xy * H.xz);
+  const pf det = pfma(H.xz, cxz, pfma(H.xy, cxy, H.xx * cxx));
+  const pv3 ad = {pfma(cxz, f.z, pfma(cxy, f.y, cxx * f.x)), pfma(cyz, f.z, pfma(cyy, f.y, cxy * f.x)),
+                  pfma(czz, f.z, pfma(cyz, f.y, cxz * f.x))};
+  const pf inv = pdiv(pfs(1.f), det);
+  const pv3 xn = pfma(ad, inv, x);
+  const vec3<float> xn0 = lane0(xn), xn1 = lane1(xn);
+  const float d0 = det.v.x, d1 = det.v.y;
+  if (act0) {
+    if (!isfinite(d0)) set_err(c.err, 1);
+    else if (!(fabsf(d0) > 1e-8f)) set_err(c.err, 4);
+    else if (!(isfinite(xn0.x) && isfinite(xn0.y) && isfinite(xn0.z))) set_err(c.err, 1);
+    else pos.st(v0, xn0);
+  }
+  if (act1) {
+    if (!isfinite(d1)) set_err(c.err, 1);
+    else if (!(fabsf(d1) > 1e-8f)) set_err(c.err, 4);
+    else if (!(isfinite(xn1.x) && isfinite(xn1.y) && isfinite(xn1.z))) set_err(c.err, 1);
+    else pos.st(v1, xn1);
+  }
+}
+
+// PAIR (FP32 only): each thread solves two vertices of a color at once with paired FP32 instructions
+// (solve_ell16_pair).
+template <typename R, int MODE, bool SMEM, int OCC, bool PAIR = false>
 __global__ void __launch_bounds__(OCC ? 256 : 512, OCC ? OCC : 1) k_persistent_ell16(StepCtx<R> c, PersistentPlan p,
                                                                                     Ell16View e) {
   extern __shared__ float s_pos[];
   __shared__ int s_item;
-  // ring start rounded up to 16 bytes (the launch adds 16 bytes of slack for this)
-  uint4* ring = nullptr;
-  if constexpr (STAGES > 0)
-    ring = reinterpret_cast<uint4*>((reinterpret_cast<uintptr_t>(s_pos) + size_t(e.ring_offset) + 15) & ~uintptr_t(15));
   for (;;) {
     __syncthreads();
     if (threadIdx.x == 0) s_item = atomicAdd(p.queue, 1);
@@ -489,8 +561,18 @@ __global__ void __launch_bounds__(OCC ? 256 : 512, OCC ? OCC : 1) k_persistent_e
       for (int col = cb; col + 1 < ce; ++col) {
         const int a = __ldg(p.color_ranges + col), b = __ldg(p.color_ranges + col + 1);
         const int r = col - w;
-        for (int j = threadIdx.x; j < b - a; j += blockDim.x)
-          solve_ell16<R, MODE, STAGES>(c, pos, e, ring, r, b - a, j, __ldg(p.color_verts + a + j), vs, it);
+        if constexpr (PAIR) {
+          const int bd = blockDim.x;
+          for (int j = threadIdx.x; j < b - a; j += 2 * bd) {
+            const bool has1 = j + bd < b - a;
+            const int v0 = __ldg(p.color_verts + a + j);
+            const int v1 = has1 ? __ldg(p.color_verts + a + j + bd) : v0;
+            solve_ell16_pair(c, pos, e, r, b - a, j, has1 ? j + bd : j, v0, v1, has1, vs);
+          }
+        } else {
+          for (int j = threadIdx.x; j < b - a; j += blockDim.x)
+            solve_ell16<R, MODE>(c, pos, e, r, b - a, j, __ldg(p.color_verts + a + j), vs, it);
+        }
         __syncthreads();
       }
     }

@@ -22,8 +22,8 @@ Beyond the reference keywords:
   manifold fans), ``"csr"`` (adjacency + element records; any lanes per vertex), ``"auto"``.
 * ``min_blocks_per_sm``: 2..4 compiles the persistent stencil kernel for that many resident CTAs of
   256 threads per SM (a register budget); 0 leaves the compiler's choice.
-* ``record_stages``: 4 makes the ell16 persistent kernel stream its stencil records through a 4-deep
-  shared-memory ring per thread (``cp.async``) instead of holding the next record in registers; 0 = off.
+* ``pair_vertices``: the ell16 persistent kernel (FP32) solves two vertices per thread, one in each lane
+  of Blackwell's paired FP32 instructions (FFMA2 / FADD2 / FMUL2), halving the arithmetic instructions.
 
 Particle self-contact (``particle_enable_self_contact=True`` and the ``particle_self_contact_*``
 keywords) runs on the per-color schedule with the csr layout; see ``collision.py`` for the filters and
@@ -97,7 +97,7 @@ class SolverVBD:
         positions_in_shared: str = "auto",
         layout: str = "auto",
         min_blocks_per_sm: int = 0,
-        record_stages: int = 0,
+        pair_vertices: bool = False,
     ):
         if rigid_avbd_beta < 0:
             raise ValueError(f"rigid_avbd_beta must be >= 0, got {rigid_avbd_beta}")
@@ -217,7 +217,7 @@ class SolverVBD:
         prm.positions_in_shared = {"auto": 0, "off": 1, "on": 2}[positions_in_shared]
         prm.layout = _lib.LAYOUT[layout]
         prm.min_blocks_per_sm = int(min_blocks_per_sm)
-        prm.record_stages = int(record_stages)
+        prm.pair_vertices = int(bool(pair_vertices))
         self._prm = prm
 
         h = C.c_void_p()
