@@ -125,7 +125,7 @@ def test_paired_vertices_need_fp32_ell16_persistent():
     model = model_from_golden(g)
     for kw in (dict(layout="ell"), dict(layout="csr"), dict(precision="mixed"), dict(schedule="per_color")):
         args = dict(dict(schedule="persistent", layout="ell16"), **kw)
-        with pytest.raises(_lib.VbdError, match="invalid argument"):
+        with pytest.raises(_lib.VbdError, match="invalid argument|unsupported"):
             SolverVBD(model, iterations=2, pair_vertices=True, **args)
 
 
