@@ -2,8 +2,8 @@
 // values living in the two lanes of a float2, and every add, multiply and fused multiply-add is one paired
 // instruction (sm_100 FADD2 / FMUL2 / FFMA2 through __fadd2_rn / __fmul2_rn / __ffma2_rn). Each lane is
 // rounded exactly like the scalar instruction, so a lane computes what the scalar code computes up to the
-// compiler's choice of where to fuse a multiply and an add. Square roots, divisions and atan2 stay scalar per
-// lane. Only the FP32 sweep uses this.
+// compiler's choice of where to fuse a multiply and an add. Square roots and divisions stay scalar per lane;
+// atan2 evaluates the polynomial of vatan2 (vbd_math.cuh) in paired instructions. Only the FP32 sweep uses this.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -28,7 +28,27 @@ __device__ __forceinline__ pf pfms(pf a, pf b, pf c) { return {__ffma2_rn(make_f
 __device__ __forceinline__ pf pmax(pf a, pf b) { return pf2(fmaxf(a.v.x, b.v.x), fmaxf(a.v.y, b.v.y)); }
 __device__ __forceinline__ pf prsqrt(pf a) { return pf2(rsqrtf(a.v.x), rsqrtf(a.v.y)); }
 __device__ __forceinline__ pf pdiv(pf a, pf b) { return pf2(a.v.x / b.v.x, a.v.y / b.v.y); }
-__device__ __forceinline__ pf patan2(pf y, pf x) { return pf2(atan2f(y.v.x, x.v.x), atan2f(y.v.y, x.v.y)); }
+// vatan2 (vbd_math.cuh) with the polynomial in paired instructions
+__device__ __forceinline__ pf patan2(pf y, pf x) {
+  const float ax0 = fabsf(x.v.x), ay0 = fabsf(y.v.x), ax1 = fabsf(x.v.y), ay1 = fabsf(y.v.y);
+  const pf t = pf2(__fdividef(fminf(ax0, ay0), fmaxf(fmaxf(ax0, ay0), 1.0e-30f)),
+                   __fdividef(fminf(ax1, ay1), fmaxf(fmaxf(ax1, ay1), 1.0e-30f)));
+  const pf t2 = t * t;
+  pf p = pfma(pfs(-0.0040540580f), t2, pfs(0.0218612288f));
+  p = pfma(p, t2, pfs(-0.0559098861f));
+  p = pfma(p, t2, pfs(0.0964200441f));
+  p = pfma(p, t2, pfs(-0.1390853351f));
+  p = pfma(p, t2, pfs(0.1994653599f));
+  p = pfma(p, t2, pfs(-0.3332985605f));
+  p = pfma(p, t2, pfs(0.9999993329f));
+  const pf r = p * t;
+  float r0 = r.v.x, r1 = r.v.y;
+  if (ay0 > ax0) r0 = 1.57079632679489662f - r0;
+  if (ay1 > ax1) r1 = 1.57079632679489662f - r1;
+  if (x.v.x < 0.f) r0 = 3.14159265358979324f - r0;
+  if (x.v.y < 0.f) r1 = 3.14159265358979324f - r1;
+  return pf2(copysignf(r0, y.v.x), copysignf(r1, y.v.y));
+}
 
 struct pv3 {
   pf x, y, z;
