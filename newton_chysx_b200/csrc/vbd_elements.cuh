@@ -45,7 +45,7 @@ __host__ __device__ __forceinline__ void membrane_add(int ord, vec3<R> x0, vec3<
   const R J = Jsq * invJ;
   const R lnh = lmbd + mu;
   const R lsafe = (lnh < R(0) ? R(-1) : R(1)) * vmax(vabs(lnh), R(1.0e-6));
-  const R alpha = R(1) + mu / lsafe;
+  const R alpha = R(1) + vdiv_fast(mu, lsafe);
   const vec3<R> g0 = invJ * (f11 * f0 - f01 * f1);
   const vec3<R> g1 = invJ * (f00 * f1 - f01 * f0);
   const R s = lnh * (J - alpha);
@@ -100,28 +100,29 @@ __host__ __device__ __forceinline__ void bending_add(int ord, const vec3<R> x[4]
   const R eps2 = R(1.0e-12);
   if (s1 < eps2 || s2 < eps2 || se < eps2) return;
   const R il1 = vrsqrt(s1), il2 = vrsqrt(s2), ile = vrsqrt(se);
-  const vec3<R> n1 = N1 * il1, n2 = N2 * il2, eh = e * ile;
-  const R s = dot(cross(n1, n2), eh);
-  const R c = dot(n1, n2);
-  const R theta = vatan2(s, c);
+  // theta = atan2((n1 x n2) . e/|e|, n1 . n2), evaluated on the unnormalised normals: both arguments carry
+  // the common factor |N1| |N2| > 0, which atan2 ignores
+  const R theta = vatan2(dot(cross(N1, N2), e) * ile, dot(N1, N2));
   const R k = ke * rest_length;
   const R dE = k * (theta - rest_angle);
   const R le = se * ile;  // |e|
-  // dtheta/dx_ord = alpha n1 + beta n2
-  R alpha, beta;
+  // dtheta/dx_ord = alpha n1 + beta n2 = a N1 + b N2 with a = alpha / |N1|, b = beta / |N2|
+  const R q1 = il1 * il1, q2 = il2 * il2;
+  R a, b;
   if (ord <= 1) {
-    alpha = ord == 0 ? -le * il1 : R(0);
-    beta = ord == 1 ? -le * il2 : R(0);
+    a = ord == 0 ? -le * q1 : R(0);
+    b = ord == 1 ? -le * q2 : R(0);
   } else {
     const vec3<R> a1 = ord == 2 ? x03 : -x02;
     const vec3<R> a2 = ord == 2 ? x13 : -x12;
-    alpha = dot(a1, eh) * il1;
-    beta = dot(a2, eh) * il2;
+    a = dot(a1, e) * (ile * q1);
+    b = dot(a2, e) * (ile * q2);
   }
-  const vec3<R> d = alpha * n1 + beta * n2;
+  const vec3<R> d = a * N1 + b * N2;
   f = f + (-dE) * d;
   R hk = k;
   if (kd > R(0)) {
+    const vec3<R> n1 = N1 * il1, n2 = N2 * il2, eh = e * ile;
     const vec3<R> d0 = (-le * il1) * n1, d1 = (-le * il2) * n2;
     const vec3<R> d2 = (dot(x03, eh) * il1) * n1 + (dot(x13, eh) * il2) * n2;
     const vec3<R> d3 = (-dot(x02, eh) * il1) * n1 - (dot(x12, eh) * il2) * n2;
@@ -214,7 +215,7 @@ __host__ __device__ __forceinline__ void tet_add(int ord, const vec3<R> x[4], co
   const R J = dot(F0, C0);
   const R lnh = lmbd + mu;
   const R lsafe = (lnh < R(0) ? R(-1) : R(1)) * vmax(vabs(lnh), R(1.0e-6));
-  const R alpha = R(1) + mu / lsafe;
+  const R alpha = R(1) + vdiv_fast(mu, lsafe);
   const R s = lnh * (J - alpha);
   // row selection by comparisons, not by a computed index, so that dm stays in registers
   vec3<R> m;
