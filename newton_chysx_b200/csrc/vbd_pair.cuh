@@ -28,6 +28,8 @@ __device__ __forceinline__ pf pfms(pf a, pf b, pf c) { return {__ffma2_rn(make_f
 __device__ __forceinline__ pf pmax(pf a, pf b) { return pf2(fmaxf(a.v.x, b.v.x), fmaxf(a.v.y, b.v.y)); }
 __device__ __forceinline__ pf prsqrt(pf a) { return pf2(rsqrtf(a.v.x), rsqrtf(a.v.y)); }
 __device__ __forceinline__ pf pdiv(pf a, pf b) { return pf2(a.v.x / b.v.x, a.v.y / b.v.y); }
+// vdiv_fast per lane
+__device__ __forceinline__ pf pdiv_fast(pf a, pf b) { return pf2(__fdividef(a.v.x, b.v.x), __fdividef(a.v.y, b.v.y)); }
 // vatan2 (vbd_math.cuh) with the polynomial in paired instructions
 __device__ __forceinline__ pf patan2(pf y, pf x) {
   const float ax0 = fabsf(x.v.x), ay0 = fabsf(y.v.x), ax1 = fabsf(x.v.y), ay1 = fabsf(y.v.y);
@@ -102,7 +104,7 @@ __device__ __forceinline__ void pmembrane_add(pv3 x0, pv3 x1, pv3 x2, pf D00, pf
   const pf lnh = lmbd + mu;
   const pf lsafe = pf2(copysignf(fmaxf(fabsf(lnh.v.x), 1.0e-6f), lnh.v.x < 0.f ? -1.f : 1.f),
                        copysignf(fmaxf(fabsf(lnh.v.y), 1.0e-6f), lnh.v.y < 0.f ? -1.f : 1.f));
-  const pf alpha = pfs(1.f) + pdiv(mu, lsafe);
+  const pf alpha = pfs(1.f) + pdiv_fast(mu, lsafe);
   const pv3 g0 = pfma(f0, f11, f1 * (-f01)) * invJ;
   const pv3 g1 = pfma(f1, f00, f0 * (-f01)) * invJ;
   const pf s = lnh * (J - alpha);
@@ -139,10 +141,8 @@ __device__ __forceinline__ void pbending_add(const pv3 x[4], pf rest_angle, pf k
   if (bad0) s1.v.x = s2.v.x = se.v.x = 1.f, kk.v.x = 0.f;
   if (bad1) s1.v.y = s2.v.y = se.v.y = 1.f, kk.v.y = 0.f;
   const pf il1 = prsqrt(s1), il2 = prsqrt(s2), ile = prsqrt(se);
-  const pv3 n1 = N1 * il1, n2 = N2 * il2, eh = e * ile;
-  const pf sn = pdot(pcross(n1, n2), eh);
-  const pf cs = pdot(n1, n2);
-  const pf theta = patan2(sn, cs);
+  // the angle from the unnormalised normals (atan2 ignores the common factor |N1| |N2|), as bending_add
+  const pf theta = patan2(pdot(pcross(N1, N2), e) * ile, pdot(N1, N2));
   const pf dE = kk * (theta - rest_angle);
   const pf le = se * ile;
   // dtheta/dx_role = alpha n1 + beta n2 (bending_add): roles 0, 1: -|e| / |N_i| on their own normal; roles 2, 3:
@@ -150,9 +150,10 @@ __device__ __forceinline__ void pbending_add(const pv3 x[4], pf rest_angle, pf k
   const pf c0 = pf2(role0 == 0, role1 == 0), c1 = pf2(role0 == 1, role1 == 1);
   const pf c2 = pf2(role0 == 2, role1 == 2), c3 = pf2(role0 == 3, role1 == 3);
   const pv3 a1 = pfma(x03, c2, x02 * (-c3)), a2 = pfma(x13, c2, x12 * (-c3));
-  const pf alpha = pfms(c0, le, pdot(a1, eh)) * il1;
-  const pf beta = pfms(c1, le, pdot(a2, eh)) * il2;
-  const pv3 d = pfma(n1, alpha, n2 * beta);
+  // d = alpha n1 + beta n2 = a N1 + b N2 with a = alpha / |N1|, b = beta / |N2|
+  const pf a = pfms(c0, le, pdot(a1, e) * ile) * (il1 * il1);
+  const pf b = pfms(c1, le, pdot(a2, e) * ile) * (il2 * il2);
+  const pv3 d = pfma(N1, a, N2 * b);
   f = pfma(d, -dE, f);
   psouter_add(H, d, kk);
 }
