@@ -404,8 +404,8 @@ def cpu_baseline(args, seconds=15.0):
         q = m.particle_q.numpy().astype(np.float64)
         qd = np.zeros_like(q)
         t = time.perf_counter()
-        cnt, p, s, bp, bv, nn = orc.soft_contacts(q, m.particle_radius.numpy(), m.particle_flags.numpy(), m.shape_type,
-                                                  m.shape_pos, m.shape_radius, 0.01)  # fmt: skip
+        cnt, p, s, bp, bv, nn = orc.soft_contacts_shapes(q, m.particle_radius.numpy(), m.particle_flags.numpy(),
+                                                         m.shape_type, m.shape_transform, m.shape_scale, 0.01)  # fmt: skip
         contacts = orc.make_contacts(cnt, p, s, bp, bv, nn)
         orc.step(om, q, qd, None, contacts, DT, ITERATIONS, precision=32, nthreads=threads)
         elapsed += time.perf_counter() - t
@@ -617,8 +617,9 @@ def cpu_baseline_selfcontact(m, q, qd):
                          margin=SC_KW["particle_self_contact_margin"], vt_filter=vt, ee_filter=ee)  # fmt: skip
     q = q.astype(np.float64)
     t = time.perf_counter()
-    cnt, p, s, bp, bv, nn = orc.soft_contacts(q, m.particle_radius.cpu().numpy(), m.particle_flags.cpu().numpy(),
-                                              m.shape_type, m.shape_pos, m.shape_radius, 0.01)  # fmt: skip
+    cnt, p, s, bp, bv, nn = orc.soft_contacts_shapes(q, m.particle_radius.cpu().numpy(),
+                                                     m.particle_flags.cpu().numpy(), m.shape_type, m.shape_transform,
+                                                     m.shape_scale, 0.01)  # fmt: skip
     orc.step(om, q, qd.astype(np.float64), None, orc.make_contacts(cnt, p, s, bp, bv, nn), DT, SC_ITERATIONS,
              precision=32, nthreads=threads, self_contact=sc)  # fmt: skip
     el = time.perf_counter() - t
@@ -768,8 +769,8 @@ def cpu_baseline_soft(sample_worlds=256, seconds=10.0):
     om = orc.Model(oracle_model_dict(m))
     q = m.particle_q.double().numpy()
     qd = m.particle_qd.double().numpy()
-    cnt, p, s, bp, bv, nn = orc.soft_contacts(q, m.particle_radius.numpy(), m.particle_flags.numpy(), m.shape_type,
-                                              m.shape_pos, m.shape_radius, 0.01)  # fmt: skip
+    cnt, p, s, bp, bv, nn = orc.soft_contacts_shapes(q, m.particle_radius.numpy(), m.particle_flags.numpy(),
+                                                     m.shape_type, m.shape_transform, m.shape_scale, 0.01)  # fmt: skip
     t = time.perf_counter()
     n = 0
     while n == 0 or time.perf_counter() - t < seconds:

@@ -358,6 +358,21 @@ int vbd_soft_contacts(int32_t particle_count, const float* q_dev, const float* r
                       int32_t* particle_dev, int32_t* shape_dev, float* body_pos_dev, float* body_vel_dev,
                       float* normal_dev, void* stream);
 
+/* Soft contacts against static analytic shapes, as CollisionPipeline.collide writes them for shapes without a
+   body (create_soft_contacts, geometry/kernels.py:1001-1140, with the SDFs and gradients of
+   geometry/kernels.py:132-600). shape_type holds the reference's GeoType values: 1 plane (local +Z normal;
+   scale (width, length), 0 = infinite, else the reference's Chebyshev distance to the quad), 3 sphere (r),
+   4 capsule (r, half height; along local Z), 5 ellipsoid (rx, ry, rz), 6 cylinder (r, half height; along local
+   Z), 7 box (half extents); other types return VBD_ERR_UNSUPPORTED. shape_transform_host [S,7]: position and
+   rotation quaternion (x, y, z, w) of each shape; shape_scale_host [S,3]; at most 16 shapes. Contacts are
+   written as vbd_soft_contacts writes them: the contact point on the surface in world (the body frame of a
+   static shape), zero body velocity, the world normal; slots from an atomic counter. */
+int vbd_soft_contacts_shapes(int32_t particle_count, const float* q_dev, const float* radius_dev,
+                             const int32_t* flags_dev, int32_t shape_count, const int32_t* shape_type_host,
+                             const float* shape_transform_host, const float* shape_scale_host, float margin,
+                             int32_t soft_contact_max, int32_t* count_dev, int32_t* particle_dev, int32_t* shape_dev,
+                             float* body_pos_dev, float* body_vel_dev, float* normal_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

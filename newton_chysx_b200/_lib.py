@@ -135,6 +135,10 @@ SIGNATURES = {
         C.c_int,
     ),
     "vbd_collider_destroy": ([_vp], C.c_int),
+    "vbd_soft_contacts_shapes": (
+        [C.c_int32, _vp, _vp, _vp, C.c_int32, _ip, _fp, _fp, C.c_float, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+        C.c_int,
+    ),
     "vbd_soft_contacts": (
         [C.c_int32, _vp, _vp, _vp, C.c_int32, _ip, _fp, _fp, _fp, C.c_float, C.c_int32, _vp, _vp, _vp, _vp, _vp,
          _vp, _vp],

@@ -19,6 +19,7 @@
 #include "vbd_ring.cuh"
 #include "vbd_soft.h"
 #include "vbd_ell16_pair.h"
+#include "vbd_shapes.cuh"
 
 using namespace vbd;
 
@@ -123,6 +124,50 @@ __global__ void k_soft_contacts(int n, const float* __restrict__ q, const float*
         body_vel[3 * k + j] = 0.f;
         normal[3 * k + j] = nn[j];
       }
+    }
+  }
+}
+
+struct ShapeXformTable {
+  int type[kMaxContactShapes];
+  float4 p[kMaxContactShapes];  // position
+  float4 q[kMaxContactShapes];  // rotation (x, y, z, w)
+  float4 sc[kMaxContactShapes];  // scale
+};
+
+__device__ __forceinline__ vec3<float> rot_q(float4 q, vec3<float> v) {
+  const vec3<float> u = {q.x, q.y, q.z};
+  return v * (2.f * q.w * q.w - 1.f) + cross(u, v) * (2.f * q.w) + u * (2.f * dot(u, v));
+}
+
+// create_soft_contacts (geometry/kernels.py:1001-1140) for static analytic shapes: one thread per
+// (particle, shape), the particle in the shape frame, shape_sdf, and for d < margin + radius a contact at the
+// closest surface point x_local - n d and the normal, both mapped back to world; slots from an atomic counter.
+__global__ void k_soft_contacts_shapes(int n, const float* __restrict__ q, const float* __restrict__ radius,
+                                       const int* __restrict__ flags, int S, const ShapeXformTable shapes, float margin,
+                                       int cmax, int* count, int* particle, int* shape, float* body_pos, float* body_vel,
+                                       float* normal) {
+  const long tid = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (tid >= long(n) * S) return;
+  const int i = int(tid / S), s = int(tid % S);
+  if (!(flags[i] & 1)) return;
+  const float4 P = shapes.p[s], Q = shapes.q[s], SC = shapes.sc[s];
+  const float4 Qi = make_float4(-Q.x, -Q.y, -Q.z, Q.w);
+  const vec3<float> xl = rot_q(Qi, vec3<float>{q[3 * i] - P.x, q[3 * i + 1] - P.y, q[3 * i + 2] - P.z});
+  const float sc[3] = {SC.x, SC.y, SC.z};
+  float d;
+  vec3<float> nn;
+  shape_sdf(shapes.type[s], xl, sc, d, nn);
+  if (d < margin + radius[i]) {
+    const int k = atomicAdd(count, 1);
+    if (k < cmax) {
+      const vec3<float> bp = rot_q(Q, xl - nn * d) + vec3<float>{P.x, P.y, P.z};
+      const vec3<float> wn = rot_q(Q, nn);
+      particle[k] = i;
+      shape[k] = s;
+      body_pos[3 * k] = bp.x, body_pos[3 * k + 1] = bp.y, body_pos[3 * k + 2] = bp.z;
+      body_vel[3 * k] = body_vel[3 * k + 1] = body_vel[3 * k + 2] = 0.f;
+      normal[3 * k] = wn.x, normal[3 * k + 1] = wn.y, normal[3 * k + 2] = wn.z;
     }
   }
 }
@@ -1960,6 +2005,39 @@ int vbd_soft_contacts(int32_t n, const float* q, const float* radius, const int3
   const long total = long(n) * S;
   k_soft_contacts<<<int((total + 255) / 256), 256, 0, st>>>(n, q, radius, flags, S, tab, margin, cmax, count, particle,
                                                             shape, body_pos, body_vel, normal);
+  CK(cudaGetLastError());
+  return VBD_OK;
+}
+
+int vbd_soft_contacts_shapes(int32_t n, const float* q, const float* radius, const int32_t* flags, int32_t S,
+                             const int32_t* shape_type, const float* shape_transform, const float* shape_scale,
+                             float margin, int32_t cmax, int32_t* count, int32_t* particle, int32_t* shape,
+                             float* body_pos, float* body_vel, float* normal, void* stream) {
+  if (n < 0 || S < 0 || S > kMaxContactShapes || cmax < 0 || !count ||
+      (S && (!shape_type || !shape_transform || !shape_scale)))
+    return VBD_ERR_INVALID_ARGUMENT;
+  if (n > 0 && S > 0 && (!q || !radius || !flags || (cmax > 0 && (!particle || !shape || !body_pos || !body_vel || !normal))))
+    return VBD_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaMemsetAsync(count, 0, sizeof(int), st));
+  if (n == 0 || S == 0) return VBD_OK;
+  ShapeXformTable tab;
+  std::memset(&tab, 0, sizeof(tab));
+  for (int s = 0; s < S; ++s) {
+    const int t = shape_type[s];
+    if (t != GEO_PLANE && t != GEO_SPHERE && t != GEO_CAPSULE && t != GEO_ELLIPSOID && t != GEO_CYLINDER && t != GEO_BOX)
+      return VBD_ERR_UNSUPPORTED;
+    const float* X = shape_transform + 7 * s;
+    const float ql = std::sqrt(X[3] * X[3] + X[4] * X[4] + X[5] * X[5] + X[6] * X[6]);
+    if (!(ql > 0.f)) return VBD_ERR_INVALID_ARGUMENT;
+    tab.type[s] = t;
+    tab.p[s] = make_float4(X[0], X[1], X[2], 0.f);
+    tab.q[s] = make_float4(X[3] / ql, X[4] / ql, X[5] / ql, X[6] / ql);
+    tab.sc[s] = make_float4(shape_scale[3 * s], shape_scale[3 * s + 1], shape_scale[3 * s + 2], 0.f);
+  }
+  const long total = long(n) * S;
+  k_soft_contacts_shapes<<<int((total + 255) / 256), 256, 0, st>>>(n, q, radius, flags, S, tab, margin, cmax, count,
+                                                                   particle, shape, body_pos, body_vel, normal);
   CK(cudaGetLastError());
   return VBD_OK;
 }

@@ -35,8 +35,19 @@ class ParticleFlags(enum.IntEnum):
 
 
 class GeoType(enum.IntEnum):
-    PLANE = 0
-    SPHERE = 1
+    """``newton/_src/geometry/types.py:68-110`` (the same values)."""
+
+    NONE = 0
+    PLANE = 1
+    HFIELD = 2
+    SPHERE = 3
+    CAPSULE = 4
+    ELLIPSOID = 5
+    CYLINDER = 6
+    BOX = 7
+    MESH = 8
+    CONE = 9
+    CONVEX_MESH = 10
 
 
 @dataclasses.dataclass
@@ -58,6 +69,32 @@ def quat_from_axis_angle(axis, angle):
     a = a / np.linalg.norm(a)
     s = math.sin(angle * 0.5)
     return (float(a[0] * s), float(a[1] * s), float(a[2] * s), math.cos(angle * 0.5))
+
+
+def quat_between_vectors(a, b):
+    """The rotation taking direction a to direction b (x, y, z, w)."""
+    a = np.asarray(a, dtype=np.float64) / np.linalg.norm(a)
+    b = np.asarray(b, dtype=np.float64) / np.linalg.norm(b)
+    c = float(np.dot(a, b))
+    if c < -1.0 + 1e-9:  # opposite: half a turn about any axis perpendicular to a
+        axis = np.cross(a, (1.0, 0.0, 0.0))
+        if np.linalg.norm(axis) < 1e-6:
+            axis = np.cross(a, (0.0, 1.0, 0.0))
+        return quat_from_axis_angle(axis, math.pi)
+    v = np.cross(a, b)
+    q = np.array([v[0], v[1], v[2], 1.0 + c])
+    q /= np.linalg.norm(q)
+    return tuple(float(x) for x in q)
+
+
+def _xform(xform):
+    """(position, quaternion xyzw) from None, a (p, q) pair or a 7-vector."""
+    if xform is None:
+        return (0.0, 0.0, 0.0), quat_identity()
+    if len(xform) == 2:
+        return tuple(float(v) for v in xform[0]), tuple(float(v) for v in xform[1])
+    x = [float(v) for v in xform]
+    return tuple(x[:3]), tuple(x[3:7]) if len(x) >= 7 else quat_identity()
 
 
 def quat_to_matrix(q):
@@ -620,21 +657,47 @@ class ModelBuilder:
                 h = mesh_hinges(self.tri_indices[t0:self._t])
                 self.add_edges(h[:, 0], h[:, 1], h[:, 2], h[:, 3], edge_ke=edge_ke, edge_kd=edge_kd)
 
-    # -- shapes
-    def add_ground_plane(self, cfg: ShapeConfig | None = None):
-        cfg = cfg or self.default_shape_cfg
-        self.shapes.append(dict(type=GeoType.PLANE, pos=(0.0, 0.0, 0.0), normal=self.up_vector, radius=0.0,
-                                ke=cfg.ke, kd=cfg.kd, mu=cfg.mu, body=-1))  # fmt: skip
-        return len(self.shapes) - 1
-
-    def add_shape_sphere(self, body=-1, xform=None, radius=1.0, cfg: ShapeConfig | None = None):
+    # -- shapes (builder.py:5900-6340): static collision shapes for particle contacts
+    def _add_shape(self, body, type_, xform, scale, cfg):
         if body != -1:
-            raise NotImplementedError("only static spheres (body=-1) are supported")
+            raise NotImplementedError("only static shapes (body=-1) collide with particles here")
         cfg = cfg or self.default_shape_cfg
-        p = (0.0, 0.0, 0.0) if xform is None else tuple(float(v) for v in (xform[0] if len(xform) == 2 else xform[:3]))
-        self.shapes.append(dict(type=GeoType.SPHERE, pos=p, normal=(0.0, 0.0, 1.0), radius=float(radius), ke=cfg.ke,
+        p, q = _xform(xform)
+        self.shapes.append(dict(type=GeoType(type_), pos=p, rot=q, scale=tuple(float(v) for v in scale), ke=cfg.ke,
                                 kd=cfg.kd, mu=cfg.mu, body=-1))  # fmt: skip
         return len(self.shapes) - 1
+
+    def add_shape_plane(self, plane=(0.0, 0.0, 1.0, 0.0), xform=None, width=10.0, length=10.0, body=-1,
+                        cfg: ShapeConfig | None = None):  # fmt: skip
+        """A plane with normal along the local Z of xform, or from the equation a x + b y + c z + d = 0; width
+        and length 0 make it infinite."""
+        if xform is None:
+            nrm = np.asarray(plane[:3], dtype=np.float64)
+            ln = np.linalg.norm(nrm)
+            nrm = nrm / ln
+            pos = -(plane[3] / ln) * nrm
+            xform = (tuple(pos), quat_between_vectors((0.0, 0.0, 1.0), nrm))
+        return self._add_shape(body, GeoType.PLANE, xform, (width, length, 0.0), cfg)
+
+    def add_ground_plane(self, height=0.0, cfg: ShapeConfig | None = None):
+        return self.add_shape_plane(plane=(*self.up_vector, -height), width=0.0, length=0.0, cfg=cfg)
+
+    def add_shape_sphere(self, body=-1, xform=None, radius=1.0, cfg: ShapeConfig | None = None):
+        return self._add_shape(body, GeoType.SPHERE, xform, (radius, 0.0, 0.0), cfg)
+
+    def add_shape_box(self, body=-1, xform=None, hx=0.5, hy=0.5, hz=0.5, cfg: ShapeConfig | None = None):
+        return self._add_shape(body, GeoType.BOX, xform, (hx, hy, hz), cfg)
+
+    def add_shape_capsule(self, body=-1, xform=None, radius=1.0, half_height=0.5, cfg: ShapeConfig | None = None):
+        """Capsule along the local Z axis of xform."""
+        return self._add_shape(body, GeoType.CAPSULE, xform, (radius, half_height, 0.0), cfg)
+
+    def add_shape_cylinder(self, body=-1, xform=None, radius=1.0, half_height=0.5, cfg: ShapeConfig | None = None):
+        """Cylinder along the local Z axis of xform."""
+        return self._add_shape(body, GeoType.CYLINDER, xform, (radius, half_height, 0.0), cfg)
+
+    def add_shape_ellipsoid(self, body=-1, xform=None, rx=1.0, ry=0.75, rz=0.5, cfg: ShapeConfig | None = None):
+        return self._add_shape(body, GeoType.ELLIPSOID, xform, (rx, ry, rz), cfg)
 
     # -- coloring (builder.py:9304-9396)
     @property
@@ -771,10 +834,10 @@ class Model:
             m.world_particle_start = np.array(b.world_particle_start + [b._n], dtype=np.int32)
         m.shape_count = len(b.shapes)
         S = m.shape_count
+        # host copies (the contact generator takes the shape table by value): GeoType, (p, q xyzw), scale
         m.shape_type = np.array([int(s["type"]) for s in b.shapes], dtype=np.int32)
-        m.shape_pos = np.array([s["pos"] for s in b.shapes], dtype=np.float32).reshape(S, 3)
-        m.shape_normal = np.array([s["normal"] for s in b.shapes], dtype=np.float32).reshape(S, 3)
-        m.shape_radius = np.array([s["radius"] for s in b.shapes], dtype=np.float32).reshape(S)
+        m.shape_transform = np.array([list(s["pos"]) + list(s["rot"]) for s in b.shapes], dtype=np.float32).reshape(S, 7)
+        m.shape_scale = np.array([s["scale"] for s in b.shapes], dtype=np.float32).reshape(S, 3)
         m.shape_material_ke = t(np.array([s["ke"] for s in b.shapes]).reshape(S), f32)
         m.shape_material_kd = t(np.array([s["kd"] for s in b.shapes]).reshape(S), f32)
         m.shape_material_mu = t(np.array([s["mu"] for s in b.shapes]).reshape(S), f32)
@@ -859,31 +922,31 @@ class Contacts:
 
 
 def soft_contacts(model: Model, state: State, contacts: Contacts, margin: float):
-    """Particle vs static ground plane / sphere contacts on the GPU (``vbd_soft_contacts``)."""
+    """Particle contacts against the model's static analytic shapes on the GPU (``vbd_soft_contacts_shapes``)."""
     lib = _lib.load()
     S = model.shape_count
     if S == 0:
         contacts.soft_contact_count.zero_()
         return
     st = np.ascontiguousarray(model.shape_type, dtype=np.int32)
-    sp = np.ascontiguousarray(model.shape_pos, dtype=np.float32)
-    sr = np.ascontiguousarray(model.shape_radius, dtype=np.float32)
-    sn = np.ascontiguousarray(model.shape_normal, dtype=np.float32)
+    sx = np.ascontiguousarray(model.shape_transform, dtype=np.float32)
+    ss = np.ascontiguousarray(model.shape_scale, dtype=np.float32)
     ip, fp = C.POINTER(C.c_int32), C.POINTER(C.c_float)
     stream = torch.cuda.current_stream(model.device).cuda_stream
-    rc = lib.vbd_soft_contacts(
+    rc = lib.vbd_soft_contacts_shapes(
         model.particle_count, state.particle_q.data_ptr(), model.particle_radius.data_ptr(),
-        model.particle_flags.data_ptr(), S, st.ctypes.data_as(ip), sp.ctypes.data_as(fp), sr.ctypes.data_as(fp),
-        sn.ctypes.data_as(fp), float(margin), contacts.soft_contact_max, contacts.soft_contact_count.data_ptr(),
+        model.particle_flags.data_ptr(), S, st.ctypes.data_as(ip), sx.ctypes.data_as(fp), ss.ctypes.data_as(fp),
+        float(margin), contacts.soft_contact_max, contacts.soft_contact_count.data_ptr(),
         contacts.soft_contact_particle.data_ptr(), contacts.soft_contact_shape.data_ptr(),
         contacts.soft_contact_body_pos.data_ptr(), contacts.soft_contact_body_vel.data_ptr(),
         contacts.soft_contact_normal.data_ptr(), C.c_void_p(stream),
     )  # fmt: skip
-    _lib.check(rc, "vbd_soft_contacts")
+    _lib.check(rc, "vbd_soft_contacts_shapes")
 
 
 class CollisionPipeline:
-    """Particle-shape part of ``newton/_src/sim/collide.py:485`` (static planes and spheres)."""
+    """Particle-shape part of ``newton/_src/sim/collide.py:485`` (static planes, spheres, boxes, capsules,
+    cylinders and ellipsoids)."""
 
     def __init__(self, model: Model, soft_contact_max=None, soft_contact_margin=0.01, **_ignored):
         self.model = model

@@ -1231,6 +1231,105 @@ int step(const Model& M, double* q_in, const double* qd_in, const double* f_ext,
 
 }  // namespace
 
+// ------------------------------------------------------------------------------------ particle-shape contacts
+// create_soft_contacts (geometry/kernels.py:1001-1140) for static shapes of the analytic types, with the SDFs
+// and gradients of geometry/kernels.py:132-600 (capsule and cylinder along the shape's local Z, straight
+// cylinders): the particle in the shape frame, d and n from the shape's SDF, and for d < margin + radius the
+// contact point x_local - n d and the normal mapped back to world. Contacts in particle-major order.
+namespace sdf {
+using D3 = V3<double>;
+enum { PLANE = 1, SPHERE = 3, CAPSULE = 4, ELLIPSOID = 5, CYLINDER = 6, BOX = 7 };
+inline double sgn(double x) { return x < 0.0 ? -1.0 : 1.0; }  // wp.sign: -1 below zero, 1 otherwise
+inline D3 qrot(const double* q, D3 v) {  // q = (x, y, z, w)
+  const D3 u = v3(q[0], q[1], q[2]);
+  const double w = q[3];
+  return v * (2.0 * w * w - 1.0) + cross(u, v) * (2.0 * w) + u * (2.0 * dot(u, v));
+}
+inline D3 normalize0(D3 a) {  // wp.normalize: the zero vector stays zero
+  const double l = length(a);
+  return l > 0.0 ? a / l : a;
+}
+// geometry/kernels.py:165-195
+inline double sphere(D3 p, double r) { return length(p) - r; }
+inline D3 sphere_grad(D3 p) {
+  const double l = length(p);
+  return l > 1.0e-8 ? p / l : v3(0.0, 0.0, 1.0);
+}
+// :198-259
+inline double box(D3 p, double hx, double hy, double hz) {
+  const double qx = std::fabs(p.x) - hx, qy = std::fabs(p.y) - hy, qz = std::fabs(p.z) - hz;
+  const D3 e = v3(std::max(qx, 0.0), std::max(qy, 0.0), std::max(qz, 0.0));
+  return length(e) + std::min(std::max(qx, std::max(qy, qz)), 0.0);
+}
+inline D3 box_grad(D3 p, double hx, double hy, double hz) {
+  const double qx = std::fabs(p.x) - hx, qy = std::fabs(p.y) - hy, qz = std::fabs(p.z) - hz;
+  if (qx > 0.0 || qy > 0.0 || qz > 0.0) {
+    const D3 c = v3(std::min(std::max(p.x, -hx), hx), std::min(std::max(p.y, -hy), hy), std::min(std::max(p.z, -hz), hz));
+    return normalize0(p - c);
+  }
+  if ((qx > qy && qx > qz) || (qy == 0.0 && qz == 0.0)) return v3(sgn(p.x), 0.0, 0.0);
+  if ((qy > qx && qy > qz) || (qx == 0.0 && qz == 0.0)) return v3(0.0, sgn(p.y), 0.0);
+  return v3(0.0, 0.0, sgn(p.z));
+}
+// :262-329 (up axis Z)
+inline double capsule(D3 p, double r, double hh) {
+  if (p.z > hh) return length(v3(p.x, p.y, p.z - hh)) - r;
+  if (p.z < -hh) return length(v3(p.x, p.y, p.z + hh)) - r;
+  return length(v3(p.x, p.y, 0.0)) - r;
+}
+inline D3 capsule_grad(D3 p, double hh) {
+  D3 v = v3(p.x, p.y, 0.0), g = v3(0.0, 0.0, 1.0);
+  if (p.z > hh) {
+    v = v3(p.x, p.y, p.z - hh);
+  } else if (p.z < -hh) {
+    v = v3(p.x, p.y, p.z + hh);
+    g = v3(0.0, 0.0, -1.0);
+  }
+  const double l = length(v);
+  return l > 1.0e-8 ? v / l : g;
+}
+// :332-446 (straight cylinder, up axis Z)
+inline double cylinder(D3 p, double r, double hh) {
+  const double dx = length(v3(p.x, p.y, 0.0)) - r, dy = std::fabs(p.z) - hh;
+  const double ex = std::max(dx, 0.0), ey = std::max(dy, 0.0);
+  return std::min(std::max(dx, dy), 0.0) + std::sqrt(ex * ex + ey * ey);
+}
+inline D3 cylinder_grad(D3 p, double r, double hh) {
+  const D3 v = v3(p.x, p.y, 0.0);
+  const double vl = length(v);
+  const D3 radial = vl > 1.0e-8 ? v / vl : v3(0.0, 0.0, 1.0);
+  const D3 axial = v3(0.0, 0.0, sgn(p.z));
+  const double dx = vl - r, dy = std::fabs(p.z) - hh;
+  if (dx > 0.0 && dy > 0.0) {
+    const D3 g = radial * dx + axial * dy;
+    const double gl = length(g);
+    return gl > 1.0e-8 ? g / gl : radial;
+  }
+  return dx > dy ? radial : axial;
+}
+// :449-512
+inline void ellipsoid(D3 p, D3 radii, double& d, D3& n) {
+  const D3 r = v3(std::max(std::fabs(radii.x), 1.0e-8), std::max(std::fabs(radii.y), 1.0e-8),
+                  std::max(std::fabs(radii.z), 1.0e-8));
+  const D3 ir = v3(1.0 / r.x, 1.0 / r.y, 1.0 / r.z);
+  const D3 q0 = v3(p.x * ir.x, p.y * ir.y, p.z * ir.z);
+  const D3 q1 = v3(p.x * ir.x * ir.x, p.y * ir.y * ir.y, p.z * ir.z * ir.z);
+  const double k0 = length(q0), k1 = length(q1);
+  d = k1 > 1.0e-8 ? k0 * (k0 - 1.0) / k1 : -std::min(std::min(r.x, r.y), r.z);
+  n = v3(0.0, 0.0, 1.0);
+  if (!(k1 < 1.0e-8)) {
+    const D3 g = q1 * (k0 / k1);
+    const double gl = length(g);
+    if (gl > 1.0e-8) n = g / gl;
+  }
+}
+// :568-589
+inline double plane(D3 p, double w, double l) {
+  if (w > 0.0 && l > 0.0) return std::max(std::max(std::fabs(p.x) - w, std::fabs(p.y) - l), std::fabs(p.z));
+  return p.z;
+}
+}  // namespace sdf
+
 extern "C" {
 
 struct OracleModel {
@@ -1609,6 +1708,54 @@ int oracle_soft_contacts(int n, const double* q, const double* radius, const int
             body_vel[3 * count + j] = 0.0;
             normal[3 * count + j] = nn[j];
           }
+        }
+        ++count;
+      }
+    }
+  }
+  return count;
+}
+
+
+// shape_xform [S,7] = (position, quaternion xyzw), shape_scale [S,3]. Returns the number of contacts found,
+// or -1 for a shape type without an analytic SDF here.
+int oracle_soft_contacts_shapes(int n, const double* q, const double* radius, const int* flags, int S,
+                                const int* shape_type, const double* shape_xform, const double* shape_scale,
+                                double margin, int max_contacts, int* particle, int* shape, double* body_pos,
+                                double* body_vel, double* normal) {
+  using sdf::D3;
+  for (int s = 0; s < S; ++s)
+    if (shape_type[s] != sdf::PLANE && shape_type[s] != sdf::SPHERE && shape_type[s] != sdf::CAPSULE &&
+        shape_type[s] != sdf::ELLIPSOID && shape_type[s] != sdf::CYLINDER && shape_type[s] != sdf::BOX)
+      return -1;
+  int count = 0;
+  for (int i = 0; i < n; ++i) {
+    if (!(flags[i] & 1)) continue;
+    const D3 x = v3(q[3 * i], q[3 * i + 1], q[3 * i + 2]);
+    for (int s = 0; s < S; ++s) {
+      const double* X = shape_xform + 7 * s;
+      const double* sc = shape_scale + 3 * s;
+      const double qi[4] = {-X[3], -X[4], -X[5], X[6]};
+      const D3 xl = sdf::qrot(qi, x - v3(X[0], X[1], X[2]));
+      double d = 1.0e6;
+      D3 nn = v3(0.0, 0.0, 0.0);
+      switch (shape_type[s]) {
+        case sdf::SPHERE: d = sdf::sphere(xl, sc[0]), nn = sdf::sphere_grad(xl); break;
+        case sdf::BOX: d = sdf::box(xl, sc[0], sc[1], sc[2]), nn = sdf::box_grad(xl, sc[0], sc[1], sc[2]); break;
+        case sdf::CAPSULE: d = sdf::capsule(xl, sc[0], sc[1]), nn = sdf::capsule_grad(xl, sc[1]); break;
+        case sdf::CYLINDER: d = sdf::cylinder(xl, sc[0], sc[1]), nn = sdf::cylinder_grad(xl, sc[0], sc[1]); break;
+        case sdf::ELLIPSOID: sdf::ellipsoid(xl, v3(sc[0], sc[1], sc[2]), d, nn); break;
+        default: d = sdf::plane(xl, sc[0] * 0.5, sc[1] * 0.5), nn = v3(0.0, 0.0, 1.0); break;
+      }
+      if (d < margin + radius[i]) {
+        if (count < max_contacts) {
+          const D3 bp = sdf::qrot(X + 3, xl - nn * d) + v3(X[0], X[1], X[2]);
+          const D3 wn = sdf::qrot(X + 3, nn);
+          particle[count] = i;
+          shape[count] = s;
+          body_pos[3 * count] = bp.x, body_pos[3 * count + 1] = bp.y, body_pos[3 * count + 2] = bp.z;
+          body_vel[3 * count] = body_vel[3 * count + 1] = body_vel[3 * count + 2] = 0.0;
+          normal[3 * count] = wn.x, normal[3 * count + 1] = wn.y, normal[3 * count + 2] = wn.z;
         }
         ++count;
       }

@@ -108,6 +108,9 @@ def lib():
         _lib.oracle_build_adjacency.argtypes = [C.c_int, C.c_int, _ip, C.c_int, _ip, _ip, _ip, _ip, _ip]
         _lib.oracle_soft_contacts.argtypes = [
             C.c_int, _dp, _dp, _ip, C.c_int, _ip, _dp, _dp, C.c_double, C.c_int, _ip, _ip, _dp, _dp, _dp,
+        ]
+        _lib.oracle_soft_contacts_shapes.argtypes = [
+            C.c_int, _dp, _dp, _ip, C.c_int, _ip, _dp, _dp, C.c_double, C.c_int, _ip, _ip, _dp, _dp, _dp,
         ]  # fmt: skip
         _lib.oracle_max_threads.restype = C.c_int
         _lib.oracle_vbd_step_sc.argtypes = [
@@ -292,6 +295,31 @@ def soft_contacts(q, radius, flags, shape_type, shape_pos, shape_radius, margin,
     bv, bvp = _d(np.zeros(3 * max_contacts))
     nn, nnp = _d(np.zeros(3 * max_contacts))
     cnt = lib().oracle_soft_contacts(n, qp, rp, flp, S, stp, spp, srp, margin, max_contacts, pp, shpp, bpp, bvp, nnp)
+    return cnt, part, shp, bp.reshape(-1, 3), bv.reshape(-1, 3), nn.reshape(-1, 3)
+
+
+def soft_contacts_shapes(q, radius, flags, shape_type, shape_transform, shape_scale, margin, max_contacts=None):
+    """Particle-shape contacts against static analytic shapes (GeoType values: plane 1, sphere 3, capsule 4,
+    ellipsoid 5, cylinder 6, box 7) with transforms [S, 7] (position, quaternion xyzw) and scales [S, 3], in
+    (particle, shape) order."""
+    n = len(radius)
+    S = len(shape_type)
+    max_contacts = max_contacts or n * max(S, 1)
+    qq, qp = _d(np.asarray(q).reshape(-1))
+    r, rp = _d(radius)
+    fl, flp = _i(flags)
+    st, stp = _i(shape_type)
+    sx, sxp = _d(np.asarray(shape_transform).reshape(-1))
+    ss, ssp = _d(np.asarray(shape_scale).reshape(-1))
+    part, pp = _i(-np.ones(max_contacts))
+    shp, shpp = _i(-np.ones(max_contacts))
+    bp, bpp = _d(np.zeros(3 * max_contacts))
+    bv, bvp = _d(np.zeros(3 * max_contacts))
+    nn, nnp = _d(np.zeros(3 * max_contacts))
+    cnt = lib().oracle_soft_contacts_shapes(n, qp, rp, flp, S, stp, sxp, ssp, margin, max_contacts, pp, shpp, bpp, bvp,
+                                            nnp)  # fmt: skip
+    if cnt < 0:
+        raise ValueError("a shape type without an analytic SDF")
     return cnt, part, shp, bp.reshape(-1, 3), bv.reshape(-1, 3), nn.reshape(-1, 3)
 
 

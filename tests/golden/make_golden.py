@@ -248,6 +248,15 @@ def load_reference(ref: str) -> dict:
         },
         ns,
     )
+    # particle-shape contact generation: the analytic SDFs of create_soft_contacts (geometry/kernels.py:132-600)
+    ns["Axis"] = types.SimpleNamespace(X=0, Y=1, Z=2)
+    _lift(
+        os.path.join(ref, "newton/_src/geometry/kernels.py"),
+        {"_sdf_point_to_z_up", "_sdf_vector_from_z_up", "sdf_sphere", "sdf_sphere_grad", "sdf_box", "sdf_box_grad",
+         "sdf_capsule", "sdf_capsule_grad", "sdf_cylinder", "sdf_cylinder_grad", "sdf_ellipsoid", "sdf_ellipsoid_grad",
+         "sdf_plane"},
+        ns,
+    )  # fmt: skip
     _lift(os.path.join(ref, "newton/_src/utils/mesh.py"), set(), ns, classes={"MeshAdjacency": {"*"}})
     _lift(
         os.path.join(ref, "newton/_src/sim/builder.py"),
@@ -869,6 +878,78 @@ def selfcontact_cases(ns, seed=11):
             "closest": np.array(cp), "norm": np.array(norm)}  # fmt: skip
 
 
+GEO_PLANE, GEO_SPHERE, GEO_CAPSULE, GEO_ELLIPSOID, GEO_CYLINDER, GEO_BOX = 1, 3, 4, 5, 6, 7
+
+
+def shape_contact_cases(ns, seed=17):
+    """Particle-shape soft contacts against static analytic shapes, computed as create_soft_contacts
+    (geometry/kernels.py:1001-1140) does for shapes without a body: the particle in the shape frame, the
+    shape's lifted SDF and gradient, and for d < margin + radius the contact point x_local - n d and the normal
+    mapped back to world. Contacts are listed in thread-id order (particle-major), the order of a serial
+    launch."""
+    rng = np.random.default_rng(seed)
+
+    def quat(axis, ang):
+        return wp.quat_from_axis_angle(np.asarray(axis, dtype=float), ang)
+
+    shapes = [  # type, position, rotation (x, y, z, w), scale
+        (GEO_PLANE, (0.0, 0.0, 0.0), wp.quat_identity(), (0.0, 0.0, 0.0)),
+        (GEO_PLANE, (-0.6, 0.5, 0.25), quat((1.0, 0.2, 0.0), 0.4), (0.6, 0.4, 0.0)),
+        (GEO_SPHERE, (0.5, 0.0, 0.3), wp.quat_identity(), (0.25, 0.0, 0.0)),
+        (GEO_BOX, (-0.4, -0.4, 0.3), quat((0.3, 1.0, 0.2), 0.7), (0.3, 0.2, 0.1)),
+        (GEO_CAPSULE, (0.2, 0.6, 0.35), quat((1.0, 0.0, 0.3), 1.1), (0.1, 0.2, 0.0)),
+        (GEO_CYLINDER, (0.6, -0.6, 0.2), quat((0.0, 1.0, 1.0), 0.5), (0.15, 0.1, 0.0)),
+        (GEO_ELLIPSOID, (-0.1, 0.0, 0.5), quat((1.0, 1.0, 0.0), 0.9), (0.3, 0.2, 0.15)),
+    ]
+    n = 6000
+    q = np.stack([rng.uniform(-1.0, 1.0, n), rng.uniform(-1.0, 1.0, n), rng.uniform(-0.1, 0.8, n)], axis=1)
+    radius = rng.uniform(0.005, 0.02, n)
+    flags = np.where(rng.uniform(size=n) < 0.9, 1, 0).astype(np.int32)
+    margin = 0.02
+    out = {k: [] for k in ("particle", "shape", "body_pos", "body_vel", "normal", "distance")}
+    for i in range(n):
+        if not (flags[i] & 1):
+            continue
+        for s, (typ, pos, rot, sc) in enumerate(shapes):
+            X_ws = (np.asarray(pos, dtype=float), np.asarray(rot, dtype=float))
+            X_sw = wp.transform_inverse(X_ws)
+            x_local = wp.transform_point(X_sw, wp.vec3(*q[i]))
+            scale = wp.vec3(*sc)
+            d, nn, v = 1.0e6, wp.vec3(), wp.vec3()
+            if typ == GEO_SPHERE:
+                d, nn = ns["sdf_sphere"](x_local, scale[0]), ns["sdf_sphere_grad"](x_local, scale[0])
+            if typ == GEO_BOX:
+                d = ns["sdf_box"](x_local, scale[0], scale[1], scale[2])
+                nn = ns["sdf_box_grad"](x_local, scale[0], scale[1], scale[2])
+            if typ == GEO_CAPSULE:
+                d = ns["sdf_capsule"](x_local, scale[0], scale[1], 2)
+                nn = ns["sdf_capsule_grad"](x_local, scale[0], scale[1], 2)
+            if typ == GEO_CYLINDER:
+                d = ns["sdf_cylinder"](x_local, scale[0], scale[1], 2)
+                nn = ns["sdf_cylinder_grad"](x_local, scale[0], scale[1], 2)
+            if typ == GEO_ELLIPSOID:
+                d, nn = ns["sdf_ellipsoid"](x_local, scale), ns["sdf_ellipsoid_grad"](x_local, scale)
+            if typ == GEO_PLANE:
+                d, nn = ns["sdf_plane"](x_local, scale[0] * 0.5, scale[1] * 0.5), wp.vec3(0.0, 0.0, 1.0)
+            if d < margin + radius[i]:
+                out["particle"].append(i)
+                out["shape"].append(s)
+                out["body_pos"].append(np.asarray(wp.transform_point(X_ws, x_local - nn * d)))
+                out["body_vel"].append(np.asarray(wp.transform_vector(X_ws, v)))
+                out["normal"].append(np.asarray(wp.transform_vector(X_ws, nn)))
+                out["distance"].append(d)
+    res = {k: np.asarray(v) for k, v in out.items()}
+    res["particle"] = res["particle"].astype(np.int32)
+    res["shape"] = res["shape"].astype(np.int32)
+    res.update(
+        q=q, radius=radius, flags=flags, margin=np.float64(margin),
+        shape_type=np.array([t for t, _, _, _ in shapes], dtype=np.int32),
+        shape_transform=np.array([list(p) + list(r) for _, p, r, _ in shapes], dtype=np.float64),
+        shape_scale=np.array([sc for _, _, _, sc in shapes], dtype=np.float64),
+    )  # fmt: skip
+    return res
+
+
 def soft_cases(ns, seed=13):
     """Per-element goldens of the volumetric Neo-Hookean tetrahedron and of the spring."""
     rng = np.random.default_rng(seed)
@@ -966,6 +1047,8 @@ def main():
     print("selfcontact_elements.npz written")
 
     np.savez_compressed(os.path.join(args.out, "soft_elements.npz"), **soft_cases(ns))
+    np.savez_compressed(os.path.join(args.out, "soft_contact_shapes.npz"), **shape_contact_cases(ns))
+    print("soft_contact_shapes.npz written")
     print("soft_elements.npz written")
 
     # Volumetric: a 3 x 2 x 2-cell tetrahedral block (add_soft_grid, 5 tetrahedra per cell, damped), 4 mm

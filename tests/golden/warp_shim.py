@@ -314,6 +314,31 @@ def transform_vector(X, v):
     return Vec(_quat_rotate(X[1], v.a))
 
 
+def transform_inverse(X):
+    p, q = X
+    qi = np.array([-q[0], -q[1], -q[2], q[3]])
+    return (-_quat_rotate(qi, np.asarray(p, dtype=DTYPE)), qi)
+
+
+def _quat_mul(a, b):
+    ax, ay, az, aw = a
+    bx, by, bz, bw = b
+    return np.array([aw * bx + ax * bw + ay * bz - az * by, aw * by - ax * bz + ay * bw + az * bx,
+                     aw * bz + ax * by - ay * bx + az * bw, aw * bw - ax * bx - ay * by - az * bz])  # fmt: skip
+
+
+def transform_multiply(A, B):
+    return (_quat_rotate(A[1], np.asarray(B[0], dtype=DTYPE)) + A[0], _quat_mul(A[1], B[1]))
+
+
+def cw_mul(a, b):
+    return Vec(a.a * b.a)
+
+
+def cw_div(a, b):
+    return Vec(a.a / b.a)
+
+
 # ---------------------------------------------------------------- arrays and launches
 class Array:
     """A host array of scalars, Vec or Mat values; truthy when non-empty, like a Warp array."""

@@ -70,8 +70,8 @@ def _oracle_trajectory(model, frames, precision):
     for _ in range(frames):
         for _ in range(10):
             qc = q.astype(np.float32).astype(np.float64)  # contacts from float32 positions, as on the GPU
-            cnt, p, s, bp, bv, nn = orc.soft_contacts(qc, r, fl, model.shape_type, model.shape_pos, model.shape_radius,
-                                                      0.01)  # fmt: skip
+            cnt, p, s, bp, bv, nn = orc.soft_contacts_shapes(qc, r, fl, model.shape_type, model.shape_transform,
+                                                             model.shape_scale, 0.01)  # fmt: skip
             c = orc.make_contacts(cnt, p, s, bp, bv, nn)
             _, q, qd = orc.step(om, q, qd, None, c, 1.0 / 600.0, 10, precision=precision, nthreads=orc.max_threads())
         out.append(q.copy())
@@ -250,9 +250,10 @@ def test_soft_contacts_match_oracle():
     torch.cuda.synchronize()
     n = int(c.soft_contact_count.item())
     got = sorted(zip(c.soft_contact_particle.cpu().numpy()[:n].tolist(), c.soft_contact_shape.cpu().numpy()[:n].tolist()))
-    cnt, p, s, bp, bv, nn = orc.soft_contacts(model.particle_q.cpu().numpy(), model.particle_radius.cpu().numpy(),
-                                              model.particle_flags.cpu().numpy(), model.shape_type, model.shape_pos,
-                                              model.shape_radius, 0.01)  # fmt: skip
+    cnt, p, s, bp, bv, nn = orc.soft_contacts_shapes(
+        model.particle_q.cpu().numpy(), model.particle_radius.cpu().numpy(), model.particle_flags.cpu().numpy(),
+        model.shape_type, model.shape_transform, model.shape_scale, 0.01,
+    )  # fmt: skip
     want = sorted(zip(p[:cnt].tolist(), s[:cnt].tolist()))
     assert n == cnt and got == want
 
