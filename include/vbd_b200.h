@@ -329,12 +329,14 @@ int vbd_color_particles(int32_t particle_count, int32_t tri_count, const int32_t
                         const float* edge_bending_properties_host, int32_t include_bending, float target_ratio,
                         int32_t* colors_out);
 
-/* The same greedy coloring and balancing on any particle graph, given as pair_count (a, b) index pairs
-   (duplicates and a == b ignored): the graph of ModelBuilder.color for models with tetrahedra, whose six
-   vertex pairs per active tet (mu * lambda != 0) join the triangle and hinge pairs
-   (construct_tetmesh_graph_edges, graph_coloring.py:53-96). Returns the number of colors or an error. */
-int vbd_color_graph(int32_t particle_count, int32_t pair_count, const int32_t* pairs_host, float target_ratio,
-                    int32_t* colors_out);
+/* Coloring of any particle graph, given as pair_count (a, b) index pairs (duplicates and a == b ignored), e.g.
+   the graph of ModelBuilder.color (construct_particle_graph, graph_coloring.py:200-240: triangle edges, hinge
+   vertex pairs, the six vertex pairs of every active tet). algorithm: 0 = MCS (the maximum cardinality search
+   order, the reference's default ColoringAlgorithm.MCS), 1 = degree-ordered greedy (ColoringAlgorithm.GREEDY);
+   then the balancing pass of vbd_color_particles when target_ratio > 1. Returns the number of colors or an
+   error. */
+int vbd_color_graph(int32_t particle_count, int32_t pair_count, const int32_t* pairs_host, int32_t algorithm,
+                    float target_ratio, int32_t* colors_out);
 
 /* Vertex -> (element, order) adjacency in the reference layout (ParticleForceElementAdjacencyInfo,
    particle_vbd_kernels.py:66-151, fill order :639-738): offsets count two ints per entry. */

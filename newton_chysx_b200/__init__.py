@@ -7,6 +7,7 @@ Public API mirrors the reference names: ``ModelBuilder``, ``Model``, ``State``, 
 
 from .sim import (
     CollisionPipeline,
+    ColoringAlgorithm,
     Contacts,
     Control,
     GeoType,
@@ -28,6 +29,7 @@ class solvers:  # noqa: N801 - mirrors ``newton.solvers``
 
 __all__ = [
     "CollisionPipeline",
+    "ColoringAlgorithm",
     "Contacts",
     "Control",
     "GeoType",

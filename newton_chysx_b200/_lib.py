@@ -116,7 +116,7 @@ SIGNATURES = {
         [C.c_int32, C.c_int32, _ip, _fp, C.c_int32, _ip, _fp, C.c_int32, C.c_float, _ip],
         C.c_int,
     ),
-    "vbd_color_graph": ([C.c_int32, C.c_int32, _ip, C.c_float, _ip], C.c_int),
+    "vbd_color_graph": ([C.c_int32, C.c_int32, _ip, C.c_int32, C.c_float, _ip], C.c_int),
     "vbd_build_adjacency": ([C.c_int32, C.c_int32, _ip, C.c_int32, _ip, _ip, _ip, _ip, _ip], C.c_int),
     "vbd_step_noalloc": (
         [C.POINTER(VbdModelDesc), C.POINTER(VbdRefAdjacency), C.c_int32, C.c_float, _vp, _vp, _vp, _vp, _vp,

@@ -241,36 +241,32 @@ def particle_graph_pairs(tri_indices, tri_materials, edge_indices, edge_props, i
     return np.ascontiguousarray(np.concatenate(parts).astype(np.int32))
 
 
+class ColoringAlgorithm(enum.Enum):
+    """``newton/_src/sim/graph_coloring.py:12-14``."""
+
+    MCS = 0
+    GREEDY = 1
+
+
 def color_particles(n, tri_indices, tri_materials, edge_indices, edge_props, include_bending=False,
-                    balance_colors=True, target_max_min_color_ratio=1.1, tet_indices=None,
-                    tet_materials=None):  # fmt: skip
+                    balance_colors=True, target_max_min_color_ratio=1.1, tet_indices=None, tet_materials=None,
+                    coloring_algorithm=ColoringAlgorithm.MCS):  # fmt: skip
     """Color groups (list of int32 arrays, particles in index order) for VBD's Gauss-Seidel sweep."""
     if n == 0:
         return []
     lib = _lib.load()
-    tri = np.ascontiguousarray(np.asarray(tri_indices, dtype=np.int32).reshape(-1, 3))
-    tm = np.ascontiguousarray(np.asarray(tri_materials, dtype=np.float32).reshape(-1, 5))
-    ed = np.ascontiguousarray(np.asarray(edge_indices, dtype=np.int32).reshape(-1, 4))
-    ep = np.ascontiguousarray(np.asarray(edge_props, dtype=np.float32).reshape(-1, 2))
-    has_tets = tet_indices is not None and len(np.asarray(tet_indices).reshape(-1)) > 0
-    if len(tri) == 0 and (not include_bending or len(ed) == 0) and not has_tets:
+    pairs = particle_graph_pairs(tri_indices, tri_materials, edge_indices, edge_props, include_bending,
+                                 np.zeros((0, 4)) if tet_indices is None else tet_indices,
+                                 np.zeros((0, 3)) if tet_materials is None else tet_materials)  # fmt: skip
+    if len(pairs) == 0:
         return [np.arange(n, dtype=np.int32)]
     colors = np.zeros(n, dtype=np.int32)
     ip = C.POINTER(C.c_int32)
-    fp = C.POINTER(C.c_float)
     ratio = float(target_max_min_color_ratio if balance_colors else 0.0)
-    if has_tets:
-        pairs = particle_graph_pairs(tri, tm, ed, ep, include_bending, tet_indices, tet_materials)
-        if len(pairs) == 0:
-            return [np.arange(n, dtype=np.int32)]
-        ncol = lib.vbd_color_graph(n, len(pairs), pairs.ctypes.data_as(ip), ratio, colors.ctypes.data_as(ip))
-    else:
-        ncol = lib.vbd_color_particles(
-            n, len(tri), tri.ctypes.data_as(ip), tm.ctypes.data_as(fp), len(ed), ed.ctypes.data_as(ip),
-            ep.ctypes.data_as(fp), int(bool(include_bending)), ratio, colors.ctypes.data_as(ip),
-        )  # fmt: skip
+    ncol = lib.vbd_color_graph(n, len(pairs), pairs.ctypes.data_as(ip), ColoringAlgorithm(coloring_algorithm).value,
+                               ratio, colors.ctypes.data_as(ip))  # fmt: skip
     if ncol < 0:
-        _lib.check(ncol, "vbd_color_particles")
+        _lib.check(ncol, "vbd_color_graph")
     order = np.argsort(colors, kind="stable")
     bounds = np.searchsorted(colors[order], np.arange(ncol + 1))
     return [order[bounds[c]:bounds[c + 1]].astype(np.int32) for c in range(ncol)]
@@ -708,10 +704,12 @@ class ModelBuilder:
     def particle_color_groups(self, groups):
         self._color_groups = [_ChunkedGroup([np.asarray(g, dtype=np.int32)], len(g)) for g in groups]
 
-    def color(self, include_bending=False, balance_colors=True, target_max_min_color_ratio=1.1):
+    def color(self, include_bending=False, balance_colors=True, target_max_min_color_ratio=1.1,
+              coloring_algorithm=ColoringAlgorithm.MCS):  # fmt: skip
         self.particle_color_groups = color_particles(
             self._n, self.tri_indices, self.tri_materials, self.edge_indices, self.edge_bending_properties,
             include_bending, balance_colors, target_max_min_color_ratio, self.tet_indices, self.tet_materials,
+            coloring_algorithm,
         )  # fmt: skip
 
     def set_coloring(self, groups):

@@ -28,9 +28,10 @@ def graph_edges(b: sim.ModelBuilder, include_bending: bool):
 
 @pytest.mark.parametrize("n", [2, 5, 16, 33])
 @pytest.mark.parametrize("include_bending", [False, True])
-def test_coloring_is_valid_and_complete(n, include_bending):
+@pytest.mark.parametrize("algorithm", [sim.ColoringAlgorithm.MCS, sim.ColoringAlgorithm.GREEDY])
+def test_coloring_is_valid_and_complete(n, include_bending, algorithm):
     b = cloth_grid_builder(n=n)
-    b.color(include_bending=include_bending)
+    b.color(include_bending=include_bending, coloring_algorithm=algorithm)
     groups = b.particle_color_groups
     colors = -np.ones(b.particle_count, dtype=int)
     for c, g in enumerate(groups):
@@ -70,3 +71,16 @@ def test_world_merge_keeps_each_world_valid():
     for a, c in graph_edges(top, True):
         assert colors[a] != colors[c]
     assert top.world_particle_start == [0, 16, 41]
+
+
+def test_mcs_is_optimal_on_a_chordal_graph():
+    """Maximum cardinality search colors chordal graphs optimally (clique number); a fan of triangles around a
+    hub plus a chain of triangles is chordal with clique number 3."""
+    b = sim.ModelBuilder()
+    k = 9
+    pts = [(0.0, 0.0, 0.0)] + [(np.cos(a), np.sin(a), 0.0) for a in np.linspace(0.0, 1.5 * np.pi, k)]
+    b.add_particles(pts, (0.0, 0.0, 0.0), 1.0)
+    hub = np.zeros(k - 1, dtype=int)
+    b.add_triangles(hub, np.arange(1, k), np.arange(2, k + 1), tri_ke=1.0, tri_ka=1.0)
+    b.color(coloring_algorithm=sim.ColoringAlgorithm.MCS, balance_colors=False)
+    assert len(b.particle_color_groups) == 3

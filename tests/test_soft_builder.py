@@ -88,9 +88,9 @@ def test_color_graph_entry_point():
     ip = C.POINTER(C.c_int32)
     pairs = np.array([[0, 1], [1, 2], [2, 0], [2, 3], [3, 3]], dtype=np.int32)
     colors = np.zeros(4, np.int32)
-    n = lib.vbd_color_graph(4, len(pairs), pairs.ctypes.data_as(ip), 0.0, colors.ctypes.data_as(ip))
+    n = lib.vbd_color_graph(4, len(pairs), pairs.ctypes.data_as(ip), 0, 0.0, colors.ctypes.data_as(ip))
     assert n == 3
     for a, c in pairs:
         assert a == c or colors[a] != colors[c]
     bad = np.array([[0, 9]], dtype=np.int32)
-    assert lib.vbd_color_graph(4, 1, bad.ctypes.data_as(ip), 0.0, colors.ctypes.data_as(ip)) == _lib.VBD_ERR_INVALID_ARGUMENT
+    assert lib.vbd_color_graph(4, 1, bad.ctypes.data_as(ip), 0, 0.0, colors.ctypes.data_as(ip)) == _lib.VBD_ERR_INVALID_ARGUMENT
