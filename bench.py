@@ -126,6 +126,96 @@ def build_batch(seed: int, count: int):
     return top, sides
 
 
+def build_batch_range(seed: int, count: int, lo: int, hi: int):
+    """Instances lo..hi-1 of build_batch(seed, count), with the same materials, pins and placement."""
+    from newton_chysx_b200 import sim
+
+    sides, E, bend, pins = instance_params(seed, count)
+    templates = {int(n): build_instance(int(n), 1.0e4, 1.0e-4, [], 0) for n in np.unique(sides[lo:hi])}
+    top = sim.ModelBuilder(up_axis="Z", gravity=-9.81)
+    for i in range(lo, hi):
+        n = int(sides[i])
+        top.add_world(_instance_from_template(templates[n], n, float(E[i]), float(bend[i]), pins[i], i))
+    top.add_ground_plane()
+    return top
+
+
+def run_e2e(args, rank, dev, dist, states, shape, vi_step, world):
+    """End-to-end rate: host-resident state of the whole batch, per substep H2D of (q, qd), contacts, step and
+    D2H of (q, qd), over --e2e-chunks instance groups pipelined on separate streams."""
+    import torch
+
+    import newton_chysx_b200 as nb
+
+    C = max(1, args.e2e_chunks)
+    bounds = [round(args.instances * c / C) for c in range(C + 1)]
+    hq_all = states[0].particle_q.cpu()
+    hqd_all = states[0].particle_qd.cpu()
+    chunks, v0 = [], 0
+    for c in range(C):
+        model = build_batch_range(rank_seed(args.seed, rank), args.instances, bounds[c], bounds[c + 1]).finalize(dev)
+        model.soft_contact_ke, model.soft_contact_kd, model.soft_contact_mu = 1.0e3, 10.0, 0.5
+        solver = nb.SolverVBD(model, iterations=ITERATIONS, **shape)
+        pipe = nb.CollisionPipeline(model, soft_contact_margin=0.01)
+        contacts = pipe.contacts()
+        s_in, s_out = model.state(), model.state()
+        n = model.particle_count
+        hq = hq_all[v0:v0 + n].clone().pin_memory()
+        hqd = hqd_all[v0:v0 + n].clone().pin_memory()
+        v0 += n
+        stream = torch.cuda.Stream(dev)
+        stream.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(stream):
+            s_in.particle_q.copy_(hq)
+            s_in.particle_qd.copy_(hqd)
+            pipe.collide(s_in, contacts)
+            solver.step(s_in, s_out, None, contacts, DT)  # sizes every buffer before capture
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=stream):
+                pipe.collide(s_in, contacts)
+                solver.step(s_in, s_out, None, contacts, DT)
+        torch.cuda.current_stream(dev).wait_stream(stream)
+        chunks.append(dict(model=model, solver=solver, graph=g, s_in=s_in, s_out=s_out, hq=hq, hqd=hqd,
+                           oq=torch.empty_like(hq).pin_memory(), oqd=torch.empty_like(hqd).pin_memory(),
+                           stream=stream))  # fmt: skip
+    assert v0 == hq_all.shape[0], "the chunks must cover the batch"
+    Ke = max(1, min(args.steps, args.e2e_steps))
+    cur = torch.cuda.current_stream(dev)
+
+    def run(k):
+        # each group's substeps run in order on its own stream; groups are independent until the final join
+        for ch in chunks:
+            ch["stream"].wait_stream(cur)
+        for _ in range(k):
+            for ch in chunks:
+                with torch.cuda.stream(ch["stream"]):
+                    ch["s_in"].particle_q.copy_(ch["hq"], non_blocking=True)
+                    ch["s_in"].particle_qd.copy_(ch["hqd"], non_blocking=True)
+                    ch["graph"].replay()
+                    ch["oq"].copy_(ch["s_out"].particle_q, non_blocking=True)
+                    ch["oqd"].copy_(ch["s_out"].particle_qd, non_blocking=True)
+        for ch in chunks:
+            cur.wait_stream(ch["stream"])
+
+    run(1)  # warm-up
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    run(Ke)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks([e0.elapsed_time(e1)], device=dev)[0]
+    h2d = sum(2 * ch["hq"].numel() * 4 for ch in chunks)
+    d2h = sum(2 * ch["oq"].numel() * 4 for ch in chunks)
+    for ch in chunks:
+        ch["graph"] = None
+    return {"value": world * vi_step * Ke / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "steps": Ke, "chunks": C, "ms_per_step": ms / Ke}  # fmt: skip
+
+
 def max_over_ranks(values, device=None):
     """Element-wise max of per-rank timings (the multi-GPU time is the slowest rank's)."""
     import torch
@@ -288,35 +378,13 @@ def run_ours(args):
     bvi = bytes_per_vertex_iteration(V, T, E, contacts=True)
     achieved = bvi * vi_step / (solve_ms / K * 1e-3) / 1e9
 
-    # end to end through the public API with host buffers: pinned H2D of the step's inputs
-    # (q, qd), contact generation, the step, D2H of the result (q, qd)
+    # end to end through the public API with host buffers: every substep, pinned H2D of the inputs (q, qd),
+    # contact generation, the step and D2H of the result (q, qd). The batch is split into --e2e-chunks groups of
+    # instances, each its own Model and SolverVBD on its own CUDA stream, so that the copies of one group overlap
+    # the solve of another (the copy engines and the SMs work at the same time).
     e2e = None
     if not args.no_e2e:
-        hq = torch.empty((V, 3), dtype=torch.float32, pin_memory=True)
-        hqd = torch.empty((V, 3), dtype=torch.float32, pin_memory=True)
-        hq.copy_(states[0].particle_q)
-        hqd.copy_(states[0].particle_qd)
-        oq = torch.empty_like(hq, pin_memory=True)
-        oqd = torch.empty_like(hqd, pin_memory=True)
-        Ke = max(1, min(K, args.e2e_steps))
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(Ke):
-            states[0].particle_q.copy_(hq, non_blocking=True)
-            states[0].particle_qd.copy_(hqd, non_blocking=True)
-            g_collide[0].replay()
-            g_solve[0].replay()
-            oq.copy_(states[1].particle_q, non_blocking=True)
-            oqd.copy_(states[1].particle_qd, non_blocking=True)
-        e1.record()
-        torch.cuda.synchronize()
-        e2e_ms = max_over_ranks([e0.elapsed_time(e1)], device=dev)[0]
-        e2e = {"value": world * vi_step * Ke / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 2 * hq.numel() * 4,
-               "d2h_bytes_per_step": 2 * oq.numel() * 4, "steps": Ke}  # fmt: skip
-
+        e2e = run_e2e(args, rank, dev, dist, states, shape, vi_step, world)
     traffic, traffic_src = args.traffic, "--traffic (ncu capture)" if args.traffic is not None else None
     if traffic is None and solver.layout in NCU_TRAFFIC_PER_VI:
         per_vi, traffic_src = NCU_TRAFFIC_PER_VI[solver.layout]
@@ -1023,6 +1091,7 @@ def main():
     ap.add_argument("--no-tune", dest="tune", action="store_false", help="use the launch-shape flags, not the autotuner")
     ap.add_argument("--tune-instances", type=int, default=1024)
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-chunks", type=int, default=4, help="instance groups pipelined on separate streams in e2e")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
