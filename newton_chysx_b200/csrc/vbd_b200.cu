@@ -314,6 +314,18 @@ int download(std::vector<T>& h, const T* d, size_t n) {
   return VBD_OK;
 }
 
+// The stencil records carry mu and lambda pre-multiplied by the triangle's area, so the kernels cannot apply
+// the reference's floor of 1e-6 on |lambda + mu| (particle_vbd_kernels.py:919-921) to the material values; it
+// is applied here instead: a model with an active triangle (mu > 0 or lambda > 0) whose |lambda + mu| is
+// below the floor uses the CSR layout.
+bool needs_lnh_floor(const std::vector<float>& mat, int T) {
+  for (int t = 0; t < T; ++t) {
+    const float mu = mat[5 * t], lm = mat[5 * t + 1];
+    if ((mu > 0.f || lm > 0.f) && !(std::fabs(lm + mu) >= 1.0e-6f)) return true;
+  }
+  return false;
+}
+
 // Builds the stencil records (vbd_ell.cuh) for the ranges in h->ranges_host / h->range_verts_host from
 // the caller's model arrays. Runs on the host at creation and on refresh.
 int build_ell(VbdSolver* h) {
@@ -325,6 +337,7 @@ int build_ell(VbdSolver* h) {
       (rc = download(rl, m.edge_rest_length_dev, size_t(h->E))) ||
       (rc = download(bp, m.edge_bending_properties_dev, size_t(2) * h->E)))
     return rc;
+  if (needs_lnh_floor(mat, h->T)) return VBD_ERR_UNSUPPORTED;
   const int R = int(h->ranges_host.size()) - 1;
   h->ell_nf.assign(R, 0);
   h->ell_ne.assign(R, 0);
@@ -461,6 +474,7 @@ int build_ring(VbdSolver* h) {
       (rc = download(rl, m.edge_rest_length_dev, size_t(h->E))) ||
       (rc = download(bp, m.edge_bending_properties_dev, size_t(2) * h->E)))
     return rc;
+  if (needs_lnh_floor(mat, h->T)) return VBD_ERR_UNSUPPORTED;
   // interior hinges with stiffness, by their edge
   auto key = [](int a, int b) { return a < b ? (uint64_t(unsigned(a)) << 32) | unsigned(b) : (uint64_t(unsigned(b)) << 32) | unsigned(a); };
   std::vector<std::pair<uint64_t, int>> emap;
@@ -1727,16 +1741,21 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
   if ((params->layout == VBD_LAYOUT_ELL || params->layout == VBD_LAYOUT_ELL16 || params->layout == VBD_LAYOUT_RING) &&
       h->L != 1)
     return fail(VBD_ERR_INVALID_ARGUMENT);
-  bool any_hinge_damping = false;
+  bool any_hinge_damping = false, lnh_floor = false;
   {
-    std::vector<float> bp;
+    std::vector<float> bp, tm;
     if (h->E && (rc = download(bp, m.edge_bending_properties_dev, size_t(2) * h->E))) return fail(rc);
     for (int e = 0; e < h->E; ++e) any_hinge_damping |= bp[2 * e] > 0.f && bp[2 * e + 1] > 0.f;
+    if (h->T && (rc = download(tm, m.tri_materials_dev, size_t(5) * h->T))) return fail(rc);
+    lnh_floor = needs_lnh_floor(tm, h->T);
   }
+  if (lnh_floor && (params->layout == VBD_LAYOUT_ELL || params->layout == VBD_LAYOUT_ELL16 ||
+                    params->layout == VBD_LAYOUT_RING))
+    return fail(VBD_ERR_UNSUPPORTED);
   const bool ell16_ok = h->schedule == VBD_SCHEDULE_PERSISTENT && h->max_inst_v < 65536 && !any_hinge_damping;
   if ((params->layout == VBD_LAYOUT_ELL16 || params->layout == VBD_LAYOUT_RING) && !ell16_ok)
     return fail(VBD_ERR_UNSUPPORTED);
-  if (params->layout == VBD_LAYOUT_CSR || h->L != 1 || h->soft)
+  if (params->layout == VBD_LAYOUT_CSR || h->L != 1 || h->soft || lnh_floor)
     h->layout = VBD_LAYOUT_CSR;
   else if (params->layout == VBD_LAYOUT_RING)
     h->layout = VBD_LAYOUT_RING;

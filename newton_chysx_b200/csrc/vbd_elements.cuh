@@ -31,10 +31,13 @@ namespace vbd {
 
 // Membrane contribution of one triangle for the vertex of order `ord` (0, 1, 2).
 // pose = D^-1 row-major (00, 01, 10, 11); mat = (mu, lambda, damping, area).
+// lnh_floor: the floor of |lambda + mu| in alpha = 1 + mu / (lambda + mu), 1e-6 for material values (the
+// reference's); 0 when mu and lambda come pre-multiplied by the area (stencil records), whose builder checks
+// the floor on the material values instead.
 template <typename R>
 __host__ __device__ __forceinline__ void membrane_add(int ord, vec3<R> x0, vec3<R> x1, vec3<R> x2, const R pose[4],
                                                       R mu, R lmbd, R damping, R area, R dt, const vec3<R>* xp,
-                                                      vec3<R>& f, sym3<R>& H) {
+                                                      vec3<R>& f, sym3<R>& H, R lnh_floor = R(1.0e-6)) {
   const vec3<R> x01 = x1 - x0, x02 = x2 - x0;
   const R D00 = pose[0], D01 = pose[1], D10 = pose[2], D11 = pose[3];
   const vec3<R> f0 = x01 * D00 + x02 * D10;
@@ -44,7 +47,7 @@ __host__ __device__ __forceinline__ void membrane_add(int ord, vec3<R> x0, vec3<
   const R invJ = vrsqrt(Jsq);
   const R J = Jsq * invJ;
   const R lnh = lmbd + mu;
-  const R lsafe = (lnh < R(0) ? R(-1) : R(1)) * vmax(vabs(lnh), R(1.0e-6));
+  const R lsafe = lnh_floor > R(0) ? (lnh < R(0) ? R(-1) : R(1)) * vmax(vabs(lnh), lnh_floor) : (lnh == R(0) ? R(1) : lnh);
   const R alpha = R(1) + vdiv_fast(mu, lsafe);
   const vec3<R> g0 = invJ * (f11 * f0 - f01 * f1);
   const vec3<R> g1 = invJ * (f00 * f1 - f01 * f0);

@@ -89,7 +89,7 @@ __device__ __forceinline__ void solve_ell(const StepCtx<R>& c, const P& pos, con
         xp[1] = ld3<R>(c.qprev[nb.x]);
         xp[2] = ld3<R>(c.qprev[nb.y]);
       }
-      membrane_add<R>(0, x, pos.ld(nb.x), pos.ld(nb.y), pose, R(mat.x), R(mat.y), R(kd), R(1), c.dt, xp, f, H);
+      membrane_add<R>(0, x, pos.ld(nb.x), pos.ld(nb.y), pose, R(mat.x), R(mat.y), R(kd), R(1), c.dt, xp, f, H, R(0));
     }
   }
   // Hinges, pipelined the same way.
@@ -272,7 +272,7 @@ __device__ __forceinline__ void ell16_face(const StepCtx<R>& c, const P& pos, in
     xp[1] = ld3<R>(c.qprev[ia]);
     xp[2] = ld3<R>(c.qprev[ib]);
   }
-  membrane_add<R>(0, x, pos.ld(ia), pos.ld(ib), pose, R(muA), R(lmA), R(kd), R(1), c.dt, xp, f, H);
+  membrane_add<R>(0, x, pos.ld(ia), pos.ld(ib), pose, R(muA), R(lmA), R(kd), R(1), c.dt, xp, f, H, R(0));
 }
 
 // Bending term of one 16-byte hinge record for the solved vertex at x.

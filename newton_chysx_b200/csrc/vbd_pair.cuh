@@ -102,8 +102,9 @@ __device__ __forceinline__ void pmembrane_add(pv3 x0, pv3 x1, pv3 x2, pf D00, pf
   const pf invJ = prsqrt(Jsq);
   const pf J = Jsq * invJ;
   const pf lnh = lmbd + mu;
-  const pf lsafe = pf2(copysignf(fmaxf(fabsf(lnh.v.x), 1.0e-6f), lnh.v.x < 0.f ? -1.f : 1.f),
-                       copysignf(fmaxf(fabsf(lnh.v.y), 1.0e-6f), lnh.v.y < 0.f ? -1.f : 1.f));
+  // mu and lambda come pre-multiplied by the area: no floor here (membrane_add with lnh_floor = 0); a lane with
+  // mu = lambda = 0 divides by 1 and adds exactly zero
+  const pf lsafe = pf2(lnh.v.x == 0.f ? 1.f : lnh.v.x, lnh.v.y == 0.f ? 1.f : lnh.v.y);
   const pf alpha = pfs(1.f) + pdiv_fast(mu, lsafe);
   const pv3 g0 = pfma(f0, f11, f1 * (-f01)) * invJ;
   const pv3 g1 = pfma(f1, f00, f0 * (-f01)) * invJ;

@@ -96,7 +96,7 @@ __device__ __forceinline__ void solve_ring(const StepCtx<R>& c, const P& pos, co
             xp[1] = ld3<R>(c.qprev[vs + int(A.x & 0xffffu)]);
             xp[2] = ld3<R>(c.qprev[vs + int(An.x & 0xffffu)]);
           }
-          membrane_add<R>(0, zero3<R>(), a_cur, a_next, pose, R(muA), R(lmA), R(kd), R(1), c.dt, xp, f, H);
+          membrane_add<R>(0, zero3<R>(), a_cur, a_next, pose, R(muA), R(lmA), R(kd), R(1), c.dt, xp, f, H, R(0));
         }
         const vec3<R> N = cross(a_cur, a_next);
         const R s1 = dot(N, N);

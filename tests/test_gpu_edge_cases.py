@@ -148,3 +148,43 @@ def test_shape_table_limit():
                                       out_i.data_ptr(), out_i.data_ptr(), out_f.data_ptr(), out_f.data_ptr(),
                                       out_f.data_ptr(), None)  # fmt: skip
     assert rc == _lib.VBD_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("layout,schedule", [("csr", "per_color"), ("ell", "per_color"), ("ell", "persistent"),
+                                             ("ell16", "persistent")])  # fmt: skip
+def test_sliver_triangles_match_oracle(layout, schedule):
+    """Triangles whose rest area is ~1e-6 of nominal (the precision stress sheet at 16 x 16): the stencil records
+    carry mu and lambda times the area, which for slivers falls below the 1e-6 floor the reference applies to
+    |lambda + mu|; the floor must act on the material values, as in the reference. FP64 against the FP64 oracle
+    (1e-7: the slivers make the 3x3 blocks ill-conditioned, which amplifies the order of the sums)."""
+    import bench
+
+    b, sites = bench.build_precision_model(n=16, seed=4, sliver_fraction=0.05)
+    assert len(sites) > 0
+    model = b.finalize("cuda")
+    solver = SolverVBD(model, iterations=5, precision="fp64", schedule=schedule, layout=layout)
+    assert solver.layout == layout
+    om = orc.Model(oracle_model_dict(model))
+    q = model.particle_q.double().cpu().numpy()
+    qd = np.zeros_like(q)
+    for _ in range(3):
+        s0, s1 = _states(model, q, qd, torch.float64)
+        solver.step(s0, s1, None, None, DT)
+        torch.cuda.synchronize()
+        _, q_o, qd_o = orc.step(om, q, qd, None, None, DT, 5, precision=64)
+        assert np.abs(s1.particle_q.cpu().numpy() - q_o).max() <= 1e-7
+        q, qd = q_o, qd_o
+
+
+def test_tiny_material_falls_back_to_csr():
+    """A triangle with 0 < |lambda + mu| < 1e-6 needs the reference's floor on the material values: the stencil
+    layouts refuse the model and the automatic choice takes CSR."""
+    b = cloth_grid_builder(n=8)
+    mats = b.tri_materials
+    mats[3, :2] = (4.0e-7, 1.0e-7)
+    b._tri_mat = [mats]
+    model = b.finalize("cuda")
+    with pytest.raises(_lib.VbdError, match="unsupported"):
+        SolverVBD(model, iterations=2, schedule="persistent", layout="ell16")
+    assert SolverVBD(model, iterations=2, schedule="persistent").layout == "csr"
+    _fp64_vs_oracle(model, 3)
