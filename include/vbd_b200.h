@@ -126,6 +126,10 @@ typedef struct VbdSolverParams {
   int32_t pair_vertices;        /* ELL16 + persistent, FP32: 1 = each thread solves two vertices of a color at
                                    once, one per lane of the paired FP32 instructions (FFMA2/FADD2/FMUL2);
                                    0 = one vertex per thread */
+  int32_t instance_per_warp;    /* persistent schedule, CSR layout, lanes_per_vertex 1..8: 1 = each warp takes
+                                   instances from the work queue on its own (colors separated by __syncwarp, eight
+                                   instances side by side in a CTA of 256; positions in shared memory per warp when
+                                   they fit), for batches of small instances; 0 = one instance per CTA */
 } VbdSolverParams;
 
 typedef struct VbdContactsDesc {

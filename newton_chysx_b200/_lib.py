@@ -64,6 +64,7 @@ class VbdSolverParams(C.Structure):
         ("schedule", C.c_int32), ("lanes_per_vertex", C.c_int32), ("block_size", C.c_int32),
         ("contact_slots", C.c_int32), ("positions_in_shared", C.c_int32), ("layout", C.c_int32),
         ("min_blocks_per_sm", C.c_int32), ("pair_vertices", C.c_int32),
+        ("instance_per_warp", C.c_int32),
     ]  # fmt: skip
 
 

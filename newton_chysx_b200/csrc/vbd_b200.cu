@@ -21,6 +21,7 @@
 #include "vbd_soft.h"
 #include "vbd_ell16_pair.h"
 #include "vbd_shapes.cuh"
+#include "vbd_warp.h"
 
 using namespace vbd;
 
@@ -199,6 +200,8 @@ struct VbdSolver {
   int max_inst_v = 0;
   int occ = 0;  // ELL persistent kernel: compiled occupancy target (CTAs of 256 per SM), 0 = none
   bool pair = false;  // ELL16 persistent kernel, FP32: two vertices per thread in paired FP32 arithmetic
+  bool warp_inst = false;  // persistent CSR kernel: one warp per instance (k_persistent_warp)
+  int slice = 0;           // its shared-memory floats per warp (positions), 0 = positions in global memory
   int K = 1;
   // packed model
   int4* tri_idx = nullptr;
@@ -1213,6 +1216,16 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
       } else {
         launch_persistent_ell<R, MODE, false>(0, c, p, e, h->grid_persistent, h->block, 0, st);
       }
+    } else if (h->warp_inst) {
+      if constexpr (std::is_same<R, float>::value) {
+        if (h->smem_bytes > 0)
+          launch_persistent_warp<R, MODE, true>(h->soft, h->L, c, p, h->slice, h->grid_persistent, h->block,
+                                               h->smem_bytes, st);
+        else
+          launch_persistent_warp<R, MODE, false>(h->soft, h->L, c, p, 0, h->grid_persistent, h->block, 0, st);
+      } else {
+        launch_persistent_warp<R, MODE, false>(h->soft, h->L, c, p, 0, h->grid_persistent, h->block, 0, st);
+      }
     } else if (h->soft) {
       if constexpr (std::is_same<R, float>::value) {
         if (h->smem_bytes > 0)
@@ -1339,6 +1352,14 @@ const void* persistent_kernel(VbdSolver* h) {
       return sm ? persistent_ell_fn<float, MODE_MIXED, true>(h->occ) : persistent_ell_fn<float, MODE_MIXED, false>(h->occ);
     return sm ? persistent_ell_fn<float, MODE_FP32, true>(h->occ) : persistent_ell_fn<float, MODE_FP32, false>(h->occ);
   }
+  if (h->warp_inst) {
+    if (h->precision == VBD_PRECISION_FP64) return persistent_warp_fn<double, MODE_FP64, false>(h->soft, h->L);
+    if (h->precision == VBD_PRECISION_MIXED)
+      return sm ? persistent_warp_fn<float, MODE_MIXED, true>(h->soft, h->L)
+                : persistent_warp_fn<float, MODE_MIXED, false>(h->soft, h->L);
+    return sm ? persistent_warp_fn<float, MODE_FP32, true>(h->soft, h->L)
+              : persistent_warp_fn<float, MODE_FP32, false>(h->soft, h->L);
+  }
   if (h->soft) {
     if (h->precision == VBD_PRECISION_FP64) return persistent_soft_fn<double, MODE_FP64, false>(h->L);
     if (h->precision == VBD_PRECISION_MIXED)
@@ -1360,7 +1381,8 @@ int occupancy_grid(VbdSolver* h) {
   if (dyn > 0) CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, h->block, dyn));
   if (per_sm < 1) return VBD_ERR_INVALID_ARGUMENT;
-  h->grid_persistent = std::min(h->W, sms * per_sm);
+  const int per_cta = h->warp_inst ? h->block / 32 : 1;  // instances a CTA works on at once
+  h->grid_persistent = std::min((h->W + per_cta - 1) / per_cta, sms * per_sm);
   return VBD_OK;
 }
 
@@ -1790,6 +1812,29 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
       h->ranges_host = h->color_offsets;
     }
     if ((rc = h->layout == VBD_LAYOUT_RING ? build_ring(h) : build_ell(h))) return fail(rc);
+  }
+  if (params->instance_per_warp != 0) {
+    // one warp per instance: CSR layout, persistent schedule, lanes per vertex 1..8, whole warps per block
+    if (params->instance_per_warp != 1 || h->schedule != VBD_SCHEDULE_PERSISTENT || h->layout != VBD_LAYOUT_CSR ||
+        (h->L != 1 && h->L != 2 && h->L != 4 && h->L != 8) || h->occ != 0 || params->pair_vertices != 0)
+      return fail(VBD_ERR_INVALID_ARGUMENT);
+    h->warp_inst = true;
+    h->block = params->block_size ? params->block_size : 256;
+    h->smem_bytes = 0;
+    h->slice = 0;
+    if (h->precision != VBD_PRECISION_FP64 && params->positions_in_shared != 1) {
+      int dev = 0, optin = 0;
+      if (cudaGetDevice(&dev) != cudaSuccess ||
+          cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+        return fail(VBD_ERR_CUDA);
+      const size_t need = size_t(h->block / 32) * 12 * size_t(h->max_inst_v);
+      if (need > 0 && need + 64 <= size_t(optin)) {
+        h->smem_bytes = need;
+        h->slice = 3 * h->max_inst_v;
+      } else if (params->positions_in_shared == 2) {
+        return fail(VBD_ERR_UNSUPPORTED);
+      }
+    }
   }
   if (params->pair_vertices != 0) {
     if (params->pair_vertices != 1 || h->layout != VBD_LAYOUT_ELL16 || h->schedule != VBD_SCHEDULE_PERSISTENT ||

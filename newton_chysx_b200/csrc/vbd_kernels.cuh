@@ -622,4 +622,53 @@ __global__ void k_persistent(StepCtx<R> c, PersistentPlan p) {
   }
 }
 
+// One warp per instance (small instances): each warp of the CTA takes instances from the work queue on its own,
+// so a color needs only __syncwarp between its rounds, not a CTA barrier, and eight instances run side by side
+// in a CTA of 256. SMEM: each warp keeps its instance's positions in its own slice of shared memory (slice
+// floats per warp).
+template <typename R, int L, int MODE, bool SMEM, bool SOFT>
+__global__ void k_persistent_warp(StepCtx<R> c, PersistentPlan p, int slice) {
+  extern __shared__ float s_pos[];
+  const int lane = threadIdx.x & 31;
+  float* mine = s_pos + size_t(threadIdx.x >> 5) * size_t(slice);
+  for (;;) {
+    int q = 0;
+    if (lane == 0) q = atomicAdd(p.queue, 1);
+    q = __shfl_sync(0xffffffffu, q, 0);
+    if (q >= p.W) return;
+    const int w = __ldg(p.inst_order + q);
+    const int vs = __ldg(p.inst_vstart + w), ve = __ldg(p.inst_vstart + w + 1);
+    using Pos = typename std::conditional<SMEM, SmemPos, GlobalPos<R>>::type;
+    Pos pos;
+    if constexpr (SMEM) {
+      pos = SmemPos{mine, vs};
+    } else {
+      pos = GlobalPos<R>{c.pos};
+    }
+    for (int i = vs + lane; i < ve; i += 32) forward_particle(c, pos, i);
+    __syncwarp();
+    const int cb = __ldg(p.inst_cptr + w), ce = __ldg(p.inst_cptr + w + 1);
+    constexpr int per_round = 32 / L;
+    const int grp_local = lane / L, sub = lane % L;
+    for (int it = 0; it < p.iterations; ++it) {
+      for (int col = cb; col + 1 < ce; ++col) {
+        const int a = __ldg(p.color_ranges + col), b = __ldg(p.color_ranges + col + 1);
+        if (SOFT && c.n_same_springs) {
+          for (int g = a + lane; g < b; g += 32) spring_prepass_vertex<R>(c, pos, __ldg(p.color_verts + g));
+          __syncwarp();
+        }
+        for (int base = a; base < b; base += per_round) {
+          const int g = base + grp_local;
+          const bool valid = g < b;
+          const int v = valid ? __ldg(p.color_verts + g) : 0;
+          solve_group<R, L, MODE, Pos, false, SOFT>(c, pos, v, valid, sub, it);
+        }
+        __syncwarp();
+      }
+    }
+    for (int i = vs + lane; i < ve; i += 32) finalize_particle(c, pos, i);
+    __syncwarp();
+  }
+}
+
 }  // namespace vbd

@@ -24,6 +24,8 @@ Beyond the reference keywords:
   256 threads per SM (a register budget); 0 leaves the compiler's choice.
 * ``pair_vertices``: the ell16 persistent kernel (FP32) solves two vertices per thread, one in each lane
   of Blackwell's paired FP32 instructions (FFMA2 / FADD2 / FMUL2), halving the arithmetic instructions.
+* ``instance_per_warp``: the persistent csr kernel gives each warp its own instance (colors separated by
+  ``__syncwarp`` instead of a CTA barrier), for batches of small instances such as soft-body blocks.
 
 Particle self-contact (``particle_enable_self_contact=True`` and the ``particle_self_contact_*``
 keywords) runs on the per-color schedule with the csr layout; see ``collision.py`` for the filters and
@@ -98,6 +100,7 @@ class SolverVBD:
         layout: str = "auto",
         min_blocks_per_sm: int = 0,
         pair_vertices: bool = False,
+        instance_per_warp: bool = False,
     ):
         if rigid_avbd_beta < 0:
             raise ValueError(f"rigid_avbd_beta must be >= 0, got {rigid_avbd_beta}")
@@ -218,6 +221,7 @@ class SolverVBD:
         prm.layout = _lib.LAYOUT[layout]
         prm.min_blocks_per_sm = int(min_blocks_per_sm)
         prm.pair_vertices = int(bool(pair_vertices))
+        prm.instance_per_warp = int(bool(instance_per_warp))
         self._prm = prm
 
         h = C.c_void_p()

@@ -190,3 +190,48 @@ def test_soft_step_graph_capture_replays_identically():
     graph.replay()
     torch.cuda.synchronize()
     assert torch.equal(st_out.particle_q, eager)
+
+
+@pytest.mark.parametrize("lanes,shared", [(4, "auto"), (8, "auto"), (8, "off"), (1, "auto")])
+def test_instance_per_warp_matches(lanes, shared):
+    """One warp per instance on the persistent CSR kernel: the golden soft block in FP32 (1e-4) and FP64 (1e-9
+    against the oracle), and a batch of builder blocks against one instance per CTA."""
+    g = load_golden(GOLDEN)
+    model = model_from_golden(g)
+    solver = SolverVBD(model, iterations=int(g["iterations"]), friction_epsilon=float(g["friction_epsilon"]),
+                       schedule="persistent", lanes_per_vertex=lanes, positions_in_shared=shared,
+                       instance_per_warp=True)  # fmt: skip
+    for s in range(int(g["substeps"])):
+        _, st_out = _substep(solver, g, s)
+        assert np.abs(st_out.particle_q.cpu().numpy() - g[f"s{s}_q_out"]).max() <= 1e-4
+    solver64 = SolverVBD(model, iterations=int(g["iterations"]), friction_epsilon=float(g["friction_epsilon"]),
+                         precision="fp64", schedule="persistent", lanes_per_vertex=lanes, instance_per_warp=True)  # fmt: skip
+    om = orc.Model(oracle_model_dict(model, float(g["friction_epsilon"]), float(g["beta"])))
+    _, st_out = _substep(solver64, g, 0, torch.float64)
+    q_o, _ = _oracle_step(om, g, 0, g["s0_q_in"], g["s0_qd_in"], g["s0_f_ext"])
+    assert np.abs(st_out.particle_q.cpu().numpy() - q_o).max() <= 1e-9
+    inner = soft_block_builder()
+    inner.color()
+    b = sim.ModelBuilder()
+    for _ in range(20):
+        b.add_world(inner)
+    bm = b.finalize("cuda")
+    runs = []
+    for warp in (True, False):
+        sv = SolverVBD(bm, iterations=5, schedule="persistent", lanes_per_vertex=lanes, positions_in_shared=shared,
+                       instance_per_warp=warp)  # fmt: skip
+        s0, s1 = bm.state(), bm.state()
+        for _ in range(3):
+            sv.step(s0, s1, None, None, 1.0 / 600.0)
+            s0, s1 = s1, s0
+        torch.cuda.synchronize()
+        runs.append(s0.particle_q.clone())
+    assert (runs[0] - runs[1]).abs().max().item() <= 1e-6
+
+
+def test_instance_per_warp_needs_csr_persistent():
+    g = load_golden(GOLDEN)
+    model = model_from_golden(g)
+    for kw in (dict(schedule="per_color"), dict(schedule="persistent", lanes_per_vertex=16)):
+        with pytest.raises(_lib.VbdError, match="invalid argument"):
+            SolverVBD(model, iterations=2, instance_per_warp=True, **kw)
