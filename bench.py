@@ -746,7 +746,8 @@ def run_soft(args):
     t0 = time.perf_counter()
     m = build_soft_model(dev, W)
     build_s = time.perf_counter() - t0
-    solver = nb.SolverVBD(m, iterations=ITERATIONS, schedule="persistent", lanes_per_vertex=args.lanes)
+    solver = nb.SolverVBD(m, iterations=ITERATIONS, schedule="persistent", lanes_per_vertex=args.lanes,
+                          instance_per_warp=args.warp)  # fmt: skip
     pipe = nb.CollisionPipeline(m, soft_contact_margin=0.01)
     contacts = pipe.contacts()
     s0, s1 = m.state(), m.state()
@@ -793,6 +794,7 @@ def run_soft(args):
         "config": {"workload": f"{W} tetrahedral blocks 8x4x4 cells hung by springs over a ground plane",
                    "vertices": V, "tets": T, "springs": S, "iterations": ITERATIONS, "dt": DT,
                    "schedule": solver.schedule, "lanes_per_vertex": solver.lanes_per_vertex,
+                   "instance_per_warp": bool(args.warp), "shared_bytes": solver.shared_bytes,
                    "build_s": round(build_s, 1),
                    "timed": "ground contact generation + step, one CUDA graph per two substeps",
                    "l2": "per-instance working set stays on chip for its iterations; DRAM sees it once per substep"},
@@ -1088,6 +1090,7 @@ def main():
     ap.add_argument("--layout", choices=["auto", "ring", "ell16", "ell", "csr"], default="auto")
     ap.add_argument("--occ", type=int, default=0, help="resident 256-thread CTAs per SM the kernel is compiled for")
     ap.add_argument("--pair", action="store_true", help="ell16: two vertices per thread in paired FP32 instructions")
+    ap.add_argument("--warp", action="store_true", help="soft workload: one warp per instance")
     ap.add_argument("--no-tune", dest="tune", action="store_false", help="use the launch-shape flags, not the autotuner")
     ap.add_argument("--tune-instances", type=int, default=1024)
     ap.add_argument("--e2e-steps", type=int, default=5)

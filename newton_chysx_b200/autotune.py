@@ -8,7 +8,8 @@ changes the speed of the sweep on a B200:
   ids, one lane per vertex) or ``csr`` (adjacency + element records) with 1, 2 or 4 lanes per vertex;
 * the persistent kernel's register budget (``min_blocks_per_sm``: 2, 3, 4 CTAs of 256 threads per SM,
   or the compiler's choice), whether an instance's positions live in shared memory, and whether the ell16
-  kernel pairs two vertices per thread in paired FP32 instructions (``pair_vertices``);
+  kernel pairs two vertices per thread in paired FP32 instructions (``pair_vertices``), and whether the csr
+  kernel gives each warp its own instance (``instance_per_warp``);
 * the block size of the per-color schedule.
 
 Each candidate is a separate solver on the same model; results do not depend on the choice beyond
@@ -37,6 +38,8 @@ def candidates(model: Model, schedule: str):
             out.append(dict(layout=layout, lanes_per_vertex=1, positions_in_shared="on"))
         for lanes, shared in itertools.product((1, 2, 4), ("off", "on")):
             out.append(dict(layout="csr", lanes_per_vertex=lanes, positions_in_shared=shared))
+        for lanes in (2, 4, 8):
+            out.append(dict(layout="csr", lanes_per_vertex=lanes, instance_per_warp=True))
         return out
     out = []
     for block in (64, 128, 256):
