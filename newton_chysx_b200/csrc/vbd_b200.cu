@@ -438,13 +438,10 @@ int build_ell(VbdSolver* h) {
         for (long long j = 0; j < n; ++j) {
           const long long i = h->ell_ebase[r] + s * n + j;
           const int4 id = hidx[i];
-          const int role = int(unsigned(id.w) >> 30);
-          const int ids[4] = {id.x, id.y, id.z, id.w & 0x3fffffff};
-          unsigned o[3] = {0u, 0u, 0u};
-          for (int q = 0, k = 0; q < 4; ++q)
-            if (q != role) o[k++] = unsigned(ids[q] - vs);
+          const unsigned o[4] = {unsigned(id.x - vs), unsigned(id.y - vs), unsigned(id.z - vs),
+                                 unsigned((id.w & 0x3fffffff) - vs)};
           const bool live = hprop[i].y > 0.f;
-          hr[i] = make_uint4(live ? (o[0] | (o[1] << 16)) : 0u, live ? (o[2] | (unsigned(role) << 16)) : 0u,
+          hr[i] = make_uint4(live ? (o[0] | (o[1] << 16)) : 0u, live ? (o[2] | (o[3] << 16)) : 0u,
                              __float_as_uint_host(hprop[i].x), __float_as_uint_host(hprop[i].y));
         }
     }

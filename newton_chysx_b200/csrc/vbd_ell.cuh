@@ -236,10 +236,10 @@ namespace vbd {
 // vertex ids are 16-bit offsets from the instance's first particle, so that
 //   face  = 32 bytes in two 16-byte halves (two arrays, each read fully coalesced):
 //           A = (a | b << 16, mu A, lambda A, D'00)      B = (D'01, D'10, D'11, damping)
-//   hinge = 16 bytes: (i0 | i1 << 16, i2 | role << 16, rest angle, ke * rest length)
-//           where i0, i1, i2 are the hinge's other three vertices in (o0, o1, v0, v1) order and role
-//           (0..3) is the solved vertex's place among the four. Hinge damping is not stored: models
-//           with non-zero hinge damping use the 32-bit stencil layout.
+//   hinge = 16 bytes: (o0 | o1 << 16, v0 | v1 << 16, rest angle, ke * rest length)
+//           the hinge's four vertices in their (o0, o1, v0, v1) order; the solved vertex's role is the
+//           place of its own id among them. Hinge damping is not stored: models with non-zero hinge
+//           damping use the 32-bit stencil layout.
 // Stencil records are read once per sweep and never again before the next iteration: ask L2 for the
 // records a few slots ahead (no registers held), and load them with the streaming hint so that they do
 // not push the vertex positions out of L1.
@@ -275,21 +275,20 @@ __device__ __forceinline__ void ell16_face(const StepCtx<R>& c, const P& pos, in
   membrane_add<R>(0, x, pos.ld(ia), pos.ld(ib), pose, R(muA), R(lmA), R(kd), R(1), c.dt, xp, f, H, R(0));
 }
 
-// Bending term of one 16-byte hinge record for the solved vertex at x.
+// Bending term of one 16-byte hinge record for the solved vertex (instance-local id lv): the record lists the
+// hinge's four vertices in their (o0, o1, v0, v1) order, so the solved vertex's role is where lv appears and all
+// four positions are gathered (the solved vertex's own gather reads its current position).
 template <typename R, typename P>
-__device__ __forceinline__ void ell16_hinge(const P& pos, int vs, vec3<R> x, uint4 hh, R dt, vec3<R>& f, sym3<R>& H) {
+__device__ __forceinline__ void ell16_hinge(const P& pos, int vs, int lv, uint4 hh, R dt, vec3<R>& f, sym3<R>& H) {
   const float k = __uint_as_float(hh.w);
   if (!(k > 0.f)) return;
-  const int role = int((hh.y >> 16) & 3u);
-  const vec3<R> o0 = pos.ld(vs + int(hh.x & 0xffffu));
-  const vec3<R> o1 = pos.ld(vs + int(hh.x >> 16));
-  const vec3<R> o2 = pos.ld(vs + int(hh.y & 0xffffu));
-  // put the solved vertex back at its place among the four
+  const int i0 = int(hh.x & 0xffffu), i1 = int(hh.x >> 16), i2 = int(hh.y & 0xffffu), i3 = int(hh.y >> 16);
+  const int role = i0 == lv ? 0 : (i1 == lv ? 1 : (i2 == lv ? 2 : 3));
   vec3<R> xs[4];
-  xs[0] = role == 0 ? x : o0;
-  xs[1] = role == 0 ? o0 : (role == 1 ? x : o1);
-  xs[2] = role <= 1 ? o1 : (role == 2 ? x : o2);
-  xs[3] = role == 3 ? x : o2;
+  xs[0] = pos.ld(vs + i0);
+  xs[1] = pos.ld(vs + i1);
+  xs[2] = pos.ld(vs + i2);
+  xs[3] = pos.ld(vs + i3);
   bending_add<R>(role, xs, R(__uint_as_float(hh.z)), R(1), R(k), R(0), dt, nullptr, f, H);
 }
 
@@ -344,7 +343,7 @@ __device__ __forceinline__ void solve_ell16(const StepCtx<R>& c, const P& pos, c
           ph += n;
           h_n = __ldcs(ph);
         }
-        ell16_hinge<R>(pos, vs, x, hh, c.dt, f, H);
+        ell16_hinge<R>(pos, vs, v - vs, hh, c.dt, f, H);
       }
     }
   }
@@ -471,25 +470,13 @@ __device__ __forceinline__ void solve_ell16_pair(const StepCtx<float>& c, const 
       if (!on0 && !on1) continue;
       if (!on0) k0 = 0.f;
       if (!on1) k1 = 0.f;
-      const int role0 = int((h0.y >> 16) & 3u), role1 = int((h1.y >> 16) & 3u);
-      vec3<float> a[4], b[4];
-      {
-        const vec3<float> o0 = pos.ld(vs + int(h0.x & 0xffffu)), o1 = pos.ld(vs + int(h0.x >> 16)),
-                          o2 = pos.ld(vs + int(h0.y & 0xffffu));
-        a[0] = role0 == 0 ? xs0 : o0;
-        a[1] = role0 == 0 ? o0 : (role0 == 1 ? xs0 : o1);
-        a[2] = role0 <= 1 ? o1 : (role0 == 2 ? xs0 : o2);
-        a[3] = role0 == 3 ? xs0 : o2;
-      }
-      {
-        const vec3<float> o0 = pos.ld(vs + int(h1.x & 0xffffu)), o1 = pos.ld(vs + int(h1.x >> 16)),
-                          o2 = pos.ld(vs + int(h1.y & 0xffffu));
-        b[0] = role1 == 0 ? xs1 : o0;
-        b[1] = role1 == 0 ? o0 : (role1 == 1 ? xs1 : o1);
-        b[2] = role1 <= 1 ? o1 : (role1 == 2 ? xs1 : o2);
-        b[3] = role1 == 3 ? xs1 : o2;
-      }
-      const pv3 xh[4] = {pv3_of(a[0], b[0]), pv3_of(a[1], b[1]), pv3_of(a[2], b[2]), pv3_of(a[3], b[3])};
+      const int lv0 = v0 - vs, lv1 = v1 - vs;
+      const int a0 = int(h0.x & 0xffffu), a1 = int(h0.x >> 16), a2 = int(h0.y & 0xffffu), a3 = int(h0.y >> 16);
+      const int b0 = int(h1.x & 0xffffu), b1 = int(h1.x >> 16), b2 = int(h1.y & 0xffffu), b3 = int(h1.y >> 16);
+      const int role0 = a0 == lv0 ? 0 : (a1 == lv0 ? 1 : (a2 == lv0 ? 2 : 3));
+      const int role1 = b0 == lv1 ? 0 : (b1 == lv1 ? 1 : (b2 == lv1 ? 2 : 3));
+      const pv3 xh[4] = {pv3_of(pos.ld(vs + a0), pos.ld(vs + b0)), pv3_of(pos.ld(vs + a1), pos.ld(vs + b1)),
+                         pv3_of(pos.ld(vs + a2), pos.ld(vs + b2)), pv3_of(pos.ld(vs + a3), pos.ld(vs + b3))};
       pbending_add(xh, pf2(__uint_as_float(h0.z), __uint_as_float(h1.z)), pf2(k0, k1), role0, role1, f, H);
     }
   }
