@@ -26,6 +26,12 @@
 
 namespace vbd {
 
+// Stencil records are read once per sweep and never again before the next iteration: ask L2 for the
+// records a few slots ahead (no registers held), and load them with the streaming hint so that they do
+// not push the vertex positions out of L1.
+constexpr int kRecordPrefetch = 3;
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 struct EllView {
   const int* range_nf;    // [ranges] face slots of the range
   const int* range_ne;    // [ranges] hinge slots
@@ -58,6 +64,11 @@ __device__ __forceinline__ void solve_ell(const StepCtx<R>& c, const P& pos, con
     const float2* pm = e.face_mat + b0;
     const int2* pn = e.face_nb + b0;
     const float4* pd = e.face_dm + b0;
+    for (int q = 1; q < kRecordPrefetch && q < nf; ++q) {
+      prefetch_l2(pm + (long long)q * n);
+      prefetch_l2(pn + (long long)q * n);
+      prefetch_l2(pd + (long long)q * n);
+    }
     const float* pk = e.face_kd ? e.face_kd + b0 : nullptr;
     float2 mat_n = make_float2(0.f, 0.f);
     int2 nb_n = make_int2(0, 0);
@@ -72,6 +83,11 @@ __device__ __forceinline__ void solve_ell(const StepCtx<R>& c, const P& pos, con
       const int2 nb = nb_n;
       const float4 dm = dm_n;
       const float kd = pk ? __ldg(pk) : 0.f;
+      if (s + kRecordPrefetch < nf) {
+        prefetch_l2(pm + (long long)kRecordPrefetch * n);
+        prefetch_l2(pn + (long long)kRecordPrefetch * n);
+        prefetch_l2(pd + (long long)kRecordPrefetch * n);
+      }
       if (s + 1 < nf) {
         pm += n;
         pn += n;
@@ -98,6 +114,10 @@ __device__ __forceinline__ void solve_ell(const StepCtx<R>& c, const P& pos, con
     const float2* pp = e.hinge_prop + b0;
     const int4* pi = e.hinge_idx + b0;
     const float* pk = e.hinge_kd ? e.hinge_kd + b0 : nullptr;
+    for (int q = 1; q < kRecordPrefetch && q < ne; ++q) {
+      prefetch_l2(pp + (long long)q * n);
+      prefetch_l2(pi + (long long)q * n);
+    }
     float2 pr_n = make_float2(0.f, 0.f);
     int4 id_n = make_int4(0, 0, 0, 0);
     if (ne > 0) {
@@ -108,6 +128,10 @@ __device__ __forceinline__ void solve_ell(const StepCtx<R>& c, const P& pos, con
       const float2 pr = pr_n;
       const int4 id = id_n;
       const float kd = pk ? __ldg(pk) : 0.f;
+      if (s + kRecordPrefetch < ne) {
+        prefetch_l2(pp + (long long)kRecordPrefetch * n);
+        prefetch_l2(pi + (long long)kRecordPrefetch * n);
+      }
       if (s + 1 < ne) {
         pp += n;
         pi += n;
@@ -240,11 +264,7 @@ namespace vbd {
 //           the hinge's four vertices in their (o0, o1, v0, v1) order; the solved vertex's role is the
 //           place of its own id among them. Hinge damping is not stored: models with non-zero hinge
 //           damping use the 32-bit stencil layout.
-// Stencil records are read once per sweep and never again before the next iteration: ask L2 for the
-// records a few slots ahead (no registers held), and load them with the streaming hint so that they do
-// not push the vertex positions out of L1.
-constexpr int kRecordPrefetch = 3;
-__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 
 struct Ell16View {
   const int* range_nf;
