@@ -285,12 +285,12 @@ __device__ __forceinline__ void ell16_face(const StepCtx<R>& c, const P& pos, in
   const R pose[4] = {R(__uint_as_float(A.w)), R(__uint_as_float(B.x)), R(__uint_as_float(B.y)),
                      R(__uint_as_float(B.z))};
   const float kd = __uint_as_float(B.w);
-  const int ia = int(A.x & 0xffffu), ib = int(A.x >> 16);  // instance-local ids (pos is the instance's view)
+  const int ia = vs + int(A.x & 0xffffu), ib = vs + int(A.x >> 16);
   vec3<R> xp[3];
   if (kd > 0.f) {
     xp[0] = ld3<R>(c.qprev[v]);
-    xp[1] = ld3<R>(c.qprev[vs + ia]);
-    xp[2] = ld3<R>(c.qprev[vs + ib]);
+    xp[1] = ld3<R>(c.qprev[ia]);
+    xp[2] = ld3<R>(c.qprev[ib]);
   }
   membrane_add<R>(0, x, pos.ld(ia), pos.ld(ib), pose, R(muA), R(lmA), R(kd), R(1), c.dt, xp, f, H, R(0));
 }
@@ -305,10 +305,10 @@ __device__ __forceinline__ void ell16_hinge(const P& pos, int vs, int lv, uint4 
   const int i0 = int(hh.x & 0xffffu), i1 = int(hh.x >> 16), i2 = int(hh.y & 0xffffu), i3 = int(hh.y >> 16);
   const int role = i0 == lv ? 0 : (i1 == lv ? 1 : (i2 == lv ? 2 : 3));
   vec3<R> xs[4];
-  xs[0] = pos.ld(i0);
-  xs[1] = pos.ld(i1);
-  xs[2] = pos.ld(i2);
-  xs[3] = pos.ld(i3);
+  xs[0] = pos.ld(vs + i0);
+  xs[1] = pos.ld(vs + i1);
+  xs[2] = pos.ld(vs + i2);
+  xs[3] = pos.ld(vs + i3);
   bending_add<R>(role, xs, R(__uint_as_float(hh.z)), R(1), R(k), R(0), dt, nullptr, f, H);
 }
 
@@ -318,7 +318,7 @@ __device__ __forceinline__ void solve_ell16(const StepCtx<R>& c, const P& pos, c
   const pos4_t<R> in4 = c.inertia[v];
   const R m = R(in4.w);
   if (m == R(0)) return;
-  const vec3<R> x = pos.ld(v - vs);
+  const vec3<R> x = pos.ld(v);
   vec3<R> f = zero3<R>();
   sym3<R> H = szero<R>();
   const int nf = __ldg(e.range_nf + r), ne = __ldg(e.range_ne + r);
@@ -410,7 +410,7 @@ __device__ __forceinline__ void solve_ell16(const StepCtx<R>& c, const P& pos, c
     set_err(c.err, 1);
     return;
   }
-  pos.st(v - vs, xn);
+  pos.st(v, xn);
 }
 
 // Two vertices of one color range (records j0 and j1, particles v0 and v1) solved together, one per lane of
@@ -423,7 +423,7 @@ __device__ __forceinline__ void solve_ell16_pair(const StepCtx<float>& c, const 
   const float4 in0 = c.inertia[v0], in1 = c.inertia[v1];
   const bool act0 = in0.w != 0.f, act1 = has1 && in1.w != 0.f;
   if (!act0 && !act1) return;
-  const vec3<float> xs0 = pos.ld(v0 - vs), xs1 = pos.ld(v1 - vs);
+  const vec3<float> xs0 = pos.ld(v0), xs1 = pos.ld(v1);
   const pv3 x = pv3_of(xs0, xs1);
   pv3 f = {pfs(0.f), pfs(0.f), pfs(0.f)};
   psym H = {pfs(0.f), pfs(0.f), pfs(0.f), pfs(0.f), pfs(0.f), pfs(0.f)};
@@ -466,8 +466,8 @@ __device__ __forceinline__ void solve_ell16_pair(const StepCtx<float>& c, const 
       if (!on0 && !on1) continue;
       if (!on0) mu0 = lm0 = 0.f;  // an inactive face in one lane adds exactly zero
       if (!on1) mu1 = lm1 = 0.f;
-      const pv3 xa = pv3_of(pos.ld(int(A0.x & 0xffffu)), pos.ld(int(A1.x & 0xffffu)));
-      const pv3 xb = pv3_of(pos.ld(int(A0.x >> 16)), pos.ld(int(A1.x >> 16)));
+      const pv3 xa = pv3_of(pos.ld(vs + int(A0.x & 0xffffu)), pos.ld(vs + int(A1.x & 0xffffu)));
+      const pv3 xb = pv3_of(pos.ld(vs + int(A0.x >> 16)), pos.ld(vs + int(A1.x >> 16)));
       pmembrane_add(x, xa, xb, pf2(__uint_as_float(A0.w), __uint_as_float(A1.w)),
                     pf2(__uint_as_float(B0.x), __uint_as_float(B1.x)), pf2(__uint_as_float(B0.y), __uint_as_float(B1.y)),
                     pf2(__uint_as_float(B0.z), __uint_as_float(B1.z)), pf2(mu0, mu1), pf2(lm0, lm1), f, H);
@@ -495,8 +495,8 @@ __device__ __forceinline__ void solve_ell16_pair(const StepCtx<float>& c, const 
       const int b0 = int(h1.x & 0xffffu), b1 = int(h1.x >> 16), b2 = int(h1.y & 0xffffu), b3 = int(h1.y >> 16);
       const int role0 = a0 == lv0 ? 0 : (a1 == lv0 ? 1 : (a2 == lv0 ? 2 : 3));
       const int role1 = b0 == lv1 ? 0 : (b1 == lv1 ? 1 : (b2 == lv1 ? 2 : 3));
-      const pv3 xh[4] = {pv3_of(pos.ld(a0), pos.ld(b0)), pv3_of(pos.ld(a1), pos.ld(b1)), pv3_of(pos.ld(a2), pos.ld(b2)),
-                         pv3_of(pos.ld(a3), pos.ld(b3))};
+      const pv3 xh[4] = {pv3_of(pos.ld(vs + a0), pos.ld(vs + b0)), pv3_of(pos.ld(vs + a1), pos.ld(vs + b1)),
+                         pv3_of(pos.ld(vs + a2), pos.ld(vs + b2)), pv3_of(pos.ld(vs + a3), pos.ld(vs + b3))};
       pbending_add(xh, pf2(__uint_as_float(h0.z), __uint_as_float(h1.z)), pf2(k0, k1), role0, role1, f, H);
     }
   }
@@ -529,13 +529,13 @@ __device__ __forceinline__ void solve_ell16_pair(const StepCtx<float>& c, const 
     if (!isfinite(d0)) set_err(c.err, 1);
     else if (!(fabsf(d0) > 1e-8f)) set_err(c.err, 4);
     else if (!(isfinite(xn0.x) && isfinite(xn0.y) && isfinite(xn0.z))) set_err(c.err, 1);
-    else pos.st(v0 - vs, xn0);
+    else pos.st(v0, xn0);
   }
   if (act1) {
     if (!isfinite(d1)) set_err(c.err, 1);
     else if (!(fabsf(d1) > 1e-8f)) set_err(c.err, 4);
     else if (!(isfinite(xn1.x) && isfinite(xn1.y) && isfinite(xn1.z))) set_err(c.err, 1);
-    else pos.st(v1 - vs, xn1);
+    else pos.st(v1, xn1);
   }
 }
 
@@ -555,13 +555,11 @@ __global__ void __launch_bounds__(OCC ? 256 : 512, OCC ? OCC : 1) k_persistent_e
     const int w = __ldg(p.inst_order + q);
     const int vs = __ldg(p.inst_vstart + w), ve = __ldg(p.inst_vstart + w + 1);
     using Pos = typename std::conditional<SMEM, SmemPos, GlobalPos<R>>::type;
-    Pos pos, lpos;  // indexed by particle id / by instance-local id (the sweep's view)
+    Pos pos;
     if constexpr (SMEM) {
       pos = SmemPos{s_pos, vs};
-      lpos = SmemPos{s_pos, 0};
     } else {
       pos = GlobalPos<R>{c.pos};
-      lpos = GlobalPos<R>{c.pos + vs};
     }
     for (int i = vs + threadIdx.x; i < ve; i += blockDim.x) forward_particle(c, pos, i);
     __syncthreads();
@@ -576,11 +574,11 @@ __global__ void __launch_bounds__(OCC ? 256 : 512, OCC ? OCC : 1) k_persistent_e
             const bool has1 = j + bd < b - a;
             const int v0 = __ldg(p.color_verts + a + j);
             const int v1 = has1 ? __ldg(p.color_verts + a + j + bd) : v0;
-            solve_ell16_pair(c, lpos, e, r, b - a, j, has1 ? j + bd : j, v0, v1, has1, vs);
+            solve_ell16_pair(c, pos, e, r, b - a, j, has1 ? j + bd : j, v0, v1, has1, vs);
           }
         } else {
           for (int j = threadIdx.x; j < b - a; j += blockDim.x)
-            solve_ell16<R, MODE>(c, lpos, e, r, b - a, j, __ldg(p.color_verts + a + j), vs, it);
+            solve_ell16<R, MODE>(c, pos, e, r, b - a, j, __ldg(p.color_verts + a + j), vs, it);
         }
         __syncthreads();
       }
