@@ -66,3 +66,62 @@ def test_soft_block_step(golden_dir, precision, tol):
         _, q_out, qd_out = orc.step(model, g[f"s{s}_q_in"], g[f"s{s}_qd_in"], g[f"s{s}_f_ext"], c, float(g["dt"]),
                                     int(g["iterations"]), precision)  # fmt: skip
         assert np.abs(q_out - g[f"s{s}_q_out"]).max() <= tol, (s, np.abs(q_out - g[f"s{s}_q_out"]).max())
+
+
+def _nh_energy(x, Dinv, mu, lam):
+    """Stable Neo-Hookean energy of one tetrahedron with the reference's Lame shift (lambda_nh = lambda + mu,
+    alpha = 1 + mu / lambda_nh): V (mu / 2 (tr F^T F - 3) + lambda_nh / 2 (det F - alpha)^2), whose gradient is
+    the first Piola stress mu F + lambda_nh (det F - alpha) cof F that the element code assembles."""
+    D = Dinv.reshape(3, 3)
+    V = 1.0 / (np.linalg.det(D) * 6.0)
+    F = np.stack([x[1] - x[0], x[2] - x[0], x[3] - x[0]], axis=1) @ D
+    lnh = lam + mu
+    alpha = 1.0 + mu / lnh
+    return V * (0.5 * mu * (np.sum(F * F) - 3.0) + 0.5 * lnh * (np.linalg.det(F) - alpha) ** 2)
+
+
+def test_tetrahedron_force_is_the_energy_gradient():
+    """The finite-difference pattern of the reference's test_tet_energy (test_softbody.py:378-470): the force on
+    each vertex equals minus the derivative of the element energy (central differences, FP64), and the vertex
+    Hessian block is symmetric positive semi-definite."""
+    rng = np.random.default_rng(42)
+    for _ in range(30):
+        rest = rng.standard_normal((4, 3))
+        if np.linalg.det((rest[1:] - rest[0]).T) < 0:
+            rest[[0, 1]] = rest[[1, 0]]
+        Dinv = np.linalg.inv((rest[1:] - rest[0]).T)
+        mu, lam = abs(rng.standard_normal()) + 0.1, abs(rng.standard_normal()) + 0.1
+        x = rest + 0.3 * rng.standard_normal((4, 3))
+        for order in range(4):
+            f, H = orc.tet_element(64, order, x.reshape(-1), x.reshape(-1), Dinv.reshape(-1), mu, lam, 0.0, 1e-3)
+            g = np.zeros(3)
+            h = 1e-6
+            for k in range(3):
+                xp, xm = x.copy(), x.copy()
+                xp[order, k] += h
+                xm[order, k] -= h
+                g[k] = (_nh_energy(xp, Dinv, mu, lam) - _nh_energy(xm, Dinv, mu, lam)) / (2 * h)
+            assert np.abs(f + g).max() <= 1e-6 * max(1.0, np.abs(g).max())
+            H = np.asarray(H).reshape(3, 3)
+            assert np.abs(H - H.T).max() <= 1e-12 * max(1.0, np.abs(H).max())
+            assert np.linalg.eigvalsh(0.5 * (H + H.T)).min() >= -1e-9 * max(1.0, np.abs(H).max())
+
+
+def test_spring_force_is_the_energy_gradient():
+    rng = np.random.default_rng(7)
+    for _ in range(30):
+        x = rng.standard_normal((2, 3))
+        rest, ke = abs(rng.standard_normal()) + 0.1, abs(rng.standard_normal()) * 100.0 + 1.0
+        f0, f1, _ = orc.spring_element(64, x.reshape(-1), x.reshape(-1), rest, ke, 0.0, 1e-3)
+
+        def energy(y):
+            return 0.5 * ke * (np.linalg.norm(y[0] - y[1]) - rest) ** 2
+
+        for end, f in ((0, f0), (1, f1)):
+            g = np.zeros(3)
+            for k in range(3):
+                yp, ym = x.copy(), x.copy()
+                yp[end, k] += 1e-6
+                ym[end, k] -= 1e-6
+                g[k] = (energy(yp) - energy(ym)) / 2e-6
+            assert np.abs(np.asarray(f) + g).max() <= 1e-6 * max(1.0, np.abs(g).max())
