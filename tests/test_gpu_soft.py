@@ -235,3 +235,29 @@ def test_instance_per_warp_needs_csr_persistent():
     for kw in (dict(schedule="per_color"), dict(schedule="persistent", lanes_per_vertex=16)):
         with pytest.raises(_lib.VbdError, match="invalid argument"):
             SolverVBD(model, iterations=2, instance_per_warp=True, **kw)
+
+
+def test_damped_soft_block_falls_freely():
+    """The pattern of test_cloth.py:1026-1076 for volumetric elements: a tetrahedral block with tet damping and a
+    damped spring between two of its corners, released at rest, falls as free particles (elastic and damping
+    forces stay zero under a uniform translation)."""
+    b = sim.ModelBuilder(up_axis="Z", gravity=-9.81)
+    b.add_soft_grid(pos=(0.0, 0.0, 2.0), rot=sim.quat_identity(), vel=(0.0, 0.0, 0.0), dim_x=3, dim_y=2, dim_z=2,
+                    cell_x=0.05, cell_y=0.05, cell_z=0.05, density=500.0, k_mu=2.0e4, k_lambda=3.0e4, k_damp=1.0e-2,
+                    tri_ke=10.0, tri_ka=10.0, tri_kd=1e-2, edge_ke=1e-2, edge_kd=1e-3)  # fmt: skip
+    b.add_spring(0, b.particle_count - 1, 100.0, 1.0, 0.0)
+    b.color()
+    model = b.finalize("cuda")
+    solver = SolverVBD(model, iterations=5)
+    s0, s1 = model.state(), model.state()
+    q0 = s0.particle_q.clone()
+    dt, n = 1.0 / 600.0, 60
+    for _ in range(n):
+        solver.step(s0, s1, None, None, dt)
+        s0, s1 = s1, s0
+    torch.cuda.synchronize()
+    diff = (s0.particle_q - q0).cpu().numpy()
+    expected = -9.81 * dt * dt * n * (n + 1) / 2  # implicit Euler
+    assert np.abs(diff[:, 2] - expected).max() <= 1e-4 * abs(expected) + 1e-6
+    assert np.abs(diff[:, :2]).max() <= 1e-6
+    assert solver.device_errors() & ~4 == 0
