@@ -258,6 +258,7 @@ def test_damped_soft_block_falls_freely():
     torch.cuda.synchronize()
     diff = (s0.particle_q - q0).cpu().numpy()
     expected = -9.81 * dt * dt * n * (n + 1) / 2  # implicit Euler
-    assert np.abs(diff[:, 2] - expected).max() <= 1e-4 * abs(expected) + 1e-6
-    assert np.abs(diff[:, :2]).max() <= 1e-6
+    # FP32 positions near z = 2 m carry ~2e-7 m of rounding per substep
+    assert np.abs(diff[:, 2] - expected).max() <= 1e-3 * abs(expected) + 1e-5
+    assert np.abs(diff[:, :2]).max() <= 1e-5
     assert solver.device_errors() & ~4 == 0
