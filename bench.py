@@ -248,8 +248,9 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
-                                 f".clocks_{os.getpid()}.csv")  # fmt: skip
+        import tempfile
+
+        self.path = os.path.join(tempfile.gettempdir(), f"vbd_clocks_{os.getpid()}_{index}.csv")
 
     def __enter__(self):
         try:
