@@ -295,26 +295,6 @@ __device__ __forceinline__ void ell16_face(const StepCtx<R>& c, const P& pos, in
   membrane_add<R>(0, x, pos.ld(ia), pos.ld(ib), pose, R(muA), R(lmA), R(kd), R(1), c.dt, xp, f, H, R(0));
 }
 
-// The four positions of a hinge record (nothing for an empty or zero-stiffness record).
-template <typename R, typename P>
-__device__ __forceinline__ void ell16_hinge_gather(const P& pos, int vs, uint4 hh, vec3<R> xs[4]) {
-  if (!(__uint_as_float(hh.w) > 0.f)) return;
-  xs[0] = pos.ld(vs + int(hh.x & 0xffffu));
-  xs[1] = pos.ld(vs + int(hh.x >> 16));
-  xs[2] = pos.ld(vs + int(hh.y & 0xffffu));
-  xs[3] = pos.ld(vs + int(hh.y >> 16));
-}
-
-// Bending term of a hinge record whose positions were gathered already.
-template <typename R>
-__device__ __forceinline__ void ell16_hinge_eval(int lv, uint4 hh, const vec3<R> xs[4], R dt, vec3<R>& f, sym3<R>& H) {
-  const float k = __uint_as_float(hh.w);
-  if (!(k > 0.f)) return;
-  const int i0 = int(hh.x & 0xffffu), i1 = int(hh.x >> 16), i2 = int(hh.y & 0xffffu);
-  const int role = i0 == lv ? 0 : (i1 == lv ? 1 : (i2 == lv ? 2 : 3));
-  bending_add<R>(role, xs, R(__uint_as_float(hh.z)), R(1), R(k), R(0), dt, nullptr, f, H);
-}
-
 // Bending term of one 16-byte hinge record for the solved vertex (instance-local id lv): the record lists the
 // hinge's four vertices in their (o0, o1, v0, v1) order, so the solved vertex's role is where lv appears and all
 // four positions are gathered (the solved vertex's own gather reads its current position).
@@ -372,23 +352,18 @@ __device__ __forceinline__ void solve_ell16(const StepCtx<R>& c, const P& pos, c
       }
     }
     {
-      // hinges, software-pipelined two deep: while slot s is evaluated, the positions of slot s + 1 are being
-      // gathered (its record arrived one slot earlier) and the record of slot s + 2 is loading
       const uint4* ph = e.hinge + eb;
-      const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
-      uint4 h1 = ne > 0 ? __ldcs(ph) : zero;
-      uint4 h2 = ne > 1 ? __ldcs(ph + n) : zero;
-      for (int q = 2; q < kRecordPrefetch + 1 && q < ne; ++q) prefetch_l2(ph + (long long)q * n);
-      vec3<R> g[4] = {zero3<R>(), zero3<R>(), zero3<R>(), zero3<R>()};
-      ell16_hinge_gather<R>(pos, vs, h1, g);
+      uint4 h_n = make_uint4(0u, 0u, 0u, 0u);
+      if (ne > 0) h_n = __ldcs(ph);
+      for (int q = 1; q < kRecordPrefetch && q < ne; ++q) prefetch_l2(ph + (long long)q * n);
       for (int s = 0; s < ne; ++s) {
-        const uint4 hh = h1;
-        vec3<R> xs[4] = {g[0], g[1], g[2], g[3]};
-        h1 = h2;
-        if (s + 1 + kRecordPrefetch < ne) prefetch_l2(ph + (long long)(s + 1 + kRecordPrefetch) * n);
-        h2 = s + 2 < ne ? __ldcs(ph + (long long)(s + 2) * n) : zero;
-        if (s + 1 < ne) ell16_hinge_gather<R>(pos, vs, h1, g);
-        ell16_hinge_eval<R>(v - vs, hh, xs, c.dt, f, H);
+        const uint4 hh = h_n;
+        if (s + kRecordPrefetch < ne) prefetch_l2(ph + (long long)kRecordPrefetch * n);
+        if (s + 1 < ne) {
+          ph += n;
+          h_n = __ldcs(ph);
+        }
+        ell16_hinge<R>(pos, vs, v - vs, hh, c.dt, f, H);
       }
     }
   }
