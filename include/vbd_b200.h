@@ -369,7 +369,9 @@ int vbd_soft_contacts(int32_t particle_count, const float* q_dev, const float* r
    geometry/kernels.py:132-600). shape_type holds the reference's GeoType values: 1 plane (local +Z normal;
    scale (width, length), 0 = infinite, else the reference's Chebyshev distance to the quad), 3 sphere (r),
    4 capsule (r, half height; along local Z), 5 ellipsoid (rx, ry, rz), 6 cylinder (r, half height; along local
-   Z), 7 box (half extents); other types return VBD_ERR_UNSUPPORTED. shape_transform_host [S,7]: position and
+   Z), 7 box (half extents), 9 cone (base radius, half height; base at local z = -half height, apex at
+   +half height); 2 (heightfield) needs vbd_soft_contacts_shapes_hf; other types (meshes, Gaussians) return
+   VBD_ERR_UNSUPPORTED. shape_transform_host [S,7]: position and
    rotation quaternion (x, y, z, w) of each shape; shape_scale_host [S,3]; at most 16 shapes. Contacts are
    written as vbd_soft_contacts writes them: the contact point on the surface in world (the body frame of a
    static shape), zero body velocity, the world normal; slots from an atomic counter. */
@@ -378,6 +380,35 @@ int vbd_soft_contacts_shapes(int32_t particle_count, const float* q_dev, const f
                              const float* shape_transform_host, const float* shape_scale_host, float margin,
                              int32_t soft_contact_max, int32_t* count_dev, int32_t* particle_dev, int32_t* shape_dev,
                              float* body_pos_dev, float* body_vel_dev, float* normal_dev, void* stream);
+
+/* One heightfield grid (HeightfieldData, utils/heightfield.py:65-77, as the reference builder fills it,
+   sim/builder.py:10698-10718): nrow x ncol elevations normalized to [0, 1] starting at data_offset in the
+   concatenated elevation array; height z = min_z + e (max_z - min_z); the grid spans [-hx, hx] x [-hy, hy] of the
+   shape frame. The shape's scale is already applied (hx = |hx sx|, hy = |hy sy|, min_z sz, max_z sz). */
+typedef struct VbdHeightfield {
+  int32_t data_offset;
+  int32_t nrow;
+  int32_t ncol;
+  float hx;
+  float hy;
+  float min_z;
+  float max_z;
+} VbdHeightfield;
+
+/* vbd_soft_contacts_shapes with heightfield shapes (GeoType 2, sample_sdf_grad_heightfield,
+   utils/heightfield.py:94-205): shape s of type 2 takes grid shape_heightfield_index_host[s] of
+   heightfields_host[heightfield_count]; elevations_dev holds elevation_count floats. Grids with nrow or ncol
+   below 2 give no contacts, as in the reference. Returns VBD_ERR_INVALID_ARGUMENT for an index out of range, a
+   grid that overruns elevation_count, or a non-positive or non-finite hx or hy (for which the reference's cell
+   index is undefined). */
+int vbd_soft_contacts_shapes_hf(int32_t particle_count, const float* q_dev, const float* radius_dev,
+                                const int32_t* flags_dev, int32_t shape_count, const int32_t* shape_type_host,
+                                const float* shape_transform_host, const float* shape_scale_host,
+                                const int32_t* shape_heightfield_index_host, int32_t heightfield_count,
+                                const VbdHeightfield* heightfields_host, const float* elevations_dev,
+                                int64_t elevation_count, float margin, int32_t soft_contact_max, int32_t* count_dev,
+                                int32_t* particle_dev, int32_t* shape_dev, float* body_pos_dev, float* body_vel_dev,
+                                float* normal_dev, void* stream);
 
 #ifdef __cplusplus
 }

@@ -11,6 +11,7 @@ from .sim import (
     Contacts,
     Control,
     GeoType,
+    Heightfield,
     Model,
     ModelBuilder,
     ParticleFlags,
@@ -33,6 +34,7 @@ __all__ = [
     "Contacts",
     "Control",
     "GeoType",
+    "Heightfield",
     "Model",
     "ModelBuilder",
     "ParticleFlags",

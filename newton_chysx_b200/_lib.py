@@ -80,6 +80,11 @@ class VbdBodyState(C.Structure):
     _fields_ = [("body_q_dev", _vp), ("body_q_prev_dev", _vp), ("body_qd_dev", _vp)]
 
 
+class VbdHeightfield(C.Structure):
+    _fields_ = [("data_offset", C.c_int32), ("nrow", C.c_int32), ("ncol", C.c_int32), ("hx", C.c_float),
+                ("hy", C.c_float), ("min_z", C.c_float), ("max_z", C.c_float)]  # fmt: skip
+
+
 class VbdRefAdjacency(C.Structure):
     _fields_ = [("face_offsets_dev", _vp), ("faces_dev", _vp), ("edge_offsets_dev", _vp), ("edges_dev", _vp)]
 
@@ -138,6 +143,11 @@ SIGNATURES = {
     "vbd_collider_destroy": ([_vp], C.c_int),
     "vbd_soft_contacts_shapes": (
         [C.c_int32, _vp, _vp, _vp, C.c_int32, _ip, _fp, _fp, C.c_float, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+        C.c_int,
+    ),
+    "vbd_soft_contacts_shapes_hf": (
+        [C.c_int32, _vp, _vp, _vp, C.c_int32, _ip, _fp, _fp, _ip, C.c_int32, C.POINTER(VbdHeightfield), _vp,
+         C.c_int64, C.c_float, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
         C.c_int,
     ),
     "vbd_soft_contacts": (

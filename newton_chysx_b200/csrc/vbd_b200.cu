@@ -5,6 +5,7 @@
 // collision pipeline's particle-shape contact generation for planes and spheres
 // (geometry/kernels.py:1001-1140). See vbd_kernels.cuh for the device side.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -135,6 +136,8 @@ struct ShapeXformTable {
   float4 p[kMaxContactShapes];  // position
   float4 q[kMaxContactShapes];  // rotation (x, y, z, w)
   float4 sc[kMaxContactShapes];  // scale
+  int4 hf[kMaxContactShapes];    // heightfields: (data_offset, nrow, ncol, 0)
+  float4 hfe[kMaxContactShapes];  // heightfields: (hx, hy, min_z, max_z), scale applied
 };
 
 __device__ __forceinline__ vec3<float> rot_q(float4 q, vec3<float> v) {
@@ -146,9 +149,9 @@ __device__ __forceinline__ vec3<float> rot_q(float4 q, vec3<float> v) {
 // (particle, shape), the particle in the shape frame, shape_sdf, and for d < margin + radius a contact at the
 // closest surface point x_local - n d and the normal, both mapped back to world; slots from an atomic counter.
 __global__ void k_soft_contacts_shapes(int n, const float* __restrict__ q, const float* __restrict__ radius,
-                                       const int* __restrict__ flags, int S, const ShapeXformTable shapes, float margin,
-                                       int cmax, int* count, int* particle, int* shape, float* body_pos, float* body_vel,
-                                       float* normal) {
+                                       const int* __restrict__ flags, int S, const ShapeXformTable shapes,
+                                       const float* __restrict__ elev, float margin, int cmax, int* count,
+                                       int* particle, int* shape, float* body_pos, float* body_vel, float* normal) {
   const long tid = long(blockIdx.x) * blockDim.x + threadIdx.x;
   if (tid >= long(n) * S) return;
   const int i = int(tid / S), s = int(tid % S);
@@ -159,7 +162,10 @@ __global__ void k_soft_contacts_shapes(int n, const float* __restrict__ q, const
   const float sc[3] = {SC.x, SC.y, SC.z};
   float d;
   vec3<float> nn;
-  shape_sdf(shapes.type[s], xl, sc, d, nn);
+  if (shapes.type[s] == GEO_HFIELD)
+    heightfield_sdf(shapes.hf[s], shapes.hfe[s], elev, xl, d, nn);
+  else
+    shape_sdf(shapes.type[s], xl, sc, d, nn);
   if (d < margin + radius[i]) {
     const int k = atomicAdd(count, 1);
     if (k < cmax) {
@@ -2096,23 +2102,23 @@ int vbd_soft_contacts(int32_t n, const float* q, const float* radius, const int3
   return VBD_OK;
 }
 
-int vbd_soft_contacts_shapes(int32_t n, const float* q, const float* radius, const int32_t* flags, int32_t S,
-                             const int32_t* shape_type, const float* shape_transform, const float* shape_scale,
-                             float margin, int32_t cmax, int32_t* count, int32_t* particle, int32_t* shape,
-                             float* body_pos, float* body_vel, float* normal, void* stream) {
-  if (n < 0 || S < 0 || S > kMaxContactShapes || cmax < 0 || !count ||
+int vbd_soft_contacts_shapes_hf(int32_t n, const float* q, const float* radius, const int32_t* flags, int32_t S,
+                                const int32_t* shape_type, const float* shape_transform, const float* shape_scale,
+                                const int32_t* shape_heightfield_index, int32_t heightfield_count,
+                                const VbdHeightfield* heightfields, const float* heightfield_elevations,
+                                int64_t elevation_count, float margin, int32_t cmax, int32_t* count, int32_t* particle,
+                                int32_t* shape, float* body_pos, float* body_vel, float* normal, void* stream) {
+  if (n < 0 || S < 0 || S > kMaxContactShapes || cmax < 0 || !count || heightfield_count < 0 || elevation_count < 0 ||
       (S && (!shape_type || !shape_transform || !shape_scale)))
     return VBD_ERR_INVALID_ARGUMENT;
   if (n > 0 && S > 0 && (!q || !radius || !flags || (cmax > 0 && (!particle || !shape || !body_pos || !body_vel || !normal))))
     return VBD_ERR_INVALID_ARGUMENT;
-  cudaStream_t st = (cudaStream_t)stream;
-  CK(cudaMemsetAsync(count, 0, sizeof(int), st));
-  if (n == 0 || S == 0) return VBD_OK;
   ShapeXformTable tab;
   std::memset(&tab, 0, sizeof(tab));
   for (int s = 0; s < S; ++s) {
     const int t = shape_type[s];
-    if (t != GEO_PLANE && t != GEO_SPHERE && t != GEO_CAPSULE && t != GEO_ELLIPSOID && t != GEO_CYLINDER && t != GEO_BOX)
+    if (t != GEO_PLANE && t != GEO_SPHERE && t != GEO_CAPSULE && t != GEO_ELLIPSOID && t != GEO_CYLINDER &&
+        t != GEO_BOX && t != GEO_CONE && t != GEO_HFIELD)
       return VBD_ERR_UNSUPPORTED;
     const float* X = shape_transform + 7 * s;
     const float ql = std::sqrt(X[3] * X[3] + X[4] * X[4] + X[5] * X[5] + X[6] * X[6]);
@@ -2121,12 +2127,41 @@ int vbd_soft_contacts_shapes(int32_t n, const float* q, const float* radius, con
     tab.p[s] = make_float4(X[0], X[1], X[2], 0.f);
     tab.q[s] = make_float4(X[3] / ql, X[4] / ql, X[5] / ql, X[6] / ql);
     tab.sc[s] = make_float4(shape_scale[3 * s], shape_scale[3 * s + 1], shape_scale[3 * s + 2], 0.f);
+    if (t == GEO_HFIELD) {  // every grid read of heightfield_sdf stays inside [data_offset, data_offset + nrow ncol)
+      if (!shape_heightfield_index || !heightfields) return VBD_ERR_INVALID_ARGUMENT;
+      const int k = shape_heightfield_index[s];
+      if (k < 0 || k >= heightfield_count) return VBD_ERR_INVALID_ARGUMENT;
+      const VbdHeightfield& h = heightfields[k];
+      if (h.nrow < 0 || h.ncol < 0 || h.data_offset < 0) return VBD_ERR_INVALID_ARGUMENT;
+      if (h.nrow > 1 && h.ncol > 1) {
+        if (!heightfield_elevations || int64_t(h.data_offset) + int64_t(h.nrow) * h.ncol > elevation_count ||
+            !(h.hx > 0.f) || !(h.hy > 0.f) || !std::isfinite(h.hx) || !std::isfinite(h.hy))
+          return VBD_ERR_INVALID_ARGUMENT;
+      }
+      tab.hf[s] = make_int4(h.data_offset, h.nrow, h.ncol, 0);
+      tab.hfe[s] = make_float4(h.hx, h.hy, h.min_z, h.max_z);
+    }
   }
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaMemsetAsync(count, 0, sizeof(int), st));
+  if (n == 0 || S == 0) return VBD_OK;
   const long total = long(n) * S;
-  k_soft_contacts_shapes<<<int((total + 255) / 256), 256, 0, st>>>(n, q, radius, flags, S, tab, margin, cmax, count,
-                                                                   particle, shape, body_pos, body_vel, normal);
+  k_soft_contacts_shapes<<<int((total + 255) / 256), 256, 0, st>>>(n, q, radius, flags, S, tab, heightfield_elevations,
+                                                                   margin, cmax, count, particle, shape, body_pos,
+                                                                   body_vel, normal);
   CK(cudaGetLastError());
   return VBD_OK;
+}
+
+int vbd_soft_contacts_shapes(int32_t n, const float* q, const float* radius, const int32_t* flags, int32_t S,
+                             const int32_t* shape_type, const float* shape_transform, const float* shape_scale,
+                             float margin, int32_t cmax, int32_t* count, int32_t* particle, int32_t* shape,
+                             float* body_pos, float* body_vel, float* normal, void* stream) {
+  for (int s = 0; s < S && shape_type; ++s)
+    if (shape_type[s] == GEO_HFIELD) return VBD_ERR_UNSUPPORTED;  // needs the grids: vbd_soft_contacts_shapes_hf
+  return vbd_soft_contacts_shapes_hf(n, q, radius, flags, S, shape_type, shape_transform, shape_scale, nullptr, 0,
+                                     nullptr, nullptr, 0, margin, cmax, count, particle, shape, body_pos, body_vel,
+                                     normal, stream);
 }
 
 int vbd_set_self_contact(VbdHandle h, const VbdSelfContactDesc* d) {

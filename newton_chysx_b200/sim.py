@@ -653,14 +653,14 @@ class ModelBuilder:
                 h = mesh_hinges(self.tri_indices[t0:self._t])
                 self.add_edges(h[:, 0], h[:, 1], h[:, 2], h[:, 3], edge_ke=edge_ke, edge_kd=edge_kd)
 
-    # -- shapes (builder.py:5900-6340): static collision shapes for particle contacts
-    def _add_shape(self, body, type_, xform, scale, cfg):
+    # -- shapes (builder.py:5900-6470): static collision shapes for particle contacts
+    def _add_shape(self, body, type_, xform, scale, cfg, src=None):
         if body != -1:
             raise NotImplementedError("only static shapes (body=-1) collide with particles here")
         cfg = cfg or self.default_shape_cfg
         p, q = _xform(xform)
         self.shapes.append(dict(type=GeoType(type_), pos=p, rot=q, scale=tuple(float(v) for v in scale), ke=cfg.ke,
-                                kd=cfg.kd, mu=cfg.mu, body=-1))  # fmt: skip
+                                kd=cfg.kd, mu=cfg.mu, body=-1, src=src))  # fmt: skip
         return len(self.shapes) - 1
 
     def add_shape_plane(self, plane=(0.0, 0.0, 1.0, 0.0), xform=None, width=10.0, length=10.0, body=-1,
@@ -694,6 +694,20 @@ class ModelBuilder:
 
     def add_shape_ellipsoid(self, body=-1, xform=None, rx=1.0, ry=0.75, rz=0.5, cfg: ShapeConfig | None = None):
         return self._add_shape(body, GeoType.ELLIPSOID, xform, (rx, ry, rz), cfg)
+
+    def add_shape_cone(self, body=-1, xform=None, radius=1.0, half_height=0.5, cfg: ShapeConfig | None = None):
+        """Cone along the local Z axis of xform: base of the given radius at z = -half_height, apex at
+        +half_height (``builder.py:6287-6340``)."""
+        return self._add_shape(body, GeoType.CONE, xform, (radius, half_height, 0.0), cfg)
+
+    def add_shape_heightfield(self, xform=None, heightfield: Heightfield | None = None, scale=None,
+                              cfg: ShapeConfig | None = None):  # fmt: skip
+        """A static heightfield (``builder.py:6423-6467``); scale (default (1, 1, 1)) multiplies hx, hy and
+        min_z/max_z as the reference's finalize does."""
+        if heightfield is None:
+            raise ValueError("add_shape_heightfield() requires a Heightfield instance.")
+        scale = (1.0, 1.0, 1.0) if scale is None else tuple(scale)
+        return self._add_shape(-1, GeoType.HFIELD, xform, scale, cfg, src=heightfield)
 
     # -- coloring (builder.py:9304-9396)
     @property
@@ -762,6 +776,31 @@ class ModelBuilder:
 
     def finalize(self, device="cuda") -> Model:
         return Model._from_builder(self, device)
+
+
+class Heightfield:
+    """A 2D elevation grid (``newton/_src/geometry/types.py:2095-2142``): the data are normalized to [0, 1];
+    heights are ``min_z + data (max_z - min_z)``, with min_z and max_z taken from the data unless both are given;
+    the grid spans [-hx, hx] x [-hy, hy]."""
+
+    def __init__(self, data, nrow: int, ncol: int, hx: float = 1.0, hy: float = 1.0, min_z: float | None = None,
+                 max_z: float | None = None):  # fmt: skip
+        if nrow < 2 or ncol < 2:
+            raise ValueError(f"Heightfield requires nrow >= 2 and ncol >= 2, got nrow={nrow}, ncol={ncol}")
+        if (min_z is None) != (max_z is None):
+            raise ValueError("min_z and max_z must both be provided or both omitted")
+        raw = np.array(data, dtype=np.float32).reshape(nrow, ncol)
+        lo, hi = float(raw.min()), float(raw.max())
+        self._data = (raw - lo) / (hi - lo) if hi > lo else np.zeros_like(raw)
+        self.nrow, self.ncol = nrow, ncol
+        self.hx, self.hy = hx, hy
+        self.min_z = lo if min_z is None else float(min_z)
+        self.max_z = hi if max_z is None else float(max_z)
+
+    @property
+    def data(self):
+        """The normalized [0, 1] elevations, shape (nrow, ncol)."""
+        return self._data
 
 
 # ----------------------------------------------------------------------------- model, state, contacts
@@ -840,6 +879,19 @@ class Model:
         m.shape_material_kd = t(np.array([s["kd"] for s in b.shapes]).reshape(S), f32)
         m.shape_material_mu = t(np.array([s["mu"] for s in b.shapes]).reshape(S), f32)
         m.shape_body = t(np.array([s["body"] for s in b.shapes], dtype=np.int32).reshape(S), i32)
+        # heightfields as the reference's finalize packs them (builder.py:10690-10735): one row (data_offset, nrow,
+        # ncol, |hx sx|, |hy sy|, min_z sz, max_z sz) per heightfield shape, elevations concatenated
+        m.shape_heightfield_index = np.full(S, -1, dtype=np.int32)
+        rows, chunks, off = [], [], 0
+        for i, sh in enumerate(b.shapes):
+            if sh["type"] == GeoType.HFIELD and sh.get("src") is not None:
+                hf, (sx, sy, sz) = sh["src"], sh["scale"]
+                m.shape_heightfield_index[i] = len(rows)
+                rows.append((off, hf.nrow, hf.ncol, abs(hf.hx * sx), abs(hf.hy * sy), hf.min_z * sz, hf.max_z * sz))
+                chunks.append(np.asarray(hf.data, dtype=np.float32).reshape(-1))
+                off += hf.nrow * hf.ncol
+        m.heightfield_data = np.array(rows, dtype=np.float64).reshape(-1, 7)
+        m.heightfield_elevations = t(np.concatenate(chunks) if chunks else np.zeros(1, np.float32), f32)
         m.body_com = None
         return m
 
@@ -920,7 +972,7 @@ class Contacts:
 
 
 def soft_contacts(model: Model, state: State, contacts: Contacts, margin: float):
-    """Particle contacts against the model's static analytic shapes on the GPU (``vbd_soft_contacts_shapes``)."""
+    """Particle contacts against the model's static shapes on the GPU (``vbd_soft_contacts_shapes_hf``)."""
     lib = _lib.load()
     S = model.shape_count
     if S == 0:
@@ -929,22 +981,29 @@ def soft_contacts(model: Model, state: State, contacts: Contacts, margin: float)
     st = np.ascontiguousarray(model.shape_type, dtype=np.int32)
     sx = np.ascontiguousarray(model.shape_transform, dtype=np.float32)
     ss = np.ascontiguousarray(model.shape_scale, dtype=np.float32)
+    hidx = np.ascontiguousarray(getattr(model, "shape_heightfield_index", np.full(S, -1)), dtype=np.int32)
+    rows = getattr(model, "heightfield_data", np.zeros((0, 7)))
+    hfs = (_lib.VbdHeightfield * max(len(rows), 1))()
+    for k, r in enumerate(rows):
+        hfs[k] = _lib.VbdHeightfield(int(r[0]), int(r[1]), int(r[2]), *(float(v) for v in r[3:]))
+    elev = getattr(model, "heightfield_elevations", None)
     ip, fp = C.POINTER(C.c_int32), C.POINTER(C.c_float)
     stream = torch.cuda.current_stream(model.device).cuda_stream
-    rc = lib.vbd_soft_contacts_shapes(
+    rc = lib.vbd_soft_contacts_shapes_hf(
         model.particle_count, state.particle_q.data_ptr(), model.particle_radius.data_ptr(),
         model.particle_flags.data_ptr(), S, st.ctypes.data_as(ip), sx.ctypes.data_as(fp), ss.ctypes.data_as(fp),
-        float(margin), contacts.soft_contact_max, contacts.soft_contact_count.data_ptr(),
-        contacts.soft_contact_particle.data_ptr(), contacts.soft_contact_shape.data_ptr(),
-        contacts.soft_contact_body_pos.data_ptr(), contacts.soft_contact_body_vel.data_ptr(),
-        contacts.soft_contact_normal.data_ptr(), C.c_void_p(stream),
+        hidx.ctypes.data_as(ip), len(rows), hfs, None if elev is None else elev.data_ptr(),
+        0 if elev is None else elev.numel(), float(margin), contacts.soft_contact_max,
+        contacts.soft_contact_count.data_ptr(), contacts.soft_contact_particle.data_ptr(),
+        contacts.soft_contact_shape.data_ptr(), contacts.soft_contact_body_pos.data_ptr(),
+        contacts.soft_contact_body_vel.data_ptr(), contacts.soft_contact_normal.data_ptr(), C.c_void_p(stream),
     )  # fmt: skip
-    _lib.check(rc, "vbd_soft_contacts_shapes")
+    _lib.check(rc, "vbd_soft_contacts_shapes_hf")
 
 
 class CollisionPipeline:
-    """Particle-shape part of ``newton/_src/sim/collide.py:485`` (static planes, spheres, boxes, capsules,
-    cylinders and ellipsoids)."""
+    """Particle-shape part of ``newton/_src/sim/collide.py:485`` (static planes, heightfields, spheres, boxes,
+    capsules, cylinders, cones and ellipsoids)."""
 
     def __init__(self, model: Model, soft_contact_max=None, soft_contact_margin=0.01, **_ignored):
         self.model = model

@@ -1238,7 +1238,7 @@ int step(const Model& M, double* q_in, const double* qd_in, const double* f_ext,
 // contact point x_local - n d and the normal mapped back to world. Contacts in particle-major order.
 namespace sdf {
 using D3 = V3<double>;
-enum { PLANE = 1, SPHERE = 3, CAPSULE = 4, ELLIPSOID = 5, CYLINDER = 6, BOX = 7 };
+enum { PLANE = 1, HFIELD = 2, SPHERE = 3, CAPSULE = 4, ELLIPSOID = 5, CYLINDER = 6, BOX = 7, CONE = 9 };
 inline double sgn(double x) { return x < 0.0 ? -1.0 : 1.0; }  // wp.sign: -1 below zero, 1 otherwise
 inline D3 qrot(const double* q, D3 v) {  // q = (x, y, z, w)
   const D3 u = v3(q[0], q[1], q[2]);
@@ -1321,6 +1321,56 @@ inline void ellipsoid(D3 p, D3 radii, double& d, D3& n) {
     const D3 g = q1 * (k0 / k1);
     const double gl = length(g);
     if (gl > 1.0e-8) n = g / gl;
+  }
+}
+// :141-161 (capped cone with top radius 0) and :515-564: base radius r at z = -hh, apex at z = +hh
+inline double cone(D3 p, double r, double hh) {
+  const double qx = std::sqrt(p.x * p.x + p.y * p.y), qy = p.z;
+  const double k2x = -r, k2y = 2.0 * hh;  // (top radius - bottom radius, 2 hh)
+  const double cax = qx - std::min(qx, qy < 0.0 ? r : 0.0), cay = std::fabs(qy) - hh;
+  const double den = k2x * k2x + k2y * k2y;
+  const double t = den > 0.0 ? std::min(std::max(((0.0 - qx) * k2x + (hh - qy) * k2y) / den, 0.0), 1.0) : 0.0;
+  const double cbx = qx + k2x * t, cby = qy - hh + k2y * t;
+  const double sg = (cbx < 0.0 && cay < 0.0) ? -1.0 : 1.0;
+  return sg * std::sqrt(std::min(cax * cax + cay * cay, cbx * cbx + cby * cby));
+}
+inline D3 cone_grad(D3 p, double r, double hh) {
+  if (hh <= 0.0) return v3(0.0, 0.0, sgn(p.z));
+  const double rr = length(v3(p.x, p.y, 0.0));
+  const double dx = rr - r * (hh - p.z) / (2.0 * hh), dy = std::fabs(p.z) - hh;
+  if (dx > dy) return rr > 0.0 ? normalize0(v3(p.x / rr, p.y / rr, r / (2.0 * hh))) : v3(0.0, 0.0, 1.0);
+  return v3(0.0, 0.0, sgn(p.z));
+}
+// utils/heightfield.py:94-205: grid g = (data_offset, nrow, ncol), extents e = (hx, hy, min_z, max_z), normalized
+// elevations; the clamped point's cell triangle (diagonal from (col, row) to (col + 1, row + 1)) gives the plane
+// distance and normal, and outside the footprint the lateral gap is folded in.
+inline void heightfield(const int* g, const double* e, const double* elev, D3 p, double& d, D3& n) {
+  const int nrow = g[1], ncol = g[2];
+  if (nrow <= 1 || ncol <= 1) {
+    d = 1.0e10, n = v3(0.0, 0.0, 1.0);
+    return;
+  }
+  const double hx = e[0], hy = e[1], zmin = e[2], zr = e[3] - e[2];
+  const double dx = 2.0 * hx / double(ncol - 1), dy = 2.0 * hy / double(nrow - 1);
+  const double cx = std::min(std::max(p.x, -hx), hx), cy = std::min(std::max(p.y, -hy), hy);
+  const double ox = p.x - cx, oy = p.y - cy, lat = ox * ox + oy * oy;
+  const double colf = std::min(std::max((cx + hx) / dx, 0.0), double(ncol - 1));
+  const double rowf = std::min(std::max((cy + hy) / dy, 0.0), double(nrow - 1));
+  const int col = std::min(int(colf), ncol - 2), row = std::min(int(rowf), nrow - 2);
+  const double fx = colf - col, fy = rowf - row;
+  const double* z = elev + g[0] + long(row) * ncol + col;
+  const double h00 = zmin + z[0] * zr, h10 = zmin + z[1] * zr, h01 = zmin + z[ncol] * zr, h11 = zmin + z[ncol + 1] * zr;
+  const D3 v0 = v3(-hx + col * dx, -hy + row * dy, h00);
+  const D3 e1 = fx >= fy ? v3(dx, 0.0, h10 - h00) : v3(dx, dy, h11 - h00);
+  const D3 e2 = fx >= fy ? v3(dx, dy, h11 - h00) : v3(0.0, dy, h01 - h00);
+  const D3 nrm = normalize0(cross(e1, e2));
+  const double dp = dot(p - v0, nrm);
+  if (lat > 0.0) {
+    d = std::sqrt(lat + dp * dp);
+    const D3 raw = v3(ox, oy, 0.0) + nrm * dp;
+    n = dot(raw, raw) > 1.0e-20 ? normalize0(raw) : v3(0.0, 0.0, 1.0);
+  } else {
+    d = dp, n = nrm;
   }
 }
 // :568-589
@@ -1719,15 +1769,21 @@ int oracle_soft_contacts(int n, const double* q, const double* radius, const int
 
 // shape_xform [S,7] = (position, quaternion xyzw), shape_scale [S,3]. Returns the number of contacts found,
 // or -1 for a shape type without an analytic SDF here.
+// Heightfield shapes (type 2) take grid hf_index[s]: hf_grid[3k..] = (data_offset, nrow, ncol),
+// hf_ext[4k..] = (hx, hy, min_z, max_z) with the shape's scale applied, over the elevations `elev`.
 int oracle_soft_contacts_shapes(int n, const double* q, const double* radius, const int* flags, int S,
                                 const int* shape_type, const double* shape_xform, const double* shape_scale,
+                                const int* hf_index, const int* hf_grid, const double* hf_ext, const double* elev,
                                 double margin, int max_contacts, int* particle, int* shape, double* body_pos,
                                 double* body_vel, double* normal) {
   using sdf::D3;
-  for (int s = 0; s < S; ++s)
-    if (shape_type[s] != sdf::PLANE && shape_type[s] != sdf::SPHERE && shape_type[s] != sdf::CAPSULE &&
-        shape_type[s] != sdf::ELLIPSOID && shape_type[s] != sdf::CYLINDER && shape_type[s] != sdf::BOX)
+  for (int s = 0; s < S; ++s) {
+    const int t = shape_type[s];
+    if (t != sdf::PLANE && t != sdf::SPHERE && t != sdf::CAPSULE && t != sdf::ELLIPSOID && t != sdf::CYLINDER &&
+        t != sdf::BOX && t != sdf::CONE && t != sdf::HFIELD)
       return -1;
+    if (t == sdf::HFIELD && (!hf_index || !hf_grid || !hf_ext || !elev)) return -1;
+  }
   int count = 0;
   for (int i = 0; i < n; ++i) {
     if (!(flags[i] & 1)) continue;
@@ -1745,6 +1801,12 @@ int oracle_soft_contacts_shapes(int n, const double* q, const double* radius, co
         case sdf::CAPSULE: d = sdf::capsule(xl, sc[0], sc[1]), nn = sdf::capsule_grad(xl, sc[1]); break;
         case sdf::CYLINDER: d = sdf::cylinder(xl, sc[0], sc[1]), nn = sdf::cylinder_grad(xl, sc[0], sc[1]); break;
         case sdf::ELLIPSOID: sdf::ellipsoid(xl, v3(sc[0], sc[1], sc[2]), d, nn); break;
+        case sdf::CONE: d = sdf::cone(xl, sc[0], sc[1]), nn = sdf::cone_grad(xl, sc[0], sc[1]); break;
+        case sdf::HFIELD: {
+          const int k = hf_index[s];
+          sdf::heightfield(hf_grid + 3 * k, hf_ext + 4 * k, elev, xl, d, nn);
+          break;
+        }
         default: d = sdf::plane(xl, sc[0] * 0.5, sc[1] * 0.5), nn = v3(0.0, 0.0, 1.0); break;
       }
       if (d < margin + radius[i]) {

@@ -110,7 +110,8 @@ def lib():
             C.c_int, _dp, _dp, _ip, C.c_int, _ip, _dp, _dp, C.c_double, C.c_int, _ip, _ip, _dp, _dp, _dp,
         ]
         _lib.oracle_soft_contacts_shapes.argtypes = [
-            C.c_int, _dp, _dp, _ip, C.c_int, _ip, _dp, _dp, C.c_double, C.c_int, _ip, _ip, _dp, _dp, _dp,
+            C.c_int, _dp, _dp, _ip, C.c_int, _ip, _dp, _dp, _ip, _ip, _dp, _dp, C.c_double, C.c_int, _ip, _ip, _dp,
+            _dp, _dp,
         ]  # fmt: skip
         _lib.oracle_max_threads.restype = C.c_int
         _lib.oracle_vbd_step_sc.argtypes = [
@@ -298,10 +299,13 @@ def soft_contacts(q, radius, flags, shape_type, shape_pos, shape_radius, margin,
     return cnt, part, shp, bp.reshape(-1, 3), bv.reshape(-1, 3), nn.reshape(-1, 3)
 
 
-def soft_contacts_shapes(q, radius, flags, shape_type, shape_transform, shape_scale, margin, max_contacts=None):
-    """Particle-shape contacts against static analytic shapes (GeoType values: plane 1, sphere 3, capsule 4,
-    ellipsoid 5, cylinder 6, box 7) with transforms [S, 7] (position, quaternion xyzw) and scales [S, 3], in
-    (particle, shape) order."""
+def soft_contacts_shapes(q, radius, flags, shape_type, shape_transform, shape_scale, margin, max_contacts=None,
+                         heightfield_index=None, heightfields=None, elevations=None):
+    """Particle-shape contacts against static analytic shapes (GeoType values: plane 1, heightfield 2, sphere 3,
+    capsule 4, ellipsoid 5, cylinder 6, box 7, cone 9) with transforms [S, 7] (position, quaternion xyzw) and
+    scales [S, 3], in (particle, shape) order. Heightfield shape s uses grid ``heightfield_index[s]`` of
+    ``heightfields`` (rows of (data_offset, nrow, ncol, hx, hy, min_z, max_z), scale applied) over the
+    concatenated normalized ``elevations``."""
     n = len(radius)
     S = len(shape_type)
     max_contacts = max_contacts or n * max(S, 1)
@@ -316,7 +320,15 @@ def soft_contacts_shapes(q, radius, flags, shape_type, shape_transform, shape_sc
     bp, bpp = _d(np.zeros(3 * max_contacts))
     bv, bvp = _d(np.zeros(3 * max_contacts))
     nn, nnp = _d(np.zeros(3 * max_contacts))
-    cnt = lib().oracle_soft_contacts_shapes(n, qp, rp, flp, S, stp, sxp, ssp, margin, max_contacts, pp, shpp, bpp, bvp,
+    hfi = hfg = hfe = elv = None
+    if heightfields is not None and len(heightfields):
+        hf = np.asarray(heightfields, dtype=np.float64).reshape(-1, 7)
+        hfi = _i(heightfield_index)
+        hfg = _i(hf[:, :3].astype(np.int64))
+        hfe = _d(hf[:, 3:])
+        elv = _d(np.asarray(elevations).reshape(-1))
+    cnt = lib().oracle_soft_contacts_shapes(n, qp, rp, flp, S, stp, sxp, ssp, *(None if a is None else a[1] for a in
+                                            (hfi, hfg, hfe, elv)), margin, max_contacts, pp, shpp, bpp, bvp,
                                             nnp)  # fmt: skip
     if cnt < 0:
         raise ValueError("a shape type without an analytic SDF")

@@ -254,9 +254,11 @@ def load_reference(ref: str) -> dict:
         os.path.join(ref, "newton/_src/geometry/kernels.py"),
         {"_sdf_point_to_z_up", "_sdf_vector_from_z_up", "sdf_sphere", "sdf_sphere_grad", "sdf_box", "sdf_box_grad",
          "sdf_capsule", "sdf_capsule_grad", "sdf_cylinder", "sdf_cylinder_grad", "sdf_ellipsoid", "sdf_ellipsoid_grad",
-         "sdf_plane"},
+         "sdf_plane", "_sdf_capped_cone_z", "sdf_cone", "sdf_cone_grad"},
         ns,
     )  # fmt: skip
+    _lift(os.path.join(ref, "newton/_src/utils/heightfield.py"),
+          {"_heightfield_surface_query", "sample_sdf_grad_heightfield"}, ns)  # fmt: skip
     _lift(os.path.join(ref, "newton/_src/utils/mesh.py"), set(), ns, classes={"MeshAdjacency": {"*"}})
     _lift(
         os.path.join(ref, "newton/_src/sim/builder.py"),
@@ -950,6 +952,86 @@ def shape_contact_cases(ns, seed=17):
     return res
 
 
+GEO_HFIELD, GEO_CONE = 2, 9
+
+
+def shape_contact_cases_cone_hfield(ns, seed=19):
+    """Particle contacts against cones (``sdf_cone``/``sdf_cone_grad``, geometry/kernels.py:515-564) and
+    heightfields (``sample_sdf_grad_heightfield``, utils/heightfield.py:178-205) through create_soft_contacts'
+    frame handling, for shapes without a body. The heightfields' extents carry the shape scale as the reference
+    builder bakes it (sim/builder.py:10698-10718): hx |sx|, hy |sy|, min_z sz, max_z sz; elevations are normalized
+    to [0, 1] as ``Heightfield`` stores them (geometry/types.py:2128-2134). One grid has a single row and gives no
+    contacts."""
+    rng = np.random.default_rng(seed)
+
+    def quat(axis, ang):
+        return wp.quat_from_axis_angle(np.asarray(axis, dtype=float), ang)
+
+    grids = []  # (raw elevations, hx, hy, min_z, max_z, scale)
+    gx, gy = np.meshgrid(np.linspace(-1.0, 1.0, 17), np.linspace(-1.0, 1.0, 13))
+    grids.append((np.sin(2.0 * gx) * np.cos(3.0 * gy), 0.8, 0.6, -0.05, 0.15, (1.0, 1.0, 1.0)))
+    grids.append((rng.uniform(0.0, 1.0, (9, 7)), 0.3, 0.4, 0.0, 0.1, (1.5, -0.5, 2.0)))
+    grids.append((rng.uniform(0.0, 1.0, (1, 5)), 0.3, 0.3, 0.0, 0.1, (1.0, 1.0, 1.0)))
+    shapes = [  # type, position, rotation (x, y, z, w), scale (cones), heightfield index
+        (GEO_CONE, (0.4, 0.3, 0.3), wp.quat_identity(), (0.25, 0.2, 0.0), -1),
+        (GEO_CONE, (-0.5, 0.5, 0.35), quat((1.0, 0.3, 0.2), 2.2), (0.2, 0.3, 0.0), -1),
+        (GEO_CONE, (0.5, -0.5, 0.25), quat((0.2, 1.0, 0.0), 0.8), (0.3, 0.0, 0.0), -1),
+        (GEO_HFIELD, (0.0, 0.0, 0.1), quat((0.0, 0.0, 1.0), 0.3), (1.0, 1.0, 1.0), 0),
+        (GEO_HFIELD, (-0.4, -0.4, 0.3), quat((1.0, 0.5, 0.0), 0.25), (1.5, -0.5, 2.0), 1),
+        (GEO_HFIELD, (0.5, 0.6, 0.2), wp.quat_identity(), (1.0, 1.0, 1.0), 2),
+    ]
+    elevations, hdata, off = [], [], 0
+    for raw, hx, hy, zmin, zmax, sc in grids:
+        raw = np.asarray(raw, dtype=np.float32)
+        lo, hi = float(raw.min()), float(raw.max())
+        data = (raw - lo) / (hi - lo) if hi > lo else np.zeros_like(raw)
+        hdata.append(types.SimpleNamespace(data_offset=off, nrow=raw.shape[0], ncol=raw.shape[1],
+                                           hx=abs(hx * sc[0]), hy=abs(hy * sc[1]), min_z=zmin * sc[2],
+                                           max_z=zmax * sc[2]))  # fmt: skip
+        elevations.append(data.astype(np.float32).reshape(-1))
+        off += data.size
+    elev = np.concatenate(elevations).astype(np.float64)
+    n = 6000
+    q = np.stack([rng.uniform(-1.0, 1.0, n), rng.uniform(-1.0, 1.0, n), rng.uniform(-0.1, 0.7, n)], axis=1)
+    radius = rng.uniform(0.005, 0.02, n)
+    flags = np.where(rng.uniform(size=n) < 0.9, 1, 0).astype(np.int32)
+    margin = 0.02
+    out = {k: [] for k in ("particle", "shape", "body_pos", "body_vel", "normal", "distance")}
+    for i in range(n):
+        if not (flags[i] & 1):
+            continue
+        for s, (typ, pos, rot, sc, hk) in enumerate(shapes):
+            X_ws = (np.asarray(pos, dtype=float), np.asarray(rot, dtype=float))
+            x_local = wp.transform_point(wp.transform_inverse(X_ws), wp.vec3(*q[i]))
+            scale = wp.vec3(*sc)
+            d, nn, v = 1.0e6, wp.vec3(), wp.vec3()
+            if typ == GEO_CONE:
+                d = ns["sdf_cone"](x_local, scale[0], scale[1], 2)
+                nn = ns["sdf_cone_grad"](x_local, scale[0], scale[1], 2)
+            if typ == GEO_HFIELD:
+                d, nn = ns["sample_sdf_grad_heightfield"](hdata[hk], elev, x_local)
+            if d < margin + radius[i]:
+                out["particle"].append(i)
+                out["shape"].append(s)
+                out["body_pos"].append(np.asarray(wp.transform_point(X_ws, x_local - nn * d)))
+                out["body_vel"].append(np.asarray(wp.transform_vector(X_ws, v)))
+                out["normal"].append(np.asarray(wp.transform_vector(X_ws, nn)))
+                out["distance"].append(d)
+    res = {k: np.asarray(v) for k, v in out.items()}
+    res["particle"] = res["particle"].astype(np.int32)
+    res["shape"] = res["shape"].astype(np.int32)
+    res.update(
+        q=q, radius=radius, flags=flags, margin=np.float64(margin),
+        shape_type=np.array([t for t, _, _, _, _ in shapes], dtype=np.int32),
+        shape_transform=np.array([list(p) + list(r) for _, p, r, _, _ in shapes], dtype=np.float64),
+        shape_scale=np.array([sc for _, _, _, sc, _ in shapes], dtype=np.float64),
+        shape_heightfield_index=np.array([k for _, _, _, _, k in shapes], dtype=np.int32),
+        heightfields=np.array([[h.data_offset, h.nrow, h.ncol, h.hx, h.hy, h.min_z, h.max_z] for h in hdata]),
+        elevations=elev.astype(np.float32),
+    )  # fmt: skip
+    return res
+
+
 def soft_cases(ns, seed=13):
     """Per-element goldens of the volumetric Neo-Hookean tetrahedron and of the spring."""
     rng = np.random.default_rng(seed)
@@ -1049,6 +1131,8 @@ def main():
     np.savez_compressed(os.path.join(args.out, "soft_elements.npz"), **soft_cases(ns))
     np.savez_compressed(os.path.join(args.out, "soft_contact_shapes.npz"), **shape_contact_cases(ns))
     print("soft_contact_shapes.npz written")
+    np.savez_compressed(os.path.join(args.out, "soft_contact_cone_hfield.npz"), **shape_contact_cases_cone_hfield(ns))
+    print("soft_contact_cone_hfield.npz written")
     print("soft_elements.npz written")
 
     # Volumetric: a 3 x 2 x 2-cell tetrahedral block (add_soft_grid, 5 tetrahedra per cell, damped), 4 mm

@@ -197,6 +197,10 @@ def length(a):
     return float(np.sqrt(np.dot(a.a, a.a)))
 
 
+def length_sq(a):
+    return float(np.dot(a.a, a.a))
+
+
 def normalize(a):
     n = length(a)
     return Vec(a.a / n) if n > 0.0 else Vec(np.zeros_like(a.a))

@@ -18,7 +18,8 @@ from tests.helpers import load_golden
 pytestmark = pytest.mark.gpu
 
 
-def _gpu_contacts(q, radius, flags, shape_type, shape_transform, shape_scale, margin):
+def _gpu_contacts(q, radius, flags, shape_type, shape_transform, shape_scale, margin, hf_index=None,
+                  heightfields=None, elevations=None):
     lib = _lib.load()
     n, S = len(radius), len(shape_type)
     cmax = n * S
@@ -36,10 +37,21 @@ def _gpu_contacts(q, radius, flags, shape_type, shape_transform, shape_scale, ma
     sx = np.ascontiguousarray(shape_transform, dtype=np.float32)
     ss = np.ascontiguousarray(shape_scale, dtype=np.float32)
     ip, fp = C.POINTER(C.c_int32), C.POINTER(C.c_float)
-    rc = lib.vbd_soft_contacts_shapes(n, qd.data_ptr(), rd.data_ptr(), fd.data_ptr(), S, st.ctypes.data_as(ip),
-                                      sx.ctypes.data_as(fp), ss.ctypes.data_as(fp), float(margin), cmax, cnt.data_ptr(),
-                                      part.data_ptr(), shp.data_ptr(), bp.data_ptr(), bv.data_ptr(), nn.data_ptr(),
-                                      None)  # fmt: skip
+    if heightfields is None:
+        rc = lib.vbd_soft_contacts_shapes(n, qd.data_ptr(), rd.data_ptr(), fd.data_ptr(), S, st.ctypes.data_as(ip),
+                                          sx.ctypes.data_as(fp), ss.ctypes.data_as(fp), float(margin), cmax,
+                                          cnt.data_ptr(), part.data_ptr(), shp.data_ptr(), bp.data_ptr(), bv.data_ptr(),
+                                          nn.data_ptr(), None)  # fmt: skip
+    else:
+        hi = np.ascontiguousarray(hf_index, dtype=np.int32)
+        hfs = (_lib.VbdHeightfield * len(heightfields))(
+            *[_lib.VbdHeightfield(int(r[0]), int(r[1]), int(r[2]), *map(float, r[3:])) for r in heightfields])
+        ev = torch.as_tensor(np.asarray(elevations, dtype=np.float32), device=dev)
+        rc = lib.vbd_soft_contacts_shapes_hf(n, qd.data_ptr(), rd.data_ptr(), fd.data_ptr(), S, st.ctypes.data_as(ip),
+                                             sx.ctypes.data_as(fp), ss.ctypes.data_as(fp), hi.ctypes.data_as(ip),
+                                             len(heightfields), hfs, ev.data_ptr(), ev.numel(), float(margin), cmax,
+                                             cnt.data_ptr(), part.data_ptr(), shp.data_ptr(), bp.data_ptr(),
+                                             bv.data_ptr(), nn.data_ptr(), None)  # fmt: skip
     _lib.check(rc, "vbd_soft_contacts_shapes")
     torch.cuda.synchronize()
     k = int(cnt.item())
@@ -116,3 +128,144 @@ def test_collision_pipeline_shapes_match_oracle():
     near -= set(zip(lo[1][:lo[0]].tolist(), lo[2][:lo[0]].tolist()))
     assert len(set(s[:cnt].tolist())) == model.shape_count
     _compare(gpu, list(zip(p[:cnt].tolist(), s[:cnt].tolist())), bp[:cnt], nn[:cnt], near)
+
+
+def test_cone_and_heightfield_contacts_match_reference():
+    """Cones and heightfields (scaled, rotated, one grid of a single row) against goldens from the reference's
+    ``sdf_cone``/``sdf_cone_grad`` and ``sample_sdf_grad_heightfield``."""
+    g = load_golden("soft_contact_cone_hfield.npz")
+    hf = dict(hf_index=g["shape_heightfield_index"], heightfields=g["heightfields"], elevations=g["elevations"])
+    gpu = _gpu_contacts(g["q"], g["radius"], g["flags"], g["shape_type"], g["shape_transform"], g["shape_scale"],
+                        float(g["margin"]), **hf)  # fmt: skip
+    near = set()
+    for s in range(len(g["shape_type"])):
+        one = dict(heightfield_index=g["shape_heightfield_index"][s:s + 1], heightfields=g["heightfields"],
+                   elevations=g["elevations"])  # fmt: skip
+        args = (g["q"], g["radius"], g["flags"], g["shape_type"][s:s + 1], g["shape_transform"][s:s + 1],
+                g["shape_scale"][s:s + 1])  # fmt: skip
+        loose = orc.soft_contacts_shapes(*args, float(g["margin"]) + 1e-5, **one)
+        tight = orc.soft_contacts_shapes(*args, float(g["margin"]) - 1e-5, **one)
+        near |= {(p, s) for p in set(loose[1][:loose[0]].tolist()) - set(tight[1][:tight[0]].tolist())}
+    pairs = list(zip(g["particle"].tolist(), g["shape"].tolist()))
+    _compare(gpu, pairs, g["body_pos"], g["normal"], near)
+    assert {s for _, s in gpu} == {0, 1, 2, 3, 4}
+
+
+def test_heightfield_arguments_are_checked():
+    """A heightfield without its grid table, an index out of range and a grid overrunning the elevations are
+    refused before any launch; the plain entry point refuses heightfields."""
+    lib = _lib.load()
+    dev = torch.device("cuda")
+    q = torch.zeros((4, 3), device=dev)
+    r = torch.full((4,), 0.01, device=dev)
+    fl = torch.ones(4, dtype=torch.int32, device=dev)
+    cnt = torch.zeros(1, dtype=torch.int32, device=dev)
+    oi = torch.zeros(64, dtype=torch.int32, device=dev)
+    of = torch.zeros((64, 3), device=dev)
+    ev = torch.zeros(12, device=dev)
+    ip, fp = C.POINTER(C.c_int32), C.POINTER(C.c_float)
+    st = np.array([2], dtype=np.int32)
+    sx = np.array([0, 0, 0, 0, 0, 0, 1], dtype=np.float32)
+    ss = np.ones(3, dtype=np.float32)
+
+    def call(idx, grids, n_elev):
+        hi = np.array([idx], dtype=np.int32)
+        hfs = (_lib.VbdHeightfield * max(len(grids), 1))(*grids)
+        return lib.vbd_soft_contacts_shapes_hf(4, q.data_ptr(), r.data_ptr(), fl.data_ptr(), 1, st.ctypes.data_as(ip),
+                                               sx.ctypes.data_as(fp), ss.ctypes.data_as(fp), hi.ctypes.data_as(ip),
+                                               len(grids), hfs, ev.data_ptr(), n_elev, 0.01, 64, cnt.data_ptr(),
+                                               oi.data_ptr(), oi.data_ptr(), of.data_ptr(), of.data_ptr(),
+                                               of.data_ptr(), None)  # fmt: skip
+
+    good = _lib.VbdHeightfield(0, 3, 4, 1.0, 1.0, 0.0, 1.0)
+    assert call(0, [good], 12) == _lib.VBD_OK
+    assert call(1, [good], 12) == _lib.VBD_ERR_INVALID_ARGUMENT
+    assert call(0, [good], 11) == _lib.VBD_ERR_INVALID_ARGUMENT
+    assert call(0, [_lib.VbdHeightfield(0, 3, 4, 0.0, 1.0, 0.0, 1.0)], 12) == _lib.VBD_ERR_INVALID_ARGUMENT
+    assert call(0, [], 12) == _lib.VBD_ERR_INVALID_ARGUMENT
+    rc = lib.vbd_soft_contacts_shapes(4, q.data_ptr(), r.data_ptr(), fl.data_ptr(), 1, st.ctypes.data_as(ip),
+                                      sx.ctypes.data_as(fp), ss.ctypes.data_as(fp), 0.01, 64, cnt.data_ptr(),
+                                      oi.data_ptr(), oi.data_ptr(), of.data_ptr(), of.data_ptr(), of.data_ptr(),
+                                      None)  # fmt: skip
+    assert rc == _lib.VBD_ERR_UNSUPPORTED
+    torch.cuda.synchronize()
+    assert int(cnt.item()) == 4  # the good call: all four particles lie on the flat grid (z = 0, inside the margin)
+
+
+def _terrain(n=33, seed=5):
+    gx, gy = np.meshgrid(np.linspace(-1.0, 1.0, n), np.linspace(-1.0, 1.0, n))
+    z = 0.05 * np.sin(3.0 * gx) * np.cos(2.0 * gy) + 0.01 * np.random.default_rng(seed).uniform(size=gx.shape)
+    return sim.Heightfield(z, n, n, hx=0.8, hy=0.8)
+
+
+def test_collision_pipeline_cone_heightfield_match_oracle():
+    b = sim.ModelBuilder()
+    rng = np.random.default_rng(4)
+    pts = np.stack([rng.uniform(-1.0, 1.0, 20000), rng.uniform(-1.0, 1.0, 20000), rng.uniform(-0.1, 0.6, 20000)], 1)
+    b.add_particles(pts, (0.0, 0.0, 0.0), 1.0, radius=0.01)
+    q = sim.quat_from_axis_angle((0.2, 1.0, 0.3), 0.6)
+    b.add_shape_heightfield(xform=((0.0, 0.0, 0.05), sim.quat_from_axis_angle((0.0, 0.0, 1.0), 0.4)),
+                            heightfield=_terrain(), scale=(1.0, 0.8, 1.5))  # fmt: skip
+    b.add_shape_cone(xform=((0.3, -0.2, 0.3), q), radius=0.2, half_height=0.25)
+    b.add_shape_cone(xform=((-0.4, 0.4, 0.35), sim.quat_identity()), radius=0.3, half_height=0.15)
+    model = b.finalize("cuda")
+    pipe = sim.CollisionPipeline(model, soft_contact_margin=0.01)
+    contacts = pipe.contacts()
+    pipe.collide(model.state(), contacts)
+    torch.cuda.synchronize()
+    k = int(contacts.soft_contact_count.item())
+    gpu = {(int(a), int(s)): (x, y, z) for a, s, x, y, z in zip(
+        contacts.soft_contact_particle[:k].cpu().numpy(), contacts.soft_contact_shape[:k].cpu().numpy(),
+        contacts.soft_contact_body_pos[:k].cpu().numpy(), contacts.soft_contact_body_vel[:k].cpu().numpy(),
+        contacts.soft_contact_normal[:k].cpu().numpy())}  # fmt: skip
+    qf = model.particle_q.cpu().numpy().astype(np.float64)
+    r = model.particle_radius.cpu().numpy().astype(np.float64)
+    fl = model.particle_flags.cpu().numpy()
+    args = (model.shape_type, model.shape_transform.astype(np.float64), model.shape_scale.astype(np.float64))
+    hf = dict(heightfield_index=model.shape_heightfield_index, heightfields=model.heightfield_data,
+              elevations=model.heightfield_elevations.cpu().numpy())  # fmt: skip
+    cnt, p, s, bp, _, nn = orc.soft_contacts_shapes(qf, r, fl, *args, 0.01, **hf)
+    lo = orc.soft_contacts_shapes(qf, r, fl, *args, 0.01 - 1e-5, **hf)
+    hi = orc.soft_contacts_shapes(qf, r, fl, *args, 0.01 + 1e-5, **hf)
+    near = set(zip(hi[1][:hi[0]].tolist(), hi[2][:hi[0]].tolist()))
+    near -= set(zip(lo[1][:lo[0]].tolist(), lo[2][:lo[0]].tolist()))
+    assert len(set(s[:cnt].tolist())) == model.shape_count
+    _compare(gpu, list(zip(p[:cnt].tolist(), s[:cnt].tolist())), bp[:cnt], nn[:cnt], near)
+
+
+def test_cloth_settles_on_heightfield():
+    """A cloth dropped on terrain through CollisionPipeline + SolverVBD comes to rest on it: after 0.5 s every
+    particle over the terrain has its centre above the plane of the terrain triangle under it, within 0.1 m of it,
+    and the device error word stays clear."""
+    from newton_chysx_b200 import SolverVBD
+
+    n, side = 24, 1.0
+    mu, lam = 1.0e4 * 1e-3 / 2.6, 1.0e4 * 1e-3 * 0.3 / 0.91
+    b = sim.ModelBuilder(gravity=-9.81)
+    b.add_cloth_grid(pos=(-0.5, -0.5, 0.25), rot=sim.quat_identity(), vel=(0.0, 0.0, 0.0), dim_x=n - 1, dim_y=n - 1,
+                     cell_x=side / (n - 1), cell_y=side / (n - 1), mass=0.2 / (n * n), tri_ke=mu, tri_ka=lam,
+                     tri_kd=0.0, edge_ke=1e-4, edge_kd=0.0, particle_radius=5e-3)  # fmt: skip
+    b.color(include_bending=True)
+    b.add_shape_heightfield(heightfield=_terrain())
+    model = b.finalize("cuda")
+    model.soft_contact_ke = 1.0e4
+    solver = SolverVBD(model, iterations=10)
+    pipe = sim.CollisionPipeline(model, soft_contact_margin=0.02)
+    contacts = pipe.contacts()
+    s0, s1 = model.state(), model.state()
+    for _ in range(300):
+        pipe.collide(s0, contacts)
+        solver.step(s0, s1, None, contacts, 1.0 / 600.0)
+        s0, s1 = s1, s0
+    torch.cuda.synchronize()
+    assert solver.device_errors() == 0
+    x = s0.particle_q.cpu().numpy().astype(np.float64)
+    assert np.isfinite(x).all()
+    # signed distance of every particle to its terrain triangle's plane, from the oracle's query with a wide margin
+    cnt, p, _, bp, _, nn = orc.soft_contacts_shapes(
+        x, np.zeros(len(x)), np.ones(len(x), np.int32), model.shape_type, model.shape_transform.astype(np.float64),
+        model.shape_scale.astype(np.float64), 1.0, heightfield_index=model.shape_heightfield_index,
+        heightfields=model.heightfield_data, elevations=model.heightfield_elevations.cpu().numpy())  # fmt: skip
+    assert cnt == len(x)
+    d = np.einsum("ij,ij->i", x[p[:cnt]] - bp[:cnt], nn[:cnt])
+    assert d.min() >= 0.0 and d.max() <= 0.1, (d.min(), d.max())

@@ -4,6 +4,7 @@ the reference's own SDF functions (``sdf_box``, ``sdf_capsule``, ``sdf_cylinder`
 ``create_soft_contacts``; and the builder's shape table in the reference's GeoType, transform and scale layout."""
 
 import numpy as np
+import pytest
 
 from newton_chysx_b200 import sim
 from oracle import vbd_oracle as orc
@@ -50,3 +51,43 @@ def test_builder_shape_table():
     ym = yb.finalize("cpu")
     np.testing.assert_allclose(sim.quat_to_matrix(ym.shape_transform[0, 3:]) @ [0, 0, 1], [0, 1, 0], atol=1e-6)
     np.testing.assert_allclose(ym.shape_transform[0, :3], [0.0, 0.1, 0.0], atol=1e-7)
+
+
+def test_oracle_cone_and_heightfield_contacts_match_reference():
+    """Cones (``sdf_cone``/``sdf_cone_grad``) and heightfields (``sample_sdf_grad_heightfield``, one of them
+    scaled with a negative Y scale, one a single row that gives no contacts) against goldens from the reference's
+    own functions."""
+    g = load_golden("soft_contact_cone_hfield.npz")
+    cnt, p, s, bp, bv, nn = orc.soft_contacts_shapes(
+        g["q"], g["radius"], g["flags"], g["shape_type"], g["shape_transform"], g["shape_scale"], float(g["margin"]),
+        heightfield_index=g["shape_heightfield_index"], heightfields=g["heightfields"], elevations=g["elevations"])
+    assert cnt == len(g["particle"]) and cnt > 1000
+    np.testing.assert_array_equal(p[:cnt], g["particle"])
+    np.testing.assert_array_equal(s[:cnt], g["shape"])
+    assert np.abs(bp[:cnt] - g["body_pos"]).max() <= 1e-12
+    assert np.abs(nn[:cnt] - g["normal"]).max() <= 1e-12
+    assert np.abs(bv[:cnt]).max() == 0.0
+    assert set(np.unique(g["shape"])) == {0, 1, 2, 3, 4}
+
+
+def test_builder_cone_and_heightfield_table():
+    """Cones store (radius, half height, 0); heightfields are packed as the reference's finalize packs them: extents
+    times |scale| in X and Y, min_z and max_z times the Z scale, normalized elevations concatenated."""
+    b = sim.ModelBuilder(up_axis="Z")
+    b.add_shape_cone(xform=((0.1, 0.2, 0.3), sim.quat_identity()), radius=0.4, half_height=0.25)
+    raw = np.arange(12, dtype=np.float32).reshape(3, 4) ** 2
+    hf = sim.Heightfield(raw, 3, 4, hx=0.5, hy=0.25)
+    assert hf.min_z == 0.0 and hf.max_z == 121.0 and hf.data.max() == 1.0 and hf.data.min() == 0.0
+    b.add_shape_heightfield(heightfield=hf, scale=(2.0, -1.0, 0.5))
+    b.add_shape_heightfield(heightfield=sim.Heightfield(np.ones((2, 2)), 2, 2, min_z=-1.0, max_z=1.0))
+    b.add_particle((0.0, 0.0, 0.0), (0.0, 0.0, 0.0), 1.0)
+    m = b.finalize("cpu")
+    assert list(m.shape_type) == [9, 2, 2]
+    np.testing.assert_allclose(m.shape_scale[0], [0.4, 0.25, 0.0])
+    assert list(m.shape_heightfield_index) == [-1, 0, 1]
+    np.testing.assert_allclose(m.heightfield_data[0], [0, 3, 4, 1.0, 0.25, 0.0, 60.5])
+    np.testing.assert_allclose(m.heightfield_data[1], [12, 2, 2, 1.0, 1.0, -1.0, 1.0])
+    np.testing.assert_allclose(m.heightfield_elevations.numpy()[:12], raw.reshape(-1) / 121.0, rtol=1e-6)
+    assert m.heightfield_elevations.numel() == 16 and float(m.heightfield_elevations[12:].abs().sum()) == 0.0
+    with pytest.raises(ValueError):
+        sim.Heightfield(np.zeros((1, 3)), 1, 3)
