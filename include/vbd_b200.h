@@ -370,7 +370,7 @@ int vbd_soft_contacts(int32_t particle_count, const float* q_dev, const float* r
    scale (width, length), 0 = infinite, else the reference's Chebyshev distance to the quad), 3 sphere (r),
    4 capsule (r, half height; along local Z), 5 ellipsoid (rx, ry, rz), 6 cylinder (r, half height; along local
    Z), 7 box (half extents), 9 cone (base radius, half height; base at local z = -half height, apex at
-   +half height); 2 (heightfield) needs vbd_soft_contacts_shapes_hf; other types (meshes, Gaussians) return
+   +half height); heightfields (2) and meshes (8, 10) need vbd_soft_contacts_table; other types return
    VBD_ERR_UNSUPPORTED. shape_transform_host [S,7]: position and
    rotation quaternion (x, y, z, w) of each shape; shape_scale_host [S,3]; at most 16 shapes. Contacts are
    written as vbd_soft_contacts writes them: the contact point on the surface in world (the body frame of a
@@ -395,20 +395,46 @@ typedef struct VbdHeightfield {
   float max_z;
 } VbdHeightfield;
 
-/* vbd_soft_contacts_shapes with heightfield shapes (GeoType 2, sample_sdf_grad_heightfield,
-   utils/heightfield.py:94-205): shape s of type 2 takes grid shape_heightfield_index_host[s] of
-   heightfields_host[heightfield_count]; elevations_dev holds elevation_count floats. Grids with nrow or ncol
-   below 2 give no contacts, as in the reference. Returns VBD_ERR_INVALID_ARGUMENT for an index out of range, a
-   grid that overruns elevation_count, or a non-positive or non-finite hx or hy (for which the reference's cell
-   index is undefined). */
-int vbd_soft_contacts_shapes_hf(int32_t particle_count, const float* q_dev, const float* radius_dev,
-                                const int32_t* flags_dev, int32_t shape_count, const int32_t* shape_type_host,
-                                const float* shape_transform_host, const float* shape_scale_host,
-                                const int32_t* shape_heightfield_index_host, int32_t heightfield_count,
-                                const VbdHeightfield* heightfields_host, const float* elevations_dev,
-                                int64_t elevation_count, float margin, int32_t soft_contact_max, int32_t* count_dev,
-                                int32_t* particle_dev, int32_t* shape_dev, float* body_pos_dev, float* body_vel_dev,
-                                float* normal_dev, void* stream);
+/* A static triangle mesh for particle contacts (GeoType 8 MESH and 10 CONVEX_MESH; the wp.Mesh the reference
+   builds from Mesh.vertices and Mesh.indices, geometry/types.py:1436-1453, with zero velocities). points_host
+   [point_count,3] in the mesh frame, indices_host [tri_count,3]. Builds a bounding-volume hierarchy and the
+   angle-weighted pseudo-normals that decide inside and outside on the host and uploads them (synchronous). */
+typedef struct VbdMeshImpl* VbdMeshHandle;
+int vbd_mesh_create(const float* points_host, int32_t point_count, const int32_t* indices_host, int32_t tri_count,
+                    VbdMeshHandle* out);
+int vbd_mesh_destroy(VbdMeshHandle mesh);
+
+/* The shapes a contact generation runs against, in the reference Model's layout (at most 16 shapes).
+   shape_type_host [S]: GeoType values; shape_transform_host [S,7]: position and rotation (x, y, z, w);
+   shape_scale_host [S,3]. Heightfield shape s (type 2) takes grid shape_heightfield_index_host[s] of
+   heightfields_host[heightfield_count] over elevations_dev (elevation_count floats). Mesh shape s (types 8 and
+   10) takes shape_mesh_host[s]; its scale must have no zero component. The arrays for a kind of shape may be
+   NULL when no shape of that kind is present. */
+typedef struct VbdShapeTable {
+  int32_t shape_count;
+  const int32_t* shape_type_host;
+  const float* shape_transform_host;
+  const float* shape_scale_host;
+  const int32_t* shape_heightfield_index_host;
+  int32_t heightfield_count;
+  const VbdHeightfield* heightfields_host;
+  const float* elevations_dev;
+  int64_t elevation_count;
+  const VbdMeshHandle* shape_mesh_host;
+} VbdShapeTable;
+
+/* vbd_soft_contacts_shapes over a full shape table: the analytic types, heightfields (sample_sdf_grad_heightfield,
+   utils/heightfield.py:94-205; grids with nrow or ncol below 2 give no contacts, as in the reference) and
+   triangle meshes (geometry/kernels.py:1091-1113: the particle in the mesh's unscaled frame, the closest point
+   within margin + radius / min|scale| and its pseudo-normal sign; distance and normal from the scaled closest
+   point). Returns VBD_ERR_INVALID_ARGUMENT for a heightfield index out of range, a grid that overruns
+   elevation_count, a non-positive or non-finite hx or hy (for which the reference's cell index is undefined),
+   a missing mesh handle or a mesh scale with a zero or non-finite component; VBD_ERR_UNSUPPORTED for Gaussians
+   and unknown types. */
+int vbd_soft_contacts_table(int32_t particle_count, const float* q_dev, const float* radius_dev,
+                            const int32_t* flags_dev, const VbdShapeTable* shapes, float margin,
+                            int32_t soft_contact_max, int32_t* count_dev, int32_t* particle_dev, int32_t* shape_dev,
+                            float* body_pos_dev, float* body_vel_dev, float* normal_dev, void* stream);
 
 #ifdef __cplusplus
 }

@@ -12,6 +12,7 @@ from .sim import (
     Control,
     GeoType,
     Heightfield,
+    Mesh,
     Model,
     ModelBuilder,
     ParticleFlags,
@@ -35,6 +36,7 @@ __all__ = [
     "Control",
     "GeoType",
     "Heightfield",
+    "Mesh",
     "Model",
     "ModelBuilder",
     "ParticleFlags",

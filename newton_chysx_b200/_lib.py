@@ -85,6 +85,15 @@ class VbdHeightfield(C.Structure):
                 ("hy", C.c_float), ("min_z", C.c_float), ("max_z", C.c_float)]  # fmt: skip
 
 
+class VbdShapeTable(C.Structure):
+    _fields_ = [
+        ("shape_count", C.c_int32), ("shape_type_host", _ip), ("shape_transform_host", _fp),
+        ("shape_scale_host", _fp), ("shape_heightfield_index_host", _ip), ("heightfield_count", C.c_int32),
+        ("heightfields_host", C.POINTER(VbdHeightfield)), ("elevations_dev", _vp), ("elevation_count", C.c_int64),
+        ("shape_mesh_host", C.POINTER(_vp)),
+    ]  # fmt: skip
+
+
 class VbdRefAdjacency(C.Structure):
     _fields_ = [("face_offsets_dev", _vp), ("faces_dev", _vp), ("edge_offsets_dev", _vp), ("edges_dev", _vp)]
 
@@ -145,11 +154,12 @@ SIGNATURES = {
         [C.c_int32, _vp, _vp, _vp, C.c_int32, _ip, _fp, _fp, C.c_float, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
         C.c_int,
     ),
-    "vbd_soft_contacts_shapes_hf": (
-        [C.c_int32, _vp, _vp, _vp, C.c_int32, _ip, _fp, _fp, _ip, C.c_int32, C.POINTER(VbdHeightfield), _vp,
-         C.c_int64, C.c_float, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "vbd_soft_contacts_table": (
+        [C.c_int32, _vp, _vp, _vp, C.POINTER(VbdShapeTable), C.c_float, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
         C.c_int,
     ),
+    "vbd_mesh_create": ([_fp, C.c_int32, _ip, C.c_int32, C.POINTER(_vp)], C.c_int),
+    "vbd_mesh_destroy": ([_vp], C.c_int),
     "vbd_soft_contacts": (
         [C.c_int32, _vp, _vp, _vp, C.c_int32, _ip, _fp, _fp, _fp, C.c_float, C.c_int32, _vp, _vp, _vp, _vp, _vp,
          _vp, _vp],

@@ -16,6 +16,7 @@
 
 #include "vbd_b200.h"
 #include "vbd_adjoint.cuh"
+#include "vbd_mesh.cuh"
 #include "vbd_collide.cuh"
 #include "vbd_ell.cuh"
 #include "vbd_ring.cuh"
@@ -138,6 +139,7 @@ struct ShapeXformTable {
   float4 sc[kMaxContactShapes];  // scale
   int4 hf[kMaxContactShapes];    // heightfields: (data_offset, nrow, ncol, 0)
   float4 hfe[kMaxContactShapes];  // heightfields: (hx, hy, min_z, max_z), scale applied
+  MeshView mesh[kMaxContactShapes];  // triangle meshes
 };
 
 __device__ __forceinline__ vec3<float> rot_q(float4 q, vec3<float> v) {
@@ -162,10 +164,25 @@ __global__ void k_soft_contacts_shapes(int n, const float* __restrict__ q, const
   const float sc[3] = {SC.x, SC.y, SC.z};
   float d;
   vec3<float> nn;
-  if (shapes.type[s] == GEO_HFIELD)
+  const int type = shapes.type[s];
+  if (type == GEO_HFIELD) {
     heightfield_sdf(shapes.hf[s], shapes.hfe[s], elev, xl, d, nn);
-  else
-    shape_sdf(shapes.type[s], xl, sc, d, nn);
+  } else if (type == GEO_MESH || type == GEO_CONVEX_MESH) {  // geometry/kernels.py:1091-1113
+    d = 1.0e6f;
+    nn = {0.f, 0.f, 0.f};
+    const float ms = fminf(fminf(fabsf(sc[0]), fabsf(sc[1])), fabsf(sc[2]));
+    const vec3<float> xs = {xl.x / sc[0], xl.y / sc[1], xl.z / sc[2]};
+    vec3<float> cp;
+    float sg;
+    int face;
+    if (mesh_query_point_sign(shapes.mesh[s], xs, margin + radius[i] / ms, cp, sg, face)) {
+      const vec3<float> delta = xl - vec3<float>{cp.x * sc[0], cp.y * sc[1], cp.z * sc[2]};
+      d = length(delta) * sg;
+      nn = geo_normalize(delta) * sg;
+    }
+  } else {
+    shape_sdf(type, xl, sc, d, nn);
+  }
   if (d < margin + radius[i]) {
     const int k = atomicAdd(count, 1);
     if (k < cmax) {
@@ -2102,51 +2119,57 @@ int vbd_soft_contacts(int32_t n, const float* q, const float* radius, const int3
   return VBD_OK;
 }
 
-int vbd_soft_contacts_shapes_hf(int32_t n, const float* q, const float* radius, const int32_t* flags, int32_t S,
-                                const int32_t* shape_type, const float* shape_transform, const float* shape_scale,
-                                const int32_t* shape_heightfield_index, int32_t heightfield_count,
-                                const VbdHeightfield* heightfields, const float* heightfield_elevations,
-                                int64_t elevation_count, float margin, int32_t cmax, int32_t* count, int32_t* particle,
-                                int32_t* shape, float* body_pos, float* body_vel, float* normal, void* stream) {
-  if (n < 0 || S < 0 || S > kMaxContactShapes || cmax < 0 || !count || heightfield_count < 0 || elevation_count < 0 ||
-      (S && (!shape_type || !shape_transform || !shape_scale)))
+int vbd_soft_contacts_table(int32_t n, const float* q, const float* radius, const int32_t* flags,
+                            const VbdShapeTable* tb, float margin, int32_t cmax, int32_t* count, int32_t* particle,
+                            int32_t* shape, float* body_pos, float* body_vel, float* normal, void* stream) {
+  if (!tb) return VBD_ERR_INVALID_ARGUMENT;
+  const int S = tb->shape_count;
+  if (n < 0 || S < 0 || S > kMaxContactShapes || cmax < 0 || !count || tb->heightfield_count < 0 ||
+      tb->elevation_count < 0 || (S && (!tb->shape_type_host || !tb->shape_transform_host || !tb->shape_scale_host)))
     return VBD_ERR_INVALID_ARGUMENT;
   if (n > 0 && S > 0 && (!q || !radius || !flags || (cmax > 0 && (!particle || !shape || !body_pos || !body_vel || !normal))))
     return VBD_ERR_INVALID_ARGUMENT;
   ShapeXformTable tab;
   std::memset(&tab, 0, sizeof(tab));
   for (int s = 0; s < S; ++s) {
-    const int t = shape_type[s];
+    const int t = tb->shape_type_host[s];
     if (t != GEO_PLANE && t != GEO_SPHERE && t != GEO_CAPSULE && t != GEO_ELLIPSOID && t != GEO_CYLINDER &&
-        t != GEO_BOX && t != GEO_CONE && t != GEO_HFIELD)
+        t != GEO_BOX && t != GEO_CONE && t != GEO_HFIELD && t != GEO_MESH && t != GEO_CONVEX_MESH)
       return VBD_ERR_UNSUPPORTED;
-    const float* X = shape_transform + 7 * s;
+    const float* X = tb->shape_transform_host + 7 * s;
+    const float* sc = tb->shape_scale_host + 3 * s;
     const float ql = std::sqrt(X[3] * X[3] + X[4] * X[4] + X[5] * X[5] + X[6] * X[6]);
     if (!(ql > 0.f)) return VBD_ERR_INVALID_ARGUMENT;
     tab.type[s] = t;
     tab.p[s] = make_float4(X[0], X[1], X[2], 0.f);
     tab.q[s] = make_float4(X[3] / ql, X[4] / ql, X[5] / ql, X[6] / ql);
-    tab.sc[s] = make_float4(shape_scale[3 * s], shape_scale[3 * s + 1], shape_scale[3 * s + 2], 0.f);
+    tab.sc[s] = make_float4(sc[0], sc[1], sc[2], 0.f);
     if (t == GEO_HFIELD) {  // every grid read of heightfield_sdf stays inside [data_offset, data_offset + nrow ncol)
-      if (!shape_heightfield_index || !heightfields) return VBD_ERR_INVALID_ARGUMENT;
-      const int k = shape_heightfield_index[s];
-      if (k < 0 || k >= heightfield_count) return VBD_ERR_INVALID_ARGUMENT;
-      const VbdHeightfield& h = heightfields[k];
+      if (!tb->shape_heightfield_index_host || !tb->heightfields_host) return VBD_ERR_INVALID_ARGUMENT;
+      const int k = tb->shape_heightfield_index_host[s];
+      if (k < 0 || k >= tb->heightfield_count) return VBD_ERR_INVALID_ARGUMENT;
+      const VbdHeightfield& h = tb->heightfields_host[k];
       if (h.nrow < 0 || h.ncol < 0 || h.data_offset < 0) return VBD_ERR_INVALID_ARGUMENT;
       if (h.nrow > 1 && h.ncol > 1) {
-        if (!heightfield_elevations || int64_t(h.data_offset) + int64_t(h.nrow) * h.ncol > elevation_count ||
+        if (!tb->elevations_dev || int64_t(h.data_offset) + int64_t(h.nrow) * h.ncol > tb->elevation_count ||
             !(h.hx > 0.f) || !(h.hy > 0.f) || !std::isfinite(h.hx) || !std::isfinite(h.hy))
           return VBD_ERR_INVALID_ARGUMENT;
       }
       tab.hf[s] = make_int4(h.data_offset, h.nrow, h.ncol, 0);
       tab.hfe[s] = make_float4(h.hx, h.hy, h.min_z, h.max_z);
     }
+    if (t == GEO_MESH || t == GEO_CONVEX_MESH) {
+      if (!tb->shape_mesh_host || !tb->shape_mesh_host[s]) return VBD_ERR_INVALID_ARGUMENT;
+      for (int k = 0; k < 3; ++k)
+        if (!(sc[k] != 0.f) || !std::isfinite(sc[k])) return VBD_ERR_INVALID_ARGUMENT;
+      tab.mesh[s] = tb->shape_mesh_host[s]->view;
+    }
   }
   cudaStream_t st = (cudaStream_t)stream;
   CK(cudaMemsetAsync(count, 0, sizeof(int), st));
   if (n == 0 || S == 0) return VBD_OK;
   const long total = long(n) * S;
-  k_soft_contacts_shapes<<<int((total + 255) / 256), 256, 0, st>>>(n, q, radius, flags, S, tab, heightfield_elevations,
+  k_soft_contacts_shapes<<<int((total + 255) / 256), 256, 0, st>>>(n, q, radius, flags, S, tab, tb->elevations_dev,
                                                                    margin, cmax, count, particle, shape, body_pos,
                                                                    body_vel, normal);
   CK(cudaGetLastError());
@@ -2157,11 +2180,17 @@ int vbd_soft_contacts_shapes(int32_t n, const float* q, const float* radius, con
                              const int32_t* shape_type, const float* shape_transform, const float* shape_scale,
                              float margin, int32_t cmax, int32_t* count, int32_t* particle, int32_t* shape,
                              float* body_pos, float* body_vel, float* normal, void* stream) {
-  for (int s = 0; s < S && shape_type; ++s)
-    if (shape_type[s] == GEO_HFIELD) return VBD_ERR_UNSUPPORTED;  // needs the grids: vbd_soft_contacts_shapes_hf
-  return vbd_soft_contacts_shapes_hf(n, q, radius, flags, S, shape_type, shape_transform, shape_scale, nullptr, 0,
-                                     nullptr, nullptr, 0, margin, cmax, count, particle, shape, body_pos, body_vel,
-                                     normal, stream);
+  for (int s = 0; s < S && shape_type; ++s)  // grids and meshes come with vbd_soft_contacts_table
+    if (shape_type[s] == GEO_HFIELD || shape_type[s] == GEO_MESH || shape_type[s] == GEO_CONVEX_MESH)
+      return VBD_ERR_UNSUPPORTED;
+  VbdShapeTable tb;
+  std::memset(&tb, 0, sizeof(tb));
+  tb.shape_count = S;
+  tb.shape_type_host = shape_type;
+  tb.shape_transform_host = shape_transform;
+  tb.shape_scale_host = shape_scale;
+  return vbd_soft_contacts_table(n, q, radius, flags, &tb, margin, cmax, count, particle, shape, body_pos, body_vel,
+                                 normal, stream);
 }
 
 int vbd_set_self_contact(VbdHandle h, const VbdSelfContactDesc* d) {

@@ -15,7 +15,9 @@ enum GeoTypeCode {
   GEO_ELLIPSOID = 5,
   GEO_CYLINDER = 6,
   GEO_BOX = 7,
-  GEO_CONE = 9
+  GEO_MESH = 8,
+  GEO_CONE = 9,
+  GEO_CONVEX_MESH = 10
 };
 
 __device__ __forceinline__ float geo_sign(float x) { return x < 0.f ? -1.f : 1.f; }  // wp.sign

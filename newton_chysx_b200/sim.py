@@ -700,6 +700,22 @@ class ModelBuilder:
         +half_height (``builder.py:6287-6340``)."""
         return self._add_shape(body, GeoType.CONE, xform, (radius, half_height, 0.0), cfg)
 
+    def add_shape_mesh(self, body=-1, xform=None, mesh: Mesh | None = None, scale=None,
+                       cfg: ShapeConfig | None = None):  # fmt: skip
+        """A static triangle mesh (``builder.py:6341-6380``); scale defaults to (1, 1, 1)."""
+        if mesh is None:
+            raise ValueError("add_shape_mesh() requires a Mesh instance.")
+        scale = (1.0, 1.0, 1.0) if scale is None else tuple(scale)
+        return self._add_shape(body, GeoType.MESH, xform, scale, cfg, src=mesh)
+
+    def add_shape_convex_hull(self, body=-1, xform=None, mesh: Mesh | None = None, scale=None,
+                              cfg: ShapeConfig | None = None):  # fmt: skip
+        """A static convex mesh (``builder.py:6382-6421``): the mesh given is taken as the hull."""
+        if mesh is None:
+            raise ValueError("add_shape_convex_hull() requires a Mesh instance.")
+        scale = (1.0, 1.0, 1.0) if scale is None else tuple(scale)
+        return self._add_shape(body, GeoType.CONVEX_MESH, xform, scale, cfg, src=mesh)
+
     def add_shape_heightfield(self, xform=None, heightfield: Heightfield | None = None, scale=None,
                               cfg: ShapeConfig | None = None):  # fmt: skip
         """A static heightfield (``builder.py:6423-6467``); scale (default (1, 1, 1)) multiplies hx, hy and
@@ -803,6 +819,39 @@ class Heightfield:
         return self._data
 
 
+class Mesh:
+    """A triangle mesh for collision (``newton/_src/geometry/types.py:131-190``, the collision part): vertices
+    [V, 3] and triangle indices [T, 3] (or flat), counter-clockwise seen from outside."""
+
+    def __init__(self, vertices, indices, normals=None, uvs=None, compute_inertia=True, is_solid=True, **_render):
+        del normals, uvs, compute_inertia, _render
+        self.vertices = np.asarray(vertices, dtype=np.float32).reshape(-1, 3)
+        self.indices = np.asarray(indices, dtype=np.int32).reshape(-1)
+        if len(self.indices) % 3 or (len(self.indices) and (self.indices.min() < 0 or
+                                                            self.indices.max() >= len(self.vertices))):
+            raise ValueError("Mesh indices must be triangles of vertex ids")
+        self.is_solid = is_solid
+
+
+class _DeviceMesh:
+    """A mesh's hierarchy and pseudo-normals on the GPU (``vbd_mesh_create``), freed with the model."""
+
+    def __init__(self, mesh: Mesh):
+        self._lib = _lib.load()
+        h = C.c_void_p()
+        pts = np.ascontiguousarray(mesh.vertices, dtype=np.float32)
+        idx = np.ascontiguousarray(mesh.indices, dtype=np.int32)
+        rc = self._lib.vbd_mesh_create(pts.ctypes.data_as(C.POINTER(C.c_float)), len(pts),
+                                       idx.ctypes.data_as(C.POINTER(C.c_int32)), len(idx) // 3, C.byref(h))  # fmt: skip
+        _lib.check(rc, "vbd_mesh_create")
+        self.handle = h.value
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            self._lib.vbd_mesh_destroy(self.handle)
+            self.handle = None
+
+
 # ----------------------------------------------------------------------------- model, state, contacts
 class Model:
     """Arrays of a finalized cloth model (the reference ``Model`` fields the VBD path reads)."""
@@ -892,6 +941,18 @@ class Model:
                 off += hf.nrow * hf.ncol
         m.heightfield_data = np.array(rows, dtype=np.float64).reshape(-1, 7)
         m.heightfield_elevations = t(np.concatenate(chunks) if chunks else np.zeros(1, np.float32), f32)
+        # triangle meshes: one device hierarchy per distinct Mesh (the reference's Mesh.finalize, one wp.Mesh each)
+        m.shape_mesh_index = np.full(S, -1, dtype=np.int32)
+        m.meshes, m._device_meshes, seen = [], [], {}
+        for i, sh in enumerate(b.shapes):
+            if sh["type"] in (GeoType.MESH, GeoType.CONVEX_MESH) and sh.get("src") is not None:
+                key = id(sh["src"])
+                if key not in seen:
+                    seen[key] = len(m.meshes)
+                    m.meshes.append(sh["src"])
+                    if dev.type == "cuda":
+                        m._device_meshes.append(_DeviceMesh(sh["src"]))
+                m.shape_mesh_index[i] = seen[key]
         m.body_com = None
         return m
 
@@ -972,12 +1033,13 @@ class Contacts:
 
 
 def soft_contacts(model: Model, state: State, contacts: Contacts, margin: float):
-    """Particle contacts against the model's static shapes on the GPU (``vbd_soft_contacts_shapes_hf``)."""
+    """Particle contacts against the model's static shapes on the GPU (``vbd_soft_contacts_table``)."""
     lib = _lib.load()
     S = model.shape_count
     if S == 0:
         contacts.soft_contact_count.zero_()
         return
+    ip, fp = C.POINTER(C.c_int32), C.POINTER(C.c_float)
     st = np.ascontiguousarray(model.shape_type, dtype=np.int32)
     sx = np.ascontiguousarray(model.shape_transform, dtype=np.float32)
     ss = np.ascontiguousarray(model.shape_scale, dtype=np.float32)
@@ -987,23 +1049,28 @@ def soft_contacts(model: Model, state: State, contacts: Contacts, margin: float)
     for k, r in enumerate(rows):
         hfs[k] = _lib.VbdHeightfield(int(r[0]), int(r[1]), int(r[2]), *(float(v) for v in r[3:]))
     elev = getattr(model, "heightfield_elevations", None)
-    ip, fp = C.POINTER(C.c_int32), C.POINTER(C.c_float)
+    midx = getattr(model, "shape_mesh_index", np.full(S, -1))
+    dmeshes = getattr(model, "_device_meshes", [])
+    handles = (C.c_void_p * S)(*[dmeshes[k].handle if k >= 0 else None for k in midx])
+    tb = _lib.VbdShapeTable(
+        S, st.ctypes.data_as(ip), sx.ctypes.data_as(fp), ss.ctypes.data_as(fp), hidx.ctypes.data_as(ip), len(rows),
+        hfs, None if elev is None else elev.data_ptr(), 0 if elev is None else elev.numel(),
+        C.cast(handles, C.POINTER(C.c_void_p)),
+    )  # fmt: skip
     stream = torch.cuda.current_stream(model.device).cuda_stream
-    rc = lib.vbd_soft_contacts_shapes_hf(
+    rc = lib.vbd_soft_contacts_table(
         model.particle_count, state.particle_q.data_ptr(), model.particle_radius.data_ptr(),
-        model.particle_flags.data_ptr(), S, st.ctypes.data_as(ip), sx.ctypes.data_as(fp), ss.ctypes.data_as(fp),
-        hidx.ctypes.data_as(ip), len(rows), hfs, None if elev is None else elev.data_ptr(),
-        0 if elev is None else elev.numel(), float(margin), contacts.soft_contact_max,
+        model.particle_flags.data_ptr(), C.byref(tb), float(margin), contacts.soft_contact_max,
         contacts.soft_contact_count.data_ptr(), contacts.soft_contact_particle.data_ptr(),
         contacts.soft_contact_shape.data_ptr(), contacts.soft_contact_body_pos.data_ptr(),
         contacts.soft_contact_body_vel.data_ptr(), contacts.soft_contact_normal.data_ptr(), C.c_void_p(stream),
     )  # fmt: skip
-    _lib.check(rc, "vbd_soft_contacts_shapes_hf")
+    _lib.check(rc, "vbd_soft_contacts_table")
 
 
 class CollisionPipeline:
     """Particle-shape part of ``newton/_src/sim/collide.py:485`` (static planes, heightfields, spheres, boxes,
-    capsules, cylinders, cones and ellipsoids)."""
+    capsules, cylinders, cones, ellipsoids and triangle meshes)."""
 
     def __init__(self, model: Model, soft_contact_max=None, soft_contact_margin=0.01, **_ignored):
         self.model = model

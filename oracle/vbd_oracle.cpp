@@ -1238,7 +1238,7 @@ int step(const Model& M, double* q_in, const double* qd_in, const double* f_ext,
 // contact point x_local - n d and the normal mapped back to world. Contacts in particle-major order.
 namespace sdf {
 using D3 = V3<double>;
-enum { PLANE = 1, HFIELD = 2, SPHERE = 3, CAPSULE = 4, ELLIPSOID = 5, CYLINDER = 6, BOX = 7, CONE = 9 };
+enum { PLANE = 1, HFIELD = 2, SPHERE = 3, CAPSULE = 4, ELLIPSOID = 5, CYLINDER = 6, BOX = 7, MESH = 8, CONE = 9, CONVEX_MESH = 10 };
 inline double sgn(double x) { return x < 0.0 ? -1.0 : 1.0; }  // wp.sign: -1 below zero, 1 otherwise
 inline D3 qrot(const double* q, D3 v) {  // q = (x, y, z, w)
   const D3 u = v3(q[0], q[1], q[2]);
@@ -1372,6 +1372,56 @@ inline void heightfield(const int* g, const double* e, const double* elev, D3 p,
   } else {
     d = dp, n = nrm;
   }
+}
+// Triangle meshes (geometry/kernels.py:1091-1113 through wp.mesh_query_point_sign_normal, which is Warp-native):
+// the closest point over all triangles (brute force; ties keep the lowest triangle) closer than max_dist, and the
+// sign from the angle-weighted pseudo-normal of its feature (Baerentzen and Aanaes, IEEE TVCG 11(3), 2005): the
+// face normal inside a triangle, the sum of the faces' unit normals on an edge, the angle-weighted sum at a vertex.
+struct MeshQ {
+  int V, T;
+  const double* pts;
+  const int* tri;
+};
+inline D3 mpt(const MeshQ& m, int v) { return v3(m.pts[3 * v], m.pts[3 * v + 1], m.pts[3 * v + 2]); }
+inline D3 face_normal(const MeshQ& m, int t) {
+  const D3 a = mpt(m, m.tri[3 * t]), b = mpt(m, m.tri[3 * t + 1]), c = mpt(m, m.tri[3 * t + 2]);
+  return normalize0(cross(b - a, c - a));
+}
+inline bool mesh_query(const MeshQ& m, D3 p, double max_dist, D3& cp, double& sign) {
+  double best = max_dist * max_dist;
+  int bt = -1, feat = 6;
+  for (int t = 0; t < m.T; ++t) {
+    double w[3];
+    int f;
+    const D3 c = tri_closest(mpt(m, m.tri[3 * t]), mpt(m, m.tri[3 * t + 1]), mpt(m, m.tri[3 * t + 2]), p, w, f);
+    const double d2 = dot(c - p, c - p);
+    if (d2 < best) best = d2, bt = t, feat = f, cp = c;
+  }
+  if (bt < 0) return false;
+  D3 pn = v3(0.0, 0.0, 0.0);
+  const int* tv = m.tri + 3 * bt;
+  if (feat == 6) {
+    pn = face_normal(m, bt);
+  } else if (feat >= 3) {  // edge AB, AC or BC: every face holding both ends
+    const int e0 = feat == 5 ? tv[1] : tv[0], e1 = feat == 3 ? tv[1] : tv[2];
+    for (int t = 0; t < m.T; ++t) {
+      const int* u = m.tri + 3 * t;
+      const bool h0 = u[0] == e0 || u[1] == e0 || u[2] == e0, h1 = u[0] == e1 || u[1] == e1 || u[2] == e1;
+      if (h0 && h1) pn = pn + face_normal(m, t);
+    }
+  } else {  // vertex: incident faces weighted by their angle there
+    const int v = tv[feat];
+    for (int t = 0; t < m.T; ++t) {
+      const int* u = m.tri + 3 * t;
+      for (int k = 0; k < 3; ++k)
+        if (u[k] == v) {
+          const D3 x = mpt(m, u[k]), e1 = mpt(m, u[(k + 1) % 3]) - x, e2 = mpt(m, u[(k + 2) % 3]) - x;
+          pn = pn + face_normal(m, t) * std::atan2(length(cross(e1, e2)), dot(e1, e2));
+        }
+    }
+  }
+  sign = dot(p - cp, pn) < 0.0 ? -1.0 : 1.0;
+  return true;
 }
 // :568-589
 inline double plane(D3 p, double w, double l) {
@@ -1774,15 +1824,19 @@ int oracle_soft_contacts(int n, const double* q, const double* radius, const int
 int oracle_soft_contacts_shapes(int n, const double* q, const double* radius, const int* flags, int S,
                                 const int* shape_type, const double* shape_xform, const double* shape_scale,
                                 const int* hf_index, const int* hf_grid, const double* hf_ext, const double* elev,
-                                double margin, int max_contacts, int* particle, int* shape, double* body_pos,
-                                double* body_vel, double* normal) {
+                                const int* mesh_index, const int* mesh_vert_off, const int* mesh_tri_off,
+                                const double* mesh_pts, const int* mesh_tris, double margin, int max_contacts,
+                                int* particle, int* shape, double* body_pos, double* body_vel, double* normal) {
   using sdf::D3;
   for (int s = 0; s < S; ++s) {
     const int t = shape_type[s];
     if (t != sdf::PLANE && t != sdf::SPHERE && t != sdf::CAPSULE && t != sdf::ELLIPSOID && t != sdf::CYLINDER &&
-        t != sdf::BOX && t != sdf::CONE && t != sdf::HFIELD)
+        t != sdf::BOX && t != sdf::CONE && t != sdf::HFIELD && t != sdf::MESH && t != sdf::CONVEX_MESH)
       return -1;
     if (t == sdf::HFIELD && (!hf_index || !hf_grid || !hf_ext || !elev)) return -1;
+    if ((t == sdf::MESH || t == sdf::CONVEX_MESH) && (!mesh_index || !mesh_vert_off || !mesh_tri_off || !mesh_pts ||
+                                                       !mesh_tris))
+      return -1;
   }
   int count = 0;
   for (int i = 0; i < n; ++i) {
@@ -1805,6 +1859,21 @@ int oracle_soft_contacts_shapes(int n, const double* q, const double* radius, co
         case sdf::HFIELD: {
           const int k = hf_index[s];
           sdf::heightfield(hf_grid + 3 * k, hf_ext + 4 * k, elev, xl, d, nn);
+          break;
+        }
+        case sdf::MESH:
+        case sdf::CONVEX_MESH: {  // the query in the unscaled frame; distance and normal from the scaled point
+          const int k = mesh_index[s];
+          const sdf::MeshQ m{mesh_vert_off[k + 1] - mesh_vert_off[k], mesh_tri_off[k + 1] - mesh_tri_off[k],
+                             mesh_pts + 3 * mesh_vert_off[k], mesh_tris + 3 * mesh_tri_off[k]};
+          const double ms = std::min(std::min(std::fabs(sc[0]), std::fabs(sc[1])), std::fabs(sc[2]));
+          D3 cp;
+          double sg;
+          if (sdf::mesh_query(m, v3(xl.x / sc[0], xl.y / sc[1], xl.z / sc[2]), margin + radius[i] / ms, cp, sg)) {
+            const D3 delta = xl - v3(cp.x * sc[0], cp.y * sc[1], cp.z * sc[2]);
+            d = length(delta) * sg;
+            nn = sdf::normalize0(delta) * sg;
+          }
           break;
         }
         default: d = sdf::plane(xl, sc[0] * 0.5, sc[1] * 0.5), nn = v3(0.0, 0.0, 1.0); break;

@@ -140,3 +140,70 @@ def cloth_grid_builder(n=32, side=1.0, E=1e4, nu=0.3, h=1e-3, density=0.2, bend=
         b.set_particle_flags(flags)
     b.color(include_bending=True)
     return b
+
+
+def _outward(v, tris, inside_point_fn):
+    """Flip triangles whose normal points toward `inside_point_fn(centroid)` (a point inside the solid)."""
+    a, b, c = v[tris[:, 0]], v[tris[:, 1]], v[tris[:, 2]]
+    n = np.cross(b - a, c - a)
+    cen = (a + b + c) / 3.0
+    flip = np.einsum("ij,ij->i", n, cen - inside_point_fn(cen)) < 0.0
+    tris = tris.copy()
+    tris[flip] = tris[flip][:, [0, 2, 1]]
+    return tris
+
+
+def box_mesh(hx, hy, hz):
+    """A closed box of half extents (hx, hy, hz): 8 vertices, 12 triangles wound counter-clockwise from outside."""
+    v = np.array([[(-hx, hx)[i & 1], (-hy, hy)[(i >> 1) & 1], (-hz, hz)[(i >> 2) & 1]] for i in range(8)])
+    tris = []
+    for k in range(3):
+        for side in (0, 1):
+            ids = [i for i in range(8) if ((i >> k) & 1) == side]  # 4 corners, in bit order
+            tris += [[ids[0], ids[1], ids[3]], [ids[0], ids[3], ids[2]]]
+    return v, _outward(v, np.array(tris), lambda c: np.zeros_like(c))
+
+
+def icosphere(radius=1.0, subdivisions=2):
+    t = (1.0 + 5.0**0.5) / 2.0
+    v = [[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t], [t, 0, -1],
+         [t, 0, 1], [-t, 0, -1], [-t, 0, 1]]  # fmt: skip
+    f = [[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2], [10, 7, 6],
+         [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5], [2, 4, 11], [6, 2, 10],
+         [8, 6, 7], [9, 8, 1]]  # fmt: skip
+    v = [np.asarray(p, dtype=np.float64) / np.linalg.norm(p) for p in v]
+    for _ in range(subdivisions):
+        mid, nf = {}, []
+
+        def m(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in mid:
+                p = v[a] + v[b]
+                v.append(p / np.linalg.norm(p))
+                mid[key] = len(v) - 1
+            return mid[key]
+
+        for a, b, c in f:
+            ab, bc, ca = m(a, b), m(b, c), m(c, a)
+            nf += [[a, ab, ca], [b, bc, ab], [c, ca, bc], [ab, bc, ca]]
+        f = nf
+    v = np.array(v) * radius
+    return v, _outward(v, np.array(f), lambda c: np.zeros_like(c))
+
+
+def torus_mesh(R=0.3, r=0.1, nu=24, nv=12):
+    """A closed torus around the Z axis (tube radius r at distance R): non-convex, genus one."""
+    u, w = np.meshgrid(np.arange(nu) * 2 * np.pi / nu, np.arange(nv) * 2 * np.pi / nv, indexing="ij")
+    v = np.stack([(R + r * np.cos(w)) * np.cos(u), (R + r * np.cos(w)) * np.sin(u), r * np.sin(w)], -1).reshape(-1, 3)
+    tris = []
+    for i in range(nu):
+        for j in range(nv):
+            a, b = i * nv + j, ((i + 1) % nu) * nv + j
+            c, d = ((i + 1) % nu) * nv + (j + 1) % nv, i * nv + (j + 1) % nv
+            tris += [[a, b, c], [a, c, d]]
+
+    def tube_centre(c):
+        ang = np.arctan2(c[:, 1], c[:, 0])
+        return np.stack([R * np.cos(ang), R * np.sin(ang), np.zeros(len(c))], -1)
+
+    return v, _outward(v, np.array(tris), tube_centre)

@@ -239,13 +239,15 @@ def test_instance_per_warp_needs_csr_persistent():
 
 def test_damped_soft_block_falls_freely():
     """The pattern of test_cloth.py:1026-1076 for volumetric elements: a tetrahedral block with tet damping and a
-    damped spring between two of its corners, released at rest, falls as free particles (elastic and damping
-    forces stay zero under a uniform translation)."""
+    spring between two of its corners, released at rest, falls as free particles (elastic and damping forces stay
+    zero under a uniform translation). The spring is undamped: the reference's spring damping acts on each end's
+    own displacement, h_d (x_prev - x) (particle_vbd_kernels.py:2288-2290), so a damped spring slows the fall
+    (by 8.9 mm here in the oracle as on the GPU)."""
     b = sim.ModelBuilder(up_axis="Z", gravity=-9.81)
-    b.add_soft_grid(pos=(0.0, 0.0, 2.0), rot=sim.quat_identity(), vel=(0.0, 0.0, 0.0), dim_x=3, dim_y=2, dim_z=2,
+    b.add_soft_grid(pos=(0.0, 0.0, 0.25), rot=sim.quat_identity(), vel=(0.0, 0.0, 0.0), dim_x=3, dim_y=2, dim_z=2,
                     cell_x=0.05, cell_y=0.05, cell_z=0.05, density=500.0, k_mu=2.0e4, k_lambda=3.0e4, k_damp=1.0e-2,
                     tri_ke=10.0, tri_ka=10.0, tri_kd=1e-2, edge_ke=1e-2, edge_kd=1e-3)  # fmt: skip
-    b.add_spring(0, b.particle_count - 1, 100.0, 1.0, 0.0)
+    b.add_spring(0, b.particle_count - 1, 100.0, 0.0, 0.0)
     b.color()
     model = b.finalize("cuda")
     solver = SolverVBD(model, iterations=5)
@@ -258,7 +260,8 @@ def test_damped_soft_block_falls_freely():
     torch.cuda.synchronize()
     diff = (s0.particle_q - q0).cpu().numpy()
     expected = -9.81 * dt * dt * n * (n + 1) / 2  # implicit Euler
-    # FP32 positions near z = 2 m carry ~2e-7 m of rounding per substep
-    assert np.abs(diff[:, 2] - expected).max() <= 1e-3 * abs(expected) + 1e-5
+    # FP32 positions near z = 0.3 m round by up to 1.5e-8 m per substep; every particle moves alike, so the
+    # rounding biases the velocity the same way each step and adds up to about n^2 / 2 * 1.5e-8 = 2.7e-5 m
+    assert np.abs(diff[:, 2] - expected).max() <= 1e-4
     assert np.abs(diff[:, :2]).max() <= 1e-5
     assert solver.device_errors() & ~4 == 0

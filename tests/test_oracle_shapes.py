@@ -91,3 +91,53 @@ def test_builder_cone_and_heightfield_table():
     assert m.heightfield_elevations.numel() == 16 and float(m.heightfield_elevations[12:].abs().sum()) == 0.0
     with pytest.raises(ValueError):
         sim.Heightfield(np.zeros((1, 3)), 1, 3)
+
+
+def test_oracle_box_mesh_matches_reference_box_sdf():
+    """A closed box mesh through the mesh query (closest point + pseudo-normal sign) gives the reference's own
+    ``sdf_box``/``sdf_box_grad`` contacts: outside, the closest point of a box is the clamped point; inside, the
+    nearest face. The mesh carries half the box's extents at scale 2, so the scaled path is exercised. A mesh
+    query only searches margin + radius / min|scale| around the surface (in the mesh's unscaled frame), so particles
+    deeper inside than that have no mesh contact, as in the reference; the comparison covers the rest."""
+    from tests.helpers import box_mesh
+
+    g = load_golden("soft_contact_shapes.npz")
+    s = int(np.flatnonzero(g["shape_type"] == 7)[0])
+    v, tris = box_mesh(*(0.5 * g["shape_scale"][s]))
+    cnt, p, _, bp, bv, nn = orc.soft_contacts_shapes(
+        g["q"], g["radius"], g["flags"], np.array([8]), g["shape_transform"][s:s + 1], np.array([[2.0, 2.0, 2.0]]),
+        float(g["margin"]), mesh_index=[0], meshes=[(v, tris)])  # fmt: skip
+    reach = 2.0 * (float(g["margin"]) + g["radius"][g["particle"]] / 2.0)
+    sel = (g["shape"] == s) & (g["distance"] > -reach)
+    assert cnt == sel.sum() and cnt > 100 and ((g["shape"] == s) & ~sel).sum() > 0
+    np.testing.assert_array_equal(p[:cnt], g["particle"][sel])
+    assert np.abs(bp[:cnt] - g["body_pos"][sel]).max() <= 1e-12
+    assert np.abs(nn[:cnt] - g["normal"][sel]).max() <= 1e-12
+    assert np.abs(bv[:cnt]).max() == 0.0
+
+
+def test_oracle_mesh_sign_and_distance():
+    """Icosphere: distances within the tessellation error of the sphere's, inside negative. Torus (non-convex):
+    points in the tube are inside, points in the hole and outside are outside."""
+    from tests.helpers import icosphere, torus_mesh
+
+    rng = np.random.default_rng(2)
+    v, f = icosphere(0.5, 3)
+    q = rng.normal(size=(400, 3))
+    q *= (rng.uniform(0.3, 0.7, 400) / np.linalg.norm(q, axis=1))[:, None]
+    ident = np.array([[0, 0, 0, 0, 0, 0, 1.0]])
+    cnt, p, _, bp, _, nn = orc.soft_contacts_shapes(q, np.zeros(400), np.ones(400, np.int32), np.array([8]), ident,
+                                                    np.ones((1, 3)), 1.0, mesh_index=[0], meshes=[(v, f)])  # fmt: skip
+    assert cnt == 400
+    d = np.einsum("ij,ij->i", q[p[:cnt]] - bp[:cnt], nn[:cnt])
+    exact = np.linalg.norm(q[p[:cnt]], axis=1) - 0.5
+    far = np.abs(exact) > 0.003  # the facets lie up to ~2.3 mm inside the sphere at this tessellation
+    assert np.abs(d - exact).max() < 0.003 and ((d < 0) == (exact < 0))[far].all() and far.sum() > 300
+    v, f = torus_mesh(0.3, 0.1)
+    pts = np.array([[0.3, 0.0, 0.0], [0.0, -0.32, 0.02], [0.0, 0.0, 0.0], [0.5, 0.0, 0.0], [0.3, 0.0, 0.15]])
+    cnt, p, _, bp, _, nn = orc.soft_contacts_shapes(pts, np.zeros(5), np.ones(5, np.int32), np.array([8]), ident,
+                                                    np.ones((1, 3)), 1.0, mesh_index=[0], meshes=[(v, f)])  # fmt: skip
+    assert cnt == 5
+    d = np.einsum("ij,ij->i", pts[p[:cnt]] - bp[:cnt], nn[:cnt])
+    assert (d[:2] < 0).all() and (d[2:] > 0).all()
+    np.testing.assert_allclose(d[[0, 2, 3, 4]], [-0.1, 0.2, 0.1, 0.05], atol=0.01)
