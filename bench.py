@@ -853,6 +853,137 @@ def cpu_baseline_soft(sample_worlds=256, seconds=10.0):
             "sample": f"{n} substeps of {sample_worlds} blocks of the same workload (contacts of the first substep)"}  # fmt: skip
 
 
+def build_contact_scene(dev, n_particles, seed=7):
+    """Particles spread over 2 m x 2 m x 0.8 m above nine static shapes, one of every kind the contact generator
+    handles: ground plane, sphere, box, capsule, cone, ellipsoid, a 257 x 257 heightfield, an icosphere mesh
+    (1,280 triangles, non-uniform scale) and a torus mesh (576 triangles, rotated)."""
+    import numpy as np
+
+    import newton_chysx_b200 as nb
+    from tests.helpers import icosphere, torus_mesh
+
+    rng = np.random.default_rng(seed)
+    b = nb.ModelBuilder(up_axis="Z")
+    pts = np.stack([rng.uniform(-1.0, 1.0, n_particles), rng.uniform(-1.0, 1.0, n_particles),
+                    rng.uniform(-0.05, 0.75, n_particles)], 1)  # fmt: skip
+    b.add_particles(pts, (0.0, 0.0, 0.0), 1.0, radius=0.005)
+    q = nb.quat_from_axis_angle((0.2, 1.0, 0.3), 0.6)
+    b.add_ground_plane()
+    b.add_shape_sphere(xform=((0.5, 0.5, 0.3), nb.quat_identity()), radius=0.2)
+    b.add_shape_box(xform=((-0.5, -0.5, 0.3), q), hx=0.2, hy=0.15, hz=0.1)
+    b.add_shape_capsule(xform=((0.0, 0.6, 0.35), q), radius=0.08, half_height=0.2)
+    b.add_shape_cone(xform=((-0.6, 0.4, 0.3), nb.quat_identity()), radius=0.2, half_height=0.2)
+    b.add_shape_ellipsoid(xform=((0.6, -0.1, 0.5), q), rx=0.2, ry=0.15, rz=0.1)
+    g = np.linspace(-1.0, 1.0, 257)
+    gx, gy = np.meshgrid(g, g)
+    b.add_shape_heightfield(xform=((0.0, 0.0, 0.05), nb.quat_identity()),
+                            heightfield=nb.Heightfield(0.05 * np.sin(4 * gx) * np.cos(3 * gy), 257, 257, 1.0, 1.0))
+    b.add_shape_mesh(xform=((0.1, -0.5, 0.3), nb.quat_identity()), mesh=nb.Mesh(*icosphere(0.2, 3)),
+                     scale=(1.2, 1.0, 0.8))  # fmt: skip
+    b.add_shape_mesh(xform=((-0.1, 0.0, 0.4), q), mesh=nb.Mesh(*torus_mesh(0.25, 0.06)))
+    return b.finalize(dev)
+
+
+def run_contacts(args):
+    """Particle-shape contact generation (CollisionPipeline.collide -> vbd_soft_contacts_table): --contact-particles
+    particles (default 8M) against nine shapes of every kind. One launch tests every (particle, shape) pair; the
+    metric is pair tests per second. Algorithmic DRAM bytes per launch: each particle's position, radius and flags
+    read once (20 B) plus each contact written (particle and shape ids, point, velocity, normal: 44 B); the mesh
+    and heightfield queries are arithmetic- and gather-bound, which the roofline fraction shows."""
+    import torch
+
+    import newton_chysx_b200 as nb
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    N = args.contact_particles
+    t0 = time.perf_counter()
+    m = build_contact_scene(dev, N)
+    build_s = time.perf_counter() - t0
+    S = m.shape_count
+    pipe = nb.CollisionPipeline(m, soft_contact_max=N, soft_contact_margin=0.01)
+    contacts = pipe.contacts()
+    state = m.state()
+    for _ in range(args.warmup):
+        pipe.collide(state, contacts)
+    torch.cuda.synchronize()
+    K = args.steps
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index or 0) as clk:
+        e0.record()
+        for _ in range(K):
+            pipe.collide(state, contacts)
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / K
+    count = int(contacts.soft_contact_count.item())
+    pairs = N * S
+    alg = 20 * N + 44 * min(count, N)
+    peak, peak_src = _peaks()
+    achieved = alg / (ms * 1e-3) / 1e9
+    out = {
+        "metric": "particle-shape contact pair tests/s on 1 B200 (contact generation for the VBD step)",
+        "value": pairs / (ms * 1e-3), "unit": "pairs/s", "n_gpus": 1, "steps": K, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded particles over nine analytic, heightfield and mesh shapes)",
+        "config": {"workload": f"{N} particles x {S} static shapes (plane, sphere, box, capsule, cone, ellipsoid, "
+                               "257x257 heightfield, 1280- and 576-triangle meshes)",
+                   "particles": N, "shapes": S, "contacts_found": count, "margin": 0.01, "build_s": round(build_s, 1),
+                   "l2": f"inputs {20 * N / 1e6:.0f} MB > L2, no flush"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_source": peak_src, "algorithmic_bytes_per_launch": alg,
+                     "note": "one thread per (particle, shape): mesh BVH and heightfield queries make it "
+                             "arithmetic- and gather-bound"},
+        "gpu_launches": K, "clocks": clk.summary(),
+    }  # fmt: skip
+    if not args.no_e2e:
+        hq = state.particle_q.cpu().pin_memory()
+        hc = torch.empty(1, dtype=torch.int32).pin_memory()
+        hn = torch.empty_like(contacts.soft_contact_normal, device="cpu").pin_memory()
+        hp = torch.empty_like(contacts.soft_contact_particle, device="cpu").pin_memory()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(K):
+            state.particle_q.copy_(hq, non_blocking=True)
+            pipe.collide(state, contacts)
+            hc.copy_(contacts.soft_contact_count, non_blocking=True)
+            hp.copy_(contacts.soft_contact_particle, non_blocking=True)
+            hn.copy_(contacts.soft_contact_normal, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        ms_e = e0.elapsed_time(e1) / K
+        out["e2e"] = {"value": pairs / (ms_e * 1e-3), "unit": "pairs/s", "h2d_bytes_per_step": hq.numel() * 4,
+                      "d2h_bytes_per_step": 4 + hp.numel() * 4 + hn.numel() * 4, "steps": K}  # fmt: skip
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_contacts(m, seconds=min(args.cpu_seconds, 10.0))
+    return out
+
+
+def cpu_baseline_contacts(m, seconds=10.0):
+    """The oracle's contact generation (one host thread, a serial loop over particles and shapes) on leading
+    slices of the same particles, grown until `seconds` have passed."""
+    import numpy as np
+
+    from oracle import vbd_oracle as orc
+
+    q = m.particle_q.double().cpu().numpy()
+    r = m.particle_radius.double().cpu().numpy()
+    fl = m.particle_flags.cpu().numpy()
+    args = (m.shape_type, m.shape_transform.astype(np.float64), m.shape_scale.astype(np.float64))
+    kw = dict(heightfield_index=m.shape_heightfield_index, heightfields=m.heightfield_data,
+              elevations=m.heightfield_elevations.cpu().numpy(), mesh_index=m.shape_mesh_index,
+              meshes=[(x.vertices, x.indices) for x in m.meshes])  # fmt: skip
+    n, done, t = 2048, 0, time.perf_counter()
+    while time.perf_counter() - t < seconds and n <= len(r):
+        orc.soft_contacts_shapes(q[:n], r[:n], fl[:n], *args, 0.01, max_contacts=n, **kw)
+        done += n
+        n *= 2
+    el = time.perf_counter() - t
+    return {"value": done * m.shape_count / el, "unit": "pairs/s", "cores": 1, "kind": "port",
+            "sample": f"{done} particles x {m.shape_count} shapes (leading slices of the same particles; the oracle "
+                      "queries meshes by brute force)"}
+
+
 def run_adjoint(args):
     """Differentiable config: 64 x 64 hanging cloth (a curtain: the whole top row pinned, bending ke 1e-2),
     60 frames x 10 substeps x 10 iterations; loss = mean squared distance of the final positions to a
@@ -1081,8 +1212,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["batched", "plain", "precision", "selfcontact", "adjoint", "soft"],
-                    default="batched")
+    ap.add_argument("--workload", choices=["batched", "plain", "precision", "selfcontact", "adjoint", "soft",
+                                           "contacts"], default="batched")  # fmt: skip
+    ap.add_argument("--contact-particles", type=int, default=8 << 20, help="contacts workload: particle count")
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--lanes", type=int, default=0)
@@ -1121,6 +1253,8 @@ def main():
         out = run_adjoint(args)
     elif args.workload == "soft":
         out = run_soft(args)
+    elif args.workload == "contacts":
+        out = run_contacts(args)
     else:
         out = run_ours(args)
     if out is not None:

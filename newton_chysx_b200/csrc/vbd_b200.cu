@@ -147,52 +147,56 @@ __device__ __forceinline__ vec3<float> rot_q(float4 q, vec3<float> v) {
   return v * (2.f * q.w * q.w - 1.f) + cross(u, v) * (2.f * q.w) + u * (2.f * dot(u, v));
 }
 
-// create_soft_contacts (geometry/kernels.py:1001-1140) for static analytic shapes: one thread per
-// (particle, shape), the particle in the shape frame, shape_sdf, and for d < margin + radius a contact at the
-// closest surface point x_local - n d and the normal, both mapped back to world; slots from an atomic counter.
+// create_soft_contacts (geometry/kernels.py:1001-1140) for static shapes: one thread per particle, looping over the
+// shapes (the reference launches one thread per (particle, shape); here the shape, hence the branch taken, is the
+// same across a warp). For each shape the particle in the shape frame, its distance and normal, and for
+// d < margin + radius a contact at the closest surface point x_local - n d and the normal, both mapped back to
+// world; slots from an atomic counter (warp-aggregating it by hand measured slower).
 __global__ void k_soft_contacts_shapes(int n, const float* __restrict__ q, const float* __restrict__ radius,
                                        const int* __restrict__ flags, int S, const ShapeXformTable shapes,
                                        const float* __restrict__ elev, float margin, int cmax, int* count,
                                        int* particle, int* shape, float* body_pos, float* body_vel, float* normal) {
-  const long tid = long(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (tid >= long(n) * S) return;
-  const int i = int(tid / S), s = int(tid % S);
-  if (!(flags[i] & 1)) return;
-  const float4 P = shapes.p[s], Q = shapes.q[s], SC = shapes.sc[s];
-  const float4 Qi = make_float4(-Q.x, -Q.y, -Q.z, Q.w);
-  const vec3<float> xl = rot_q(Qi, vec3<float>{q[3 * i] - P.x, q[3 * i + 1] - P.y, q[3 * i + 2] - P.z});
-  const float sc[3] = {SC.x, SC.y, SC.z};
-  float d;
-  vec3<float> nn;
-  const int type = shapes.type[s];
-  if (type == GEO_HFIELD) {
-    heightfield_sdf(shapes.hf[s], shapes.hfe[s], elev, xl, d, nn);
-  } else if (type == GEO_MESH || type == GEO_CONVEX_MESH) {  // geometry/kernels.py:1091-1113
-    d = 1.0e6f;
-    nn = {0.f, 0.f, 0.f};
-    const float ms = fminf(fminf(fabsf(sc[0]), fabsf(sc[1])), fabsf(sc[2]));
-    const vec3<float> xs = {xl.x / sc[0], xl.y / sc[1], xl.z / sc[2]};
-    vec3<float> cp;
-    float sg;
-    int face;
-    if (mesh_query_point_sign(shapes.mesh[s], xs, margin + radius[i] / ms, cp, sg, face)) {
-      const vec3<float> delta = xl - vec3<float>{cp.x * sc[0], cp.y * sc[1], cp.z * sc[2]};
-      d = length(delta) * sg;
-      nn = geo_normalize(delta) * sg;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !(flags[i] & 1)) return;
+  const vec3<float> x = {q[3 * i], q[3 * i + 1], q[3 * i + 2]};
+  const float r = radius[i];
+  for (int s = 0; s < S; ++s) {
+    const float4 P = shapes.p[s], Q = shapes.q[s], SC = shapes.sc[s];
+    const float4 Qi = make_float4(-Q.x, -Q.y, -Q.z, Q.w);
+    const vec3<float> xl = rot_q(Qi, vec3<float>{x.x - P.x, x.y - P.y, x.z - P.z});
+    const float sc[3] = {SC.x, SC.y, SC.z};
+    float d;
+    vec3<float> nn;
+    const int type = shapes.type[s];
+    if (type == GEO_HFIELD) {
+      heightfield_sdf(shapes.hf[s], shapes.hfe[s], elev, xl, d, nn);
+    } else if (type == GEO_MESH || type == GEO_CONVEX_MESH) {  // geometry/kernels.py:1091-1113
+      d = 1.0e6f;
+      nn = {0.f, 0.f, 0.f};
+      const float ms = fminf(fminf(fabsf(sc[0]), fabsf(sc[1])), fabsf(sc[2]));
+      const vec3<float> xs = {xl.x / sc[0], xl.y / sc[1], xl.z / sc[2]};
+      vec3<float> cp;
+      float sg;
+      int face;
+      if (mesh_query_point_sign(shapes.mesh[s], xs, margin + r / ms, cp, sg, face)) {
+        const vec3<float> delta = xl - vec3<float>{cp.x * sc[0], cp.y * sc[1], cp.z * sc[2]};
+        d = length(delta) * sg;
+        nn = geo_normalize(delta) * sg;
+      }
+    } else {
+      shape_sdf(type, xl, sc, d, nn);
     }
-  } else {
-    shape_sdf(type, xl, sc, d, nn);
-  }
-  if (d < margin + radius[i]) {
-    const int k = atomicAdd(count, 1);
-    if (k < cmax) {
-      const vec3<float> bp = rot_q(Q, xl - nn * d) + vec3<float>{P.x, P.y, P.z};
-      const vec3<float> wn = rot_q(Q, nn);
-      particle[k] = i;
-      shape[k] = s;
-      body_pos[3 * k] = bp.x, body_pos[3 * k + 1] = bp.y, body_pos[3 * k + 2] = bp.z;
-      body_vel[3 * k] = body_vel[3 * k + 1] = body_vel[3 * k + 2] = 0.f;
-      normal[3 * k] = wn.x, normal[3 * k + 1] = wn.y, normal[3 * k + 2] = wn.z;
+    if (d < margin + r) {
+      const int k = atomicAdd(count, 1);
+      if (k < cmax) {
+        const vec3<float> bp = rot_q(Q, xl - nn * d) + vec3<float>{P.x, P.y, P.z};
+        const vec3<float> wn = rot_q(Q, nn);
+        particle[k] = i;
+        shape[k] = s;
+        body_pos[3 * k] = bp.x, body_pos[3 * k + 1] = bp.y, body_pos[3 * k + 2] = bp.z;
+        body_vel[3 * k] = body_vel[3 * k + 1] = body_vel[3 * k + 2] = 0.f;
+        normal[3 * k] = wn.x, normal[3 * k + 1] = wn.y, normal[3 * k + 2] = wn.z;
+      }
     }
   }
 }
@@ -2168,8 +2172,7 @@ int vbd_soft_contacts_table(int32_t n, const float* q, const float* radius, cons
   cudaStream_t st = (cudaStream_t)stream;
   CK(cudaMemsetAsync(count, 0, sizeof(int), st));
   if (n == 0 || S == 0) return VBD_OK;
-  const long total = long(n) * S;
-  k_soft_contacts_shapes<<<int((total + 255) / 256), 256, 0, st>>>(n, q, radius, flags, S, tab, tb->elevations_dev,
+  k_soft_contacts_shapes<<<(n + 255) / 256, 256, 0, st>>>(n, q, radius, flags, S, tab, tb->elevations_dev,
                                                                    margin, cmax, count, particle, shape, body_pos,
                                                                    body_vel, normal);
   CK(cudaGetLastError());
