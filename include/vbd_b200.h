@@ -409,7 +409,10 @@ int vbd_mesh_destroy(VbdMeshHandle mesh);
    shape_scale_host [S,3]. Heightfield shape s (type 2) takes grid shape_heightfield_index_host[s] of
    heightfields_host[heightfield_count] over elevations_dev (elevation_count floats). Mesh shape s (types 8 and
    10) takes shape_mesh_host[s]; its scale must have no zero component. The arrays for a kind of shape may be
-   NULL when no shape of that kind is present. */
+   NULL when no shape of that kind is present. shape_flags_host [S] (ShapeFlags bits; NULL = all collide): shapes
+   without COLLIDE_PARTICLES (1 << 2) are skipped. shape_world_host [S] and particle_world_dev [particle_count]
+   (NULL = all global): a particle and a shape of different worlds do not collide unless either is global (-1),
+   as create_soft_contacts filters them (geometry/kernels.py:1031-1043). */
 typedef struct VbdShapeTable {
   int32_t shape_count;
   const int32_t* shape_type_host;
@@ -421,6 +424,9 @@ typedef struct VbdShapeTable {
   const float* elevations_dev;
   int64_t elevation_count;
   const VbdMeshHandle* shape_mesh_host;
+  const int32_t* shape_flags_host;
+  const int32_t* shape_world_host;
+  const int32_t* particle_world_dev;
 } VbdShapeTable;
 
 /* vbd_soft_contacts_shapes over a full shape table: the analytic types, heightfields (sample_sdf_grad_heightfield,

@@ -90,7 +90,8 @@ class VbdShapeTable(C.Structure):
         ("shape_count", C.c_int32), ("shape_type_host", _ip), ("shape_transform_host", _fp),
         ("shape_scale_host", _fp), ("shape_heightfield_index_host", _ip), ("heightfield_count", C.c_int32),
         ("heightfields_host", C.POINTER(VbdHeightfield)), ("elevations_dev", _vp), ("elevation_count", C.c_int64),
-        ("shape_mesh_host", C.POINTER(_vp)),
+        ("shape_mesh_host", C.POINTER(_vp)), ("shape_flags_host", _ip), ("shape_world_host", _ip),
+        ("particle_world_dev", _vp),
     ]  # fmt: skip
 
 

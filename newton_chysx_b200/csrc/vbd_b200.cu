@@ -140,6 +140,8 @@ struct ShapeXformTable {
   int4 hf[kMaxContactShapes];    // heightfields: (data_offset, nrow, ncol, 0)
   float4 hfe[kMaxContactShapes];  // heightfields: (hx, hy, min_z, max_z), scale applied
   MeshView mesh[kMaxContactShapes];  // triangle meshes
+  int world[kMaxContactShapes];      // world index, -1 = global
+  int id[kMaxContactShapes];         // the shape's index in the model (shapes not colliding with particles are left out)
 };
 
 __device__ __forceinline__ vec3<float> rot_q(float4 q, vec3<float> v) {
@@ -152,15 +154,25 @@ __device__ __forceinline__ vec3<float> rot_q(float4 q, vec3<float> v) {
 // same across a warp). For each shape the particle in the shape frame, its distance and normal, and for
 // d < margin + radius a contact at the closest surface point x_local - n d and the normal, both mapped back to
 // world; slots from an atomic counter (warp-aggregating it by hand measured slower).
-__global__ void k_soft_contacts_shapes(int n, const float* __restrict__ q, const float* __restrict__ radius,
-                                       const int* __restrict__ flags, int S, const ShapeXformTable shapes,
-                                       const float* __restrict__ elev, float margin, int cmax, int* count,
-                                       int* particle, int* shape, float* body_pos, float* body_vel, float* normal) {
+// WORLDS: some shape belongs to a world (else the world filter can never apply and is compiled out). Four
+// 256-thread CTAs per SM: the loop is latency-bound, and 4 resident CTAs ran faster than 3.
+template <bool WORLDS>
+__global__ void __launch_bounds__(256, 4)
+    k_soft_contacts_shapes(int n, const float* __restrict__ q, const float* __restrict__ radius,
+                           const int* __restrict__ flags, int S, const ShapeXformTable shapes,
+                           const float* __restrict__ elev, const int* __restrict__ particle_world, float margin,
+                           int cmax, int* count, int* particle, int* shape, float* body_pos, float* body_vel,
+                           float* normal) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || !(flags[i] & 1)) return;
   const vec3<float> x = {q[3 * i], q[3 * i + 1], q[3 * i + 2]};
   const float r = radius[i];
+  const int pw = WORLDS && particle_world ? particle_world[i] : -1;
   for (int s = 0; s < S; ++s) {
+    if (WORLDS) {  // other world (geometry/kernels.py:1036-1043)
+      const int sw = shapes.world[s];
+      if (pw != -1 && sw != -1 && pw != sw) continue;
+    }
     const float4 P = shapes.p[s], Q = shapes.q[s], SC = shapes.sc[s];
     const float4 Qi = make_float4(-Q.x, -Q.y, -Q.z, Q.w);
     const vec3<float> xl = rot_q(Qi, vec3<float>{x.x - P.x, x.y - P.y, x.z - P.z});
@@ -192,7 +204,7 @@ __global__ void k_soft_contacts_shapes(int n, const float* __restrict__ q, const
         const vec3<float> bp = rot_q(Q, xl - nn * d) + vec3<float>{P.x, P.y, P.z};
         const vec3<float> wn = rot_q(Q, nn);
         particle[k] = i;
-        shape[k] = s;
+        shape[k] = shapes.id[s];
         body_pos[3 * k] = bp.x, body_pos[3 * k + 1] = bp.y, body_pos[3 * k + 2] = bp.z;
         body_vel[3 * k] = body_vel[3 * k + 1] = body_vel[3 * k + 2] = 0.f;
         normal[3 * k] = wn.x, normal[3 * k + 1] = wn.y, normal[3 * k + 2] = wn.z;
@@ -2135,13 +2147,17 @@ int vbd_soft_contacts_table(int32_t n, const float* q, const float* radius, cons
     return VBD_ERR_INVALID_ARGUMENT;
   ShapeXformTable tab;
   std::memset(&tab, 0, sizeof(tab));
-  for (int s = 0; s < S; ++s) {
-    const int t = tb->shape_type_host[s];
+  int m = 0;  // shapes that collide with particles, in model order (COLLIDE_PARTICLES, geometry/kernels.py:1033-1034)
+  for (int s0 = 0; s0 < S; ++s0) {
+    if (tb->shape_flags_host && !(tb->shape_flags_host[s0] & 4)) continue;
+    const int s = m++, t = tb->shape_type_host[s0];
+    tab.id[s] = s0;
+    tab.world[s] = tb->shape_world_host ? tb->shape_world_host[s0] : -1;
     if (t != GEO_PLANE && t != GEO_SPHERE && t != GEO_CAPSULE && t != GEO_ELLIPSOID && t != GEO_CYLINDER &&
         t != GEO_BOX && t != GEO_CONE && t != GEO_HFIELD && t != GEO_MESH && t != GEO_CONVEX_MESH)
       return VBD_ERR_UNSUPPORTED;
-    const float* X = tb->shape_transform_host + 7 * s;
-    const float* sc = tb->shape_scale_host + 3 * s;
+    const float* X = tb->shape_transform_host + 7 * s0;
+    const float* sc = tb->shape_scale_host + 3 * s0;
     const float ql = std::sqrt(X[3] * X[3] + X[4] * X[4] + X[5] * X[5] + X[6] * X[6]);
     if (!(ql > 0.f)) return VBD_ERR_INVALID_ARGUMENT;
     tab.type[s] = t;
@@ -2150,7 +2166,7 @@ int vbd_soft_contacts_table(int32_t n, const float* q, const float* radius, cons
     tab.sc[s] = make_float4(sc[0], sc[1], sc[2], 0.f);
     if (t == GEO_HFIELD) {  // every grid read of heightfield_sdf stays inside [data_offset, data_offset + nrow ncol)
       if (!tb->shape_heightfield_index_host || !tb->heightfields_host) return VBD_ERR_INVALID_ARGUMENT;
-      const int k = tb->shape_heightfield_index_host[s];
+      const int k = tb->shape_heightfield_index_host[s0];
       if (k < 0 || k >= tb->heightfield_count) return VBD_ERR_INVALID_ARGUMENT;
       const VbdHeightfield& h = tb->heightfields_host[k];
       if (h.nrow < 0 || h.ncol < 0 || h.data_offset < 0) return VBD_ERR_INVALID_ARGUMENT;
@@ -2163,18 +2179,20 @@ int vbd_soft_contacts_table(int32_t n, const float* q, const float* radius, cons
       tab.hfe[s] = make_float4(h.hx, h.hy, h.min_z, h.max_z);
     }
     if (t == GEO_MESH || t == GEO_CONVEX_MESH) {
-      if (!tb->shape_mesh_host || !tb->shape_mesh_host[s]) return VBD_ERR_INVALID_ARGUMENT;
+      if (!tb->shape_mesh_host || !tb->shape_mesh_host[s0]) return VBD_ERR_INVALID_ARGUMENT;
       for (int k = 0; k < 3; ++k)
         if (!(sc[k] != 0.f) || !std::isfinite(sc[k])) return VBD_ERR_INVALID_ARGUMENT;
-      tab.mesh[s] = tb->shape_mesh_host[s]->view;
+      tab.mesh[s] = tb->shape_mesh_host[s0]->view;
     }
   }
   cudaStream_t st = (cudaStream_t)stream;
   CK(cudaMemsetAsync(count, 0, sizeof(int), st));
-  if (n == 0 || S == 0) return VBD_OK;
-  k_soft_contacts_shapes<<<(n + 255) / 256, 256, 0, st>>>(n, q, radius, flags, S, tab, tb->elevations_dev,
-                                                                   margin, cmax, count, particle, shape, body_pos,
-                                                                   body_vel, normal);
+  if (n == 0 || m == 0) return VBD_OK;
+  bool worlds = false;
+  for (int s = 0; s < m; ++s) worlds = worlds || tab.world[s] != -1;
+  auto kern = worlds && tb->particle_world_dev ? k_soft_contacts_shapes<true> : k_soft_contacts_shapes<false>;
+  kern<<<(n + 255) / 256, 256, 0, st>>>(n, q, radius, flags, m, tab, tb->elevations_dev, tb->particle_world_dev,
+                                         margin, cmax, count, particle, shape, body_pos, body_vel, normal);
   CK(cudaGetLastError());
   return VBD_OK;
 }

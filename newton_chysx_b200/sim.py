@@ -57,6 +57,7 @@ class ShapeConfig:
     ke: float = 2.5e3
     kd: float = 100.0
     mu: float = 1.0
+    has_particle_collision: bool = True
 
 
 # ----------------------------------------------------------------------------- quaternions (x, y, z, w)
@@ -660,7 +661,8 @@ class ModelBuilder:
         cfg = cfg or self.default_shape_cfg
         p, q = _xform(xform)
         self.shapes.append(dict(type=GeoType(type_), pos=p, rot=q, scale=tuple(float(v) for v in scale), ke=cfg.ke,
-                                kd=cfg.kd, mu=cfg.mu, body=-1, src=src))  # fmt: skip
+                                kd=cfg.kd, mu=cfg.mu, body=-1, src=src, world=self.current_world,
+                                flags=4 if cfg.has_particle_collision else 0))  # fmt: skip
         return len(self.shapes) - 1
 
     def add_shape_plane(self, plane=(0.0, 0.0, 1.0, 0.0), xform=None, width=10.0, length=10.0, body=-1,
@@ -786,7 +788,7 @@ class ModelBuilder:
             self._tet_pose.append(builder.tet_poses)
             self._tet_mat.append(builder.tet_materials)
             self._tt += builder._tt
-        self.shapes.extend(dict(s) for s in builder.shapes)
+        self.shapes.extend(dict(s, world=w) for s in builder.shapes)
         translated = [_ChunkedGroup([c + start for c in g.chunks], g.size) for g in builder._color_groups]
         self._color_groups = _merge_chunked(self._color_groups, translated)
 
@@ -928,6 +930,9 @@ class Model:
         m.shape_material_kd = t(np.array([s["kd"] for s in b.shapes]).reshape(S), f32)
         m.shape_material_mu = t(np.array([s["mu"] for s in b.shapes]).reshape(S), f32)
         m.shape_body = t(np.array([s["body"] for s in b.shapes], dtype=np.int32).reshape(S), i32)
+        # ShapeFlags COLLIDE_PARTICLES (1 << 2) and world indices (-1 = global), builder.py:417, 3288, 5866
+        m.shape_flags = np.array([s.get("flags", 4) for s in b.shapes], dtype=np.int32).reshape(S)
+        m.shape_world = np.array([s.get("world", -1) for s in b.shapes], dtype=np.int32).reshape(S)
         # heightfields as the reference's finalize packs them (builder.py:10690-10735): one row (data_offset, nrow,
         # ncol, |hx sx|, |hy sy|, min_z sz, max_z sz) per heightfield shape, elevations concatenated
         m.shape_heightfield_index = np.full(S, -1, dtype=np.int32)
@@ -1052,10 +1057,14 @@ def soft_contacts(model: Model, state: State, contacts: Contacts, margin: float)
     midx = getattr(model, "shape_mesh_index", np.full(S, -1))
     dmeshes = getattr(model, "_device_meshes", [])
     handles = (C.c_void_p * S)(*[dmeshes[k].handle if k >= 0 else None for k in midx])
+    sfl = np.ascontiguousarray(getattr(model, "shape_flags", np.full(S, 4)), dtype=np.int32)
+    swl = np.ascontiguousarray(getattr(model, "shape_world", np.full(S, -1)), dtype=np.int32)
+    pw = getattr(model, "particle_world", None)
     tb = _lib.VbdShapeTable(
         S, st.ctypes.data_as(ip), sx.ctypes.data_as(fp), ss.ctypes.data_as(fp), hidx.ctypes.data_as(ip), len(rows),
         hfs, None if elev is None else elev.data_ptr(), 0 if elev is None else elev.numel(),
-        C.cast(handles, C.POINTER(C.c_void_p)),
+        C.cast(handles, C.POINTER(C.c_void_p)), sfl.ctypes.data_as(ip), swl.ctypes.data_as(ip),
+        None if pw is None else pw.data_ptr(),
     )  # fmt: skip
     stream = torch.cuda.current_stream(model.device).cuda_stream
     rc = lib.vbd_soft_contacts_table(

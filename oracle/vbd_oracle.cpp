@@ -1825,7 +1825,8 @@ int oracle_soft_contacts_shapes(int n, const double* q, const double* radius, co
                                 const int* shape_type, const double* shape_xform, const double* shape_scale,
                                 const int* hf_index, const int* hf_grid, const double* hf_ext, const double* elev,
                                 const int* mesh_index, const int* mesh_vert_off, const int* mesh_tri_off,
-                                const double* mesh_pts, const int* mesh_tris, double margin, int max_contacts,
+                                const double* mesh_pts, const int* mesh_tris, const int* shape_flags,
+                                const int* shape_world, const int* particle_world, double margin, int max_contacts,
                                 int* particle, int* shape, double* body_pos, double* body_vel, double* normal) {
   using sdf::D3;
   for (int s = 0; s < S; ++s) {
@@ -1843,6 +1844,9 @@ int oracle_soft_contacts_shapes(int n, const double* q, const double* radius, co
     if (!(flags[i] & 1)) continue;
     const D3 x = v3(q[3 * i], q[3 * i + 1], q[3 * i + 2]);
     for (int s = 0; s < S; ++s) {
+      if (shape_flags && !(shape_flags[s] & 4)) continue;  // COLLIDE_PARTICLES (geometry/kernels.py:1033-1034)
+      const int pw = particle_world ? particle_world[i] : -1, sw = shape_world ? shape_world[s] : -1;
+      if (pw != -1 && sw != -1 && pw != sw) continue;  // geometry/kernels.py:1036-1043
       const double* X = shape_xform + 7 * s;
       const double* sc = shape_scale + 3 * s;
       const double qi[4] = {-X[3], -X[4], -X[5], X[6]};

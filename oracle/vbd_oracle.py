@@ -110,8 +110,8 @@ def lib():
             C.c_int, _dp, _dp, _ip, C.c_int, _ip, _dp, _dp, C.c_double, C.c_int, _ip, _ip, _dp, _dp, _dp,
         ]
         _lib.oracle_soft_contacts_shapes.argtypes = [
-            C.c_int, _dp, _dp, _ip, C.c_int, _ip, _dp, _dp, _ip, _ip, _dp, _dp, _ip, _ip, _ip, _dp, _ip, C.c_double,
-            C.c_int, _ip, _ip, _dp, _dp, _dp,
+            C.c_int, _dp, _dp, _ip, C.c_int, _ip, _dp, _dp, _ip, _ip, _dp, _dp, _ip, _ip, _ip, _dp, _ip, _ip, _ip, _ip,
+            C.c_double, C.c_int, _ip, _ip, _dp, _dp, _dp,
         ]  # fmt: skip
         _lib.oracle_max_threads.restype = C.c_int
         _lib.oracle_vbd_step_sc.argtypes = [
@@ -300,10 +300,12 @@ def soft_contacts(q, radius, flags, shape_type, shape_pos, shape_radius, margin,
 
 
 def soft_contacts_shapes(q, radius, flags, shape_type, shape_transform, shape_scale, margin, max_contacts=None,
-                         heightfield_index=None, heightfields=None, elevations=None, mesh_index=None, meshes=None):
+                         heightfield_index=None, heightfields=None, elevations=None, mesh_index=None, meshes=None,
+                         shape_flags=None, shape_world=None, particle_world=None):
     """Particle-shape contacts against static analytic shapes (GeoType values: plane 1, heightfield 2, sphere 3,
     capsule 4, ellipsoid 5, cylinder 6, box 7, cone 9) with transforms [S, 7] (position, quaternion xyzw) and
-    scales [S, 3], in (particle, shape) order. Heightfield shape s uses grid ``heightfield_index[s]`` of
+    scales [S, 3], in (particle, shape) order, skipping shapes without the COLLIDE_PARTICLES flag (1 << 2) and
+    pairs of different worlds unless either is global (-1). Heightfield shape s uses grid ``heightfield_index[s]`` of
     ``heightfields`` (rows of (data_offset, nrow, ncol, hx, hy, min_z, max_z), scale applied) over the
     concatenated normalized ``elevations``. Mesh shape s (types 8, 10) uses ``meshes[mesh_index[s]]``, a
     (points [V, 3], triangles [T, 3]) pair."""
@@ -335,9 +337,12 @@ def soft_contacts_shapes(q, radius, flags, shape_type, shape_transform, shape_sc
         mto = _i(np.cumsum([0] + [len(np.asarray(t).reshape(-1, 3)) for _, t in meshes]))
         mpt = _d(np.concatenate([np.asarray(p, dtype=np.float64).reshape(-1) for p, _ in meshes]))
         mtr = _i(np.concatenate([np.asarray(t).reshape(-1) for _, t in meshes]))
+    sfl = None if shape_flags is None else _i(shape_flags)
+    swl = None if shape_world is None else _i(shape_world)
+    pwl = None if particle_world is None else _i(particle_world)
     cnt = lib().oracle_soft_contacts_shapes(n, qp, rp, flp, S, stp, sxp, ssp, *(None if a is None else a[1] for a in
-                                            (hfi, hfg, hfe, elv, mi, mvo, mto, mpt, mtr)), margin, max_contacts, pp,
-                                            shpp, bpp, bvp, nnp)  # fmt: skip
+                                            (hfi, hfg, hfe, elv, mi, mvo, mto, mpt, mtr, sfl, swl, pwl)), margin,
+                                            max_contacts, pp, shpp, bpp, bvp, nnp)  # fmt: skip
     if cnt < 0:
         raise ValueError("a shape type without an analytic SDF")
     return cnt, part, shp, bp.reshape(-1, 3), bv.reshape(-1, 3), nn.reshape(-1, 3)

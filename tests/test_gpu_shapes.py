@@ -397,3 +397,32 @@ def test_cloth_drapes_over_mesh_box():
     inside = (np.abs(loc[:, 0]) < 0.2) & (np.abs(loc[:, 1]) < 0.15) & (np.abs(loc[:, 2]) < 0.1)
     assert not inside.any()
     assert x[:, 2].max() < 0.25
+
+
+def test_collision_pipeline_worlds_match_oracle():
+    """World filtering and the COLLIDE_PARTICLES flag on the GPU against the oracle (three worlds, one sphere each,
+    one of them not colliding with particles, and a global ground plane)."""
+    from tests.test_oracle_shapes import _world_scene
+
+    m = _world_scene("cuda")
+    pipe = sim.CollisionPipeline(m, soft_contact_margin=0.01)
+    contacts = pipe.contacts()
+    pipe.collide(m.state(), contacts)
+    torch.cuda.synchronize()
+    k = int(contacts.soft_contact_count.item())
+    gpu = {(int(a), int(s)): (x, y, z) for a, s, x, y, z in zip(
+        contacts.soft_contact_particle[:k].cpu().numpy(), contacts.soft_contact_shape[:k].cpu().numpy(),
+        contacts.soft_contact_body_pos[:k].cpu().numpy(), contacts.soft_contact_body_vel[:k].cpu().numpy(),
+        contacts.soft_contact_normal[:k].cpu().numpy())}  # fmt: skip
+    qf = m.particle_q.cpu().numpy().astype(np.float64)
+    r = m.particle_radius.cpu().numpy().astype(np.float64)
+    fl = m.particle_flags.cpu().numpy()
+    args = (m.shape_type, m.shape_transform.astype(np.float64), m.shape_scale.astype(np.float64))
+    kw = dict(shape_flags=m.shape_flags, shape_world=m.shape_world, particle_world=m.particle_world.cpu().numpy())
+    cnt, p, s, bp, _, nn = orc.soft_contacts_shapes(qf, r, fl, *args, 0.01, **kw)
+    lo = orc.soft_contacts_shapes(qf, r, fl, *args, 0.01 - 1e-5, **kw)
+    hi = orc.soft_contacts_shapes(qf, r, fl, *args, 0.01 + 1e-5, **kw)
+    near = set(zip(hi[1][:hi[0]].tolist(), hi[2][:hi[0]].tolist()))
+    near -= set(zip(lo[1][:lo[0]].tolist(), lo[2][:lo[0]].tolist()))
+    assert {sh for _, sh in gpu} == {0, 1, 3}
+    _compare(gpu, list(zip(p[:cnt].tolist(), s[:cnt].tolist())), bp[:cnt], nn[:cnt], near)

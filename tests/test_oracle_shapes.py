@@ -141,3 +141,40 @@ def test_oracle_mesh_sign_and_distance():
     d = np.einsum("ij,ij->i", pts[p[:cnt]] - bp[:cnt], nn[:cnt])
     assert (d[:2] < 0).all() and (d[2:] > 0).all()
     np.testing.assert_allclose(d[[0, 2, 3, 4]], [-0.1, 0.2, 0.1, 0.05], atol=0.01)
+
+
+def _world_scene(device):
+    """Three worlds with a sphere each at the same place (the third's sphere does not collide with particles) and a
+    global ground plane; particles of every world spread over the spheres."""
+    rng = np.random.default_rng(9)
+    top = sim.ModelBuilder(up_axis="Z")
+    for w in range(3):
+        b = sim.ModelBuilder(up_axis="Z")
+        pts = np.stack([rng.uniform(-0.4, 0.4, 3000), rng.uniform(-0.4, 0.4, 3000), rng.uniform(-0.02, 0.5, 3000)], 1)
+        b.add_particles(pts, (0.0, 0.0, 0.0), 1.0, radius=0.01)
+        cfg = sim.ShapeConfig(has_particle_collision=(w != 2))
+        b.add_shape_sphere(xform=((0.0, 0.0, 0.2), sim.quat_identity()), radius=0.2, cfg=cfg)
+        top.add_world(b)
+    top.add_ground_plane()
+    return top.finalize(device)
+
+
+def test_shape_worlds_and_particle_collision_flag():
+    """create_soft_contacts' filters (geometry/kernels.py:1031-1043): a shape without COLLIDE_PARTICLES gets no
+    contacts; a particle and a shape of different worlds do not collide unless either is global."""
+    m = _world_scene("cpu")
+    assert list(m.shape_world) == [0, 1, 2, -1] and list(m.shape_flags) == [4, 4, 0, 4]
+    pw = m.particle_world.numpy()
+    assert list(np.unique(pw)) == [0, 1, 2]
+    args = (m.particle_q.double().numpy(), m.particle_radius.double().numpy(), m.particle_flags.numpy(), m.shape_type,
+            m.shape_transform.astype(np.float64), m.shape_scale.astype(np.float64), 0.01)  # fmt: skip
+    cnt, p, s, _, _, _ = orc.soft_contacts_shapes(*args, shape_flags=m.shape_flags, shape_world=m.shape_world,
+                                                  particle_world=pw)  # fmt: skip
+    p, s = p[:cnt], s[:cnt]
+    assert set(s.tolist()) == {0, 1, 3}
+    sph = s < 3
+    assert (pw[p[sph]] == s[sph]).all()  # every sphere contact is within the particle's own world
+    assert set(pw[p[s == 3]].tolist()) == {0, 1, 2}  # the global plane touches every world
+    # without the filters the same particles also touch the other worlds' spheres
+    cnt_all, _, s_all, _, _, _ = orc.soft_contacts_shapes(*args)
+    assert cnt_all > cnt and set(s_all[:cnt_all].tolist()) == {0, 1, 2, 3}
