@@ -442,6 +442,22 @@ int vbd_soft_contacts_table(int32_t particle_count, const float* q_dev, const fl
                             int32_t soft_contact_max, int32_t* count_dev, int32_t* particle_dev, int32_t* shape_dev,
                             float* body_pos_dev, float* body_vel_dev, float* normal_dev, void* stream);
 
+/* A model's static shapes uploaded once for contact generation, any number of shapes and worlds: the shapes with
+   COLLIDE_PARTICLES, their records and, per world, the list of its shapes (create_soft_contacts' world filter,
+   geometry/kernels.py:1036-1043). Takes the VbdShapeTable fields except particle_world_dev; world indices must
+   be -1 (global) or non-negative. The mesh handles and the elevation array the table names must outlive the set. */
+typedef struct VbdShapeSetImpl* VbdShapeSetHandle;
+int vbd_shape_set_create(const VbdShapeTable* shapes, VbdShapeSetHandle* out);
+int vbd_shape_set_destroy(VbdShapeSetHandle set);
+
+/* Soft contacts of every active particle against a shape set, written as vbd_soft_contacts_shapes writes them. A
+   particle of world w (particle_world_dev; NULL = all global) tests the global shapes and world w's shapes; a
+   global particle tests every shape. */
+int vbd_soft_contacts_set(VbdShapeSetHandle set, int32_t particle_count, const float* q_dev, const float* radius_dev,
+                          const int32_t* flags_dev, const int32_t* particle_world_dev, float margin,
+                          int32_t soft_contact_max, int32_t* count_dev, int32_t* particle_dev, int32_t* shape_dev,
+                          float* body_pos_dev, float* body_vel_dev, float* normal_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -160,6 +160,12 @@ SIGNATURES = {
         C.c_int,
     ),
     "vbd_mesh_create": ([_fp, C.c_int32, _ip, C.c_int32, C.POINTER(_vp)], C.c_int),
+    "vbd_shape_set_create": ([C.POINTER(VbdShapeTable), C.POINTER(_vp)], C.c_int),
+    "vbd_shape_set_destroy": ([_vp], C.c_int),
+    "vbd_soft_contacts_set": (
+        [_vp, C.c_int32, _vp, _vp, _vp, _vp, C.c_float, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+        C.c_int,
+    ),
     "vbd_mesh_destroy": ([_vp], C.c_int),
     "vbd_soft_contacts": (
         [C.c_int32, _vp, _vp, _vp, C.c_int32, _ip, _fp, _fp, _fp, C.c_float, C.c_int32, _vp, _vp, _vp, _vp, _vp,

@@ -16,7 +16,7 @@
 
 #include "vbd_b200.h"
 #include "vbd_adjoint.cuh"
-#include "vbd_mesh.cuh"
+#include "vbd_contactgen.cuh"
 #include "vbd_collide.cuh"
 #include "vbd_ell.cuh"
 #include "vbd_ring.cuh"
@@ -132,34 +132,19 @@ __global__ void k_soft_contacts(int n, const float* __restrict__ q, const float*
   }
 }
 
-struct ShapeXformTable {
-  int type[kMaxContactShapes];
-  float4 p[kMaxContactShapes];  // position
-  float4 q[kMaxContactShapes];  // rotation (x, y, z, w)
-  float4 sc[kMaxContactShapes];  // scale
-  int4 hf[kMaxContactShapes];    // heightfields: (data_offset, nrow, ncol, 0)
-  float4 hfe[kMaxContactShapes];  // heightfields: (hx, hy, min_z, max_z), scale applied
-  MeshView mesh[kMaxContactShapes];  // triangle meshes
-  int world[kMaxContactShapes];      // world index, -1 = global
-  int id[kMaxContactShapes];         // the shape's index in the model (shapes not colliding with particles are left out)
+// The shapes of one vbd_soft_contacts_table call, passed by value as a kernel parameter.
+struct ShapeParamTable {
+  ShapeRec rec[kMaxContactShapes];
 };
 
-__device__ __forceinline__ vec3<float> rot_q(float4 q, vec3<float> v) {
-  const vec3<float> u = {q.x, q.y, q.z};
-  return v * (2.f * q.w * q.w - 1.f) + cross(u, v) * (2.f * q.w) + u * (2.f * dot(u, v));
-}
-
-// create_soft_contacts (geometry/kernels.py:1001-1140) for static shapes: one thread per particle, looping over the
-// shapes (the reference launches one thread per (particle, shape); here the shape, hence the branch taken, is the
-// same across a warp). For each shape the particle in the shape frame, its distance and normal, and for
-// d < margin + radius a contact at the closest surface point x_local - n d and the normal, both mapped back to
-// world; slots from an atomic counter (warp-aggregating it by hand measured slower).
-// WORLDS: some shape belongs to a world (else the world filter can never apply and is compiled out). Four
-// 256-thread CTAs per SM: the loop is latency-bound, and 4 resident CTAs ran faster than 3.
+// create_soft_contacts (geometry/kernels.py:1001-1140) over a parameter table: one thread per particle, looping over
+// the shapes (the reference launches one thread per (particle, shape); here the shape, hence the branch taken, is
+// the same across a warp). WORLDS: some shape belongs to a world (else the world filter can never apply and is
+// compiled out). Four 256-thread CTAs per SM: the loop is latency-bound, and 4 resident CTAs ran faster than 3.
 template <bool WORLDS>
 __global__ void __launch_bounds__(256, 4)
     k_soft_contacts_shapes(int n, const float* __restrict__ q, const float* __restrict__ radius,
-                           const int* __restrict__ flags, int S, const ShapeXformTable shapes,
+                           const int* __restrict__ flags, int S, const ShapeParamTable shapes,
                            const float* __restrict__ elev, const int* __restrict__ particle_world, float margin,
                            int cmax, int* count, int* particle, int* shape, float* body_pos, float* body_vel,
                            float* normal) {
@@ -170,46 +155,11 @@ __global__ void __launch_bounds__(256, 4)
   const int pw = WORLDS && particle_world ? particle_world[i] : -1;
   for (int s = 0; s < S; ++s) {
     if (WORLDS) {  // other world (geometry/kernels.py:1036-1043)
-      const int sw = shapes.world[s];
+      const int sw = shapes.rec[s].world;
       if (pw != -1 && sw != -1 && pw != sw) continue;
     }
-    const float4 P = shapes.p[s], Q = shapes.q[s], SC = shapes.sc[s];
-    const float4 Qi = make_float4(-Q.x, -Q.y, -Q.z, Q.w);
-    const vec3<float> xl = rot_q(Qi, vec3<float>{x.x - P.x, x.y - P.y, x.z - P.z});
-    const float sc[3] = {SC.x, SC.y, SC.z};
-    float d;
-    vec3<float> nn;
-    const int type = shapes.type[s];
-    if (type == GEO_HFIELD) {
-      heightfield_sdf(shapes.hf[s], shapes.hfe[s], elev, xl, d, nn);
-    } else if (type == GEO_MESH || type == GEO_CONVEX_MESH) {  // geometry/kernels.py:1091-1113
-      d = 1.0e6f;
-      nn = {0.f, 0.f, 0.f};
-      const float ms = fminf(fminf(fabsf(sc[0]), fabsf(sc[1])), fabsf(sc[2]));
-      const vec3<float> xs = {xl.x / sc[0], xl.y / sc[1], xl.z / sc[2]};
-      vec3<float> cp;
-      float sg;
-      int face;
-      if (mesh_query_point_sign(shapes.mesh[s], xs, margin + r / ms, cp, sg, face)) {
-        const vec3<float> delta = xl - vec3<float>{cp.x * sc[0], cp.y * sc[1], cp.z * sc[2]};
-        d = length(delta) * sg;
-        nn = geo_normalize(delta) * sg;
-      }
-    } else {
-      shape_sdf(type, xl, sc, d, nn);
-    }
-    if (d < margin + r) {
-      const int k = atomicAdd(count, 1);
-      if (k < cmax) {
-        const vec3<float> bp = rot_q(Q, xl - nn * d) + vec3<float>{P.x, P.y, P.z};
-        const vec3<float> wn = rot_q(Q, nn);
-        particle[k] = i;
-        shape[k] = shapes.id[s];
-        body_pos[3 * k] = bp.x, body_pos[3 * k + 1] = bp.y, body_pos[3 * k + 2] = bp.z;
-        body_vel[3 * k] = body_vel[3 * k + 1] = body_vel[3 * k + 2] = 0.f;
-        normal[3 * k] = wn.x, normal[3 * k + 1] = wn.y, normal[3 * k + 2] = wn.z;
-      }
-    }
+    soft_contact_shape(shapes.rec[s], elev, x, r, margin, i, cmax, count, particle, shape, body_pos, body_vel,
+                       normal);
   }
 }
 
@@ -2145,51 +2095,19 @@ int vbd_soft_contacts_table(int32_t n, const float* q, const float* radius, cons
     return VBD_ERR_INVALID_ARGUMENT;
   if (n > 0 && S > 0 && (!q || !radius || !flags || (cmax > 0 && (!particle || !shape || !body_pos || !body_vel || !normal))))
     return VBD_ERR_INVALID_ARGUMENT;
-  ShapeXformTable tab;
+  ShapeParamTable tab;
   std::memset(&tab, 0, sizeof(tab));
   int m = 0;  // shapes that collide with particles, in model order (COLLIDE_PARTICLES, geometry/kernels.py:1033-1034)
   for (int s0 = 0; s0 < S; ++s0) {
     if (tb->shape_flags_host && !(tb->shape_flags_host[s0] & 4)) continue;
-    const int s = m++, t = tb->shape_type_host[s0];
-    tab.id[s] = s0;
-    tab.world[s] = tb->shape_world_host ? tb->shape_world_host[s0] : -1;
-    if (t != GEO_PLANE && t != GEO_SPHERE && t != GEO_CAPSULE && t != GEO_ELLIPSOID && t != GEO_CYLINDER &&
-        t != GEO_BOX && t != GEO_CONE && t != GEO_HFIELD && t != GEO_MESH && t != GEO_CONVEX_MESH)
-      return VBD_ERR_UNSUPPORTED;
-    const float* X = tb->shape_transform_host + 7 * s0;
-    const float* sc = tb->shape_scale_host + 3 * s0;
-    const float ql = std::sqrt(X[3] * X[3] + X[4] * X[4] + X[5] * X[5] + X[6] * X[6]);
-    if (!(ql > 0.f)) return VBD_ERR_INVALID_ARGUMENT;
-    tab.type[s] = t;
-    tab.p[s] = make_float4(X[0], X[1], X[2], 0.f);
-    tab.q[s] = make_float4(X[3] / ql, X[4] / ql, X[5] / ql, X[6] / ql);
-    tab.sc[s] = make_float4(sc[0], sc[1], sc[2], 0.f);
-    if (t == GEO_HFIELD) {  // every grid read of heightfield_sdf stays inside [data_offset, data_offset + nrow ncol)
-      if (!tb->shape_heightfield_index_host || !tb->heightfields_host) return VBD_ERR_INVALID_ARGUMENT;
-      const int k = tb->shape_heightfield_index_host[s0];
-      if (k < 0 || k >= tb->heightfield_count) return VBD_ERR_INVALID_ARGUMENT;
-      const VbdHeightfield& h = tb->heightfields_host[k];
-      if (h.nrow < 0 || h.ncol < 0 || h.data_offset < 0) return VBD_ERR_INVALID_ARGUMENT;
-      if (h.nrow > 1 && h.ncol > 1) {
-        if (!tb->elevations_dev || int64_t(h.data_offset) + int64_t(h.nrow) * h.ncol > tb->elevation_count ||
-            !(h.hx > 0.f) || !(h.hy > 0.f) || !std::isfinite(h.hx) || !std::isfinite(h.hy))
-          return VBD_ERR_INVALID_ARGUMENT;
-      }
-      tab.hf[s] = make_int4(h.data_offset, h.nrow, h.ncol, 0);
-      tab.hfe[s] = make_float4(h.hx, h.hy, h.min_z, h.max_z);
-    }
-    if (t == GEO_MESH || t == GEO_CONVEX_MESH) {
-      if (!tb->shape_mesh_host || !tb->shape_mesh_host[s0]) return VBD_ERR_INVALID_ARGUMENT;
-      for (int k = 0; k < 3; ++k)
-        if (!(sc[k] != 0.f) || !std::isfinite(sc[k])) return VBD_ERR_INVALID_ARGUMENT;
-      tab.mesh[s] = tb->shape_mesh_host[s0]->view;
-    }
+    const int rc = fill_shape_rec(tb, s0, tab.rec[m++]);
+    if (rc != VBD_OK) return rc;
   }
   cudaStream_t st = (cudaStream_t)stream;
   CK(cudaMemsetAsync(count, 0, sizeof(int), st));
   if (n == 0 || m == 0) return VBD_OK;
   bool worlds = false;
-  for (int s = 0; s < m; ++s) worlds = worlds || tab.world[s] != -1;
+  for (int s = 0; s < m; ++s) worlds = worlds || tab.rec[s].world != -1;
   auto kern = worlds && tb->particle_world_dev ? k_soft_contacts_shapes<true> : k_soft_contacts_shapes<false>;
   kern<<<(n + 255) / 256, 256, 0, st>>>(n, q, radius, flags, m, tab, tb->elevations_dev, tb->particle_world_dev,
                                          margin, cmax, count, particle, shape, body_pos, body_vel, normal);

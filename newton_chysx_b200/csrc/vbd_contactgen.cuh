@@ -1,0 +1,118 @@
+// One particle against one static shape, as create_soft_contacts does it (geometry/kernels.py:1001-1140): the
+// particle in the shape frame, the shape's signed distance and outward normal (analytic SDFs, heightfield query,
+// mesh query), and for d < margin + radius a contact at the closest surface point x_local - n d with the normal
+// mapped back to world, in a slot taken from an atomic counter. Shared by the kernel-parameter path (at most
+// kMaxContactShapes shapes per call) and the device-resident shape sets (any number of shapes and worlds).
+#pragma once
+#include <cmath>
+
+#include "vbd_b200.h"
+#include "vbd_mesh.cuh"
+#include "vbd_shapes.cuh"
+
+namespace vbd {
+
+// A static shape: transform (p, q xyzw), scale, and the data of its kind.
+struct ShapeRec {
+  float4 p;
+  float4 q;    // unit quaternion (x, y, z, w)
+  float4 sc;   // scale
+  int4 hf;     // heightfield grid (data_offset, nrow, ncol, 0)
+  float4 hfe;  // heightfield extents (hx, hy, min_z, max_z), scale applied
+  MeshView mesh;
+  int type;   // GeoType
+  int world;  // -1 = global
+  int id;     // index in the model
+  int pad;
+};
+
+__host__ __device__ __forceinline__ vec3<float> rot_q(float4 q, vec3<float> v) {
+  const vec3<float> u = {q.x, q.y, q.z};
+  return v * (2.f * q.w * q.w - 1.f) + cross(u, v) * (2.f * q.w) + u * (2.f * dot(u, v));
+}
+
+__device__ __forceinline__ void soft_contact_shape(const ShapeRec& sh, const float* __restrict__ elev,
+                                                   vec3<float> x, float r, float margin, int i, int cmax,
+                                                   int* count, int* particle, int* shape, float* body_pos,
+                                                   float* body_vel, float* normal) {
+  const float4 P = sh.p, Q = sh.q, SC = sh.sc;
+  const float4 Qi = make_float4(-Q.x, -Q.y, -Q.z, Q.w);
+  const vec3<float> xl = rot_q(Qi, vec3<float>{x.x - P.x, x.y - P.y, x.z - P.z});
+  const float sc[3] = {SC.x, SC.y, SC.z};
+  float d;
+  vec3<float> nn;
+  const int type = sh.type;
+  if (type == GEO_HFIELD) {
+    heightfield_sdf(sh.hf, sh.hfe, elev, xl, d, nn);
+  } else if (type == GEO_MESH || type == GEO_CONVEX_MESH) {  // geometry/kernels.py:1091-1113
+    d = 1.0e6f;
+    nn = {0.f, 0.f, 0.f};
+    const float ms = fminf(fminf(fabsf(sc[0]), fabsf(sc[1])), fabsf(sc[2]));
+    const vec3<float> xs = {xl.x / sc[0], xl.y / sc[1], xl.z / sc[2]};
+    vec3<float> cp;
+    float sg;
+    int face;
+    if (mesh_query_point_sign(sh.mesh, xs, margin + r / ms, cp, sg, face)) {
+      const vec3<float> delta = xl - vec3<float>{cp.x * sc[0], cp.y * sc[1], cp.z * sc[2]};
+      d = length(delta) * sg;
+      nn = geo_normalize(delta) * sg;
+    }
+  } else {
+    shape_sdf(type, xl, sc, d, nn);
+  }
+  if (d < margin + r) {
+    const int k = atomicAdd(count, 1);
+    if (k < cmax) {
+      const vec3<float> bp = rot_q(Q, xl - nn * d) + vec3<float>{P.x, P.y, P.z};
+      const vec3<float> wn = rot_q(Q, nn);
+      particle[k] = i;
+      shape[k] = sh.id;
+      body_pos[3 * k] = bp.x, body_pos[3 * k + 1] = bp.y, body_pos[3 * k + 2] = bp.z;
+      body_vel[3 * k] = body_vel[3 * k + 1] = body_vel[3 * k + 2] = 0.f;
+      normal[3 * k] = wn.x, normal[3 * k + 1] = wn.y, normal[3 * k + 2] = wn.z;
+    }
+  }
+}
+
+// Host: fills the record of model shape s0 from a VbdShapeTable and checks it, so that every device read the
+// record leads to stays in bounds. Returns VBD_OK, VBD_ERR_INVALID_ARGUMENT or VBD_ERR_UNSUPPORTED.
+inline int fill_shape_rec(const VbdShapeTable* tb, int s0, ShapeRec& rec) {
+  const int t = tb->shape_type_host[s0];
+  if (t != GEO_PLANE && t != GEO_SPHERE && t != GEO_CAPSULE && t != GEO_ELLIPSOID && t != GEO_CYLINDER &&
+      t != GEO_BOX && t != GEO_CONE && t != GEO_HFIELD && t != GEO_MESH && t != GEO_CONVEX_MESH)
+    return VBD_ERR_UNSUPPORTED;
+  const float* X = tb->shape_transform_host + 7 * s0;
+  const float* sc = tb->shape_scale_host + 3 * s0;
+  const float ql = std::sqrt(X[3] * X[3] + X[4] * X[4] + X[5] * X[5] + X[6] * X[6]);
+  if (!(ql > 0.f)) return VBD_ERR_INVALID_ARGUMENT;
+  rec = ShapeRec();
+  rec.type = t;
+  rec.id = s0;
+  rec.world = tb->shape_world_host ? tb->shape_world_host[s0] : -1;
+  rec.p = make_float4(X[0], X[1], X[2], 0.f);
+  rec.q = make_float4(X[3] / ql, X[4] / ql, X[5] / ql, X[6] / ql);
+  rec.sc = make_float4(sc[0], sc[1], sc[2], 0.f);
+  if (t == GEO_HFIELD) {  // every grid read of heightfield_sdf stays inside [data_offset, data_offset + nrow ncol)
+    if (!tb->shape_heightfield_index_host || !tb->heightfields_host) return VBD_ERR_INVALID_ARGUMENT;
+    const int k = tb->shape_heightfield_index_host[s0];
+    if (k < 0 || k >= tb->heightfield_count) return VBD_ERR_INVALID_ARGUMENT;
+    const VbdHeightfield& h = tb->heightfields_host[k];
+    if (h.nrow < 0 || h.ncol < 0 || h.data_offset < 0) return VBD_ERR_INVALID_ARGUMENT;
+    if (h.nrow > 1 && h.ncol > 1) {
+      if (!tb->elevations_dev || int64_t(h.data_offset) + int64_t(h.nrow) * h.ncol > tb->elevation_count ||
+          !(h.hx > 0.f) || !(h.hy > 0.f) || !std::isfinite(h.hx) || !std::isfinite(h.hy))
+        return VBD_ERR_INVALID_ARGUMENT;
+    }
+    rec.hf = make_int4(h.data_offset, h.nrow, h.ncol, 0);
+    rec.hfe = make_float4(h.hx, h.hy, h.min_z, h.max_z);
+  }
+  if (t == GEO_MESH || t == GEO_CONVEX_MESH) {
+    if (!tb->shape_mesh_host || !tb->shape_mesh_host[s0]) return VBD_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < 3; ++k)
+      if (!(sc[k] != 0.f) || !std::isfinite(sc[k])) return VBD_ERR_INVALID_ARGUMENT;
+    rec.mesh = tb->shape_mesh_host[s0]->view;
+  }
+  return VBD_OK;
+}
+
+}  // namespace vbd

@@ -958,8 +958,14 @@ class Model:
                     if dev.type == "cuda":
                         m._device_meshes.append(_DeviceMesh(sh["src"]))
                 m.shape_mesh_index[i] = seen[key]
+        m._shape_set = _ShapeSet(m) if dev.type == "cuda" and S > 0 else None
         m.body_com = None
         return m
+
+    def refresh_shapes(self):
+        """Re-upload the shapes to the GPU after their host arrays (shape_transform, shape_scale, shape_type,
+        shape_flags, shape_world, heightfields) were changed in place."""
+        self._shape_set = _ShapeSet(self) if self.device.type == "cuda" and self.shape_count > 0 else None
 
     def set_gravity(self, gravity, world=None):
         g = torch.as_tensor(gravity, dtype=torch.float32, device=self.device).reshape(-1, 3)
@@ -1037,44 +1043,71 @@ class Contacts:
         self.soft_contact_count.zero_()
 
 
-def soft_contacts(model: Model, state: State, contacts: Contacts, margin: float):
-    """Particle contacts against the model's static shapes on the GPU (``vbd_soft_contacts_table``)."""
-    lib = _lib.load()
+def _shape_table(model: Model):
+    """The model's shapes as a ``VbdShapeTable`` (the reference Model's layout), with the host arrays it points to."""
     S = model.shape_count
-    if S == 0:
-        contacts.soft_contact_count.zero_()
-        return
     ip, fp = C.POINTER(C.c_int32), C.POINTER(C.c_float)
-    st = np.ascontiguousarray(model.shape_type, dtype=np.int32)
-    sx = np.ascontiguousarray(model.shape_transform, dtype=np.float32)
-    ss = np.ascontiguousarray(model.shape_scale, dtype=np.float32)
-    hidx = np.ascontiguousarray(getattr(model, "shape_heightfield_index", np.full(S, -1)), dtype=np.int32)
+    keep = dict(
+        st=np.ascontiguousarray(model.shape_type, dtype=np.int32),
+        sx=np.ascontiguousarray(model.shape_transform, dtype=np.float32),
+        ss=np.ascontiguousarray(model.shape_scale, dtype=np.float32),
+        hidx=np.ascontiguousarray(getattr(model, "shape_heightfield_index", np.full(S, -1)), dtype=np.int32),
+        sfl=np.ascontiguousarray(getattr(model, "shape_flags", np.full(S, 4)), dtype=np.int32),
+        swl=np.ascontiguousarray(getattr(model, "shape_world", np.full(S, -1)), dtype=np.int32),
+    )  # fmt: skip
     rows = getattr(model, "heightfield_data", np.zeros((0, 7)))
-    hfs = (_lib.VbdHeightfield * max(len(rows), 1))()
+    keep["hfs"] = hfs = (_lib.VbdHeightfield * max(len(rows), 1))()
     for k, r in enumerate(rows):
         hfs[k] = _lib.VbdHeightfield(int(r[0]), int(r[1]), int(r[2]), *(float(v) for v in r[3:]))
     elev = getattr(model, "heightfield_elevations", None)
     midx = getattr(model, "shape_mesh_index", np.full(S, -1))
     dmeshes = getattr(model, "_device_meshes", [])
-    handles = (C.c_void_p * S)(*[dmeshes[k].handle if k >= 0 else None for k in midx])
-    sfl = np.ascontiguousarray(getattr(model, "shape_flags", np.full(S, 4)), dtype=np.int32)
-    swl = np.ascontiguousarray(getattr(model, "shape_world", np.full(S, -1)), dtype=np.int32)
-    pw = getattr(model, "particle_world", None)
+    keep["handles"] = handles = (C.c_void_p * max(S, 1))(*[dmeshes[k].handle if k >= 0 else None for k in midx])
     tb = _lib.VbdShapeTable(
-        S, st.ctypes.data_as(ip), sx.ctypes.data_as(fp), ss.ctypes.data_as(fp), hidx.ctypes.data_as(ip), len(rows),
-        hfs, None if elev is None else elev.data_ptr(), 0 if elev is None else elev.numel(),
-        C.cast(handles, C.POINTER(C.c_void_p)), sfl.ctypes.data_as(ip), swl.ctypes.data_as(ip),
-        None if pw is None else pw.data_ptr(),
+        S, keep["st"].ctypes.data_as(ip), keep["sx"].ctypes.data_as(fp), keep["ss"].ctypes.data_as(fp),
+        keep["hidx"].ctypes.data_as(ip), len(rows), hfs, None if elev is None else elev.data_ptr(),
+        0 if elev is None else elev.numel(), C.cast(handles, C.POINTER(C.c_void_p)), keep["sfl"].ctypes.data_as(ip),
+        keep["swl"].ctypes.data_as(ip), None,
     )  # fmt: skip
+    return tb, keep
+
+
+class _ShapeSet:
+    """The model's shapes on the GPU (``vbd_shape_set_create``), built once at finalize, freed with the model."""
+
+    def __init__(self, model: Model):
+        self._lib = _lib.load()
+        tb, keep = _shape_table(model)
+        h = C.c_void_p()
+        _lib.check(self._lib.vbd_shape_set_create(C.byref(tb), C.byref(h)), "vbd_shape_set_create")
+        self.handle = h.value
+        del keep
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            self._lib.vbd_shape_set_destroy(self.handle)
+            self.handle = None
+
+
+def soft_contacts(model: Model, state: State, contacts: Contacts, margin: float):
+    """Particle contacts against the model's static shapes on the GPU (``vbd_soft_contacts_set``): any number of
+    shapes; a particle of world w meets the global shapes and world w's."""
+    lib = _lib.load()
+    if model.shape_count == 0:
+        contacts.soft_contact_count.zero_()
+        return
+    if getattr(model, "_shape_set", None) is None:
+        model._shape_set = _ShapeSet(model)
+    pw = getattr(model, "particle_world", None)
     stream = torch.cuda.current_stream(model.device).cuda_stream
-    rc = lib.vbd_soft_contacts_table(
-        model.particle_count, state.particle_q.data_ptr(), model.particle_radius.data_ptr(),
-        model.particle_flags.data_ptr(), C.byref(tb), float(margin), contacts.soft_contact_max,
-        contacts.soft_contact_count.data_ptr(), contacts.soft_contact_particle.data_ptr(),
+    rc = lib.vbd_soft_contacts_set(
+        model._shape_set.handle, model.particle_count, state.particle_q.data_ptr(), model.particle_radius.data_ptr(),
+        model.particle_flags.data_ptr(), None if pw is None else pw.data_ptr(), float(margin),
+        contacts.soft_contact_max, contacts.soft_contact_count.data_ptr(), contacts.soft_contact_particle.data_ptr(),
         contacts.soft_contact_shape.data_ptr(), contacts.soft_contact_body_pos.data_ptr(),
         contacts.soft_contact_body_vel.data_ptr(), contacts.soft_contact_normal.data_ptr(), C.c_void_p(stream),
     )  # fmt: skip
-    _lib.check(rc, "vbd_soft_contacts_table")
+    _lib.check(rc, "vbd_soft_contacts_set")
 
 
 class CollisionPipeline:

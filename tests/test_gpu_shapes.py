@@ -426,3 +426,53 @@ def test_collision_pipeline_worlds_match_oracle():
     near -= set(zip(lo[1][:lo[0]].tolist(), lo[2][:lo[0]].tolist()))
     assert {sh for _, sh in gpu} == {0, 1, 3}
     _compare(gpu, list(zip(p[:cnt].tolist(), s[:cnt].tolist())), bp[:cnt], nn[:cnt], near)
+
+
+def test_many_worlds_and_shapes_match_oracle():
+    """More shapes than one kernel parameter table holds: 40 worlds with a sphere and a rotated box each (80 world
+    shapes), a global ground plane, a global capsule that does not collide with particles, and particles in every
+    world plus 2,000 global particles (which meet every shape), through the model's device shape set."""
+    rng = np.random.default_rng(12)
+    top = sim.ModelBuilder(up_axis="Z")
+    q = sim.quat_from_axis_angle((0.3, 1.0, 0.2), 0.7)
+    for w in range(40):
+        b = sim.ModelBuilder(up_axis="Z")
+        pts = np.stack([rng.uniform(-0.5, 0.5, 500), rng.uniform(-0.5, 0.5, 500), rng.uniform(-0.02, 0.5, 500)], 1)
+        b.add_particles(pts, (0.0, 0.0, 0.0), 1.0, radius=0.01)
+        c = rng.uniform(-0.2, 0.2, 2)
+        b.add_shape_sphere(xform=((c[0], c[1], 0.2), sim.quat_identity()), radius=0.15)
+        b.add_shape_box(xform=((-c[0], -c[1], 0.25), q), hx=0.1, hy=0.15, hz=0.05)
+        top.add_world(b)
+    pts = np.stack([rng.uniform(-0.5, 0.5, 2000), rng.uniform(-0.5, 0.5, 2000), rng.uniform(-0.02, 0.5, 2000)], 1)
+    top.add_particles(pts, (0.0, 0.0, 0.0), 1.0, radius=0.01)
+    top.add_ground_plane()
+    top.add_shape_capsule(xform=((0.0, 0.0, 0.2), q), radius=0.2, half_height=0.2,
+                          cfg=sim.ShapeConfig(has_particle_collision=False))  # fmt: skip
+    m = top.finalize("cuda")
+    assert m.shape_count == 82 and (m.shape_world[:80] >= 0).all() and list(m.shape_world[80:]) == [-1, -1]
+    pipe = sim.CollisionPipeline(m, soft_contact_max=200000, soft_contact_margin=0.01)
+    contacts = pipe.contacts()
+    pipe.collide(m.state(), contacts)
+    torch.cuda.synchronize()
+    k = int(contacts.soft_contact_count.item())
+    gpu = {(int(a), int(s)): (x, y, z) for a, s, x, y, z in zip(
+        contacts.soft_contact_particle[:k].cpu().numpy(), contacts.soft_contact_shape[:k].cpu().numpy(),
+        contacts.soft_contact_body_pos[:k].cpu().numpy(), contacts.soft_contact_body_vel[:k].cpu().numpy(),
+        contacts.soft_contact_normal[:k].cpu().numpy())}  # fmt: skip
+    qf = m.particle_q.cpu().numpy().astype(np.float64)
+    r = m.particle_radius.cpu().numpy().astype(np.float64)
+    fl = m.particle_flags.cpu().numpy()
+    args = (m.shape_type, m.shape_transform.astype(np.float64), m.shape_scale.astype(np.float64))
+    kw = dict(shape_flags=m.shape_flags, shape_world=m.shape_world, particle_world=m.particle_world.cpu().numpy(),
+              max_contacts=200000)  # fmt: skip
+    cnt, p, s, bp, _, nn = orc.soft_contacts_shapes(qf, r, fl, *args, 0.01, **kw)
+    lo = orc.soft_contacts_shapes(qf, r, fl, *args, 0.01 - 1e-5, **kw)
+    hi = orc.soft_contacts_shapes(qf, r, fl, *args, 0.01 + 1e-5, **kw)
+    near = set(zip(hi[1][:hi[0]].tolist(), hi[2][:hi[0]].tolist()))
+    near -= set(zip(lo[1][:lo[0]].tolist(), lo[2][:lo[0]].tolist()))
+    assert k == cnt or abs(k - cnt) <= len(near)
+    pw = m.particle_world.cpu().numpy()
+    glob = np.flatnonzero(pw == -1)
+    assert {sh for pp, sh in gpu if pp in set(glob.tolist())} >= set(range(0, 80, 7))  # global particles meet worlds
+    assert 81 not in {sh for _, sh in gpu}
+    _compare(gpu, list(zip(p[:cnt].tolist(), s[:cnt].tolist())), bp[:cnt], nn[:cnt], near)
