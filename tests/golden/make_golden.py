@@ -259,6 +259,11 @@ def load_reference(ref: str) -> dict:
     )  # fmt: skip
     _lift(os.path.join(ref, "newton/_src/utils/heightfield.py"),
           {"_heightfield_surface_query", "sample_sdf_grad_heightfield"}, ns)  # fmt: skip
+    # the contact generation kernel itself, for analytic shapes and heightfields (no mesh shapes are launched)
+    ns["GeoType"] = types.SimpleNamespace(PLANE=1, HFIELD=2, SPHERE=3, CAPSULE=4, ELLIPSOID=5, CYLINDER=6, BOX=7, MESH=8,
+                                          CONE=9, CONVEX_MESH=10)  # fmt: skip
+    ns["ShapeFlags"] = types.SimpleNamespace(COLLIDE_PARTICLES=1 << 2)
+    _lift(os.path.join(ref, "newton/_src/geometry/kernels.py"), {"counter_increment", "create_soft_contacts"}, ns)
     _lift(os.path.join(ref, "newton/_src/utils/mesh.py"), set(), ns, classes={"MeshAdjacency": {"*"}})
     _lift(
         os.path.join(ref, "newton/_src/sim/builder.py"),
@@ -1032,6 +1037,62 @@ def shape_contact_cases_cone_hfield(ns, seed=19):
     return res
 
 
+def create_soft_contacts_cases(ns, seed=23):
+    """The reference's ``create_soft_contacts`` kernel (geometry/kernels.py:1001-1140) run as-is, one serial launch
+    over every (particle, shape) thread, so the contact list comes in thread order (particle-major). Three worlds
+    with their own shapes, global shapes, a shape without COLLIDE_PARTICLES, particles in every world and global
+    ones, inactive particles; planes, sphere, box, capsule, cylinder, cone, ellipsoid and a heightfield."""
+    rng = np.random.default_rng(seed)
+
+    def quat(axis, ang):
+        return wp.quat_from_axis_angle(np.asarray(axis, dtype=float), ang)
+
+    gx, gy = np.meshgrid(np.linspace(-1.0, 1.0, 9), np.linspace(-1.0, 1.0, 7))
+    raw = (0.1 * np.sin(2.0 * gx) * np.cos(3.0 * gy)).astype(np.float32)
+    elev = ((raw - raw.min()) / (raw.max() - raw.min())).astype(np.float32).reshape(-1)
+    hfd = types.SimpleNamespace(data_offset=0, nrow=7, ncol=9, hx=0.5, hy=0.4, min_z=0.0, max_z=0.12)
+    shapes = [  # type, position, rotation, scale, world, flags
+        (GEO_PLANE, (0.0, 0.0, 0.0), wp.quat_identity(), (0.0, 0.0, 0.0), -1, 4),
+        (GEO_SPHERE, (0.2, 0.1, 0.25), wp.quat_identity(), (0.2, 0.0, 0.0), 0, 4),
+        (GEO_BOX, (-0.2, 0.0, 0.25), quat((0.3, 1.0, 0.2), 0.7), (0.2, 0.15, 0.1), 1, 4),
+        (GEO_CAPSULE, (0.0, 0.2, 0.3), quat((1.0, 0.0, 0.3), 1.1), (0.1, 0.2, 0.0), 2, 4),
+        (GEO_CONE, (0.1, -0.2, 0.3), quat((0.2, 1.0, 0.0), 0.8), (0.25, 0.2, 0.0), 0, 4),
+        (GEO_CYLINDER, (0.0, 0.0, 0.3), quat((0.0, 1.0, 1.0), 0.5), (0.15, 0.1, 0.0), -1, 0),
+        (GEO_ELLIPSOID, (-0.1, -0.1, 0.45), quat((1.0, 1.0, 0.0), 0.9), (0.25, 0.2, 0.15), -1, 4),
+        (GEO_HFIELD, (0.0, 0.0, 0.02), quat((0.0, 0.0, 1.0), 0.3), (1.0, 1.0, 1.0), 2, 4),
+        (GEO_PLANE, (0.3, 0.3, 0.2), quat((1.0, 0.2, 0.0), 0.4), (0.6, 0.4, 0.0), 1, 4),
+    ]
+    n = 2400
+    q = np.stack([rng.uniform(-0.6, 0.6, n), rng.uniform(-0.6, 0.6, n), rng.uniform(-0.05, 0.6, n)], axis=1)
+    radius = rng.uniform(0.005, 0.02, n)
+    flags = np.where(rng.uniform(size=n) < 0.9, 1, 0).astype(np.int32)
+    pworld = rng.integers(-1, 3, n).astype(np.int32)
+    S, margin, cmax = len(shapes), 0.02, n * len(shapes)
+    shape_type = np.array([sh[0] for sh in shapes], dtype=np.int32)
+    shape_world = np.array([sh[4] for sh in shapes], dtype=np.int32)
+    shape_flags = np.array([sh[5] for sh in shapes], dtype=np.int32)
+    xforms = [(np.asarray(sh[1], dtype=float), np.asarray(sh[2], dtype=float)) for sh in shapes]
+    scales = [wp.vec3(*sh[3]) for sh in shapes]
+    count, tids = [0], [0] * (n * S)
+    out_p, out_s = [0] * cmax, [0] * cmax
+    out_bp, out_bv, out_n = [None] * cmax, [None] * cmax, [None] * cmax
+    hf_index = np.array([0 if t == GEO_HFIELD else -1 for t in shape_type], dtype=np.int32)
+    wp.launch(ns["create_soft_contacts"], n * S, [wp.vec3(*x) for x in q], radius, flags, pworld, [],
+              xforms, [-1] * S, shape_type, scales, [0] * S, shape_world, margin, cmax, S, shape_flags, hf_index,
+              [hfd], elev.astype(np.float64), count, out_p, out_s, out_bp, out_bv, out_n, tids)  # fmt: skip
+    k = count[0]
+    return dict(
+        q=q, radius=radius, flags=flags, particle_world=pworld, margin=np.float64(margin), shape_type=shape_type,
+        shape_world=shape_world, shape_flags=shape_flags,
+        shape_transform=np.array([list(sh[1]) + list(sh[2]) for sh in shapes], dtype=np.float64),
+        shape_scale=np.array([sh[3] for sh in shapes], dtype=np.float64), shape_heightfield_index=hf_index,
+        heightfields=np.array([[0, 7, 9, 0.5, 0.4, 0.0, 0.12]]), elevations=elev,
+        particle=np.array(out_p[:k], dtype=np.int32), shape=np.array(out_s[:k], dtype=np.int32),
+        body_pos=np.array([np.asarray(v) for v in out_bp[:k]]), body_vel=np.array([np.asarray(v) for v in out_bv[:k]]),
+        normal=np.array([np.asarray(v) for v in out_n[:k]]),
+    )  # fmt: skip
+
+
 def soft_cases(ns, seed=13):
     """Per-element goldens of the volumetric Neo-Hookean tetrahedron and of the spring."""
     rng = np.random.default_rng(seed)
@@ -1133,6 +1194,8 @@ def main():
     print("soft_contact_shapes.npz written")
     np.savez_compressed(os.path.join(args.out, "soft_contact_cone_hfield.npz"), **shape_contact_cases_cone_hfield(ns))
     print("soft_contact_cone_hfield.npz written")
+    np.savez_compressed(os.path.join(args.out, "create_soft_contacts.npz"), **create_soft_contacts_cases(ns))
+    print("create_soft_contacts.npz written")
     print("soft_elements.npz written")
 
     # Volumetric: a 3 x 2 x 2-cell tetrahedral block (add_soft_grid, 5 tetrahedra per cell, damped), 4 mm

@@ -476,3 +476,60 @@ def test_many_worlds_and_shapes_match_oracle():
     assert {sh for pp, sh in gpu if pp in set(glob.tolist())} >= set(range(0, 80, 7))  # global particles meet worlds
     assert 81 not in {sh for _, sh in gpu}
     _compare(gpu, list(zip(p[:cnt].tolist(), s[:cnt].tolist())), bp[:cnt], nn[:cnt], near)
+
+
+@pytest.mark.parametrize("path", ["table", "set"])
+def test_reference_create_soft_contacts_kernel_golden(path):
+    """Both device paths (the parameter table and the shape set) against the reference's ``create_soft_contacts``
+    kernel run as-is: worlds, the particle-collision flag, a heightfield and seven analytic shapes."""
+    g = load_golden("create_soft_contacts.npz")
+    lib = _lib.load()
+    dev = torch.device("cuda")
+    n, S = len(g["radius"]), len(g["shape_type"])
+    cmax = n * S
+    qd = torch.as_tensor(g["q"].astype(np.float32), device=dev).contiguous()
+    rd = torch.as_tensor(g["radius"].astype(np.float32), device=dev)
+    fd = torch.as_tensor(g["flags"], device=dev)
+    pw = torch.as_tensor(g["particle_world"], device=dev)
+    ev = torch.as_tensor(g["elevations"].astype(np.float32), device=dev)
+    cnt = torch.zeros(1, dtype=torch.int32, device=dev)
+    part = torch.full((cmax,), -1, dtype=torch.int32, device=dev)
+    shp = torch.full((cmax,), -1, dtype=torch.int32, device=dev)
+    bp, bv, nn = (torch.zeros((cmax, 3), dtype=torch.float32, device=dev) for _ in range(3))
+    ip, fp = C.POINTER(C.c_int32), C.POINTER(C.c_float)
+    arrs = dict(st=g["shape_type"].astype(np.int32), sx=g["shape_transform"].astype(np.float32),
+                ss=g["shape_scale"].astype(np.float32), hi=g["shape_heightfield_index"].astype(np.int32),
+                sf=g["shape_flags"].astype(np.int32), sw=g["shape_world"].astype(np.int32))  # fmt: skip
+    hf = g["heightfields"][0]
+    hfs = (_lib.VbdHeightfield * 1)(_lib.VbdHeightfield(int(hf[0]), int(hf[1]), int(hf[2]), *map(float, hf[3:])))
+    tb = _lib.VbdShapeTable(S, arrs["st"].ctypes.data_as(ip), arrs["sx"].ctypes.data_as(fp),
+                            arrs["ss"].ctypes.data_as(fp), arrs["hi"].ctypes.data_as(ip), 1, hfs, ev.data_ptr(),
+                            ev.numel(), None, arrs["sf"].ctypes.data_as(ip), arrs["sw"].ctypes.data_as(ip),
+                            pw.data_ptr())  # fmt: skip
+    outs = (cmax, cnt.data_ptr(), part.data_ptr(), shp.data_ptr(), bp.data_ptr(), bv.data_ptr(), nn.data_ptr(), None)
+    if path == "table":
+        rc = lib.vbd_soft_contacts_table(n, qd.data_ptr(), rd.data_ptr(), fd.data_ptr(), C.byref(tb), float(g["margin"]),
+                                         *outs)  # fmt: skip
+        _lib.check(rc, "vbd_soft_contacts_table")
+        torch.cuda.synchronize()
+    else:
+        h = C.c_void_p()
+        _lib.check(lib.vbd_shape_set_create(C.byref(tb), C.byref(h)), "vbd_shape_set_create")
+        rc = lib.vbd_soft_contacts_set(h, n, qd.data_ptr(), rd.data_ptr(), fd.data_ptr(), pw.data_ptr(),
+                                       float(g["margin"]), *outs)  # fmt: skip
+        _lib.check(rc, "vbd_soft_contacts_set")
+        torch.cuda.synchronize()
+        lib.vbd_shape_set_destroy(h)
+    k = int(cnt.item())
+    gpu = {(int(a), int(b)): (x, y, z) for a, b, x, y, z in zip(
+        part[:k].cpu().numpy(), shp[:k].cpu().numpy(), bp[:k].cpu().numpy(), bv[:k].cpu().numpy(),
+        nn[:k].cpu().numpy())}  # fmt: skip
+    kw = dict(heightfield_index=g["shape_heightfield_index"], heightfields=g["heightfields"], elevations=g["elevations"],
+              shape_flags=g["shape_flags"], shape_world=g["shape_world"], particle_world=g["particle_world"])  # fmt: skip
+    args = (g["q"], g["radius"], g["flags"], g["shape_type"], g["shape_transform"], g["shape_scale"])
+    lo = orc.soft_contacts_shapes(*args, float(g["margin"]) - 1e-5, **kw)
+    hi_ = orc.soft_contacts_shapes(*args, float(g["margin"]) + 1e-5, **kw)
+    near = set(zip(hi_[1][:hi_[0]].tolist(), hi_[2][:hi_[0]].tolist()))
+    near -= set(zip(lo[1][:lo[0]].tolist(), lo[2][:lo[0]].tolist()))
+    pairs = list(zip(g["particle"].tolist(), g["shape"].tolist()))
+    _compare(gpu, pairs, g["body_pos"], g["normal"], near)

@@ -178,3 +178,26 @@ def test_shape_worlds_and_particle_collision_flag():
     # without the filters the same particles also touch the other worlds' spheres
     cnt_all, _, s_all, _, _, _ = orc.soft_contacts_shapes(*args)
     assert cnt_all > cnt and set(s_all[:cnt_all].tolist()) == {0, 1, 2, 3}
+
+
+def test_oracle_matches_reference_create_soft_contacts_kernel():
+    """The reference's ``create_soft_contacts`` kernel itself, run serially through the Warp stand-in: three worlds
+    with their own shapes, global shapes, a shape without COLLIDE_PARTICLES, inactive and global particles, and a
+    heightfield. A serial launch lists contacts in thread order (particle-major), the oracle's loop order, so the
+    lists must agree entry by entry."""
+    g = load_golden("create_soft_contacts.npz")
+    cnt, p, s, bp, bv, nn = orc.soft_contacts_shapes(
+        g["q"], g["radius"], g["flags"], g["shape_type"], g["shape_transform"], g["shape_scale"], float(g["margin"]),
+        heightfield_index=g["shape_heightfield_index"], heightfields=g["heightfields"], elevations=g["elevations"],
+        shape_flags=g["shape_flags"], shape_world=g["shape_world"], particle_world=g["particle_world"])  # fmt: skip
+    assert cnt == len(g["particle"]) and cnt > 500
+    np.testing.assert_array_equal(p[:cnt], g["particle"])
+    np.testing.assert_array_equal(s[:cnt], g["shape"])
+    assert np.abs(bp[:cnt] - g["body_pos"]).max() <= 1e-12
+    assert np.abs(nn[:cnt] - g["normal"]).max() <= 1e-12
+    assert np.abs(bv[:cnt]).max() == 0.0
+    # every filter is exercised: the non-colliding shape has no contact, cross-world pairs are absent, global
+    # particles touch world shapes
+    pw, sw = g["particle_world"][g["particle"]], g["shape_world"][g["shape"]]
+    assert 5 not in set(g["shape"].tolist())
+    assert ((pw == -1) | (sw == -1) | (pw == sw)).all() and ((pw == -1) & (sw >= 0)).any()
