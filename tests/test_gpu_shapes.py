@@ -533,3 +533,30 @@ def test_reference_create_soft_contacts_kernel_golden(path):
     near -= set(zip(lo[1][:lo[0]].tolist(), lo[2][:lo[0]].tolist()))
     pairs = list(zip(g["particle"].tolist(), g["shape"].tolist()))
     _compare(gpu, pairs, g["body_pos"], g["normal"], near)
+
+
+def test_shape_set_contact_overflow():
+    """More contacts than soft_contact_max through the shape set: the count reports them all, as the reference's
+    counter does, only the first soft_contact_max slots are written, and the slots past them stay untouched."""
+    m = _world_scene_many()
+    full = sim.CollisionPipeline(m, soft_contact_max=m.particle_count * m.shape_count, soft_contact_margin=0.01)
+    cf = full.contacts()
+    full.collide(m.state(), cf)
+    small = sim.CollisionPipeline(m, soft_contact_max=50, soft_contact_margin=0.01)
+    cs = small.contacts()
+    cs.soft_contact_particle = torch.full((60,), -7, dtype=torch.int32, device="cuda")  # 10 guard slots
+    small.collide(m.state(), cs)
+    torch.cuda.synchronize()
+    total = int(cf.soft_contact_count.item())
+    assert total > 50 and int(cs.soft_contact_count.item()) == total
+    written = cs.soft_contact_particle[:50].cpu().numpy()
+    assert (written >= 0).all() and (written < m.particle_count).all()
+    assert (cs.soft_contact_particle[50:].cpu().numpy() == -7).all()
+    pairs = set(zip(cf.soft_contact_particle[:total].cpu().tolist(), cf.soft_contact_shape[:total].cpu().tolist()))
+    assert set(zip(written.tolist(), cs.soft_contact_shape[:50].cpu().tolist())) <= pairs
+
+
+def _world_scene_many():
+    from tests.test_oracle_shapes import _world_scene
+
+    return _world_scene("cuda")
