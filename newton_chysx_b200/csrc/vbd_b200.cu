@@ -133,35 +133,7 @@ __global__ void k_soft_contacts(int n, const float* __restrict__ q, const float*
 }
 
 // The shapes of one vbd_soft_contacts_table call, passed by value as a kernel parameter.
-struct ShapeParamTable {
-  ShapeRec rec[kMaxContactShapes];
-};
-
-// create_soft_contacts (geometry/kernels.py:1001-1140) over a parameter table: one thread per particle, looping over
-// the shapes (the reference launches one thread per (particle, shape); here the shape, hence the branch taken, is
-// the same across a warp). WORLDS: some shape belongs to a world (else the world filter can never apply and is
-// compiled out). Four 256-thread CTAs per SM: the loop is latency-bound, and 4 resident CTAs ran faster than 3.
-template <bool WORLDS>
-__global__ void __launch_bounds__(256, 4)
-    k_soft_contacts_shapes(int n, const float* __restrict__ q, const float* __restrict__ radius,
-                           const int* __restrict__ flags, int S, const ShapeParamTable shapes,
-                           const float* __restrict__ elev, const int* __restrict__ particle_world, float margin,
-                           int cmax, int* count, int* particle, int* shape, float* body_pos, float* body_vel,
-                           float* normal) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || !(flags[i] & 1)) return;
-  const vec3<float> x = {q[3 * i], q[3 * i + 1], q[3 * i + 2]};
-  const float r = radius[i];
-  const int pw = WORLDS && particle_world ? particle_world[i] : -1;
-  for (int s = 0; s < S; ++s) {
-    if (WORLDS) {  // other world (geometry/kernels.py:1036-1043)
-      const int sw = shapes.rec[s].world;
-      if (pw != -1 && sw != -1 && pw != sw) continue;
-    }
-    soft_contact_shape(shapes.rec[s], elev, x, r, margin, i, cmax, count, particle, shape, body_pos, body_vel,
-                       normal);
-  }
-}
+static_assert(kMaxContactShapes == kParamTableShapes, "one parameter-table size");
 
 }  // namespace
 

@@ -22,6 +22,8 @@ struct VbdShapeSetImpl {
   int m, n_global, W;
   const float* elev;
   void* buffer;
+  vbd::ShapeParamTable small;  // the records again when m <= kParamTableShapes: launched as a kernel parameter
+  bool worlds;                 // some shape belongs to a world
 };
 
 namespace {
@@ -111,6 +113,8 @@ int vbd_shape_set_create(const VbdShapeTable* tb, VbdShapeSetHandle* out) {
   set->W = W;
   set->elev = tb->elevations_dev;
   set->buffer = buf;
+  set->worlds = W > 0;
+  if (m <= vbd::kParamTableShapes) std::copy(recs.begin(), recs.end(), set->small.rec);
   *out = set;
   return VBD_OK;
 }
@@ -132,6 +136,12 @@ int vbd_soft_contacts_set(VbdShapeSetHandle set, int32_t n, const float* q, cons
   cudaStream_t st = (cudaStream_t)stream;
   if (cudaMemsetAsync(count, 0, sizeof(int), st) != cudaSuccess) return VBD_ERR_CUDA;
   if (n == 0 || set->m == 0) return VBD_OK;
+  if (set->m <= vbd::kParamTableShapes) {  // small sets: records in the constant bank measured faster
+    auto kern = set->worlds && particle_world ? vbd::k_soft_contacts_shapes<true> : vbd::k_soft_contacts_shapes<false>;
+    kern<<<(n + 255) / 256, 256, 0, st>>>(n, q, radius, flags, set->m, set->small, set->elev, particle_world, margin,
+                                           cmax, count, particle, shape, body_pos, body_vel, normal);
+    return cudaGetLastError() == cudaSuccess ? VBD_OK : VBD_ERR_CUDA;
+  }
   k_soft_contacts_set<<<(n + 255) / 256, 256, 0, st>>>(n, q, radius, flags, particle_world, set->recs, set->m,
                                                        set->global, set->n_global, set->world_off, set->world_list,
                                                        set->W, set->elev, margin, cmax, count, particle, shape,
