@@ -43,7 +43,7 @@ DT = 1.0 / 600.0
 # DRAM bytes (read + write) per vertex-iteration of the solve kernel, from one ncu capture per layout of the
 # first 512 instances of this workload; the traffic of a full launch scales with its vertex-iterations.
 NCU_TRAFFIC_PER_VI = {
-    "ell16": (513.0, "ncu capture, 512 instances (profiles/k_persistent_ell16_batched512.md), scaled by vertex-iterations"),
+    "ell16": (513.0, "ncu capture of the first 512 instances of this batch, scaled by vertex-iterations"),
 }
 
 
@@ -65,7 +65,7 @@ def instance_params(seed: int, count: int):
     return sides, E, bend, pins
 
 
-def build_instance(n, E, bend, pins, world_index):
+def build_instance(n, E, bend, pins):
     from newton_chysx_b200 import sim
 
     nu, h, density = 0.3, 1.0e-3, 0.2
@@ -73,8 +73,9 @@ def build_instance(n, E, bend, pins, world_index):
     lam = E * h * nu / (1.0 - nu * nu)
     b = sim.ModelBuilder(up_axis="Z", gravity=-9.81)
     cell = 1.0 / (n - 1)
-    col, row = world_index % 64, world_index // 64
-    b.add_cloth_grid(pos=(1.5 * col, 1.5 * row, 0.6), rot=sim.quat_identity(), vel=(0.0, 0.0, 0.0), dim_x=n - 1,
+    # every instance sits in its own frame, its corner at the origin: worlds do not interact, and far from the
+    # origin FP32 positions would round to ~8e-6 m at 96 m (an offset grid of 64 x 64 instances 1.5 m apart)
+    b.add_cloth_grid(pos=(0.0, 0.0, 0.6), rot=sim.quat_identity(), vel=(0.0, 0.0, 0.0), dim_x=n - 1,
                      dim_y=n - 1, cell_x=cell, cell_y=cell, mass=density / (n * n), tri_ke=mu, tri_ka=lam, tri_kd=0.0,
                      edge_ke=bend, edge_kd=0.0, particle_radius=5.0e-3)  # fmt: skip
     corners = [0, n - 1, n * (n - 1), n * n - 1]
@@ -86,8 +87,8 @@ def build_instance(n, E, bend, pins, world_index):
     return b
 
 
-def _instance_from_template(tpl, n, E, bend, pins, world_index):
-    """A copy of the side-n template builder with this instance's materials, pins and placement.
+def _instance_from_template(tpl, n, E, bend, pins):
+    """A copy of the side-n template builder with this instance's materials and pins.
 
     Topology, rest poses, areas, rest angles and the coloring depend only on n (materials scale
     the triangle/hinge stiffnesses but never zero them, so the coloring graph is unchanged)."""
@@ -103,8 +104,7 @@ def _instance_from_template(tpl, n, E, bend, pins, world_index):
     props = tpl.edge_bending_properties.copy()
     props[:, 0] = bend
     b._edge_prop = [props]
-    col, row = world_index % 64, world_index // 64
-    b._q = [tpl.particle_q + np.array([1.5 * col, 1.5 * row, 0.0])]
+    b._q = [tpl.particle_q.copy()]
     flags = tpl.particle_flags.copy()
     corners = [0, n - 1, n * (n - 1), n * n - 1]
     for c in pins:
@@ -113,47 +113,84 @@ def _instance_from_template(tpl, n, E, bend, pins, world_index):
     return b
 
 
-def build_batch(seed: int, count: int):
+_TEMPLATES: dict[int, object] = {}
+
+
+def templates(sides):
+    """Side-n template builders (E 1e4, bending 1e-4, no pins), built once per side and shared by every
+    batch this process builds."""
+    for n in np.unique(np.asarray(sides)):
+        if int(n) not in _TEMPLATES:
+            _TEMPLATES[int(n)] = build_instance(int(n), 1.0e4, 1.0e-4, [])
+    return _TEMPLATES
+
+
+def build_batch_indices(seed: int, count: int, indices):
+    """Instances `indices` (increasing) of the count-instance batch of `seed` as the worlds of one builder,
+    each with its own materials and pins, and a ground plane."""
     from newton_chysx_b200 import sim
 
     sides, E, bend, pins = instance_params(seed, count)
-    templates = {int(n): build_instance(int(n), 1.0e4, 1.0e-4, [], 0) for n in np.unique(sides)}
+    indices = np.asarray(indices, dtype=np.int64)
+    tpl = templates(sides[indices])
     top = sim.ModelBuilder(up_axis="Z", gravity=-9.81)
-    for i in range(count):
+    for i in indices:
         n = int(sides[i])
-        top.add_world(_instance_from_template(templates[n], n, float(E[i]), float(bend[i]), pins[i], i))
-    top.add_ground_plane()
-    return top, sides
-
-
-def build_batch_range(seed: int, count: int, lo: int, hi: int):
-    """Instances lo..hi-1 of build_batch(seed, count), with the same materials, pins and placement."""
-    from newton_chysx_b200 import sim
-
-    sides, E, bend, pins = instance_params(seed, count)
-    templates = {int(n): build_instance(int(n), 1.0e4, 1.0e-4, [], 0) for n in np.unique(sides[lo:hi])}
-    top = sim.ModelBuilder(up_axis="Z", gravity=-9.81)
-    for i in range(lo, hi):
-        n = int(sides[i])
-        top.add_world(_instance_from_template(templates[n], n, float(E[i]), float(bend[i]), pins[i], i))
+        top.add_world(_instance_from_template(tpl[n], n, float(E[i]), float(bend[i]), pins[i]))
     top.add_ground_plane()
     return top
 
 
-def run_e2e(args, rank, dev, dist, states, shape, vi_step, world):
-    """End-to-end rate: host-resident state of the whole batch, per substep H2D of (q, qd), contacts, step and
+def build_batch(seed: int, count: int):
+    top = build_batch_indices(seed, count, np.arange(count))
+    return top, instance_params(seed, count)[0]
+
+
+def lpt_partition(costs, parts: int):
+    """Longest-processing-time-first assignment: instances in decreasing cost, each to the shard with the
+    least cost so far (ties to the lower shard). Returns each shard's instance indices in increasing order
+    and the shards' total costs."""
+    import heapq
+
+    costs = np.asarray(costs, dtype=np.float64)
+    order = np.argsort(-costs, kind="stable")
+    heap = [(0.0, r) for r in range(parts)]
+    shards: list[list[int]] = [[] for _ in range(parts)]
+    load = np.zeros(parts)
+    for i in order:
+        c, r = heapq.heappop(heap)
+        shards[r].append(int(i))
+        load[r] = c + costs[i]
+        heapq.heappush(heap, (load[r], r))
+    return [np.sort(np.asarray(s, dtype=np.int64)) for s in shards], load
+
+
+def shard_plan(seed: int, per_rank: int, world: int):
+    """One global batch of per_rank x world instances, split over the ranks by LPT on V_i x C_i (vertices
+    times colors, the persistent kernel's work per instance). Weak scaling: each rank gets about per_rank
+    instances' worth of work. With one rank the shard is the whole batch in its original order."""
+    total = per_rank * world
+    sides = instance_params(seed, total)[0]
+    tpl = templates(sides)
+    colors = np.array([len(tpl[int(n)]._color_groups) for n in sides], dtype=np.float64)
+    shards, load = lpt_partition(sides.astype(np.float64) ** 2 * colors, world)
+    return total, shards, load
+
+
+def run_e2e(args, dev, dist, states, shape, total, shard, vi_all_ranks):
+    """End-to-end rate: host-resident state of the rank's shard, per substep H2D of (q, qd), contacts, step and
     D2H of (q, qd), over --e2e-chunks instance groups pipelined on separate streams."""
     import torch
 
     import newton_chysx_b200 as nb
 
     C = max(1, args.e2e_chunks)
-    bounds = [round(args.instances * c / C) for c in range(C + 1)]
+    bounds = [round(len(shard) * c / C) for c in range(C + 1)]
     hq_all = states[0].particle_q.cpu()
     hqd_all = states[0].particle_qd.cpu()
     chunks, v0 = [], 0
     for c in range(C):
-        model = build_batch_range(rank_seed(args.seed, rank), args.instances, bounds[c], bounds[c + 1]).finalize(dev)
+        model = build_batch_indices(args.seed, total, shard[bounds[c]:bounds[c + 1]]).finalize(dev)
         model.soft_contact_ke, model.soft_contact_kd, model.soft_contact_mu = 1.0e3, 10.0, 0.5
         solver = nb.SolverVBD(model, iterations=ITERATIONS, **shape)
         pipe = nb.CollisionPipeline(model, soft_contact_margin=0.01)
@@ -212,7 +249,7 @@ def run_e2e(args, rank, dev, dist, states, shape, vi_step, world):
     d2h = sum(2 * ch["oq"].numel() * 4 for ch in chunks)
     for ch in chunks:
         ch["graph"] = None
-    return {"value": world * vi_step * Ke / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+    return {"value": vi_all_ranks * Ke / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "steps": Ke, "chunks": C, "ms_per_step": ms / Ke}  # fmt: skip
 
 
@@ -226,11 +263,6 @@ def max_over_ranks(values, device=None):
     t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return [float(v) for v in t.tolist()]
-
-
-def rank_seed(seed: int, rank: int) -> int:
-    """Each rank simulates its own batch of the same size (weak scaling, no data-path collective)."""
-    return seed + rank
 
 
 def bytes_per_vertex_iteration(V, T, E, contacts=True):
@@ -306,34 +338,40 @@ def run_ours(args):
     torch.cuda.set_device(dev)
 
     t0 = time.time()
+    total, shards, load = shard_plan(args.seed, args.instances, world)
+    shard = shards[rank]
+    sides_all = instance_params(args.seed, total)[0]
     if args.tune:
-        # launch shape from the autotuner, timed on the batch's first instances (same size distribution)
+        # launch shape from the autotuner, timed on the shard's first instances (same size distribution)
         from newton_chysx_b200 import autotune
 
-        sub, _ = build_batch(rank_seed(args.seed, rank), min(args.instances, args.tune_instances))
-        sub_model = sub.finalize(dev)
+        sub_model = build_batch_indices(args.seed, total, shard[: args.tune_instances]).finalize(dev)
         sub_model.soft_contact_ke, sub_model.soft_contact_kd, sub_model.soft_contact_mu = 1.0e3, 10.0, 0.5
         shape = autotune.tune(sub_model, schedule="persistent", iterations=ITERATIONS, dt=DT)
-        del sub, sub_model
+        del sub_model
     else:
         shape = dict(schedule="persistent", lanes_per_vertex=args.lanes, block_size=args.block,
                      positions_in_shared=args.shared, layout=args.layout, min_blocks_per_sm=args.occ,
                      pair_vertices=args.pair)  # fmt: skip
     tune_s = time.time() - t0
-    builder, sides = build_batch(rank_seed(args.seed, rank), args.instances)
-    model = builder.finalize(dev)
+    model = build_batch_indices(args.seed, total, shard).finalize(dev)
     model.soft_contact_ke, model.soft_contact_kd, model.soft_contact_mu = 1.0e3, 10.0, 0.5
     solver = nb.SolverVBD(model, iterations=ITERATIONS, **shape)
     pipe = nb.CollisionPipeline(model, soft_contact_margin=0.01)
     contacts = pipe.contacts()
     setup_s = time.time() - t0
     V, T, E = model.particle_count, model.tri_count, model.edge_count
+    assert V == int(np.sum(sides_all[shard].astype(np.int64) ** 2)), "the model must hold the shard's instances"
+    vi_all_ranks = float(np.sum(sides_all.astype(np.float64) ** 2)) * ITERATIONS  # every rank's vertices
     states = [model.state(), model.state()]
 
-    # settle the batch for a few substeps so that contacts and motion are present, then capture
-    for k in range(max(args.warmup, 3)):
-        pipe.collide(states[k % 2], contacts)
-        solver.step(states[k % 2], states[(k + 1) % 2], None, contacts, DT)
+    # settle the batch for a few substeps so that contacts and motion are present, then capture; substep n reads
+    # states[n % 2] and writes states[(n + 1) % 2] through every phase, so the batch follows one trajectory
+    nsub = 0
+    for _ in range(max(args.warmup, 3)):
+        pipe.collide(states[nsub % 2], contacts)
+        solver.step(states[nsub % 2], states[(nsub + 1) % 2], None, contacts, DT)
+        nsub += 1
     torch.cuda.synchronize()
     stream = torch.cuda.Stream(dev)
     stream.wait_stream(torch.cuda.current_stream(dev))
@@ -347,9 +385,10 @@ def run_ours(args):
                 solver.step(states[p], states[1 - p], None, contacts, DT)
     torch.cuda.current_stream(dev).wait_stream(stream)
     torch.cuda.synchronize()
-    for k in range(args.warmup):
-        g_collide[k % 2].replay()
-        g_solve[k % 2].replay()
+    for _ in range(args.warmup):
+        g_collide[nsub % 2].replay()
+        g_solve[nsub % 2].replay()
+        nsub += 1
     torch.cuda.synchronize()
 
     K = args.steps
@@ -358,26 +397,33 @@ def run_ours(args):
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    n0 = nsub
     with ClockSampler(dev.index) as clocks:
         ev0.record()
         for k in range(K):
-            g_collide[k % 2].replay()
+            g_collide[(n0 + k) % 2].replay()
             ev[k][0].record()
-            g_solve[k % 2].replay()
+            g_solve[(n0 + k) % 2].replay()
             ev[k][1].record()
         ev1.record()
         torch.cuda.synchronize()
+    nsub += K
     solve_ms = sum(a.elapsed_time(b) for a, b in ev)
     total_ms = ev0.elapsed_time(ev1)
     solve_ms, total_ms = max_over_ranks([solve_ms, total_ms], device=dev)
     errors = solver.device_errors()
 
     vi_step = float(V) * ITERATIONS
-    value = world * vi_step * K / (solve_ms * 1e-3)
-    value_with_contacts = world * vi_step * K / (total_ms * 1e-3)
+    value = vi_all_ranks * K / (solve_ms * 1e-3)
+    value_with_contacts = vi_all_ranks * K / (total_ms * 1e-3)
     peak, peak_src = _peaks()
     bvi = bytes_per_vertex_iteration(V, T, E, contacts=True)
     achieved = bvi * vi_step / (solve_ms / K * 1e-3) / 1e9
+
+    # position error of the timed FP32 batch against FP64 on a sample of its instances (rank 0's shard)
+    pos = None
+    if rank == 0 and not args.no_pos_err:
+        pos = position_error(args, dev, total, shard, model, states, nsub, g_collide, g_solve, shape)
 
     # end to end through the public API with host buffers: every substep, pinned H2D of the inputs (q, qd),
     # contact generation, the step and D2H of the result (q, qd). The batch is split into --e2e-chunks groups of
@@ -385,7 +431,11 @@ def run_ours(args):
     # the solve of another (the copy engines and the SMs work at the same time).
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(args, rank, dev, dist, states, shape, vi_step, world)
+        e2e = run_e2e(args, dev, dist, states, shape, total, shard, vi_all_ranks)
+    # the plain drop-in on the same GPU: one SolverVBD per cloth, eager per-instance step calls
+    plain = None
+    if rank == 0 and args.plain_sample > 0:
+        plain = run_plain(args, total, shard[: args.plain_sample])
     traffic, traffic_src = args.traffic, "--traffic (ncu capture)" if args.traffic is not None else None
     if traffic is None and solver.layout in NCU_TRAFFIC_PER_VI:
         per_vi, traffic_src = NCU_TRAFFIC_PER_VI[solver.layout]
@@ -408,6 +458,9 @@ def run_ours(args):
             "config": {
                 "workload": f"batched cloth VBD, {args.instances} instances/GPU, side U{{16..128}}, ground contact",
                 "instances_per_gpu": args.instances,
+                "instances_total": total,
+                "instances_rank0": len(shard),
+                "shard_cost_spread": float(load.max() / load.min()) if world > 1 else 1.0,
                 "vertices_per_gpu": V,
                 "triangles_per_gpu": T,
                 "hinges_per_gpu": E,
@@ -422,7 +475,7 @@ def run_ours(args):
                 "autotuned": bool(args.tune),
                 "tune_s": round(tune_s, 1),
                 "l2": "inputs larger than L2 (~10 GB working set), no flush",
-                "parallelism": f"instance sharding x{world} (no collective)",
+                "parallelism": f"instance sharding x{world}, LPT on vertices x colors (no collective)",
                 "timed": "solve only (forward, iterations, velocity); contact generation outside the solve events",
                 "setup_s": round(setup_s, 1),
             },
@@ -445,6 +498,12 @@ def run_ours(args):
             "clocks": clocks.summary(),
             "device_errors": errors,
         }
+        if pos is not None:
+            out["pos_err"] = pos["value"]
+            out["pos_err_detail"] = pos
+        if plain is not None:
+            out["plain"] = plain
+            out["batched_over_plain"] = (value / world) / plain["value"]
         if not args.no_cpu_baseline and world == 1:
             out["cpu_baseline"] = cpu_baseline(args, seconds=args.cpu_seconds)
     if dist:
@@ -466,7 +525,7 @@ def cpu_baseline(args, seconds=15.0):
     elapsed = 0.0
     used = 0
     for i in range(args.instances):
-        b = build_instance(int(sides[i]), float(E[i]), float(bend[i]), pins[i], i)
+        b = build_instance(int(sides[i]), float(E[i]), float(bend[i]), pins[i])
         b.add_ground_plane()
         m = b.finalize("cpu")
         om = orc.Model(oracle_model_dict(m))
@@ -516,7 +575,7 @@ def run_reference(args):
     }  # fmt: skip
 
 
-def run_plain(args):
+def run_plain(args, total=None, indices=None):
     """The plain drop-in used per instance: one SolverVBD per cloth, one step call per instance per
     substep (per-color launches), on a sample of the batch; the rate is per vertex-iteration."""
     import torch
@@ -525,17 +584,20 @@ def run_plain(args):
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     torch.cuda.set_device(dev)
-    sides, E, bend, pins = instance_params(args.seed, args.instances)
-    idx = np.arange(min(args.plain_sample, args.instances))
+    total = args.instances if total is None else total
+    sides, E, bend, pins = instance_params(args.seed, total)
+    idx = np.arange(min(args.plain_sample, total)) if indices is None else np.asarray(indices)
+    t0 = time.time()
     items = []
     for i in idx:
-        b = build_instance(int(sides[i]), float(E[i]), float(bend[i]), pins[i], int(i))
+        b = build_instance(int(sides[i]), float(E[i]), float(bend[i]), pins[i])
         b.add_ground_plane()
         m = b.finalize(dev)
         m.soft_contact_ke, m.soft_contact_kd, m.soft_contact_mu = 1.0e3, 10.0, 0.5
         solver = nb.SolverVBD(m, iterations=ITERATIONS, schedule="per_color", lanes_per_vertex=args.lanes or 4)
         pipe = nb.CollisionPipeline(m, soft_contact_margin=0.01)
         items.append((m, solver, pipe, pipe.contacts(), [m.state(), m.state()]))
+    setup_s = time.time() - t0
     V = sum(m.particle_count for m, *_ in items)
 
     def substep(k):
@@ -543,20 +605,115 @@ def run_plain(args):
             pipe.collide(st[k % 2], c)
             solver.step(st[k % 2], st[(k + 1) % 2], None, c, DT)
 
-    for k in range(args.warmup):
+    W = max(args.warmup, 3)
+    for k in range(W):
         substep(k)
     torch.cuda.synchronize()
+    K = max(1, min(args.steps, args.plain_steps))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    for k in range(args.steps):
+    for k in range(W, W + K):
         substep(k)
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    return {"workload": "plain per-instance drop-in", "value": V * ITERATIONS * args.steps / (ms * 1e-3), "unit": UNIT,
-            "instances": len(items), "vertices": V, "ms_per_step": ms / args.steps,
-            "launches_per_instance_step": items[0][1].launches_per_step + 1,
-            "note": "sample of the batch's first instances; eager per-instance step calls"}  # fmt: skip
+    return {"workload": "plain per-instance drop-in", "value": V * ITERATIONS * K / (ms * 1e-3), "unit": UNIT,
+            "instances": len(items), "vertices": V, "steps": K, "ms_per_step": ms / K,
+            "launches_per_instance_step": items[0][1].launches_per_step + 1, "setup_s": round(setup_s, 1),
+            "note": "first instances of the batch, each its own Model and SolverVBD (per-color schedule); every substep "
+                    "one eager collide + step call per instance from Python, no CUDA graph; contact generation "
+                    "inside the timed region"}  # fmt: skip
+
+
+def error_sample(sides, E, pool, count):
+    """A sample of `count` instances of `pool` that holds the largest and the smallest side and both ends of
+    Young's modulus, filled with instances spread evenly through the pool."""
+    pool = np.asarray(pool)
+    picks = [pool[np.argmax(sides[pool])], pool[np.argmin(sides[pool])], pool[np.argmin(E[pool])],
+             pool[np.argmax(E[pool])]]  # fmt: skip
+    seen = {int(p) for p in picks}
+    for j in np.linspace(0, len(pool) - 1, max(count, 1)).round().astype(int):
+        if len(seen) >= count:
+            break
+        seen.add(int(pool[j]))
+    return np.array(sorted(seen), dtype=np.int64)
+
+
+def position_error(args, dev, total, shard, model, states, nsub, g_collide, g_solve, shape):
+    """Position error of the FP32 batch against FP64, on a sample of the shard's instances (error_sample),
+    as max over vertices of |x_fp32 - x_fp64|_2 / L, with L = 1 m the cloth side.
+
+    * per substep: after the timed region, each of --err-substeps more substeps of the whole batch (the
+      benchmark's graphs) runs beside the FP64 solver (precision="fp64", the same step in double precision)
+      stepping the sample from the same FP32 input state with contacts generated from the same positions;
+    * trajectory: the sample alone, from the initial state, for as many substeps as the batch ran before its
+      timed region ended, once in FP32 with the benchmark's launch shape and once in FP64."""
+    import torch
+
+    import newton_chysx_b200 as nb
+
+    t0 = time.time()
+    sides, E, _, _ = instance_params(args.seed, total)
+    sample = error_sample(sides, E, shard, args.err_sample)
+    local = np.searchsorted(shard, sample)  # world index in the rank's model
+    ws = model.world_particle_start if model.world_particle_start is not None else np.array([0, model.particle_count])
+    sel = torch.cat([torch.arange(int(ws[w]), int(ws[w + 1]), device=dev) for w in local])
+    sm = build_batch_indices(args.seed, total, sample).finalize(dev)
+    sm.soft_contact_ke, sm.soft_contact_kd, sm.soft_contact_mu = 1.0e3, 10.0, 0.5
+    assert sm.particle_count == sel.numel()
+
+    def f64_states():
+        out = [sm.state(), sm.state()]
+        for s in out:
+            s.particle_q, s.particle_qd, s.particle_f = (t.double() for t in (s.particle_q, s.particle_qd, s.particle_f))
+        return out
+
+    def f32_view(s):
+        v = type(s)()
+        v.particle_q = s.particle_q.float()
+        return v
+
+    def err(a, b):
+        return float(torch.linalg.norm(a.double() - b.double(), dim=1).max())
+
+    s64 = nb.SolverVBD(sm, iterations=ITERATIONS, schedule="persistent", precision="fp64")
+    pipe = nb.CollisionPipeline(sm, soft_contact_margin=0.01)
+    c64 = pipe.contacts()
+    a64, b64 = f64_states()
+    per_substep = []
+    for _ in range(args.err_substeps):
+        src, dst = states[nsub % 2], states[(nsub + 1) % 2]
+        a64.particle_q.copy_(src.particle_q[sel].double())
+        a64.particle_qd.copy_(src.particle_qd[sel].double())
+        pipe.collide(f32_view(a64), c64)
+        s64.step(a64, b64, None, c64, DT)
+        g_collide[nsub % 2].replay()
+        g_solve[nsub % 2].replay()
+        nsub += 1
+        torch.cuda.synchronize()
+        per_substep.append(err(dst.particle_q[sel], b64.particle_q))
+
+    s32 = nb.SolverVBD(sm, iterations=ITERATIONS, **shape)
+    c32 = pipe.contacts()
+    t32 = [sm.state(), sm.state()]
+    t64 = f64_states()
+    n_traj = max(args.warmup, 3) + args.warmup + args.steps
+    traj = []
+    for k in range(n_traj):
+        pipe.collide(t32[k % 2], c32)
+        s32.step(t32[k % 2], t32[(k + 1) % 2], None, c32, DT)
+        pipe.collide(f32_view(t64[k % 2]), c64)
+        s64.step(t64[k % 2], t64[(k + 1) % 2], None, c64, DT)
+        traj.append(err(t32[(k + 1) % 2].particle_q, t64[(k + 1) % 2].particle_q))
+    torch.cuda.synchronize()
+    worst = max(max(per_substep, default=0.0), max(traj, default=0.0))
+    return {"value": worst, "unit": "m per m of cloth side (max vertex |x32 - x64|_2 / L, L = 1 m)",
+            "bound": 1e-4, "within_bound": bool(worst <= 1e-4), "per_substep": per_substep,
+            "per_substep_after_substep": nsub - len(per_substep), "trajectory_max": max(traj, default=0.0),
+            "trajectory_substeps": n_traj, "fp32_layout": s32.layout,
+            "reference": "precision='fp64' (the same step in FP64, held to the FP64 oracle at 1e-9 m by the tests)",
+            "instances": [int(i) for i in sample], "sides": [int(sides[i]) for i in sample],
+            "E_range": [float(E[sample].min()), float(E[sample].max())], "s": round(time.time() - t0, 1)}  # fmt: skip
 
 
 SC_ITERATIONS = 20
@@ -1206,6 +1363,18 @@ def run_precision(args):
     return out
 
 
+def relaunch(gpus: int, argv) -> int:
+    """Runs this script as `gpus` ranks under torch.distributed.run on 127.0.0.1 and returns its exit code."""
+    import socket
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={gpus}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__), *argv]  # fmt: skip
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1231,7 +1400,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--plain-sample", type=int, default=256)
+    ap.add_argument("--plain-sample", type=int, default=256, help="instances of the plain drop-in leg (0: off)")
+    ap.add_argument("--plain-steps", type=int, default=5, help="timed substeps of the plain drop-in leg")
+    ap.add_argument("--err-sample", type=int, default=16, help="instances of the FP64 position-error leg")
+    ap.add_argument("--err-substeps", type=int, default=3, help="substeps of the per-substep FP64 comparison")
+    ap.add_argument("--no-pos-err", action="store_true")
     ap.add_argument("--precision-n", type=int, default=1024)
     ap.add_argument("--precision-frames", type=int, default=60)
     ap.add_argument("--traffic", type=float, default=None, help="DRAM bytes per launch from an ncu capture")
@@ -1241,6 +1414,12 @@ def main():
     ap.add_argument("--adjoint-directions", type=int, default=32)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: relaunch this command under torchrun (rank 0 prints the JSON line)
+        sys.exit(relaunch(args.gpus, sys.argv[1:]))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}; the ranks decide", file=sys.stderr)
     if args.impl == "reference":
         out = run_reference(args)
     elif args.workload == "plain":
