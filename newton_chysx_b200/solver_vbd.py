@@ -30,6 +30,13 @@ Beyond the reference keywords:
 Particle self-contact (``particle_enable_self_contact=True`` and the ``particle_self_contact_*``
 keywords) runs on the per-color schedule with the csr layout; see ``collision.py`` for the filters and
 the stand-alone detector.
+
+Arrays. The model, states and contacts may hold torch tensors (this package's ``sim``), the reference's Warp
+arrays, or any device array with ``__cuda_array_interface__``; each is checked for its element type, size and
+contiguity (``interop``). With Warp arrays the step launches on Warp's current stream of the device, as the
+reference does; otherwise on torch's current stream. The reference Model's ``particle_world_start``
+([world_count + 2], ``newton/_src/sim/model.py:172-187``) gives the worlds of a batched model, as this
+package's ``world_particle_start`` does.
 """
 
 from __future__ import annotations
@@ -39,12 +46,13 @@ import ctypes as C
 import numpy as np
 import torch
 
-from . import _lib
+from . import _lib, interop
+from .interop import F32, F64, I32
 from .sim import Contacts, Model, State
 
 
-def _ptr(t):
-    return None if t is None else C.c_void_p(t.data_ptr())
+def _ptr(obj, what="array", typestr=None, count=None, at_least=None):
+    return interop.pointer(obj, what, typestr, count, at_least)
 
 
 class SolverVBD:
@@ -143,67 +151,73 @@ class SolverVBD:
             raise ValueError(f"precision must be one of {list(_lib.PRECISION)}")
         if schedule not in _lib.SCHEDULE:
             raise ValueError(f"schedule must be one of {list(_lib.SCHEDULE)}")
-        if model.device is None or model.device.type != "cuda":
+        device = interop.torch_device(getattr(model, "device", None))
+        if device.type != "cuda":
             raise RuntimeError("SolverVBD needs a CUDA model (finalize(device='cuda'))")
         self.precision = precision
-        self.device = model.device
+        self.device = device
         self._lib = _lib.load()
+        self._warp = interop.from_warp(model.particle_mass)
 
-        groups = [g.to(torch.int32) for g in model.particle_color_groups]
-        self._color_offsets = np.concatenate([[0], np.cumsum([int(g.numel()) for g in groups])]).astype(np.int32)
-        self._color_particles = torch.cat(groups).contiguous()
+        groups = [np.ascontiguousarray(interop.to_host(g), dtype=np.int32).reshape(-1)
+                  for g in model.particle_color_groups]  # fmt: skip
+        self._color_offsets = np.concatenate([[0], np.cumsum([g.size for g in groups])]).astype(np.int32)
+        self._color_particles = torch.as_tensor(np.concatenate(groups), device=device).contiguous()
         if self._color_offsets[-1] != model.particle_count:
             raise ValueError("particle_color_groups must cover every particle exactly once")
-        self._world_start = None
-        if getattr(model, "world_particle_start", None) is not None and model.world_count > 1:
-            self._world_start = np.ascontiguousarray(model.world_particle_start, dtype=np.int32)
+        self._world_start = interop.world_starts(model)
 
+        V, T, Ecount = int(model.particle_count), int(model.tri_count), int(model.edge_count)
+        S = int(model.shape_count)
         md = _lib.VbdModelDesc()
-        md.particle_count = model.particle_count
-        md.tri_count = model.tri_count
-        md.edge_count = model.edge_count
-        md.shape_count = model.shape_count
-        md.particle_mass_dev = _ptr(model.particle_mass)
-        md.particle_inv_mass_dev = _ptr(model.particle_inv_mass)
-        md.particle_flags_dev = _ptr(model.particle_flags)
-        md.particle_radius_dev = _ptr(model.particle_radius)
-        md.tri_indices_dev = _ptr(model.tri_indices) if model.tri_count else None
-        md.tri_poses_dev = _ptr(model.tri_poses) if model.tri_count else None
-        md.tri_materials_dev = _ptr(model.tri_materials) if model.tri_count else None
-        md.tri_areas_dev = _ptr(model.tri_areas) if model.tri_count else None
-        md.edge_indices_dev = _ptr(model.edge_indices) if model.edge_count else None
-        md.edge_rest_angle_dev = _ptr(model.edge_rest_angle) if model.edge_count else None
-        md.edge_rest_length_dev = _ptr(model.edge_rest_length) if model.edge_count else None
-        md.edge_bending_properties_dev = _ptr(model.edge_bending_properties) if model.edge_count else None
+        md.particle_count = V
+        md.tri_count = T
+        md.edge_count = Ecount
+        md.shape_count = S
+        md.particle_mass_dev = _ptr(model.particle_mass, "model.particle_mass", F32, V)
+        md.particle_inv_mass_dev = _ptr(model.particle_inv_mass, "model.particle_inv_mass", F32, V)
+        md.particle_flags_dev = _ptr(model.particle_flags, "model.particle_flags", I32, V)
+        md.particle_radius_dev = _ptr(model.particle_radius, "model.particle_radius", F32, V)
+        if T:
+            md.tri_indices_dev = _ptr(model.tri_indices, "model.tri_indices", I32, 3 * T)
+            md.tri_poses_dev = _ptr(model.tri_poses, "model.tri_poses", F32, 4 * T)
+            md.tri_materials_dev = _ptr(model.tri_materials, "model.tri_materials", F32, 5 * T)
+            md.tri_areas_dev = _ptr(model.tri_areas, "model.tri_areas", F32, T)
+        if Ecount:
+            md.edge_indices_dev = _ptr(model.edge_indices, "model.edge_indices", I32, 4 * Ecount)
+            md.edge_rest_angle_dev = _ptr(model.edge_rest_angle, "model.edge_rest_angle", F32, Ecount)
+            md.edge_rest_length_dev = _ptr(model.edge_rest_length, "model.edge_rest_length", F32, Ecount)
+            md.edge_bending_properties_dev = _ptr(model.edge_bending_properties, "model.edge_bending_properties",
+                                                  F32, 2 * Ecount)  # fmt: skip
         md.color_count = len(groups)
         md.color_offsets_host = self._color_offsets.ctypes.data_as(C.POINTER(C.c_int32))
-        md.color_particles_dev = _ptr(self._color_particles)
+        md.color_particles_dev = _ptr(self._color_particles, "particle_color_groups", I32, V)
         md.world_count = 0 if self._world_start is None else len(self._world_start) - 1
         md.world_particle_start_host = (
             None if self._world_start is None else self._world_start.ctypes.data_as(C.POINTER(C.c_int32))
         )
-        md.gravity_dev = _ptr(model.gravity)
+        md.gravity_dev = _ptr(model.gravity, "model.gravity", F32, at_least=3)
         md.soft_contact_ke = float(model.soft_contact_ke)
         md.soft_contact_kd = float(model.soft_contact_kd)
         md.soft_contact_mu = float(model.soft_contact_mu)
-        if model.shape_count:
-            md.shape_material_ke_dev = _ptr(model.shape_material_ke)
-            md.shape_material_kd_dev = _ptr(model.shape_material_kd)
-            md.shape_material_mu_dev = _ptr(model.shape_material_mu)
-            md.shape_body_dev = _ptr(model.shape_body)
-        md.body_com_dev = _ptr(getattr(model, "body_com", None))
+        if S:
+            md.shape_material_ke_dev = _ptr(model.shape_material_ke, "model.shape_material_ke", F32, S)
+            md.shape_material_kd_dev = _ptr(model.shape_material_kd, "model.shape_material_kd", F32, S)
+            md.shape_material_mu_dev = _ptr(model.shape_material_mu, "model.shape_material_mu", F32, S)
+            md.shape_body_dev = _ptr(model.shape_body, "model.shape_body", I32, S)
+        md.body_com_dev = _ptr(getattr(model, "body_com", None), "model.body_com", F32)
         ns, nt = int(getattr(model, "spring_count", 0) or 0), int(getattr(model, "tet_count", 0) or 0)
         if ns:
             md.spring_count = ns
-            md.spring_indices_dev = _ptr(model.spring_indices)
-            md.spring_rest_length_dev = _ptr(model.spring_rest_length)
-            md.spring_stiffness_dev = _ptr(model.spring_stiffness)
-            md.spring_damping_dev = _ptr(model.spring_damping)
+            md.spring_indices_dev = _ptr(model.spring_indices, "model.spring_indices", I32, 2 * ns)
+            md.spring_rest_length_dev = _ptr(model.spring_rest_length, "model.spring_rest_length", F32, ns)
+            md.spring_stiffness_dev = _ptr(model.spring_stiffness, "model.spring_stiffness", F32, ns)
+            md.spring_damping_dev = _ptr(model.spring_damping, "model.spring_damping", F32, ns)
         if nt:
             md.tet_count = nt
-            md.tet_indices_dev = _ptr(model.tet_indices)
-            md.tet_poses_dev = _ptr(model.tet_poses)
-            md.tet_materials_dev = _ptr(model.tet_materials)
+            md.tet_indices_dev = _ptr(model.tet_indices, "model.tet_indices", I32, 4 * nt)
+            md.tet_poses_dev = _ptr(model.tet_poses, "model.tet_poses", F32, 9 * nt)
+            md.tet_materials_dev = _ptr(model.tet_materials, "model.tet_materials", F32, at_least=3 * nt)
         self._md = md
 
         prm = _lib.VbdSolverParams()
@@ -269,8 +283,8 @@ class SolverVBD:
         d.vertex_buffer_size = int(vertex_buffer)
         d.edge_buffer_size = int(edge_buffer)
         d.detection_interval = int(self.particle_collision_detection_interval)
-        self._rest_q = m.particle_q.detach().to(torch.float32).contiguous()
-        d.rest_q_dev = _ptr(self._rest_q)
+        self._rest_q = interop.as_torch(m.particle_q, self.device).detach().to(torch.float32).contiguous()
+        d.rest_q_dev = _ptr(self._rest_q, "model.particle_q", F32, 3 * m.particle_count)
         ip = C.POINTER(C.c_int32)
         if vt is not None:
             d.vt_filter_host, d.vt_filter_offsets_host = vt[0].ctypes.data_as(ip), vt[1].ctypes.data_as(ip)
@@ -282,62 +296,63 @@ class SolverVBD:
     def self_contact_counts(self) -> tuple[int, int, int]:
         """(vertex-triangle pairs, edge-edge pairs, overflow flags) of the last detection of the last step."""
         nv, ne, fl = C.c_int32(), C.c_int32(), C.c_int32()
-        stream = C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        stream = self._stream()
         _lib.check(self._lib.vbd_get_self_contact_counts(self._h, C.byref(nv), C.byref(ne), C.byref(fl), stream),
                    "vbd_get_self_contact_counts")  # fmt: skip
         return nv.value, ne.value, fl.value
 
     # ------------------------------------------------------------------ reference API
+    def _stream(self):
+        return C.c_void_p(interop.launch_stream(self.device, self._warp))
+
     def step(self, state_in: State, state_out: State, control, contacts: Contacts | None, dt: float) -> None:
-        q_in, q_out, qd_in, qd_out = state_in.particle_q, state_out.particle_q, state_in.particle_qd, state_out.particle_qd
-        f = state_in.particle_f
-        want = torch.float64 if self.precision == "fp64" else torch.float32
-        for name, t in (("state_in.particle_q", q_in), ("state_out.particle_q", q_out), ("state_in.particle_qd", qd_in),
-                        ("state_out.particle_qd", qd_out)):  # fmt: skip
-            if t is None or t.dtype != want or not t.is_cuda or not t.is_contiguous():
-                raise TypeError(f"{name} must be a contiguous {want} CUDA tensor")
-            if t.numel() != 3 * self.model.particle_count:
-                raise ValueError(f"{name} must hold particle_count x 3 values")
-        if f is not None and (f.dtype != want or not f.is_contiguous() or f.numel() != 3 * self.model.particle_count):
-            raise TypeError(f"state_in.particle_f must be a contiguous {want} tensor of particle_count x 3")
+        n3 = 3 * int(self.model.particle_count)
+        want = F64 if self.precision == "fp64" else F32
+        q_in = _ptr(state_in.particle_q, "state_in.particle_q", want, n3)
+        q_out = _ptr(state_out.particle_q, "state_out.particle_q", want, n3)
+        qd_in = _ptr(state_in.particle_qd, "state_in.particle_qd", want, n3)
+        qd_out = _ptr(state_out.particle_qd, "state_out.particle_qd", want, n3)
+        for name, p in (("state_in.particle_q", q_in), ("state_out.particle_q", q_out),
+                        ("state_in.particle_qd", qd_in), ("state_out.particle_qd", qd_out)):  # fmt: skip
+            if p is None:
+                raise TypeError(f"{name} must be a device array of particle_count x 3 values")
+        f = _ptr(getattr(state_in, "particle_f", None), "state_in.particle_f", want, n3)
         cdesc = None
         if contacts is not None and contacts.soft_contact_max > 0 and self.model.shape_count > 0:
-            for t in (contacts.soft_contact_particle, contacts.soft_contact_shape):
-                if t.dtype != torch.int32 or t.numel() < contacts.soft_contact_max or not t.is_contiguous():
-                    raise TypeError("contact index arrays must be contiguous int32 of soft_contact_max entries")
-            for t in (contacts.soft_contact_body_pos, contacts.soft_contact_body_vel, contacts.soft_contact_normal):
-                if t.dtype != torch.float32 or t.numel() < 3 * contacts.soft_contact_max or not t.is_contiguous():
-                    raise TypeError("contact vec3 arrays must be contiguous float32 of soft_contact_max x 3")
+            cmax = int(contacts.soft_contact_max)
             cdesc = _lib.VbdContactsDesc()
-            cdesc.soft_contact_count_dev = _ptr(contacts.soft_contact_count)
-            cdesc.soft_contact_max = int(contacts.soft_contact_max)
-            cdesc.soft_contact_particle_dev = _ptr(contacts.soft_contact_particle)
-            cdesc.soft_contact_shape_dev = _ptr(contacts.soft_contact_shape)
-            cdesc.soft_contact_body_pos_dev = _ptr(contacts.soft_contact_body_pos)
-            cdesc.soft_contact_body_vel_dev = _ptr(contacts.soft_contact_body_vel)
-            cdesc.soft_contact_normal_dev = _ptr(contacts.soft_contact_normal)
+            cdesc.soft_contact_count_dev = _ptr(contacts.soft_contact_count, "contacts.soft_contact_count", I32,
+                                                at_least=1)  # fmt: skip
+            cdesc.soft_contact_max = cmax
+            cdesc.soft_contact_particle_dev = _ptr(contacts.soft_contact_particle, "contacts.soft_contact_particle",
+                                                   I32, at_least=cmax)  # fmt: skip
+            cdesc.soft_contact_shape_dev = _ptr(contacts.soft_contact_shape, "contacts.soft_contact_shape", I32,
+                                                at_least=cmax)  # fmt: skip
+            cdesc.soft_contact_body_pos_dev = _ptr(contacts.soft_contact_body_pos, "contacts.soft_contact_body_pos",
+                                                   F32, at_least=3 * cmax)  # fmt: skip
+            cdesc.soft_contact_body_vel_dev = _ptr(contacts.soft_contact_body_vel, "contacts.soft_contact_body_vel",
+                                                   F32, at_least=3 * cmax)  # fmt: skip
+            cdesc.soft_contact_normal_dev = _ptr(contacts.soft_contact_normal, "contacts.soft_contact_normal", F32,
+                                                 at_least=3 * cmax)  # fmt: skip
         bodies = None
         if getattr(state_in, "body_q", None) is not None:
             bodies = _lib.VbdBodyState()
             if self.integrate_with_external_rigid_solver:
-                bodies.body_q_dev = _ptr(state_out.body_q)
-                bodies.body_q_prev_dev = _ptr(state_in.body_q)
-                bodies.body_qd_dev = _ptr(state_out.body_qd)
+                bodies.body_q_dev = _ptr(state_out.body_q, "state_out.body_q", F32)
+                bodies.body_q_prev_dev = _ptr(state_in.body_q, "state_in.body_q", F32)
+                bodies.body_qd_dev = _ptr(state_out.body_qd, "state_out.body_qd", F32)
             else:
-                bodies.body_q_dev = _ptr(state_in.body_q)
-                bodies.body_qd_dev = _ptr(state_in.body_qd)
-        stream = C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+                bodies.body_q_dev = _ptr(state_in.body_q, "state_in.body_q", F32)
+                bodies.body_qd_dev = _ptr(state_in.body_qd, "state_in.body_qd", F32)
         fn = self._lib.vbd_step_f64 if self.precision == "fp64" else self._lib.vbd_step
-        rc = fn(
-            self._h, _ptr(q_in), _ptr(q_out), _ptr(qd_in), _ptr(qd_out), _ptr(f),
-            None if cdesc is None else C.byref(cdesc), None if bodies is None else C.byref(bodies), float(dt), stream,
-        )  # fmt: skip
+        rc = fn(self._h, q_in, q_out, qd_in, qd_out, f, None if cdesc is None else C.byref(cdesc),
+                None if bodies is None else C.byref(bodies), float(dt), self._stream())  # fmt: skip
         if rc == _lib.VBD_ERR_UNSUPPORTED:
             raise RuntimeError("contact buffers must grow while a CUDA graph is being captured; step once before capturing")
         _lib.check(rc, "vbd_step")
 
     def notify_model_changed(self, flags: int = 0) -> None:
-        stream = C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        stream = self._stream()
         _lib.check(self._lib.vbd_refresh_model(self._h, stream), "vbd_refresh_model")
 
     def rebuild_bvh(self, state: State) -> None:
@@ -351,14 +366,14 @@ class SolverVBD:
     # ------------------------------------------------------------------ diagnostics
     def device_errors(self) -> int:
         bits = C.c_int32()
-        stream = C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        stream = self._stream()
         _lib.check(self._lib.vbd_get_error(self._h, C.byref(bits), stream), "vbd_get_error")
         return bits.value
 
     def residuals(self) -> np.ndarray:
         """FP64 per-iteration sums of |f|^2 of the last step (precision='mixed')."""
         out = np.zeros(max(self.iterations, 1), dtype=np.float64)
-        stream = C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        stream = self._stream()
         _lib.check(self._lib.vbd_get_residuals(self._h, out.ctypes.data_as(C.POINTER(C.c_double)), self.iterations,
                                                stream), "vbd_get_residuals")  # fmt: skip
         return out
