@@ -9,21 +9,26 @@
 // This entry point runs the per-color step on the model arrays exactly as the caller holds them
 // (the reference layout, plus the reference-layout vertex adjacency that vbd_build_adjacency writes
 // into caller-owned buffers). Its per-particle scratch (positions, previous positions, inertial
-// targets, contact slots) lives in one file-scope __device__ array, g_noalloc_scratch, of fixed size:
-// VBD_NOALLOC_MAX_PARTICLES (32768) particles, 2,228,224 bytes. Every GPU that loads the library holds
-// that array until the process exits. The host code gets the array's device address once per device
-// with cudaGetSymbolAddress. It does that on the first call made with that device current, so make
-// the first call before any stream capture.
+// targets, contact slots) and an error word live in one file-scope __device__ array, g_noalloc_scratch,
+// of fixed size: VBD_NOALLOC_MAX_PARTICLES (32768) particles, 2,097,408 bytes. Every GPU that loads the
+// library holds that array until the process exits. The host code gets the array's device address once
+// per device with cudaGetSymbolAddress. It does that on the first call made with that device current, so
+// make the first call before any stream capture.
 //
 // All calls on a device share the one array and it keeps the last call's contents. The kernels
-// rewrite everything they read before reading it, and the contact slot counters are cleared at the
-// start of every call. Two calls whose kernels overlap on the GPU (different streams, or different
+// rewrite everything they read before reading it; the contact slots and the error word are cleared at
+// the start of every call. Two calls whose kernels overlap on the GPU (different streams, or different
 // host threads on the same device) race on the array; serialise them.
 //
-// Limits: FP32 only; at most VBD_NOALLOC_MAX_PARTICLES particles; at most
-// VBD_NOALLOC_MAX_CONTACT_SLOTS contacts per particle; particle-shape contacts on static shapes with a
-// fixed penalty (the AVBD ramp rigid_avbd_linear_beta = 0, the reference default). Larger models
-// return VBD_ERR_TOO_LARGE before any GPU work.
+// Contacts: each particle keeps its VBD_NOALLOC_MAX_CONTACT_SLOTS contacts of lowest index in the
+// contact list (a sorted insertion with atomicMin, so the kept set and its order do not depend on
+// thread timing); a particle with more sets VBD_DEVERR_CONTACT_OVERFLOW in the error word, which
+// vbd_step_noalloc_error reads back, together with the solve's VBD_DEVERR_* bits.
+//
+// Limits: FP32 only; at most VBD_NOALLOC_MAX_PARTICLES particles; particle-shape contacts on static
+// shapes with a fixed penalty (the AVBD ramp rigid_avbd_linear_beta = 0, the reference default). Larger
+// models return VBD_ERR_TOO_LARGE before any GPU work.
+#include <climits>
 #include <mutex>
 
 #include "vbd_b200.h"
@@ -36,16 +41,19 @@ namespace {
 constexpr int kMaxP = VBD_NOALLOC_MAX_PARTICLES;
 constexpr int kSlots = VBD_NOALLOC_MAX_CONTACT_SLOTS;
 
+constexpr int kEmpty = INT_MAX;  // an unused contact slot
+
 struct NoAllocScratch {
   float4 pos[kMaxP];
   float4 qprev[kMaxP];
-  float4 inertia[kMaxP];  // w = mass, or 0 for a fixed particle
-  int slot_cnt[kMaxP];
-  int slots[kMaxP * kSlots];
+  float4 inertia[kMaxP];      // w = mass, or 0 for a fixed particle
+  int slots[kMaxP * kSlots];  // per particle its kept contact indices in increasing order, kEmpty after
+  int err;                    // VBD_DEVERR_* bits of the last call
+  int pad_[63];
 };
 
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
-static_assert(sizeof(NoAllocScratch) == 2228224, "scratch size stated in the header");
+static_assert(sizeof(NoAllocScratch) == 2097408, "scratch size stated in the header");
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
@@ -103,7 +111,9 @@ __global__ void k_na_forward(NaCtx c) {
   const float m = c.mass[i], im = c.inv_mass[i];
   const float ms = ((fl & 1) && m != 0.f) ? m : 0.f;
   c.s->qprev[i] = make_float4(q.x, q.y, q.z, 0.f);
-  c.s->slot_cnt[i] = 0;
+  static_assert(kSlots == 4, "one int4 store clears a particle's slots");
+  reinterpret_cast<int4*>(c.s->slots)[i] = make_int4(kEmpty, kEmpty, kEmpty, kEmpty);
+  if (i == 0) c.s->err = 0;
   vec3<float> x = q;
   if ((fl & 1) && im != 0.f) {
     vec3<float> fe = {0.f, 0.f, 0.f};
@@ -122,9 +132,20 @@ __global__ void k_na_contacts(NaCtx c) {
   if (count > c.c_max) count = c.c_max;
   if (t >= count) return;
   const int p = c.c_particle[t], s = c.c_shape[t];
-  if (p < 0 || p >= c.V || s < 0 || s >= c.S) return;
-  const int k = atomicAdd(c.s->slot_cnt + p, 1);
-  if (k < kSlots) c.s->slots[p * kSlots + k] = t;
+  if (p < 0 || p >= c.V || s < 0 || s >= c.S) {
+    atomicOr(&c.s->err, VBD_DEVERR_BAD_CONTACT);
+    return;
+  }
+  // sorted insertion: slot j ends with the smallest index of those that reach it, and the larger one of each
+  // exchange moves on to slot j + 1, so the slots end with the kSlots smallest indices in increasing order
+  int* slot = c.s->slots + p * kSlots;
+  int val = t;
+  for (int j = 0; j < kSlots; ++j) {
+    const int old = atomicMin(slot + j, val);
+    if (old == kEmpty) return;
+    val = max(old, val);
+  }
+  atomicOr(&c.s->err, VBD_DEVERR_CONTACT_OVERFLOW);  // `val` is dropped: the largest index seen here
 }
 
 // one thread per vertex of the color; the element math is shared with the main kernels
@@ -168,17 +189,9 @@ __global__ void k_na_color(NaCtx c, const int* __restrict__ verts, int n) {
   H.xx += md;
   H.yy += md;
   H.zz += md;
-  int nc = c.s->slot_cnt[v];
-  if (nc > kSlots) nc = kSlots;
-  int ids[kSlots];
-  for (int j = 0; j < nc; ++j) ids[j] = c.s->slots[v * kSlots + j];
-  for (int a = 1; a < nc; ++a)  // contact index order
-    for (int b = a; b > 0 && ids[b - 1] > ids[b]; --b) {
-      const int tmp = ids[b];
-      ids[b] = ids[b - 1];
-      ids[b - 1] = tmp;
-    }
-  for (int j = 0; j < nc; ++j) {
+  const int4 kept = reinterpret_cast<const int4*>(c.s->slots)[v];  // contact index order
+  const int ids[kSlots] = {kept.x, kept.y, kept.z, kept.w};
+  for (int j = 0; j < kSlots && ids[j] != kEmpty; ++j) {
     const int t = ids[j], s = c.c_shape[t];
     const vec3<float> bx = {c.c_body_pos[3 * t], c.c_body_pos[3 * t + 1], c.c_body_pos[3 * t + 2]};
     const vec3<float> nn = {c.c_normal[3 * t], c.c_normal[3 * t + 1], c.c_normal[3 * t + 2]};
@@ -193,9 +206,19 @@ __global__ void k_na_color(NaCtx c, const int* __restrict__ verts, int n) {
     }
   }
   const float d = sdet(H);
-  if (!(fabsf(d) > 1e-8f) || !isfinite(d)) return;  // the reference skips the update
+  if (!isfinite(d)) {
+    atomicOr(&c.s->err, VBD_DEVERR_NONFINITE);
+    return;
+  }
+  if (!(fabsf(d) > 1e-8f)) {  // the reference skips the update
+    atomicOr(&c.s->err, VBD_DEVERR_SINGULAR_SKIPPED);
+    return;
+  }
   const vec3<float> xn = x + sadj_mul(H, f) * (1.f / d);
-  if (isfinite(xn.x) && isfinite(xn.y) && isfinite(xn.z)) c.s->pos[v] = make_float4(xn.x, xn.y, xn.z, 0.f);
+  if (isfinite(xn.x) && isfinite(xn.y) && isfinite(xn.z))
+    c.s->pos[v] = make_float4(xn.x, xn.y, xn.z, 0.f);
+  else
+    atomicOr(&c.s->err, VBD_DEVERR_NONFINITE);
 }
 
 __global__ void k_na_finalize(NaCtx c) {
@@ -299,7 +322,7 @@ extern "C" int vbd_step_noalloc(const VbdModelDesc* m, const VbdRefAdjacency* ad
   }
   cudaStream_t st = (cudaStream_t)stream;
   const int V = c.V;
-  k_na_forward<<<(V + 255) / 256, 256, 0, st>>>(c);  // also clears the contact slot counters
+  k_na_forward<<<(V + 255) / 256, 256, 0, st>>>(c);  // also clears the contact slots and the error word
   if (has_c) k_na_contacts<<<(c.c_max + 255) / 256, 256, 0, st>>>(c);
   for (int it = 0; it < iterations; ++it)
     for (int col = 0; col < m->color_count; ++col) {
@@ -308,4 +331,18 @@ extern "C" int vbd_step_noalloc(const VbdModelDesc* m, const VbdRefAdjacency* ad
     }
   k_na_finalize<<<(V + 255) / 256, 256, 0, st>>>(c);
   return cudaGetLastError() == cudaSuccess ? VBD_OK : VBD_ERR_CUDA;
+}
+
+extern "C" int vbd_step_noalloc_error(int32_t* bits, void* stream) {
+  if (!bits) return VBD_ERR_INVALID_ARGUMENT;
+  NoAllocScratch* scratch = nullptr;
+  int rc = scratch_for_current_device(&scratch);
+  if (rc != VBD_OK) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  int value = 0;
+  if (cudaMemcpyAsync(&value, &scratch->err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return VBD_ERR_CUDA;
+  *bits = value;
+  return VBD_OK;
 }
