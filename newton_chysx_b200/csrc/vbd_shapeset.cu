@@ -24,6 +24,7 @@ struct VbdShapeSetImpl {
   void* buffer;
   vbd::ShapeParamTable small;  // the records again when m <= kParamTableShapes: launched as a kernel parameter
   bool worlds;                 // some shape belongs to a world
+  bool param_table;            // launch small sets with `small` (else the global-memory kernel for every size)
 };
 
 namespace {
@@ -114,8 +115,15 @@ int vbd_shape_set_create(const VbdShapeTable* tb, VbdShapeSetHandle* out) {
   set->elev = tb->elevations_dev;
   set->buffer = buf;
   set->worlds = W > 0;
+  set->param_table = true;
   if (m <= vbd::kParamTableShapes) std::copy(recs.begin(), recs.end(), set->small.rec);
   *out = set;
+  return VBD_OK;
+}
+
+int vbd_shape_set_use_parameter_table(VbdShapeSetHandle set, int32_t enable) {
+  if (!set || (enable != 0 && enable != 1)) return VBD_ERR_INVALID_ARGUMENT;
+  set->param_table = enable != 0;
   return VBD_OK;
 }
 
@@ -136,7 +144,7 @@ int vbd_soft_contacts_set(VbdShapeSetHandle set, int32_t n, const float* q, cons
   cudaStream_t st = (cudaStream_t)stream;
   if (cudaMemsetAsync(count, 0, sizeof(int), st) != cudaSuccess) return VBD_ERR_CUDA;
   if (n == 0 || set->m == 0) return VBD_OK;
-  if (set->m <= vbd::kParamTableShapes) {  // small sets: records in the constant bank measured faster
+  if (set->param_table && set->m <= vbd::kParamTableShapes) {  // small sets: records in the constant bank measured faster
     auto kern = set->worlds && particle_world ? vbd::k_soft_contacts_shapes<true> : vbd::k_soft_contacts_shapes<false>;
     kern<<<(n + 255) / 256, 256, 0, st>>>(n, q, radius, flags, set->m, set->small, set->elev, particle_world, margin,
                                            cmax, count, particle, shape, body_pos, body_vel, normal);

@@ -963,9 +963,13 @@ class Model:
         return m
 
     def refresh_shapes(self):
-        """Re-upload the shapes to the GPU after their host arrays (shape_transform, shape_scale, shape_type,
-        shape_flags, shape_world, heightfields) were changed in place."""
-        self._shape_set = _ShapeSet(self) if self.device.type == "cuda" and self.shape_count > 0 else None
+        """Rebuild the GPU shape set from the host shape arrays (shape_transform, shape_scale, shape_type,
+        shape_flags, shape_world, heightfields) now. Contact generation also does so by itself at its next call
+        when those arrays changed; a CUDA graph keeps the shapes of its capture."""
+        if self.device.type == "cuda" and self.shape_count > 0:
+            if self._shape_set is not None:
+                self._shape_set.fingerprint = None
+            _current_shape_set(self)
 
     def set_gravity(self, gravity, world=None):
         g = torch.as_tensor(gravity, dtype=torch.float32, device=self.device).reshape(-1, 3)
@@ -1072,41 +1076,85 @@ def _shape_table(model: Model):
     return tb, keep
 
 
+_SHAPE_FIELDS = ("shape_type", "shape_transform", "shape_scale", "shape_flags", "shape_world", "shape_heightfield_index",
+                 "heightfield_data", "shape_mesh_index")  # fmt: skip
+
+
+def _shape_fingerprint(model: Model):
+    """A cheap digest of the host shape arrays a shape set is built from, and of the elevation array's address
+    (its contents are read on the device at every launch, so in-place edits need no rebuild)."""
+    parts = []
+    for k in _SHAPE_FIELDS:
+        a = getattr(model, k, None)
+        parts.append(None if a is None else (np.asarray(a).dtype.str, np.asarray(a).shape,
+                                             np.ascontiguousarray(a).tobytes()))  # fmt: skip
+    elev = getattr(model, "heightfield_elevations", None)
+    return hash(tuple(parts)), None if elev is None else elev.data_ptr()
+
+
 class _ShapeSet:
-    """The model's shapes on the GPU (``vbd_shape_set_create``), built once at finalize, freed with the model."""
+    """The model's shapes on the GPU (``vbd_shape_set_create``), built at finalize and rebuilt when the host shape
+    arrays change; freed with the model."""
 
     def __init__(self, model: Model):
         self._lib = _lib.load()
+        self.fingerprint = _shape_fingerprint(model)
         tb, keep = _shape_table(model)
         h = C.c_void_p()
-        _lib.check(self._lib.vbd_shape_set_create(C.byref(tb), C.byref(h)), "vbd_shape_set_create")
+        with torch.cuda.device(model.device):
+            _lib.check(self._lib.vbd_shape_set_create(C.byref(tb), C.byref(h)), "vbd_shape_set_create")
         self.handle = h.value
+        self.device = model.device
         del keep
+
+    def use_parameter_table(self, enable: bool):
+        """Sets of up to 16 shapes launch with their records as a kernel parameter (default); False sends every
+        size through the global-memory kernel. Both give the same contacts."""
+        _lib.check(self._lib.vbd_shape_set_use_parameter_table(self.handle, int(bool(enable))),
+                   "vbd_shape_set_use_parameter_table")  # fmt: skip
 
     def __del__(self):
         if getattr(self, "handle", None):
-            self._lib.vbd_shape_set_destroy(self.handle)
+            try:
+                with torch.cuda.device(self.device):
+                    self._lib.vbd_shape_set_destroy(self.handle)
+            except Exception:
+                pass
             self.handle = None
+
+
+def _current_shape_set(model: Model) -> _ShapeSet:
+    """The model's shape set, rebuilt first when the host shape arrays (shape_transform, shape_scale, shape_type,
+    shape_flags, shape_world, heightfields) changed since it was built, as the reference reads the model's arrays
+    at every create_soft_contacts launch. A replaced set is kept until the model is freed: a CUDA graph captured
+    before the change may still read it (the graph keeps the shapes of its capture; capture again after an edit)."""
+    ss = getattr(model, "_shape_set", None)
+    if ss is None or ss.fingerprint != _shape_fingerprint(model):
+        if ss is not None:
+            model._retired_shape_sets = getattr(model, "_retired_shape_sets", []) + [ss]
+        model._shape_set = ss = _ShapeSet(model)
+    return ss
 
 
 def soft_contacts(model: Model, state: State, contacts: Contacts, margin: float):
     """Particle contacts against the model's static shapes on the GPU (``vbd_soft_contacts_set``): any number of
-    shapes; a particle of world w meets the global shapes and world w's."""
+    shapes; a particle of world w meets the global shapes and world w's. Edits of the host shape arrays after
+    finalize take effect at the next call."""
     lib = _lib.load()
     if model.shape_count == 0:
         contacts.soft_contact_count.zero_()
         return
-    if getattr(model, "_shape_set", None) is None:
-        model._shape_set = _ShapeSet(model)
+    ss = _current_shape_set(model)
     pw = getattr(model, "particle_world", None)
     stream = torch.cuda.current_stream(model.device).cuda_stream
-    rc = lib.vbd_soft_contacts_set(
-        model._shape_set.handle, model.particle_count, state.particle_q.data_ptr(), model.particle_radius.data_ptr(),
-        model.particle_flags.data_ptr(), None if pw is None else pw.data_ptr(), float(margin),
-        contacts.soft_contact_max, contacts.soft_contact_count.data_ptr(), contacts.soft_contact_particle.data_ptr(),
-        contacts.soft_contact_shape.data_ptr(), contacts.soft_contact_body_pos.data_ptr(),
-        contacts.soft_contact_body_vel.data_ptr(), contacts.soft_contact_normal.data_ptr(), C.c_void_p(stream),
-    )  # fmt: skip
+    with torch.cuda.device(model.device):
+        rc = lib.vbd_soft_contacts_set(
+            ss.handle, model.particle_count, state.particle_q.data_ptr(), model.particle_radius.data_ptr(),
+            model.particle_flags.data_ptr(), None if pw is None else pw.data_ptr(), float(margin),
+            contacts.soft_contact_max, contacts.soft_contact_count.data_ptr(), contacts.soft_contact_particle.data_ptr(),
+            contacts.soft_contact_shape.data_ptr(), contacts.soft_contact_body_pos.data_ptr(),
+            contacts.soft_contact_body_vel.data_ptr(), contacts.soft_contact_normal.data_ptr(), C.c_void_p(stream),
+        )  # fmt: skip
     _lib.check(rc, "vbd_soft_contacts_set")
 
 

@@ -478,10 +478,12 @@ def test_many_worlds_and_shapes_match_oracle():
     _compare(gpu, list(zip(p[:cnt].tolist(), s[:cnt].tolist())), bp[:cnt], nn[:cnt], near)
 
 
-@pytest.mark.parametrize("path", ["table", "set"])
+@pytest.mark.parametrize("path", ["table", "set", "set_global"])
 def test_reference_create_soft_contacts_kernel_golden(path):
-    """Both device paths (the parameter table and the shape set) against the reference's ``create_soft_contacts``
-    kernel run as-is: worlds, the particle-collision flag, a heightfield and seven analytic shapes."""
+    """Every device path against the reference's ``create_soft_contacts`` kernel run as-is: worlds, the
+    particle-collision flag, a heightfield and seven analytic shapes. "table" is ``vbd_soft_contacts_table``;
+    "set" a shape set (9 shapes: its records launch as a kernel parameter); "set_global" the same set forced
+    through the global-memory kernel with its per-world shape lists."""
     g = load_golden("create_soft_contacts.npz")
     lib = _lib.load()
     dev = torch.device("cuda")
@@ -515,6 +517,8 @@ def test_reference_create_soft_contacts_kernel_golden(path):
     else:
         h = C.c_void_p()
         _lib.check(lib.vbd_shape_set_create(C.byref(tb), C.byref(h)), "vbd_shape_set_create")
+        if path == "set_global":
+            _lib.check(lib.vbd_shape_set_use_parameter_table(h, 0), "vbd_shape_set_use_parameter_table")
         rc = lib.vbd_soft_contacts_set(h, n, qd.data_ptr(), rd.data_ptr(), fd.data_ptr(), pw.data_ptr(),
                                        float(g["margin"]), *outs)  # fmt: skip
         _lib.check(rc, "vbd_soft_contacts_set")
@@ -535,10 +539,13 @@ def test_reference_create_soft_contacts_kernel_golden(path):
     _compare(gpu, pairs, g["body_pos"], g["normal"], near)
 
 
-def test_shape_set_contact_overflow():
-    """More contacts than soft_contact_max through the shape set: the count reports them all, as the reference's
-    counter does, only the first soft_contact_max slots are written, and the slots past them stay untouched."""
+@pytest.mark.parametrize("param_table", [True, False])
+def test_shape_set_contact_overflow(param_table):
+    """More contacts than soft_contact_max through the shape set, in both of its kernels: the count reports them
+    all, as the reference's counter does, only the first soft_contact_max slots are written, and the slots past
+    them stay untouched."""
     m = _world_scene_many()
+    sim._current_shape_set(m).use_parameter_table(param_table)
     full = sim.CollisionPipeline(m, soft_contact_max=m.particle_count * m.shape_count, soft_contact_margin=0.01)
     cf = full.contacts()
     full.collide(m.state(), cf)
@@ -560,3 +567,44 @@ def _world_scene_many():
     from tests.test_oracle_shapes import _world_scene
 
     return _world_scene("cuda")
+
+
+def test_shapes_edited_after_finalize_take_effect():
+    """The reference reads the model's shape arrays at every create_soft_contacts launch. Moving a sphere,
+    scaling it and switching its particle-collision flag off after finalize change the next contacts without a
+    refresh call; a graph captured before the edit keeps the shapes of its capture."""
+    b = sim.ModelBuilder(up_axis="Z")
+    pts = np.stack(np.meshgrid(np.linspace(-0.5, 0.5, 21), np.linspace(-0.5, 0.5, 21), [0.0], indexing="ij"), -1)
+    b.add_particles(pts.reshape(-1, 3), (0.0, 0.0, 0.0), 1.0, radius=5e-3)
+    # radius 0.02 centred 0.02 below the sheet: touches the centre particle only (the next ones, 0.05 m away, are
+    # 0.034 m from its surface, beyond margin + radius = 0.015 m)
+    b.add_shape_sphere(xform=((0.0, 0.0, -0.02), sim.quat_identity()), radius=0.02)
+    m = b.finalize("cuda")
+    pipe = sim.CollisionPipeline(m, soft_contact_margin=0.01)
+    c, s = pipe.contacts(), m.state()
+
+    def touched():
+        pipe.collide(s, c)
+        torch.cuda.synchronize()
+        k = int(c.soft_contact_count.item())
+        return set(c.soft_contact_particle[:k].cpu().tolist())
+
+    centre = 10 * 21 + 10
+    assert touched() == {centre}
+    g = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side), torch.cuda.graph(g, stream=side):
+        pipe.collide(s, c)
+    torch.cuda.current_stream().wait_stream(side)
+    m.shape_transform[0, 0] = 0.25  # move the sphere under particle (15, 10)
+    assert touched() == {15 * 21 + 10}
+    m.shape_scale[0, 0] = 0.3  # radius 0.3: a disc of particles
+    many = touched()
+    assert len(many) > 20 and 15 * 21 + 10 in many
+    g.replay()  # the captured graph still sees the sphere as it was captured
+    torch.cuda.synchronize()
+    k = int(c.soft_contact_count.item())
+    assert set(c.soft_contact_particle[:k].cpu().tolist()) == {centre}
+    m.shape_flags[0] &= ~4  # COLLIDE_PARTICLES off
+    assert touched() == set()
