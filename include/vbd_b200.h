@@ -216,6 +216,11 @@ int vbd_get_config(VbdHandle h, int32_t* schedule, int32_t* lanes_per_vertex, in
 
 int vbd_destroy(VbdHandle h);
 
+/* Diagnostics: vbd_eval_atan2 writes out[i] = the step's FP32 device atan2 of (y[i], x[i]) (the Abramowitz &
+   Stegun 4.4.49 polynomial with the quadrant fix-up that the bending term uses in place of atan2f), for tests
+   against the library atan2f. Device arrays of n floats. */
+int vbd_eval_atan2(int32_t n, const float* y_dev, const float* x_dev, float* out_dev, void* stream);
+
 /* ---------------------------------------------------------------- step without allocation */
 
 /* Vertex -> element adjacency in the reference layout, as vbd_build_adjacency writes it (offsets
@@ -237,18 +242,26 @@ typedef struct VbdRefAdjacency {
    Takes the model arrays in the reference layout (only the particle, triangle, hinge, color, gravity
    and shape-material fields of VbdModelDesc are read) and the adjacency above, and runs the same
    per-color FP32 step as vbd_step with the same side effects on the state arrays. It calls no
-   cudaMalloc/cudaFree: its per-particle scratch is one fixed __device__ array of 2,228,224 bytes
-   (VBD_NOALLOC_MAX_PARTICLES particles) that every GPU loading the library keeps until exit. The first
-   call with a device current looks up that array's address (cudaGetSymbolAddress); make it before any
-   stream capture. All calls share the array: calls that overlap on the GPU race and must be serialised.
-   Limits: at most VBD_NOALLOC_MAX_PARTICLES particles (else VBD_ERR_TOO_LARGE, nothing launched), at
-   most VBD_NOALLOC_MAX_CONTACT_SLOTS contacts per particle, static shapes with a fixed penalty
-   (avbd beta = 0, the reference default), no springs or tetrahedra (else VBD_ERR_UNSUPPORTED). Inputs are
-   trusted like the reference kernels trust theirs. */
+   cudaMalloc/cudaFree: its per-particle scratch and an error word are one fixed __device__ array of
+   2,097,408 bytes (VBD_NOALLOC_MAX_PARTICLES particles) that every GPU loading the library keeps until
+   exit. The first call with a device current looks up that array's address (cudaGetSymbolAddress); make
+   it before any stream capture. All calls share the array: calls that overlap on the GPU race and must be
+   serialised.
+   Contacts: each particle keeps the VBD_NOALLOC_MAX_CONTACT_SLOTS contacts of lowest index in the contact
+   list, whatever the thread timing; a particle with more drops the rest and sets
+   VBD_DEVERR_CONTACT_OVERFLOW (read it with vbd_step_noalloc_error).
+   Limits: at most VBD_NOALLOC_MAX_PARTICLES particles (else VBD_ERR_TOO_LARGE, nothing launched),
+   static shapes with a fixed penalty (avbd beta = 0, the reference default), no springs or tetrahedra
+   (else VBD_ERR_UNSUPPORTED). Inputs are trusted like the reference kernels trust theirs. */
 int vbd_step_noalloc(const VbdModelDesc* model, const VbdRefAdjacency* adjacency, int32_t iterations,
                      float friction_epsilon, float* q_in_dev, float* q_out_dev, const float* qd_in_dev,
                      float* qd_out_dev, const float* particle_f_dev, const VbdContactsDesc* contacts, float dt,
                      void* stream);
+
+/* The VBD_DEVERR_* bits of the last vbd_step_noalloc call on the current device (cleared when a call
+   starts): contact overflow, contacts out of range, non-finite or singular (skipped) block solves. Waits for
+   `stream`, then copies one int from the fixed array; allocates nothing. */
+int vbd_step_noalloc_error(int32_t* bits, void* stream);
 
 /* ---------------------------------------------------------------- particle self-contact */
 
@@ -449,6 +462,10 @@ int vbd_soft_contacts_table(int32_t particle_count, const float* q_dev, const fl
 typedef struct VbdShapeSetImpl* VbdShapeSetHandle;
 int vbd_shape_set_create(const VbdShapeTable* shapes, VbdShapeSetHandle* out);
 int vbd_shape_set_destroy(VbdShapeSetHandle set);
+/* Sets of up to 16 shapes launch with their records as a kernel parameter, read through the constant bank (the
+   default, enable = 1); enable = 0 sends every size through the global-memory kernel and its world lists. Both
+   give the same contacts. */
+int vbd_shape_set_use_parameter_table(VbdShapeSetHandle set, int32_t enable);
 
 /* Soft contacts of every active particle against a shape set, written as vbd_soft_contacts_shapes writes them. A
    particle of world w (particle_world_dev; NULL = all global) tests the global shapes and world w's shapes; a

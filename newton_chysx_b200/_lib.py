@@ -20,10 +20,12 @@ VBD_ERR_UNSUPPORTED = -4
 VBD_ERR_EMPTY_COLORING = -5
 VBD_ERR_TOO_LARGE = -6
 VBD_NOALLOC_MAX_PARTICLES = 32768
+VBD_NOALLOC_MAX_CONTACT_SLOTS = 4
 
 VBD_DEVERR_NONFINITE = 1
 VBD_DEVERR_CONTACT_OVERFLOW = 2
 VBD_DEVERR_SINGULAR_SKIPPED = 4
+VBD_DEVERR_BAD_CONTACT = 8
 
 PRECISION = {"fp32": 0, "mixed": 1, "fp64": 2}
 SCHEDULE = {"auto": 0, "per_color": 1, "persistent": 2}
@@ -139,6 +141,8 @@ SIGNATURES = {
          C.POINTER(VbdContactsDesc), C.c_float, _vp],
         C.c_int,
     ),
+    "vbd_step_noalloc_error": ([_ip, _vp], C.c_int),
+    "vbd_eval_atan2": ([C.c_int32, _vp, _vp, _vp, _vp], C.c_int),
     "vbd_set_self_contact": ([_vp, C.POINTER(VbdSelfContactDesc)], C.c_int),
     "vbd_get_self_contact_counts": ([_vp, _ip, _ip, _ip, _vp], C.c_int),
     "vbd_build_contact_filters": ([C.c_int32, C.c_int32, _ip, C.c_int32, _ip, C.c_int32, _ip, _ip, _ip, _ip], C.c_int),
@@ -162,6 +166,7 @@ SIGNATURES = {
     "vbd_mesh_create": ([_fp, C.c_int32, _ip, C.c_int32, C.POINTER(_vp)], C.c_int),
     "vbd_shape_set_create": ([C.POINTER(VbdShapeTable), C.POINTER(_vp)], C.c_int),
     "vbd_shape_set_destroy": ([_vp], C.c_int),
+    "vbd_shape_set_use_parameter_table": ([_vp, C.c_int32], C.c_int),
     "vbd_soft_contacts_set": (
         [_vp, C.c_int32, _vp, _vp, _vp, _vp, C.c_float, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
         C.c_int,
