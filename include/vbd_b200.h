@@ -46,11 +46,12 @@ extern "C" {
 #define VBD_LAYOUT_CSR 1  /* vertex -> element adjacency, element records gathered by id (any lanes/vertex) */
 #define VBD_LAYOUT_ELL 2  /* per-incidence stencil records in sweep order, slot-major (one lane/vertex) */
 #define VBD_LAYOUT_ELL16 3 /* the same with 16-bit instance-local vertex ids: 32-byte face and 16-byte hinge
-                              records (persistent schedule, instances below 65536 particles, no hinge damping) */
+                              records (persistent schedule, instances below 65536 particles); hinge damping,
+                              when the model has some, in a side array read by a kernel variant of its own */
 #define VBD_LAYOUT_RING 4  /* one-ring fan records (16-bit instance-local ids): each vertex walks its fan once,
                               sharing every incident face normal between the membrane, the two spoke hinges and
                               the rim hinge of that face (persistent schedule, instances below 65536 particles,
-                              manifold fans of at most 8 triangles, no hinge damping) */
+                              manifold fans of at most 8 triangles); a damped hinge is evaluated on its own */
 
 typedef struct VbdModelDesc {
   int32_t particle_count; /* V */
@@ -331,6 +332,14 @@ int vbd_collider_detect(VbdColliderHandle h, int32_t what, const float* pos_dev,
                         int32_t* vertex_colliding_triangles_count_dev, float* vertex_colliding_triangles_min_dist_dev,
                         int32_t* edge_colliding_edges_dev, int32_t* edge_colliding_edges_count_dev,
                         float* edge_colliding_edges_min_dist_dev, int32_t* resize_flags_dev, void* stream);
+/* record_triangle_contacting_vertices (tri_mesh_collision.py:170-200, geometry/kernels.py:1373-1384): every
+   later vertex-triangle detection also fills the caller's triangle -> colliding vertices buffers, triangle t's
+   at vertices_dev[t * buffer_size ...]: the vertex ids of its pairs (the buffer_size smallest, increasing; -1
+   past them), count_dev[t] = all pairs found (may exceed the buffer; resize flag 1 is then set) and
+   min_dist_dev[t] = the smallest pair distance (max_query_radius when none). buffer_size 0 turns it off. The
+   buffers must outlive the detections. */
+int vbd_collider_set_triangle_buffers(VbdColliderHandle h, int32_t buffer_size, int32_t* vertices_dev,
+                                      int32_t* count_dev, float* min_dist_dev);
 int vbd_collider_destroy(VbdColliderHandle h);
 
 /* ---------------------------------------------------------------- host-side model preparation */

@@ -21,6 +21,7 @@
 #include "vbd_ell.cuh"
 #include "vbd_ring.cuh"
 #include "vbd_soft.h"
+#include "vbd_ell16_damped.h"
 #include "vbd_ell16_pair.h"
 #include "vbd_shapes.cuh"
 #include "vbd_warp.h"
@@ -215,6 +216,7 @@ struct VbdSolver {
   uint4 *ring_A = nullptr, *ring_B = nullptr;
   float4* ring_H = nullptr;
   unsigned* ring_hdr = nullptr;
+  float2* ring_kd = nullptr;
   std::vector<int> ell_nf, ell_ne;
   std::vector<long long> ell_fbase, ell_ebase;
   long long ell_faces = 0, ell_hinges = 0;
@@ -239,7 +241,7 @@ struct VbdSolver {
                   slot_cnt, slots, c_k, c_ke, c_kd, c_mu, err, residual, range_nf, range_ne, range_fbase,
                   range_ebase, face_nb, face_dm, face_mat, face_kd, hinge_idx, hinge_prop, hinge_kd, adj_work,
                   ell16_faceA, ell16_faceB, ell16_hinge, sc_pos_cd, sc_disp, sc_ts, ring_nslot, ring_base,
-                  ring_vbase, ring_A, ring_B, ring_H, ring_hdr, spr_idx, spr_prop, spr_off, spr_adj, sspr_off,
+                  ring_vbase, ring_A, ring_B, ring_H, ring_hdr, ring_kd, spr_idx, spr_prop, spr_off, spr_adj, sspr_off,
                   sspr_adj, spr_acc, tet_idx, tet_pose, tet_off, tet_adj};
     for (void* p : ps)
       if (p) cudaFree(p);
@@ -409,6 +411,8 @@ int build_ell(VbdSolver* h) {
     if ((rc = upload_into(&h->ell16_faceA, fa)) || (rc = upload_into(&h->ell16_faceB, fb)) ||
         (rc = upload_into(&h->ell16_hinge, hr)))
       return rc;
+    dfree(h->hinge_kd);  // hinge damping: a float per hinge record, in the same slots
+    if (hdamp && (rc = upload_into(&h->hinge_kd, hkd))) return rc;
     return VBD_OK;
   }
   if ((rc = upload_into(&h->face_nb, fnb)) || (rc = upload_into(&h->face_dm, fdm)) ||
@@ -443,7 +447,6 @@ int build_ring(VbdSolver* h) {
   for (int e = 0; e < h->E; ++e) {
     const int* ei = &h->h_edges[4 * size_t(e)];
     if (ei[0] < 0 || ei[1] < 0 || !(bp[2 * e] > 0.f)) continue;
-    if (bp[2 * e + 1] > 0.f) return VBD_ERR_UNSUPPORTED;  // hinge damping is not stored
     emap.push_back({key(ei[2], ei[3]), e});
     for (int q = 0; q < 4; ++q) live_count[ei[q]]++;
   }
@@ -534,6 +537,8 @@ int build_ring(VbdSolver* h) {
   }
   std::vector<uint4> A(size_t(std::max(nrec, 1LL)), make_uint4(0u, 0u, 0u, 0u)), B(A.size(), make_uint4(0u, 0u, 0u, 0u));
   std::vector<float4> Hh(A.size(), make_float4(0.f, 0.f, 0.f, 0.f));
+  std::vector<float2> KD(A.size(), make_float2(0.f, 0.f));  // (spoke, rim) hinge damping per slot
+  bool any_kd = false;
   std::vector<unsigned> hdr(size_t(std::max(nv, 1LL)), 0u);
   for (int r = 0; r < R; ++r) {
     const int a0 = h->ranges_host[r];
@@ -552,6 +557,7 @@ int build_ring(VbdSolver* h) {
         float mu = 0.f, lm = 0.f, kd = 0.f;
         double P00 = 0, P01 = 0, P10 = 0, P11 = 0;
         float4 hv = make_float4(0.f, 0.f, 0.f, 0.f);
+        float2 hkd = make_float2(0.f, 0.f);
         if (inext >= 0) {  // face i
           const int t = F.tri[i], ord = F.ord[i];
           const double D00 = pose[4 * t], D01 = pose[4 * t + 1], D10 = pose[4 * t + 2], D11 = pose[4 * t + 3];
@@ -575,6 +581,7 @@ int build_ring(VbdSolver* h) {
             const float sgn = (ei[0] == v ? 1.f : -1.f) * (ei[2] == F.ring[i] ? 1.f : -1.f);
             hv.z = sgn * ra[e];
             hv.w = bp[2 * e] * rl[e];
+            hkd.y = bp[2 * e + 1];
             o_loc = unsigned(o - vs);
             ++found;
           }
@@ -588,6 +595,7 @@ int build_ring(VbdSolver* h) {
             const float sgn = (ei[0] == rn ? 1.f : -1.f) * (ei[2] == v ? 1.f : -1.f);
             hv.x = sgn * ra[e];
             hv.y = bp[2 * e] * rl[e];
+            hkd.x = bp[2 * e + 1];
             ++found;
           }
         }
@@ -597,6 +605,8 @@ int build_ring(VbdSolver* h) {
         B[idx] = make_uint4(__float_as_uint_host(float(P01)), __float_as_uint_host(float(P10)),
                             __float_as_uint_host(float(P11)), __float_as_uint_host(kd));
         Hh[idx] = hv;
+        KD[idx] = hkd;
+        any_kd |= hkd.x > 0.f || hkd.y > 0.f;
       }
       if (found != live_count[v]) return VBD_ERR_UNSUPPORTED;  // a hinge the fan walk would miss
     }
@@ -606,6 +616,8 @@ int build_ring(VbdSolver* h) {
       (rc = upload_into(&h->ring_vbase, vbase)) || (rc = upload_into(&h->ring_A, A)) || (rc = upload_into(&h->ring_B, B)) ||
       (rc = upload_into(&h->ring_H, Hh)) || (rc = upload_into(&h->ring_hdr, hdr)))
     return rc;
+  dfree(h->ring_kd);
+  if (any_kd && (rc = upload_into(&h->ring_kd, KD))) return rc;
   return VBD_OK;
 }
 
@@ -618,6 +630,7 @@ RingView ring_view(const VbdSolver* h) {
   e.B = h->ring_B;
   e.H = h->ring_H;
   e.hdr = h->ring_hdr;
+  e.kd = h->ring_kd;
   return e;
 }
 
@@ -630,6 +643,7 @@ Ell16View ell16_view(const VbdSolver* h) {
   e.faceA = h->ell16_faceA;
   e.faceB = h->ell16_faceB;
   e.hinge = h->ell16_hinge;
+  e.hinge_kd = h->ell_hinge_damping ? h->hinge_kd : nullptr;
   return e;
 }
 
@@ -957,6 +971,7 @@ int sc_detect(ScBuffers& b, const ScSetup& p, const int4* tri_idx, const int4* e
   q.vt_foff = b.vt_foff, q.vt_f = b.vt_f, q.ee_foff = b.ee_foff, q.ee_f = b.ee_f;
   q.bstart = b.bstart, q.ekey = b.ekey, q.eprim = b.eprim, q.stats = b.stats, q.flags = b.flags;
   q.gcap = (unsigned)std::min<long long>(b.gcap, 0xFFFFFFFFLL);
+  q.tv = b.tb > 0 ? b.tv : nullptr, q.tv_count = b.tv_count, q.tv_min = b.tv_min, q.tb = b.tb;
   pos4_t<R>* lo = (pos4_t<R>*)b.blo;
   pos4_t<R>* hi = (pos4_t<R>*)b.bhi;
   for (int kind = 0; kind < 2; ++kind) {
@@ -1157,10 +1172,17 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
           launch_persistent_ell16_pair<true>(h->occ, c, p, e, h->grid_persistent, h->block, h->smem_bytes, st);
         else if (MODE == MODE_FP32 && h->pair)
           launch_persistent_ell16_pair<false>(h->occ, c, p, e, h->grid_persistent, h->block, 0, st);
+        else if (h->ell_hinge_damping && h->smem_bytes > 0)
+          launch_persistent_ell16_damped<R, MODE, true>(h->occ, c, p, e, h->grid_persistent, h->block, h->smem_bytes,
+                                                        st);
+        else if (h->ell_hinge_damping)
+          launch_persistent_ell16_damped<R, MODE, false>(h->occ, c, p, e, h->grid_persistent, h->block, 0, st);
         else if (h->smem_bytes > 0)
           launch_persistent_ell16<R, MODE, true>(h->occ, c, p, e, h->grid_persistent, h->block, h->smem_bytes, st);
         else
           launch_persistent_ell16<R, MODE, false>(h->occ, c, p, e, h->grid_persistent, h->block, 0, st);
+      } else if (h->ell_hinge_damping) {
+        launch_persistent_ell16_damped<R, MODE, false>(0, c, p, e, h->grid_persistent, h->block, 0, st);
       } else {
         launch_persistent_ell16<R, MODE, false>(0, c, p, e, h->grid_persistent, h->block, 0, st);
       }
@@ -1298,6 +1320,14 @@ const void* persistent_kernel(VbdSolver* h) {
   }
   if (h->layout == VBD_LAYOUT_ELL16 && h->pair)
     return sm ? persistent_ell16_pair_fn<true>(h->occ) : persistent_ell16_pair_fn<false>(h->occ);
+  if (h->layout == VBD_LAYOUT_ELL16 && h->ell_hinge_damping) {
+    if (h->precision == VBD_PRECISION_FP64) return persistent_ell16_damped_fn<double, MODE_FP64, false>(0);
+    if (h->precision == VBD_PRECISION_MIXED)
+      return sm ? persistent_ell16_damped_fn<float, MODE_MIXED, true>(h->occ)
+                : persistent_ell16_damped_fn<float, MODE_MIXED, false>(h->occ);
+    return sm ? persistent_ell16_damped_fn<float, MODE_FP32, true>(h->occ)
+              : persistent_ell16_damped_fn<float, MODE_FP32, false>(h->occ);
+  }
   if (h->layout == VBD_LAYOUT_ELL16) {
     if (h->precision == VBD_PRECISION_FP64) return persistent_ell16_fn<double, MODE_FP64, false>(0);
     if (h->precision == VBD_PRECISION_MIXED)
@@ -1732,9 +1762,9 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
   if (lnh_floor && (params->layout == VBD_LAYOUT_ELL || params->layout == VBD_LAYOUT_ELL16 ||
                     params->layout == VBD_LAYOUT_RING))
     return fail(VBD_ERR_UNSUPPORTED);
-  const bool ell16_ok = h->schedule == VBD_SCHEDULE_PERSISTENT && h->max_inst_v < 65536 && !any_hinge_damping;
-  if ((params->layout == VBD_LAYOUT_ELL16 || params->layout == VBD_LAYOUT_RING) && !ell16_ok)
-    return fail(VBD_ERR_UNSUPPORTED);
+  const bool ell16_ok = h->schedule == VBD_SCHEDULE_PERSISTENT && h->max_inst_v < 65536;
+  if (params->layout == VBD_LAYOUT_ELL16 && !ell16_ok) return fail(VBD_ERR_UNSUPPORTED);
+  if (params->layout == VBD_LAYOUT_RING && !ell16_ok) return fail(VBD_ERR_UNSUPPORTED);
   if (params->layout == VBD_LAYOUT_CSR || h->L != 1 || h->soft || lnh_floor)
     h->layout = VBD_LAYOUT_CSR;
   else if (params->layout == VBD_LAYOUT_RING)
@@ -1798,6 +1828,7 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
     if (params->pair_vertices != 1 || h->layout != VBD_LAYOUT_ELL16 || h->schedule != VBD_SCHEDULE_PERSISTENT ||
         h->precision != VBD_PRECISION_FP32)
       return fail(VBD_ERR_INVALID_ARGUMENT);
+    if (any_hinge_damping) return fail(VBD_ERR_UNSUPPORTED);  // the paired bending has no damping term
     h->pair = true;
   }
   if (h->schedule == VBD_SCHEDULE_PERSISTENT && (rc = occupancy_grid(h))) return fail(rc);
@@ -1810,6 +1841,12 @@ int vbd_refresh_model(VbdHandle h, void* stream) {
   if (!h) return VBD_ERR_INVALID_ARGUMENT;
   int rc = pack_model(h, (cudaStream_t)stream);
   if (rc) return rc;
+  if (h->pair && h->E) {  // the paired kernel has no hinge damping term
+    std::vector<float> bp;
+    if ((rc = download(bp, h->md.edge_bending_properties_dev, size_t(2) * h->E))) return rc;
+    for (int e = 0; e < h->E; ++e)
+      if (bp[2 * e] > 0.f && bp[2 * e + 1] > 0.f) return VBD_ERR_UNSUPPORTED;
+  }
   if (h->layout == VBD_LAYOUT_ELL || h->layout == VBD_LAYOUT_ELL16 || h->layout == VBD_LAYOUT_RING) {
     if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return VBD_ERR_CUDA;
     if (h->layout == VBD_LAYOUT_RING) {
@@ -2366,8 +2403,14 @@ int vbd_collider_detect(VbdColliderHandle c, int32_t what, const float* pos_dev,
   if (c->V) k_col_pos<<<(c->V + 255) / 256, 256, 0, st>>>(c->V, pos_dev, c->pos);
   CK(cudaMemsetAsync(c->b.flags, 0, 4 * sizeof(int), st));
   ScSetup p{double(max_query_radius), double(min_query_radius), c->ee_eps, ref_pos_dev, nullptr};
+  const bool tris = (what & 1) && c->b.tb > 0 && c->T > 0;
+  const long long nt = (long long)c->T * c->b.tb;
+  if (tris)
+    k_sc_tri_init<<<unsigned((std::max<long long>(nt, c->T) + 255) / 256), 256, 0, st>>>(
+        c->T, c->b.tb, c->b.tv, c->b.tv_count, c->b.tv_min, max_query_radius);
   int rc = sc_detect<float>(c->b, p, c->tri_idx, c->edge_idx, c->pos, what, st);
   if (rc) return rc;
+  if (tris) k_sc_tri_finish<<<unsigned((nt + 255) / 256), 256, 0, st>>>(c->T, c->b.tb, c->b.tv);
   if ((what & 1) && c->V)
     k_col_export<<<(c->V + 255) / 256, 256, 0, st>>>(c->V, c->b.vb, c->b.vt_tri, c->b.vt_count, (const float*)c->b.vt_min,
                                                      vt_dev, vt_count_dev, vt_min_dev);
@@ -2376,6 +2419,17 @@ int vbd_collider_detect(VbdColliderHandle c, int32_t what, const float* pos_dev,
                                                      ee_dev, ee_count_dev, ee_min_dev);
   if (resize_flags_dev) k_col_flags<<<1, 32, 0, st>>>(c->b.flags, resize_flags_dev);
   CK(cudaGetLastError());
+  return VBD_OK;
+}
+
+int vbd_collider_set_triangle_buffers(VbdColliderHandle c, int32_t buffer_size, int32_t* vertices_dev,
+                                      int32_t* count_dev, float* min_dist_dev) {
+  if (!c || buffer_size < 0 || (buffer_size > 0 && c->T > 0 && (!vertices_dev || !count_dev || !min_dist_dev)))
+    return VBD_ERR_INVALID_ARGUMENT;
+  c->b.tb = buffer_size;
+  c->b.tv = buffer_size > 0 ? vertices_dev : nullptr;
+  c->b.tv_count = buffer_size > 0 ? count_dev : nullptr;
+  c->b.tv_min = buffer_size > 0 ? min_dist_dev : nullptr;
   return VBD_OK;
 }
 

@@ -165,7 +165,7 @@ __device__ __forceinline__ void solve_ell(const StepCtx<R>& c, const P& pos, con
   if (c.has_contacts) contacts_add<R>(c, v, x, f, H);
   if (MODE == MODE_MIXED && c.residual) {
     const double r2 = double(f.x) * double(f.x) + double(f.y) * double(f.y) + double(f.z) * double(f.z);
-    atomicAdd(c.residual + 32 * iteration + (threadIdx.x & 31), r2);  // 32 slots, summed on the host
+    residual_add(c.residual, iteration, r2);
   }
   vec3<R> dlt;
   double det_used;
@@ -262,8 +262,10 @@ namespace vbd {
 //           A = (a | b << 16, mu A, lambda A, D'00)      B = (D'01, D'10, D'11, damping)
 //   hinge = 16 bytes: (o0 | o1 << 16, v0 | v1 << 16, rest angle, ke * rest length)
 //           the hinge's four vertices in their (o0, o1, v0, v1) order; the solved vertex's role is the
-//           place of its own id among them. Hinge damping is not stored: models with non-zero hinge
-//           damping use the 32-bit stencil layout.
+//           place of its own id among them.
+//   hinge damping kd: a float per hinge record in a side array, present only when some hinge of the model
+//           is damped; the kernel variant that reads it (HD = true) adds the reference's Rayleigh term, which
+//           needs the four vertices' positions at the start of the step.
 
 
 struct Ell16View {
@@ -274,14 +276,16 @@ struct Ell16View {
   const uint4* faceA;
   const uint4* faceB;
   const uint4* hinge;
+  const float* hinge_kd;  // [hinge records]; NULL when no hinge is damped
 };
 
 // Membrane term of one 32-byte face record (A, B halves) for the solved vertex v at x.
 template <typename R, typename P>
 __device__ __forceinline__ void ell16_face(const StepCtx<R>& c, const P& pos, int v, int vs, vec3<R> x, uint4 A, uint4 B,
                                            vec3<R>& f, sym3<R>& H) {
+  // a dead slot or an inactive triangle (mu A = lambda A = 0, ids 0) adds exact zeros: no early exit, so the
+  // lanes of a warp run one instruction stream over their faces
   const float muA = __uint_as_float(A.y), lmA = __uint_as_float(A.z);
-  if (!(muA > 0.f || lmA > 0.f)) return;
   const R pose[4] = {R(__uint_as_float(A.w)), R(__uint_as_float(B.x)), R(__uint_as_float(B.y)),
                      R(__uint_as_float(B.z))};
   const float kd = __uint_as_float(B.w);
@@ -298,10 +302,12 @@ __device__ __forceinline__ void ell16_face(const StepCtx<R>& c, const P& pos, in
 // Bending term of one 16-byte hinge record for the solved vertex (instance-local id lv): the record lists the
 // hinge's four vertices in their (o0, o1, v0, v1) order, so the solved vertex's role is where lv appears and all
 // four positions are gathered (the solved vertex's own gather reads its current position).
-template <typename R, typename P>
-__device__ __forceinline__ void ell16_hinge(const P& pos, int vs, int lv, uint4 hh, R dt, vec3<R>& f, sym3<R>& H) {
+// HD: the model has damped hinges; kd is this record's damping (0 for an undamped hinge), and a damped hinge
+// reads the four vertices' positions at the start of the step (c.qprev).
+template <typename R, bool HD, typename P>
+__device__ __forceinline__ void ell16_hinge(const StepCtx<R>& c, const P& pos, int vs, int lv, uint4 hh, float kd,
+                                            vec3<R>& f, sym3<R>& H) {
   const float k = __uint_as_float(hh.w);
-  if (!(k > 0.f)) return;
   const int i0 = int(hh.x & 0xffffu), i1 = int(hh.x >> 16), i2 = int(hh.y & 0xffffu), i3 = int(hh.y >> 16);
   const int role = i0 == lv ? 0 : (i1 == lv ? 1 : (i2 == lv ? 2 : 3));
   vec3<R> xs[4];
@@ -309,10 +315,22 @@ __device__ __forceinline__ void ell16_hinge(const P& pos, int vs, int lv, uint4 
   xs[1] = pos.ld(vs + i1);
   xs[2] = pos.ld(vs + i2);
   xs[3] = pos.ld(vs + i3);
-  bending_add<R>(role, xs, R(__uint_as_float(hh.z)), R(1), R(k), R(0), dt, nullptr, f, H);
+  if constexpr (HD) {
+    if (kd > 0.f && k > 0.f) {
+      vec3<R> xp[4];
+      xp[0] = ld3<R>(c.qprev[vs + i0]);
+      xp[1] = ld3<R>(c.qprev[vs + i1]);
+      xp[2] = ld3<R>(c.qprev[vs + i2]);
+      xp[3] = ld3<R>(c.qprev[vs + i3]);
+      bending_add<R>(role, xs, R(__uint_as_float(hh.z)), R(1), R(k), R(kd), c.dt, xp, f, H);
+      return;
+    }
+  }
+  // dead slots (k = 0, ids 0) and degenerate hinges add exact zeros without an early exit
+  bending_add_nb<R>(role, xs, R(__uint_as_float(hh.z)), R(k), f, H);
 }
 
-template <typename R, int MODE, typename P>
+template <typename R, int MODE, bool HD, typename P>
 __device__ __forceinline__ void solve_ell16(const StepCtx<R>& c, const P& pos, const Ell16View& e, int r, int n, int j,
                                             int v, int vs, int iteration) {
   const pos4_t<R> in4 = c.inertia[v];
@@ -353,17 +371,23 @@ __device__ __forceinline__ void solve_ell16(const StepCtx<R>& c, const P& pos, c
     }
     {
       const uint4* ph = e.hinge + eb;
+      const float* pk = HD ? e.hinge_kd + eb : nullptr;
       uint4 h_n = make_uint4(0u, 0u, 0u, 0u);
       if (ne > 0) h_n = __ldcs(ph);
       for (int q = 1; q < kRecordPrefetch && q < ne; ++q) prefetch_l2(ph + (long long)q * n);
       for (int s = 0; s < ne; ++s) {
         const uint4 hh = h_n;
+        float kd = 0.f;
+        if constexpr (HD) {
+          kd = __ldcs(pk);
+          pk += n;
+        }
         if (s + kRecordPrefetch < ne) prefetch_l2(ph + (long long)kRecordPrefetch * n);
         if (s + 1 < ne) {
           ph += n;
           h_n = __ldcs(ph);
         }
-        ell16_hinge<R>(pos, vs, v - vs, hh, c.dt, f, H);
+        ell16_hinge<R, HD>(c, pos, vs, v - vs, hh, kd, f, H);
       }
     }
   }
@@ -375,7 +399,7 @@ __device__ __forceinline__ void solve_ell16(const StepCtx<R>& c, const P& pos, c
   if (c.has_contacts) contacts_add<R>(c, v, x, f, H);
   if (MODE == MODE_MIXED && c.residual) {
     const double r2 = double(f.x) * double(f.x) + double(f.y) * double(f.y) + double(f.z) * double(f.z);
-    atomicAdd(c.residual + 32 * iteration + (threadIdx.x & 31), r2);
+    residual_add(c.residual, iteration, r2);
   }
   vec3<R> dlt;
   double det_used;
@@ -541,9 +565,11 @@ __device__ __forceinline__ void solve_ell16_pair(const StepCtx<float>& c, const 
 
 // PAIR (FP32 only): each thread solves two vertices of a color at once with paired FP32 instructions
 // (solve_ell16_pair).
-template <typename R, int MODE, bool SMEM, int OCC, bool PAIR = false>
+// HD (not with PAIR): the model has damped hinges (Ell16View::hinge_kd).
+template <typename R, int MODE, bool SMEM, int OCC, bool PAIR = false, bool HD = false>
 __global__ void __launch_bounds__(OCC ? 256 : 512, OCC ? OCC : 1) k_persistent_ell16(StepCtx<R> c, PersistentPlan p,
                                                                                     Ell16View e) {
+  static_assert(!(PAIR && HD), "the paired kernel does not evaluate hinge damping");
   extern __shared__ float s_pos[];
   __shared__ int s_item;
   for (;;) {
@@ -578,7 +604,7 @@ __global__ void __launch_bounds__(OCC ? 256 : 512, OCC ? OCC : 1) k_persistent_e
           }
         } else {
           for (int j = threadIdx.x; j < b - a; j += blockDim.x)
-            solve_ell16<R, MODE>(c, pos, e, r, b - a, j, __ldg(p.color_verts + a + j), vs, it);
+            solve_ell16<R, MODE, HD>(c, pos, e, r, b - a, j, __ldg(p.color_verts + a + j), vs, it);
         }
         __syncthreads();
       }

@@ -15,6 +15,9 @@
 //   uint4 B: (D'01, D'10, D'11, membrane damping)         D' = rest inverse re-expressed for (v, r_i, r_{i+1})
 //   float4 H: (spoke rest angle, spoke ke l0, rim rest angle, rim ke l0)   zero stiffness: no hinge
 //   per vertex: k | closed << 8
+//   float2 kd: (spoke damping, rim damping), a side array present only when some hinge is damped; a damped
+//   hinge is evaluated by the generic bending routine on its four positions (the shared normals carry no
+//   velocity), which needs the positions at the start of the step
 // Each hinge is evaluated in a fixed orientation: spoke i as (o0, o1, v0, v1) = (r_{i+1}, r_{i-1}, v, r_i)
 // and rim i as (v, o_i, r_i, r_{i+1}). Swapping the two opposite vertices or the two edge vertices of a
 // hinge negates the reference's dihedral angle (particle_vbd_kernels.py:1057-1190), so the rest angle is
@@ -34,7 +37,21 @@ struct RingView {
   const uint4* B;
   const float4* H;
   const unsigned* hdr;
+  const float2* kd;  // [slots] (spoke, rim) hinge damping; NULL when no hinge is damped
 };
+
+// A damped hinge in the ring's orientation (o0, o1, v0, v1), the solved vertex in role `role`: positions as
+// offsets from the solved vertex x, ids for the positions at the start of the step.
+template <typename R>
+__device__ __forceinline__ void ring_damped_hinge(const StepCtx<R>& c, int role, vec3<R> x, const vec3<R> a[4],
+                                                  const int id[4], R rest_angle, R k, R kd, vec3<R>& f, sym3<R>& H) {
+  vec3<R> xs[4], xp[4];
+  for (int q = 0; q < 4; ++q) {
+    xs[q] = x + a[q];
+    xp[q] = ld3<R>(c.qprev[id[q]]);
+  }
+  bending_add<R>(role, xs, rest_angle, R(1), k, kd, c.dt, xp, f, H);
+}
 
 // Dihedral angle of a hinge from its two face normals (unit) and its unit edge, in the reference's
 // orientation convention: theta = atan2((n1 x n2) . e, n1 . n2).
@@ -60,25 +77,35 @@ __device__ __forceinline__ void solve_ring(const StepCtx<R>& c, const P& pos, co
     const R eps2 = R(1.0e-12);
     // slot 0
     uint4 A = __ldg(e.A + b0);
-    const vec3<R> a_first = pos.ld(vs + int(A.x & 0xffffu)) - x;
+    const int id_first = vs + int(A.x & 0xffffu);
+    const vec3<R> a_first = pos.ld(id_first) - x;
     vec3<R> a_cur = a_first, a_prev = zero3<R>(), a_second = zero3<R>();
+    int id_cur = id_first, id_prev = v, id_second = v;  // particle ids of r_i, r_{i-1}, r_1
     vec3<R> n_prev = zero3<R>(), n_first = zero3<R>();  // unit normals of faces i - 1 and 0
     R il_prev = R(0), il_first = R(0);                   // their inverse lengths (0: degenerate or absent)
     bool have_prev = false, have_first = false;
     float4 H0 = make_float4(0.f, 0.f, 0.f, 0.f);
+    float kd0 = 0.f;  // spoke damping of slot 0
     for (int i = 0; i < k; ++i) {
       const long long bi = b0 + (long long)i * n;
       const uint4 B = __ldg(e.B + bi);
       const float4 Hh = __ldg(e.H + bi);
-      if (i == 0) H0 = Hh;
+      const float2 hkd = e.kd ? __ldg(e.kd + bi) : make_float2(0.f, 0.f);
+      if (i == 0) {
+        H0 = Hh;
+        kd0 = hkd.x;
+      }
       const int inext = i + 1 < k ? i + 1 : (closed ? 0 : -1);
       uint4 An = A;
       vec3<R> a_next = zero3<R>();
+      int id_next = v;
       if (inext > 0) {
         An = __ldg(e.A + b0 + (long long)inext * n);
-        a_next = pos.ld(vs + int(An.x & 0xffffu)) - x;
+        id_next = vs + int(An.x & 0xffffu);
+        a_next = pos.ld(id_next) - x;
       } else if (inext == 0) {
         a_next = a_first;
+        id_next = id_first;
       }
       bool have_face = false;
       vec3<R> n_cur = zero3<R>();
@@ -93,8 +120,8 @@ __device__ __forceinline__ void solve_ring(const StepCtx<R>& c, const P& pos, co
           vec3<R> xp[3];
           if (kd > 0.f) {
             xp[0] = ld3<R>(c.qprev[v]);
-            xp[1] = ld3<R>(c.qprev[vs + int(A.x & 0xffffu)]);
-            xp[2] = ld3<R>(c.qprev[vs + int(An.x & 0xffffu)]);
+            xp[1] = ld3<R>(c.qprev[id_cur]);
+            xp[2] = ld3<R>(c.qprev[id_next]);  // r_0's on the face that closes a fan
           }
           membrane_add<R>(0, zero3<R>(), a_cur, a_next, pose, R(muA), R(lmA), R(kd), R(1), c.dt, xp, f, H, R(0));
         }
@@ -108,7 +135,11 @@ __device__ __forceinline__ void solve_ring(const StepCtx<R>& c, const P& pos, co
         // rim hinge i: (v, o_i, r_i, r_{i+1}), the solved vertex is the first opposite vertex
         const float kr = Hh.w;
         const unsigned o = A.x >> 16;
-        if (kr > 0.f && o != 0xffffu && il_cur > R(0)) {
+        if (kr > 0.f && o != 0xffffu && hkd.y > 0.f) {
+          const vec3<R> ha[4] = {zero3<R>(), pos.ld(vs + int(o)) - x, a_cur, a_next};
+          const int hid[4] = {v, vs + int(o), id_cur, id_next};
+          ring_damped_hinge<R>(c, 0, x, ha, hid, R(Hh.z), R(kr), R(hkd.y), f, H);
+        } else if (kr > 0.f && o != 0xffffu && il_cur > R(0)) {
           const vec3<R> b = pos.ld(vs + int(o)) - x;
           const vec3<R> N2 = cross(a_next - b, a_cur - b);
           const vec3<R> ed = a_next - a_cur;
@@ -127,9 +158,14 @@ __device__ __forceinline__ void solve_ring(const StepCtx<R>& c, const P& pos, co
       // face k - 1)
       if (i == 0) {
         a_second = a_next;
+        id_second = id_next;
         n_first = n_cur;
         il_first = il_cur;
         have_first = have_face;
+      } else if (have_face && have_prev && Hh.y > 0.f && hkd.x > 0.f) {
+        const vec3<R> ha[4] = {a_next, a_prev, zero3<R>(), a_cur};
+        const int hid[4] = {id_next, id_prev, v, id_cur};
+        ring_damped_hinge<R>(c, 2, x, ha, hid, R(Hh.x), R(Hh.y), R(hkd.x), f, H);
       } else if (have_face && have_prev && Hh.y > 0.f && il_cur > R(0) && il_prev > R(0)) {
         const R se = dot(a_cur, a_cur);
         if (se >= eps2) {
@@ -144,13 +180,20 @@ __device__ __forceinline__ void solve_ring(const StepCtx<R>& c, const P& pos, co
       }
       a_prev = a_cur;
       a_cur = a_next;
+      id_prev = id_cur;
+      id_cur = id_next;
       n_prev = n_cur;
       il_prev = il_cur;
       have_prev = have_face;
       A = An;
     }
-    // spoke 0 of a closed fan: faces 0 and k - 1 (the last face computed, now in n_prev)
-    if (closed && have_first && have_prev && H0.y > 0.f && il_first > R(0) && il_prev > R(0)) {
+    // spoke 0 of a closed fan: faces 0 and k - 1 (the last face computed, now in n_prev; a_prev and id_prev
+    // are r_{k-1}'s)
+    if (closed && have_first && have_prev && H0.y > 0.f && kd0 > 0.f) {
+      const vec3<R> ha[4] = {a_second, a_prev, zero3<R>(), a_first};
+      const int hid[4] = {id_second, id_prev, v, id_first};
+      ring_damped_hinge<R>(c, 2, x, ha, hid, R(H0.x), R(H0.y), R(kd0), f, H);
+    } else if (closed && have_first && have_prev && H0.y > 0.f && il_first > R(0) && il_prev > R(0)) {
       const R se = dot(a_first, a_first);
       if (se >= eps2) {
         const R ile = vrsqrt(se);
@@ -173,7 +216,7 @@ __device__ __forceinline__ void solve_ring(const StepCtx<R>& c, const P& pos, co
   if (c.has_contacts) contacts_add<R>(c, v, x, f, H);
   if (MODE == MODE_MIXED && c.residual) {
     const double r2 = double(f.x) * double(f.x) + double(f.y) * double(f.y) + double(f.z) * double(f.z);
-    atomicAdd(c.residual + 32 * iteration + (threadIdx.x & 31), r2);
+    residual_add(c.residual, iteration, r2);
   }
   vec3<R> dlt;
   double det_used;

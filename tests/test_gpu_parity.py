@@ -47,8 +47,6 @@ def _run_golden_substep(solver, g, s, dtype=torch.float32):
 @pytest.mark.parametrize("schedule,lanes,shared,layout", LAUNCH)
 def test_fp32_step_matches_reference_goldens(name, schedule, lanes, shared, layout):
     g = load_golden(name)
-    if layout in ("ell16", "ring") and np.any(g["model_edge_bending_properties"][:, 1] > 0.0):
-        pytest.skip("the 16-bit stencil and one-ring layouts do not store hinge damping")
     model = model_from_golden(g)
     solver = SolverVBD(model, iterations=int(g["iterations"]), friction_epsilon=float(g["friction_epsilon"]),
                        rigid_avbd_beta=float(g["beta"]), schedule=schedule, lanes_per_vertex=lanes,
@@ -127,12 +125,19 @@ def test_paired_vertices_need_fp32_ell16_persistent():
         args = dict(dict(schedule="persistent", layout="ell16"), **kw)
         with pytest.raises(_lib.VbdError, match="invalid argument|unsupported"):
             SolverVBD(model, iterations=2, pair_vertices=True, **args)
+    # the paired bending has no damping term
+    damped = model_from_golden(load_golden("step_grid_ground.npz"))
+    with pytest.raises(_lib.VbdError, match="unsupported"):
+        SolverVBD(damped, iterations=2, pair_vertices=True, schedule="persistent", layout="ell16")
 
 
 @pytest.mark.parametrize("name", FIXTURES)
-@pytest.mark.parametrize("schedule", ["per_color", "persistent"])
-@pytest.mark.parametrize("layout", ["ell", "csr"])
+@pytest.mark.parametrize("schedule,layout", [("per_color", "ell"), ("per_color", "csr"), ("persistent", "ell"),
+                                             ("persistent", "csr"), ("persistent", "ell16"), ("persistent", "ring")])
 def test_fp64_step_matches_fp64_oracle(name, schedule, layout):
+    """Every layout in FP64 against the FP64 oracle; step_grid_ground and step_complex_rest_angle carry hinge
+    damping, which the 16-bit stencil layout reads from its side array and the one-ring layout evaluates per
+    damped hinge."""
     g = load_golden(name)
     model = model_from_golden(g)
     solver = SolverVBD(model, iterations=int(g["iterations"]), friction_epsilon=float(g["friction_epsilon"]),
