@@ -15,6 +15,9 @@
 // color (apply_truncation_ts with t = 1 and no bound when self-contact is off,
 // particle_vbd_kernels.py:2877-2897). That is q += H^-1 f; this code applies it to q directly.
 #pragma once
+#include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
+
 #include <type_traits>
 
 #include "vbd_elements.cuh"
@@ -112,6 +115,16 @@ struct StepCtx {
 
 __device__ __forceinline__ void set_err(int* err, int bit) {
   if (err) atomicOr(err, bit);
+}
+
+// FP64 sum of |f|^2 over the lanes of a warp that reach this call (any subset: lanes that returned early for a
+// fixed vertex are absent), one atomic per group of converged lanes into slot (iteration, warp mod 32); the host
+// adds the 32 slots. Per-lane atomics on 32 shared addresses cost a mixed-precision substep ~60 % more.
+__device__ __forceinline__ void residual_add(double* residual, int iteration, double r2) {
+  namespace cg = cooperative_groups;
+  const cg::coalesced_group g = cg::coalesced_threads();
+  const double s = cg::reduce(g, r2, cg::plus<double>());
+  if (g.thread_rank() == 0) atomicAdd(residual + 32 * iteration + ((threadIdx.x >> 5) & 31), s);
 }
 
 __device__ __forceinline__ vec3<float> ldv3(const float* a, int i) { return {a[3 * i], a[3 * i + 1], a[3 * i + 2]}; }
