@@ -150,6 +150,7 @@ SIGNATURES = {
         [C.c_int32, C.c_int32, _vp, C.c_int32, _vp, C.c_int32, C.c_int32, C.c_float, _ip, _ip, _ip, _ip, C.POINTER(_vp)],
         C.c_int,
     ),
+    "vbd_collider_set_triangle_buffers": ([_vp, C.c_int32, _vp, _vp, _vp], C.c_int),
     "vbd_collider_detect": (
         [_vp, C.c_int32, _vp, C.c_float, C.c_float, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
         C.c_int,

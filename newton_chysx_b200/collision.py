@@ -8,7 +8,11 @@
 (``newton/_src/solvers/vbd/tri_mesh_collision.py:91-413``) and the same buffers (vertex -> colliding
 triangles, edge -> colliding edges, counts, minimum distances, ``resize_flags``), computed by the
 library's grid-based detector (``vbd_collider_*``). Within a buffer the pairs are kept in increasing
-primitive id; the reference keeps them in its BVH's traversal order.
+primitive id; the reference keeps them in its BVH's traversal order. With
+``record_triangle_contacting_vertices`` the vertex-triangle detection also fills the triangle -> colliding
+vertices buffers (``triangle_colliding_vertices``, ``_count``, ``_offsets``, ``_buffer_sizes``, ``_min_dist``;
+``tri_mesh_collision.py:170-200``, ``geometry/kernels.py:1373-1384``), each triangle's vertices in increasing
+id where the reference has them in the order its threads arrived.
 """
 
 from __future__ import annotations
@@ -88,15 +92,14 @@ class TriMeshCollisionDetector:
                  edge_filtering_list_offsets=None, triangle_triangle_collision_buffer_pre_alloc=8,
                  triangle_triangle_collision_buffer_max_alloc=256, edge_edge_parallel_epsilon=1e-5,
                  collision_detection_block_size=16):  # fmt: skip
-        if record_triangle_contacting_vertices:
-            raise NotImplementedError("triangle -> colliding vertex buffers are not recorded by this detector")
         self.model = model
         self.device = model.device
         self.vertex_positions = model.particle_q if vertex_positions is None else vertex_positions
         self.vertex_collision_buffer_pre_alloc = int(vertex_collision_buffer_pre_alloc)
         self.edge_collision_buffer_pre_alloc = int(edge_collision_buffer_pre_alloc)
         self.edge_edge_parallel_epsilon = float(edge_edge_parallel_epsilon)
-        self.record_triangle_contacting_vertices = False
+        self.record_triangle_contacting_vertices = bool(record_triangle_contacting_vertices)
+        self.triangle_collision_buffer_pre_alloc = int(triangle_collision_buffer_pre_alloc)
         V, E = model.particle_count, model.edge_count
         vb, eb = self.vertex_collision_buffer_pre_alloc, self.edge_collision_buffer_pre_alloc
         dev = self.device
@@ -112,6 +115,17 @@ class TriMeshCollisionDetector:
         self.edge_colliding_edges_buffer_sizes = torch.full((E,), eb, dtype=i32, device=dev)
         self.edge_colliding_edges_offsets = torch.arange(0, (E + 1) * eb, eb, dtype=i32, device=dev)
         self.triangle_colliding_vertices_min_dist = torch.zeros(model.tri_count, dtype=torch.float32, device=dev)
+        T, tb = model.tri_count, self.triangle_collision_buffer_pre_alloc
+        if self.record_triangle_contacting_vertices:
+            self.triangle_colliding_vertices = torch.full((T * tb,), -1, dtype=i32, device=dev)
+            self.triangle_colliding_vertices_count = torch.zeros(T, dtype=i32, device=dev)
+            self.triangle_colliding_vertices_buffer_sizes = torch.full((T,), tb, dtype=i32, device=dev)
+            self.triangle_colliding_vertices_offsets = torch.arange(0, (T + 1) * tb, tb, dtype=i32, device=dev)
+        else:
+            self.triangle_colliding_vertices = None
+            self.triangle_colliding_vertices_count = None
+            self.triangle_colliding_vertices_buffer_sizes = None
+            self.triangle_colliding_vertices_offsets = None
         self.resize_flags = torch.zeros(4, dtype=i32, device=dev)
         self._h = None
         self.set_collision_filter_list(vertex_triangle_filtering_list, vertex_triangle_filtering_list_offsets,
@@ -142,6 +156,12 @@ class TriMeshCollisionDetector:
                 self.vertex_collision_buffer_pre_alloc, self.edge_collision_buffer_pre_alloc,
                 self.edge_edge_parallel_epsilon, vo, vf, eo, ef, C.byref(h)), "vbd_collider_create")  # fmt: skip
         self._h = h
+        if self.record_triangle_contacting_vertices:
+            _lib.check(lib.vbd_collider_set_triangle_buffers(
+                h, self.triangle_collision_buffer_pre_alloc, C.c_void_p(self.triangle_colliding_vertices.data_ptr()),
+                C.c_void_p(self.triangle_colliding_vertices_count.data_ptr()),
+                C.c_void_p(self.triangle_colliding_vertices_min_dist.data_ptr())),
+                "vbd_collider_set_triangle_buffers")  # fmt: skip
 
     def refit(self, new_pos=None):
         """The grid is rebuilt by every detection; this only records the positions to use."""
@@ -171,7 +191,8 @@ class TriMeshCollisionDetector:
 
     def vertex_triangle_collision_detection(self, max_query_radius, min_query_radius=0.0,
                                             min_distance_filtering_ref_pos=None):  # fmt: skip
-        self.triangle_colliding_vertices_min_dist.fill_(float(max_query_radius))
+        if not self.record_triangle_contacting_vertices:  # recorded: the detection initialises and fills it
+            self.triangle_colliding_vertices_min_dist.fill_(float(max_query_radius))
         self._detect(1, max_query_radius, min_query_radius, min_distance_filtering_ref_pos)
 
     def edge_edge_collision_detection(self, max_query_radius, min_query_radius=0.0,

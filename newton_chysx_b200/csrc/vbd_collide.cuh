@@ -19,6 +19,7 @@
 // For the solve, the recorded pairs are compacted into dense lists, and every vertex gets a sorted list of
 // (pair, slot) entries naming the pairs it belongs to, so that its solve gathers its contact terms itself.
 #pragma once
+#include <climits>
 #include <cub/cub.cuh>
 
 #include "vbd_selfcontact.cuh"
@@ -44,7 +45,11 @@ struct ScBuffers {
   int* ee_edge = nullptr;        // [E * eb]
   int* ee_count = nullptr;       // [E]
   void* ee_min = nullptr;        // [E] R
-  int* flags = nullptr;          // [4] overflow flags: 0 vertex buffers, 2 edge buffers; 3 internal (grid)
+  int* flags = nullptr;          // [4] overflow flags: 0 vertex, 1 triangle, 2 edge buffers; 3 internal (grid)
+  int* tv = nullptr;             // caller's triangle -> colliding vertices buffers (stand-alone detector only)
+  int* tv_count = nullptr;
+  float* tv_min = nullptr;
+  int tb = 0;
   int* tmp = nullptr;            // [max(V, E) + 1]
   int* vt_off = nullptr;         // [V + 1]
   int2* vt_pairs = nullptr;      // [V * vb] (vertex, triangle)
@@ -195,7 +200,44 @@ struct ScQuery {
   const double* stats;
   int* flags;
   unsigned gcap;  // grid entries written (bucket ranges are clamped to it)
+  // triangle -> colliding vertices (the stand-alone detector's record_triangle_contacting_vertices); tv NULL = off
+  int* tv;         // [T, tb] vertex ids, kept increasing, INT_MAX past the stored ones during the query
+  int* tv_count;   // [T] pairs found (may exceed tb)
+  float* tv_min;   // [T] minimum distance, as float bits (distances are >= 0, so integer order is value order)
+  int tb;
 };
+
+// Triangle side of a vertex-triangle pair (vertex_triangle_collision_detection_kernel with its
+// triangle_colliding_vertices buffers, geometry/kernels.py:1373-1384): count, minimum distance, and the vertex in
+// the triangle's list, which keeps the tb smallest vertex ids in increasing order whatever the thread timing (a
+// sorted insertion: slot j keeps the smallest id of those that reach it, the larger one moves on).
+__device__ __forceinline__ void record_triangle_vertex(const ScQuery& s, int t, int v, float dist) {
+  atomicAdd(s.tv_count + t, 1);
+  atomicMin(reinterpret_cast<int*>(s.tv_min) + t, __float_as_int(dist));
+  int* slot = s.tv + size_t(t) * s.tb;
+  int val = v;
+  for (int j = 0; j < s.tb; ++j) {
+    const int old = atomicMin(slot + j, val);
+    if (old == INT_MAX) return;
+    val = max(old, val);
+  }
+  atomicOr(s.flags + 1, 1);  // TRI_COLLISION_BUFFER_OVERFLOW_INDEX
+}
+
+__global__ void k_sc_tri_init(int T, int tb, int* tv, int* tv_count, float* tv_min, float radius) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < (long long)T * tb) tv[i] = INT_MAX;
+  if (i < T) {
+    tv_count[i] = 0;
+    tv_min[i] = radius;
+  }
+}
+
+// Slots past the stored vertices read -1.
+__global__ void k_sc_tri_finish(int T, int tb, int* tv) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < (long long)T * tb && tv[i] == INT_MAX) tv[i] = -1;
+}
 
 template <typename R>
 __device__ __forceinline__ vec3<R> rest_at(const float* q, int i) {
@@ -249,6 +291,7 @@ __global__ void k_sc_query_vt(ScQuery s, const pos4_t<R>* __restrict__ pos, cons
             mn = vmin(mn, dist);
             insert_smallest(list, min(cnt, s.vb), s.vb, t);
             ++cnt;
+            if (s.tv) record_triangle_vertex(s, t, v, float(dist));
           }
         }
       }

@@ -245,3 +245,111 @@ def test_selfcontact_needs_per_color_csr():
         SolverVBD(model, layout="ell", **kw)
     with pytest.raises(ValueError):
         SolverVBD(model, **dict(kw, particle_self_contact_margin=1e-3))
+
+
+def _point_triangle_distance(p, a, b, c):
+    """|p - closest point of triangle abc| (float64, vectorised): the closest point of the plane, clamped into the
+    triangle through its edges when it falls outside."""
+    ab, ac, ap = b - a, c - a, p - a
+    n = np.cross(ab, ac)
+    nn = np.einsum("ij,ij->i", n, n)
+    q = p - n * (np.einsum("ij,ij->i", ap, n) / nn)[:, None]
+
+    def inside(u, v, w):
+        return np.einsum("ij,ij->i", np.cross(v - u, q - u), n) >= 0.0
+
+    def seg(u, v):
+        d = v - u
+        t = np.clip(np.einsum("ij,ij->i", p - u, d) / np.einsum("ij,ij->i", d, d), 0.0, 1.0)
+        return np.linalg.norm(p - (u + d * t[:, None]), axis=1)
+
+    plane = np.linalg.norm(p - q, axis=1)
+    edges = np.minimum(np.minimum(seg(a, b), seg(b, c)), seg(c, a))
+    return np.where(inside(a, b, c) & inside(b, c, a) & inside(c, a, b), plane, edges)
+
+
+def _check_triangle_side(det, tri, q, pairs, T, tb, margin):
+    """The detector's triangle -> colliding vertices buffers against the pair set (vertex, triangle): per triangle
+    the count of its pairs, its tb smallest vertex ids in increasing order (-1 after), and the smallest pair
+    distance (margin when none) to 1e-6."""
+    got = det.triangle_colliding_vertices.cpu().numpy().reshape(T, tb)
+    cnt = det.triangle_colliding_vertices_count.cpu().numpy()
+    mind = det.triangle_colliding_vertices_min_dist.cpu().numpy()
+    by_tri = {}
+    for v, t in pairs:
+        by_tri.setdefault(int(t), []).append(int(v))
+    want_cnt = np.zeros(T, dtype=np.int64)
+    want_min = np.full(T, margin)
+    for t, vs in by_tri.items():
+        vs = sorted(vs)
+        want_cnt[t] = len(vs)
+        row = np.full(tb, -1)
+        row[: min(tb, len(vs))] = vs[:tb]
+        np.testing.assert_array_equal(got[t], row)
+        qv = q[vs].astype(np.float64)
+        abc = [np.repeat(q[tri[t, k]][None].astype(np.float64), len(vs), 0) for k in range(3)]
+        want_min[t] = _point_triangle_distance(qv, *abc).min()
+    np.testing.assert_array_equal(cnt, want_cnt)
+    empty = want_cnt == 0
+    assert np.all(got[empty] == -1)
+    assert np.abs(mind - want_min).max() <= 1e-6
+    overflow = bool(np.any(want_cnt > tb))
+    assert bool(det.resize_flags[1].item()) == overflow
+    return overflow
+
+
+@pytest.mark.parametrize("name", SCENES)
+def test_detector_records_triangle_contacting_vertices(name):
+    """record_triangle_contacting_vertices: the reference records every vertex-triangle pair on the triangle's side
+    as well (geometry/kernels.py:1373-1384). The golden scenes' vertex buffers (the reference's own detection, no
+    overflow) hold every pair, so they give each triangle's colliding vertices and count."""
+    g = load_golden(name)
+    model = model_from_golden(g)
+    tb = 16
+    det = TriMeshCollisionDetector(model, record_triangle_contacting_vertices=True,
+                                   triangle_collision_buffer_pre_alloc=tb, vertex_collision_buffer_pre_alloc=32,
+                                   edge_collision_buffer_pre_alloc=64,
+                                   vertex_triangle_filtering_list=g["sc_vt_filter"],
+                                   vertex_triangle_filtering_list_offsets=g["sc_vt_filter_offsets"],
+                                   edge_filtering_list=g["sc_ee_filter"],
+                                   edge_filtering_list_offsets=g["sc_ee_filter_offsets"])  # fmt: skip
+    tri = g["model_tri_indices"]
+    margin = float(g["sc_margin"])
+    seen = 0
+    for s in range(int(g["substeps"])):
+        q = g[f"s{s}_q_in"].astype(np.float32)
+        det.refit(_t(q))
+        kw = dict(min_query_radius=float(g.get("sc_rest_exclusion", 0.0)), min_distance_filtering_ref_pos=model.particle_q)
+        det.vertex_triangle_collision_detection(margin, **kw)
+        torch.cuda.synchronize()
+        vt = g[f"s{s}_cd0_vt"].reshape(-1, 2)
+        assert np.all(g[f"s{s}_cd0_vt_count"] <= 32)  # the reference kept every pair
+        pairs = [(int(v), int(t)) for v, t in vt if v >= 0]
+        seen += len(pairs)
+        _check_triangle_side(det, tri, q, pairs, model.tri_count, tb, margin)
+    assert seen > 0
+
+
+@pytest.mark.parametrize("tb", [16, 2])
+def test_detector_triangle_buffers_match_brute_force(tb):
+    """Triangle buffers on a crumpled two-layer sheet against the oracle's brute-force pairs; with 2 slots per
+    triangle the buffers overflow, keep the smallest vertex ids and raise resize flag 1."""
+    model, q = _crumpled()
+    margin = 6e-3
+    vt, ee = build_contact_filters(model.particle_count, model.tri_indices, model.edge_indices, 2)
+    det = TriMeshCollisionDetector(model, record_triangle_contacting_vertices=True,
+                                   triangle_collision_buffer_pre_alloc=tb, vertex_collision_buffer_pre_alloc=32,
+                                   vertex_triangle_filtering_list=vt[0], vertex_triangle_filtering_list_offsets=vt[1],
+                                   edge_filtering_list=ee[0], edge_filtering_list_offsets=ee[1])  # fmt: skip
+    det.refit(_t(q))
+    det.vertex_triangle_collision_detection(margin)
+    torch.cuda.synchronize()
+    om = _oracle(model, None)
+    osc = orc.SelfContact(np.zeros((model.particle_count, 3)), radius=margin, margin=margin, vt_filter=vt,
+                          ee_filter=ee, vertex_buffer=32, edge_buffer=64)  # fmt: skip
+    ref = orc.collide(om, osc, q.astype(np.float64), precision=32, nthreads=orc.max_threads())
+    assert np.all(ref["vt_count"] <= 32)
+    pairs = [(int(v), int(t)) for v, t in ref["vt"].reshape(-1, 2) if v >= 0]
+    assert len(pairs) > model.particle_count // 4
+    overflow = _check_triangle_side(det, model.tri_indices.cpu().numpy(), q, pairs, model.tri_count, tb, margin)
+    assert overflow == (tb == 2)
