@@ -139,40 +139,6 @@ __host__ __device__ __forceinline__ void bending_add(int ord, const vec3<R> x[4]
   souter_add(H, d, hk);
 }
 
-// bending_add without damping and without early exits, for the stencil sweeps: a live hinge (k > 0 and |N1|,
-// |N2|, |e| >= 1e-6) adds the same terms with the same arithmetic; a dead slot or a degenerate hinge adds exact
-// zeros (its stiffness is replaced by 0 and every intermediate stays finite: the inverse lengths are taken of
-// max(s, 1e-12), the live threshold, so that products such as |e|^-1 |N1|^-2 stay below 1e18 and a zero times
-// them is zero), so a warp's lanes run one instruction stream over their hinges without divergent exits.
-template <typename R>
-__host__ __device__ __forceinline__ void bending_add_nb(int ord, const vec3<R> x[4], R rest_angle, R k, vec3<R>& f,
-                                                        sym3<R>& H) {
-  const vec3<R> x02 = x[2] - x[0], x03 = x[3] - x[0], x13 = x[3] - x[1], x12 = x[2] - x[1], e = x[3] - x[2];
-  const vec3<R> N1 = cross(x02, x03), N2 = cross(x13, x12);
-  const R s1 = dot(N1, N1), s2 = dot(N2, N2), se = dot(e, e);
-  const R eps2 = R(1.0e-12);
-  const bool live = k > R(0) && !(s1 < eps2 || s2 < eps2 || se < eps2);
-  const R il1 = vrsqrt(vmax(s1, eps2)), il2 = vrsqrt(vmax(s2, eps2)), ile = vrsqrt(vmax(se, eps2));
-  const R theta = vatan2(dot(cross(N1, N2), e) * ile, dot(N1, N2));
-  const R kk = live ? k : R(0);
-  const R dE = kk * (theta - rest_angle);
-  const R le = se * ile;
-  const R q1 = il1 * il1, q2 = il2 * il2;
-  R a, b;
-  if (ord <= 1) {
-    a = ord == 0 ? -le * q1 : R(0);
-    b = ord == 1 ? -le * q2 : R(0);
-  } else {
-    const vec3<R> a1 = ord == 2 ? x03 : -x02;
-    const vec3<R> a2 = ord == 2 ? x13 : -x12;
-    a = dot(a1, e) * (ile * q1);
-    b = dot(a2, e) * (ile * q2);
-  }
-  const vec3<R> d = a * N1 + b * N2;
-  f = f + (-dE) * d;
-  souter_add(H, d, kk);
-}
-
 // Penalty contact with a static or moving shape point. pen > 0 is the penetration depth, n the unit
 // normal, rel the particle's displacement this step relative to the shape point.
 template <typename R>

@@ -283,9 +283,8 @@ struct Ell16View {
 template <typename R, typename P>
 __device__ __forceinline__ void ell16_face(const StepCtx<R>& c, const P& pos, int v, int vs, vec3<R> x, uint4 A, uint4 B,
                                            vec3<R>& f, sym3<R>& H) {
-  // a dead slot or an inactive triangle (mu A = lambda A = 0, ids 0) adds exact zeros: no early exit, so the
-  // lanes of a warp run one instruction stream over their faces
   const float muA = __uint_as_float(A.y), lmA = __uint_as_float(A.z);
+  if (!(muA > 0.f || lmA > 0.f)) return;
   const R pose[4] = {R(__uint_as_float(A.w)), R(__uint_as_float(B.x)), R(__uint_as_float(B.y)),
                      R(__uint_as_float(B.z))};
   const float kd = __uint_as_float(B.w);
@@ -308,6 +307,7 @@ template <typename R, bool HD, typename P>
 __device__ __forceinline__ void ell16_hinge(const StepCtx<R>& c, const P& pos, int vs, int lv, uint4 hh, float kd,
                                             vec3<R>& f, sym3<R>& H) {
   const float k = __uint_as_float(hh.w);
+  if (!(k > 0.f)) return;
   const int i0 = int(hh.x & 0xffffu), i1 = int(hh.x >> 16), i2 = int(hh.y & 0xffffu), i3 = int(hh.y >> 16);
   const int role = i0 == lv ? 0 : (i1 == lv ? 1 : (i2 == lv ? 2 : 3));
   vec3<R> xs[4];
@@ -316,7 +316,7 @@ __device__ __forceinline__ void ell16_hinge(const StepCtx<R>& c, const P& pos, i
   xs[2] = pos.ld(vs + i2);
   xs[3] = pos.ld(vs + i3);
   if constexpr (HD) {
-    if (kd > 0.f && k > 0.f) {
+    if (kd > 0.f) {
       vec3<R> xp[4];
       xp[0] = ld3<R>(c.qprev[vs + i0]);
       xp[1] = ld3<R>(c.qprev[vs + i1]);
@@ -326,8 +326,7 @@ __device__ __forceinline__ void ell16_hinge(const StepCtx<R>& c, const P& pos, i
       return;
     }
   }
-  // dead slots (k = 0, ids 0) and degenerate hinges add exact zeros without an early exit
-  bending_add_nb<R>(role, xs, R(__uint_as_float(hh.z)), R(k), f, H);
+  bending_add<R>(role, xs, R(__uint_as_float(hh.z)), R(1), R(k), R(0), c.dt, nullptr, f, H);
 }
 
 template <typename R, int MODE, bool HD, typename P>

@@ -37,17 +37,6 @@ static void run_bending(int ord, const double* x, const double* xp, int boundary
 }
 
 template <typename R>
-static void run_bending_nb(int ord, const double* x, double ra, double k, double* out) {
-  vec3<R> X[4];
-  for (int i = 0; i < 4; ++i) X[i] = {R(x[3 * i]), R(x[3 * i + 1]), R(x[3 * i + 2])};
-  vec3<R> f = zero3<R>();
-  sym3<R> H = szero<R>();
-  bending_add_nb<R>(ord, X, R(ra), R(k), f, H);
-  double o[12] = {f.x, f.y, f.z, H.xx, H.xy, H.xz, H.xy, H.yy, H.yz, H.xz, H.yz, H.zz};
-  for (int i = 0; i < 12; ++i) out[i] = o[i];
-}
-
-template <typename R>
 static void run_contact(double pen, const double* n, const double* rel, double ke, double kd, double mu, double eps,
                         double dt, double* out) {
   vec3<R> f = zero3<R>();
@@ -68,10 +57,6 @@ void host_bending(int prec, int ord, const double* x, const double* xp, int boun
                   double kd, double dt, double* out) {
   if (prec == 64) run_bending<double>(ord, x, xp, boundary, ra, rl, ke, kd, dt, out);
   else run_bending<float>(ord, x, xp, boundary, ra, rl, ke, kd, dt, out);
-}
-void host_bending_nb(int prec, int ord, const double* x, double ra, double k, double* out) {
-  if (prec == 64) run_bending_nb<double>(ord, x, ra, k, out);
-  else run_bending_nb<float>(ord, x, ra, k, out);
 }
 void host_contact(int prec, double pen, const double* n, const double* rel, double ke, double kd, double mu,
                   double eps, double dt, double* out) {
