@@ -1780,13 +1780,15 @@ int vbd_create(const VbdModelDesc* model, const VbdSolverParams* params, VbdHand
       h->schedule == VBD_SCHEDULE_PERSISTENT && h->block > 512)
     return fail(VBD_ERR_INVALID_ARGUMENT);
   if (params->min_blocks_per_sm != 0) {
+    // the kernel is compiled for min_blocks_per_sm CTAs of 256 threads (its register budget); CTAs of 128 threads
+    // run twice as many instances side by side on an SM under the same budget
     if (params->min_blocks_per_sm < 2 || params->min_blocks_per_sm > 4 ||
         (h->layout != VBD_LAYOUT_ELL && h->layout != VBD_LAYOUT_ELL16 && h->layout != VBD_LAYOUT_RING) ||
         h->schedule != VBD_SCHEDULE_PERSISTENT || h->precision == VBD_PRECISION_FP64 ||
-        (params->block_size != 0 && params->block_size != 256))
+        (params->block_size != 0 && params->block_size != 256 && params->block_size != 128))
       return fail(VBD_ERR_INVALID_ARGUMENT);
     h->occ = params->min_blocks_per_sm;
-    h->block = 256;
+    h->block = params->block_size ? params->block_size : 256;
   }
   if (h->layout == VBD_LAYOUT_ELL || h->layout == VBD_LAYOUT_ELL16 || h->layout == VBD_LAYOUT_RING) {
     if (h->schedule == VBD_SCHEDULE_PERSISTENT) {
