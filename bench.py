@@ -1294,9 +1294,18 @@ def run_precision(args):
     b, _ = build_precision_model(args.precision_n)
     model = b.finalize(dev)
     iters, frames = 30, args.precision_frames
+    # sliver-adjacent vertices: those of triangles below 1e-3 of the median rest area
+    areas = model.tri_areas.cpu().numpy()
+    sliver = np.zeros(model.particle_count, dtype=bool)
+    sliver[np.unique(model.tri_indices.cpu().numpy()[areas < 1e-3 * np.median(areas)].ravel())] = True
     out = {"workload": f"precision stress {args.precision_n}x{args.precision_n}", "frames": frames, "substeps": 10,
-           "iterations": iters, "vertices": model.particle_count, "triangles": model.tri_count}  # fmt: skip
+           "iterations": iters, "vertices": model.particle_count, "triangles": model.tri_count,
+           "sliver_adjacent_vertices": int(sliver.sum())}  # fmt: skip
     solvers = {p: nb.SolverVBD(model, iterations=iters, precision=p, schedule="per_color") for p in ("fp64", "fp32", "mixed")}
+    # mixed precision at further FP64-solve thresholds (one-substep errors only)
+    extra = {f"mixed_threshold_{t:g}": nb.SolverVBD(model, iterations=iters, precision="mixed", schedule="per_color",
+                                                     fp64_solve_threshold=t) for t in args.mixed_thresholds}  # fmt: skip
+    solvers.update(extra)
 
     def states(dtype):
         s0, s1 = model.state(), model.state()
@@ -1331,6 +1340,11 @@ def run_precision(args):
         d = np.linalg.norm(a - b, axis=1)
         return {"max_m": float(d.max()), "rms_m": float(np.sqrt((d * d).mean()))}
 
+    def err_split(a, b):
+        d = np.linalg.norm(a - b, axis=1)
+        return {"sliver_max_m": float(d[sliver].max()), "rest_max_m": float(d[~sliver].max()),
+                "rest_rms_m": float(np.sqrt((d[~sliver] ** 2).mean()))}  # fmt: skip
+
     sample_frames = sorted({0, frames // 4, frames // 2, frames - 1})
     ref, samples, t64 = run("fp64", sample_frames=sample_frames)
     pert, _, _ = run("fp64", perturb=1e-12)
@@ -1338,6 +1352,32 @@ def run_precision(args):
                    "device_errors": solvers["fp64"].device_errors()}  # fmt: skip
     out["fp64_sensitivity_floor"] = {"perturbation_m": 1e-12,
                                      "per_frame_max_m": [err(a, b)["max_m"] for a, b in zip(ref, pert, strict=True)]}  # fmt: skip
+    # the error of one substep that rounding the state to FP32 alone causes: the FP64 step from the FP32-rounded
+    # state against the FP64 step from the exact state (no FP32 arithmetic at all)
+    floor = {}
+    for f, (q, qd) in samples.items():
+        outs = []
+        for rounded in (False, True):
+            s_in, s_out = states(torch.float64)
+            s_in.particle_q.copy_(q.float().double() if rounded else q)
+            s_in.particle_qd.copy_(qd.float().double() if rounded else qd)
+            solvers["fp64"].step(s_in, s_out, None, None, DT)
+            outs.append(s_out.particle_q.cpu().numpy())
+        torch.cuda.synchronize()
+        floor[f"frame_{f}"] = err_split(outs[1], outs[0])
+    out["fp64_from_fp32_rounded_state"] = floor
+    for name in extra:
+        one = {}
+        for f, (q, qd) in samples.items():
+            outs = []
+            for key, dtype in (("fp64", torch.float64), (name, torch.float32)):
+                s_in, s_out = states(dtype)
+                s_in.particle_q.copy_(q)
+                s_in.particle_qd.copy_(qd)
+                solvers[key].step(s_in, s_out, None, None, DT)
+                outs.append(s_out.particle_q.double().cpu().numpy())
+            one[f"frame_{f}"] = err_split(outs[1], outs[0])
+        out[name] = {"one_substep_error": one}
     for prec in ("fp32", "mixed"):
         traj, _, t = run(prec)
         o = {"vertex_iters_per_s": model.particle_count * iters * frames * 10 / (t * 1e-3),
@@ -1355,7 +1395,8 @@ def run_precision(args):
             s_in.particle_qd.copy_(qd)
             solvers[prec].step(s_in, s_out, None, None, DT)
             torch.cuda.synchronize()
-            one[f"frame_{f}"] = err(s_out.particle_q.double().cpu().numpy(), s64_out.particle_q.cpu().numpy())
+            a, b64 = s_out.particle_q.double().cpu().numpy(), s64_out.particle_q.cpu().numpy()
+            one[f"frame_{f}"] = dict(err(a, b64), **err_split(a, b64))
         o["one_substep_error"] = one
         if prec == "mixed":
             o["residual_last_step"] = solvers[prec].residuals().tolist()
@@ -1407,6 +1448,8 @@ def main():
     ap.add_argument("--no-pos-err", action="store_true")
     ap.add_argument("--precision-n", type=int, default=1024)
     ap.add_argument("--precision-frames", type=int, default=60)
+    ap.add_argument("--mixed-thresholds", type=float, nargs="*", default=[],
+                    help="precision workload: further FP64-solve thresholds of mixed precision to compare")
     ap.add_argument("--traffic", type=float, default=None, help="DRAM bytes per launch from an ncu capture")
     ap.add_argument("--sc-n", type=int, default=256, help="selfcontact workload: grid side (vertices)")
     ap.add_argument("--sc-settle-frames", type=int, default=40, help="selfcontact workload: untimed frames first")

@@ -1,8 +1,8 @@
 """Generate golden vectors for the cloth VBD path by executing the reference's own code.
 
-Run in a container that has the reference checkout (read-only) at ``/root/reference``::
+Run where a checkout of the reference project is readable, naming its root (or set ``VBD_REFERENCE_ROOT``)::
 
-    python tests/golden/make_golden.py [--ref /root/reference] [--out tests/golden]
+    python tests/golden/make_golden.py --ref PATH/TO/newton-ChysX [--out tests/golden]
 
 Warp is not installed, so ``warp_shim.py`` stands in for the Warp builtins and the
 reference's kernel bodies run as plain float64 Python. The functions are lifted out of
@@ -1131,9 +1131,12 @@ def rot_z(deg):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("VBD_REFERENCE_ROOT"),
+                    help="root of the reference checkout (default: $VBD_REFERENCE_ROOT)")
     ap.add_argument("--out", default=HERE)
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("name the reference checkout with --ref or VBD_REFERENCE_ROOT")
     ns = load_reference(args.ref)
 
     np.savez_compressed(os.path.join(args.out, "elements.npz"), **element_cases(ns))
