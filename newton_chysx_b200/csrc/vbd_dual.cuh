@@ -98,6 +98,14 @@ VBD_DUAL_T VBD_HD Dual<R, N> vrsqrt(const Dual<R, N>& a) {
   for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * k;
   return r;
 }
+VBD_DUAL_T VBD_HD Dual<R, N> vrcp(const Dual<R, N>& a) {
+  Dual<R, N> r;
+  r.v = vrcp(a.v);
+  const R k = -r.v * r.v;
+#pragma unroll
+  for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * k;
+  return r;
+}
 VBD_DUAL_T VBD_HD Dual<R, N> vatan2(const Dual<R, N>& y, const Dual<R, N>& x) {
   Dual<R, N> r;
   r.v = vatan2(y.v, x.v);

@@ -11,7 +11,7 @@
 //                Because the unit normals n1, n2 are orthogonal to the unit edge e and
 //                n2 = cos(theta) n1 + sin(theta) (e x n1), that expression reduces exactly to the classic
 //                dihedral gradient (Bridson et al. 2003, "Simulation of clothing with folds and
-//                wrinkles"), with N1 = x02 x x03, N2 = x13 x x12:
+//                wrinkles"), with N1 = x02 x x03, N2 = x13 x x12 (formed as x02 x e and e x x13):
 //                  dtheta/dx0 = -|e| / |N1| n1
 //                  dtheta/dx1 = -|e| / |N2| n2
 //                  dtheta/dx2 =  (x03 . e) / |N1| n1 + (x13 . e) / |N2| n2
@@ -49,16 +49,18 @@ __host__ __device__ __forceinline__ void membrane_add(int ord, vec3<R> x0, vec3<
   const R lnh = lmbd + mu;
   const R lsafe = lnh_floor > R(0) ? (lnh < R(0) ? R(-1) : R(1)) * vmax(vabs(lnh), lnh_floor) : (lnh == R(0) ? R(1) : lnh);
   const R alpha = R(1) + vdiv_fast(mu, lsafe);
-  const vec3<R> g0 = invJ * (f11 * f0 - f01 * f1);
-  const vec3<R> g1 = invJ * (f00 * f1 - f01 * f0);
   const R s = lnh * (J - alpha);
   const R m0 = R(ord == 0), m1 = R(ord == 1), m2 = R(ord == 2);
   const R d0 = D00 * (m1 - m0) + D10 * (m2 - m0);
   const R d1 = D01 * (m1 - m0) + D11 * (m2 - m0);
-  // force = -(P0 d0 + P1 d1),  P_i = mu f_i + s g_i
-  vec3<R> force = -((mu * f0 + s * g0) * d0 + (mu * f1 + s * g1) * d1);
+  // with g0 = (f11 f0 - f01 f1) / J and g1 = (f00 f1 - f01 f0) / J the derivative of J is dJ = g0 d0 + g1 d1 =
+  // e0 f0 + e1 f1, and the force -(P0 d0 + P1 d1) with P_i = mu f_i + s g_i is -(c0 f0 + c1 f1): scalar
+  // coefficients instead of the vectors g0, g1
+  const R e0 = invJ * (f11 * d0 - f01 * d1), e1 = invJ * (f00 * d1 - f01 * d0);
+  const vec3<R> dJ = e0 * f0 + e1 * f1;
+  const R c0 = mu * d0 + s * e0, c1 = mu * d1 + s * e1;
+  vec3<R> force = -(c0 * f0 + c1 * f1);
   const R r = vmax(R(0), s) * invJ;
-  const vec3<R> dJ = g0 * d0 + g1 * d1;
   const vec3<R> w = f1 * d0 - f0 * d1;
   const R Ic = mu * (d0 * d0 + d1 * d1) + r * (d0 * d0 * f11 + d1 * d1 * f00 - R(2) * d0 * d1 * f01);
   sym3<R> h = sdiag(Ic);
@@ -96,36 +98,38 @@ __host__ __device__ __forceinline__ void membrane_add(int ord, vec3<R> x0, vec3<
 template <typename R>
 __host__ __device__ __forceinline__ void bending_add(int ord, const vec3<R> x[4], R rest_angle, R rest_length, R ke,
                                                      R kd, R dt, const vec3<R>* xp, vec3<R>& f, sym3<R>& H) {
-  const vec3<R> x02 = x[2] - x[0], x03 = x[3] - x[0], x13 = x[3] - x[1], x12 = x[2] - x[1], e = x[3] - x[2];
-  const vec3<R> N1 = cross(x02, x03), N2 = cross(x13, x12);
+  // with x03 = x02 + e and x12 = x13 - e: N1 = x02 x x03 = x02 x e, N2 = x13 x x12 = e x x13
+  const vec3<R> x02 = x[2] - x[0], x13 = x[3] - x[1], e = x[3] - x[2];
+  const vec3<R> N1 = cross(x02, e), N2 = cross(e, x13);
   const R s1 = dot(N1, N1), s2 = dot(N2, N2), se = dot(e, e);
   // |N1|, |N2|, |e| < 1e-6 (degenerate hinge): no contribution
   const R eps2 = R(1.0e-12);
   if (s1 < eps2 || s2 < eps2 || se < eps2) return;
-  const R il1 = vrsqrt(s1), il2 = vrsqrt(s2), ile = vrsqrt(se);
-  // theta = atan2((n1 x n2) . e/|e|, n1 . n2), evaluated on the unnormalised normals: both arguments carry
-  // the common factor |N1| |N2| > 0, which atan2 ignores
-  const R theta = vatan2(dot(cross(N1, N2), e) * ile, dot(N1, N2));
+  const R ile = vrsqrt(se);
+  const R le = se * ile;  // |e|
+  // theta = atan2((n1 x n2) . e/|e|, n1 . n2) on the unnormalised normals (atan2 ignores their common factor
+  // |N1| |N2| > 0); N1 x N2 = (x02 . N2) e, so (N1 x N2) . e/|e| = (x02 . N2) |e|
+  const R theta = vatan2(dot(x02, N2) * le, dot(N1, N2));
   const R k = ke * rest_length;
   const R dE = k * (theta - rest_angle);
-  const R le = se * ile;  // |e|
-  // dtheta/dx_ord = alpha n1 + beta n2 = a N1 + b N2 with a = alpha / |N1|, b = beta / |N2|
-  const R q1 = il1 * il1, q2 = il2 * il2;
-  R a, b;
-  if (ord <= 1) {
-    a = ord == 0 ? -le * q1 : R(0);
-    b = ord == 1 ? -le * q2 : R(0);
-  } else {
-    const vec3<R> a1 = ord == 2 ? x03 : -x02;
-    const vec3<R> a2 = ord == 2 ? x13 : -x12;
-    a = dot(a1, e) * (ile * q1);
-    b = dot(a2, e) * (ile * q2);
-  }
+  // dtheta/dx_ord = a N1 + b N2. With u1 = x02 . e/|e| and u2 = x13 . e/|e| (x03 . e = x02 . e + |e|^2,
+  // x12 . e = x13 . e - |e|^2):  a |N1|^2 = -|e|, 0, u1 + |e|, -u1  and  b |N2|^2 = 0, -|e|, u2, |e| - u2  for
+  // ord = 0, 1, 2, 3: (c_a |e| + d u1) / |N1|^2 and (c_b |e| + d u2) / |N2|^2 with per-role constants, one
+  // instruction stream for every lane of a warp whatever the roles of their hinges
+  const R q1 = vrcp(s1), q2 = vrcp(s2);
+  const R u1 = dot(x02, e) * ile, u2 = dot(x13, e) * ile;
+  const R ca = ord == 0 ? R(-1) : (ord == 2 ? R(1) : R(0));
+  const R cb = ord == 1 ? R(-1) : (ord == 3 ? R(1) : R(0));
+  const R dd = ord == 2 ? R(1) : (ord == 3 ? R(-1) : R(0));
+  const R a = (ca * le + dd * u1) * q1;
+  const R b = (cb * le + dd * u2) * q2;
   const vec3<R> d = a * N1 + b * N2;
   f = f + (-dE) * d;
   R hk = k;
   if (kd > R(0)) {
+    const R il1 = vrsqrt(s1), il2 = vrsqrt(s2);
     const vec3<R> n1 = N1 * il1, n2 = N2 * il2, eh = e * ile;
+    const vec3<R> x03 = x02 + e, x12 = x13 - e;
     const vec3<R> d0 = (-le * il1) * n1, d1 = (-le * il2) * n2;
     const vec3<R> d2 = (dot(x03, eh) * il1) * n1 + (dot(x13, eh) * il2) * n2;
     const vec3<R> d3 = (-dot(x02, eh) * il1) * n1 - (dot(x12, eh) * il2) * n2;

@@ -76,6 +76,15 @@ __host__ __device__ __forceinline__ float vrsqrt(float x) {
 #endif
 }
 __host__ __device__ __forceinline__ double vrsqrt(double x) { return 1.0 / sqrt(x); }
+// reciprocal: the hardware approximation on the device for float (through the fast division), exact elsewhere
+__host__ __device__ __forceinline__ float vrcp(float x) {
+#ifdef __CUDA_ARCH__
+  return __fdividef(1.0f, x);
+#else
+  return 1.0f / x;
+#endif
+}
+__host__ __device__ __forceinline__ double vrcp(double x) { return 1.0 / x; }
 // a / b for material ratios: the fast (2 ulp) division on the device for float, exact elsewhere
 __host__ __device__ __forceinline__ float vdiv_fast(float a, float b) {
 #ifdef __CUDA_ARCH__
