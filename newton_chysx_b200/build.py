@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
-SOURCES = ["vbd_b200.cu", "vbd_soft.cu", "vbd_ell16_pair.cu", "vbd_ell16_damped.cu", "vbd_warp.cu", "vbd_noalloc.cu", "vbd_mesh.cu", "vbd_shapeset.cu", "vbd_diag.cu"]
+SOURCES = ["vbd_b200.cu", "vbd_soft.cu", "vbd_ell16_pair.cu", "vbd_ell16_damped.cu", "vbd_sc_persistent.cu", "vbd_warp.cu", "vbd_noalloc.cu", "vbd_mesh.cu", "vbd_shapeset.cu", "vbd_diag.cu"]
 OUT = os.path.join(HERE, "libvbd_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

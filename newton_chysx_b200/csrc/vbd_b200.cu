@@ -23,6 +23,7 @@
 #include "vbd_soft.h"
 #include "vbd_ell16_damped.h"
 #include "vbd_ell16_pair.h"
+#include "vbd_sc_persistent.h"
 #include "vbd_shapes.cuh"
 #include "vbd_warp.h"
 
@@ -234,6 +235,9 @@ struct VbdSolver {
   int sc_interval = 0;
   const float* sc_rest_q = nullptr;
   void *sc_pos_cd = nullptr, *sc_disp = nullptr, *sc_ts = nullptr;
+  // self-contact on the persistent schedule: per-instance edge ranges and the instance key of every vertex
+  int *sc_estart = nullptr, *sc_world = nullptr;
+  int grid_sc = 0;
 
   ~VbdSolver() {
     void* ps[] = {tri_idx, tri_pose, tri_mat, edge_idx, edge_prop, face_off, face_adj, edge_off, edge_adj,
@@ -242,7 +246,7 @@ struct VbdSolver {
                   range_ebase, face_nb, face_dm, face_mat, face_kd, hinge_idx, hinge_prop, hinge_kd, adj_work,
                   ell16_faceA, ell16_faceB, ell16_hinge, sc_pos_cd, sc_disp, sc_ts, ring_nslot, ring_base,
                   ring_vbase, ring_A, ring_B, ring_H, ring_hdr, ring_kd, spr_idx, spr_prop, spr_off, spr_adj, sspr_off,
-                  sspr_adj, spr_acc, tet_idx, tet_pose, tet_off, tet_adj};
+                  sspr_adj, spr_acc, tet_idx, tet_pose, tet_off, tet_adj, sc_estart, sc_world};
     for (void* p : ps)
       if (p) cudaFree(p);
     sc_release(sc);
@@ -972,6 +976,7 @@ int sc_detect(ScBuffers& b, const ScSetup& p, const int4* tri_idx, const int4* e
   q.bstart = b.bstart, q.ekey = b.ekey, q.eprim = b.eprim, q.stats = b.stats, q.flags = b.flags;
   q.gcap = (unsigned)std::min<long long>(b.gcap, 0xFFFFFFFFLL);
   q.tv = b.tb > 0 ? b.tv : nullptr, q.tv_count = b.tv_count, q.tv_min = b.tv_min, q.tb = b.tb;
+  q.world = b.world;
   pos4_t<R>* lo = (pos4_t<R>*)b.blo;
   pos4_t<R>* hi = (pos4_t<R>*)b.bhi;
   for (int kind = 0; kind < 2; ++kind) {
@@ -1147,7 +1152,45 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
   }
   const int iters = h->prm.iterations;
   if (MODE == MODE_MIXED) CK(cudaMemsetAsync(h->residual, 0, sizeof(double) * 32 * std::max(iters, 1), st));
-  if (h->schedule == VBD_SCHEDULE_PERSISTENT) {
+  if (h->sc_on && h->schedule == VBD_SCHEDULE_PERSISTENT) {
+    // self-contact, one instance per CTA: the detections stay grid-wide launches over all instances (pairs within
+    // an instance only); between them one persistent launch runs the forward step and its truncation, then one per
+    // detection interval runs the iterations, each color followed by the truncation of the instance's own pairs
+    c.disp = (pos4_t<R>*)h->sc_disp;
+    c.pos_cd = (pos4_t<R>*)h->sc_pos_cd;
+    c.ent_off = h->sc.ent_off;
+    c.ent = h->sc.ent;
+    c.vt_pairs = h->sc.vt_pairs;
+    c.ee_pairs = h->sc.ee_pairs;
+    c.sc_radius = h->sc_radius;
+    c.sc_ee_eps = h->sc_ee_eps;
+    c.dual_in_solve = 1;
+    int rc = sc_collide<R>(h, q_in, st);
+    if (rc) return rc;
+    if (has_c) {
+      CK(cudaMemsetAsync(h->slot_cnt, 0, sizeof(int) * h->V, st));
+      k_contact_prepare<R><<<(c.c_max + 255) / 256, 256, 0, st>>>(c);
+    }
+    PersistentPlan p{h->W, h->inst_order, h->inst_vstart, h->inst_cptr, h->color_ranges, h->color_verts, h->queue,
+                     iters};
+    ScPersistentPlan s{h->sc_estart, h->sc.vt_off, h->sc.ee_off, h->sc.vt_pairs, h->sc.ee_pairs, h->tri_idx,
+                       h->edge_idx, h->sc_ts, h->sc_ee_eps, h->sc_relax, h->sc_margin * h->sc_relax * 0.5,
+                       0, 0, 0, 0};
+    CK(cudaMemsetAsync(h->queue, 0, sizeof(int), st));
+    launch_persistent_sc<R, MODE>(h->L, c, p, s, h->grid_sc, h->block, st);
+    s.phase = 1;
+    int it = 0;
+    do {
+      // a detection at iteration `it` (interval 0: iteration 0 only; a negative interval: none)
+      if (iters > 0 && h->sc_interval >= 0 && (rc = sc_collide<R>(h, nullptr, st))) return rc;
+      const int it1 = h->sc_interval >= 1 ? std::min(iters, it + h->sc_interval) : iters;
+      s.it0 = it, s.it1 = it1, s.finalize = it1 == iters;
+      CK(cudaMemsetAsync(h->queue, 0, sizeof(int), st));
+      launch_persistent_sc<R, MODE>(h->L, c, p, s, h->grid_sc, h->block, st);
+      it = it1;
+    } while (it < iters);
+    CK(cudaGetLastError());
+  } else if (h->schedule == VBD_SCHEDULE_PERSISTENT) {
     CK(cudaMemsetAsync(h->queue, 0, sizeof(int), st));
     if (has_c) {
       CK(cudaMemsetAsync(h->slot_cnt, 0, sizeof(int) * h->V, st));
@@ -2149,7 +2192,10 @@ int vbd_set_self_contact(VbdHandle h, const VbdSelfContactDesc* d) {
       d->edge_buffer_size < 1 || !(d->edge_parallel_epsilon >= 0.0) || !(d->rest_exclusion_radius >= 0.0))
     return VBD_ERR_INVALID_ARGUMENT;
   if (d->rest_exclusion_radius > 0.0 && !d->rest_q_dev) return VBD_ERR_INVALID_ARGUMENT;
-  if (h->schedule != VBD_SCHEDULE_PER_COLOR || h->layout != VBD_LAYOUT_CSR) return VBD_ERR_UNSUPPORTED;
+  const bool persistent = h->schedule == VBD_SCHEDULE_PERSISTENT;
+  if ((h->schedule != VBD_SCHEDULE_PER_COLOR && !persistent) || h->layout != VBD_LAYOUT_CSR) return VBD_ERR_UNSUPPORTED;
+  // persistent: cloth only, the AVBD penalty fixed (its dual update would need a grid-wide pass per iteration)
+  if (persistent && (h->soft || h->warp_inst || h->prm.avbd_linear_beta != 0.f)) return VBD_ERR_UNSUPPORTED;
   const long long V = h->V, E = h->E;
   if (V * d->vertex_buffer_size >= (1LL << 29) || E * d->edge_buffer_size >= (1LL << 29) ||
       4 * V * d->vertex_buffer_size + 2 * E * d->edge_buffer_size >= (1LL << 31))
@@ -2185,6 +2231,34 @@ int vbd_set_self_contact(VbdHandle h, const VbdSelfContactDesc* d) {
   h->sc_rest_excl = d->rest_exclusion_radius;
   h->sc_interval = d->detection_interval;
   h->sc_rest_q = d->rest_q_dev;
+  for (int** p : {&h->sc_estart, &h->sc_world}) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
+  if (persistent) {
+    // the edges of an instance must be one contiguous range (add_world appends them world by world); pairs across
+    // instances are skipped by the detection (the instance key of a vertex is its instance's first particle)
+    std::vector<int> wstart(size_t(h->W) + 1);
+    CK(cudaMemcpy(wstart.data(), h->inst_vstart, sizeof(int) * wstart.size(), cudaMemcpyDeviceToHost));
+    std::vector<int> we(h->E), estart(size_t(h->W) + 1);
+    for (int e = 0; e < h->E; ++e) {
+      const int v0 = h->h_edges[4 * size_t(e) + 2];
+      we[e] = int(std::upper_bound(wstart.begin(), wstart.end(), v0) - wstart.begin()) - 1;
+      if (e > 0 && we[e] < we[e - 1]) return VBD_ERR_UNSUPPORTED;
+    }
+    for (int w = 0; w <= h->W; ++w) estart[w] = int(std::lower_bound(we.begin(), we.end(), w) - we.begin());
+    if ((rc = upload(&h->sc_estart, estart)) || (rc = upload(&h->sc_world, h->inst_start_of_vertex))) return rc;
+    h->sc.world = h->sc_world;
+    const void* fn = f64 ? persistent_sc_fn<double, MODE_FP64>(h->L)
+                         : (h->precision == VBD_PRECISION_MIXED ? persistent_sc_fn<float, MODE_MIXED>(h->L)
+                                                                : persistent_sc_fn<float, MODE_FP32>(h->L));
+    int dev = 0, sms = 0, per_sm = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, h->block, 0));
+    if (per_sm < 1) return VBD_ERR_INVALID_ARGUMENT;
+    h->grid_sc = std::min(h->W, sms * per_sm);
+  }
   h->sc_on = true;
   return VBD_OK;
 }

@@ -46,6 +46,7 @@ struct ScBuffers {
   int* ee_count = nullptr;       // [E]
   void* ee_min = nullptr;        // [E] R
   int* flags = nullptr;          // [4] overflow flags: 0 vertex, 1 triangle, 2 edge buffers; 3 internal (grid)
+  const int* world = nullptr;    // [V] instance key per vertex: pairs across instances are skipped; null = all kept
   int* tv = nullptr;             // caller's triangle -> colliding vertices buffers (stand-alone detector only)
   int* tv_count = nullptr;
   float* tv_min = nullptr;
@@ -116,7 +117,7 @@ __global__ void k_sc_boxes(int kind, int P, const pos4_t<R>* __restrict__ pos, c
   }
 }
 
-__global__ void k_sc_cell(double* stats, int P, double margin) {
+static __global__ void k_sc_cell(double* stats, int P, double margin) {
   const double mean = P > 0 ? stats[0] / P : 0.0;
   const double mx = __longlong_as_double((long long)*(unsigned long long*)(stats + 1));
   double c = fmax(2.0 * margin + mean, mx) * 1.01;
@@ -201,6 +202,7 @@ struct ScQuery {
   int* flags;
   unsigned gcap;  // grid entries written (bucket ranges are clamped to it)
   // triangle -> colliding vertices (the stand-alone detector's record_triangle_contacting_vertices); tv NULL = off
+  const int* world;  // [V] instance key per vertex (pairs across instances skipped), or null
   int* tv;         // [T, tb] vertex ids, kept increasing, INT_MAX past the stored ones during the query
   int* tv_count;   // [T] pairs found (may exceed tb)
   float* tv_min;   // [T] minimum distance, as float bits (distances are >= 0, so integer order is value order)
@@ -224,7 +226,7 @@ __device__ __forceinline__ void record_triangle_vertex(const ScQuery& s, int t, 
   atomicOr(s.flags + 1, 1);  // TRI_COLLISION_BUFFER_OVERFLOW_INDEX
 }
 
-__global__ void k_sc_tri_init(int T, int tb, int* tv, int* tv_count, float* tv_min, float radius) {
+static __global__ void k_sc_tri_init(int T, int tb, int* tv, int* tv_count, float* tv_min, float radius) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i < (long long)T * tb) tv[i] = INT_MAX;
   if (i < T) {
@@ -234,7 +236,7 @@ __global__ void k_sc_tri_init(int T, int tb, int* tv, int* tv_count, float* tv_m
 }
 
 // Slots past the stored vertices read -1.
-__global__ void k_sc_tri_finish(int T, int tb, int* tv) {
+static __global__ void k_sc_tri_finish(int T, int tb, int* tv) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i < (long long)T * tb && tv[i] == INT_MAX) tv[i] = -1;
 }
@@ -277,6 +279,7 @@ __global__ void k_sc_query_vt(ScQuery s, const pos4_t<R>* __restrict__ pos, cons
             continue;
           const int4 ti = __ldg(s.tri_idx + t);
           if (v == ti.x || v == ti.y || v == ti.z) continue;
+          if (s.world && __ldg(s.world + ti.x) != __ldg(s.world + v)) continue;
           if (sorted_contains(s.vt_foff, s.vt_f, v, t)) continue;
           R bary[3];
           const R dist = length(tri_closest(ld3<R>(pos[ti.x]), ld3<R>(pos[ti.y]), ld3<R>(pos[ti.z]), p, bary) - p);
@@ -334,6 +337,7 @@ __global__ void k_sc_query_ee(ScQuery s, const pos4_t<R>* __restrict__ pos, cons
             continue;
           const int4 fi = __ldg(s.edge_idx + f);
           if (ei.z == fi.z || ei.z == fi.w || ei.w == fi.z || ei.w == fi.w) continue;
+          if (s.world && __ldg(s.world + fi.z) != __ldg(s.world + ei.z)) continue;
           if (sorted_contains(s.ee_foff, s.ee_f, e, f)) continue;
           R ss, tt, dist;
           edge_closest(p0, p1, ld3<R>(pos[fi.z]), ld3<R>(pos[fi.w]), R(s.ee_eps), ss, tt, dist);
@@ -356,13 +360,13 @@ __global__ void k_sc_query_ee(ScQuery s, const pos4_t<R>* __restrict__ pos, cons
 }
 
 // tmp[i] = number of stored pairs of primitive i (tmp[P] = 0 for the scan)
-__global__ void k_sc_stored(int P, int cap, const int* __restrict__ count, int* tmp) {
+static __global__ void k_sc_stored(int P, int cap, const int* __restrict__ count, int* tmp) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < P) tmp[i] = min(count[i], cap);
   if (i == P) tmp[i] = 0;
 }
 
-__global__ void k_sc_pairs(int P, int cap, const int* __restrict__ count, const int* __restrict__ list,
+static __global__ void k_sc_pairs(int P, int cap, const int* __restrict__ count, const int* __restrict__ list,
                            const int* __restrict__ off, int2* pairs) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P) return;
@@ -405,7 +409,7 @@ __global__ void k_sc_entries(const int4* __restrict__ tri_idx, const int4* __res
   }
 }
 
-__global__ void k_sc_sort_entries(int V, const int* __restrict__ off, unsigned* ent) {
+static __global__ void k_sc_sort_entries(int V, const int* __restrict__ off, unsigned* ent) {
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= V) return;
   const int b = off[v], e = off[v + 1];
@@ -444,47 +448,41 @@ __device__ __forceinline__ void ts_min(double* ts, int i, double t) {
 
 // Step fractions of every recorded pair (apply_planar_truncation_parallel_by_collision): per vertex the
 // minimum over its pairs. All fractions lie in [0, 1], so the minimum of their bit patterns is theirs.
+// Division planes of one vertex-triangle (vt) or edge-edge pair and the step fractions of its vertices
+// (apply_planar_truncation_parallel_by_collision, particle_vbd_kernels.py:2744-2874): the per-vertex minimum is
+// kept with an integer atomicMin on the fraction's bits (fractions lie in [0, 1]).
 template <typename R>
-__global__ void k_sc_trunc_pairs(const int4* __restrict__ tri_idx, const int4* __restrict__ edge_idx,
-                                 const int* __restrict__ n_vt, const int* __restrict__ n_ee,
-                                 const int2* __restrict__ vt_pairs, const int2* __restrict__ ee_pairs,
-                                 const pos4_t<R>* __restrict__ pos_cd, const pos4_t<R>* __restrict__ disp, R eps, R gamma,
-                                 R* ts) {
-  const int nv = *n_vt, ne = *n_ee;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv + ne; i += gridDim.x * blockDim.x) {
-    int ids[4];
-    if (i < nv) {
-      const int2 pr = vt_pairs[i];
-      const int4 t = __ldg(tri_idx + pr.y);
-      ids[0] = pr.x, ids[1] = t.x, ids[2] = t.y, ids[3] = t.z;
-    } else {
-      const int2 pr = ee_pairs[i - nv];
-      const int4 a = __ldg(edge_idx + pr.x), b = __ldg(edge_idx + pr.y);
-      ids[0] = a.z, ids[1] = a.w, ids[2] = b.z, ids[3] = b.w;
-    }
-    vec3<R> x[4], dx[4], n, d;
-    bool cut[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) x[k] = ld3<R>(pos_cd[ids[k]]), dx[k] = ld3<R>(disp[ids[k]]);
-    if (i < nv)
-      vt_plane(x, dx, cut, n, d);
-    else
-      ee_plane(x, dx, cut, n, d);
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-      if (cut[k]) {
-        const R t = plane_t(x[k], dx[k], n, d, eps, gamma);
-        if (t < R(1)) ts_min(ts, ids[k], t);
-      }
+__device__ __forceinline__ void trunc_pair(bool vt, int2 pr, const int4* __restrict__ tri_idx,
+                                           const int4* __restrict__ edge_idx, const pos4_t<R>* __restrict__ pos_cd,
+                                           const pos4_t<R>* __restrict__ disp, R eps, R gamma, R* ts) {
+  int ids[4];
+  if (vt) {
+    const int4 t = __ldg(tri_idx + pr.y);
+    ids[0] = pr.x, ids[1] = t.x, ids[2] = t.y, ids[3] = t.z;
+  } else {
+    const int4 a = __ldg(edge_idx + pr.x), b = __ldg(edge_idx + pr.y);
+    ids[0] = a.z, ids[1] = a.w, ids[2] = b.z, ids[3] = b.w;
   }
+  vec3<R> x[4], dx[4], n, d;
+  bool cut[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) x[k] = ld3<R>(pos_cd[ids[k]]), dx[k] = ld3<R>(disp[ids[k]]);
+  if (vt)
+    vt_plane(x, dx, cut, n, d);
+  else
+    ee_plane(x, dx, cut, n, d);
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (cut[k]) {
+      const R t = plane_t(x[k], dx[k], n, d, eps, gamma);
+      if (t < R(1)) ts_min(ts, ids[k], t);
+    }
 }
 
 // disp *= t, |disp| <= max_d, q = q_cd + disp (apply_truncation_ts); resets t to 1 for the next pass.
 template <typename R>
-__global__ void k_sc_trunc_apply(int V, R* ts, R max_d, const pos4_t<R>* __restrict__ pos_cd, pos4_t<R>* disp,
-                                 pos4_t<R>* pos) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= V) return;
+__device__ __forceinline__ void trunc_vertex(int i, R* ts, R max_d, const pos4_t<R>* __restrict__ pos_cd,
+                                             pos4_t<R>* disp, pos4_t<R>* pos) {
   const R t = ts[i];
   ts[i] = R(1);
   vec3<R> d = ld3<R>(disp[i]) * t;
@@ -492,6 +490,24 @@ __global__ void k_sc_trunc_apply(int V, R* ts, R max_d, const pos4_t<R>* __restr
   if (len > max_d) d = {d.x * max_d / len, d.y * max_d / len, d.z * max_d / len};
   disp[i] = pk4(d, R(0));
   pos[i] = pk4(ld3<R>(pos_cd[i]) + d, R(0));
+}
+
+template <typename R>
+__global__ void k_sc_trunc_pairs(const int4* __restrict__ tri_idx, const int4* __restrict__ edge_idx,
+                                 const int* __restrict__ n_vt, const int* __restrict__ n_ee,
+                                 const int2* __restrict__ vt_pairs, const int2* __restrict__ ee_pairs,
+                                 const pos4_t<R>* __restrict__ pos_cd, const pos4_t<R>* __restrict__ disp, R eps, R gamma,
+                                 R* ts) {
+  const int nv = *n_vt, ne = *n_ee;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv + ne; i += gridDim.x * blockDim.x)
+    trunc_pair<R>(i < nv, i < nv ? vt_pairs[i] : ee_pairs[i - nv], tri_idx, edge_idx, pos_cd, disp, eps, gamma, ts);
+}
+
+template <typename R>
+__global__ void k_sc_trunc_apply(int V, R* ts, R max_d, const pos4_t<R>* __restrict__ pos_cd, pos4_t<R>* disp,
+                                 pos4_t<R>* pos) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < V) trunc_vertex<R>(i, ts, max_d, pos_cd, disp, pos);
 }
 
 template <typename R>

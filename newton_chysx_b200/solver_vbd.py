@@ -28,8 +28,11 @@ Beyond the reference keywords:
   ``__syncwarp`` instead of a CTA barrier), for batches of small instances such as soft-body blocks.
 
 Particle self-contact (``particle_enable_self_contact=True`` and the ``particle_self_contact_*``
-keywords) runs on the per-color schedule with the csr layout; see ``collision.py`` for the filters and
-the stand-alone detector.
+keywords) runs with the csr layout, on the per-color schedule for one cloth and on the persistent schedule
+(one CTA per world, the detections grid-wide between persistent launches) for a model of several worlds; on
+the persistent schedule a world's vertices and edges only meet its own triangles and edges, and the AVBD
+penalty ramp (``rigid_avbd_beta``) must be 0. See ``collision.py`` for the filters and the stand-alone
+detector.
 
 Arrays. The model, states and contacts may hold torch tensors (this package's ``sim``), the reference's Warp
 arrays, or any device array with ``__cuda_array_interface__``; each is checked for its element type, size and
@@ -130,9 +133,14 @@ class SolverVBD:
                     "particle_self_contact_margin is smaller than particle_self_contact_radius, this will result in "
                     "missing contacts and cause instability."
                 )
-            if schedule not in ("auto", "per_color") or layout not in ("auto", "csr"):
-                raise ValueError("particle self-contact runs on the per_color schedule with the csr layout")
-            schedule, layout = "per_color", "csr"
+            if layout not in ("auto", "csr") or schedule not in ("auto", "per_color", "persistent"):
+                raise ValueError("particle self-contact runs with the csr layout on the per_color or persistent schedule")
+            if schedule == "auto":
+                # several worlds: one CTA per world (pairs within a world); one cloth: per-color launches
+                soft = int(getattr(model, "spring_count", 0) or 0) + int(getattr(model, "tet_count", 0) or 0) > 0
+                worlds = interop.world_starts(model)
+                schedule = "persistent" if worlds is not None and linear_beta == 0.0 and not soft else "per_color"
+            layout = "csr"
             if lanes_per_vertex == 0:
                 # a vertex's self-contact entries (tens of edge-edge pairs) join its faces and hinges: 16 lanes
                 # per vertex measured fastest on a 256 x 256 sheet draped on a sphere (9.6 ms vs 21 ms per

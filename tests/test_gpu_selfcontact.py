@@ -15,7 +15,7 @@ import torch
 from newton_chysx_b200 import SolverVBD, sim
 from newton_chysx_b200.collision import TriMeshCollisionDetector, build_contact_filters
 from oracle import vbd_oracle as orc
-from tests.helpers import load_golden, model_from_golden, oracle_model_dict
+from tests.helpers import contacts_from_golden, load_golden, model_from_golden, oracle_model_dict
 
 pytestmark = pytest.mark.gpu
 
@@ -237,14 +237,20 @@ def test_selfcontact_graph_capture_and_determinism():
     assert torch.isfinite(a).all()
 
 
-def test_selfcontact_needs_per_color_csr():
+def test_selfcontact_launch_constraints():
+    """Self-contact runs with the csr layout; the persistent schedule needs a fixed AVBD penalty (rigid_avbd_beta
+    0); the margin may not be below the radius."""
+    from newton_chysx_b200 import _lib
+
     model, q, qd, kw = _layers_scene(8)
-    with pytest.raises(ValueError):
-        SolverVBD(model, schedule="persistent", **kw)
+    assert SolverVBD(model, **kw).schedule == "per_color"  # one world
+    assert SolverVBD(model, schedule="persistent", **kw).schedule == "persistent"
     with pytest.raises(ValueError):
         SolverVBD(model, layout="ell", **kw)
     with pytest.raises(ValueError):
         SolverVBD(model, **dict(kw, particle_self_contact_margin=1e-3))
+    with pytest.raises(_lib.VbdError, match="unsupported"):
+        SolverVBD(model, schedule="persistent", rigid_avbd_beta=1.0e3, **kw)
 
 
 def _point_triangle_distance(p, a, b, c):
@@ -353,3 +359,139 @@ def test_detector_triangle_buffers_match_brute_force(tb):
     assert len(pairs) > model.particle_count // 4
     overflow = _check_triangle_side(det, model.tri_indices.cpu().numpy(), q, pairs, model.tri_count, tb, margin)
     assert overflow == (tb == 2)
+
+
+def _two_worlds(g, offset=(4.0, 0.0, 0.0)):
+    """The golden scene twice, as worlds 0 and 1 of one model, the second moved by `offset` (far beyond the contact
+    margin, so the worlds never touch): the reference's add_world union with each world its own instance."""
+    m = model_from_golden(g)
+    V = m.particle_count
+    off = torch.tensor(offset, dtype=torch.float32, device="cuda")
+    cat = torch.cat
+    m.particle_q = cat([m.particle_q, m.particle_q + off])
+    m.particle_qd = cat([m.particle_qd, m.particle_qd])
+    for k in ("particle_mass", "particle_inv_mass", "particle_radius", "particle_flags", "tri_poses", "tri_materials",
+              "tri_areas", "edge_rest_angle", "edge_rest_length", "edge_bending_properties"):  # fmt: skip
+        setattr(m, k, cat([getattr(m, k), getattr(m, k)]))
+    m.tri_indices = cat([m.tri_indices, m.tri_indices + V])
+    e2 = m.edge_indices.clone()
+    e2[e2 >= 0] += V
+    m.edge_indices = cat([m.edge_indices, e2])
+    m.particle_color_groups = [cat([c, c + V]) for c in m.particle_color_groups]
+    m.particle_colors = cat([m.particle_colors, m.particle_colors])
+    m.particle_count, m.tri_count, m.edge_count = 2 * V, 2 * m.tri_count, 2 * m.edge_count
+    m.world_count = 2
+    m.world_particle_start = np.array([0, V, 2 * V], dtype=np.int32)
+    return m, V, np.asarray(offset)
+
+
+def _two_world_inputs(g, s, V, offset, dtype=np.float64):
+    q = np.concatenate([g[f"s{s}_q_in"], g[f"s{s}_q_in"] + offset]).astype(dtype)
+    qd = np.concatenate([g[f"s{s}_qd_in"], g[f"s{s}_qd_in"]]).astype(dtype)
+    f = np.concatenate([g[f"s{s}_f_ext"], g[f"s{s}_f_ext"]]).astype(dtype)
+    c1 = contacts_from_golden(g, s)
+    n = int(c1.soft_contact_count.item())
+    c = sim.Contacts(2 * max(c1.soft_contact_max, 1), "cuda")
+    c.soft_contact_count.fill_(2 * n)
+    for name in ("soft_contact_shape", "soft_contact_body_pos", "soft_contact_body_vel", "soft_contact_normal"):
+        a = getattr(c1, name)[:n]
+        getattr(c, name)[: 2 * n] = torch.cat([a, a])
+    p = c1.soft_contact_particle[:n]
+    c.soft_contact_particle[: 2 * n] = torch.cat([p, p + V])
+    return q, qd, f, c
+
+
+@pytest.mark.parametrize("name", SCENES)
+def test_persistent_self_contact_two_worlds_match_reference_goldens(name):
+    """Self-contact on a model of two worlds runs one world per CTA (persistent schedule, the detection keeping
+    pairs within a world): each world follows the reference's goldens of its scene, within 1e-4 m per substep."""
+    g = load_golden(name)
+    model, V, offset = _two_worlds(g)
+    solver = _solver(g, model)
+    assert solver.schedule == "persistent" and solver.layout == "csr"
+    for s in range(int(g["substeps"])):
+        q, qd, f, c = _two_world_inputs(g, s, V, offset)
+        st_in, st_out = sim.State(), sim.State()
+        st_in.particle_q, st_in.particle_qd, st_in.particle_f = _t(q), _t(qd), _t(f)
+        st_out.particle_q = torch.zeros_like(st_in.particle_q)
+        st_out.particle_qd = torch.zeros_like(st_in.particle_qd)
+        solver.step(st_in, st_out, None, c if model.shape_count else None, float(g["dt"]))
+        torch.cuda.synchronize()
+        out = st_out.particle_q.cpu().numpy().astype(np.float64)
+        ref = g[f"s{s}_q_out"]
+        assert np.abs(out[:V] - ref).max() <= 1e-4, (name, s)
+        assert np.abs(out[V:] - offset - ref).max() <= 1e-4, (name, s)
+        qd_out = st_out.particle_qd.cpu().numpy()
+        assert np.abs(qd_out[:V] - g[f"s{s}_qd_out"]).max() <= 1e-4 / float(g["dt"])
+    nv, ne, flags = solver.self_contact_counts()
+    assert nv + ne > 0 and flags == 0
+    assert solver.device_errors() & ~4 == 0
+
+
+@pytest.mark.parametrize("name", SCENES)
+def test_persistent_self_contact_fp64_matches_per_color_fp64(name):
+    """FP64: the persistent schedule on two worlds against the per-color schedule on the same model, which the tests
+    above hold to the FP64 oracle; the worlds are apart, so both find the same pairs."""
+    g = load_golden(name)
+    model, V, offset = _two_worlds(g)
+    outs = []
+    for schedule in ("persistent", "per_color"):
+        solver = _solver(g, model, schedule=schedule, precision="fp64")
+        assert solver.schedule == schedule
+        res = []
+        for s in range(int(g["substeps"])):
+            q, qd, f, c = _two_world_inputs(g, s, V, offset)
+            st_in, st_out = _step_with(solver, q, qd, f, c if model.shape_count else None, float(g["dt"]))
+            res.append(st_out.particle_q.cpu().numpy())
+        outs.append(res)
+    for a, b in zip(*outs, strict=True):
+        assert np.abs(a - b).max() <= 1e-9
+
+
+def _step_with(solver, q, qd, f, contacts, dt):
+    st_in, st_out = sim.State(), sim.State()
+    st_in.particle_q, st_in.particle_qd, st_in.particle_f = (_t(a, torch.float64) for a in (q, qd, f))
+    st_out.particle_q = torch.zeros_like(st_in.particle_q)
+    st_out.particle_qd = torch.zeros_like(st_in.particle_qd)
+    solver.step(st_in, st_out, None, contacts, dt)
+    torch.cuda.synchronize()
+    return st_in, st_out
+
+
+def test_persistent_self_contact_batch_matches_per_color():
+    """Four crumpled two-layer sheets of different sizes as worlds, detection every second iteration: each substep of
+    the persistent schedule (pairs within a world) against the per-color schedule (all pairs; the worlds are apart,
+    so the same ones) from the same input state, FP32. The two kernels compile the same solve separately, so their
+    multiply-adds may fuse differently: 1e-5 m, rounding level for contact-driven steps of these sheets."""
+    b = sim.ModelBuilder(up_axis="Z", gravity=-9.81)
+    rng = np.random.default_rng(11)
+    for k, n in enumerate((12, 20, 9, 16)):
+        w = sim.ModelBuilder(up_axis="Z", gravity=-9.81)
+        for layer in range(2):
+            rot = sim.quat_from_axis_angle((0.0, 0.0, 1.0), 0.3 * layer)
+            w.add_cloth_grid(pos=(3.0 * k - 0.5, -0.5, 0.004 * layer), rot=rot, vel=(0.0, 0.0, -0.5 * layer),
+                             dim_x=n - 1, dim_y=n - 1, cell_x=1.0 / (n - 1), cell_y=1.0 / (n - 1), mass=2e-4,
+                             tri_ke=5.0, tri_ka=5.0, tri_kd=0.0, edge_ke=1e-4, edge_kd=0.0, particle_radius=2e-3)  # fmt: skip
+        w.color(include_bending=True)
+        b.add_world(w)
+    model = b.finalize("cuda")
+    q0 = model.particle_q.cpu().numpy() + rng.normal(scale=1.0e-3, size=(model.particle_count, 3))
+    kw = dict(particle_enable_self_contact=True, particle_self_contact_radius=2e-3, particle_self_contact_margin=3.5e-3,
+              particle_collision_detection_interval=2)  # fmt: skip
+    pers = SolverVBD(model, iterations=6, schedule="persistent", **kw)
+    ref = SolverVBD(model, iterations=6, schedule="per_color", **kw)
+    s0, s1, t0, t1 = model.state(), model.state(), model.state(), model.state()
+    s0.particle_q.copy_(torch.as_tensor(q0, dtype=torch.float32))
+    worst, pairs = 0.0, 0
+    for _ in range(6):
+        t0.particle_q.copy_(s0.particle_q)
+        t0.particle_qd.copy_(s0.particle_qd)
+        pers.step(t0, t1, None, None, 1.0 / 600.0)
+        ref.step(s0, s1, None, None, 1.0 / 600.0)
+        torch.cuda.synchronize()
+        assert pers.self_contact_counts()[:2] == ref.self_contact_counts()[:2]
+        pairs += sum(ref.self_contact_counts()[:2])
+        worst = max(worst, (t1.particle_q - s1.particle_q).abs().max().item())
+        s0, s1 = s1, s0
+    assert pairs > 0 and torch.isfinite(s0.particle_q).all()
+    assert worst <= 1e-5, worst
