@@ -58,14 +58,17 @@ __host__ __device__ __forceinline__ void membrane_add(int ord, vec3<R> x0, vec3<
   // coefficients instead of the vectors g0, g1
   const R e0 = invJ * (f11 * d0 - f01 * d1), e1 = invJ * (f00 * d1 - f01 * d0);
   const vec3<R> dJ = e0 * f0 + e1 * f1;
-  const R c0 = mu * d0 + s * e0, c1 = mu * d1 + s * e1;
-  vec3<R> force = -(c0 * f0 + c1 * f1);
+  // the terms go straight into (f, H), scaled by the area through their scalar coefficients
+  const R c0 = area * (mu * d0 + s * e0), c1 = area * (mu * d1 + s * e1);
+  f = f - c0 * f0 - c1 * f1;
   const R r = vmax(R(0), s) * invJ;
   const vec3<R> w = f1 * d0 - f0 * d1;
-  const R Ic = mu * (d0 * d0 + d1 * d1) + r * (d0 * d0 * f11 + d1 * d1 * f00 - R(2) * d0 * d1 * f01);
-  sym3<R> h = sdiag(Ic);
-  souter_add(h, dJ, lnh - r);
-  souter_add(h, w, -r);
+  const R Ic = area * (mu * (d0 * d0 + d1 * d1) + r * (d0 * d0 * f11 + d1 * d1 * f00 - R(2) * d0 * d1 * f01));
+  H.xx += Ic;
+  H.yy += Ic;
+  H.zz += Ic;
+  souter_add(H, dJ, area * (lnh - r));
+  souter_add(H, w, -(area * r));
   if (damping > R(0)) {
     const R G00 = R(0.5) * (f00 - R(1)), G11 = R(0.5) * (f11 - R(1)), G01 = R(0.5) * f01;
     const R Gsq = G00 * G00 + G11 * G11 + R(2) * G01 * G01;
@@ -78,26 +81,25 @@ __host__ __device__ __forceinline__ void membrane_add(int ord, vec3<R> x0, vec3<
       const R dG00 = dot(f0, df0), dG11 = dot(f1, df1), dG01 = R(0.5) * (dot(f0, df1) + dot(f1, df0));
       const R dC = n00 * dG00 + n11 * dG11 + R(2) * n01 * dG01;
       const vec3<R> dCdx = d0 * (n00 * f0 + n01 * f1) + d1 * (n01 * f0 + n11 * f1);
-      const R kmu = mu * damping;
-      force = force + (-kmu * dC) * dCdx;
-      souter_add(h, dCdx, kmu * inv_dt);
+      const R kmu = area * mu * damping;
+      f = f + (-kmu * dC) * dCdx;
+      souter_add(H, dCdx, kmu * inv_dt);
       const R dCl = dG00 + dG11;
       const vec3<R> dCldx = d0 * f0 + d1 * f1;
-      const R kl = lmbd * damping;
-      force = force + (-kl * dCl) * dCldx;
-      souter_add(h, dCldx, kl * inv_dt);
+      const R kl = area * lmbd * damping;
+      f = f + (-kl * dCl) * dCldx;
+      souter_add(H, dCldx, kl * inv_dt);
     }
   }
-  f = f + force * area;
-  H = H + area * h;
 }
 
 // Dihedral bending contribution of hinge (x0 opposite-0, x1 opposite-1, x2-x3 the shared edge) for
 // the vertex of order `ord` (0..3). prop = (rest_angle, rest_length, ke, kd). xp = previous positions
 // of the four vertices, read only when kd > 0.
 template <typename R>
-__host__ __device__ __forceinline__ void bending_add(int ord, const vec3<R> x[4], R rest_angle, R rest_length, R ke,
-                                                     R kd, R dt, const vec3<R>* xp, vec3<R>& f, sym3<R>& H) {
+__host__ __device__ __forceinline__ void bending_add_coef(R ca, R cb, R dd, const vec3<R> x[4], R rest_angle,
+                                                          R rest_length, R ke, R kd, R dt, const vec3<R>* xp,
+                                                          vec3<R>& f, sym3<R>& H) {
   // with x03 = x02 + e and x12 = x13 - e: N1 = x02 x x03 = x02 x e, N2 = x13 x x12 = e x x13
   const vec3<R> x02 = x[2] - x[0], x13 = x[3] - x[1], e = x[3] - x[2];
   const vec3<R> N1 = cross(x02, e), N2 = cross(e, x13);
@@ -118,9 +120,6 @@ __host__ __device__ __forceinline__ void bending_add(int ord, const vec3<R> x[4]
   // instruction stream for every lane of a warp whatever the roles of their hinges
   const R q1 = vrcp(s1), q2 = vrcp(s2);
   const R u1 = dot(x02, e) * ile, u2 = dot(x13, e) * ile;
-  const R ca = ord == 0 ? R(-1) : (ord == 2 ? R(1) : R(0));
-  const R cb = ord == 1 ? R(-1) : (ord == 3 ? R(1) : R(0));
-  const R dd = ord == 2 ? R(1) : (ord == 3 ? R(-1) : R(0));
   const R a = (ca * le + dd * u1) * q1;
   const R b = (cb * le + dd * u2) * q2;
   const vec3<R> d = a * N1 + b * N2;
@@ -141,6 +140,16 @@ __host__ __device__ __forceinline__ void bending_add(int ord, const vec3<R> x[4]
     hk = k + dc * inv_dt;
   }
   souter_add(H, d, hk);
+}
+
+// The per-role constants of bending_add_coef for the vertex of order `ord`.
+template <typename R>
+__host__ __device__ __forceinline__ void bending_add(int ord, const vec3<R> x[4], R rest_angle, R rest_length, R ke,
+                                                     R kd, R dt, const vec3<R>* xp, vec3<R>& f, sym3<R>& H) {
+  const R ca = ord == 0 ? R(-1) : (ord == 2 ? R(1) : R(0));
+  const R cb = ord == 1 ? R(-1) : (ord == 3 ? R(1) : R(0));
+  const R dd = ord == 2 ? R(1) : (ord == 3 ? R(-1) : R(0));
+  bending_add_coef<R>(ca, cb, dd, x, rest_angle, rest_length, ke, kd, dt, xp, f, H);
 }
 
 // Penalty contact with a static or moving shape point. pen > 0 is the penetration depth, n the unit

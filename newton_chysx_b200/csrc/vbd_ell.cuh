@@ -309,7 +309,11 @@ __device__ __forceinline__ void ell16_hinge(const StepCtx<R>& c, const P& pos, i
   const float k = __uint_as_float(hh.w);
   if (!(k > 0.f)) return;
   const int i0 = int(hh.x & 0xffffu), i1 = int(hh.x >> 16), i2 = int(hh.y & 0xffffu), i3 = int(hh.y >> 16);
-  const int role = i0 == lv ? 0 : (i1 == lv ? 1 : (i2 == lv ? 2 : 3));
+  // the solved vertex's role is where its id appears; the role constants of bending_add_coef straight from it
+  const bool r0 = i0 == lv, r1 = i1 == lv, r2 = i2 == lv, r3 = !(r0 || r1 || r2);
+  const R ca = r0 ? R(-1) : (r2 ? R(1) : R(0));
+  const R cb = r1 ? R(-1) : (r3 ? R(1) : R(0));
+  const R dd = r2 ? R(1) : (r3 ? R(-1) : R(0));
   vec3<R> xs[4];
   xs[0] = pos.ld(vs + i0);
   xs[1] = pos.ld(vs + i1);
@@ -322,11 +326,11 @@ __device__ __forceinline__ void ell16_hinge(const StepCtx<R>& c, const P& pos, i
       xp[1] = ld3<R>(c.qprev[vs + i1]);
       xp[2] = ld3<R>(c.qprev[vs + i2]);
       xp[3] = ld3<R>(c.qprev[vs + i3]);
-      bending_add<R>(role, xs, R(__uint_as_float(hh.z)), R(1), R(k), R(kd), c.dt, xp, f, H);
+      bending_add_coef<R>(ca, cb, dd, xs, R(__uint_as_float(hh.z)), R(1), R(k), R(kd), c.dt, xp, f, H);
       return;
     }
   }
-  bending_add<R>(role, xs, R(__uint_as_float(hh.z)), R(1), R(k), R(0), c.dt, nullptr, f, H);
+  bending_add_coef<R>(ca, cb, dd, xs, R(__uint_as_float(hh.z)), R(1), R(k), R(0), c.dt, nullptr, f, H);
 }
 
 template <typename R, int MODE, bool HD, typename P>

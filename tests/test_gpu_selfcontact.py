@@ -461,8 +461,9 @@ def _step_with(solver, q, qd, f, contacts, dt):
 def test_persistent_self_contact_batch_matches_per_color():
     """Four crumpled two-layer sheets of different sizes as worlds, detection every second iteration: each substep of
     the persistent schedule (pairs within a world) against the per-color schedule (all pairs; the worlds are apart,
-    so the same ones) from the same input state, FP32. The two kernels compile the same solve separately, so their
-    multiply-adds may fuse differently: 1e-5 m, rounding level for contact-driven steps of these sheets."""
+    so the same ones) from the same input state, FP32, within the 1e-4 m of the FP32 parity tests: the two kernels
+    compile the same solve separately, so their multiply-adds may fuse differently, and the barrier-driven contact
+    solves of these sheets amplify that rounding to ~1e-5 m (the FP64 versions agree to 1e-9 m, above)."""
     b = sim.ModelBuilder(up_axis="Z", gravity=-9.81)
     rng = np.random.default_rng(11)
     for k, n in enumerate((12, 20, 9, 16)):
@@ -494,4 +495,4 @@ def test_persistent_self_contact_batch_matches_per_color():
         worst = max(worst, (t1.particle_q - s1.particle_q).abs().max().item())
         s0, s1 = s1, s0
     assert pairs > 0 and torch.isfinite(s0.particle_q).all()
-    assert worst <= 1e-5, worst
+    assert worst <= 1e-4, worst
