@@ -205,8 +205,7 @@ __device__ __forceinline__ void finalize_particle(const StepCtx<R>& c, const P& 
 
 // contact terms of one particle (lane 0 of the group)
 template <typename R>
-__device__ __forceinline__ void contacts_add(const StepCtx<R>& c, int v, vec3<R> x, vec3<R>& f, sym3<R>& H) {
-  int n = c.slot_cnt[v];
+__device__ __forceinline__ void contacts_add_n(const StepCtx<R>& c, int v, int n, vec3<R> x, vec3<R>& f, sym3<R>& H) {
   if (n <= 0) return;
   if (n > c.K) n = c.K;
   int ids[8];
@@ -260,6 +259,12 @@ __device__ __forceinline__ void contacts_add(const StepCtx<R>& c, int v, vec3<R>
       contact_add<R>(pen, nn, rel, k, R(c.c_kd[t]), R(c.c_mu[t]), c.fric_eps, c.dt, f, H);
     }
   }
+}
+
+// contacts_add_n with the particle's contact count read here
+template <typename R>
+__device__ __forceinline__ void contacts_add(const StepCtx<R>& c, int v, vec3<R> x, vec3<R>& f, sym3<R>& H) {
+  contacts_add_n<R>(c, v, c.slot_cnt[v], x, f, H);
 }
 
 // ---------------------------------------------------------------------------------------------
