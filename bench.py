@@ -43,7 +43,7 @@ DT = 1.0 / 600.0
 # DRAM bytes (read + write) per vertex-iteration of the solve kernel, from one ncu capture per layout of the
 # first 512 instances of this workload; the traffic of a full launch scales with its vertex-iterations.
 NCU_TRAFFIC_PER_VI = {
-    "ell16": (513.0, "ncu capture of the first 512 instances of this batch, scaled by vertex-iterations"),
+    "ell16": (508.0, "ncu capture of the first 512 instances of this batch, scaled by vertex-iterations"),
 }
 
 
