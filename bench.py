@@ -741,6 +741,37 @@ SC_KW = dict(particle_enable_self_contact=True, particle_self_contact_radius=2e-
              particle_collision_detection_interval=0, particle_topological_contact_filter_threshold=2)  # fmt: skip
 
 
+def time_selfcontact_substeps(solver, pipe, contacts, s0, s1, q_settled, qd_settled, K):
+    """ms per substep (collision generation + step) from the settled state, K substeps replayed from a CUDA graph
+    of two substeps (a ping-pong pair), timed with CUDA events."""
+    import torch
+
+    s0.particle_q.copy_(q_settled)
+    s0.particle_qd.copy_(qd_settled)
+    pipe.collide(s0, contacts)  # one eager substep first: a solver sizes its contact buffers outside the capture
+    solver.step(s0, s1, None, contacts, DT)
+    graph = torch.cuda.CUDAGraph()
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(stream), torch.cuda.graph(graph, stream=stream):
+        pipe.collide(s0, contacts)
+        solver.step(s0, s1, None, contacts, DT)
+        pipe.collide(s1, contacts)
+        solver.step(s1, s0, None, contacts, DT)
+    torch.cuda.current_stream().wait_stream(stream)
+    s0.particle_q.copy_(q_settled)
+    s0.particle_qd.copy_(qd_settled)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(K // 2):
+        graph.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    del graph
+    return e0.elapsed_time(e1) / K
+
+
 def run_selfcontact(args):
     """Config of the plain drop-in at scale: one 256 x 256 cloth (65,536 vertices, 130,050 triangles)
     dropped onto a sphere with vertex-triangle and edge-edge self-contact, 20 iterations per substep,
@@ -766,29 +797,9 @@ def run_selfcontact(args):
     torch.cuda.synchronize()
     settle_s = time.perf_counter() - t0
     q_settled, qd_settled = s0.particle_q.clone(), s0.particle_qd.clone()
-    # one substep (ping-pong pair) per graph replay
-    graph = torch.cuda.CUDAGraph()
-    stream = torch.cuda.Stream()
-    stream.wait_stream(torch.cuda.current_stream())
-    with torch.cuda.stream(stream), torch.cuda.graph(graph, stream=stream):
-        pipe.collide(s0, contacts)
-        solver.step(s0, s1, None, contacts, DT)
-        pipe.collide(s1, contacts)
-        solver.step(s1, s0, None, contacts, DT)
-    torch.cuda.current_stream().wait_stream(stream)
-    s0.particle_q.copy_(q_settled)
-    s0.particle_qd.copy_(qd_settled)
-    pairs = []
     K = max(2, args.steps + (args.steps % 2))
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
     with ClockSampler(dev.index or 0) as clk:
-        e0.record()
-        for _ in range(K // 2):
-            graph.replay()
-        e1.record()
-        torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / K
+        ms = time_selfcontact_substeps(solver, pipe, contacts, s0, s1, q_settled, qd_settled, K)
     pairs = solver.self_contact_counts()
     V = m.particle_count
     value = V * SC_ITERATIONS / (ms * 1e-3)
@@ -812,6 +823,7 @@ def run_selfcontact(args):
         hq = q_settled.cpu().pin_memory()
         hqd = qd_settled.cpu().pin_memory()
         out_q = torch.empty_like(hq).pin_memory()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record()
         for _ in range(K):
@@ -825,13 +837,121 @@ def run_selfcontact(args):
         ms_e = e0.elapsed_time(e1) / K
         out["e2e"] = {"value": V * SC_ITERATIONS / (ms_e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 2 * hq.numel() * 4,
                       "d2h_bytes_per_step": out_q.numel() * 4, "steps": K}  # fmt: skip
+    # the mixed mode (FP64 contact terms and block solve on contact vertices) timed the same way
+    mixed = nb.SolverVBD(m, iterations=SC_ITERATIONS, precision="mixed", lanes_per_vertex=args.lanes, **SC_KW)
+    ms_mixed = time_selfcontact_substeps(mixed, pipe, contacts, s0, s1, q_settled, qd_settled, K)
+    out["mixed"] = {"value": V * SC_ITERATIONS / (ms_mixed * 1e-3), "unit": UNIT, "ms_per_step": ms_mixed,
+                    "device_errors": mixed.device_errors()}  # fmt: skip
+    if not args.no_pos_err:
+        out["pos_err"], out["pos_err_detail"] = selfcontact_position_error(args, m, solver, mixed, pipe, q_settled,
+                                                                           qd_settled)  # fmt: skip
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_selfcontact(m, q_settled.cpu().numpy(), qd_settled.cpu().numpy())
+        if not args.no_pos_err:
+            ora = out["cpu_baseline"].pop("fp64_step_q")
+            q32 = out["pos_err_detail"].pop("first_fp32_q")
+            d = float(np.linalg.norm(q32 - ora, axis=1).max())
+            out["pos_err_detail"]["vs_fp64_oracle_first_substep"] = d
+            out["pos_err"] = max(out["pos_err"], d)
+            out["pos_err_detail"]["within_bound"] = bool(out["pos_err"] <= 1e-4)
+    if "pos_err_detail" in out:
+        out["pos_err_detail"].pop("first_fp32_q", None)
     return out
 
 
-def cpu_baseline_selfcontact(m, q, qd):
-    """The oracle (FP32, all host threads, box-grid detection) on one substep of the same settled state."""
+def selfcontact_position_error(args, m, solver, mixed, pipe, q_settled, qd_settled):
+    """Position error against FP64 on the settled, draped sheet with self-contact, as max over vertices of
+    |x - x_fp64|_2 / L (L = 1 m), with the number of vertices past 1e-4 m:
+    * per substep: each of --err-substeps FP32 substeps (collide + step, the timed calls) beside an FP64 substep
+      (precision="fp64", the same step in double precision) from the same FP32 input with contacts from the same
+      positions, and the mixed mode's substep from that input;
+    * trajectory: FP32 and FP64 from the settled state for the same substeps;
+    * floor: the FP64 step from the first input moved by Gaussian noise of 1e-8 m (below FP32 rounding of the
+      positions) against the FP64 step from that input. The step is discontinuous where a contact's normal
+      velocity is near zero: the damping stiffness kd ke / dt switches on and off with its sign, so any two
+      arithmetics part by this much there."""
+    import torch
+
+    import newton_chysx_b200 as nb
+
+    t0 = time.time()
+    s64 = nb.SolverVBD(m, iterations=SC_ITERATIONS, precision="fp64", lanes_per_vertex=args.lanes, **SC_KW)
+    c32, c64 = pipe.contacts(), pipe.contacts()
+    a32, b32, bmx = m.state(), m.state(), m.state()
+    a64, b64, t64a, t64b = m.state(), m.state(), m.state(), m.state()
+    for s in (a64, b64, t64a, t64b):
+        s.particle_q, s.particle_qd, s.particle_f = (t.double() for t in (s.particle_q, s.particle_qd, s.particle_f))
+    a32.particle_q.copy_(q_settled)
+    a32.particle_qd.copy_(qd_settled)
+    t64a.particle_q.copy_(q_settled.double())
+    t64a.particle_qd.copy_(qd_settled.double())
+
+    def f32_view(s):
+        v = type(s)()
+        v.particle_q = s.particle_q.float()
+        return v
+
+    def dist(a, b):
+        return torch.linalg.norm(a.double() - b.double(), dim=1)
+
+    def stat(d):
+        return {"max": float(d.max()), "above_1e-4": int((d > 1e-4).sum()), "above_1e-5": int((d > 1e-5).sum())}
+
+    per32, permx, traj, first, first_stats = [], [], [], None, {}
+    amx = m.state()
+    for k in range(max(1, args.err_substeps)):
+        # a step writes its result into its input state too (the reference's side effect): every solver starts
+        # from its own copy of the input
+        qin, qdin = a32.particle_q.clone(), a32.particle_qd.clone()
+        pipe.collide(a32, c32)
+        amx.particle_q.copy_(qin)
+        amx.particle_qd.copy_(qdin)
+        mixed.step(amx, bmx, None, c32, DT)
+        solver.step(a32, b32, None, c32, DT)
+        a64.particle_q.copy_(qin.double())
+        a64.particle_qd.copy_(qdin.double())
+        pipe.collide(f32_view(a64), c64)
+        s64.step(a64, b64, None, c64, DT)
+        pipe.collide(f32_view(t64a), c64)
+        s64.step(t64a, t64b, None, c64, DT)
+        torch.cuda.synchronize()
+        d32, dmx = dist(b32.particle_q, b64.particle_q), dist(bmx.particle_q, b64.particle_q)
+        if first is None:
+            first = b32.particle_q.cpu().numpy().astype(np.float64)
+            first_stats = {"fp32": stat(d32), "mixed": stat(dmx)}
+            gen = torch.Generator(device=qin.device).manual_seed(7)
+            fl = (m.particle_flags & 1).bool()
+            noise = torch.randn(qin.shape, generator=gen, device=qin.device, dtype=torch.float64)
+            p64, q64 = m.state(), m.state()
+            for s in (p64, q64):
+                s.particle_q, s.particle_qd, s.particle_f = (t.double() for t in (s.particle_q, s.particle_qd,
+                                                                                  s.particle_f))  # fmt: skip
+            p64.particle_q.copy_(qin.double() + 1e-8 * noise * fl[:, None])
+            p64.particle_qd.copy_(qdin.double())
+            s64.step(p64, q64, None, c64, DT)  # contacts of the unperturbed FP32 positions
+            torch.cuda.synchronize()
+            first_stats["fp64_floor"] = stat(dist(q64.particle_q, b64.particle_q))
+        per32.append(float(d32.max()))
+        permx.append(float(dmx.max()))
+        traj.append(float(dist(b32.particle_q, t64b.particle_q).max()))
+        a32, b32 = b32, a32
+        t64a, t64b = t64b, t64a
+    worst = max(per32)
+    counts = s64.self_contact_counts()
+    return worst, {"value": worst, "unit": "m per m of cloth side (max vertex |x32 - x64|_2 / L, L = 1 m)",
+                   "bound": 1e-4, "within_bound": bool(worst <= 1e-4), "per_substep": per32,
+                   "per_substep_mixed": permx, "first_substep": first_stats, "trajectory": traj,
+                   "after_settled_substeps": args.sc_settle_frames * 10 + args.warmup,
+                   "fp64_self_contact_pairs": {"vertex_triangle": counts[0], "edge_edge": counts[1]},
+                   "reference": "precision='fp64' (the same step in FP64, held to the FP64 oracle at 1e-9 m by the "
+                                "tests); with the CPU baseline on, also the FP64 oracle's own substep from the "
+                                "settled state",
+                   "first_fp32_q": first, "s": round(time.time() - t0, 1)}  # fmt: skip
+
+
+def cpu_baseline_selfcontact(m, q, qd, fp64_step=True):
+    """The oracle (FP32, all host threads, box-grid detection) on one substep of the same settled state; with
+    fp64_step, also the FP64 oracle's substep from that state (untimed), returned as fp64_step_q."""
     from newton_chysx_b200.collision import build_contact_filters
     from oracle import vbd_oracle as orc
     from tests.helpers import oracle_model_dict
@@ -846,11 +966,17 @@ def cpu_baseline_selfcontact(m, q, qd):
     cnt, p, s, bp, bv, nn = orc.soft_contacts_shapes(q, m.particle_radius.cpu().numpy(),
                                                      m.particle_flags.cpu().numpy(), m.shape_type, m.shape_transform,
                                                      m.shape_scale, 0.01)  # fmt: skip
-    orc.step(om, q, qd.astype(np.float64), None, orc.make_contacts(cnt, p, s, bp, bv, nn), DT, SC_ITERATIONS,
-             precision=32, nthreads=threads, self_contact=sc)  # fmt: skip
+    contacts = orc.make_contacts(cnt, p, s, bp, bv, nn)
+    orc.step(om, q, qd.astype(np.float64), None, contacts, DT, SC_ITERATIONS, precision=32, nthreads=threads,
+             self_contact=sc)  # fmt: skip
     el = time.perf_counter() - t
-    return {"value": m.particle_count * SC_ITERATIONS / el, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": "one substep of the same settled 256x256 state (self-contact detection on a box grid)"}  # fmt: skip
+    out = {"value": m.particle_count * SC_ITERATIONS / el, "unit": UNIT, "cores": threads, "kind": "port",
+           "sample": "one substep of the same settled 256x256 state (self-contact detection on a box grid)"}  # fmt: skip
+    if fp64_step:
+        _, q64, _ = orc.step(om, q, qd.astype(np.float64), None, contacts, DT, SC_ITERATIONS, precision=64,
+                             nthreads=threads, self_contact=sc)  # fmt: skip
+        out["fp64_step_q"] = q64
+    return out
 
 
 def build_soft_model(dev, worlds, seed=5):
@@ -966,6 +1092,7 @@ def run_soft(args):
     if not args.no_e2e:
         hq, hqd = q_w.cpu().pin_memory(), qd_w.cpu().pin_memory()
         out_q = torch.empty_like(hq).pin_memory()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record()
         for _ in range(K):

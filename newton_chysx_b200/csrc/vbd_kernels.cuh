@@ -203,9 +203,10 @@ __device__ __forceinline__ void finalize_particle(const StepCtx<R>& c, const P& 
   c.qd_out[3 * i + 2] = v.z;
 }
 
-// contact terms of one particle (lane 0 of the group)
-template <typename R>
-__device__ __forceinline__ void contacts_add_n(const StepCtx<R>& c, int v, int n, vec3<R> x, vec3<R>& f, sym3<R>& H) {
+// contact terms of one particle (lane 0 of the group), evaluated and accumulated in A (R, or double for the mixed
+// mode's FP64 contact path)
+template <typename R, typename A = R>
+__device__ __forceinline__ void contacts_add_n(const StepCtx<R>& c, int v, int n, vec3<A> x, vec3<A>& f, sym3<A>& H) {
   if (n <= 0) return;
   if (n > c.K) n = c.K;
   int ids[8];
@@ -219,7 +220,8 @@ __device__ __forceinline__ void contacts_add_n(const StepCtx<R>& c, int v, int n
     }
     ids[b + 1] = key;
   }
-  const R r = R(c.radius[v]);
+  const A r = A(c.radius[v]);
+  const A dt = A(c.dt);
   for (int j = 0; j < n; ++j) {
     const int t = ids[j];
     const int s = c.c_shape[t];
@@ -228,18 +230,18 @@ __device__ __forceinline__ void contacts_add_n(const StepCtx<R>& c, int v, int n
     vec3<float> bxf = bp;
     const float* X = (b >= 0 && c.body_q) ? c.body_q + 7 * b : nullptr;
     if (X) bxf = qrot(X + 3, bp) + vec3<float>{X[0], X[1], X[2]};
-    const vec3<R> bx = {R(bxf.x), R(bxf.y), R(bxf.z)};
+    const vec3<A> bx = {A(bxf.x), A(bxf.y), A(bxf.z)};
     const vec3<float> nf = ldv3(c.c_normal, t);
-    const vec3<R> nn = {R(nf.x), R(nf.y), R(nf.z)};
-    const R pen = -(dot(nn, x - bx) - r);
-    R k = R(c.c_k[t]);
+    const vec3<A> nn = {A(nf.x), A(nf.y), A(nf.z)};
+    const A pen = -(dot(nn, x - bx) - r);
+    A k = A(c.c_k[t]);
     if (c.beta != R(0) && c.dual_in_solve) {
       // AVBD penalty ramp with the position at the start of this iteration (unchanged until now)
-      k = vmin(k + c.beta * vmax(R(0), pen), R(c.c_ke[t]));
+      k = vmin(k + A(c.beta) * vmax(A(0), pen), A(c.c_ke[t]));
       c.c_k[t] = float(k);
     }
-    if (pen > R(0)) {
-      const vec3<R> dx = x - ld3<R>(c.qprev[v]);
+    if (pen > A(0)) {
+      const vec3<A> dx = x - ld3<A>(c.qprev[v]);
       const vec3<float> bvl = ldv3(c.c_body_vel, t);
       vec3<float> bv = bvl;
       if (X) {
@@ -255,8 +257,8 @@ __device__ __forceinline__ void contacts_add_n(const StepCtx<R>& c, int v, int n
           bv = vec3<float>{qd[0], qd[1], qd[2]} + cross(vec3<float>{qd[3], qd[4], qd[5]}, rr) + bv;
         }
       }
-      const vec3<R> rel = dx - vec3<R>{R(bv.x), R(bv.y), R(bv.z)} * c.dt;
-      contact_add<R>(pen, nn, rel, k, R(c.c_kd[t]), R(c.c_mu[t]), c.fric_eps, c.dt, f, H);
+      const vec3<A> rel = dx - vec3<A>{A(bv.x), A(bv.y), A(bv.z)} * dt;
+      contact_add<A>(pen, nn, rel, k, A(c.c_kd[t]), A(c.c_mu[t]), A(c.fric_eps), dt, f, H);
     }
   }
 }
@@ -265,6 +267,62 @@ __device__ __forceinline__ void contacts_add_n(const StepCtx<R>& c, int v, int n
 template <typename R>
 __device__ __forceinline__ void contacts_add(const StepCtx<R>& c, int v, vec3<R> x, vec3<R>& f, sym3<R>& H) {
   contacts_add_n<R>(c, v, c.slot_cnt[v], x, f, H);
+}
+
+// Contact terms and the 3x3 block solve H dlt = f of one vertex whose (f, H) hold its element and inertia sums.
+// extra: nine more sums (f xyz, then H xx yy zz xy xz yz) added after the contacts, or null. r2 = |f|^2 of the full
+// sums in FP64 (the mixed mode's residual). Returns the determinant used; the caller applies the reference's
+// |det H| > 1e-8 test.
+// FP32, FP64: all in R, the reference's arithmetic.
+// MIXED: a vertex with contacts widens its FP32 sums to FP64, adds the contact terms in FP64 and solves in FP64.
+// The contact damping stiffness kd ke / dt along the normal (1.9e8 N/m for the reference's default shape material,
+// kd = 100 averaged with the model's, over ke = 6,250, at dt = 1/600 s) is 1e8 times the membrane, bending and
+// inertia stiffness of a fine sheet; an FP32 sum of both keeps nothing of the latter (its rounding is ~10 N/m), so
+// the tangential part of the block is lost and the FP32 step of such a vertex can move it by metres. In FP64 the
+// stiff normal direction is a rank-one term known to 1e-16 and the tangential block survives. Vertices without
+// contacts solve in FP64 only when their FP32 block is ill-conditioned (|det H| < thr max|H|^3).
+template <typename R, int MODE>
+__device__ __forceinline__ double contacts_and_solve(const StepCtx<R>& c, int v, int ncont, vec3<R> x, vec3<R> f,
+                                                     sym3<R> H, const R* extra, vec3<R>& dlt, double& r2) {
+  if (MODE == MODE_MIXED && ncont > 0) {
+    const vec3<double> xd = {double(x.x), double(x.y), double(x.z)};
+    vec3<double> fd = {double(f.x), double(f.y), double(f.z)};
+    sym3<double> Hd = {double(H.xx), double(H.yy), double(H.zz), double(H.xy), double(H.xz), double(H.yz)};
+    contacts_add_n<R, double>(c, v, ncont, xd, fd, Hd);
+    if (extra) {
+      fd = fd + vec3<double>{double(extra[0]), double(extra[1]), double(extra[2])};
+      Hd = Hd + sym3<double>{double(extra[3]), double(extra[4]), double(extra[5]),
+                             double(extra[6]), double(extra[7]), double(extra[8])};
+    }
+    r2 = dot(fd, fd);
+    const double det = sdet(Hd);
+    const vec3<double> rr = sadj_mul(Hd, fd) * (1.0 / det);
+    dlt = {R(rr.x), R(rr.y), R(rr.z)};
+    return det;
+  }
+  if (ncont > 0) contacts_add_n<R>(c, v, ncont, x, f, H);
+  if (extra) {
+    f = f + vec3<R>{extra[0], extra[1], extra[2]};
+    H = H + sym3<R>{extra[3], extra[4], extra[5], extra[6], extra[7], extra[8]};
+  }
+  r2 = double(f.x) * double(f.x) + double(f.y) * double(f.y) + double(f.z) * double(f.z);
+  if (MODE == MODE_MIXED) {
+    const R hmax = vmax(vmax(vmax(vabs(H.xx), vabs(H.yy)), vmax(vabs(H.zz), vabs(H.xy))), vmax(vabs(H.xz), vabs(H.yz)));
+    const R d = sdet(H);
+    if (!(vabs(d) >= R(c.fp64_thr) * hmax * hmax * hmax)) {  // ill-conditioned or not finite: FP64
+      const sym3<double> Hd = {double(H.xx), double(H.yy), double(H.zz), double(H.xy), double(H.xz), double(H.yz)};
+      const vec3<double> fd = {double(f.x), double(f.y), double(f.z)};
+      const double det = sdet(Hd);
+      const vec3<double> rr = sadj_mul(Hd, fd) * (1.0 / det);
+      dlt = {R(rr.x), R(rr.y), R(rr.z)};
+      return det;
+    }
+    dlt = sadj_mul(H, f) * (R(1) / d);
+    return double(d);
+  }
+  const R d = sdet(H);
+  dlt = sadj_mul(H, f) * (R(1) / d);
+  return double(d);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -433,6 +491,8 @@ __device__ __forceinline__ void solve_group(const StepCtx<R>& c, const P& pos, i
   const bool leader = active && sub == 0;
   if (SC && valid && !active && sub == 0) c.disp[v] = pk4(zero3<R>(), R(0));  // as the reference's solve does
   vec3<R> x = zero3<R>();
+  vec3<R> dlt = zero3<R>();
+  double det_used = 0.0, r2 = 0.0;
   if (leader) {
     x = pos.ld(v);
     const vec3<R> in = ld3<R>(c.inertia[v]);
@@ -441,42 +501,17 @@ __device__ __forceinline__ void solve_group(const StepCtx<R>& c, const P& pos, i
     H.xx += md;
     H.yy += md;
     H.zz += md;
-    if (c.has_contacts) contacts_add<R>(c, v, x, f, H);
-    if (SOFT && c.n_same_springs && __ldg(c.sspr_off + v + 1) > __ldg(c.sspr_off + v)) {
-      const R* a = c.spr_acc + 9 * size_t(v);
-      f = f + vec3<R>{a[0], a[1], a[2]};
-      H = H + sym3<R>{a[3], a[4], a[5], a[6], a[7], a[8]};
-    }
+    const R* extra = nullptr;
+    if (SOFT && c.n_same_springs && __ldg(c.sspr_off + v + 1) > __ldg(c.sspr_off + v)) extra = c.spr_acc + 9 * size_t(v);
+    det_used = contacts_and_solve<R, MODE>(c, v, c.has_contacts ? c.slot_cnt[v] : 0, x, f, H, extra, dlt, r2);
   }
   if (MODE == MODE_MIXED && c.residual) {
     // FP64 reduction of |f|^2 (the force residual the block solve removes): warp sum, one atomic per warp
-    double r2 = leader ? double(f.x) * double(f.x) + double(f.y) * double(f.y) + double(f.z) * double(f.z) : 0.0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) r2 += __shfl_xor_sync(0xffffffffu, r2, o);
     if ((threadIdx.x & 31) == 0 && r2 != 0.0) atomicAdd(c.residual + 32 * iteration, r2);
   }
   if (!leader) return;
-  vec3<R> dlt;
-  double det_used;
-  if (MODE == MODE_MIXED) {
-    const R hmax = vmax(vmax(vmax(vabs(H.xx), vabs(H.yy)), vmax(vabs(H.zz), vabs(H.xy))), vmax(vabs(H.xz), vabs(H.yz)));
-    const R d = sdet(H);
-    if (vabs(d) < R(c.fp64_thr) * hmax * hmax * hmax) {
-      // ill-conditioned block: determinant and adjugate solve in FP64
-      const sym3<double> Hd = {double(H.xx), double(H.yy), double(H.zz), double(H.xy), double(H.xz), double(H.yz)};
-      const vec3<double> fd = {double(f.x), double(f.y), double(f.z)};
-      det_used = sdet(Hd);
-      const vec3<double> r = sadj_mul(Hd, fd) * (1.0 / det_used);
-      dlt = {R(r.x), R(r.y), R(r.z)};
-    } else {
-      det_used = double(d);
-      dlt = sadj_mul(H, f) * (R(1) / d);
-    }
-  } else {
-    const R d = sdet(H);
-    det_used = double(d);
-    dlt = sadj_mul(H, f) * (R(1) / d);
-  }
   // the reference updates only when |det H| > 1e-8 (a NaN determinant fails that test too)
   if (!isfinite(det_used)) {
     set_err(c.err, 1);

@@ -213,31 +213,11 @@ __device__ __forceinline__ void solve_ring(const StepCtx<R>& c, const P& pos, co
   H.xx += md;
   H.yy += md;
   H.zz += md;
-  if (c.has_contacts) contacts_add<R>(c, v, x, f, H);
-  if (MODE == MODE_MIXED && c.residual) {
-    const double r2 = double(f.x) * double(f.x) + double(f.y) * double(f.y) + double(f.z) * double(f.z);
-    residual_add(c.residual, iteration, r2);
-  }
   vec3<R> dlt;
-  double det_used;
-  if (MODE == MODE_MIXED) {
-    const R hmax = vmax(vmax(vmax(vabs(H.xx), vabs(H.yy)), vmax(vabs(H.zz), vabs(H.xy))), vmax(vabs(H.xz), vabs(H.yz)));
-    const R d = sdet(H);
-    if (!(vabs(d) >= R(c.fp64_thr) * hmax * hmax * hmax)) {
-      const sym3<double> Hd = {double(H.xx), double(H.yy), double(H.zz), double(H.xy), double(H.xz), double(H.yz)};
-      const vec3<double> fd = {double(f.x), double(f.y), double(f.z)};
-      det_used = sdet(Hd);
-      const vec3<double> rr = sadj_mul(Hd, fd) * (1.0 / det_used);
-      dlt = {R(rr.x), R(rr.y), R(rr.z)};
-    } else {
-      det_used = double(d);
-      dlt = sadj_mul(H, f) * (R(1) / d);
-    }
-  } else {
-    const R d = sdet(H);
-    det_used = double(d);
-    dlt = sadj_mul(H, f) * (R(1) / d);
-  }
+  double r2;
+  const int ncont = c.has_contacts ? c.slot_cnt[v] : 0;
+  const double det_used = contacts_and_solve<R, MODE>(c, v, ncont, x, f, H, nullptr, dlt, r2);
+  if (MODE == MODE_MIXED && c.residual) residual_add(c.residual, iteration, r2);
   if (!isfinite(det_used)) {
     set_err(c.err, 1);
     return;

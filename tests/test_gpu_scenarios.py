@@ -105,6 +105,66 @@ def test_hanging_cloth_fp32_error_vs_fp64(schedule):
     assert max(err) <= 1.5 * max(err_ref) + 1e-4, (err, err_ref)
 
 
+FULL_FRAMES = 120  # the plain-VBD scene's horizon: 120 frames of 10 substeps x 10 iterations
+
+
+def _per_substep_errors(precision, schedule):
+    """Along the GPU's own trajectory of the whole 120-frame horizon of the hanging-sheet scene in `precision`,
+    the first substep of every frame against the FP64 oracle's substep from the same state (contacts from the
+    same FP32 positions): max vertex |x_gpu - x_oracle|_2 per frame."""
+    model = _hanging_scene()
+    solver = SolverVBD(model, iterations=10, schedule=schedule, precision=precision)
+    pipe = CollisionPipeline(model, soft_contact_margin=0.01)
+    contacts = pipe.contacts()
+    om = orc.Model(oracle_model_dict(model))
+    r, fl = model.particle_radius.cpu().numpy(), model.particle_flags.cpu().numpy()
+    s0, s1 = model.state(), model.state()
+    if precision == "fp64":
+        for s in (s0, s1):
+            s.particle_q, s.particle_qd, s.particle_f = (t.double() for t in (s.particle_q, s.particle_qd, s.particle_f))
+    samples = []
+    for _ in range(FULL_FRAMES):
+        for k in range(10):
+            if k == 0:
+                q_in = s0.particle_q.cpu().numpy().astype(np.float64)
+                qd_in = s0.particle_qd.cpu().numpy().astype(np.float64)
+            pipe.collide(s0 if precision != "fp64" else _f32_state(s0), contacts)
+            solver.step(s0, s1, None, contacts, 1.0 / 600.0)
+            if k == 0:
+                samples.append((q_in, qd_in, s1.particle_q.cpu().numpy().astype(np.float64)))
+            s0, s1 = s1, s0
+    assert solver.device_errors() == 0
+    err = []
+    for q_in, qd_in, q_gpu in samples:
+        qc = q_in.astype(np.float32).astype(np.float64)
+        cnt, p, s, bp, bv, nn = orc.soft_contacts_shapes(qc, r, fl, model.shape_type, model.shape_transform,
+                                                         model.shape_scale, 0.01)  # fmt: skip
+        _, q_ref, _ = orc.step(om, q_in, qd_in, None, orc.make_contacts(cnt, p, s, bp, bv, nn), 1.0 / 600.0, 10,
+                               precision=64, nthreads=orc.max_threads())  # fmt: skip
+        err.append(float(np.linalg.norm(q_gpu - q_ref, axis=1).max()))
+    return err
+
+
+@pytest.mark.parametrize("schedule", ["per_color", "persistent"])
+def test_hanging_cloth_fp64_per_substep_full_horizon(schedule):
+    """The whole 120-frame horizon (1,200 substeps: the fall, first contact at frame 5 and stick/slip friction
+    on the ground to the end): at every frame the FP64 step equals the FP64 oracle's step from the same state.
+    Whole trajectories are not compared past the first frames: from the frame-10 state two FP64 runs that differ
+    by 1e-10 m part by centimetres within ten frames (the contact set and the friction regime switch on
+    thresholds), in the oracle against itself as well."""
+    err = _per_substep_errors("fp64", schedule)
+    assert max(err) <= 1e-9, max(err)
+
+
+def test_hanging_cloth_fp32_per_substep_full_horizon():
+    """Along the GPU's own FP32 trajectory of the 120-frame horizon, every frame's first FP32 substep against the
+    FP64 oracle's substep from the same FP32 state: <= 1e-4 m (cloth side 1 m) in the fall, at first contact and
+    through the friction phase."""
+    err = _per_substep_errors("fp32", "per_color")
+    assert max(err) <= 1e-4, max(err)
+    assert max(err[5:]) > 0.0  # contact frames were compared, not an idle sheet
+
+
 def test_free_fall_matches_kinematics():
     """test_cloth.py:1093-1114: an unconstrained sheet falls as 1/2 g t^2 with no horizontal drift."""
     b = cloth_grid_builder(n=16, hanging=False, pin_top_corners=False, height=4.0, up_axis="Y")
