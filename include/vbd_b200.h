@@ -449,6 +449,12 @@ typedef struct VbdShapeTable {
   const int32_t* shape_flags_host;
   const int32_t* shape_world_host;
   const int32_t* particle_world_dev;
+  /* shapes on bodies (geometry/kernels.py:1045-1056): shape s is carried by body shape_body_host[s] (-1 = static,
+     NULL = all static) of body_count bodies; body_q_dev [body_count, 7] holds the body transforms (p, q xyzw) for
+     vbd_soft_contacts_table (the shape sets take them per call instead) */
+  const int32_t* shape_body_host;
+  int32_t body_count;
+  const float* body_q_dev;
 } VbdShapeTable;
 
 /* vbd_soft_contacts_shapes over a full shape table: the analytic types, heightfields (sample_sdf_grad_heightfield,
@@ -464,10 +470,11 @@ int vbd_soft_contacts_table(int32_t particle_count, const float* q_dev, const fl
                             int32_t soft_contact_max, int32_t* count_dev, int32_t* particle_dev, int32_t* shape_dev,
                             float* body_pos_dev, float* body_vel_dev, float* normal_dev, void* stream);
 
-/* A model's static shapes uploaded once for contact generation, any number of shapes and worlds: the shapes with
+/* A model's shapes uploaded once for contact generation, any number of shapes and worlds: the shapes with
    COLLIDE_PARTICLES, their records and, per world, the list of its shapes (create_soft_contacts' world filter,
-   geometry/kernels.py:1036-1043). Takes the VbdShapeTable fields except particle_world_dev; world indices must
-   be -1 (global) or non-negative. The mesh handles and the elevation array the table names must outlive the set. */
+   geometry/kernels.py:1036-1043). Takes the VbdShapeTable fields except particle_world_dev and body_q_dev; world
+   indices must be -1 (global) or non-negative, body indices -1 (static) or below body_count. The mesh handles and
+   the elevation array the table names must outlive the set. */
 typedef struct VbdShapeSetImpl* VbdShapeSetHandle;
 int vbd_shape_set_create(const VbdShapeTable* shapes, VbdShapeSetHandle* out);
 int vbd_shape_set_destroy(VbdShapeSetHandle set);
@@ -478,11 +485,15 @@ int vbd_shape_set_use_parameter_table(VbdShapeSetHandle set, int32_t enable);
 
 /* Soft contacts of every active particle against a shape set, written as vbd_soft_contacts_shapes writes them. A
    particle of world w (particle_world_dev; NULL = all global) tests the global shapes and world w's shapes; a
-   global particle tests every shape. */
+   global particle tests every shape. body_q_dev: the body transforms [bodies, 7] (p, q xyzw) of this call
+   (state.body_q), required when a shape of the set is on a body, else ignored; such a shape's contact point is
+   written in its body's frame and its normal in world (create_soft_contacts, geometry/kernels.py:1045-1056,
+   1128-1140). */
 int vbd_soft_contacts_set(VbdShapeSetHandle set, int32_t particle_count, const float* q_dev, const float* radius_dev,
-                          const int32_t* flags_dev, const int32_t* particle_world_dev, float margin,
-                          int32_t soft_contact_max, int32_t* count_dev, int32_t* particle_dev, int32_t* shape_dev,
-                          float* body_pos_dev, float* body_vel_dev, float* normal_dev, void* stream);
+                          const int32_t* flags_dev, const int32_t* particle_world_dev, const float* body_q_dev,
+                          float margin, int32_t soft_contact_max, int32_t* count_dev, int32_t* particle_dev,
+                          int32_t* shape_dev, float* body_pos_dev, float* body_vel_dev, float* normal_dev,
+                          void* stream);
 
 #ifdef __cplusplus
 }

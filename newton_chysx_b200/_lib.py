@@ -93,7 +93,7 @@ class VbdShapeTable(C.Structure):
         ("shape_scale_host", _fp), ("shape_heightfield_index_host", _ip), ("heightfield_count", C.c_int32),
         ("heightfields_host", C.POINTER(VbdHeightfield)), ("elevations_dev", _vp), ("elevation_count", C.c_int64),
         ("shape_mesh_host", C.POINTER(_vp)), ("shape_flags_host", _ip), ("shape_world_host", _ip),
-        ("particle_world_dev", _vp),
+        ("particle_world_dev", _vp), ("shape_body_host", _ip), ("body_count", C.c_int32), ("body_q_dev", _vp),
     ]  # fmt: skip
 
 
@@ -169,7 +169,7 @@ SIGNATURES = {
     "vbd_shape_set_destroy": ([_vp], C.c_int),
     "vbd_shape_set_use_parameter_table": ([_vp, C.c_int32], C.c_int),
     "vbd_soft_contacts_set": (
-        [_vp, C.c_int32, _vp, _vp, _vp, _vp, C.c_float, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+        [_vp, C.c_int32, _vp, _vp, _vp, _vp, _vp, C.c_float, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
         C.c_int,
     ),
     "vbd_mesh_destroy": ([_vp], C.c_int),

@@ -2160,11 +2160,16 @@ int vbd_soft_contacts_table(int32_t n, const float* q, const float* radius, cons
   cudaStream_t st = (cudaStream_t)stream;
   CK(cudaMemsetAsync(count, 0, sizeof(int), st));
   if (n == 0 || m == 0) return VBD_OK;
-  bool worlds = false;
-  for (int s = 0; s < m; ++s) worlds = worlds || tab.rec[s].world != -1;
+  bool worlds = false, bodies = false;
+  for (int s = 0; s < m; ++s) {
+    worlds = worlds || tab.rec[s].world != -1;
+    bodies = bodies || tab.rec[s].body >= 0;
+  }
+  if (bodies && !tb->body_q_dev) return VBD_ERR_INVALID_ARGUMENT;
   auto kern = worlds && tb->particle_world_dev ? k_soft_contacts_shapes<true> : k_soft_contacts_shapes<false>;
   kern<<<(n + 255) / 256, 256, 0, st>>>(n, q, radius, flags, m, tab, tb->elevations_dev, tb->particle_world_dev,
-                                         margin, cmax, count, particle, shape, body_pos, body_vel, normal);
+                                         tb->body_q_dev, margin, cmax, count, particle, shape, body_pos, body_vel,
+                                         normal);
   CK(cudaGetLastError());
   return VBD_OK;
 }

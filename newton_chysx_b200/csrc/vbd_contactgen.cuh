@@ -1,8 +1,9 @@
-// One particle against one static shape, as create_soft_contacts does it (geometry/kernels.py:1001-1140): the
-// particle in the shape frame, the shape's signed distance and outward normal (analytic SDFs, heightfield query,
-// mesh query), and for d < margin + radius a contact at the closest surface point x_local - n d with the normal
-// mapped back to world, in a slot taken from an atomic counter. Shared by the kernel-parameter path (at most
-// kMaxContactShapes shapes per call) and the device-resident shape sets (any number of shapes and worlds).
+// One particle against one shape, as create_soft_contacts does it (geometry/kernels.py:1001-1140): the shape's
+// world frame X_ws = body_q[body] X_bs (X_bs alone for a static shape, body -1), the particle in the shape frame,
+// the shape's signed distance and outward normal (analytic SDFs, heightfield query, mesh query), and for
+// d < margin + radius a contact at the closest surface point x_local - n d mapped to the body frame by X_bs, with
+// the normal mapped to world by X_ws, in a slot taken from an atomic counter. Shared by the kernel-parameter path
+// (at most kMaxContactShapes shapes per call) and the device-resident shape sets (any number of shapes and worlds).
 #pragma once
 #include <cmath>
 
@@ -12,7 +13,8 @@
 
 namespace vbd {
 
-// A static shape: transform (p, q xyzw), scale, and the data of its kind.
+// A shape: transform in its body's frame (p, q xyzw; the world frame for a static shape), scale, and the data of
+// its kind.
 struct ShapeRec {
   float4 p;
   float4 q;    // unit quaternion (x, y, z, w)
@@ -23,7 +25,7 @@ struct ShapeRec {
   int type;   // GeoType
   int world;  // -1 = global
   int id;     // index in the model
-  int pad;
+  int body;   // -1 = static (geometry/kernels.py:1045-1049)
 };
 
 __host__ __device__ __forceinline__ vec3<float> rot_q(float4 q, vec3<float> v) {
@@ -31,13 +33,28 @@ __host__ __device__ __forceinline__ vec3<float> rot_q(float4 q, vec3<float> v) {
   return v * (2.f * q.w * q.w - 1.f) + cross(u, v) * (2.f * q.w) + u * (2.f * dot(u, v));
 }
 
+// Hamilton product a b of quaternions (x, y, z, w): the rotation b followed by a.
+__host__ __device__ __forceinline__ float4 mul_q(float4 a, float4 b) {
+  return make_float4(a.w * b.x + b.w * a.x + a.y * b.z - a.z * b.y, a.w * b.y + b.w * a.y + a.z * b.x - a.x * b.z,
+                     a.w * b.z + b.w * a.z + a.x * b.y - a.y * b.x, a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z);
+}
+
+// body_q: [bodies, 7] body transforms (p, q xyzw) of this call; read only for a shape on a body.
 __device__ __forceinline__ void soft_contact_shape(const ShapeRec& sh, const float* __restrict__ elev,
-                                                   vec3<float> x, float r, float margin, int i, int cmax,
-                                                   int* count, int* particle, int* shape, float* body_pos,
-                                                   float* body_vel, float* normal) {
+                                                   const float* __restrict__ body_q, vec3<float> x, float r,
+                                                   float margin, int i, int cmax, int* count, int* particle,
+                                                   int* shape, float* body_pos, float* body_vel, float* normal) {
   const float4 P = sh.p, Q = sh.q, SC = sh.sc;
-  const float4 Qi = make_float4(-Q.x, -Q.y, -Q.z, Q.w);
-  const vec3<float> xl = rot_q(Qi, vec3<float>{x.x - P.x, x.y - P.y, x.z - P.z});
+  float4 Pw = P, Qw = Q;  // X_ws
+  if (sh.body >= 0) {
+    const float* X = body_q + 7 * sh.body;
+    const float4 Qb = make_float4(X[3], X[4], X[5], X[6]);
+    const vec3<float> pw = rot_q(Qb, vec3<float>{P.x, P.y, P.z});
+    Pw = make_float4(X[0] + pw.x, X[1] + pw.y, X[2] + pw.z, 0.f);
+    Qw = mul_q(Qb, Q);
+  }
+  const float4 Qi = make_float4(-Qw.x, -Qw.y, -Qw.z, Qw.w);
+  const vec3<float> xl = rot_q(Qi, vec3<float>{x.x - Pw.x, x.y - Pw.y, x.z - Pw.z});
   const float sc[3] = {SC.x, SC.y, SC.z};
   float d;
   vec3<float> nn;
@@ -63,8 +80,8 @@ __device__ __forceinline__ void soft_contact_shape(const ShapeRec& sh, const flo
   if (d < margin + r) {
     const int k = atomicAdd(count, 1);
     if (k < cmax) {
-      const vec3<float> bp = rot_q(Q, xl - nn * d) + vec3<float>{P.x, P.y, P.z};
-      const vec3<float> wn = rot_q(Q, nn);
+      const vec3<float> bp = rot_q(Q, xl - nn * d) + vec3<float>{P.x, P.y, P.z};  // body frame
+      const vec3<float> wn = rot_q(Qw, nn);
       particle[k] = i;
       shape[k] = sh.id;
       body_pos[3 * k] = bp.x, body_pos[3 * k + 1] = bp.y, body_pos[3 * k + 2] = bp.z;
@@ -88,9 +105,9 @@ template <bool WORLDS>
 __global__ void __launch_bounds__(256, 4)
     k_soft_contacts_shapes(int n, const float* __restrict__ q, const float* __restrict__ radius,
                            const int* __restrict__ flags, int S, const ShapeParamTable shapes,
-                           const float* __restrict__ elev, const int* __restrict__ particle_world, float margin,
-                           int cmax, int* count, int* particle, int* shape, float* body_pos, float* body_vel,
-                           float* normal) {
+                           const float* __restrict__ elev, const int* __restrict__ particle_world,
+                           const float* __restrict__ body_q, float margin, int cmax, int* count, int* particle,
+                           int* shape, float* body_pos, float* body_vel, float* normal) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || !(flags[i] & 1)) return;
   const vec3<float> x = {q[3 * i], q[3 * i + 1], q[3 * i + 2]};
@@ -101,8 +118,8 @@ __global__ void __launch_bounds__(256, 4)
       const int sw = shapes.rec[s].world;
       if (pw != -1 && sw != -1 && pw != sw) continue;
     }
-    soft_contact_shape(shapes.rec[s], elev, x, r, margin, i, cmax, count, particle, shape, body_pos, body_vel,
-                       normal);
+    soft_contact_shape(shapes.rec[s], elev, body_q, x, r, margin, i, cmax, count, particle, shape, body_pos,
+                       body_vel, normal);
   }
 }
 
@@ -121,6 +138,8 @@ inline int fill_shape_rec(const VbdShapeTable* tb, int s0, ShapeRec& rec) {
   rec.type = t;
   rec.id = s0;
   rec.world = tb->shape_world_host ? tb->shape_world_host[s0] : -1;
+  rec.body = tb->shape_body_host ? tb->shape_body_host[s0] : -1;
+  if (rec.body < -1 || (rec.body >= 0 && rec.body >= tb->body_count)) return VBD_ERR_INVALID_ARGUMENT;
   rec.p = make_float4(X[0], X[1], X[2], 0.f);
   rec.q = make_float4(X[3] / ql, X[4] / ql, X[5] / ql, X[6] / ql);
   rec.sc = make_float4(sc[0], sc[1], sc[2], 0.f);

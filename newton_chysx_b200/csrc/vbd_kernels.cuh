@@ -129,11 +129,23 @@ __device__ __forceinline__ void residual_add(double* residual, int iteration, do
 
 __device__ __forceinline__ vec3<float> ldv3(const float* a, int i) { return {a[3 * i], a[3 * i + 1], a[3 * i + 2]}; }
 
-// rotate v by quaternion (x, y, z, w)
-__device__ __forceinline__ vec3<float> qrot(const float* q, vec3<float> v) {
-  const vec3<float> u = {q[0], q[1], q[2]};
-  const float w = q[3];
-  return v * (2.f * w * w - 1.f) + cross(u, v) * (2.f * w) + u * (2.f * dot(u, v));
+// rotate v by quaternion (x, y, z, w), in A
+template <typename A>
+__device__ __forceinline__ vec3<A> qrot(const float* q, vec3<A> v) {
+  const vec3<A> u = {A(q[0]), A(q[1]), A(q[2])};
+  const A w = A(q[3]);
+  return v * (A(2) * w * w - A(1)) + cross(u, v) * (A(2) * w) + u * (A(2) * dot(u, v));
+}
+
+// body transform X (p, q xyzw) applied to point p, in A
+template <typename A>
+__device__ __forceinline__ vec3<A> xform_point(const float* X, vec3<A> p) {
+  return qrot<A>(X + 3, p) + vec3<A>{A(X[0]), A(X[1]), A(X[2])};
+}
+
+template <typename A>
+__device__ __forceinline__ vec3<A> ldv3a(const float* a, int i) {
+  return {A(a[3 * i]), A(a[3 * i + 1]), A(a[3 * i + 2])};
 }
 
 // Where the current positions live during the sweep: the solver's global float4/double4 array, or
@@ -226,11 +238,9 @@ __device__ __forceinline__ void contacts_add_n(const StepCtx<R>& c, int v, int n
     const int t = ids[j];
     const int s = c.c_shape[t];
     const int b = (c.shape_body && s >= 0) ? c.shape_body[s] : -1;
-    const vec3<float> bp = ldv3(c.c_body_pos, t);
-    vec3<float> bxf = bp;
+    const vec3<A> bp = ldv3a<A>(c.c_body_pos, t);
     const float* X = (b >= 0 && c.body_q) ? c.body_q + 7 * b : nullptr;
-    if (X) bxf = qrot(X + 3, bp) + vec3<float>{X[0], X[1], X[2]};
-    const vec3<A> bx = {A(bxf.x), A(bxf.y), A(bxf.z)};
+    const vec3<A> bx = X ? xform_point<A>(X, bp) : bp;
     const vec3<float> nf = ldv3(c.c_normal, t);
     const vec3<A> nn = {A(nf.x), A(nf.y), A(nf.z)};
     const A pen = -(dot(nn, x - bx) - r);
@@ -242,22 +252,22 @@ __device__ __forceinline__ void contacts_add_n(const StepCtx<R>& c, int v, int n
     }
     if (pen > A(0)) {
       const vec3<A> dx = x - ld3<A>(c.qprev[v]);
-      const vec3<float> bvl = ldv3(c.c_body_vel, t);
-      vec3<float> bv = bvl;
+      // velocity of the contact point (rigid_vbd_kernels.py:806-819)
+      const vec3<A> bvl = ldv3a<A>(c.c_body_vel, t);
+      vec3<A> bv = bvl;
       if (X) {
-        bv = qrot(X + 3, bvl);
+        bv = qrot<A>(X + 3, bvl);
         if (c.body_q_prev) {
-          const float* Xp = c.body_q_prev + 7 * b;
-          const vec3<float> bxp = qrot(Xp + 3, bp) + vec3<float>{Xp[0], Xp[1], Xp[2]};
-          bv = (bxf - bxp) * (1.f / float(c.dt)) + bv;
+          const vec3<A> bxp = xform_point<A>(c.body_q_prev + 7 * b, bp);
+          bv = (bx - bxp) * (A(1) / dt) + bv;
         } else if (c.body_qd) {
           const float* qd = c.body_qd + 6 * b;
-          vec3<float> com = c.body_com ? ldv3(c.body_com, b) : vec3<float>{0.f, 0.f, 0.f};
-          const vec3<float> rr = bxf - (qrot(X + 3, com) + vec3<float>{X[0], X[1], X[2]});
-          bv = vec3<float>{qd[0], qd[1], qd[2]} + cross(vec3<float>{qd[3], qd[4], qd[5]}, rr) + bv;
+          const vec3<A> com = c.body_com ? ldv3a<A>(c.body_com, b) : vec3<A>{A(0), A(0), A(0)};
+          const vec3<A> rr = bx - xform_point<A>(X, com);
+          bv = vec3<A>{A(qd[0]), A(qd[1]), A(qd[2])} + cross(vec3<A>{A(qd[3]), A(qd[4]), A(qd[5])}, rr) + bv;
         }
       }
-      const vec3<A> rel = dx - vec3<A>{A(bv.x), A(bv.y), A(bv.z)} * dt;
+      const vec3<A> rel = dx - bv * dt;
       contact_add<A>(pen, nn, rel, k, A(c.c_kd[t]), A(c.c_mu[t]), A(c.fric_eps), dt, f, H);
     }
   }
@@ -605,12 +615,8 @@ __global__ void k_contact_duals(StepCtx<R> c) {
   const int s = c.c_shape[t];
   if (v < 0 || v >= c.V || s < 0 || s >= c.S) return;
   const int b = (c.shape_body && s >= 0) ? c.shape_body[s] : -1;
-  vec3<float> bxf = ldv3(c.c_body_pos, t);
-  if (b >= 0 && c.body_q) {
-    const float* X = c.body_q + 7 * b;
-    bxf = qrot(X + 3, bxf) + vec3<float>{X[0], X[1], X[2]};
-  }
-  const vec3<R> bx = {R(bxf.x), R(bxf.y), R(bxf.z)};
+  const vec3<R> bp = ldv3a<R>(c.c_body_pos, t);
+  const vec3<R> bx = (b >= 0 && c.body_q) ? xform_point<R>(c.body_q + 7 * b, bp) : bp;
   const vec3<float> nf = ldv3(c.c_normal, t);
   const vec3<R> nn = {R(nf.x), R(nf.y), R(nf.z)};
   const R pen = -(dot(nn, ld3<R>(c.pos[v]) - bx) - R(c.radius[v]));

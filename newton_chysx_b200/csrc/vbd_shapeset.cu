@@ -1,4 +1,4 @@
-// Device-resident shape sets for particle contacts: a model's static shapes uploaded once, with the lists that
+// Device-resident shape sets for particle contacts: a model's shapes uploaded once, with the lists that
 // give each particle only the shapes it may touch (create_soft_contacts' world filter, geometry/kernels.py:
 // 1036-1043): a particle of world w tests the global shapes and the shapes of world w, a global particle tests
 // every shape. Any number of shapes and worlds.
@@ -24,6 +24,7 @@ struct VbdShapeSetImpl {
   void* buffer;
   vbd::ShapeParamTable small;  // the records again when m <= kParamTableShapes: launched as a kernel parameter
   bool worlds;                 // some shape belongs to a world
+  bool bodies;                 // some shape is on a body: launches need the body transforms
   bool param_table;            // launch small sets with `small` (else the global-memory kernel for every size)
 };
 
@@ -34,8 +35,8 @@ __global__ void __launch_bounds__(256, 4)
                         const int* __restrict__ flags, const int* __restrict__ particle_world,
                         const ShapeRec* __restrict__ recs, int m, const int* __restrict__ global, int n_global,
                         const int* __restrict__ world_off, const int* __restrict__ world_list, int W,
-                        const float* __restrict__ elev, float margin, int cmax, int* count, int* particle, int* shape,
-                        float* body_pos, float* body_vel, float* normal) {
+                        const float* __restrict__ elev, const float* __restrict__ body_q, float margin, int cmax,
+                        int* count, int* particle, int* shape, float* body_pos, float* body_vel, float* normal) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || !(flags[i] & 1)) return;
   const vbd::vec3<float> x = {q[3 * i], q[3 * i + 1], q[3 * i + 2]};
@@ -47,7 +48,8 @@ __global__ void __launch_bounds__(256, 4)
   const int w0 = own ? world_off[pw] : 0, nb = own ? world_off[pw + 1] - w0 : 0;
   for (int k = 0; k < na + nb; ++k) {
     const int s = k < na ? (pw == -1 ? k : global[k]) : world_list[w0 + k - na];
-    vbd::soft_contact_shape(recs[s], elev, x, r, margin, i, cmax, count, particle, shape, body_pos, body_vel, normal);
+    vbd::soft_contact_shape(recs[s], elev, body_q, x, r, margin, i, cmax, count, particle, shape, body_pos, body_vel,
+                            normal);
   }
 }
 
@@ -115,6 +117,7 @@ int vbd_shape_set_create(const VbdShapeTable* tb, VbdShapeSetHandle* out) {
   set->elev = tb->elevations_dev;
   set->buffer = buf;
   set->worlds = W > 0;
+  set->bodies = std::any_of(recs.begin(), recs.end(), [](const ShapeRec& r) { return r.body >= 0; });
   set->param_table = true;
   if (m <= vbd::kParamTableShapes) std::copy(recs.begin(), recs.end(), set->small.rec);
   *out = set;
@@ -135,9 +138,10 @@ int vbd_shape_set_destroy(VbdShapeSetHandle set) {
 }
 
 int vbd_soft_contacts_set(VbdShapeSetHandle set, int32_t n, const float* q, const float* radius, const int32_t* flags,
-                          const int32_t* particle_world, float margin, int32_t cmax, int32_t* count, int32_t* particle,
-                          int32_t* shape, float* body_pos, float* body_vel, float* normal, void* stream) {
-  if (!set || n < 0 || cmax < 0 || !count) return VBD_ERR_INVALID_ARGUMENT;
+                          const int32_t* particle_world, const float* body_q, float margin, int32_t cmax, int32_t* count,
+                          int32_t* particle, int32_t* shape, float* body_pos, float* body_vel, float* normal,
+                          void* stream) {
+  if (!set || n < 0 || cmax < 0 || !count || (set->bodies && !body_q)) return VBD_ERR_INVALID_ARGUMENT;
   if (n > 0 && set->m > 0 &&
       (!q || !radius || !flags || (cmax > 0 && (!particle || !shape || !body_pos || !body_vel || !normal))))
     return VBD_ERR_INVALID_ARGUMENT;
@@ -146,14 +150,14 @@ int vbd_soft_contacts_set(VbdShapeSetHandle set, int32_t n, const float* q, cons
   if (n == 0 || set->m == 0) return VBD_OK;
   if (set->param_table && set->m <= vbd::kParamTableShapes) {  // small sets: records in the constant bank measured faster
     auto kern = set->worlds && particle_world ? vbd::k_soft_contacts_shapes<true> : vbd::k_soft_contacts_shapes<false>;
-    kern<<<(n + 255) / 256, 256, 0, st>>>(n, q, radius, flags, set->m, set->small, set->elev, particle_world, margin,
-                                           cmax, count, particle, shape, body_pos, body_vel, normal);
+    kern<<<(n + 255) / 256, 256, 0, st>>>(n, q, radius, flags, set->m, set->small, set->elev, particle_world, body_q,
+                                           margin, cmax, count, particle, shape, body_pos, body_vel, normal);
     return cudaGetLastError() == cudaSuccess ? VBD_OK : VBD_ERR_CUDA;
   }
   k_soft_contacts_set<<<(n + 255) / 256, 256, 0, st>>>(n, q, radius, flags, particle_world, set->recs, set->m,
                                                        set->global, set->n_global, set->world_off, set->world_list,
-                                                       set->W, set->elev, margin, cmax, count, particle, shape,
-                                                       body_pos, body_vel, normal);
+                                                       set->W, set->elev, body_q, margin, cmax, count, particle,
+                                                       shape, body_pos, body_vel, normal);
   return cudaGetLastError() == cudaSuccess ? VBD_OK : VBD_ERR_CUDA;
 }
 

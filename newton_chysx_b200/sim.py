@@ -25,7 +25,7 @@ import math
 import numpy as np
 import torch
 
-from . import _lib
+from . import _lib, interop
 
 
 class ParticleFlags(enum.IntEnum):
@@ -303,6 +303,7 @@ class ModelBuilder:
         self._s = 0
         self._tt = 0
         self.shapes = []  # dicts: type, pos, normal, radius, ke, kd, mu, body
+        self.bodies = []  # dicts: q (p, quat xyzw), com, mass, inertia, label, kinematic, world
         self._color_groups: list[_ChunkedGroup] = []
         self.world_count = 0
         self.current_world = -1
@@ -324,6 +325,10 @@ class ModelBuilder:
     @property
     def shape_count(self):
         return len(self.shapes)
+
+    @property
+    def body_count(self):
+        return len(self.bodies)
 
     @property
     def spring_count(self):
@@ -654,14 +659,31 @@ class ModelBuilder:
                 h = mesh_hinges(self.tri_indices[t0:self._t])
                 self.add_edges(h[:, 0], h[:, 1], h[:, 2], h[:, 3], edge_ke=edge_ke, edge_kd=edge_kd)
 
-    # -- shapes (builder.py:5900-6470): static collision shapes for particle contacts
+    # -- bodies (builder.py:3814-3878): rigid bodies that carry collision shapes
+    def add_body(self, xform=None, armature=None, com=None, inertia=None, mass=0.0, label=None, lock_inertia=False,
+                 is_kinematic=False, custom_attributes=None) -> int:  # fmt: skip
+        """A rigid body at `xform` (world frame) that shapes can be attached to (``body=`` of the add_shape_*
+        methods, their xform then in the body's frame). Its motion comes from another solver: the cloth step
+        (``SolverVBD(..., integrate_with_external_rigid_solver=True)``) reads the bodies' transforms from
+        ``state_in.body_q`` and ``state_out.body_q`` and moves particle contacts with them. The mass properties are
+        kept as given; shapes added to the body do not change them (the reference adds their mass at the shape
+        density unless ``lock_inertia``), since the cloth step reads none of them."""
+        p, q = _xform(xform)
+        self.bodies.append(dict(q=tuple(p) + tuple(q), com=tuple(float(v) for v in (com or (0.0, 0.0, 0.0))),
+                                mass=float(mass),
+                                inertia=np.zeros((3, 3)) if inertia is None else np.asarray(inertia, float).reshape(3, 3),
+                                label=label, kinematic=bool(is_kinematic), world=self.current_world))  # fmt: skip
+        return len(self.bodies) - 1
+
+    # -- shapes (builder.py:5900-6470): collision shapes for particle contacts, static (body -1) or on a body
     def _add_shape(self, body, type_, xform, scale, cfg, src=None):
-        if body != -1:
-            raise NotImplementedError("only static shapes (body=-1) collide with particles here")
+        body = int(body)
+        if body < -1 or body >= len(self.bodies):
+            raise ValueError(f"body {body} does not exist (add_body first, or -1 for a static shape)")
         cfg = cfg or self.default_shape_cfg
         p, q = _xform(xform)
         self.shapes.append(dict(type=GeoType(type_), pos=p, rot=q, scale=tuple(float(v) for v in scale), ke=cfg.ke,
-                                kd=cfg.kd, mu=cfg.mu, body=-1, src=src, world=self.current_world,
+                                kd=cfg.kd, mu=cfg.mu, body=body, src=src, world=self.current_world,
                                 flags=4 if cfg.has_particle_collision else 0))  # fmt: skip
         return len(self.shapes) - 1
 
@@ -788,7 +810,9 @@ class ModelBuilder:
             self._tet_pose.append(builder.tet_poses)
             self._tet_mat.append(builder.tet_materials)
             self._tt += builder._tt
-        self.shapes.extend(dict(s, world=w) for s in builder.shapes)
+        b0 = len(self.bodies)
+        self.bodies.extend(dict(bd, world=w) for bd in builder.bodies)
+        self.shapes.extend(dict(s, world=w, body=s["body"] + b0 if s["body"] >= 0 else -1) for s in builder.shapes)
         translated = [_ChunkedGroup([c + start for c in g.chunks], g.size) for g in builder._color_groups]
         self._color_groups = _merge_chunked(self._color_groups, translated)
 
@@ -958,8 +982,21 @@ class Model:
                     if dev.type == "cuda":
                         m._device_meshes.append(_DeviceMesh(sh["src"]))
                 m.shape_mesh_index[i] = seen[key]
+        # bodies (model.py body_q / body_qd / body_com ...): transforms (p, q xyzw) and spatial velocities (v, w)
+        B = len(b.bodies)
+        m.body_count = B
+        m._shape_body_host = np.array([s["body"] for s in b.shapes], dtype=np.int32).reshape(S)
+        if B:
+            m.body_q = t(np.array([bd["q"] for bd in b.bodies], dtype=np.float64).reshape(B, 7), f32)
+            m.body_qd = torch.zeros((B, 6), dtype=torch.float32, device=dev)
+            m.body_com = t(np.array([bd["com"] for bd in b.bodies], dtype=np.float64).reshape(B, 3), f32)
+            m.body_mass = t(np.array([bd["mass"] for bd in b.bodies]).reshape(B), f32)
+            m.body_inertia = t(np.stack([bd["inertia"] for bd in b.bodies]).reshape(B, 3, 3), f32)
+            m.body_world = t(np.array([bd["world"] for bd in b.bodies], dtype=np.int32).reshape(B), i32)
+            m.body_label = [bd["label"] for bd in b.bodies]
+        else:
+            m.body_q = m.body_qd = m.body_com = None
         m._shape_set = _ShapeSet(m) if dev.type == "cuda" and S > 0 else None
-        m.body_com = None
         return m
 
     def refresh_shapes(self):
@@ -983,6 +1020,10 @@ class Model:
         s.particle_q = self.particle_q.clone()
         s.particle_qd = self.particle_qd.clone()
         s.particle_f = torch.zeros_like(self.particle_q)
+        if self.body_count:
+            s.body_q = self.body_q.clone()
+            s.body_qd = self.body_qd.clone()
+            s.body_f = torch.zeros_like(self.body_qd)
         return s
 
     def control(self, requires_grad=None, clone_variables=True) -> Control:
@@ -1019,7 +1060,7 @@ class State:
             self.particle_f.zero_()
 
     def assign(self, other: State):
-        for k in ("particle_q", "particle_qd", "particle_f"):
+        for k in ("particle_q", "particle_qd", "particle_f", "body_q", "body_qd", "body_f"):
             a, b = getattr(self, k), getattr(other, k)
             if a is not None and b is not None:
                 a.copy_(b)
@@ -1058,6 +1099,7 @@ def _shape_table(model: Model):
         hidx=np.ascontiguousarray(getattr(model, "shape_heightfield_index", np.full(S, -1)), dtype=np.int32),
         sfl=np.ascontiguousarray(getattr(model, "shape_flags", np.full(S, 4)), dtype=np.int32),
         swl=np.ascontiguousarray(getattr(model, "shape_world", np.full(S, -1)), dtype=np.int32),
+        sbd=np.ascontiguousarray(getattr(model, "_shape_body_host", np.full(S, -1)), dtype=np.int32),
     )  # fmt: skip
     rows = getattr(model, "heightfield_data", np.zeros((0, 7)))
     keep["hfs"] = hfs = (_lib.VbdHeightfield * max(len(rows), 1))()
@@ -1071,13 +1113,14 @@ def _shape_table(model: Model):
         S, keep["st"].ctypes.data_as(ip), keep["sx"].ctypes.data_as(fp), keep["ss"].ctypes.data_as(fp),
         keep["hidx"].ctypes.data_as(ip), len(rows), hfs, None if elev is None else elev.data_ptr(),
         0 if elev is None else elev.numel(), C.cast(handles, C.POINTER(C.c_void_p)), keep["sfl"].ctypes.data_as(ip),
-        keep["swl"].ctypes.data_as(ip), None,
+        keep["swl"].ctypes.data_as(ip), None, keep["sbd"].ctypes.data_as(ip), int(getattr(model, "body_count", 0)),
+        None,
     )  # fmt: skip
     return tb, keep
 
 
 _SHAPE_FIELDS = ("shape_type", "shape_transform", "shape_scale", "shape_flags", "shape_world", "shape_heightfield_index",
-                 "heightfield_data", "shape_mesh_index")  # fmt: skip
+                 "heightfield_data", "shape_mesh_index", "_shape_body_host")  # fmt: skip
 
 
 def _shape_fingerprint(model: Model):
@@ -1137,20 +1180,25 @@ def _current_shape_set(model: Model) -> _ShapeSet:
 
 
 def soft_contacts(model: Model, state: State, contacts: Contacts, margin: float):
-    """Particle contacts against the model's static shapes on the GPU (``vbd_soft_contacts_set``): any number of
-    shapes; a particle of world w meets the global shapes and world w's. Edits of the host shape arrays after
-    finalize take effect at the next call."""
+    """Particle contacts against the model's shapes on the GPU (``vbd_soft_contacts_set``): any number of shapes;
+    a particle of world w meets the global shapes and world w's; shapes on bodies move with ``state.body_q``. Edits
+    of the host shape arrays after finalize take effect at the next call."""
     lib = _lib.load()
     if model.shape_count == 0:
         contacts.soft_contact_count.zero_()
         return
     ss = _current_shape_set(model)
     pw = getattr(model, "particle_world", None)
+    bq = None
+    if getattr(model, "body_count", 0):
+        if getattr(state, "body_q", None) is None:
+            raise ValueError("the model has shapes on bodies: state.body_q must hold the body transforms")
+        bq = interop.pointer(state.body_q, "state.body_q", interop.F32, 7 * model.body_count)
     stream = torch.cuda.current_stream(model.device).cuda_stream
     with torch.cuda.device(model.device):
         rc = lib.vbd_soft_contacts_set(
             ss.handle, model.particle_count, state.particle_q.data_ptr(), model.particle_radius.data_ptr(),
-            model.particle_flags.data_ptr(), None if pw is None else pw.data_ptr(), float(margin),
+            model.particle_flags.data_ptr(), None if pw is None else pw.data_ptr(), bq, float(margin),
             contacts.soft_contact_max, contacts.soft_contact_count.data_ptr(), contacts.soft_contact_particle.data_ptr(),
             contacts.soft_contact_shape.data_ptr(), contacts.soft_contact_body_pos.data_ptr(),
             contacts.soft_contact_body_vel.data_ptr(), contacts.soft_contact_normal.data_ptr(), C.c_void_p(stream),

@@ -416,14 +416,63 @@ struct Model {
   const int *adj_tet_offsets, *adj_tets;    // reference layout: two ints (tet, order) per entry
 };
 
+// Particle-shape contacts, and the bodies that carry shapes: shape_body[s] (-1 = static; NULL = all static),
+// body_q / body_q_prev [B,7] (p, quat xyzw), body_qd [B,6] (linear, angular), body_com [B,3]; body_q_prev NULL
+// when the body velocity comes from body_qd.
 struct Contacts {
   int count, max;
   const int *particle, *shape;
   const double *body_pos, *body_vel, *normal;
+  const int* shape_body;
+  const double *body_q, *body_q_prev, *body_qd, *body_com;
 };
 
 template <typename R> inline V3<R> ld(const double* a, int i) { return {R(a[3 * i]), R(a[3 * i + 1]), R(a[3 * i + 2])}; }
 template <typename R> inline V3<R> ld(const std::vector<V3<R>>& a, int i) { return a[i]; }
+
+// v rotated by the unit quaternion q = (x, y, z, w) (wp.quat_rotate), in R.
+template <typename R> inline V3<R> quat_rotate(const double* q, V3<R> v) {
+  const V3<R> u = {R(q[0]), R(q[1]), R(q[2])};
+  const R w = R(q[3]);
+  return v * (R(2) * w * w - R(1)) + cross(u, v) * (R(2) * w) + u * (R(2) * dot(u, v));
+}
+
+// Body of contact c's shape, or -1.
+inline int contact_body(const Contacts& C, int c) { return C.shape_body && C.body_q ? C.shape_body[C.shape[c]] : -1; }
+
+// World position of contact c's point: transform_point(body_q[body], body_pos) (_eval_body_particle_contact,
+// rigid_vbd_kernels.py:790-799; update_duals_body_particle_contacts, rigid_vbd_kernels.py:3755-3799).
+template <typename R> inline V3<R> contact_point(const Contacts& C, int c) {
+  const V3<R> bp = ld<R>(C.body_pos, c);
+  const int b = contact_body(C, c);
+  if (b < 0) return bp;
+  const double* X = C.body_q + 7 * b;
+  return quat_rotate<R>(X + 3, bp) + V3<R>{R(X[0]), R(X[1]), R(X[2])};
+}
+
+// Velocity of contact c's point (rigid_vbd_kernels.py:806-819): from the body's motion over the step when
+// body_q_prev is given, else from its spatial velocity about its centre of mass; plus the contact's own velocity
+// rotated into world.
+template <typename R> inline V3<R> contact_velocity(const Contacts& C, int c, V3<R> bx, R dt) {
+  const V3<R> bvl = ld<R>(C.body_vel, c);
+  const int b = contact_body(C, c);
+  if (b < 0) return bvl;
+  const double* X = C.body_q + 7 * b;
+  const V3<R> vrot = quat_rotate<R>(X + 3, bvl);
+  if (C.body_q_prev) {
+    const double* Xp = C.body_q_prev + 7 * b;
+    const V3<R> bxp = quat_rotate<R>(Xp + 3, ld<R>(C.body_pos, c)) + V3<R>{R(Xp[0]), R(Xp[1]), R(Xp[2])};
+    return (bx - bxp) / dt + vrot;
+  }
+  const V3<R> com = C.body_com ? ld<R>(C.body_com, b) : V3<R>{R(0), R(0), R(0)};
+  const V3<R> r = bx - (quat_rotate<R>(X + 3, com) + V3<R>{R(X[0]), R(X[1]), R(X[2])});
+  V3<R> v = {R(0), R(0), R(0)}, w = {R(0), R(0), R(0)};
+  if (C.body_qd) {
+    v = V3<R>{R(C.body_qd[6 * b]), R(C.body_qd[6 * b + 1]), R(C.body_qd[6 * b + 2])};
+    w = V3<R>{R(C.body_qd[6 * b + 3]), R(C.body_qd[6 * b + 4]), R(C.body_qd[6 * b + 5])};
+  }
+  return v + cross(w, r) + vrot;
+}
 
 // ------------------------------------------------------------------------------------ self-contact
 // Closest point on triangle (a, b, c) to p, with the reference's branch order
@@ -1090,7 +1139,7 @@ int step(const Model& M, double* q_in, const double* qd_in, const double* f_ext,
     // update_duals_body_particle_contacts (rigid_vbd_kernels.py:3755-3799)
     for (int c = 0; c < ccount; ++c) {
       int p = Cn.particle[c];
-      V3<R> bx = ld<R>(Cn.body_pos, c), nn = ld<R>(Cn.normal, c);
+      V3<R> bx = contact_point<R>(Cn, c), nn = ld<R>(Cn.normal, c);
       R pen = -(dot(nn, pos[p] - bx) - R(M.radius[p]));
       pen = rmax(R(0), pen);
       pen_k[c] = rmin(pen_k[c] + beta * pen, mat_ke[c]);
@@ -1112,11 +1161,11 @@ int step(const Model& M, double* q_in, const double* qd_in, const double* f_ext,
       for (int c = 0; c < ccount; ++c) {
         int p = Cn.particle[c];
         if (M.particle_colors[p] != color) continue;
-        V3<R> bx = ld<R>(Cn.body_pos, c), nn = ld<R>(Cn.normal, c);
+        V3<R> bx = contact_point<R>(Cn, c), nn = ld<R>(Cn.normal, c);
         R pen = -(dot(nn, pos[p] - bx) - R(M.radius[p]));
         if (pen > R(0)) {
           V3<R> dx = pos[p] - q_prev[p];
-          V3<R> bv = ld<R>(Cn.body_vel, c);
+          V3<R> bv = contact_velocity<R>(Cn, c, bx, dt);
           V3<R> rel = dx - bv * dt;
           V3<R> f;
           M3<R> H;
@@ -1459,7 +1508,10 @@ struct OracleContacts {
   int count, max;
   const int *particle, *shape;
   const double *body_pos, *body_vel, *normal;
+  const int* shape_body;
+  const double *body_q, *body_q_prev, *body_qd, *body_com;
 };
+static_assert(sizeof(OracleContacts) == sizeof(Contacts), "layout");
 
 static_assert(sizeof(OracleModel) == sizeof(Model), "layout");
 
@@ -1469,7 +1521,8 @@ int oracle_vbd_step(const OracleModel* m, double* q_in, const double* qd_in, con
                     int nthreads) {
   Model M;
   std::memcpy(&M, m, sizeof(M));
-  Contacts C{c->count, c->max, c->particle, c->shape, c->body_pos, c->body_vel, c->normal};
+  Contacts C;
+  std::memcpy(&C, c, sizeof(C));
   if (nthreads < 1) nthreads = 1;
   if (precision == 64) return step<double>(M, q_in, qd_in, f_ext, C, dt, iterations, q_out, qd_out, nthreads);
   if (precision == 32)
@@ -1494,7 +1547,8 @@ int oracle_vbd_step_sc(const OracleModel* m, double* q_in, const double* qd_in, 
   std::memcpy(&M, m, sizeof(M));
   SelfContact S;
   std::memcpy(&S, sc, sizeof(S));
-  Contacts C{c->count, c->max, c->particle, c->shape, c->body_pos, c->body_vel, c->normal};
+  Contacts C;
+  std::memcpy(&C, c, sizeof(C));
   if (nthreads < 1) nthreads = 1;
   if (precision == 64) return step<double>(M, q_in, qd_in, f_ext, C, dt, iterations, q_out, qd_out, nthreads, &S);
   if (precision == 32)
@@ -1817,8 +1871,9 @@ int oracle_soft_contacts(int n, const double* q, const double* radius, const int
 }
 
 
-// shape_xform [S,7] = (position, quaternion xyzw), shape_scale [S,3]. Returns the number of contacts found,
-// or -1 for a shape type without an analytic SDF here.
+// shape_xform [S,7] = (position, quaternion xyzw) in the frame of body shape_body[s] (-1: world; shape_body or
+// body_q NULL: every shape static), body_q [B,7]; shape_scale [S,3]. Contact points are written in the body's
+// frame, normals in world. Returns the number of contacts found, or -1 for a shape type without an analytic SDF.
 // Heightfield shapes (type 2) take grid hf_index[s]: hf_grid[3k..] = (data_offset, nrow, ncol),
 // hf_ext[4k..] = (hx, hy, min_z, max_z) with the shape's scale applied, over the elevations `elev`.
 int oracle_soft_contacts_shapes(int n, const double* q, const double* radius, const int* flags, int S,
@@ -1827,7 +1882,8 @@ int oracle_soft_contacts_shapes(int n, const double* q, const double* radius, co
                                 const int* mesh_index, const int* mesh_vert_off, const int* mesh_tri_off,
                                 const double* mesh_pts, const int* mesh_tris, const int* shape_flags,
                                 const int* shape_world, const int* particle_world, double margin, int max_contacts,
-                                int* particle, int* shape, double* body_pos, double* body_vel, double* normal) {
+                                int* particle, int* shape, double* body_pos, double* body_vel, double* normal,
+                                const int* shape_body, const double* body_q) {
   using sdf::D3;
   for (int s = 0; s < S; ++s) {
     const int t = shape_type[s];
@@ -1847,10 +1903,21 @@ int oracle_soft_contacts_shapes(int n, const double* q, const double* radius, co
       if (shape_flags && !(shape_flags[s] & 4)) continue;  // COLLIDE_PARTICLES (geometry/kernels.py:1033-1034)
       const int pw = particle_world ? particle_world[i] : -1, sw = shape_world ? shape_world[s] : -1;
       if (pw != -1 && sw != -1 && pw != sw) continue;  // geometry/kernels.py:1036-1043
-      const double* X = shape_xform + 7 * s;
+      const double* X = shape_xform + 7 * s;  // X_bs
       const double* sc = shape_scale + 3 * s;
-      const double qi[4] = {-X[3], -X[4], -X[5], X[6]};
-      const D3 xl = sdf::qrot(qi, x - v3(X[0], X[1], X[2]));
+      // X_ws = body_q[body] X_bs (geometry/kernels.py:1045-1056)
+      double Xw[7] = {X[0], X[1], X[2], X[3], X[4], X[5], X[6]};
+      const int body = shape_body && body_q ? shape_body[s] : -1;
+      if (body >= 0) {
+        const double* B = body_q + 7 * body;
+        const D3 pw = sdf::qrot(B + 3, v3(X[0], X[1], X[2])) + v3(B[0], B[1], B[2]);
+        const double ax = B[3], ay = B[4], az = B[5], aw = B[6], bx = X[3], by = X[4], bz = X[5], bw = X[6];
+        const double qw[4] = {aw * bx + bw * ax + ay * bz - az * by, aw * by + bw * ay + az * bx - ax * bz,
+                              aw * bz + bw * az + ax * by - ay * bx, aw * bw - ax * bx - ay * by - az * bz};
+        Xw[0] = pw.x, Xw[1] = pw.y, Xw[2] = pw.z, Xw[3] = qw[0], Xw[4] = qw[1], Xw[5] = qw[2], Xw[6] = qw[3];
+      }
+      const double qi[4] = {-Xw[3], -Xw[4], -Xw[5], Xw[6]};
+      const D3 xl = sdf::qrot(qi, x - v3(Xw[0], Xw[1], Xw[2]));
       double d = 1.0e6;
       D3 nn = v3(0.0, 0.0, 0.0);
       switch (shape_type[s]) {
@@ -1884,8 +1951,8 @@ int oracle_soft_contacts_shapes(int n, const double* q, const double* radius, co
       }
       if (d < margin + radius[i]) {
         if (count < max_contacts) {
-          const D3 bp = sdf::qrot(X + 3, xl - nn * d) + v3(X[0], X[1], X[2]);
-          const D3 wn = sdf::qrot(X + 3, nn);
+          const D3 bp = sdf::qrot(X + 3, xl - nn * d) + v3(X[0], X[1], X[2]);  // body frame
+          const D3 wn = sdf::qrot(Xw + 3, nn);
           particle[count] = i;
           shape[count] = s;
           body_pos[3 * count] = bp.x, body_pos[3 * count + 1] = bp.y, body_pos[3 * count + 2] = bp.z;

@@ -42,7 +42,8 @@ class OracleModel(C.Structure):
 class OracleContacts(C.Structure):
     _fields_ = [
         ("count", C.c_int), ("max", C.c_int), ("particle", _ip), ("shape", _ip),
-        ("body_pos", _dp), ("body_vel", _dp), ("normal", _dp),
+        ("body_pos", _dp), ("body_vel", _dp), ("normal", _dp), ("shape_body", _ip), ("body_q", _dp),
+        ("body_q_prev", _dp), ("body_qd", _dp), ("body_com", _dp),
     ]  # fmt: skip
 
 
@@ -111,7 +112,7 @@ def lib():
         ]
         _lib.oracle_soft_contacts_shapes.argtypes = [
             C.c_int, _dp, _dp, _ip, C.c_int, _ip, _dp, _dp, _ip, _ip, _dp, _dp, _ip, _ip, _ip, _dp, _ip, _ip, _ip, _ip,
-            C.c_double, C.c_int, _ip, _ip, _dp, _dp, _dp,
+            C.c_double, C.c_int, _ip, _ip, _dp, _dp, _dp, _ip, _dp,
         ]  # fmt: skip
         _lib.oracle_max_threads.restype = C.c_int
         _lib.oracle_vbd_step_sc.argtypes = [
@@ -244,7 +245,11 @@ class Model:
             self.s.adj_tets = i("adj_tets")
 
 
-def make_contacts(count, particle, shape, body_pos, body_vel, normal):
+def make_contacts(count, particle, shape, body_pos, body_vel, normal, shape_body=None, body_q=None, body_q_prev=None,
+                  body_qd=None, body_com=None):  # fmt: skip
+    """Contacts for ``step``. With shapes on bodies: ``shape_body`` [S] (-1 = static) and the body arrays the step
+    reads (``body_q`` [B,7], ``body_q_prev`` [B,7] or None, ``body_qd`` [B,6], ``body_com`` [B,3]); contact
+    points are then in the body's frame."""
     keep = []
     p, pp = _i(particle)
     s, sp = _i(shape)
@@ -252,7 +257,19 @@ def make_contacts(count, particle, shape, body_pos, body_vel, normal):
     bv, bvp = _d(np.asarray(body_vel).reshape(-1))
     nn, nnp = _d(np.asarray(normal).reshape(-1))
     keep += [p, s, bp, bv, nn]
-    c = OracleContacts(count=int(count), max=len(p), particle=pp, shape=sp, body_pos=bpp, body_vel=bvp, normal=nnp)
+    extra = {}
+    if shape_body is not None and body_q is not None:
+        a, ap = _i(shape_body)
+        keep.append(a)
+        extra["shape_body"] = ap
+        for name, arr in (("body_q", body_q), ("body_q_prev", body_q_prev), ("body_qd", body_qd),
+                          ("body_com", body_com)):  # fmt: skip
+            if arr is not None:
+                a, ap = _d(np.asarray(arr).reshape(-1))
+                keep.append(a)
+                extra[name] = ap
+    c = OracleContacts(count=int(count), max=len(p), particle=pp, shape=sp, body_pos=bpp, body_vel=bvp, normal=nnp,
+                       **extra)  # fmt: skip
     return c, keep
 
 
@@ -301,14 +318,16 @@ def soft_contacts(q, radius, flags, shape_type, shape_pos, shape_radius, margin,
 
 def soft_contacts_shapes(q, radius, flags, shape_type, shape_transform, shape_scale, margin, max_contacts=None,
                          heightfield_index=None, heightfields=None, elevations=None, mesh_index=None, meshes=None,
-                         shape_flags=None, shape_world=None, particle_world=None):
+                         shape_flags=None, shape_world=None, particle_world=None, shape_body=None, body_q=None):
     """Particle-shape contacts against static analytic shapes (GeoType values: plane 1, heightfield 2, sphere 3,
     capsule 4, ellipsoid 5, cylinder 6, box 7, cone 9) with transforms [S, 7] (position, quaternion xyzw) and
     scales [S, 3], in (particle, shape) order, skipping shapes without the COLLIDE_PARTICLES flag (1 << 2) and
     pairs of different worlds unless either is global (-1). Heightfield shape s uses grid ``heightfield_index[s]`` of
     ``heightfields`` (rows of (data_offset, nrow, ncol, hx, hy, min_z, max_z), scale applied) over the
     concatenated normalized ``elevations``. Mesh shape s (types 8, 10) uses ``meshes[mesh_index[s]]``, a
-    (points [V, 3], triangles [T, 3]) pair."""
+    (points [V, 3], triangles [T, 3]) pair. A shape on a body (``shape_body[s]`` >= 0) has its transform in the frame
+    of ``body_q[shape_body[s]]`` (a [B, 7] array of (position, quaternion xyzw)); its contact points are returned in
+    that body's frame, as create_soft_contacts writes them."""
     n = len(radius)
     S = len(shape_type)
     max_contacts = max_contacts or n * max(S, 1)
@@ -340,9 +359,12 @@ def soft_contacts_shapes(q, radius, flags, shape_type, shape_transform, shape_sc
     sfl = None if shape_flags is None else _i(shape_flags)
     swl = None if shape_world is None else _i(shape_world)
     pwl = None if particle_world is None else _i(particle_world)
+    sbd = None if shape_body is None or body_q is None else _i(shape_body)
+    bq = None if shape_body is None or body_q is None else _d(np.asarray(body_q).reshape(-1))
     cnt = lib().oracle_soft_contacts_shapes(n, qp, rp, flp, S, stp, sxp, ssp, *(None if a is None else a[1] for a in
                                             (hfi, hfg, hfe, elv, mi, mvo, mto, mpt, mtr, sfl, swl, pwl)), margin,
-                                            max_contacts, pp, shpp, bpp, bvp, nnp)  # fmt: skip
+                                            max_contacts, pp, shpp, bpp, bvp, nnp, None if sbd is None else sbd[1],
+                                            None if bq is None else bq[1])  # fmt: skip
     if cnt < 0:
         raise ValueError("a shape type without an analytic SDF")
     return cnt, part, shp, bp.reshape(-1, 3), bv.reshape(-1, 3), nn.reshape(-1, 3)

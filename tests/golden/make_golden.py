@@ -582,9 +582,13 @@ class SelfContactRef:
 
 
 def ref_step(sc: RefScene, q_in, qd_in, f_ext, contacts, dt, iterations, friction_epsilon=1e-2, beta=0.0, selfc=None,
-             trace=None):  # fmt: skip
-    """One ``SolverVBD.step`` without rigid bodies (static shapes only); ``selfc`` turns self-contact on.
-    ``trace`` (a list) receives the collision buffers of every detection."""
+             trace=None, bodies=None):  # fmt: skip
+    """One ``SolverVBD.step``; ``selfc`` turns self-contact on. ``trace`` (a list) receives the collision buffers of
+    every detection. ``bodies``: shapes on bodies moved by an external rigid solver
+    (``integrate_with_external_rigid_solver=True``), a dict of ``shape_body`` [S], ``body_q_in`` / ``body_q_out``
+    (lists of (p, q xyzw)), ``body_qd_out`` [B, 6] and ``body_com`` [B, 3]: the contact kernels then read
+    ``state_out.body_q``, ``state_in.body_q`` as the previous pose and ``state_out.body_qd``
+    (solver_vbd.py:2157-2168, 2349-2374); without it every shape is static."""
     ns = sc.ns
     n = sc.n
     state_in_q = wp.vec_array(q_in)
@@ -609,6 +613,13 @@ def ref_step(sc: RefScene, q_in, qd_in, f_ext, contacts, dt, iterations, frictio
     mat_ke = wp.scalar_array(np.zeros(cmax))
     k_start = -1.0 if beta == 0.0 else 1.0e2
 
+    shape_body, body_q, body_q_prev, body_qd, body_com = sc.shape_body, sc.empty, None, sc.empty, sc.empty
+    if bodies is not None:
+        shape_body = wp.scalar_array(list(bodies["shape_body"]), int)
+        body_q = [(np.asarray(p, dtype=float), np.asarray(q, dtype=float)) for p, q in bodies["body_q_out"]]
+        body_q_prev = [(np.asarray(p, dtype=float), np.asarray(q, dtype=float)) for p, q in bodies["body_q_in"]]
+        body_qd = [wp.spatial_vector(*v) for v in np.asarray(bodies["body_qd_out"], dtype=float)]
+        body_com = wp.vec_array(np.asarray(bodies["body_com"], dtype=float).reshape(-1, 3))
     # _initialize_rigid_bodies -> init_body_particle_contacts (solver_vbd.py:2119-2149)
     wp.launch(
         ns["init_body_particle_contacts"], cmax, cnt, c_shape, sc.soft_ke, sc.soft_kd, sc.soft_mu,
@@ -651,7 +662,7 @@ def ref_step(sc: RefScene, q_in, qd_in, f_ext, contacts, dt, iterations, frictio
         # _solve_rigid_body_iteration with no bodies: dual update only (solver_vbd.py:2339-2376)
         wp.launch(
             ns["update_duals_body_particle_contacts"], cmax, cnt, c_particle, c_shape, c_body_pos, c_normal,
-            state_in_q, sc.radius, sc.shape_body, sc.empty, mat_ke, beta, pen_k,
+            state_in_q, sc.radius, shape_body, body_q, mat_ke, beta, pen_k,
         )  # fmt: skip
         # _solve_particle_iteration (solver_vbd.py:2151-2337)
         if selfc is not None and ((selfc.interval == 0 and _it == 0) or (selfc.interval >= 1 and _it % selfc.interval == 0)):
@@ -662,7 +673,7 @@ def ref_step(sc: RefScene, q_in, qd_in, f_ext, contacts, dt, iterations, frictio
             wp.launch(
                 ns["accumulate_particle_body_contact_force_and_hessian"], cmax, dt, color, q_prev, state_in_q,
                 sc.particle_colors, friction_epsilon, sc.radius, c_particle, cnt, cmax, pen_k, mat_kd, mat_mu,
-                sc.shape_mu, sc.shape_body, sc.empty, None, sc.empty, sc.empty, c_shape, c_body_pos, c_body_vel,
+                sc.shape_mu, shape_body, body_q, body_q_prev, body_qd, body_com, c_shape, c_body_pos, c_body_vel,
                 c_normal, forces, hessians,
             )  # fmt: skip
             if sc.spring_count:  # solver_vbd.py:2224-2243
@@ -720,7 +731,10 @@ def scene_grid(ns, *, dim, cell, pos, rot, vel, mass, mu, lam, tri_kd, edge_ke, 
 
 
 def run_scene(ns, name, b: FakeBuilder, *, gravity, soft, shapes, contact_fn, dt, iterations, substeps, seed, beta=0.0,
-              friction_epsilon=1e-2, f_ext_scale=0.0, self_contact=None, q_start=None, qd_start=None):  # fmt: skip
+              friction_epsilon=1e-2, f_ext_scale=0.0, self_contact=None, q_start=None, qd_start=None,
+              bodies=None):  # fmt: skip
+    """``bodies``: dict of ``shape_body``, ``body_com`` and ``motion(s) -> (body_q_in, body_q_out, body_qd_out)``
+    of substep s; ``contact_fn`` then also takes ``body_q_in`` (contacts are generated before the step)."""
     m = b.arrays()
     colors, groups = greedy_coloring(len(m["particle_q"]), m["tri_indices"], m["edge_indices"], m["edge_bending_properties"],
                                      m.get("tet_indices", ()), m.get("spring_indices", ()))  # fmt: skip
@@ -749,16 +763,29 @@ def run_scene(ns, name, b: FakeBuilder, *, gravity, soft, shapes, contact_fn, dt
         friction_epsilon=np.float64(friction_epsilon),
     )  # fmt: skip
     cmax = n * max(len(shapes), 1)
+    if bodies is not None:
+        out["shape_body"] = np.asarray(bodies["shape_body"], dtype=np.int32)
+        out["body_com"] = np.asarray(bodies["body_com"], dtype=np.float64).reshape(-1, 3)
     for s in range(substeps):
         f_ext = rng.normal(0.0, 1.0, size=(n, 3)) * f_ext_scale
-        contacts = contact_fn(q, m["particle_radius"], m["particle_flags"]) if contact_fn else []
+        step_bodies = None
+        if bodies is not None:
+            bq_in, bq_out, bqd_out = bodies["motion"](s)
+            step_bodies = dict(shape_body=bodies["shape_body"], body_q_in=bq_in, body_q_out=bq_out,
+                               body_qd_out=bqd_out, body_com=bodies["body_com"])  # fmt: skip
+            out[f"s{s}_body_q_in"] = np.array([list(p) + list(q) for p, q in bq_in], dtype=np.float64)
+            out[f"s{s}_body_q_out"] = np.array([list(p) + list(q) for p, q in bq_out], dtype=np.float64)
+            out[f"s{s}_body_qd_out"] = np.asarray(bqd_out, dtype=np.float64).reshape(-1, 6)
+            contacts = contact_fn(q, m["particle_radius"], m["particle_flags"], bq_in)
+        else:
+            contacts = contact_fn(q, m["particle_radius"], m["particle_flags"]) if contact_fn else []
         cnt, cp, cs, cbp, cbv, cn = contacts_to_arrays(contacts, cmax)
         out[f"s{s}_q_in"], out[f"s{s}_qd_in"], out[f"s{s}_f_ext"] = q.copy(), qd.copy(), f_ext
         out[f"s{s}_contact_count"], out[f"s{s}_contact_particle"], out[f"s{s}_contact_shape"] = cnt, cp, cs
         out[f"s{s}_contact_body_pos"], out[f"s{s}_contact_body_vel"], out[f"s{s}_contact_normal"] = cbp, cbv, cn
         trace = []
         q_in_after, q_out, qd_out = ref_step(sc, q, qd, f_ext, contacts, dt, iterations, friction_epsilon, beta, selfc,
-                                             trace)  # fmt: skip
+                                             trace, step_bodies)  # fmt: skip
         out[f"s{s}_q_in_after"], out[f"s{s}_q_out"], out[f"s{s}_qd_out"] = q_in_after, q_out, qd_out
         for k, rec in enumerate(trace):  # collision buffers of each detection of this substep
             for key, val in rec.items():
@@ -1093,6 +1120,76 @@ def create_soft_contacts_cases(ns, seed=23):
     )  # fmt: skip
 
 
+def run_create_soft_contacts(ns, q, radius, flags, shapes, body_q, margin):
+    """The reference's ``create_soft_contacts`` kernel run as-is (serially, in thread order) for global particles
+    against ``shapes`` = [(type, position, rotation, scale, body)] (transforms in the body's frame) with the body
+    transforms ``body_q`` = [(p, q xyzw)]: the contacts as (particle, shape, body_pos, body_vel, normal)."""
+    n, S = len(q), len(shapes)
+    cmax = n * S
+    count, tids = [0], [0] * (n * S)
+    out_p, out_s = [0] * cmax, [0] * cmax
+    out_bp, out_bv, out_n = [None] * cmax, [None] * cmax, [None] * cmax
+    xforms = [(np.asarray(sh[1], dtype=float), np.asarray(sh[2], dtype=float)) for sh in shapes]
+    wp.launch(ns["create_soft_contacts"], n * S, [wp.vec3(*x) for x in q], radius, flags, [-1] * n,
+              [(np.asarray(p, dtype=float), np.asarray(r, dtype=float)) for p, r in body_q], xforms,
+              [sh[4] for sh in shapes], [sh[0] for sh in shapes], [wp.vec3(*sh[3]) for sh in shapes], [0] * S,
+              [-1] * S, margin, cmax, S, [4] * S, [-1] * S, [], np.zeros(1), count, out_p, out_s, out_bp, out_bv,
+              out_n, tids)  # fmt: skip
+    k = count[0]
+    return [(out_p[i], out_s[i], np.asarray(out_bp[i]), np.asarray(out_bv[i]), np.asarray(out_n[i])) for i in range(k)]
+
+
+def create_soft_contacts_body_cases(ns, seed=29):
+    """``create_soft_contacts`` with shapes on two bodies (geometry/kernels.py:1045-1056, 1128-1140): each shape's
+    world frame is body_q[body] times its own transform; contact points come out in the body's frame and normals in
+    world. A static ground plane and sphere, box, capsule, cylinder, cone and ellipsoid on rotated, displaced
+    bodies; 1600 seeded global particles, some inactive."""
+    rng = np.random.default_rng(seed)
+
+    def quat(axis, ang):
+        return np.asarray(wp.quat_from_axis_angle(np.asarray(axis, dtype=float), ang), dtype=float)
+
+    body_q = [(np.array([0.1, -0.05, 0.2]), quat((0.3, 0.2, 1.0), 0.6)),
+              (np.array([-0.15, 0.1, 0.3]), quat((1.0, -0.4, 0.2), 1.2))]  # fmt: skip
+    shapes = [  # type, position, rotation, scale, body
+        (GEO_PLANE, (0.0, 0.0, 0.0), quat((0.0, 0.0, 1.0), 0.0), (0.0, 0.0, 0.0), -1),
+        (GEO_SPHERE, (0.05, 0.0, 0.02), quat((0.0, 0.0, 1.0), 0.0), (0.12, 0.0, 0.0), 0),
+        (GEO_BOX, (0.0, 0.1, -0.05), quat((0.2, 1.0, 0.3), 0.5), (0.1, 0.08, 0.06), 0),
+        (GEO_CAPSULE, (0.05, -0.05, 0.0), quat((1.0, 0.0, 0.2), 0.9), (0.05, 0.12, 0.0), 1),
+        (GEO_ELLIPSOID, (-0.05, 0.05, 0.05), quat((0.0, 1.0, 1.0), 0.4), (0.1, 0.07, 0.05), 1),
+        (GEO_CYLINDER, (0.1, 0.0, 0.1), quat((1.0, 1.0, 0.0), 0.3), (0.06, 0.08, 0.0), 1),
+        (GEO_CONE, (-0.1, -0.1, -0.05), quat((0.2, 1.0, 0.0), 0.8), (0.08, 0.1, 0.0), 0),
+    ]
+    n, margin = 1600, 0.02
+    q = np.stack([rng.uniform(-0.45, 0.45, n), rng.uniform(-0.45, 0.45, n), rng.uniform(-0.05, 0.55, n)], axis=1)
+    radius = rng.uniform(0.005, 0.02, n)
+    flags = np.where(rng.uniform(size=n) < 0.9, 1, 0).astype(np.int32)
+    c = run_create_soft_contacts(ns, q, radius, flags, shapes, body_q, margin)
+    return dict(
+        q=q, radius=radius, flags=flags, margin=np.float64(margin),
+        shape_type=np.array([sh[0] for sh in shapes], dtype=np.int32),
+        shape_transform=np.array([list(sh[1]) + list(sh[2]) for sh in shapes], dtype=np.float64),
+        shape_scale=np.array([sh[3] for sh in shapes], dtype=np.float64),
+        shape_body=np.array([sh[4] for sh in shapes], dtype=np.int32),
+        body_q=np.array([list(p) + list(r) for p, r in body_q], dtype=np.float64),
+        particle=np.array([x[0] for x in c], dtype=np.int32), shape=np.array([x[1] for x in c], dtype=np.int32),
+        body_pos=np.array([x[2] for x in c]).reshape(-1, 3), body_vel=np.array([x[3] for x in c]).reshape(-1, 3),
+        normal=np.array([x[4] for x in c]).reshape(-1, 3),
+    )  # fmt: skip
+
+
+def body_motion(p0, axis, w, v, dt):
+    """Pose of a body moving at constant linear velocity v and angular velocity w about a fixed axis from (p0, I):
+    motion(s) -> ([(p, q) at step s], [(p, q) at step s + 1], [(v, w axis)]) for one body."""
+    axis = np.asarray(axis, dtype=float) / np.linalg.norm(axis)
+
+    def pose(t):
+        return (np.asarray(p0, dtype=float) + np.asarray(v, dtype=float) * t,
+                np.asarray(wp.quat_from_axis_angle(axis, w * t), dtype=float))  # fmt: skip
+
+    return lambda s: (pose(s * dt), pose((s + 1) * dt), np.concatenate([np.asarray(v, dtype=float), axis * w]))
+
+
 def soft_cases(ns, seed=13):
     """Per-element goldens of the volumetric Neo-Hookean tetrahedron and of the spring."""
     rng = np.random.default_rng(seed)
@@ -1199,6 +1296,42 @@ def main():
     print("soft_contact_cone_hfield.npz written")
     np.savez_compressed(os.path.join(args.out, "create_soft_contacts.npz"), **create_soft_contacts_cases(ns))
     print("create_soft_contacts.npz written")
+    np.savez_compressed(os.path.join(args.out, "create_soft_contacts_bodies.npz"), **create_soft_contacts_body_cases(ns))
+    print("create_soft_contacts_bodies.npz written")
+
+    # A flat grid pressed onto a box and a sphere carried by two bodies that an external rigid solver moves
+    # (translating and turning) under it, over a static ground plane: contacts generated by create_soft_contacts
+    # from state_in.body_q, the step reading state_out.body_q, state_in.body_q and state_out.body_qd.
+    dt_b = 1.0 / 600.0
+    b = scene_grid(
+        ns, dim=7, cell=0.05, pos=(-0.175, -0.175, 0.204), rot=wp.quat_identity(), vel=(0.05, 0.0, -0.6), mass=1e-3,
+        mu=mu, lam=lam, tri_kd=0.0, edge_ke=1e-4, edge_kd=0.0, radius=5e-3, pinned=[],
+    )  # fmt: skip
+    moving = [body_motion((0.0, 0.0, 0.1), (0.0, 0.0, 1.0), 3.0, (0.4, 0.1, 0.5), dt_b),
+              body_motion((0.1, 0.1, 0.1), (1.0, 1.0, 0.0), -2.0, (-0.3, 0.2, 0.8), dt_b)]  # fmt: skip
+    body_shapes = [  # type, position, rotation, scale, body
+        (GEO_PLANE, (0.0, 0.0, 0.0), np.array([0.0, 0.0, 0.0, 1.0]), (0.0, 0.0, 0.0), -1),
+        (GEO_BOX, (0.0, -0.05, 0.05), np.asarray(wp.quat_from_axis_angle(np.array([0.0, 0.0, 1.0]), 0.3)),
+         (0.12, 0.1, 0.05), 0),
+        (GEO_SPHERE, (0.0, 0.0, 0.0), np.array([0.0, 0.0, 0.0, 1.0]), (0.1, 0.0, 0.0), 1),
+    ]  # fmt: skip
+
+    def motion(s):
+        parts = [m_(s) for m_ in moving]
+        return [p[0] for p in parts], [p[1] for p in parts], np.stack([p[2] for p in parts])
+
+    out = run_scene(
+        ns, "grid_bodies", b, gravity=(0.0, 0.0, -9.81), soft=(1.0e4, 1.0e-2, 0.5),
+        shapes=[(2.5e3, 1.0, 0.8), (5.0e3, 1.0, 0.6), (4.0e3, 2.0, 0.4)],
+        contact_fn=lambda q, r, f, bq: run_create_soft_contacts(ns, q, r, f, body_shapes, bq, 0.01), dt=dt_b,
+        iterations=5, substeps=3, seed=5,
+        bodies=dict(shape_body=[sh[4] for sh in body_shapes], body_com=[(0.01, 0.0, 0.0), (0.0, 0.0, 0.0)],
+                    motion=motion),
+    )  # fmt: skip
+    out["shape_type"] = np.array([sh[0] for sh in body_shapes], dtype=np.int32)
+    out["shape_transform"] = np.array([list(sh[1]) + list(sh[2]) for sh in body_shapes], dtype=np.float64)
+    out["shape_scale"] = np.array([sh[3] for sh in body_shapes], dtype=np.float64)
+    np.savez_compressed(os.path.join(args.out, "step_grid_bodies.npz"), **out)
     print("soft_elements.npz written")
 
     # Volumetric: a 3 x 2 x 2-cell tetrahedral block (add_soft_grid, 5 tetrahedra per cell, damped), 4 mm

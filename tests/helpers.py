@@ -57,6 +57,10 @@ def model_from_golden(g, device="cuda") -> sim.Model:
     m.shape_material_kd = t(shapes[:, 1], f32)
     m.shape_material_mu = t(shapes[:, 2], f32)
     m.shape_body = t(-np.ones(S), i32)
+    if "shape_body" in g:  # shapes on bodies that an external rigid solver moves
+        m.shape_body = t(g["shape_body"], i32)
+        m.body_com = t(np.asarray(g["body_com"]).reshape(-1, 3), f32)
+        m.body_count = len(m.body_com)
     m.world_particle_start = None
     if "model_spring_indices" in g:
         m.spring_count = len(g["model_spring_rest_length"])
@@ -70,6 +74,36 @@ def model_from_golden(g, device="cuda") -> sim.Model:
         m.tet_poses = t(g["model_tet_poses"], f32)
         m.tet_materials = t(g["model_tet_materials"], f32)
     return m
+
+
+def golden_solver_kw(g) -> dict:
+    """SolverVBD keywords a golden fixture needs: its bodies are moved by an external rigid solver."""
+    return dict(integrate_with_external_rigid_solver=True) if "shape_body" in g else {}
+
+
+def golden_body_states(g, s, st_in, st_out, device="cuda"):
+    """Substep s's body poses on the states (state_in.body_q, state_out.body_q, state_out.body_qd), if any."""
+    if "shape_body" not in g:
+        return
+    dev = torch.device(device)
+    st_in.body_q = torch.as_tensor(g[f"s{s}_body_q_in"], dtype=torch.float32, device=dev)
+    st_out.body_q = torch.as_tensor(g[f"s{s}_body_q_out"], dtype=torch.float32, device=dev)
+    st_in.body_qd = torch.zeros((len(st_in.body_q), 6), dtype=torch.float32, device=dev)
+    st_out.body_qd = torch.as_tensor(g[f"s{s}_body_qd_out"], dtype=torch.float32, device=dev)
+
+
+def golden_body_contacts_kw(g, s, fp32=False) -> dict:
+    """make_contacts keywords of substep s's bodies for the oracle (float32-rounded with fp32, as the GPU reads
+    them): the step reads state_out.body_q, state_in.body_q as the previous pose and state_out.body_qd."""
+    if "shape_body" not in g:
+        return {}
+
+    def r(a):
+        a = np.asarray(a, dtype=np.float64)
+        return a.astype(np.float32).astype(np.float64) if fp32 else a
+
+    return dict(shape_body=g["shape_body"], body_q=r(g[f"s{s}_body_q_out"]), body_q_prev=r(g[f"s{s}_body_q_in"]),
+                body_qd=r(g[f"s{s}_body_qd_out"]), body_com=r(g["body_com"]))  # fmt: skip
 
 
 def contacts_from_golden(g, s, device="cuda") -> sim.Contacts:

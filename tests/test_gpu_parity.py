@@ -13,11 +13,13 @@ import torch
 
 from newton_chysx_b200 import SolverVBD, _lib, sim
 from oracle import vbd_oracle as orc
-from tests.helpers import cloth_grid_builder, contacts_from_golden, load_golden, model_from_golden, oracle_model_dict
+from tests.helpers import (cloth_grid_builder, contacts_from_golden, golden_body_contacts_kw, golden_body_states,
+                           golden_solver_kw, load_golden, model_from_golden, oracle_model_dict)
 
 pytestmark = pytest.mark.gpu
 
-FIXTURES = ["step_grid_ground.npz", "step_grid_sphere.npz", "step_complex_rest_angle.npz"]
+# step_grid_bodies: shapes on two bodies moved by an external rigid solver (integrate_with_external_rigid_solver)
+FIXTURES = ["step_grid_ground.npz", "step_grid_sphere.npz", "step_complex_rest_angle.npz", "step_grid_bodies.npz"]
 # (schedule, lanes per vertex, positions in shared memory, element layout)
 LAUNCH = [("per_color", 1, "auto", "ell"), ("per_color", 1, "auto", "csr"), ("per_color", 4, "auto", "csr"),
           ("persistent", 1, "on", "ell"), ("persistent", 1, "off", "ell"), ("persistent", 1, "on", "csr"),
@@ -37,6 +39,7 @@ def _run_golden_substep(solver, g, s, dtype=torch.float32):
     st_in.particle_f = _state(g[f"s{s}_f_ext"], dtype)
     st_out.particle_q = torch.zeros_like(st_in.particle_q)
     st_out.particle_qd = torch.zeros_like(st_in.particle_qd)
+    golden_body_states(g, s, st_in, st_out)
     contacts = contacts_from_golden(g, s)
     solver.step(st_in, st_out, None, contacts, float(g["dt"]))
     torch.cuda.synchronize()
@@ -50,7 +53,7 @@ def test_fp32_step_matches_reference_goldens(name, schedule, lanes, shared, layo
     model = model_from_golden(g)
     solver = SolverVBD(model, iterations=int(g["iterations"]), friction_epsilon=float(g["friction_epsilon"]),
                        rigid_avbd_beta=float(g["beta"]), schedule=schedule, lanes_per_vertex=lanes,
-                       positions_in_shared=shared, layout=layout)  # fmt: skip
+                       positions_in_shared=shared, layout=layout, **golden_solver_kw(g))  # fmt: skip
     assert solver.schedule == schedule and solver.lanes_per_vertex == lanes and solver.layout == layout
     assert (solver.shared_bytes > 0) == (schedule == "persistent" and shared == "on")
     for s in range(int(g["substeps"])):
@@ -141,14 +144,16 @@ def test_fp64_step_matches_fp64_oracle(name, schedule, layout):
     g = load_golden(name)
     model = model_from_golden(g)
     solver = SolverVBD(model, iterations=int(g["iterations"]), friction_epsilon=float(g["friction_epsilon"]),
-                       rigid_avbd_beta=float(g["beta"]), precision="fp64", schedule=schedule, layout=layout)  # fmt: skip
+                       rigid_avbd_beta=float(g["beta"]), precision="fp64", schedule=schedule, layout=layout,
+                       **golden_solver_kw(g))  # fmt: skip
     om = orc.Model(oracle_model_dict(model, float(g["friction_epsilon"]), float(g["beta"])))
     for s in range(int(g["substeps"])):
         st_in, st_out = _run_golden_substep(solver, g, s, torch.float64)
         c = contacts_from_golden(g, s)
         oc = orc.make_contacts(int(c.soft_contact_count.item()), c.soft_contact_particle.cpu().numpy(),
                                c.soft_contact_shape.cpu().numpy(), c.soft_contact_body_pos.cpu().numpy(),
-                               c.soft_contact_body_vel.cpu().numpy(), c.soft_contact_normal.cpu().numpy())  # fmt: skip
+                               c.soft_contact_body_vel.cpu().numpy(), c.soft_contact_normal.cpu().numpy(),
+                               **golden_body_contacts_kw(g, s, fp32=True))  # fmt: skip
         _, q_o, qd_o = orc.step(om, g[f"s{s}_q_in"], g[f"s{s}_qd_in"], g[f"s{s}_f_ext"], oc, float(g["dt"]),
                                 int(g["iterations"]), precision=64)  # fmt: skip
         assert np.abs(st_out.particle_q.cpu().numpy() - q_o).max() <= 1e-9

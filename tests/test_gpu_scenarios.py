@@ -165,6 +165,79 @@ def test_hanging_cloth_fp32_per_substep_full_horizon():
     assert max(err[5:]) > 0.0  # contact frames were compared, not an idle sheet
 
 
+def test_cloth_on_a_moving_body_matches_oracle():
+    """A 16 x 16 sheet (0.5 m) dropped onto a box carried by a body that turns (3 rad/s about z) and rises
+    (0.2 m/s) under it, moved by the test as an external rigid solver would: contacts from
+    ``CollisionPipeline.collide`` at ``state_in.body_q``, the step with ``integrate_with_external_rigid_solver=True``
+    reading ``state_out.body_q``, ``state_in.body_q`` and ``state_out.body_qd``. Along the FP64 trajectory, every
+    substep against the FP64 oracle's substep from the same state, contacts and body poses: FP64 <= 1e-9 m, the
+    mixed mode (contact vertices in FP64) <= 1e-4 m. FP32 is held to 1e-3 m only: the contact damping
+    kd ke / dt = 2.3e6 N/m against the sheet's ~1 N/m tangential stiffness cost FP32 1.6e-4 m along its own
+    trajectory."""
+    b = cloth_grid_builder(n=16, side=0.5, hanging=False, height=0.262, pin_top_corners=False)
+    body = b.add_body(xform=((0.25, 0.25, 0.1), sim.quat_identity()))
+    b.add_shape_box(body=body, xform=((0.0, 0.0, 0.05), sim.quat_from_axis_angle((0.0, 0.0, 1.0), 0.2)), hx=0.15,
+                    hy=0.12, hz=0.1, cfg=sim.ShapeConfig(ke=5.0e3, kd=1.0, mu=0.6))  # fmt: skip
+    b.add_ground_plane()
+    model = b.finalize("cuda")
+    model.soft_contact_ke, model.soft_contact_kd, model.soft_contact_mu = 1.0e4, 1.0e-2, 0.5
+    solvers = {p: SolverVBD(model, iterations=10, precision=p, integrate_with_external_rigid_solver=True)
+               for p in ("fp32", "mixed", "fp64")}  # fmt: skip
+    pipe = CollisionPipeline(model, soft_contact_margin=0.01)
+    c = pipe.contacts()
+    om = orc.Model(oracle_model_dict(model))
+    sb = model._shape_body_host
+    com = model.body_com.cpu().numpy().astype(np.float64)
+    dt, w, v = 1.0 / 600.0, 3.0, np.array([0.0, 0.0, 0.2])
+
+    def pose(t):
+        return np.concatenate([np.array([0.25, 0.25, 0.1]) + v * t, sim.quat_from_axis_angle((0.0, 0.0, 1.0), w * t)])
+
+    q = model.particle_q.cpu().numpy().astype(np.float64)
+    qd = model.particle_qd.cpu().numpy().astype(np.float64)
+    err = {p: [] for p in solvers}
+    touching = 0
+    for k in range(40):
+        X0 = pose(k * dt).astype(np.float32)[None]
+        X1 = pose((k + 1) * dt).astype(np.float32)[None]
+        body_qd = np.concatenate([v, [0.0, 0.0, w]]).astype(np.float32)[None]
+        view = sim.State()
+        view.particle_q = torch.as_tensor(q.astype(np.float32), device="cuda")
+        view.body_q = torch.as_tensor(X0, device="cuda")
+        pipe.collide(view, c)  # contacts from the FP32 positions, for every precision
+        cnt = int(c.soft_contact_count.item())
+        touching += int((sb[c.soft_contact_shape[:cnt].cpu().numpy()] == 0).sum())
+        oc = orc.make_contacts(cnt, c.soft_contact_particle.cpu().numpy(), c.soft_contact_shape.cpu().numpy(),
+                               c.soft_contact_body_pos.cpu().numpy(), c.soft_contact_body_vel.cpu().numpy(),
+                               c.soft_contact_normal.cpu().numpy(), shape_body=sb, body_q=X1.astype(np.float64),
+                               body_q_prev=X0.astype(np.float64), body_qd=body_qd.astype(np.float64),
+                               body_com=com)  # fmt: skip
+        out = {}
+        for p, solver in solvers.items():
+            dtype = torch.float64 if p == "fp64" else torch.float32
+            s_in, s_out = sim.State(), sim.State()
+            src_q = q if p == "fp64" else q.astype(np.float32)
+            src_qd = qd if p == "fp64" else qd.astype(np.float32)
+            s_in.particle_q = torch.as_tensor(src_q, dtype=dtype, device="cuda")
+            s_in.particle_qd = torch.as_tensor(src_qd, dtype=dtype, device="cuda")
+            s_in.particle_f = torch.zeros_like(s_in.particle_q)
+            s_out.particle_q, s_out.particle_qd = torch.zeros_like(s_in.particle_q), torch.zeros_like(s_in.particle_q)
+            s_in.body_q, s_out.body_q = torch.as_tensor(X0, device="cuda"), torch.as_tensor(X1, device="cuda")
+            s_in.body_qd = torch.zeros_like(torch.as_tensor(body_qd, device="cuda"))
+            s_out.body_qd = torch.as_tensor(body_qd, device="cuda")
+            solver.step(s_in, s_out, None, c, dt)
+            out[p] = (s_out.particle_q.cpu().numpy().astype(np.float64), s_out.particle_qd.cpu().numpy())
+            _, q_ref, _ = orc.step(om, np.asarray(src_q, np.float64), np.asarray(src_qd, np.float64), None, oc, dt, 10,
+                                   precision=64, nthreads=orc.max_threads())  # fmt: skip
+            err[p].append(float(np.linalg.norm(out[p][0] - q_ref, axis=1).max()))
+        q, qd = out["fp64"][0], out["fp64"][1].astype(np.float64)
+    assert all(s.device_errors() == 0 for s in solvers.values())
+    assert touching > 0  # the body's box was in contact
+    assert max(err["fp64"]) <= 1e-9, max(err["fp64"])
+    assert max(err["mixed"]) <= 1e-4, max(err["mixed"])
+    assert max(err["fp32"]) <= 1e-3, max(err["fp32"])
+
+
 def test_free_fall_matches_kinematics():
     """test_cloth.py:1093-1114: an unconstrained sheet falls as 1/2 g t^2 with no horizontal drift."""
     b = cloth_grid_builder(n=16, hanging=False, pin_top_corners=False, height=4.0, up_axis="Y")

@@ -519,7 +519,7 @@ def test_reference_create_soft_contacts_kernel_golden(path):
         _lib.check(lib.vbd_shape_set_create(C.byref(tb), C.byref(h)), "vbd_shape_set_create")
         if path == "set_global":
             _lib.check(lib.vbd_shape_set_use_parameter_table(h, 0), "vbd_shape_set_use_parameter_table")
-        rc = lib.vbd_soft_contacts_set(h, n, qd.data_ptr(), rd.data_ptr(), fd.data_ptr(), pw.data_ptr(),
+        rc = lib.vbd_soft_contacts_set(h, n, qd.data_ptr(), rd.data_ptr(), fd.data_ptr(), pw.data_ptr(), None,
                                        float(g["margin"]), *outs)  # fmt: skip
         _lib.check(rc, "vbd_soft_contacts_set")
         torch.cuda.synchronize()
@@ -537,6 +537,104 @@ def test_reference_create_soft_contacts_kernel_golden(path):
     near -= set(zip(lo[1][:lo[0]].tolist(), lo[2][:lo[0]].tolist()))
     pairs = list(zip(g["particle"].tolist(), g["shape"].tolist()))
     _compare(gpu, pairs, g["body_pos"], g["normal"], near)
+
+
+@pytest.mark.parametrize("path", ["table", "set", "set_global", "pipeline"])
+def test_reference_create_soft_contacts_on_bodies(path):
+    """Shapes on two rotated, displaced bodies against the reference's ``create_soft_contacts`` run as-is: each
+    shape's world frame is body_q[body] times its own transform, contact points come out in the body's frame and
+    normals in world. "table" and "set"/"set_global" call the C ABI (the body transforms in the table, or per call
+    for a set); "pipeline" builds the scene with ``ModelBuilder.add_body`` and runs ``CollisionPipeline.collide``
+    on a state whose ``body_q`` holds the transforms."""
+    g = load_golden("create_soft_contacts_bodies.npz")
+    lib = _lib.load()
+    dev = torch.device("cuda")
+    n, S = len(g["radius"]), len(g["shape_type"])
+    cmax = n * S
+    bq = torch.as_tensor(g["body_q"].astype(np.float32), device=dev).contiguous()
+    if path == "pipeline":
+        b = sim.ModelBuilder(up_axis="Z", gravity=-9.81)
+        b.add_particles(g["q"], (0.0, 0.0, 0.0), 1.0, g["radius"], g["flags"])
+        bodies = [b.add_body() for _ in g["body_q"]]  # at the origin: the state's body_q moves them
+        kinds = {1: "plane", 3: "sphere", 4: "capsule", 5: "ellipsoid", 6: "cylinder", 7: "box", 9: "cone"}
+        for t, X, sc, body in zip(g["shape_type"], g["shape_transform"], g["shape_scale"], g["shape_body"]):
+            xf = (tuple(X[:3]), tuple(X[3:]))
+            bd = -1 if body < 0 else bodies[body]
+            k = kinds[int(t)]
+            if k == "plane":
+                b.add_shape_plane(xform=xf, width=0.0, length=0.0, body=bd)
+            elif k == "sphere":
+                b.add_shape_sphere(body=bd, xform=xf, radius=float(sc[0]))
+            elif k == "box":
+                b.add_shape_box(body=bd, xform=xf, hx=float(sc[0]), hy=float(sc[1]), hz=float(sc[2]))
+            elif k == "ellipsoid":
+                b.add_shape_ellipsoid(body=bd, xform=xf, rx=float(sc[0]), ry=float(sc[1]), rz=float(sc[2]))
+            else:
+                getattr(b, f"add_shape_{k}")(body=bd, xform=xf, radius=float(sc[0]), half_height=float(sc[1]))
+        m = b.finalize("cuda")
+        assert m.body_count == 2 and np.array_equal(m._shape_body_host, g["shape_body"])
+        np.testing.assert_allclose(m.shape_scale, g["shape_scale"], atol=1e-7)
+        state = m.state()
+        state.body_q.copy_(bq)
+        pipe = sim.CollisionPipeline(m, soft_contact_margin=float(g["margin"]))
+        c = pipe.contacts()
+        pipe.collide(state, c)
+        torch.cuda.synchronize()
+        k = int(c.soft_contact_count.item())
+        part, shp, bp, bv, nn = (c.soft_contact_particle, c.soft_contact_shape, c.soft_contact_body_pos,
+                                 c.soft_contact_body_vel, c.soft_contact_normal)  # fmt: skip
+        with pytest.raises(ValueError, match="body_q"):
+            pipe.collide(_no_bodies(state), c)
+    else:
+        qd = torch.as_tensor(g["q"].astype(np.float32), device=dev).contiguous()
+        rd = torch.as_tensor(g["radius"].astype(np.float32), device=dev)
+        fd = torch.as_tensor(g["flags"], device=dev)
+        cnt = torch.zeros(1, dtype=torch.int32, device=dev)
+        part = torch.full((cmax,), -1, dtype=torch.int32, device=dev)
+        shp = torch.full((cmax,), -1, dtype=torch.int32, device=dev)
+        bp, bv, nn = (torch.zeros((cmax, 3), dtype=torch.float32, device=dev) for _ in range(3))
+        ip, fp = C.POINTER(C.c_int32), C.POINTER(C.c_float)
+        arrs = dict(st=g["shape_type"].astype(np.int32), sx=g["shape_transform"].astype(np.float32),
+                    ss=g["shape_scale"].astype(np.float32), sb=g["shape_body"].astype(np.int32))  # fmt: skip
+        tb = _lib.VbdShapeTable(S, arrs["st"].ctypes.data_as(ip), arrs["sx"].ctypes.data_as(fp),
+                                arrs["ss"].ctypes.data_as(fp), None, 0, None, None, 0, None, None, None, None,
+                                arrs["sb"].ctypes.data_as(ip), 2, bq.data_ptr())  # fmt: skip
+        outs = (cmax, cnt.data_ptr(), part.data_ptr(), shp.data_ptr(), bp.data_ptr(), bv.data_ptr(), nn.data_ptr(),
+                None)  # fmt: skip
+        if path == "table":
+            _lib.check(lib.vbd_soft_contacts_table(n, qd.data_ptr(), rd.data_ptr(), fd.data_ptr(), C.byref(tb),
+                                                   float(g["margin"]), *outs), "vbd_soft_contacts_table")  # fmt: skip
+        else:
+            h = C.c_void_p()
+            _lib.check(lib.vbd_shape_set_create(C.byref(tb), C.byref(h)), "vbd_shape_set_create")
+            if path == "set_global":
+                _lib.check(lib.vbd_shape_set_use_parameter_table(h, 0), "vbd_shape_set_use_parameter_table")
+            # a set with shapes on bodies needs the transforms of the call
+            assert lib.vbd_soft_contacts_set(h, n, qd.data_ptr(), rd.data_ptr(), fd.data_ptr(), None, None,
+                                             float(g["margin"]), *outs) == _lib.VBD_ERR_INVALID_ARGUMENT  # fmt: skip
+            _lib.check(lib.vbd_soft_contacts_set(h, n, qd.data_ptr(), rd.data_ptr(), fd.data_ptr(), None,
+                                                 bq.data_ptr(), float(g["margin"]), *outs),
+                       "vbd_soft_contacts_set")  # fmt: skip
+            torch.cuda.synchronize()
+            lib.vbd_shape_set_destroy(h)
+        torch.cuda.synchronize()
+        k = int(cnt.item())
+    gpu = {(int(a), int(b_)): (x, y, z) for a, b_, x, y, z in zip(
+        part[:k].cpu().numpy(), shp[:k].cpu().numpy(), bp[:k].cpu().numpy(), bv[:k].cpu().numpy(),
+        nn[:k].cpu().numpy())}  # fmt: skip
+    kw = dict(shape_body=g["shape_body"], body_q=g["body_q"].astype(np.float32).astype(np.float64))
+    args = (g["q"], g["radius"], g["flags"], g["shape_type"], g["shape_transform"], g["shape_scale"])
+    lo = orc.soft_contacts_shapes(*args, float(g["margin"]) - 1e-5, **kw)
+    hi_ = orc.soft_contacts_shapes(*args, float(g["margin"]) + 1e-5, **kw)
+    near = set(zip(hi_[1][:hi_[0]].tolist(), hi_[2][:hi_[0]].tolist()))
+    near -= set(zip(lo[1][:lo[0]].tolist(), lo[2][:lo[0]].tolist()))
+    _compare(gpu, list(zip(g["particle"].tolist(), g["shape"].tolist())), g["body_pos"], g["normal"], near)
+
+
+def _no_bodies(state):
+    s = sim.State()
+    s.particle_q = state.particle_q
+    return s
 
 
 @pytest.mark.parametrize("param_table", [True, False])

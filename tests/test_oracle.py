@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 from oracle import vbd_oracle as orc
+from tests.helpers import golden_body_contacts_kw
 
 
 def _load(golden_dir, name):
@@ -67,7 +68,7 @@ def _model_from_golden(g):
     return m
 
 
-STEP_FIXTURES = ["step_grid_ground.npz", "step_grid_sphere.npz", "step_complex_rest_angle.npz"]
+STEP_FIXTURES = ["step_grid_ground.npz", "step_grid_sphere.npz", "step_complex_rest_angle.npz", "step_grid_bodies.npz"]
 
 
 @pytest.mark.parametrize("name", STEP_FIXTURES)
@@ -90,6 +91,7 @@ def test_step_matches_reference(golden_dir, name, precision, tol):
         contacts = orc.make_contacts(
             g[f"s{s}_contact_count"], g[f"s{s}_contact_particle"], g[f"s{s}_contact_shape"],
             g[f"s{s}_contact_body_pos"], g[f"s{s}_contact_body_vel"], g[f"s{s}_contact_normal"],
+            **golden_body_contacts_kw(g, s),
         )  # fmt: skip
         q_after, q_out, qd_out = orc.step(
             model, g[f"s{s}_q_in"], g[f"s{s}_qd_in"], g[f"s{s}_f_ext"], contacts, float(g["dt"]),

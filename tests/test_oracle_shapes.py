@@ -201,3 +201,24 @@ def test_oracle_matches_reference_create_soft_contacts_kernel():
     pw, sw = g["particle_world"][g["particle"]], g["shape_world"][g["shape"]]
     assert 5 not in set(g["shape"].tolist())
     assert ((pw == -1) | (sw == -1) | (pw == sw)).all() and ((pw == -1) & (sw >= 0)).any()
+
+
+def test_oracle_matches_reference_create_soft_contacts_on_bodies():
+    """``create_soft_contacts`` with shapes on two rotated, displaced bodies (geometry/kernels.py:1045-1056,
+    1128-1140), run as-is: the oracle composes body_q[body] with the shape's own transform, writes contact points in
+    the body's frame and normals in world, entry by entry in thread order."""
+    g = load_golden("create_soft_contacts_bodies.npz")
+    cnt, p, s, bp, bv, nn = orc.soft_contacts_shapes(
+        g["q"], g["radius"], g["flags"], g["shape_type"], g["shape_transform"], g["shape_scale"], float(g["margin"]),
+        shape_body=g["shape_body"], body_q=g["body_q"])  # fmt: skip
+    assert cnt == len(g["particle"]) and cnt > 300
+    np.testing.assert_array_equal(p[:cnt], g["particle"])
+    np.testing.assert_array_equal(s[:cnt], g["shape"])
+    assert np.abs(bp[:cnt] - g["body_pos"]).max() <= 1e-12
+    assert np.abs(nn[:cnt] - g["normal"]).max() <= 1e-12
+    # every body shape is touched, and its contact points are in the body frame, not in world
+    assert set(g["shape"].tolist()) == set(range(len(g["shape_type"])))
+    on_body = g["shape_body"][g["shape"]] >= 0
+    static = orc.soft_contacts_shapes(g["q"], g["radius"], g["flags"], g["shape_type"], g["shape_transform"],
+                                      g["shape_scale"], float(g["margin"]))  # fmt: skip
+    assert on_body.any() and static[0] != cnt
