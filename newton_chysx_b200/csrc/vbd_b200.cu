@@ -2166,7 +2166,9 @@ int vbd_soft_contacts_table(int32_t n, const float* q, const float* radius, cons
     bodies = bodies || tab.rec[s].body >= 0;
   }
   if (bodies && !tb->body_q_dev) return VBD_ERR_INVALID_ARGUMENT;
-  auto kern = worlds && tb->particle_world_dev ? k_soft_contacts_shapes<true> : k_soft_contacts_shapes<false>;
+  const bool w = worlds && tb->particle_world_dev;
+  auto kern = bodies ? (w ? k_soft_contacts_shapes<true, true> : k_soft_contacts_shapes<false, true>)
+                     : (w ? k_soft_contacts_shapes<true, false> : k_soft_contacts_shapes<false, false>);
   kern<<<(n + 255) / 256, 256, 0, st>>>(n, q, radius, flags, m, tab, tb->elevations_dev, tb->particle_world_dev,
                                          tb->body_q_dev, margin, cmax, count, particle, shape, body_pos, body_vel,
                                          normal);

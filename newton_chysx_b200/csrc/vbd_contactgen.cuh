@@ -39,14 +39,16 @@ __host__ __device__ __forceinline__ float4 mul_q(float4 a, float4 b) {
                      a.w * b.z + b.w * a.z + a.x * b.y - a.y * b.x, a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z);
 }
 
-// body_q: [bodies, 7] body transforms (p, q xyzw) of this call; read only for a shape on a body.
+// body_q: [bodies, 7] body transforms (p, q xyzw) of this call; read only for a shape on a body. BODIES = false
+// compiles the body frame out (every shape of the launch is static).
+template <bool BODIES>
 __device__ __forceinline__ void soft_contact_shape(const ShapeRec& sh, const float* __restrict__ elev,
                                                    const float* __restrict__ body_q, vec3<float> x, float r,
                                                    float margin, int i, int cmax, int* count, int* particle,
                                                    int* shape, float* body_pos, float* body_vel, float* normal) {
   const float4 P = sh.p, Q = sh.q, SC = sh.sc;
   float4 Pw = P, Qw = Q;  // X_ws
-  if (sh.body >= 0) {
+  if (BODIES && sh.body >= 0) {
     const float* X = body_q + 7 * sh.body;
     const float4 Qb = make_float4(X[3], X[4], X[5], X[6]);
     const vec3<float> pw = rot_q(Qb, vec3<float>{P.x, P.y, P.z});
@@ -100,8 +102,9 @@ struct ShapeParamTable {
 // create_soft_contacts (geometry/kernels.py:1001-1140) over a parameter table: one thread per particle, looping over
 // the shapes (the reference launches one thread per (particle, shape); here the shape, hence the branch taken, is
 // the same across a warp). WORLDS: some shape belongs to a world (else the world filter can never apply and is
-// compiled out). Four 256-thread CTAs per SM: the loop is latency-bound, and 4 resident CTAs ran faster than 3.
-template <bool WORLDS>
+// compiled out); BODIES: some shape is on a body. Four 256-thread CTAs per SM: the loop is latency-bound, and 4
+// resident CTAs ran faster than 3.
+template <bool WORLDS, bool BODIES>
 __global__ void __launch_bounds__(256, 4)
     k_soft_contacts_shapes(int n, const float* __restrict__ q, const float* __restrict__ radius,
                            const int* __restrict__ flags, int S, const ShapeParamTable shapes,
@@ -118,8 +121,8 @@ __global__ void __launch_bounds__(256, 4)
       const int sw = shapes.rec[s].world;
       if (pw != -1 && sw != -1 && pw != sw) continue;
     }
-    soft_contact_shape(shapes.rec[s], elev, body_q, x, r, margin, i, cmax, count, particle, shape, body_pos,
-                       body_vel, normal);
+    soft_contact_shape<BODIES>(shapes.rec[s], elev, body_q, x, r, margin, i, cmax, count, particle, shape, body_pos,
+                               body_vel, normal);
   }
 }
 

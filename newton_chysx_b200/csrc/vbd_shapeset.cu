@@ -30,6 +30,7 @@ struct VbdShapeSetImpl {
 
 namespace {
 
+template <bool BODIES>
 __global__ void __launch_bounds__(256, 4)
     k_soft_contacts_set(int n, const float* __restrict__ q, const float* __restrict__ radius,
                         const int* __restrict__ flags, const int* __restrict__ particle_world,
@@ -48,8 +49,8 @@ __global__ void __launch_bounds__(256, 4)
   const int w0 = own ? world_off[pw] : 0, nb = own ? world_off[pw + 1] - w0 : 0;
   for (int k = 0; k < na + nb; ++k) {
     const int s = k < na ? (pw == -1 ? k : global[k]) : world_list[w0 + k - na];
-    vbd::soft_contact_shape(recs[s], elev, body_q, x, r, margin, i, cmax, count, particle, shape, body_pos, body_vel,
-                            normal);
+    vbd::soft_contact_shape<BODIES>(recs[s], elev, body_q, x, r, margin, i, cmax, count, particle, shape, body_pos,
+                                    body_vel, normal);
   }
 }
 
@@ -149,15 +150,17 @@ int vbd_soft_contacts_set(VbdShapeSetHandle set, int32_t n, const float* q, cons
   if (cudaMemsetAsync(count, 0, sizeof(int), st) != cudaSuccess) return VBD_ERR_CUDA;
   if (n == 0 || set->m == 0) return VBD_OK;
   if (set->param_table && set->m <= vbd::kParamTableShapes) {  // small sets: records in the constant bank measured faster
-    auto kern = set->worlds && particle_world ? vbd::k_soft_contacts_shapes<true> : vbd::k_soft_contacts_shapes<false>;
+    const bool w = set->worlds && particle_world;
+    auto kern = set->bodies ? (w ? vbd::k_soft_contacts_shapes<true, true> : vbd::k_soft_contacts_shapes<false, true>)
+                            : (w ? vbd::k_soft_contacts_shapes<true, false> : vbd::k_soft_contacts_shapes<false, false>);
     kern<<<(n + 255) / 256, 256, 0, st>>>(n, q, radius, flags, set->m, set->small, set->elev, particle_world, body_q,
                                            margin, cmax, count, particle, shape, body_pos, body_vel, normal);
     return cudaGetLastError() == cudaSuccess ? VBD_OK : VBD_ERR_CUDA;
   }
-  k_soft_contacts_set<<<(n + 255) / 256, 256, 0, st>>>(n, q, radius, flags, particle_world, set->recs, set->m,
-                                                       set->global, set->n_global, set->world_off, set->world_list,
-                                                       set->W, set->elev, body_q, margin, cmax, count, particle,
-                                                       shape, body_pos, body_vel, normal);
+  auto kset = set->bodies ? k_soft_contacts_set<true> : k_soft_contacts_set<false>;
+  kset<<<(n + 255) / 256, 256, 0, st>>>(n, q, radius, flags, particle_world, set->recs, set->m, set->global,
+                                         set->n_global, set->world_off, set->world_list, set->W, set->elev, body_q,
+                                         margin, cmax, count, particle, shape, body_pos, body_vel, normal);
   return cudaGetLastError() == cudaSuccess ? VBD_OK : VBD_ERR_CUDA;
 }
 
