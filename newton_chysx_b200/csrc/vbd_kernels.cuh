@@ -586,8 +586,11 @@ __global__ void k_contact_prepare(StepCtx<R> c) {
     set_err(c.err, 2);
 }
 
+// With self-contact the kernel is latency-bound on its chains of dependent loads (entry, pair, element, positions);
+// capping it at 72 registers (some spills) lets 7 CTAs of 128 threads share an SM instead of 4: 8.79 ms against
+// 9.21 ms per substep on a 256 x 256 sheet draped on a sphere (80: 8.98 ms, 64: 8.89 ms).
 template <typename R, int L, int MODE, bool SC = false, bool SOFT = false>
-__global__ void k_color(StepCtx<R> c, const int* __restrict__ verts, int n, int iteration) {
+__global__ void __maxnreg__(SC ? 72 : 255) k_color(StepCtx<R> c, const int* __restrict__ verts, int n, int iteration) {
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   const int grp = gid / L, sub = gid % L;
   const bool valid = grp < n;
