@@ -1190,7 +1190,7 @@ def soft_contacts(model: Model, state: State, contacts: Contacts, margin: float)
     ss = _current_shape_set(model)
     pw = getattr(model, "particle_world", None)
     bq = None
-    if getattr(model, "body_count", 0):
+    if getattr(model, "body_count", 0) and bool(np.any(getattr(model, "_shape_body_host", np.zeros(0)) >= 0)):
         if getattr(state, "body_q", None) is None:
             raise ValueError("the model has shapes on bodies: state.body_q must hold the body transforms")
         bq = interop.pointer(state.body_q, "state.body_q", interop.F32, 7 * model.body_count)
