@@ -2,6 +2,7 @@
 
 import numpy as np
 import pytest
+import torch
 
 from newton_chysx_b200 import sim
 from tests.helpers import load_golden
@@ -81,3 +82,40 @@ def test_degenerate_triangles_are_dropped():
     areas = b.add_triangles([0, 0], [1, 1], [2, 3])
     assert areas[0] == 0.0 and areas[1] == pytest.approx(0.5)
     assert b.tri_count == 1
+
+
+def test_bodies_carry_shapes_through_worlds():
+    """add_body (builder.py:3814-3878) and shapes on bodies: a shape's body index moves with its world's bodies
+    when builders are merged, a shape on a missing body is refused, and states carry the bodies' transforms and
+    velocities."""
+    from newton_chysx_b200 import sim
+
+    b = sim.ModelBuilder(up_axis="Z", gravity=-9.81)
+    b.add_particles(np.zeros((2, 3)), (0.0, 0.0, 0.0), 1.0, np.full(2, 0.01), np.ones(2, np.int32))
+    body = b.add_body(xform=((0.1, 0.2, 0.3), sim.quat_from_axis_angle((0.0, 0.0, 1.0), 0.5)), mass=2.0,
+                      com=(0.0, 0.0, 0.05))  # fmt: skip
+    b.add_shape_sphere(body=body, radius=0.1)
+    b.add_shape_box(hx=0.1, hy=0.1, hz=0.1)
+    with pytest.raises(ValueError, match="body 3"):
+        b.add_shape_sphere(body=3, radius=0.1)
+    top = sim.ModelBuilder(up_axis="Z", gravity=-9.81)
+    top.add_world(b)
+    top.add_world(b)
+    assert top.body_count == 2 and [s["body"] for s in top.shapes] == [0, -1, 1, -1]
+    assert [bd["world"] for bd in top.bodies] == [0, 1]
+    m = top.finalize("cpu")
+    assert m.body_count == 2 and m._shape_body_host.tolist() == [0, -1, 1, -1]
+    assert m.shape_body.tolist() == [0, -1, 1, -1]
+    np.testing.assert_allclose(m.body_q[1, :3].numpy(), [0.1, 0.2, 0.3], atol=1e-7)
+    np.testing.assert_allclose(m.body_com[0].numpy(), [0.0, 0.0, 0.05], atol=1e-7)
+    st = m.state()
+    assert tuple(st.body_q.shape) == (2, 7) and tuple(st.body_qd.shape) == (2, 6)
+    st2 = m.state()
+    st2.body_q += 1.0
+    st.assign(st2)
+    assert torch.equal(st.body_q, st2.body_q)
+    static = sim.ModelBuilder(up_axis="Z", gravity=-9.81)
+    static.add_particles(np.zeros((1, 3)), (0.0, 0.0, 0.0), 1.0, np.full(1, 0.01), np.ones(1, np.int32))
+    static.add_ground_plane()
+    ms = static.finalize("cpu")
+    assert ms.body_count == 0 and ms.body_q is None and ms.state().body_q is None
