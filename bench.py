@@ -23,6 +23,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -979,6 +980,98 @@ def cpu_baseline_selfcontact(m, q, qd, fp64_step=True):
     return out
 
 
+def build_selfcontact_batch_model(dev, worlds, n=32, seed=9):
+    """Batched self-contact: `worlds` copies of an n x n sheet (0.25 m side, the drop-in material, 0.2 kg/m^2,
+    bending 1e-4) each over its own sphere of radius 0.06 m, dropped from a seeded height with a seeded sideways
+    velocity so that each sheet drapes and folds onto itself differently. The worlds sit 0.5 m apart on a square
+    grid: co-located worlds would share every cell of the collision grid (and on the per-color schedule, which
+    lets worlds collide as the reference's union model does, interpenetrate)."""
+    import torch
+
+    import newton_chysx_b200 as nb
+
+    E, nu, h, side = 1.0e4, 0.3, 1.0e-3, 0.25
+    tpl = nb.ModelBuilder(up_axis="Z", gravity=-9.81)
+    tpl.add_cloth_grid(pos=(-side / 2, -side / 2, 0.1), rot=nb.quat_identity(), vel=(0.0, 0.0, 0.0), dim_x=n - 1,
+                       dim_y=n - 1, cell_x=side / (n - 1), cell_y=side / (n - 1), mass=0.2 * side * side / (n * n),
+                       tri_ke=E * h / (2.0 * (1.0 + nu)), tri_ka=E * h * nu / (1.0 - nu * nu), tri_kd=0.0,
+                       edge_ke=1e-4, edge_kd=0.0, particle_radius=2e-3)  # fmt: skip
+    tpl.add_shape_sphere(radius=0.06)
+    tpl.color(include_bending=True)
+    b = nb.ModelBuilder(up_axis="Z", gravity=-9.81)
+    for _ in range(worlds):
+        b.add_world(tpl)
+    m = b.finalize(dev)
+    rng = np.random.default_rng(seed)
+    n1 = tpl.particle_count
+    k = int(math.ceil(math.sqrt(worlds)))
+    off = np.stack([np.arange(worlds) % k * 0.5, np.arange(worlds) // k * 0.5, rng.uniform(0.0, 0.05, worlds)], 1)
+    with torch.no_grad():
+        m.particle_q += torch.as_tensor(np.repeat(off, n1, axis=0), dtype=torch.float32, device=dev)
+        m.particle_qd[:, 0] = torch.as_tensor(np.repeat(rng.normal(0.0, 0.3, worlds), n1), dtype=torch.float32,
+                                              device=dev)  # fmt: skip
+    m.shape_transform[:, :2] += off[:, :2].astype(np.float32)  # each world's sphere under its sheet
+    m.soft_contact_ke, m.soft_contact_kd, m.soft_contact_mu = 1.0e4, 1.0e-2, 0.5
+    return m
+
+
+def run_selfcontact_batch(args):
+    """Self-contact on a batched model: --instances sheets (--sc-batch-n vertices a side, each over its own sphere)
+    with vertex-triangle and edge-edge self-contact, 20 iterations, dt = 1/600 s. The sheets fall and drape untimed
+    (--sc-settle-frames x 10 substeps); then K substeps (contact generation + step) are timed from a CUDA graph
+    on the persistent self-contact schedule (one CTA per world, detections grid-wide) and on the per-color
+    schedule, from the same settled state."""
+    import torch
+
+    import newton_chysx_b200 as nb
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    W = args.instances
+    t0 = time.perf_counter()
+    m = build_selfcontact_batch_model(dev, W, n=args.sc_batch_n)
+    build_s = time.perf_counter() - t0
+    kw = dict(SC_KW, lanes_per_vertex=args.lanes)
+    solver = nb.SolverVBD(m, iterations=SC_ITERATIONS, **kw)
+    assert solver.schedule == "persistent"
+    pipe = nb.CollisionPipeline(m, soft_contact_margin=0.01)
+    contacts = pipe.contacts()
+    s0, s1 = m.state(), m.state()
+    settle = args.sc_settle_frames * 10 + args.warmup
+    for _ in range(settle):
+        pipe.collide(s0, contacts)
+        solver.step(s0, s1, None, contacts, DT)
+        s0, s1 = s1, s0
+    torch.cuda.synchronize()
+    q_settled, qd_settled = s0.particle_q.clone(), s0.particle_qd.clone()
+    K = max(2, args.steps + (args.steps % 2))
+    with ClockSampler(dev.index or 0) as clk:
+        ms = time_selfcontact_substeps(solver, pipe, contacts, s0, s1, q_settled, qd_settled, K)
+    pairs = solver.self_contact_counts()
+    per_color = nb.SolverVBD(m, iterations=SC_ITERATIONS, schedule="per_color", **kw)
+    ms_pc = time_selfcontact_substeps(per_color, pipe, contacts, s0, s1, q_settled, qd_settled, K)
+    V = m.particle_count
+    n = args.sc_batch_n
+    return {
+        "metric": "VBD vertex-iters/s on 1 B200, batched cloth with self-contact", "value": V * SC_ITERATIONS / (ms * 1e-3),
+        "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (sheets dropped on spheres)",
+        "config": {"workload": f"{W} sheets of {n}x{n} with self-contact, each over its own sphere, 0.5 m apart",
+                   "vertices": V, "iterations": SC_ITERATIONS, "dt": DT, "settled_substeps": settle,
+                   "build_s": round(build_s, 1), "schedule": solver.schedule,
+                   "lanes_per_vertex": solver.lanes_per_vertex,
+                   "timed": "sphere contact generation + step, one CUDA graph per two substeps"},
+        "launches_per_step": solver.launches_per_step + 1,
+        "per_color": {"value": V * SC_ITERATIONS / (ms_pc * 1e-3), "unit": UNIT, "ms_per_step": ms_pc,
+                      "launches_per_step": per_color.launches_per_step + 1,
+                      "lanes_per_vertex": per_color.lanes_per_vertex},
+        "persistent_over_per_color": ms_pc / ms,
+        "self_contact_pairs": {"vertex_triangle": pairs[0], "edge_edge": pairs[1], "overflow_flags": pairs[2]},
+        "clocks": clk.summary(), "device_errors": solver.device_errors() + per_color.device_errors(),
+        "finite": bool(torch.isfinite(s0.particle_q).all().item()),
+    }  # fmt: skip
+
+
 def build_soft_model(dev, worlds, seed=5):
     """Volumetric batch: `worlds` tetrahedral blocks of 8 x 4 x 4 cells (5 tets per cell, 225 particles, 640
     tets; 2 cm cells, 500 kg/m^3, mu 2e4 Pa, lambda 3e4 Pa, damping 1e-3), each hung from a fixed anchor by
@@ -1549,8 +1642,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["batched", "plain", "precision", "selfcontact", "adjoint", "soft",
-                                           "contacts"], default="batched")  # fmt: skip
+    ap.add_argument("--workload", choices=["batched", "plain", "precision", "selfcontact", "selfcontact_batch",
+                                           "adjoint", "soft", "contacts"], default="batched")  # fmt: skip
     ap.add_argument("--contact-particles", type=int, default=8 << 20, help="contacts workload: particle count")
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--seed", type=int, default=0)
@@ -1580,6 +1673,7 @@ def main():
     ap.add_argument("--traffic", type=float, default=None, help="DRAM bytes per launch from an ncu capture")
     ap.add_argument("--sc-n", type=int, default=256, help="selfcontact workload: grid side (vertices)")
     ap.add_argument("--sc-settle-frames", type=int, default=40, help="selfcontact workload: untimed frames first")
+    ap.add_argument("--sc-batch-n", type=int, default=32, help="selfcontact_batch workload: sheet side (vertices)")
     ap.add_argument("--adjoint-frames", type=int, default=60)
     ap.add_argument("--adjoint-directions", type=int, default=32)
     args = ap.parse_args()
@@ -1598,6 +1692,8 @@ def main():
         out = run_precision(args)
     elif args.workload == "selfcontact":
         out = run_selfcontact(args)
+    elif args.workload == "selfcontact_batch":
+        out = run_selfcontact_batch(args)
     elif args.workload == "adjoint":
         out = run_adjoint(args)
     elif args.workload == "soft":
