@@ -8,9 +8,9 @@ sm_100a kernels) on the current torch CUDA stream, so a substep loop can be capt
 
 Beyond the reference keywords:
 
-* ``precision``: ``"fp32"`` (the reference's arithmetic), ``"mixed"`` (FP64 3x3 solve for
-  ill-conditioned blocks and FP64 residual sums, see ``residuals()``), ``"fp64"`` (all FP64; the
-  state arrays must be float64).
+* ``precision``: ``"fp32"`` (the reference's arithmetic), ``"mixed"`` (contact vertices add their contact
+  terms and solve in FP64, other vertices solve in FP64 when their block is ill-conditioned; FP64 residual
+  sums, see ``residuals()``), ``"fp64"`` (all FP64; the state arrays must be float64).
 * ``schedule``: ``"per_color"`` (one launch per color and iteration), ``"persistent"`` (one launch
   per substep, a CTA per cloth instance/world), ``"auto"``.
 * ``lanes_per_vertex`` / ``block_size``: launch shape (0 = default; see ``autotune``).
@@ -142,10 +142,12 @@ class SolverVBD:
                 schedule = "persistent" if worlds is not None and linear_beta == 0.0 and not soft else "per_color"
             layout = "csr"
             if lanes_per_vertex == 0:
-                # a vertex's self-contact entries (tens of edge-edge pairs) join its faces and hinges: 16 lanes
-                # per vertex measured fastest on a 256 x 256 sheet draped on a sphere (9.6 ms vs 21 ms per
-                # substep with one lane)
-                lanes_per_vertex = 16
+                # a vertex's self-contact entries join its faces and hinges in the lane split. One large sheet
+                # (per-color schedule) has tens of edge-edge entries per vertex: 16 lanes measured fastest on a
+                # 256 x 256 sheet draped on a sphere (9.6 ms vs 21 ms per substep with one lane). Batched sheets
+                # (persistent schedule) have about one: 4 lanes measured fastest (256 sheets of 32 x 32: 11.8 ms
+                # vs 15.0 ms with 16; 2,048 of 16 x 16: 14.1 ms vs 17.6 ms)
+                lanes_per_vertex = 4 if schedule == "persistent" else 16
         if model.body_count > 0 and not integrate_with_external_rigid_solver:
             raise NotImplementedError("rigid bodies (AVBD) are not part of this solver")
         if model.particle_count == 0:
