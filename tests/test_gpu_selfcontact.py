@@ -477,8 +477,9 @@ def test_persistent_self_contact_batch_matches_per_color():
         b.add_world(w)
     model = b.finalize("cuda")
     q0 = model.particle_q.cpu().numpy() + rng.normal(scale=1.0e-3, size=(model.particle_count, 3))
+    # the same lane split in both (the persistent default), so that each vertex sums its terms in the same order
     kw = dict(particle_enable_self_contact=True, particle_self_contact_radius=2e-3, particle_self_contact_margin=3.5e-3,
-              particle_collision_detection_interval=2)  # fmt: skip
+              particle_collision_detection_interval=2, lanes_per_vertex=4)  # fmt: skip
     pers = SolverVBD(model, iterations=6, schedule="persistent", **kw)
     ref = SolverVBD(model, iterations=6, schedule="per_color", **kw)
     s0, s1, t0, t1 = model.state(), model.state(), model.state(), model.state()
