@@ -276,7 +276,7 @@ def color_particles(n, tri_indices, tri_materials, edge_indices, edge_props, inc
 # ----------------------------------------------------------------------------- builder
 class ModelBuilder:
     """The particle subset of the reference ``ModelBuilder``: particles, cloth triangles and hinges,
-    springs, tetrahedra, static shapes, worlds and coloring."""
+    springs, tetrahedra, collision shapes (static or on bodies), worlds and coloring."""
 
     ShapeConfig = ShapeConfig
 
