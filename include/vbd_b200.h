@@ -183,21 +183,26 @@ int vbd_step_f64(VbdHandle h, double* q_in_dev, double* q_out_dev, const double*
    counterpart: the reference VBD kernels are built with enable_backward=False,
    particle_vbd_kernels.py:27-28) */
 
-/* The forward substep of vbd_step (per-color sweep, no particle-shape contacts) that also records
-   what its adjoint needs: y [V,3] the inertial targets and checkpoints [(iterations+1),V,3] the
-   positions at the start of every iteration and at the end. Arrays are float32, or float64 for a
-   VBD_PRECISION_FP64 solver. q_out/qd_out receive the step's result (q_in is not modified).
-   VBD_ERR_UNSUPPORTED for models with springs or tetrahedra (the adjoint covers cloth only). */
-int vbd_record_step(VbdHandle h, const void* q_in_dev, const void* qd_in_dev, const void* particle_f_dev, double dt,
-                    void* y_dev, void* checkpoints_dev, void* q_out_dev, void* qd_out_dev, void* stream);
+/* The forward substep of vbd_step (per-color sweep) that also records what its adjoint needs: y [V,3] the
+   inertial targets and checkpoints [(iterations+1),V,3] the positions at the start of every iteration and at
+   the end. Arrays are float32, or float64 for a VBD_PRECISION_FP64 solver. q_out/qd_out receive the step's
+   result (q_in is not modified). contacts: this substep's particle-shape contacts against static shapes, or
+   NULL; the adjoint must be given the same arrays. VBD_ERR_UNSUPPORTED for models with springs or tetrahedra
+   (the adjoint covers cloth only) and for contacts with the AVBD penalty ramp on (rigid_avbd_beta > 0). */
+int vbd_record_step(VbdHandle h, const void* q_in_dev, const void* qd_in_dev, const void* particle_f_dev,
+                    const VbdContactsDesc* contacts, double dt, void* y_dev, void* checkpoints_dev, void* q_out_dev,
+                    void* qd_out_dev, void* stream);
 
 /* Reverse of that substep: from dL/dq_out and dL/dqd_out (either may be NULL = 0), writes dL/dq_in
    and dL/dqd_in and ADDS the triangles' dL/dmu and dL/dlambda (Model.tri_materials columns 0 and 1)
-   into adj_tri_mu / adj_tri_lambda [T] (either may be NULL). The first call allocates
-   (colors + 2) x V x 3 work values; it returns VBD_ERR_UNSUPPORTED if that happens during a capture. */
-int vbd_adjoint_step(VbdHandle h, const void* q_in_dev, const void* y_dev, const void* checkpoints_dev, double dt,
-                     const void* adj_q_out_dev, const void* adj_qd_out_dev, void* adj_q_in_dev, void* adj_qd_in_dev,
-                     void* adj_tri_mu_dev, void* adj_tri_lambda_dev, void* stream);
+   into adj_tri_mu / adj_tri_lambda [T] (either may be NULL). contacts: the arrays the forward substep was
+   given; their contact set, points, normals and stiffness are held fixed (the derivative of the step for
+   those contacts). The first call allocates (colors + 3) x V x 3 work values; it returns
+   VBD_ERR_UNSUPPORTED if that happens during a capture. */
+int vbd_adjoint_step(VbdHandle h, const void* q_in_dev, const void* y_dev, const void* checkpoints_dev,
+                     const VbdContactsDesc* contacts, double dt, const void* adj_q_out_dev,
+                     const void* adj_qd_out_dev, void* adj_q_in_dev, void* adj_qd_in_dev, void* adj_tri_mu_dev,
+                     void* adj_tri_lambda_dev, void* stream);
 
 /* Reads and clears the device error word (VBD_DEVERR_* bits). Synchronizes `stream`. */
 int vbd_get_error(VbdHandle h, int32_t* bits, void* stream);

@@ -123,8 +123,8 @@ SIGNATURES = {
         [_vp, _vp, _vp, _vp, _vp, _vp, C.POINTER(VbdContactsDesc), C.POINTER(VbdBodyState), C.c_double, _vp],
         C.c_int,
     ),
-    "vbd_record_step": ([_vp, _vp, _vp, _vp, C.c_double, _vp, _vp, _vp, _vp, _vp], C.c_int),
-    "vbd_adjoint_step": ([_vp, _vp, _vp, _vp, C.c_double, _vp, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
+    "vbd_record_step": ([_vp, _vp, _vp, _vp, _vp, C.c_double, _vp, _vp, _vp, _vp, _vp], C.c_int),
+    "vbd_adjoint_step": ([_vp, _vp, _vp, _vp, _vp, C.c_double, _vp, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
     "vbd_get_error": ([_vp, _ip, _vp], C.c_int),
     "vbd_get_residuals": ([_vp, _dp, C.c_int32, _vp], C.c_int),
     "vbd_launches_per_step": ([_vp, _ip], C.c_int),

@@ -1,4 +1,4 @@
-// Hand-written adjoint of the fixed-iteration VBD step (one substep, no particle-shape contacts).
+// Hand-written adjoint of the fixed-iteration VBD step (one substep, with particle-shape contacts on static shapes).
 //
 // Forward map of one substep (vbd_kernels.cuh, CSR path, one lane per vertex):
 //   y   = q + (qd + (g + f_ext / m) dt) dt                    inertial target, also the first iterate
@@ -15,6 +15,10 @@
 // element's vertex coordinates (and the triangle's mu, lambda), running the same element routines
 // as the forward pass. Vertices of one color are never neighbours, so the vertices written through
 // atomics (the neighbours, the triangle parameters) are never read by the same launch.
+// A contact term depends on the vertex's position x and, through its friction and damping, on the
+// vertex's position at the start of the substep, q; its derivative in q is accumulated per vertex
+// (adj_xp) and joins dL/dq_in at the end. The contact set, the contact points and normals and the penalty
+// stiffness are held fixed (the derivative of the step for its contacts; the AVBD ramp is off).
 #pragma once
 #include "vbd_dual.cuh"
 #include "vbd_kernels.cuh"
@@ -30,6 +34,7 @@ struct AdjCtx {
   R* adj_y;               // [V*3] accumulated dL/dy
   R* adj_mu;              // [T] accumulated dL/dmu (triangle), may be NULL
   R* adj_lambda;          // [T] accumulated dL/dlambda, may be NULL
+  R* adj_xp;              // [V*3] accumulated dL/dq through the contact terms (contacts only)
 };
 
 // mass used by the solve (0 for a fixed particle), as forward_particle stores it
@@ -82,6 +87,48 @@ __device__ __forceinline__ void assemble(const StepCtx<R>& c, const R* X, int v,
   }
 }
 
+// element and contact terms of vertex v at positions X (the forward pass of the adjoint's sweep)
+template <typename R>
+__device__ __forceinline__ void assemble_all(const StepCtx<R>& c, const R* X, int v, vec3<R>& f, sym3<R>& H) {
+  assemble(c, X, v, f, H);
+  if (c.has_contacts) contacts_add<R>(c, v, ldx(X, v), f, H);
+}
+
+// Contact terms of vertex v with dual numbers over its position x (slots 0-2) and its position at the start of the
+// substep (slots 3-5, c.qprev), as contacts_add_n evaluates them for static shapes; their derivatives contracted
+// with (w, H_bar) add to ax and to adj_xp.
+template <typename R>
+__device__ __forceinline__ void contacts_adjoint(const StepCtx<R>& c, int v, vec3<R> x, vec3<R> w, const sym3<R>& Hb,
+                                                 vec3<R>& ax, R* adj_xp) {
+  int n = c.slot_cnt[v];
+  if (n > c.K) n = c.K;
+  if (n <= 0) return;
+  using D6 = Dual<R, 6>;
+  const vec3<R> xp = ld3<R>(c.qprev[v]);
+  const vec3<D6> xd = {D6::seed(x.x, 0), D6::seed(x.y, 1), D6::seed(x.z, 2)};
+  const vec3<D6> xpd = {D6::seed(xp.x, 3), D6::seed(xp.y, 4), D6::seed(xp.z, 5)};
+  const D6 r = D6(R(c.radius[v]));
+  const D6 dt = D6(c.dt);
+  vec3<R> gxp = zero3<R>();
+  for (int j = 0; j < n; ++j) {
+    const int t = c.slots[v * c.K + j];
+    const vec3<D6> bx = {D6(R(c.c_body_pos[3 * t])), D6(R(c.c_body_pos[3 * t + 1])), D6(R(c.c_body_pos[3 * t + 2]))};
+    const vec3<D6> nn = {D6(R(c.c_normal[3 * t])), D6(R(c.c_normal[3 * t + 1])), D6(R(c.c_normal[3 * t + 2]))};
+    const D6 pen = -(dot(nn, xd - bx) - r);
+    if (!(pen > D6(R(0)))) continue;
+    const vec3<D6> bv = {D6(R(c.c_body_vel[3 * t])), D6(R(c.c_body_vel[3 * t + 1])), D6(R(c.c_body_vel[3 * t + 2]))};
+    const vec3<D6> rel = (xd - xpd) - bv * dt;
+    vec3<D6> fd = {D6(R(0)), D6(R(0)), D6(R(0))};
+    sym3<D6> Hd = szero<D6>();
+    contact_add<D6>(pen, nn, rel, D6(R(c.c_k[t])), D6(R(c.c_kd[t])), D6(R(c.c_mu[t])), D6(c.fric_eps), dt, fd, Hd);
+    ax = ax + vec3<R>{contract(fd, Hd, w, Hb, 0), contract(fd, Hd, w, Hb, 1), contract(fd, Hd, w, Hb, 2)};
+    gxp = gxp + vec3<R>{contract(fd, Hd, w, Hb, 3), contract(fd, Hd, w, Hb, 4), contract(fd, Hd, w, Hb, 5)};
+  }
+  adj_xp[3 * v] += gxp.x;
+  adj_xp[3 * v + 1] += gxp.y;
+  adj_xp[3 * v + 2] += gxp.z;
+}
+
 template <typename R>
 __global__ void k_adjoint_color(AdjCtx<R> A, const int* __restrict__ verts, int n) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -95,7 +142,7 @@ __global__ void k_adjoint_color(AdjCtx<R> A, const int* __restrict__ verts, int 
   // forward quantities at this color's start
   vec3<R> f = md * (ldx(A.y, v) - x);
   sym3<R> H = sdiag(md);
-  assemble(c, A.x, v, f, H);
+  assemble_all(c, A.x, v, f, H);
   const R det = sdet(H);
   if (!(fabs(double(det)) > 1e-8) || !isfinite(double(det))) return;  // update skipped: D = 0
   const R idet = R(1) / det;
@@ -163,6 +210,7 @@ __global__ void k_adjoint_color(AdjCtx<R> A, const int* __restrict__ verts, int 
         atomic_add3(A.adj_x, vid[j], gj);
     }
   }
+  if (c.has_contacts) contacts_adjoint(c, v, x, w, Hb, ax, A.adj_xp);
   A.adj_x[3 * v] = ax.x;
   A.adj_x[3 * v + 1] = ax.y;
   A.adj_x[3 * v + 2] = ax.z;
@@ -181,7 +229,7 @@ __global__ void k_record_color(StepCtx<R> c, const R* __restrict__ xin, const R*
   const vec3<R> x = ldx(xin, v);
   vec3<R> f = md * (ldx(y, v) - x);
   sym3<R> H = sdiag(md);
-  assemble(c, xin, v, f, H);
+  assemble_all(c, xin, v, f, H);
   const R det = sdet(H);
   if (!(fabs(double(det)) > 1e-8) || !isfinite(double(det))) return;
   const vec3<R> xn = x + sadj_mul(H, f) * (R(1) / det);
@@ -211,17 +259,26 @@ __global__ void k_adjoint_begin(int n3, const R* aq, const R* aqd, R inv_dt, R* 
   ay[i] = R(0);
 }
 
-// dL/dq_in, dL/dqd_in from dL/dy (the first iterate is y) and the direct qd_out term
+// dL/dq_in, dL/dqd_in from dL/dy (the first iterate is y), the direct qd_out term and the contact terms' dL/dq
+// (axp, or NULL)
 template <typename R>
-__global__ void k_adjoint_end(StepCtx<R> c, const R* ax, const R* ay, const R* aqd, R* aq_in, R* aqd_in) {
+__global__ void k_adjoint_end(StepCtx<R> c, const R* ax, const R* ay, const R* axp, const R* aqd, R* aq_in,
+                              R* aqd_in) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= c.V) return;
   const bool moves = (c.flags[i] & 1) && c.inv_mass[i] != 0.f;
   for (int j = 0; j < 3; ++j) {
     const R gy = ay[3 * i + j] + ax[3 * i + j];
-    aq_in[3 * i + j] = gy - (aqd ? aqd[3 * i + j] / c.dt : R(0));
+    aq_in[3 * i + j] = gy - (aqd ? aqd[3 * i + j] / c.dt : R(0)) + (axp ? axp[3 * i + j] : R(0));
     if (aqd_in) aqd_in[3 * i + j] = moves ? gy * c.dt : R(0);
   }
+}
+
+// the substep's start positions where the contact terms read them (c.qprev), for the adjoint's recomputation
+template <typename R>
+__global__ void k_adjoint_qprev(StepCtx<R> c) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < c.V) c.qprev[i] = pk4(vec3<R>{c.q_in[3 * i], c.q_in[3 * i + 1], c.q_in[3 * i + 2]}, R(0));
 }
 
 // q_out = x, qd_out = (x - q) / dt

@@ -1417,10 +1417,30 @@ int occupancy_grid(VbdSolver* h) {
   return VBD_OK;
 }
 
+// The particle-shape contacts of a differentiated substep on the step context (static shapes: no body poses).
 template <typename R>
-int record_impl(VbdSolver* h, const R* q_in, const R* qd_in, const R* f_ext, R dt, R* y, R* ck, R* q_out, R* qd_out,
-                cudaStream_t st) {
+void set_contacts(StepCtx<R>& c, const VbdContactsDesc* contacts) {
+  c.has_contacts = 1;
+  c.c_count = contacts->soft_contact_count_dev;
+  c.c_max = contacts->soft_contact_max;
+  c.c_particle = contacts->soft_contact_particle_dev;
+  c.c_shape = contacts->soft_contact_shape_dev;
+  c.c_body_pos = contacts->soft_contact_body_pos_dev;
+  c.c_body_vel = contacts->soft_contact_body_vel_dev;
+  c.c_normal = contacts->soft_contact_normal_dev;
+}
+
+template <typename R>
+int record_impl(VbdSolver* h, const R* q_in, const R* qd_in, const R* f_ext, const VbdContactsDesc* contacts, R dt,
+                R* y, R* ck, R* q_out, R* qd_out, cudaStream_t st) {
+  const bool has_c = contacts && contacts->soft_contact_max > 0 && contacts->soft_contact_count_dev;
+  if (has_c) {
+    if (h->prm.avbd_linear_beta != 0.f) return VBD_ERR_UNSUPPORTED;  // the penalty ramp is not differentiated
+    int rc = ensure_contact_capacity(h, contacts->soft_contact_max, st);
+    if (rc) return rc;
+  }
   StepCtx<R> c = make_ctx<R, MODE_FP32>(h);
+  if (has_c) set_contacts(c, contacts);
   c.q_in = const_cast<R*>(q_in);
   c.qd_in = qd_in;
   c.f_ext = f_ext;
@@ -1431,6 +1451,10 @@ int record_impl(VbdSolver* h, const R* q_in, const R* qd_in, const R* f_ext, R d
   const int V = h->V, I = h->prm.iterations;
   const size_t n3 = size_t(3) * V;
   k_record_forward<R><<<(V + 255) / 256, 256, 0, st>>>(c, y);
+  if (has_c) {
+    CK(cudaMemsetAsync(h->slot_cnt, 0, sizeof(int) * V, st));
+    k_contact_prepare<R><<<(c.c_max + 255) / 256, 256, 0, st>>>(c);
+  }
   CK(cudaMemcpyAsync(ck, y, n3 * sizeof(R), cudaMemcpyDeviceToDevice, st));
   const int* cp = h->md.color_particles_dev;
   for (int it = 0; it < I; ++it) {
@@ -1447,11 +1471,17 @@ int record_impl(VbdSolver* h, const R* q_in, const R* qd_in, const R* f_ext, R d
 }
 
 template <typename R>
-int adjoint_impl(VbdSolver* h, const R* q_in, const R* y, const R* ck, R dt, const R* aq_out, const R* aqd_out, R* aq_in,
-                 R* aqd_in, R* adj_mu, R* adj_lambda, cudaStream_t st) {
+int adjoint_impl(VbdSolver* h, const R* q_in, const R* y, const R* ck, const VbdContactsDesc* contacts, R dt,
+                 const R* aq_out, const R* aqd_out, R* aq_in, R* aqd_in, R* adj_mu, R* adj_lambda, cudaStream_t st) {
   const int V = h->V, I = h->prm.iterations, C = int(h->color_offsets.size()) - 1;
   const size_t n3 = size_t(3) * V;
-  const size_t need = (size_t(std::max(C, 1)) + 2) * n3 * sizeof(R);
+  const bool has_c = contacts && contacts->soft_contact_max > 0 && contacts->soft_contact_count_dev;
+  if (has_c) {
+    if (h->prm.avbd_linear_beta != 0.f) return VBD_ERR_UNSUPPORTED;
+    int rc = ensure_contact_capacity(h, contacts->soft_contact_max, st);
+    if (rc) return rc;
+  }
+  const size_t need = (size_t(std::max(C, 1)) + 3) * n3 * sizeof(R);
   if (h->adj_work_bytes < need) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     CK(cudaStreamIsCapturing(st, &cs));
@@ -1466,12 +1496,21 @@ int adjoint_impl(VbdSolver* h, const R* q_in, const R* y, const R* ck, R dt, con
   R* S = (R*)h->adj_work;  // C color-start states
   R* ax = S + size_t(std::max(C, 1)) * n3;
   R* ay = ax + n3;
+  R* axp = ay + n3;
   StepCtx<R> c = make_ctx<R, MODE_FP32>(h);
+  if (has_c) set_contacts(c, contacts);
   c.q_in = const_cast<R*>(q_in);
   c.dt = dt;
   c.dt2r = R(1) / (dt * dt);
   k_adjoint_begin<R><<<int((n3 + 255) / 256), 256, 0, st>>>(int(n3), aq_out, aqd_out, R(1) / dt, ax, ay);
-  AdjCtx<R> A{c, nullptr, y, ax, ay, adj_mu, adj_lambda};
+  if (has_c) {
+    // this substep's start positions and contact table, as its forward pass had them
+    k_adjoint_qprev<R><<<(V + 255) / 256, 256, 0, st>>>(c);
+    CK(cudaMemsetAsync(h->slot_cnt, 0, sizeof(int) * V, st));
+    k_contact_prepare<R><<<(c.c_max + 255) / 256, 256, 0, st>>>(c);
+    CK(cudaMemsetAsync(axp, 0, n3 * sizeof(R), st));
+  }
+  AdjCtx<R> A{c, nullptr, y, ax, ay, adj_mu, adj_lambda, axp};
   const int* cp = h->md.color_particles_dev;
   for (int it = I - 1; it >= 0; --it) {
     CK(cudaMemcpyAsync(S, ck + size_t(it) * n3, n3 * sizeof(R), cudaMemcpyDeviceToDevice, st));
@@ -1487,7 +1526,7 @@ int adjoint_impl(VbdSolver* h, const R* q_in, const R* y, const R* ck, R dt, con
       if (b > a) k_adjoint_color<R><<<(b - a + 63) / 64, 64, 0, st>>>(A, cp + a, b - a);
     }
   }
-  k_adjoint_end<R><<<(V + 255) / 256, 256, 0, st>>>(c, ax, ay, aqd_out, aq_in, aqd_in);
+  k_adjoint_end<R><<<(V + 255) / 256, 256, 0, st>>>(c, ax, ay, has_c ? axp : nullptr, aqd_out, aq_in, aqd_in);
   CK(cudaGetLastError());
   return VBD_OK;
 }
@@ -1925,29 +1964,30 @@ int vbd_step_f64(VbdHandle h, double* q_in, double* q_out, const double* qd_in, 
                                       (cudaStream_t)stream);
 }
 
-int vbd_record_step(VbdHandle h, const void* q_in, const void* qd_in, const void* particle_f, double dt, void* y,
-                    void* checkpoints, void* q_out, void* qd_out, void* stream) {
+int vbd_record_step(VbdHandle h, const void* q_in, const void* qd_in, const void* particle_f,
+                    const VbdContactsDesc* contacts, double dt, void* y, void* checkpoints, void* q_out, void* qd_out,
+                    void* stream) {
   if (!h || !q_in || !qd_in || !y || !checkpoints || !q_out || !qd_out || !(dt > 0.0)) return VBD_ERR_INVALID_ARGUMENT;
   if (h->soft) return VBD_ERR_UNSUPPORTED;
   cudaStream_t st = (cudaStream_t)stream;
   if (h->precision == VBD_PRECISION_FP64)
-    return record_impl<double>(h, (const double*)q_in, (const double*)qd_in, (const double*)particle_f, dt,
+    return record_impl<double>(h, (const double*)q_in, (const double*)qd_in, (const double*)particle_f, contacts, dt,
                                (double*)y, (double*)checkpoints, (double*)q_out, (double*)qd_out, st);
-  return record_impl<float>(h, (const float*)q_in, (const float*)qd_in, (const float*)particle_f, float(dt), (float*)y,
-                            (float*)checkpoints, (float*)q_out, (float*)qd_out, st);
+  return record_impl<float>(h, (const float*)q_in, (const float*)qd_in, (const float*)particle_f, contacts,
+                            float(dt), (float*)y, (float*)checkpoints, (float*)q_out, (float*)qd_out, st);
 }
 
-int vbd_adjoint_step(VbdHandle h, const void* q_in, const void* y, const void* checkpoints, double dt,
-                     const void* adj_q_out, const void* adj_qd_out, void* adj_q_in, void* adj_qd_in, void* adj_tri_mu,
-                     void* adj_tri_lambda, void* stream) {
+int vbd_adjoint_step(VbdHandle h, const void* q_in, const void* y, const void* checkpoints,
+                     const VbdContactsDesc* contacts, double dt, const void* adj_q_out, const void* adj_qd_out,
+                     void* adj_q_in, void* adj_qd_in, void* adj_tri_mu, void* adj_tri_lambda, void* stream) {
   if (!h || !q_in || !y || !checkpoints || !adj_q_in || !(dt > 0.0)) return VBD_ERR_INVALID_ARGUMENT;
   if (h->soft) return VBD_ERR_UNSUPPORTED;
   cudaStream_t st = (cudaStream_t)stream;
   if (h->precision == VBD_PRECISION_FP64)
-    return adjoint_impl<double>(h, (const double*)q_in, (const double*)y, (const double*)checkpoints, dt,
+    return adjoint_impl<double>(h, (const double*)q_in, (const double*)y, (const double*)checkpoints, contacts, dt,
                                 (const double*)adj_q_out, (const double*)adj_qd_out, (double*)adj_q_in,
                                 (double*)adj_qd_in, (double*)adj_tri_mu, (double*)adj_tri_lambda, st);
-  return adjoint_impl<float>(h, (const float*)q_in, (const float*)y, (const float*)checkpoints, float(dt),
+  return adjoint_impl<float>(h, (const float*)q_in, (const float*)y, (const float*)checkpoints, contacts, float(dt),
                              (const float*)adj_q_out, (const float*)adj_qd_out, (float*)adj_q_in, (float*)adj_qd_in,
                              (float*)adj_tri_mu, (float*)adj_tri_lambda, st);
 }

@@ -58,6 +58,28 @@ def _ptr(obj, what="array", typestr=None, count=None, at_least=None):
     return interop.pointer(obj, what, typestr, count, at_least)
 
 
+def contacts_desc(contacts, model):
+    """The ``VbdContactsDesc`` of a ``Contacts`` (its arrays checked for type and size), or None when there is
+    nothing to collide with."""
+    if contacts is None or contacts.soft_contact_max <= 0 or model.shape_count <= 0:
+        return None
+    cmax = int(contacts.soft_contact_max)
+    cdesc = _lib.VbdContactsDesc()
+    cdesc.soft_contact_count_dev = _ptr(contacts.soft_contact_count, "contacts.soft_contact_count", I32, at_least=1)
+    cdesc.soft_contact_max = cmax
+    cdesc.soft_contact_particle_dev = _ptr(contacts.soft_contact_particle, "contacts.soft_contact_particle", I32,
+                                           at_least=cmax)  # fmt: skip
+    cdesc.soft_contact_shape_dev = _ptr(contacts.soft_contact_shape, "contacts.soft_contact_shape", I32,
+                                        at_least=cmax)  # fmt: skip
+    cdesc.soft_contact_body_pos_dev = _ptr(contacts.soft_contact_body_pos, "contacts.soft_contact_body_pos", F32,
+                                           at_least=3 * cmax)  # fmt: skip
+    cdesc.soft_contact_body_vel_dev = _ptr(contacts.soft_contact_body_vel, "contacts.soft_contact_body_vel", F32,
+                                           at_least=3 * cmax)  # fmt: skip
+    cdesc.soft_contact_normal_dev = _ptr(contacts.soft_contact_normal, "contacts.soft_contact_normal", F32,
+                                         at_least=3 * cmax)  # fmt: skip
+    return cdesc
+
+
 class SolverVBD:
     def __init__(
         self,
@@ -327,23 +349,7 @@ class SolverVBD:
             if p is None:
                 raise TypeError(f"{name} must be a device array of particle_count x 3 values")
         f = _ptr(getattr(state_in, "particle_f", None), "state_in.particle_f", want, n3)
-        cdesc = None
-        if contacts is not None and contacts.soft_contact_max > 0 and self.model.shape_count > 0:
-            cmax = int(contacts.soft_contact_max)
-            cdesc = _lib.VbdContactsDesc()
-            cdesc.soft_contact_count_dev = _ptr(contacts.soft_contact_count, "contacts.soft_contact_count", I32,
-                                                at_least=1)  # fmt: skip
-            cdesc.soft_contact_max = cmax
-            cdesc.soft_contact_particle_dev = _ptr(contacts.soft_contact_particle, "contacts.soft_contact_particle",
-                                                   I32, at_least=cmax)  # fmt: skip
-            cdesc.soft_contact_shape_dev = _ptr(contacts.soft_contact_shape, "contacts.soft_contact_shape", I32,
-                                                at_least=cmax)  # fmt: skip
-            cdesc.soft_contact_body_pos_dev = _ptr(contacts.soft_contact_body_pos, "contacts.soft_contact_body_pos",
-                                                   F32, at_least=3 * cmax)  # fmt: skip
-            cdesc.soft_contact_body_vel_dev = _ptr(contacts.soft_contact_body_vel, "contacts.soft_contact_body_vel",
-                                                   F32, at_least=3 * cmax)  # fmt: skip
-            cdesc.soft_contact_normal_dev = _ptr(contacts.soft_contact_normal, "contacts.soft_contact_normal", F32,
-                                                 at_least=3 * cmax)  # fmt: skip
+        cdesc = contacts_desc(contacts, self.model)
         bodies = None
         if getattr(state_in, "body_q", None) is not None:
             bodies = _lib.VbdBodyState()

@@ -83,3 +83,70 @@ def test_fp32_adjoint_tracks_fp64():
         grads.append((Ev.grad.double(), v0.grad.double()))
     for a, b in zip(grads[0], grads[1], strict=True):
         assert (a - b).norm() / a.norm() <= 5e-2  # FP32 adjoint: a few percent after 6 substeps
+
+
+def test_adjoint_with_ground_contact_matches_fp64_central_differences():
+    """A 10 x 10 sheet pressed 1 mm into the ground and sliding at 0.3 m/s, so that every vertex has its contact's
+    penalty and IPC friction terms active (contact damping off: no term switches with the sign of the normal
+    velocity). Six substeps whose contacts are generated along the nominal trajectory and then held fixed, as the
+    adjoint differentiates the step for its contact set: directional derivatives in (per-triangle E, initial
+    velocity) against FP64 central differences, relative 1e-3."""
+    from newton_chysx_b200 import CollisionPipeline, sim
+
+    b = cloth_grid_builder(n=10, hanging=False, height=0.004, pin_top_corners=False, bend=1e-3)
+    b.add_ground_plane(cfg=sim.ShapeConfig(ke=2.5e3, kd=0.0, mu=0.6))
+    model = b.finalize("cuda")
+    model.soft_contact_ke, model.soft_contact_kd, model.soft_contact_mu = 1.0e3, 0.0, 0.5
+    dsim = DifferentiableVBD(model, iterations=5, precision="fp64")
+    pipe = CollisionPipeline(model, soft_contact_margin=0.01)
+    rng = np.random.default_rng(5)
+    T = model.tri_count
+    E = torch.tensor(10.0 ** rng.uniform(3.5, 4.5, size=T), dtype=torch.float64, device="cuda")
+    q0 = model.particle_q.to(torch.float64)
+    qd0 = torch.zeros_like(q0)
+    qd0[:, 0] = 0.3
+    target = q0 + torch.tensor(rng.normal(0.0, 0.01, size=q0.shape), dtype=torch.float64, device="cuda")
+    dt, substeps = 1.0 / 600.0, 6
+
+    mu0, lam0 = lame_from_young(E, NU, H)
+    dsim.set_materials(mu0, lam0)
+    contacts = []
+    with torch.no_grad():
+        q, qd = q0, qd0
+        for _ in range(substeps):
+            view = sim.State()
+            view.particle_q = q.float().contiguous()
+            c = pipe.contacts()
+            pipe.collide(view, c)
+            contacts.append(c)
+            q, qd = dsim.substep(q, qd, mu0, lam0, dt, contacts=c)
+    counts = [int(k.soft_contact_count.item()) for k in contacts]
+    assert min(counts) == model.particle_count  # every vertex in contact at every substep
+
+    def loss(mu, lam, v0):
+        dsim.set_materials(mu, lam)
+        q, qd = q0, v0
+        for k in range(substeps):
+            q, qd = dsim.substep(q, qd, mu, lam, dt, contacts=contacts[k])
+        return ((q - target) ** 2).sum(dim=1).mean()
+
+    mu = mu0.clone().requires_grad_(True)
+    lam = lam0.clone().requires_grad_(True)
+    v0 = qd0.clone().requires_grad_(True)
+    loss(mu, lam, v0).backward()
+    gmu, glam, gv = mu.grad.detach(), lam.grad.detach(), v0.grad.detach()
+    assert gv.abs().max() > 0
+    h, worst = 1e-4, 0.0
+    for _ in range(6):
+        dE = torch.tensor(rng.normal(size=E.shape), device="cuda", dtype=torch.float64)
+        dv = torch.tensor(rng.normal(size=qd0.shape), device="cuda", dtype=torch.float64)
+        dE, dv = dE / dE.abs().max(), dv / dv.norm()
+        with torch.no_grad():
+            mu_p, lam_p = lame_from_young(E * (1.0 + h * dE), NU, H)
+            mu_m, lam_m = lame_from_young(E * (1.0 - h * dE), NU, H)
+            fd = float(loss(mu_p, lam_p, qd0 + h * dv) - loss(mu_m, lam_m, qd0 - h * dv))
+            d_mu = mu_p.float().double() - mu_m.float().double()
+            d_lam = lam_p.float().double() - lam_m.float().double()
+            ad = float((gmu * d_mu).sum() + (glam * d_lam).sum() + (gv * (2.0 * h * dv)).sum())
+        worst = max(worst, abs(ad - fd) / max(abs(fd), 1e-30))
+    assert worst <= 1e-3, worst

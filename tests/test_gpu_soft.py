@@ -158,7 +158,7 @@ def test_soft_model_rejects_stencil_layouts_and_adjoint():
     assert solver.layout == "csr"
     q = _state(g["s0_q_in"])
     out = torch.zeros_like(q)
-    rc = solver._lib.vbd_record_step(solver._h, q.data_ptr(), q.data_ptr(), None, 1.0 / 600.0, out.data_ptr(),
+    rc = solver._lib.vbd_record_step(solver._h, q.data_ptr(), q.data_ptr(), None, None, 1.0 / 600.0, out.data_ptr(),
                                      torch.zeros(3 * q.numel(), device="cuda").data_ptr(), out.data_ptr(),
                                      out.data_ptr(), None)  # fmt: skip
     assert rc == _lib.VBD_ERR_UNSUPPORTED
