@@ -1,4 +1,5 @@
-// Hand-written adjoint of the fixed-iteration VBD step (one substep, with particle-shape contacts on static shapes).
+// Hand-written adjoint of the fixed-iteration VBD step (one substep: membrane and bending with their damping,
+// particle-shape contacts on static shapes).
 //
 // Forward map of one substep (vbd_kernels.cuh, CSR path, one lane per vertex):
 //   y   = q + (qd + (g + f_ext / m) dt) dt                    inertial target, also the first iterate
@@ -15,9 +16,9 @@
 // element's vertex coordinates (and the triangle's mu, lambda), running the same element routines
 // as the forward pass. Vertices of one color are never neighbours, so the vertices written through
 // atomics (the neighbours, the triangle parameters) are never read by the same launch.
-// A contact term depends on the vertex's position x and, through its friction and damping, on the
-// vertex's position at the start of the substep, q; its derivative in q is accumulated per vertex
-// (adj_xp) and joins dL/dq_in at the end. The contact set, the contact points and normals and the penalty
+// A contact term and a damped element depend on positions x and, through friction and damping, on the
+// positions at the start of the substep, q; the derivatives in q are accumulated per vertex (adj_xp) and
+// join dL/dq_in at the end. The contact set, the contact points and normals and the penalty
 // stiffness are held fixed (the derivative of the step for its contacts; the AVBD ramp is off).
 #pragma once
 #include "vbd_dual.cuh"
@@ -74,8 +75,10 @@ __device__ __forceinline__ void assemble(const StepCtx<R>& c, const R* X, int v,
     const int4 ti = c.tri_idx[t];
     const float4 dm = c.tri_pose[t];
     const R pose[4] = {R(dm.x), R(dm.y), R(dm.z), R(dm.w)};
-    membrane_add<R>(ord, ldx(X, ti.x), ldx(X, ti.y), ldx(X, ti.z), pose, R(mat.x), R(mat.y), R(0), R(mat.w), c.dt,
-                    nullptr, f, H);
+    vec3<R> xp[3];
+    if (mat.z > 0.f) xp[0] = ld3<R>(c.qprev[ti.x]), xp[1] = ld3<R>(c.qprev[ti.y]), xp[2] = ld3<R>(c.qprev[ti.z]);
+    membrane_add<R>(ord, ldx(X, ti.x), ldx(X, ti.y), ldx(X, ti.z), pose, R(mat.x), R(mat.y), R(mat.z), R(mat.w), c.dt,
+                    xp, f, H);
   }
   for (int a = c.edge_off[v]; a < c.edge_off[v + 1]; ++a) {
     const int e = c.edge_adj[a] >> 2, ord = c.edge_adj[a] & 3;
@@ -83,7 +86,11 @@ __device__ __forceinline__ void assemble(const StepCtx<R>& c, const R* X, int v,
     if (!(pr.z > 0.f)) continue;
     const int4 ei = c.edge_idx[e];
     const vec3<R> xs[4] = {ldx(X, ei.x), ldx(X, ei.y), ldx(X, ei.z), ldx(X, ei.w)};
-    bending_add<R>(ord, xs, R(pr.x), R(pr.y), R(pr.z), R(0), c.dt, nullptr, f, H);
+    vec3<R> xp[4];
+    if (pr.w > 0.f)
+      xp[0] = ld3<R>(c.qprev[ei.x]), xp[1] = ld3<R>(c.qprev[ei.y]), xp[2] = ld3<R>(c.qprev[ei.z]),
+      xp[3] = ld3<R>(c.qprev[ei.w]);
+    bending_add<R>(ord, xs, R(pr.x), R(pr.y), R(pr.z), R(pr.w), c.dt, xp, f, H);
   }
 }
 
@@ -124,9 +131,81 @@ __device__ __forceinline__ void contacts_adjoint(const StepCtx<R>& c, int v, vec
     ax = ax + vec3<R>{contract(fd, Hd, w, Hb, 0), contract(fd, Hd, w, Hb, 1), contract(fd, Hd, w, Hb, 2)};
     gxp = gxp + vec3<R>{contract(fd, Hd, w, Hb, 3), contract(fd, Hd, w, Hb, 4), contract(fd, Hd, w, Hb, 5)};
   }
-  adj_xp[3 * v] += gxp.x;
-  adj_xp[3 * v + 1] += gxp.y;
-  adj_xp[3 * v + 2] += gxp.z;
+  atomic_add3(adj_xp, v, gxp);  // neighbours' damped elements add to the same entry in this launch
+}
+
+// dL/dx of an element's vertices from its dual-number terms: slot 3j+k of vertex j (the solved vertex's part to ax,
+// the others through atomics) and, from slot `sp` on, of the vertices' start positions into adj_xp.
+template <typename R, int N>
+__device__ __forceinline__ void scatter_element(const AdjCtx<R>& A, int v, const int* vid, int nv, int sp,
+                                                const vec3<Dual<R, N>>& fd, const sym3<Dual<R, N>>& Hd, vec3<R> w,
+                                                const sym3<R>& Hb, vec3<R>& ax) {
+  for (int j = 0; j < nv; ++j) {
+    const vec3<R> gj = {contract(fd, Hd, w, Hb, 3 * j), contract(fd, Hd, w, Hb, 3 * j + 1),
+                        contract(fd, Hd, w, Hb, 3 * j + 2)};
+    if (vid[j] == v)
+      ax = ax + gj;
+    else
+      atomic_add3(A.adj_x, vid[j], gj);
+    if (sp > 0)
+      atomic_add3(A.adj_xp, vid[j], vec3<R>{contract(fd, Hd, w, Hb, sp + 3 * j), contract(fd, Hd, w, Hb, sp + 3 * j + 1),
+                                            contract(fd, Hd, w, Hb, sp + 3 * j + 2)});
+  }
+}
+
+// Membrane term of face t for the solved vertex v over the face's 9 coordinates (slots 0-8), mu and lambda (9, 10)
+// and, for a damped face (N = 20), the 9 coordinates of the face's start positions (11-19).
+template <typename R, int N>
+__device__ __forceinline__ void membrane_adjoint(const AdjCtx<R>& A, int v, int t, int ord, vec3<R> w,
+                                                 const sym3<R>& Hb, vec3<R>& ax) {
+  const StepCtx<R>& c = A.c;
+  using D = Dual<R, N>;
+  const float4 mat = c.tri_mat[t];
+  const int4 ti = c.tri_idx[t];
+  const int vid[3] = {ti.x, ti.y, ti.z};
+  const float4 dm = c.tri_pose[t];
+  vec3<D> xs[3], xp[3];
+  for (int j = 0; j < 3; ++j) {
+    const vec3<R> p = ldx(A.x, vid[j]);
+    xs[j] = {D::seed(p.x, 3 * j), D::seed(p.y, 3 * j + 1), D::seed(p.z, 3 * j + 2)};
+    if (N > 11) {
+      const vec3<R> pp = ld3<R>(c.qprev[vid[j]]);
+      xp[j] = {D::seed(pp.x, 11 + 3 * j), D::seed(pp.y, 12 + 3 * j), D::seed(pp.z, 13 + 3 * j)};
+    }
+  }
+  const D pose[4] = {D(R(dm.x)), D(R(dm.y)), D(R(dm.z)), D(R(dm.w))};
+  vec3<D> fd = {D(R(0)), D(R(0)), D(R(0))};
+  sym3<D> Hd = szero<D>();
+  membrane_add<D>(ord, xs[0], xs[1], xs[2], pose, D::seed(R(mat.x), 9), D::seed(R(mat.y), 10),
+                  D(R(N > 11 ? mat.z : 0.f)), D(R(mat.w)), D(c.dt), xp, fd, Hd);
+  scatter_element<R, N>(A, v, vid, 3, N > 11 ? 11 : 0, fd, Hd, w, Hb, ax);
+  if (A.adj_mu) atomicAdd(A.adj_mu + t, contract(fd, Hd, w, Hb, 9));
+  if (A.adj_lambda) atomicAdd(A.adj_lambda + t, contract(fd, Hd, w, Hb, 10));
+}
+
+// Bending term of hinge e over its 12 coordinates (slots 0-11) and, for a damped hinge (N = 24), the 12
+// coordinates of its start positions (12-23).
+template <typename R, int N>
+__device__ __forceinline__ void bending_adjoint(const AdjCtx<R>& A, int v, int e, int ord, vec3<R> w,
+                                                const sym3<R>& Hb, vec3<R>& ax) {
+  const StepCtx<R>& c = A.c;
+  using D = Dual<R, N>;
+  const float4 pr = c.edge_prop[e];
+  const int4 ei = c.edge_idx[e];
+  const int vid[4] = {ei.x, ei.y, ei.z, ei.w};
+  vec3<D> xs[4], xp[4];
+  for (int j = 0; j < 4; ++j) {
+    const vec3<R> p = ldx(A.x, vid[j]);
+    xs[j] = {D::seed(p.x, 3 * j), D::seed(p.y, 3 * j + 1), D::seed(p.z, 3 * j + 2)};
+    if (N > 12) {
+      const vec3<R> pp = ld3<R>(c.qprev[vid[j]]);
+      xp[j] = {D::seed(pp.x, 12 + 3 * j), D::seed(pp.y, 13 + 3 * j), D::seed(pp.z, 14 + 3 * j)};
+    }
+  }
+  vec3<D> fd = {D(R(0)), D(R(0)), D(R(0))};
+  sym3<D> Hd = szero<D>();
+  bending_add<D>(ord, xs, D(R(pr.x)), D(R(pr.y)), D(R(pr.z)), D(R(N > 12 ? pr.w : 0.f)), D(c.dt), xp, fd, Hd);
+  scatter_element<R, N>(A, v, vid, 4, N > 12 ? 12 : 0, fd, Hd, w, Hb, ax);
 }
 
 template <typename R>
@@ -155,60 +234,25 @@ __global__ void k_adjoint_color(AdjCtx<R> A, const int* __restrict__ verts, int 
   // inertia term: g = md (y - x)
   vec3<R> ax = a - md * w;
   atomic_add3(A.adj_y, v, md * w);
-  // membranes: 9 coordinates + (mu, lambda)
+  // membranes: 9 coordinates + (mu, lambda) [+ 9 start coordinates with damping]
   for (int q = c.face_off[v]; q < c.face_off[v + 1]; ++q) {
     const int t = c.face_adj[q] >> 2, ord = c.face_adj[q] & 3;
     const float4 mat = c.tri_mat[t];
     if (!(mat.x > 0.f || mat.y > 0.f)) continue;
-    const int4 ti = c.tri_idx[t];
-    const int vid[3] = {ti.x, ti.y, ti.z};
-    const float4 dm = c.tri_pose[t];
-    using D11 = Dual<R, 11>;
-    vec3<D11> xs[3];
-    for (int j = 0; j < 3; ++j) {
-      const vec3<R> p = ldx(A.x, vid[j]);
-      xs[j] = {D11::seed(p.x, 3 * j), D11::seed(p.y, 3 * j + 1), D11::seed(p.z, 3 * j + 2)};
-    }
-    const D11 pose[4] = {D11(R(dm.x)), D11(R(dm.y)), D11(R(dm.z)), D11(R(dm.w))};
-    vec3<D11> fd = {D11(R(0)), D11(R(0)), D11(R(0))};
-    sym3<D11> Hd = szero<D11>();
-    membrane_add<D11>(ord, xs[0], xs[1], xs[2], pose, D11::seed(R(mat.x), 9), D11::seed(R(mat.y), 10), D11(R(0)),
-                      D11(R(mat.w)), D11(c.dt), nullptr, fd, Hd);
-    for (int j = 0; j < 3; ++j) {
-      const vec3<R> gj = {contract(fd, Hd, w, Hb, 3 * j), contract(fd, Hd, w, Hb, 3 * j + 1),
-                          contract(fd, Hd, w, Hb, 3 * j + 2)};
-      if (vid[j] == v)
-        ax = ax + gj;
-      else
-        atomic_add3(A.adj_x, vid[j], gj);
-    }
-    if (A.adj_mu) atomicAdd(A.adj_mu + t, contract(fd, Hd, w, Hb, 9));
-    if (A.adj_lambda) atomicAdd(A.adj_lambda + t, contract(fd, Hd, w, Hb, 10));
+    if (mat.z > 0.f)
+      membrane_adjoint<R, 20>(A, v, t, ord, w, Hb, ax);
+    else
+      membrane_adjoint<R, 11>(A, v, t, ord, w, Hb, ax);
   }
-  // bending hinges: 12 coordinates
+  // bending hinges: 12 coordinates [+ 12 start coordinates with damping]
   for (int q = c.edge_off[v]; q < c.edge_off[v + 1]; ++q) {
     const int e = c.edge_adj[q] >> 2, ord = c.edge_adj[q] & 3;
     const float4 pr = c.edge_prop[e];
     if (!(pr.z > 0.f)) continue;
-    const int4 ei = c.edge_idx[e];
-    const int vid[4] = {ei.x, ei.y, ei.z, ei.w};
-    using D12 = Dual<R, 12>;
-    vec3<D12> xs[4];
-    for (int j = 0; j < 4; ++j) {
-      const vec3<R> p = ldx(A.x, vid[j]);
-      xs[j] = {D12::seed(p.x, 3 * j), D12::seed(p.y, 3 * j + 1), D12::seed(p.z, 3 * j + 2)};
-    }
-    vec3<D12> fd = {D12(R(0)), D12(R(0)), D12(R(0))};
-    sym3<D12> Hd = szero<D12>();
-    bending_add<D12>(ord, xs, D12(R(pr.x)), D12(R(pr.y)), D12(R(pr.z)), D12(R(0)), D12(c.dt), nullptr, fd, Hd);
-    for (int j = 0; j < 4; ++j) {
-      const vec3<R> gj = {contract(fd, Hd, w, Hb, 3 * j), contract(fd, Hd, w, Hb, 3 * j + 1),
-                          contract(fd, Hd, w, Hb, 3 * j + 2)};
-      if (vid[j] == v)
-        ax = ax + gj;
-      else
-        atomic_add3(A.adj_x, vid[j], gj);
-    }
+    if (pr.w > 0.f)
+      bending_adjoint<R, 24>(A, v, e, ord, w, Hb, ax);
+    else
+      bending_adjoint<R, 12>(A, v, e, ord, w, Hb, ax);
   }
   if (c.has_contacts) contacts_adjoint(c, v, x, w, Hb, ax, A.adj_xp);
   A.adj_x[3 * v] = ax.x;

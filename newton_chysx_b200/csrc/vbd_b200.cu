@@ -1503,12 +1503,12 @@ int adjoint_impl(VbdSolver* h, const R* q_in, const R* y, const R* ck, const Vbd
   c.dt = dt;
   c.dt2r = R(1) / (dt * dt);
   k_adjoint_begin<R><<<int((n3 + 255) / 256), 256, 0, st>>>(int(n3), aq_out, aqd_out, R(1) / dt, ax, ay);
+  // this substep's start positions (damping and contact terms) and contact table, as its forward pass had them
+  k_adjoint_qprev<R><<<(V + 255) / 256, 256, 0, st>>>(c);
+  CK(cudaMemsetAsync(axp, 0, n3 * sizeof(R), st));
   if (has_c) {
-    // this substep's start positions and contact table, as its forward pass had them
-    k_adjoint_qprev<R><<<(V + 255) / 256, 256, 0, st>>>(c);
     CK(cudaMemsetAsync(h->slot_cnt, 0, sizeof(int) * V, st));
     k_contact_prepare<R><<<(c.c_max + 255) / 256, 256, 0, st>>>(c);
-    CK(cudaMemsetAsync(axp, 0, n3 * sizeof(R), st));
   }
   AdjCtx<R> A{c, nullptr, y, ax, ay, adj_mu, adj_lambda, axp};
   const int* cp = h->md.color_particles_dev;
@@ -1526,7 +1526,7 @@ int adjoint_impl(VbdSolver* h, const R* q_in, const R* y, const R* ck, const Vbd
       if (b > a) k_adjoint_color<R><<<(b - a + 63) / 64, 64, 0, st>>>(A, cp + a, b - a);
     }
   }
-  k_adjoint_end<R><<<(V + 255) / 256, 256, 0, st>>>(c, ax, ay, has_c ? axp : nullptr, aqd_out, aq_in, aqd_in);
+  k_adjoint_end<R><<<(V + 255) / 256, 256, 0, st>>>(c, ax, ay, axp, aqd_out, aq_in, aqd_in);
   CK(cudaGetLastError());
   return VBD_OK;
 }
