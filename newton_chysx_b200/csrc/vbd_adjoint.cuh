@@ -1,5 +1,5 @@
-// Hand-written adjoint of the fixed-iteration VBD step (one substep: membrane and bending with their damping,
-// particle-shape contacts on static shapes).
+// Hand-written adjoint of the fixed-iteration VBD step (one substep: membrane, bending, tetrahedra and springs
+// with their damping, particle-shape contacts on static shapes).
 //
 // Forward map of one substep (vbd_kernels.cuh, CSR path, one lane per vertex):
 //   y   = q + (qd + (g + f_ext / m) dt) dt                    inertial target, also the first iterate
@@ -91,6 +91,34 @@ __device__ __forceinline__ void assemble(const StepCtx<R>& c, const R* X, int v,
       xp[0] = ld3<R>(c.qprev[ei.x]), xp[1] = ld3<R>(c.qprev[ei.y]), xp[2] = ld3<R>(c.qprev[ei.z]),
       xp[3] = ld3<R>(c.qprev[ei.w]);
     bending_add<R>(ord, xs, R(pr.x), R(pr.y), R(pr.z), R(pr.w), c.dt, xp, f, H);
+  }
+  if (c.tet_off) {  // tetrahedra (solve_elasticity adds them after the hinges)
+    for (int a = c.tet_off[v]; a < c.tet_off[v + 1]; ++a) {
+      const int t = c.tet_adj[a] >> 2, ord = c.tet_adj[a] & 3;
+      const float4 r0 = c.tet_pose[3 * t], r1 = c.tet_pose[3 * t + 1], r2 = c.tet_pose[3 * t + 2];
+      if (!(r0.w > 0.f || r1.w > 0.f)) continue;
+      const int4 ti = c.tet_idx[t];
+      const R dm[9] = {R(r0.x), R(r0.y), R(r0.z), R(r1.x), R(r1.y), R(r1.z), R(r2.x), R(r2.y), R(r2.z)};
+      const vec3<R> xs[4] = {ldx(X, ti.x), ldx(X, ti.y), ldx(X, ti.z), ldx(X, ti.w)};
+      vec3<R> xp[4];
+      if (r2.w > 0.f)
+        xp[0] = ld3<R>(c.qprev[ti.x]), xp[1] = ld3<R>(c.qprev[ti.y]), xp[2] = ld3<R>(c.qprev[ti.z]),
+        xp[3] = ld3<R>(c.qprev[ti.w]);
+      tet_add<R>(ord, xs, xp, dm, R(r0.w), R(r1.w), R(r2.w), c.dt, f, H);
+    }
+  }
+  if (c.spr_off) {  // springs to other colors, then springs within the color: all at the color's start state
+    for (int pass = 0; pass < 2; ++pass) {
+      const int* off = pass == 0 ? c.spr_off : c.sspr_off;
+      const int* adj = pass == 0 ? c.spr_adj : c.sspr_adj;
+      for (int a = off[v]; a < off[v + 1]; ++a) {
+        const int sp = adj[a] >> 1, end = adj[a] & 1;
+        const int2 ij = c.spr_idx[sp];
+        const float4 pr = c.spr_prop[sp];
+        const vec3<R> xa = pr.z != 0.f ? ld3<R>(c.qprev[v]) : zero3<R>();
+        spring_add<R>(end, ldx(X, v), ldx(X, end == 0 ? ij.y : ij.x), xa, R(pr.x), R(pr.y), R(pr.z), c.dt, f, H);
+      }
+    }
   }
 }
 
@@ -208,6 +236,55 @@ __device__ __forceinline__ void bending_adjoint(const AdjCtx<R>& A, int v, int e
   scatter_element<R, N>(A, v, vid, 4, N > 12 ? 12 : 0, fd, Hd, w, Hb, ax);
 }
 
+// Tetrahedron term over its 12 coordinates (slots 0-11) and, for a damped tet (N = 24), its 12 start coordinates.
+template <typename R, int N>
+__device__ __forceinline__ void tet_adjoint(const AdjCtx<R>& A, int v, int t, int ord, vec3<R> w, const sym3<R>& Hb,
+                                            vec3<R>& ax) {
+  const StepCtx<R>& c = A.c;
+  using D = Dual<R, N>;
+  const float4 r0 = c.tet_pose[3 * t], r1 = c.tet_pose[3 * t + 1], r2 = c.tet_pose[3 * t + 2];
+  const int4 ti = c.tet_idx[t];
+  const int vid[4] = {ti.x, ti.y, ti.z, ti.w};
+  const D dm[9] = {D(R(r0.x)), D(R(r0.y)), D(R(r0.z)), D(R(r1.x)), D(R(r1.y)), D(R(r1.z)),
+                   D(R(r2.x)), D(R(r2.y)), D(R(r2.z))};
+  vec3<D> xs[4], xp[4];
+  for (int j = 0; j < 4; ++j) {
+    const vec3<R> p = ldx(A.x, vid[j]);
+    xs[j] = {D::seed(p.x, 3 * j), D::seed(p.y, 3 * j + 1), D::seed(p.z, 3 * j + 2)};
+    if (N > 12) {
+      const vec3<R> pp = ld3<R>(c.qprev[vid[j]]);
+      xp[j] = {D::seed(pp.x, 12 + 3 * j), D::seed(pp.y, 13 + 3 * j), D::seed(pp.z, 14 + 3 * j)};
+    }
+  }
+  vec3<D> fd = {D(R(0)), D(R(0)), D(R(0))};
+  sym3<D> Hd = szero<D>();
+  tet_add<D>(ord, xs, xp, dm, D(R(r0.w)), D(R(r1.w)), D(R(N > 12 ? r2.w : 0.f)), D(c.dt), fd, Hd);
+  scatter_element<R, N>(A, v, vid, 4, N > 12 ? 12 : 0, fd, Hd, w, Hb, ax);
+}
+
+// Spring term of entry (spring << 1) | end of vertex v over x_v (slots 0-2), the other end (3-5) and v's start
+// position (6-8, read by the damping).
+template <typename R>
+__device__ __forceinline__ void spring_adjoint(const AdjCtx<R>& A, int v, int a, vec3<R> w, const sym3<R>& Hb,
+                                               vec3<R>& ax) {
+  const StepCtx<R>& c = A.c;
+  using D = Dual<R, 9>;
+  const int sp = a >> 1, end = a & 1;
+  const int2 ij = c.spr_idx[sp];
+  const float4 pr = c.spr_prop[sp];
+  const int o = end == 0 ? ij.y : ij.x;
+  const vec3<R> pv = ldx(A.x, v), po = ldx(A.x, o), pa = ld3<R>(c.qprev[v]);
+  const vec3<D> xv = {D::seed(pv.x, 0), D::seed(pv.y, 1), D::seed(pv.z, 2)};
+  const vec3<D> xo = {D::seed(po.x, 3), D::seed(po.y, 4), D::seed(po.z, 5)};
+  const vec3<D> xa = {D::seed(pa.x, 6), D::seed(pa.y, 7), D::seed(pa.z, 8)};
+  vec3<D> fd = {D(R(0)), D(R(0)), D(R(0))};
+  sym3<D> Hd = szero<D>();
+  spring_add<D>(end, xv, xo, xa, D(R(pr.x)), D(R(pr.y)), D(R(pr.z)), D(c.dt), fd, Hd);
+  ax = ax + vec3<R>{contract(fd, Hd, w, Hb, 0), contract(fd, Hd, w, Hb, 1), contract(fd, Hd, w, Hb, 2)};
+  atomic_add3(A.adj_x, o, vec3<R>{contract(fd, Hd, w, Hb, 3), contract(fd, Hd, w, Hb, 4), contract(fd, Hd, w, Hb, 5)});
+  atomic_add3(A.adj_xp, v, vec3<R>{contract(fd, Hd, w, Hb, 6), contract(fd, Hd, w, Hb, 7), contract(fd, Hd, w, Hb, 8)});
+}
+
 template <typename R>
 __global__ void k_adjoint_color(AdjCtx<R> A, const int* __restrict__ verts, int n) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -253,6 +330,21 @@ __global__ void k_adjoint_color(AdjCtx<R> A, const int* __restrict__ verts, int 
       bending_adjoint<R, 24>(A, v, e, ord, w, Hb, ax);
     else
       bending_adjoint<R, 12>(A, v, e, ord, w, Hb, ax);
+  }
+  if (c.tet_off) {
+    for (int q = c.tet_off[v]; q < c.tet_off[v + 1]; ++q) {
+      const int t = c.tet_adj[q] >> 2, ord = c.tet_adj[q] & 3;
+      const float4 r0 = c.tet_pose[3 * t], r1 = c.tet_pose[3 * t + 1], r2 = c.tet_pose[3 * t + 2];
+      if (!(r0.w > 0.f || r1.w > 0.f)) continue;
+      if (r2.w > 0.f)
+        tet_adjoint<R, 24>(A, v, t, ord, w, Hb, ax);
+      else
+        tet_adjoint<R, 12>(A, v, t, ord, w, Hb, ax);
+    }
+  }
+  if (c.spr_off) {
+    for (int q = c.spr_off[v]; q < c.spr_off[v + 1]; ++q) spring_adjoint(A, v, c.spr_adj[q], w, Hb, ax);
+    for (int q = c.sspr_off[v]; q < c.sspr_off[v + 1]; ++q) spring_adjoint(A, v, c.sspr_adj[q], w, Hb, ax);
   }
   if (c.has_contacts) contacts_adjoint(c, v, x, w, Hb, ax, A.adj_xp);
   A.adj_x[3 * v] = ax.x;

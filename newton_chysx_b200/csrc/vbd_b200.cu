@@ -1968,7 +1968,6 @@ int vbd_record_step(VbdHandle h, const void* q_in, const void* qd_in, const void
                     const VbdContactsDesc* contacts, double dt, void* y, void* checkpoints, void* q_out, void* qd_out,
                     void* stream) {
   if (!h || !q_in || !qd_in || !y || !checkpoints || !q_out || !qd_out || !(dt > 0.0)) return VBD_ERR_INVALID_ARGUMENT;
-  if (h->soft) return VBD_ERR_UNSUPPORTED;
   cudaStream_t st = (cudaStream_t)stream;
   if (h->precision == VBD_PRECISION_FP64)
     return record_impl<double>(h, (const double*)q_in, (const double*)qd_in, (const double*)particle_f, contacts, dt,
@@ -1981,7 +1980,6 @@ int vbd_adjoint_step(VbdHandle h, const void* q_in, const void* y, const void* c
                      const VbdContactsDesc* contacts, double dt, const void* adj_q_out, const void* adj_qd_out,
                      void* adj_q_in, void* adj_qd_in, void* adj_tri_mu, void* adj_tri_lambda, void* stream) {
   if (!h || !q_in || !y || !checkpoints || !adj_q_in || !(dt > 0.0)) return VBD_ERR_INVALID_ARGUMENT;
-  if (h->soft) return VBD_ERR_UNSUPPORTED;
   cudaStream_t st = (cudaStream_t)stream;
   if (h->precision == VBD_PRECISION_FP64)
     return adjoint_impl<double>(h, (const double*)q_in, (const double*)y, (const double*)checkpoints, contacts, dt,
