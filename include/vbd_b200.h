@@ -187,8 +187,8 @@ int vbd_step_f64(VbdHandle h, double* q_in_dev, double* q_out_dev, const double*
    inertial targets and checkpoints [(iterations+1),V,3] the positions at the start of every iteration and at
    the end. Arrays are float32, or float64 for a VBD_PRECISION_FP64 solver. q_out/qd_out receive the step's
    result (q_in is not modified). contacts: this substep's particle-shape contacts against static shapes, or
-   NULL; the adjoint must be given the same arrays. VBD_ERR_UNSUPPORTED for models with springs or tetrahedra
-   (the adjoint covers cloth only) and for contacts with the AVBD penalty ramp on (rigid_avbd_beta > 0). */
+   NULL; the adjoint must be given the same arrays. Membranes, hinges, tetrahedra and springs with their damping
+   take part. VBD_ERR_UNSUPPORTED for contacts with the AVBD penalty ramp on (rigid_avbd_beta > 0). */
 int vbd_record_step(VbdHandle h, const void* q_in_dev, const void* qd_in_dev, const void* particle_f_dev,
                     const VbdContactsDesc* contacts, double dt, void* y_dev, void* checkpoints_dev, void* q_out_dev,
                     void* qd_out_dev, void* stream);

@@ -5,7 +5,7 @@ keeps the positions at the start of every iteration (per-iteration checkpoints).
 recomputes the per-color states of one iteration from its checkpoint and walks the colors backwards.
 Gradients flow to the input positions and velocities and to the triangles' Lame coefficients
 (``Model.tri_materials[:, 0:2]``), hence to anything they are computed from, e.g. per-triangle
-Young's moduli.
+Young's moduli. Membranes, hinges, tetrahedra and springs take part with their damping.
 
 The reference VBD has no gradient: its kernels are built with ``enable_backward=False``
 (``newton/_src/solvers/vbd/particle_vbd_kernels.py:27-28``). The check is against central finite
