@@ -217,7 +217,7 @@ def run_e2e(args, dev, dist, states, shape, total, shard, vi_all_ranks):
                            oq=torch.empty_like(hq).pin_memory(), oqd=torch.empty_like(hqd).pin_memory(),
                            stream=stream))  # fmt: skip
     assert v0 == hq_all.shape[0], "the chunks must cover the batch"
-    Ke = max(1, min(args.steps, args.e2e_steps))
+    Ke = max(1, args.e2e_steps if args.e2e_steps > 0 else args.steps)  # default: as many substeps as the timed region
     cur = torch.cuda.current_stream(dev)
 
     def run(k):
@@ -1656,7 +1656,7 @@ def main():
     ap.add_argument("--warp", action="store_true", help="soft workload: one warp per instance")
     ap.add_argument("--no-tune", dest="tune", action="store_false", help="use the launch-shape flags, not the autotuner")
     ap.add_argument("--tune-instances", type=int, default=1024)
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=0, help="substeps of the end-to-end leg (0: --steps)")
     ap.add_argument("--e2e-chunks", type=int, default=4, help="instance groups pipelined on separate streams in e2e")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
