@@ -93,14 +93,16 @@ def test_mixed_precision_keeps_contact_vertices_without_truncation(steps):
 
 
 def test_mixed_precision_on_the_draped_sheet_with_self_contact(steps):
-    """With self-contact the truncation bounds every move, and FP32 departs from FP64 by more than 1e-4 m at 21 %
-    of the vertices (measured 13,691), mixed at 1.4 % (945), within a few times the step's own discontinuity
-    floor: FP64 from an input moved by 1e-8 m departs from FP64 at a few hundred vertices by up to millimetres
-    (the FP64 oracle: 242 vertices, 1.4e-3 m)."""
+    """With self-contact the truncation bounds every move, and FP32 departs from FP64 by more than 1e-4 m at about
+    21 % of the vertices (measured 13,691 to 14,141 over builds that sum in different orders), mixed at about 1.2 %
+    (715 to 945), and mixed's largest departure is that of the step's own discontinuity floor: FP64 from an input
+    moved by 1e-8 m departs from FP64 by up to millimetres (measured 1.4e-3 to 1.6e-3 m; the FP64 oracle,
+    1.4e-3 m). How many vertices cross 1e-4 m at the floor depends on which switches one perturbation flips (59 to
+    242 measured), so the floor is compared by its largest departure."""
     ref = steps["fp64", True]
     d32, dmx, floor = _dist(steps["fp32", True], ref), _dist(steps["mixed", True], ref), _dist(steps["floor"], ref)
     n32, nmx, nfl = (int((d > 1e-4).sum()) for d in (d32, dmx, floor))
     assert nmx * 5 < n32, (nmx, n32)
     assert float(dmx.max()) < 1e-2
     assert float(floor.max()) > 1e-4 and nfl > 0  # the discontinuity is there in FP64 too
-    assert nmx <= 10 * nfl, (nmx, nfl)
+    assert float(dmx.max()) <= 3.0 * float(floor.max()), (float(dmx.max()), float(floor.max()))
