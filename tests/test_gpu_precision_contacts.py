@@ -10,7 +10,7 @@ solves those vertices in FP64.
 
 What remains is the step's own discontinuity: the damping switches on and off with the sign of a contact's normal
 velocity, which is near zero for a resting vertex, so the FP64 step from an input moved by 1e-8 m (below the FP32
-rounding of the positions) already departs from the FP64 step by up to millimetres at a few hundred vertices; the
+rounding of the positions) already departs from the FP64 step by up to millimetres at hundreds of vertices; the
 FP64 oracle does the same."""
 
 import numpy as np
@@ -42,7 +42,7 @@ def draped():
     return m, pipe, s0.particle_q.clone(), s0.particle_qd.clone()
 
 
-def _step(draped, precision, self_contact=True, noise=0.0):
+def _step(draped, precision, self_contact=True, noise=0.0, seed=7):
     m, pipe, q0, qd0 = draped
     kw = dict(bench.SC_KW, particle_enable_self_contact=self_contact)
     solver = SolverVBD(m, iterations=bench.SC_ITERATIONS, precision=precision, **kw)
@@ -57,7 +57,7 @@ def _step(draped, precision, self_contact=True, noise=0.0):
     v.particle_q = a.particle_q.float()
     pipe.collide(v, c)  # contacts from the FP32 positions in every precision
     if noise:
-        gen = torch.Generator(device=q0.device).manual_seed(7)
+        gen = torch.Generator(device=q0.device).manual_seed(seed)
         active = (m.particle_flags & 1).bool()[:, None]
         a.particle_q += noise * torch.randn(a.particle_q.shape, generator=gen, device=q0.device,
                                             dtype=a.particle_q.dtype) * active  # fmt: skip
@@ -76,7 +76,12 @@ def steps(draped):
     for sc in (False, True):
         for prec in ("fp32", "mixed", "fp64"):
             out[prec, sc] = _step(draped, prec, sc)
-    out["floor"] = _step(draped, "fp64", True, noise=1e-8)
+    # The floor: the largest departure at each vertex over FP64 steps from inputs moved by 1e-8 m and, three
+    # times over, by 1e-7 m (about the FP32 rounding of the positions, which the mixed step stores between
+    # iterations). One perturbation alone flips a varying handful of switches.
+    ref = out["fp64", True]
+    runs = [_step(draped, "fp64", True, noise=n, seed=k) for n, k in ((1e-8, 7), (1e-7, 7), (1e-7, 8), (1e-7, 9))]
+    out["floor"] = torch.stack([_dist(r, ref) for r in runs]).amax(0)  # per-vertex departure, not positions
     return out
 
 
@@ -95,14 +100,15 @@ def test_mixed_precision_keeps_contact_vertices_without_truncation(steps):
 def test_mixed_precision_on_the_draped_sheet_with_self_contact(steps):
     """With self-contact the truncation bounds every move, and FP32 departs from FP64 by more than 1e-4 m at about
     21 % of the vertices (measured 13,691 to 14,141 over builds that sum in different orders), mixed at about 1.2 %
-    (715 to 945), and mixed's largest departure is that of the step's own discontinuity floor: FP64 from an input
-    moved by 1e-8 m departs from FP64 by up to millimetres (measured 1.4e-3 to 1.6e-3 m; the FP64 oracle,
-    1.4e-3 m). How many vertices cross 1e-4 m at the floor depends on which switches one perturbation flips (59 to
-    242 measured), so the floor is compared by its largest departure."""
+    (715 to 945), and mixed's largest departure is that of the step's own discontinuity floor: FP64 from inputs
+    moved by 1e-8 m to 1e-7 m departs from FP64 by up to millimetres (over the four perturbations 1.9e-3 m, 886
+    vertices past 1e-4 m; one 1e-8 m perturbation alone measured 4.9e-4 to 1.6e-3 m over 59 to 242 vertices; the
+    FP64 oracle, 1.4e-3 m). Mixed measured 1.7e-3 m, 807 vertices past 1e-4 m."""
     ref = steps["fp64", True]
-    d32, dmx, floor = _dist(steps["fp32", True], ref), _dist(steps["mixed", True], ref), _dist(steps["floor"], ref)
+    d32, dmx, floor = _dist(steps["fp32", True], ref), _dist(steps["mixed", True], ref), steps["floor"]
     n32, nmx, nfl = (int((d > 1e-4).sum()) for d in (d32, dmx, floor))
     assert nmx * 5 < n32, (nmx, n32)
     assert float(dmx.max()) < 1e-2
     assert float(floor.max()) > 1e-4 and nfl > 0  # the discontinuity is there in FP64 too
     assert float(dmx.max()) <= 3.0 * float(floor.max()), (float(dmx.max()), float(floor.max()))
+    assert nmx <= 3 * nfl, (nmx, nfl)
