@@ -168,8 +168,8 @@ class SolverVBD:
                 # lane 0. One large sheet (per-color schedule) has tens of edge-edge entries per vertex: 16 lanes
                 # measured fastest on a 256 x 256 sheet draped on a sphere, timed from one settled state (8.91 ms
                 # per substep against 9.22 ms with 8; 21 ms with one). Batched sheets (persistent schedule) have
-                # about one: 4 lanes measured fastest (2,048 sheets of 16 x 16: 16.5 ms against 18.6 ms with 2
-                # and 18.5 ms with 8; 256 of 32 x 32: 11.8 ms against 15.0 ms with 16)
+                # about one: 4 lanes measured fastest (2,048 sheets of 16 x 16 from one settled state: 16.5 ms
+                # against 18.9 ms with 2 and 18.4 ms with 8; 256 of 32 x 32: 11.8 ms against 15.0 ms with 16)
                 lanes_per_vertex = 4 if schedule == "persistent" else 16
         if model.body_count > 0 and not integrate_with_external_rigid_solver:
             raise NotImplementedError("rigid bodies (AVBD) are not part of this solver")
