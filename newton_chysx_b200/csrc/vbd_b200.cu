@@ -1014,17 +1014,21 @@ int sc_compact(ScBuffers& b, const int4* tri_idx, const int4* edge_idx, cudaStre
   int rc;
   k_sc_stored<<<(b.V + 256) / 256, 256, 0, st>>>(b.V, b.vb, b.vt_count, b.tmp);
   if ((rc = scan<int>(b, b.tmp, b.vt_off, b.V + 1, st))) return rc;
-  if (b.V) k_sc_pairs<<<(b.V + 255) / 256, 256, 0, st>>>(b.V, b.vb, b.vt_count, b.vt_tri, b.vt_off, b.vt_pairs);
+  if (b.V)
+    k_sc_pairs<false><<<(b.V + 255) / 256, 256, 0, st>>>(b.V, b.vb, b.vt_count, b.vt_tri, b.vt_off, tri_idx, edge_idx,
+                                                          b.vt_pairs);
   k_sc_stored<<<(b.E + 256) / 256, 256, 0, st>>>(b.E, b.eb, b.ee_count, b.tmp);
   if ((rc = scan<int>(b, b.tmp, b.ee_off, b.E + 1, st))) return rc;
-  if (b.E) k_sc_pairs<<<(b.E + 255) / 256, 256, 0, st>>>(b.E, b.eb, b.ee_count, b.ee_edge, b.ee_off, b.ee_pairs);
+  if (b.E)
+    k_sc_pairs<true><<<(b.E + 255) / 256, 256, 0, st>>>(b.E, b.eb, b.ee_count, b.ee_edge, b.ee_off, tri_idx, edge_idx,
+                                                         b.ee_pairs);
   CK(cudaMemsetAsync(b.ent_cnt, 0, sizeof(int) * (size_t(b.V) + 1), st));
-  k_sc_entries<false><<<kScGridBlocks, 256, 0, st>>>(tri_idx, edge_idx, b.vt_off + b.V, b.ee_off + b.E, b.vt_pairs,
-                                                      b.ee_pairs, b.ent_cnt, nullptr, nullptr, 0, b.flags);
+  k_sc_entries<false><<<kScGridBlocks, 256, 0, st>>>(b.vt_off + b.V, b.ee_off + b.E, b.vt_pairs, b.ee_pairs,
+                                                      b.ent_cnt, nullptr, nullptr, 0, b.flags);
   if ((rc = scan<int>(b, b.ent_cnt, b.ent_off, b.V + 1, st))) return rc;
   CK(cudaMemsetAsync(b.ent_cnt, 0, sizeof(int) * (size_t(b.V) + 1), st));
-  k_sc_entries<true><<<kScGridBlocks, 256, 0, st>>>(tri_idx, edge_idx, b.vt_off + b.V, b.ee_off + b.E, b.vt_pairs,
-                                                     b.ee_pairs, b.ent_cnt, b.ent_off, b.ent, b.ecap, b.flags);
+  k_sc_entries<true><<<kScGridBlocks, 256, 0, st>>>(b.vt_off + b.V, b.ee_off + b.E, b.vt_pairs, b.ee_pairs,
+                                                     b.ent_cnt, b.ent_off, b.ent, b.ecap, b.flags);
   k_sc_sort_entries<<<(b.V + 127) / 128, 128, 0, st>>>(b.V, b.ent_off, b.ent);
   CK(cudaGetLastError());
   return VBD_OK;
@@ -1069,8 +1073,8 @@ int sc_collide(VbdSolver* h, const R* q_state, cudaStream_t st) {
 template <typename R>
 void sc_truncate(VbdSolver* h, cudaStream_t st) {
   ScBuffers& b = h->sc;
-  k_sc_trunc_pairs<R><<<kScGridBlocks, 256, 0, st>>>(h->tri_idx, h->edge_idx, b.vt_off + b.V, b.ee_off + b.E,
-                                                      b.vt_pairs, b.ee_pairs, (const pos4_t<R>*)h->sc_pos_cd,
+  k_sc_trunc_pairs<R><<<kScGridBlocks, 256, 0, st>>>(b.vt_off + b.V, b.ee_off + b.E, b.vt_pairs, b.ee_pairs,
+                                                      (const pos4_t<R>*)h->sc_pos_cd,
                                                       (const pos4_t<R>*)h->sc_disp, R(h->sc_ee_eps), R(h->sc_relax),
                                                       (R*)h->sc_ts);
   k_sc_trunc_apply<R><<<(h->V + 255) / 256, 256, 0, st>>>(h->V, (R*)h->sc_ts, R(h->sc_margin * h->sc_relax * 0.5),
@@ -1173,9 +1177,8 @@ int step_impl(VbdSolver* h, R* q_in, R* q_out, const R* qd_in, R* qd_out, const 
     }
     PersistentPlan p{h->W, h->inst_order, h->inst_vstart, h->inst_cptr, h->color_ranges, h->color_verts, h->queue,
                      iters};
-    ScPersistentPlan s{h->sc_estart, h->sc.vt_off, h->sc.ee_off, h->sc.vt_pairs, h->sc.ee_pairs, h->tri_idx,
-                       h->edge_idx, h->sc_ts, h->sc_ee_eps, h->sc_relax, h->sc_margin * h->sc_relax * 0.5,
-                       0, 0, 0, 0};
+    ScPersistentPlan s{h->sc_estart, h->sc.vt_off, h->sc.ee_off, h->sc.vt_pairs, h->sc.ee_pairs, h->sc_ts,
+                       h->sc_ee_eps, h->sc_relax, h->sc_margin * h->sc_relax * 0.5, 0, 0, 0, 0};
     CK(cudaMemsetAsync(h->queue, 0, sizeof(int), st));
     launch_persistent_sc<R, MODE>(h->L, c, p, s, h->grid_sc, h->block, st);
     s.phase = 1;

@@ -53,9 +53,9 @@ struct ScBuffers {
   int tb = 0;
   int* tmp = nullptr;            // [max(V, E) + 1]
   int* vt_off = nullptr;         // [V + 1]
-  int2* vt_pairs = nullptr;      // [V * vb] (vertex, triangle)
+  int4* vt_pairs = nullptr;      // [V * vb] the pair's vertices: the triangle's three, then the vertex
   int* ee_off = nullptr;         // [E + 1]
-  int2* ee_pairs = nullptr;      // [E * eb] (edge, edge)
+  int4* ee_pairs = nullptr;      // [E * eb] the pair's vertices: the edge's two, then the other edge's two
   int* ent_cnt = nullptr;        // [V + 1] entries per vertex, then fill cursors
   int* ent_off = nullptr;        // [V + 1]
   unsigned* ent = nullptr;       // [ecap] (kind << 31) | (slot << 29) | pair
@@ -366,19 +366,33 @@ static __global__ void k_sc_stored(int P, int cap, const int* __restrict__ count
   if (i == P) tmp[i] = 0;
 }
 
-static __global__ void k_sc_pairs(int P, int cap, const int* __restrict__ count, const int* __restrict__ list,
-                           const int* __restrict__ off, int2* pairs) {
+// Dense pair lists: each pair stored as its four vertex ids, so that the solve and the truncation read a pair's
+// positions one load after its entry. VT (vertex i, triangle t): (t0, t1, t2, i); EE (edge i, edge j): the
+// vertices of i, then those of j.
+template <bool EE>
+__global__ void k_sc_pairs(int P, int cap, const int* __restrict__ count, const int* __restrict__ list,
+                           const int* __restrict__ off, const int4* __restrict__ tri_idx,
+                           const int4* __restrict__ edge_idx, int4* pairs) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P) return;
   const int n = min(count[i], cap), o = off[i];
-  for (int k = 0; k < n; ++k) pairs[o + k] = make_int2(i, list[size_t(i) * cap + k]);
+  const int4 a = EE ? __ldg(edge_idx + i) : make_int4(0, 0, 0, 0);
+  for (int k = 0; k < n; ++k) {
+    const int j = list[size_t(i) * cap + k];
+    if (EE) {
+      const int4 b = __ldg(edge_idx + j);
+      pairs[o + k] = make_int4(a.z, a.w, b.z, b.w);
+    } else {
+      const int4 t = __ldg(tri_idx + j);
+      pairs[o + k] = make_int4(t.x, t.y, t.z, i);
+    }
+  }
 }
 
 // Per-vertex entry lists. FILL == false counts, FILL == true writes through the cursors.
 template <bool FILL>
-__global__ void k_sc_entries(const int4* __restrict__ tri_idx, const int4* __restrict__ edge_idx,
-                             const int* __restrict__ n_vt, const int* __restrict__ n_ee, const int2* __restrict__ vt_pairs,
-                             const int2* __restrict__ ee_pairs, int* cnt, const int* __restrict__ off, unsigned* ent,
+__global__ void k_sc_entries(const int* __restrict__ n_vt, const int* __restrict__ n_ee, const int4* __restrict__ vt_pairs,
+                             const int4* __restrict__ ee_pairs, int* cnt, const int* __restrict__ off, unsigned* ent,
                              long long ecap, int* flags) {
   const int nv = *n_vt, ne = *n_ee;
   auto put = [&](int vert, unsigned code) {
@@ -393,18 +407,16 @@ __global__ void k_sc_entries(const int4* __restrict__ tri_idx, const int4* __res
   };
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv + ne; i += gridDim.x * blockDim.x) {
     if (i < nv) {
-      const int2 pr = vt_pairs[i];
-      const int4 t = __ldg(tri_idx + pr.y);
-      put(pr.x, (3u << 29) | unsigned(i));
-      put(t.x, (0u << 29) | unsigned(i));
-      put(t.y, (1u << 29) | unsigned(i));
-      put(t.z, (2u << 29) | unsigned(i));
+      const int4 q = vt_pairs[i];
+      put(q.w, (3u << 29) | unsigned(i));
+      put(q.x, (0u << 29) | unsigned(i));
+      put(q.y, (1u << 29) | unsigned(i));
+      put(q.z, (2u << 29) | unsigned(i));
     } else {
       const int j = i - nv;
-      const int2 pr = ee_pairs[j];
-      const int4 e = __ldg(edge_idx + pr.x);
-      put(e.z, 0x80000000u | (0u << 29) | unsigned(j));
-      put(e.w, 0x80000000u | (1u << 29) | unsigned(j));
+      const int4 q = ee_pairs[j];
+      put(q.x, 0x80000000u | (0u << 29) | unsigned(j));
+      put(q.y, 0x80000000u | (1u << 29) | unsigned(j));
     }
   }
 }
@@ -452,17 +464,10 @@ __device__ __forceinline__ void ts_min(double* ts, int i, double t) {
 // (apply_planar_truncation_parallel_by_collision, particle_vbd_kernels.py:2744-2874): the per-vertex minimum is
 // kept with an integer atomicMin on the fraction's bits (fractions lie in [0, 1]).
 template <typename R>
-__device__ __forceinline__ void trunc_pair(bool vt, int2 pr, const int4* __restrict__ tri_idx,
-                                           const int4* __restrict__ edge_idx, const pos4_t<R>* __restrict__ pos_cd,
+__device__ __forceinline__ void trunc_pair(bool vt, int4 q, const pos4_t<R>* __restrict__ pos_cd,
                                            const pos4_t<R>* __restrict__ disp, R eps, R gamma, R* ts) {
-  int ids[4];
-  if (vt) {
-    const int4 t = __ldg(tri_idx + pr.y);
-    ids[0] = pr.x, ids[1] = t.x, ids[2] = t.y, ids[3] = t.z;
-  } else {
-    const int4 a = __ldg(edge_idx + pr.x), b = __ldg(edge_idx + pr.y);
-    ids[0] = a.z, ids[1] = a.w, ids[2] = b.z, ids[3] = b.w;
-  }
+  // the vertex first for a VT pair (the planes' order), the stored order for an EE pair
+  const int ids[4] = {vt ? q.w : q.x, vt ? q.x : q.y, vt ? q.y : q.z, vt ? q.z : q.w};
   vec3<R> x[4], dx[4], n, d;
   bool cut[4];
 #pragma unroll
@@ -493,14 +498,13 @@ __device__ __forceinline__ void trunc_vertex(int i, R* ts, R max_d, const pos4_t
 }
 
 template <typename R>
-__global__ void k_sc_trunc_pairs(const int4* __restrict__ tri_idx, const int4* __restrict__ edge_idx,
-                                 const int* __restrict__ n_vt, const int* __restrict__ n_ee,
-                                 const int2* __restrict__ vt_pairs, const int2* __restrict__ ee_pairs,
+__global__ void k_sc_trunc_pairs(const int* __restrict__ n_vt, const int* __restrict__ n_ee,
+                                 const int4* __restrict__ vt_pairs, const int4* __restrict__ ee_pairs,
                                  const pos4_t<R>* __restrict__ pos_cd, const pos4_t<R>* __restrict__ disp, R eps, R gamma,
                                  R* ts) {
   const int nv = *n_vt, ne = *n_ee;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv + ne; i += gridDim.x * blockDim.x)
-    trunc_pair<R>(i < nv, i < nv ? vt_pairs[i] : ee_pairs[i - nv], tri_idx, edge_idx, pos_cd, disp, eps, gamma, ts);
+    trunc_pair<R>(i < nv, i < nv ? vt_pairs[i] : ee_pairs[i - nv], pos_cd, disp, eps, gamma, ts);
 }
 
 template <typename R>

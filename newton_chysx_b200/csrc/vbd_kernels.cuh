@@ -95,8 +95,8 @@ struct StepCtx {
   P4* pos_cd;         // positions at the last detection
   const int* ent_off;   // [V+1] per-vertex self-contact entries
   const unsigned* ent;  // (kind << 31) | (slot << 29) | pair
-  const int2* vt_pairs;  // (vertex, triangle)
-  const int2* ee_pairs;  // (edge, edge)
+  const int4* vt_pairs;  // per pair its vertices: (t0, t1, t2, vertex)
+  const int4* ee_pairs;  // per pair its vertices: (a0, a1, b0, b1)
   double sc_radius, sc_ee_eps;
   // springs and tetrahedra (solve_group<..., SOFT = true>)
   const int2* __restrict__ spr_idx;     // endpoints
@@ -342,16 +342,8 @@ template <typename R, typename P>
 __device__ __forceinline__ void self_contact_add(const StepCtx<R>& c, const P& pos, unsigned code, vec3<R>& f,
                                                  sym3<R>& H) {
   const int pair = int(code & 0x1FFFFFFFu), slot = int((code >> 29) & 3u);
-  int ids[4];
-  if (code >> 31) {
-    const int2 pr = __ldg(c.ee_pairs + pair);
-    const int4 a = __ldg(c.edge_idx + pr.x), b = __ldg(c.edge_idx + pr.y);
-    ids[0] = a.z, ids[1] = a.w, ids[2] = b.z, ids[3] = b.w;
-  } else {
-    const int2 pr = __ldg(c.vt_pairs + pair);
-    const int4 t = __ldg(c.tri_idx + pr.y);
-    ids[0] = t.x, ids[1] = t.y, ids[2] = t.z, ids[3] = pr.x;
-  }
+  const int4 q = __ldg((code >> 31 ? c.ee_pairs : c.vt_pairs) + pair);
+  const int ids[4] = {q.x, q.y, q.z, q.w};
   vec3<R> x[4], xa[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) x[k] = pos.ld(ids[k]), xa[k] = ld3<R>(c.qprev[ids[k]]);

@@ -21,8 +21,7 @@ __device__ __forceinline__ void truncate_instance(const StepCtx<R>& c, const ScP
   R* ts = static_cast<R*>(s.ts);
   const R eps = R(s.eps), gamma = R(s.gamma);
   for (int i = threadIdx.x; i < n; i += blockDim.x)
-    trunc_pair<R>(i < nv, i < nv ? s.vt_pairs[p0 + i] : s.ee_pairs[q0 + i - nv], s.tri_idx, s.edge_idx, c.pos_cd,
-                  c.disp, eps, gamma, ts);
+    trunc_pair<R>(i < nv, i < nv ? s.vt_pairs[p0 + i] : s.ee_pairs[q0 + i - nv], c.pos_cd, c.disp, eps, gamma, ts);
   __syncthreads();
   const R max_d = R(s.max_d);
   for (int i = vs + threadIdx.x; i < ve; i += blockDim.x) trunc_vertex<R>(i, ts, max_d, c.pos_cd, c.disp, c.pos);

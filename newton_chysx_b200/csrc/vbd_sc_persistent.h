@@ -11,10 +11,8 @@ struct ScPersistentPlan {
   const int* inst_estart;  // [W+1] the edges of instance w are [inst_estart[w], inst_estart[w+1])
   const int* vt_off;       // [V+1] VT pairs of vertex v: vt_pairs[vt_off[v] .. vt_off[v+1])
   const int* ee_off;       // [E+1] EE pairs of edge e: ee_pairs[ee_off[e] .. ee_off[e+1])
-  const int2* vt_pairs;
-  const int2* ee_pairs;
-  const int4* tri_idx;
-  const int4* edge_idx;
+  const int4* vt_pairs;    // per pair its four vertices (ScBuffers::vt_pairs, ee_pairs)
+  const int4* ee_pairs;
   void* ts;                // [V] R: per-vertex step fractions of the truncation, 1 between passes
   double eps, gamma, max_d;
   int phase;               // 0: forward step and truncation; 1: iterations [it0, it1)
